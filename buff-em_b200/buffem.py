@@ -1,0 +1,297 @@
+"""Python binding of libbuffem_b200.so (the C-ABI of include/buffem_b200.h).
+
+Mirrors the names of libbuff's C++ API so scripts read like the reference's
+drivers (buff-scatter.cc:236-347, unit-test-LFField.cc:50-71):
+
+    G = SWGGeometry("E10Sphere.buffgeo")          # SWGGeometry(const char*)
+    M = G.AllocateVIEMatrix()                     # VIEMatrix.cc:465-471
+    G.AssembleVIEMatrix(omega, M)                 # VIEMatrix.cc:431-460
+    M.LUFactorize()                               # HMatrix::LUFactorize
+    J = G.AssembleRHSVector(omega, PlaneWave(E0, nhat))   # RHSVector.cc:85-124
+    M.LUSolve(J)                                  # HMatrix::LUSolve
+    PFT = G.GetPFTMatrix(J, omega, PlaneWave(...))        # GetPFT.cc:133-189
+
+All compute runs in the CUDA library; there is no CPU fallback.  Loading the
+library succeeds without a GPU (for symbol checks); compute calls then raise
+BuffError with the library's message.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libbuffem_b200.so")
+_LIB = None
+
+BG_C128, BG_C64 = 0, 1
+BG_MAT_CONST_ISO, BG_MAT_CONST_TENSOR, BG_MAT_JANUS_Z, BG_MAT_GAUSSIAN = 0, 1, 2, 3
+BG_PFT_EMT, BG_PFT_OVERLAP = 0, 1
+PFT_PABS, PFT_PSCAT = 0, 1
+
+
+class BuffError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"[{status}] {msg}")
+        self.status = status
+
+
+class bg_material(C.Structure):
+    _fields_ = [("kind", C.c_int), ("eps", C.c_double * 18), ("eps2", C.c_double * 2),
+                ("center", C.c_double * 3), ("amp", C.c_double * 2), ("width", C.c_double)]
+
+
+def Material(kind=BG_MAT_CONST_ISO, eps=1.0, tensor=None, eps2=None, center=(0, 0, 0), amp=0.0, width=1.0):
+    """Permittivity functor (closed replacement for SVTensor / MatProp)."""
+    m = bg_material()
+    m.kind = kind
+    if tensor is not None:
+        t = np.asarray(tensor, dtype=np.complex128).reshape(3, 3)
+        for i in range(3):
+            for j in range(3):
+                m.eps[2 * (3 * i + j)] = t[i, j].real
+                m.eps[2 * (3 * i + j) + 1] = t[i, j].imag
+    else:
+        m.eps[0], m.eps[1] = complex(eps).real, complex(eps).imag
+    if eps2 is not None:
+        m.eps2[0], m.eps2[1] = complex(eps2).real, complex(eps2).imag
+    for i in range(3):
+        m.center[i] = center[i]
+    m.amp[0], m.amp[1] = complex(amp).real, complex(amp).imag
+    m.width = width
+    return m
+
+
+EXPORTS = [
+    "bg_last_error", "bg_geometry_create", "bg_geometry_create_objects", "bg_geometry_destroy",
+    "bg_geometry_num_bfs", "bg_geometry_num_objects", "bg_geometry_bf_offset", "bg_geometry_faces",
+    "bg_geometry_precompute", "bg_geometry_set_singular_order", "bg_geometry_near_data",
+    "bg_matrix_create", "bg_matrix_destroy", "bg_assemble", "bg_matrix_download", "bg_matrix_upload",
+    "bg_matrix_device_ptr", "bg_lu_factor", "bg_lu_pivots", "bg_lu_solve", "bg_lu_solve_device",
+    "bg_rhs_planewave", "bg_rhs_planewave_device", "bg_pft", "bg_kernel_launch_count",
+    "bg_synchronize", "bg_stream", "bg_profile_begin", "bg_profile_read", "bg_profile_end",
+]
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise BuffError(-4, f"{LIB_PATH} is not built (run `make -C buff-em_b200`)")
+        L = C.CDLL(LIB_PATH)
+        P, I, D, VP = C.c_void_p, C.c_int, C.c_double, C.c_void_p
+        L.bg_last_error.restype = C.c_char_p
+        L.bg_geometry_create.argtypes = [C.c_char_p, C.POINTER(P)]
+        L.bg_geometry_create_objects.argtypes = [I, C.POINTER(C.c_char_p), VP, C.POINTER(bg_material),
+                                                 C.POINTER(P)]
+        L.bg_geometry_destroy.argtypes = [P]
+        L.bg_geometry_destroy.restype = None
+        for f in ("bg_geometry_num_bfs", "bg_geometry_num_objects", "bg_geometry_precompute"):
+            getattr(L, f).argtypes = [P]
+        L.bg_geometry_bf_offset.argtypes = [P, I]
+        L.bg_geometry_faces.argtypes = [P, I, VP]
+        L.bg_geometry_set_singular_order.argtypes = [P, I]
+        L.bg_geometry_near_data.argtypes = [P, C.POINTER(I), VP, VP]
+        L.bg_matrix_create.argtypes = [P, I, C.POINTER(P)]
+        L.bg_matrix_destroy.argtypes = [P]
+        L.bg_matrix_destroy.restype = None
+        L.bg_assemble.argtypes = [P, D, D, P]
+        L.bg_matrix_download.argtypes = [P, VP]
+        L.bg_matrix_upload.argtypes = [P, VP]
+        L.bg_matrix_device_ptr.argtypes = [P, C.POINTER(VP), C.POINTER(I)]
+        L.bg_lu_factor.argtypes = [P]
+        L.bg_lu_pivots.argtypes = [P, VP]
+        L.bg_lu_solve.argtypes = [P, VP, I]
+        L.bg_lu_solve_device.argtypes = [P, VP, I, I]
+        L.bg_rhs_planewave.argtypes = [P, D, D, VP, VP, VP]
+        L.bg_rhs_planewave_device.argtypes = [P, D, D, VP, VP, VP]
+        L.bg_pft.argtypes = [P, D, D, VP, VP, VP, I, VP]
+        L.bg_kernel_launch_count.restype = C.c_longlong
+        L.bg_stream.restype = VP
+        L.bg_profile_read.argtypes = [I, VP, VP, VP]
+        _LIB = L
+    return _LIB
+
+
+def _check(st):
+    if st < 0:
+        raise BuffError(st, lib().bg_last_error().decode(errors="replace"))
+    return st
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class PlaneWave:
+    """Plane wave E = E0 exp(i k nhat.x) (SCUFF-EM PlaneWave(E0, nHat))."""
+
+    def __init__(self, E0, nHat):
+        self.E0 = np.ascontiguousarray(E0, dtype=np.complex128).reshape(3)
+        self.nHat = np.ascontiguousarray(nHat, dtype=np.float64).reshape(3)
+
+
+class HMatrix:
+    """Device-resident VIE matrix (replaces libhmat's HMatrix for this path)."""
+
+    def __init__(self, geom, precision=BG_C128):
+        self.G = geom
+        h = C.c_void_p()
+        _check(lib().bg_matrix_create(geom.h, precision, C.byref(h)))
+        self.h = h
+        self.NR = self.NC = geom.TotalBFs
+        self.precision = precision
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().bg_matrix_destroy(self.h)
+            self.h = None
+
+    def LUFactorize(self):
+        info = _check(lib().bg_lu_factor(self.h))
+        if info > 0:
+            raise BuffError(info, f"singular matrix: zero pivot at {info}")
+        return self
+
+    def LUSolve(self, B):
+        """Solve in place; B is an N-vector or N x nrhs complex array (Fortran order)."""
+        arr = B if isinstance(B, np.ndarray) else np.asarray(B)
+        if arr.dtype != np.complex128:
+            raise TypeError("LUSolve needs complex128")
+        nrhs = 1 if arr.ndim == 1 else arr.shape[1]
+        buf = np.asfortranarray(arr)
+        _check(lib().bg_lu_solve(self.h, _ptr(buf), nrhs))
+        if buf is not arr:
+            arr[...] = buf
+        return arr
+
+    def pivots(self):
+        p = np.zeros(self.NR, dtype=np.int32)
+        _check(lib().bg_lu_pivots(self.h, _ptr(p)))
+        return p
+
+    def download(self):
+        dt = np.complex128 if self.precision == BG_C128 else np.complex64
+        out = np.zeros((self.NR, self.NC), dtype=dt, order="F")
+        _check(lib().bg_matrix_download(self.h, _ptr(out)))
+        return out
+
+    def upload(self, A):
+        dt = np.complex128 if self.precision == BG_C128 else np.complex64
+        a = np.asfortranarray(A, dtype=dt)
+        _check(lib().bg_matrix_upload(self.h, _ptr(a)))
+
+    def device_ptr(self):
+        p = C.c_void_p()
+        ld = C.c_int()
+        _check(lib().bg_matrix_device_ptr(self.h, C.byref(p), C.byref(ld)))
+        return p.value, ld.value
+
+
+class SWGGeometry:
+    """Replaces buff::SWGGeometry (libbuff.h:200-272) for the VIE hot path."""
+
+    def __init__(self, GeoFileName=None, meshfiles=None, materials=None, displacements=None,
+                 singular_order=None):
+        h = C.c_void_p()
+        if GeoFileName is not None:
+            _check(lib().bg_geometry_create(GeoFileName.encode(), C.byref(h)))
+        else:
+            if isinstance(meshfiles, str):
+                meshfiles, materials = [meshfiles], [materials]
+            n = len(meshfiles)
+            names = (C.c_char_p * n)(*[m.encode() for m in meshfiles])
+            mats = (bg_material * n)(*materials)
+            self._disp = None
+            dptr = None
+            if displacements is not None:
+                self._disp = np.ascontiguousarray(displacements, dtype=np.float64).reshape(n, 3)
+                dptr = _ptr(self._disp)
+            _check(lib().bg_geometry_create_objects(n, names, dptr, mats, C.byref(h)))
+        self.h = h
+        self.TotalBFs = lib().bg_geometry_num_bfs(h)
+        self.NumObjects = lib().bg_geometry_num_objects(h)
+        self.BFIndexOffset = [lib().bg_geometry_bf_offset(h, i) for i in range(self.NumObjects + 1)]
+        if singular_order is not None:
+            _check(lib().bg_geometry_set_singular_order(h, int(singular_order)))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().bg_geometry_destroy(self.h)
+            self.h = None
+
+    def faces(self, obj=0):
+        n = self.BFIndexOffset[obj + 1] - self.BFIndexOffset[obj]
+        out = np.zeros((n, 9), dtype=np.int32)
+        _check(lib().bg_geometry_faces(self.h, obj, _ptr(out)))
+        return out
+
+    def precompute(self):
+        _check(lib().bg_geometry_precompute(self.h))
+
+    def near_data(self):
+        cnt = C.c_int()
+        _check(lib().bg_geometry_near_data(self.h, C.byref(cnt), None, None))
+        pairs = np.zeros((cnt.value, 2), dtype=np.int32)
+        data = np.zeros((cnt.value, 6), dtype=np.float64)
+        _check(lib().bg_geometry_near_data(self.h, C.byref(cnt), _ptr(pairs), _ptr(data)))
+        return pairs, data
+
+    def AllocateVIEMatrix(self, precision=BG_C128):
+        return HMatrix(self, precision)
+
+    def AssembleVIEMatrix(self, Omega, M=None):
+        if M is None:
+            M = self.AllocateVIEMatrix()
+        Omega = complex(Omega)
+        _check(lib().bg_assemble(self.h, Omega.real, Omega.imag, M.h))
+        return M
+
+    def AllocateRHSVector(self):
+        return np.zeros(self.TotalBFs, dtype=np.complex128)
+
+    def AssembleRHSVector(self, Omega, IF, RHS=None):
+        Omega = complex(Omega)
+        out = self.AllocateRHSVector() if RHS is None else RHS
+        _check(lib().bg_rhs_planewave(self.h, Omega.real, Omega.imag, _ptr(IF.E0), _ptr(IF.nHat), _ptr(out)))
+        return out
+
+    def GetPFTMatrix(self, J, Omega, IF=None, method=BG_PFT_EMT):
+        """Rows = objects, columns = (PAbs, PScat)."""
+        Omega = complex(Omega)
+        Jc = np.ascontiguousarray(J, dtype=np.complex128)
+        out = np.zeros((self.NumObjects, 2))
+        E0 = _ptr(IF.E0) if IF is not None else None
+        nh = _ptr(IF.nHat) if IF is not None else None
+        _check(lib().bg_pft(self.h, Omega.real, Omega.imag, _ptr(Jc), E0, nh, method, _ptr(out)))
+        return out
+
+
+def launch_count():
+    return lib().bg_kernel_launch_count()
+
+
+def synchronize():
+    _check(lib().bg_synchronize())
+
+
+PROF_CLASSES = ("lu_gemm", "lu_panel", "lu_laswp", "trsm_leaf")
+
+
+def profile_begin():
+    _check(lib().bg_profile_begin())
+
+
+def profile_read():
+    n = len(PROF_CLASSES)
+    cnt = np.zeros(n, dtype=np.int64)
+    ms = np.zeros(n)
+    fl = np.zeros(n)
+    _check(lib().bg_profile_read(n, _ptr(cnt), _ptr(ms), _ptr(fl)))
+    return {k: dict(launches=int(cnt[i]), ms=float(ms[i]), flops=float(fl[i])) for i, k in enumerate(PROF_CLASSES)}
+
+
+def profile_end():
+    _check(lib().bg_profile_end())

@@ -1,0 +1,408 @@
+// C-ABI entry points (include/buffem_b200.h).  Argument checking, ownership
+// and error reporting live here; all compute is dispatched to the CUDA
+// kernels.  No exception crosses the ABI; errors are status codes plus a
+// thread-local message.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+
+namespace bg {
+
+static thread_local std::string t_err;
+std::atomic<long long> g_launches{0};
+
+void set_error(const char *fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  t_err = buf;
+}
+
+static cudaStream_t s_stream = nullptr;
+static std::mutex s_mu;
+static int s_dev_ok = 0;
+
+int ensure_device() {
+  std::lock_guard<std::mutex> lk(s_mu);
+  if (s_dev_ok) return BG_OK;
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    set_error("no CUDA device available (%s); this library has no CPU fallback",
+              e == cudaSuccess ? "0 devices" : cudaGetErrorString(e));
+    return BG_ERR_CUDA;
+  }
+  int dev = 0;
+  BG_CUDA_TRY(cudaGetDevice(&dev));
+  cudaDeviceProp p;
+  BG_CUDA_TRY(cudaGetDeviceProperties(&p, dev));
+  if (p.major < 10) {
+    set_error("device %s (sm_%d%d) is not sm_100a; kernels are built for B200 only", p.name, p.major, p.minor);
+    return BG_ERR_CUDA;
+  }
+  BG_CUDA_TRY(cudaStreamCreateWithFlags(&s_stream, cudaStreamNonBlocking));
+  s_dev_ok = 1;
+  return BG_OK;
+}
+
+cudaStream_t stream() { return s_stream; }
+
+// ------------------------------------------------------------- profiling
+struct ProfRec { cudaEvent_t a, b; int cls; double flops; };
+static bool s_prof = false;
+static std::vector<ProfRec> s_recs;
+static std::vector<cudaEvent_t> s_pool;
+static cudaEvent_t s_open[PROF_NCLASS];
+static cudaEvent_t take_event() {
+  if (!s_pool.empty()) { cudaEvent_t e = s_pool.back(); s_pool.pop_back(); return e; }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+bool prof_on() { return s_prof; }
+void prof_start(int cls) {
+  if (!s_prof) return;
+  s_open[cls] = take_event();
+  cudaEventRecord(s_open[cls], s_stream);
+}
+void prof_stop(int cls, double flops) {
+  if (!s_prof) return;
+  cudaEvent_t e = take_event();
+  cudaEventRecord(e, s_stream);
+  s_recs.push_back(ProfRec{s_open[cls], e, cls, flops});
+}
+
+int parse_buffgeo(const char *path, std::vector<std::string> &meshes, std::vector<double> &disp,
+                  std::vector<bg_material> &mats);
+
+}  // namespace bg
+
+using namespace bg;
+
+extern "C" {
+
+const char *bg_last_error(void) { return t_err.c_str(); }
+
+static int finish_geometry(bg_geometry *g) {
+  g->bfOffset.assign(g->objs.size() + 1, 0);
+  g->vOffset.assign(g->objs.size() + 1, 0);
+  g->tOffset.assign(g->objs.size() + 1, 0);
+  for (size_t i = 0; i < g->objs.size(); i++) {
+    g->bfOffset[i + 1] = g->bfOffset[i] + g->objs[i].nif;
+    g->vOffset[i + 1] = g->vOffset[i] + g->objs[i].nv;
+    g->tOffset[i + 1] = g->tOffset[i] + g->objs[i].nt;
+  }
+  g->N = g->bfOffset.back();
+  g->NV = g->vOffset.back();
+  g->NT = g->tOffset.back();
+  if (g->N <= 0) { set_error("geometry has no interior faces"); return BG_ERR_ARG; }
+  return BG_OK;
+}
+
+static int check_material(const bg_material &m) {
+  if (m.kind < BG_MAT_CONST_ISO || m.kind > BG_MAT_GAUSSIAN) { set_error("unknown material kind %d", m.kind); return BG_ERR_ARG; }
+  if (m.kind == BG_MAT_GAUSSIAN && !(m.width > 0)) { set_error("gaussian material needs width > 0"); return BG_ERR_ARG; }
+  return BG_OK;
+}
+
+int bg_geometry_create_objects(int nobj, const char *const *meshfiles, const double *displacements,
+                               const bg_material *materials, bg_geometry **out) {
+  if (!out || nobj <= 0 || !meshfiles || !materials) { set_error("bg_geometry_create_objects: bad arguments"); return BG_ERR_ARG; }
+  *out = nullptr;
+  bg_geometry *g = new (std::nothrow) bg_geometry();
+  if (!g) { set_error("out of host memory"); return BG_ERR_NOMEM; }
+  g->objs.resize(nobj);
+  for (int i = 0; i < nobj; i++) {
+    if (!meshfiles[i]) { delete g; set_error("mesh file %d is NULL", i); return BG_ERR_ARG; }
+    int st = check_material(materials[i]);
+    if (!st) st = load_object(g->objs[i], meshfiles[i], displacements ? displacements + 3 * i : nullptr);
+    if (st) { delete g; return st; }
+    g->objs[i].mat = materials[i];
+  }
+  int st = finish_geometry(g);
+  if (st) { delete g; return st; }
+  *out = g;
+  return BG_OK;
+}
+
+int bg_geometry_create(const char *path, bg_geometry **out) {
+  if (!path || !out) { set_error("bg_geometry_create: bad arguments"); return BG_ERR_ARG; }
+  std::vector<std::string> meshes;
+  std::vector<double> disp;
+  std::vector<bg_material> mats;
+  int st = parse_buffgeo(path, meshes, disp, mats);
+  if (st) return st;
+  std::vector<const char *> names;
+  for (auto &s : meshes) names.push_back(s.c_str());
+  return bg_geometry_create_objects((int)meshes.size(), names.data(), disp.data(), mats.data(), out);
+}
+
+static void dfree(void *p) { if (p) cudaFree(p); }
+
+void bg_geometry_destroy(bg_geometry *g) {
+  if (!g) return;
+  DevGeom &d = g->dev;
+  dfree(d.V4); dfree(d.tetVI); dfree(d.tetVol); dfree(d.tetP4); dfree(d.tetObj); dfree(d.bfTet);
+  dfree(d.bfQ); dfree(d.bfLoc); dfree(d.tetFI); dfree(d.bfV); dfree(d.bfArea); dfree(d.bfRadius); dfree(d.mats); dfree(d.objOrigin);
+  NearData &n = g->near;
+  dfree(n.pairs); dfree(n.pairTP); dfree(n.fibbi); dfree(n.tp); dfree(n.tpOrdA); dfree(n.tpOrdB); dfree(n.tpMom);
+  dfree(g->d_scratch);
+  delete g;
+}
+
+int bg_geometry_num_bfs(const bg_geometry *g) { return g ? g->N : BG_ERR_ARG; }
+int bg_geometry_num_objects(const bg_geometry *g) { return g ? (int)g->objs.size() : BG_ERR_ARG; }
+int bg_geometry_bf_offset(const bg_geometry *g, int obj) {
+  if (!g || obj < 0 || obj > (int)g->objs.size()) { set_error("bad object index"); return BG_ERR_ARG; }
+  return g->bfOffset[obj];
+}
+
+int bg_geometry_faces(const bg_geometry *g, int obj, int *out) {
+  if (!g || !out || obj < 0 || obj >= (int)g->objs.size()) { set_error("bg_geometry_faces: bad arguments"); return BG_ERR_ARG; }
+  const Object &o = g->objs[obj];
+  for (int i = 0; i < o.nif; i++) {
+    const Face &F = o.F[i];
+    int *q = out + 9 * i;
+    q[0] = F.iV1; q[1] = F.iV2; q[2] = F.iV3; q[3] = F.iQP; q[4] = F.iQM;
+    q[5] = F.iPTet; q[6] = F.iMTet; q[7] = F.PIndex; q[8] = F.MIndex;
+  }
+  return BG_OK;
+}
+
+int bg_geometry_set_singular_order(bg_geometry *g, int n) {
+  if (!g || n < 2 || n > 16) { set_error("singular order must be in [2,16]"); return BG_ERR_ARG; }
+  if (g->precomputed && n != g->singular_order) { set_error("singular order must be set before the precompute"); return BG_ERR_STATE; }
+  g->singular_order = n;
+  return BG_OK;
+}
+
+int bg_geometry_precompute(bg_geometry *g) {
+  if (!g) { set_error("null geometry"); return BG_ERR_ARG; }
+  if (g->precomputed) return BG_OK;
+  int st = upload_geometry(g);
+  if (!st) st = build_near_lists(g);
+  if (!st) st = precompute_near(g);
+  if (!st) g->precomputed = true;
+  return st;
+}
+
+int bg_geometry_near_data(bg_geometry *g, int *count, int *pairs, double *data) {
+  if (!g || !count) { set_error("bg_geometry_near_data: bad arguments"); return BG_ERR_ARG; }
+  int st = bg_geometry_precompute(g);
+  if (st) return st;
+  *count = g->near.npairs;
+  if (pairs) BG_CUDA_TRY(cudaMemcpy(pairs, g->near.pairs, sizeof(int2) * g->near.npairs, cudaMemcpyDeviceToHost));
+  if (data) BG_CUDA_TRY(cudaMemcpy(data, g->near.fibbi, sizeof(double) * 6 * g->near.npairs, cudaMemcpyDeviceToHost));
+  return BG_OK;
+}
+
+int bg_matrix_create(bg_geometry *g, int precision, bg_matrix **out) {
+  if (!g || !out || (precision != BG_C128 && precision != BG_C64)) { set_error("bg_matrix_create: bad arguments"); return BG_ERR_ARG; }
+  *out = nullptr;
+  int st = ensure_device();
+  if (st) return st;
+  bg_matrix *m = new (std::nothrow) bg_matrix();
+  if (!m) { set_error("out of host memory"); return BG_ERR_NOMEM; }
+  m->g = g;
+  m->N = g->N;
+  m->precision = precision;
+  m->ld = (size_t)g->N;
+  size_t esz = precision == BG_C128 ? 16 : 8;
+  cudaError_t e = cudaMalloc(&m->d, esz * m->ld * (size_t)m->N);
+  if (e != cudaSuccess) {
+    delete m;
+    set_error("cannot allocate %.2f GB matrix on the device: %s", esz * (double)g->N * g->N / 1e9, cudaGetErrorString(e));
+    return BG_ERR_NOMEM;
+  }
+  e = cudaMalloc(&m->d_ipiv, sizeof(int) * (size_t)m->N);
+  if (e != cudaSuccess) { cudaFree(m->d); delete m; set_error("cannot allocate pivots"); return BG_ERR_NOMEM; }
+  *out = m;
+  return BG_OK;
+}
+
+void bg_matrix_destroy(bg_matrix *m) {
+  if (!m) return;
+  dfree(m->d); dfree(m->d_ipiv); dfree(m->d_work);
+  delete m;
+}
+
+int bg_assemble(bg_geometry *g, double wr, double wi, bg_matrix *m) {
+  if (!g || !m) { set_error("bg_assemble: null argument"); return BG_ERR_ARG; }
+  if (m->g != g && m->N != g->N) { set_error("wrong-size matrix passed to bg_assemble (%d != %d)", m->N, g->N); return BG_ERR_ARG; }
+  if (m->N != g->N) { set_error("wrong-size matrix passed to bg_assemble (%d != %d)", m->N, g->N); return BG_ERR_ARG; }
+  if (m->precision != BG_C128) { set_error("bg_assemble: only complex128 matrices are assembled here"); return BG_ERR_ARG; }
+  if (wr == 0.0 && wi == 0.0) { set_error("bg_assemble: omega must be nonzero"); return BG_ERR_ARG; }
+  int st = bg_geometry_precompute(g);
+  if (st) return st;
+  m->factored = false;
+  st = assemble_far(g, wr, wi, m->d, m->ld);
+  if (!st) st = assemble_near(g, wr, wi, m->d, m->ld);
+  if (!st) st = assemble_gram(g, wr, wi, m->d, m->ld);
+  return st;
+}
+
+int bg_matrix_download(const bg_matrix *m, void *host) {
+  if (!m || !host) { set_error("bg_matrix_download: bad arguments"); return BG_ERR_ARG; }
+  size_t esz = m->precision == BG_C128 ? 16 : 8;
+  BG_CUDA_TRY(cudaStreamSynchronize(stream()));
+  BG_CUDA_TRY(cudaMemcpy(host, m->d, esz * m->ld * (size_t)m->N, cudaMemcpyDeviceToHost));
+  return BG_OK;
+}
+
+int bg_matrix_upload(bg_matrix *m, const void *host) {
+  if (!m || !host) { set_error("bg_matrix_upload: bad arguments"); return BG_ERR_ARG; }
+  size_t esz = m->precision == BG_C128 ? 16 : 8;
+  BG_CUDA_TRY(cudaStreamSynchronize(stream()));
+  BG_CUDA_TRY(cudaMemcpy(m->d, host, esz * m->ld * (size_t)m->N, cudaMemcpyHostToDevice));
+  m->factored = false;
+  return BG_OK;
+}
+
+int bg_matrix_device_ptr(bg_matrix *m, void **dptr, int *ld) {
+  if (!m || !dptr || !ld) { set_error("bg_matrix_device_ptr: bad arguments"); return BG_ERR_ARG; }
+  *dptr = m->d;
+  *ld = (int)m->ld;
+  return BG_OK;
+}
+
+int bg_lu_factor(bg_matrix *m) {
+  if (!m) { set_error("bg_lu_factor: null matrix"); return BG_ERR_ARG; }
+  if (m->precision != BG_C128) { set_error("bg_lu_factor: complex128 matrices only"); return BG_ERR_ARG; }
+  int st = lu_factor(m);
+  if (st < 0) return st;
+  m->factored = true;
+  m->info = st;
+  return st;
+}
+
+int bg_lu_pivots(const bg_matrix *m, int *ipiv) {
+  if (!m || !ipiv) { set_error("bg_lu_pivots: bad arguments"); return BG_ERR_ARG; }
+  if (!m->factored) { set_error("matrix is not factored"); return BG_ERR_STATE; }
+  BG_CUDA_TRY(cudaStreamSynchronize(stream()));
+  BG_CUDA_TRY(cudaMemcpy(ipiv, m->d_ipiv, sizeof(int) * m->N, cudaMemcpyDeviceToHost));
+  return BG_OK;
+}
+
+int bg_lu_solve_device(bg_matrix *m, void *dB, int ldb, int nrhs) {
+  if (!m || !dB || nrhs <= 0 || ldb < m->N) { set_error("bg_lu_solve_device: bad arguments"); return BG_ERR_ARG; }
+  if (!m->factored) { set_error("bg_lu_solve: matrix is not LU-factored"); return BG_ERR_STATE; }
+  if (m->info > 0) { set_error("bg_lu_solve: factorization is singular (info=%d)", m->info); return BG_ERR_NUMERIC; }
+  return lu_solve(m, dB, ldb, nrhs);
+}
+
+int bg_lu_solve(bg_matrix *m, double *B, int nrhs) {
+  if (!m || !B || nrhs <= 0) { set_error("bg_lu_solve: bad arguments"); return BG_ERR_ARG; }
+  if (!m->factored) { set_error("bg_lu_solve: matrix is not LU-factored"); return BG_ERR_STATE; }
+  size_t bytes = 16 * (size_t)m->N * nrhs;
+  void *dB = nullptr;
+  BG_CUDA_TRY(cudaMallocAsync(&dB, bytes, stream()));
+  int st = BG_OK;
+  cudaError_t e = cudaMemcpyAsync(dB, B, bytes, cudaMemcpyHostToDevice, stream());
+  if (e != cudaSuccess) { set_error("H2D: %s", cudaGetErrorString(e)); st = BG_ERR_CUDA; }
+  if (!st) st = bg_lu_solve_device(m, dB, m->N, nrhs);
+  if (!st) {
+    e = cudaMemcpyAsync(B, dB, bytes, cudaMemcpyDeviceToHost, stream());
+    if (e != cudaSuccess) { set_error("D2H: %s", cudaGetErrorString(e)); st = BG_ERR_CUDA; }
+  }
+  cudaFreeAsync(dB, stream());
+  cudaError_t e2 = cudaStreamSynchronize(stream());
+  if (!st && e2 != cudaSuccess) { set_error("solve: %s", cudaGetErrorString(e2)); st = BG_ERR_CUDA; }
+  return st;
+}
+
+int bg_rhs_planewave_device(bg_geometry *g, double wr, double wi, const double *E0, const double *nhat, void *out) {
+  if (!g || !E0 || !nhat || !out) { set_error("bg_rhs_planewave: bad arguments"); return BG_ERR_ARG; }
+  if (wr == 0.0 && wi == 0.0) { set_error("bg_rhs_planewave: omega must be nonzero"); return BG_ERR_ARG; }
+  int st = upload_geometry(g);
+  if (st) return st;
+  return rhs_planewave(g, wr, wi, E0, nhat, out);
+}
+
+int bg_rhs_planewave(bg_geometry *g, double wr, double wi, const double *E0, const double *nhat, double *out) {
+  if (!g || !out) { set_error("bg_rhs_planewave: bad arguments"); return BG_ERR_ARG; }
+  int st = upload_geometry(g);
+  if (st) return st;
+  size_t bytes = 16 * (size_t)g->N;
+  void *d = nullptr;
+  BG_CUDA_TRY(cudaMallocAsync(&d, bytes, stream()));
+  st = bg_rhs_planewave_device(g, wr, wi, E0, nhat, d);
+  if (!st) {
+    cudaError_t e = cudaMemcpyAsync(out, d, bytes, cudaMemcpyDeviceToHost, stream());
+    if (e != cudaSuccess) { set_error("D2H: %s", cudaGetErrorString(e)); st = BG_ERR_CUDA; }
+  }
+  cudaFreeAsync(d, stream());
+  cudaError_t e2 = cudaStreamSynchronize(stream());
+  if (!st && e2 != cudaSuccess) { set_error("rhs: %s", cudaGetErrorString(e2)); st = BG_ERR_CUDA; }
+  return st;
+}
+
+int bg_pft(bg_geometry *g, double wr, double wi, const double *J, const double *E0, const double *nhat, int method,
+           double *out) {
+  if (!g || !J || !out || (method != BG_PFT_EMT && method != BG_PFT_OVERLAP)) { set_error("bg_pft: bad arguments"); return BG_ERR_ARG; }
+  if (method == BG_PFT_EMT && (!E0 || !nhat)) { set_error("bg_pft: EMT needs the incident plane wave"); return BG_ERR_ARG; }
+  int st = upload_geometry(g);
+  if (st) return st;
+  size_t bytes = 16 * (size_t)g->N;
+  void *d = nullptr;
+  BG_CUDA_TRY(cudaMallocAsync(&d, bytes, stream()));
+  cudaError_t e = cudaMemcpyAsync(d, J, bytes, cudaMemcpyHostToDevice, stream());
+  if (e != cudaSuccess) { set_error("H2D: %s", cudaGetErrorString(e)); st = BG_ERR_CUDA; }
+  if (!st) st = pft(g, wr, wi, d, E0, nhat, method, out);
+  cudaFreeAsync(d, stream());
+  cudaError_t e2 = cudaStreamSynchronize(stream());
+  if (!st && e2 != cudaSuccess) { set_error("pft: %s", cudaGetErrorString(e2)); st = BG_ERR_CUDA; }
+  return st;
+}
+
+long long bg_kernel_launch_count(void) { return g_launches.load(); }
+
+int bg_profile_begin(void) {
+  int st = ensure_device();
+  if (st) return st;
+  for (auto &r : s_recs) { s_pool.push_back(r.a); s_pool.push_back(r.b); }
+  s_recs.clear();
+  s_prof = true;
+  return BG_OK;
+}
+
+int bg_profile_read(int n, long long *counts, double *ms, double *flops) {
+  if (n <= 0 || !counts || !ms || !flops) { set_error("bg_profile_read: bad arguments"); return BG_ERR_ARG; }
+  BG_CUDA_TRY(cudaStreamSynchronize(s_stream));
+  for (int i = 0; i < n; i++) { counts[i] = 0; ms[i] = 0; flops[i] = 0; }
+  for (auto &r : s_recs) {
+    if (r.cls >= n) continue;
+    float t = 0;
+    BG_CUDA_TRY(cudaEventElapsedTime(&t, r.a, r.b));
+    counts[r.cls]++;
+    ms[r.cls] += t;
+    flops[r.cls] += r.flops;
+  }
+  return BG_OK;
+}
+
+int bg_profile_end(void) {
+  s_prof = false;
+  return BG_OK;
+}
+
+int bg_synchronize(void) {
+  int st = ensure_device();
+  if (st) return st;
+  BG_CUDA_TRY(cudaStreamSynchronize(stream()));
+  return BG_OK;
+}
+
+void *bg_stream(void) {
+  if (ensure_device()) return nullptr;
+  return (void *)stream();
+}
+
+}  // extern "C"

@@ -1,0 +1,147 @@
+// Internal declarations shared by the host geometry code, the C-ABI layer and
+// the CUDA kernels of the B200 BUFF-EM hot path.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/buffem_b200.h"
+
+namespace bg {
+
+// ---------------------------------------------------------------- errors
+void set_error(const char *fmt, ...);
+extern std::atomic<long long> g_launches;
+
+#define BG_CUDA_TRY(expr)                                                          \
+  do {                                                                             \
+    cudaError_t _e = (expr);                                                       \
+    if (_e != cudaSuccess) {                                                       \
+      ::bg::set_error("%s:%d: %s: %s", __FILE__, __LINE__, #expr,                  \
+                      cudaGetErrorString(_e));                                     \
+      return BG_ERR_CUDA;                                                          \
+    }                                                                              \
+  } while (0)
+
+#define BG_LAUNCHED()                                                              \
+  do {                                                                             \
+    ::bg::g_launches.fetch_add(1, std::memory_order_relaxed);                      \
+    cudaError_t _e = cudaGetLastError();                                           \
+    if (_e != cudaSuccess) {                                                       \
+      ::bg::set_error("%s:%d: kernel launch: %s", __FILE__, __LINE__,              \
+                      cudaGetErrorString(_e));                                     \
+      return BG_ERR_CUDA;                                                          \
+    }                                                                              \
+  } while (0)
+
+cudaStream_t stream();
+int ensure_device();
+
+// kernel-class profiling (CUDA events around launches when enabled)
+enum { PROF_GEMM = 0, PROF_PANEL = 1, PROF_LASWP = 2, PROF_TRSM = 3, PROF_NCLASS = 8 };
+bool prof_on();
+void prof_start(int cls);
+void prof_stop(int cls, double flops);
+
+// ---------------------------------------------------------------- host mesh
+struct Face {
+  int iV1, iV2, iV3, iQP, iQM, iPTet, iMTet, PIndex, MIndex, Index;
+  double cen[3], area, radius;
+};
+
+struct Object {
+  std::string meshfile;
+  int nv = 0, nt = 0, nif = 0, ntf = 0;
+  std::vector<double> V;       // 3*nv (after displacement)
+  std::vector<int> VI, FI;     // 4*nt each
+  std::vector<double> vol;     // signed volume per tet
+  std::vector<Face> F;         // interior faces first
+  bg_material mat{};
+  double origin[3] = {0, 0, 0};
+};
+
+// Reads a gmsh mesh (ReadGMSHFile.cc:66-261) and builds the face list
+// (InitFaceList.cc:69-279).  Returns BG_OK or an error status.
+int load_object(Object &o, const char *meshfile, const double *disp);
+
+// ---------------------------------------------------------------- device SoA
+// All indices are global over the objects of a geometry (vertex and tet
+// indices carry per-object offsets), so basis functions of different objects
+// never share a vertex index, matching CompareBFs' OA != OB rule.
+struct DevGeom {
+  int N = 0, NT = 0, NV = 0;
+  double *V4 = nullptr;      // 4 doubles per vertex (x, y, z, 0)
+  int4 *tetVI = nullptr;     // global vertex indices
+  double *tetVol = nullptr;  // signed volume
+  double *tetP4 = nullptr;   // 4-point rule points: 16 doubles per tet (x,y,z,0)*4
+  int *tetObj = nullptr;
+  // per basis function (global index a), side s in {0: P, 1: M}
+  int2 *bfTet = nullptr;     // (PTet, MTet) global tet indices
+  int2 *bfQ = nullptr;       // (QP, QM) global vertex indices
+  int2 *bfLoc = nullptr;     // (PIndex, MIndex): local index of Q in each tet
+  int4 *tetFI = nullptr;     // global basis-function index of the face opposite vertex k, -1 if exterior
+  int4 *bfV = nullptr;       // (V1, V2, V3, obj)
+  double *bfArea = nullptr;
+  double *bfRadius = nullptr;
+  bg_material *mats = nullptr;  // per object
+  double *objOrigin = nullptr;  // 3 per object
+};
+
+struct NearData {
+  // near basis-function pairs (same object, >=1 common vertex), a <= b
+  int npairs = 0;
+  int2 *pairs = nullptr;       // (a, b)
+  int4 *pairTP = nullptr;      // indices of the 4 tet pairs (PP, PM, MP, MM); sign bit 30 => swapped
+  double *fibbi = nullptr;     // 6 per pair
+  // distinct tetrahedron pairs feeding the near pairs
+  int ntp = 0, ntp_reg = 0;    // first ntp_reg are regular (<=1 common vertex)
+  int4 *tp = nullptr;          // (tA, tB, c, 0); singular pairs: vertex order in tpOrd
+  int4 *tpOrdA = nullptr, *tpOrdB = nullptr;  // common-first vertex orders (global vertex ids)
+  double *tpMom = nullptr;     // 24 moments per tet pair
+};
+
+}  // namespace bg
+
+struct bg_geometry {
+  std::vector<bg::Object> objs;
+  std::vector<int> bfOffset, vOffset, tOffset;
+  int N = 0, NV = 0, NT = 0;
+  bg::DevGeom dev;
+  bg::NearData near;
+  int singular_order = 10;
+  bool uploaded = false, precomputed = false;
+  double *d_scratch = nullptr;  // general scratch (PFT partial sums etc.)
+  size_t scratch_bytes = 0;
+};
+
+struct bg_matrix {
+  bg_geometry *g = nullptr;
+  int N = 0, precision = BG_C128;
+  size_t ld = 0;
+  void *d = nullptr;
+  int *d_ipiv = nullptr;       // 1-based pivots (LAPACK)
+  bool factored = false;
+  int info = 0;
+  void *d_work = nullptr;      // LU workspace
+  size_t work_bytes = 0;
+};
+
+namespace bg {
+// kernels entry points (implemented in .cu files); all return BG status
+int upload_geometry(bg_geometry *g);
+int build_near_lists(bg_geometry *g);
+int precompute_near(bg_geometry *g);
+int assemble_far(bg_geometry *g, double wr, double wi, void *M, size_t ld);
+int assemble_near(bg_geometry *g, double wr, double wi, void *M, size_t ld);
+int assemble_gram(bg_geometry *g, double wr, double wi, void *M, size_t ld);
+int rhs_planewave(bg_geometry *g, double wr, double wi, const double *E0, const double *nhat, void *out);
+int pft(bg_geometry *g, double wr, double wi, const void *dJ, const double *E0, const double *nhat, int method,
+        double *out);
+int lu_factor(bg_matrix *m);
+int lu_solve(bg_matrix *m, void *dB, int ldb, int nrhs);
+void gauss_legendre01(int n, double *x, double *w);
+}  // namespace bg

@@ -1,0 +1,1096 @@
+// sm_100a kernels of the VIE assembly path: far-field G entries, the
+// frequency-independent near-field integrals (regular 16x16 rule and the
+// singular relative-coordinate rule, both as tetrahedron-pair moments), the
+// per-frequency near entries, V^-1 Gram blocks, plane-wave RHS and the
+// absorbed/scattered power (EMT and overlap).
+//
+// Reference semantics (HomerReid/buff-em, src/libs/libbuff):
+//   GMatrixElements.cc:59-167,270-424   kernels and dispatcher
+//   Cubature.cc:161-527, TetCR.cc:35-95 fixed tetrahedron rules
+//   VIEMatrix.cc:51-72,122-316,321-460  Gram blocks and assembly
+//   RHSVector.cc:62-124                 plane-wave RHS
+//   EMTPFT.cc:151-493, OPFT.cc:62-119   power
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "internal.h"
+
+namespace bg {
+
+// ----------------------------------------------------------------- tables
+// Fixed tetrahedron rules (TetCR.cc:35-95): points (u1,u2,u3) in the unit
+// simplex, weights summing to 1/6.  All orbits are complete, so the point set
+// does not depend on which vertex is taken as origin.
+__constant__ double c_tcr16[64];
+__constant__ double c_tcr33[132];
+__constant__ double c_glx[16], c_glw[16];   // Gauss-Legendre on [0,1], current singular order
+static double h_tcr16[64], h_tcr33[132];
+static int s_tables_ok = 0, s_gl_n = 0;
+
+static void fill_rule(double *dst, const char *pat, const double *vals, double w, int *np) {
+  for (const char *p = pat; *p;) {
+    if (*p == ' ') { p++; continue; }
+    double *q = dst + 4 * (*np);
+    q[0] = vals[p[0] - 'A']; q[1] = vals[p[1] - 'A']; q[2] = vals[p[2] - 'A']; q[3] = w;
+    (*np)++;
+    p += 3;
+  }
+}
+
+static int init_tables() {
+  if (s_tables_ok) return BG_OK;
+  int np;
+  const double v16[5] = {0.771642902067237, 0.076119032644254315, 0.07183164526766925, 0.11970052779780202,
+                         0.40423391346726440};
+  np = 0;
+  fill_rule(h_tcr16, "ABB BAB BBA BBB", v16, 8.3956323500204695e-3, &np);
+  fill_rule(h_tcr16, "CDE CED CEE DCE DEC DEE ECD ECE EDC EDE EEC EED", v16, 0.011090344772215399, &np);
+  const double v33[11] = {0.25, 0.31407428362944793, 0.05777714911165610, 0.06254680497480394,
+                          0.81235958507558810, 0.04120213879937276, 0.30021473119185615, 0.61738099120939840,
+                          0.05292032110257111, 0.25198057383388334, 0.44311853122966216};
+  np = 0;
+  fill_rule(h_tcr33, "AAA", v33, 0.017783308938202055, &np);
+  fill_rule(h_tcr33, "BBB CBB BCB BBC", v33, -0.019099406118263309, &np);
+  fill_rule(h_tcr33, "DDD EDD DED DDE", v33, 3.8252276536630236e-3, &np);
+  fill_rule(h_tcr33, "FFG FFH FGF FGH FHF FHG GFF GFH GHF HFF HFG HGF", v33, 0.0035475499144103266, &np);
+  fill_rule(h_tcr33, "IJJ IJK IKJ JIJ JIK JJI JJK JKI JKJ KIJ KJI KJJ", v33, 0.013950789384495153, &np);
+  BG_CUDA_TRY(cudaMemcpyToSymbol(c_tcr16, h_tcr16, sizeof h_tcr16));
+  BG_CUDA_TRY(cudaMemcpyToSymbol(c_tcr33, h_tcr33, sizeof h_tcr33));
+  s_tables_ok = 1;
+  return BG_OK;
+}
+
+void gauss_legendre01(int n, double *x, double *w) {
+  for (int i = 0; i < n; i++) {
+    double z = std::cos(M_PI * (i + 0.75) / (n + 0.5)), pp = 0.0;
+    for (int it = 0; it < 100; it++) {
+      double p1 = 1.0, p2 = 0.0;
+      for (int j = 1; j <= n; j++) {
+        double p3 = p2;
+        p2 = p1;
+        p1 = ((2.0 * j - 1.0) * z * p2 - (j - 1.0) * p3) / j;
+      }
+      pp = n * (z * p1 - p2) / (z * z - 1.0);
+      double z1 = z;
+      z = z1 - p1 / pp;
+      if (std::fabs(z - z1) < 1e-16) break;
+    }
+    x[i] = 0.5 * (1.0 - z);
+    w[i] = 1.0 / ((1.0 - z * z) * pp * pp);
+  }
+}
+
+static int set_gl(int n) {
+  if (s_gl_n == n) return BG_OK;
+  double x[16] = {0}, w[16] = {0};
+  gauss_legendre01(n, x, w);
+  BG_CUDA_TRY(cudaMemcpyToSymbol(c_glx, x, sizeof x));
+  BG_CUDA_TRY(cudaMemcpyToSymbol(c_glw, w, sizeof w));
+  s_gl_n = n;
+  return BG_OK;
+}
+
+// ----------------------------------------------------------------- complex
+struct cd { double r, i; };
+__device__ __forceinline__ cd cmk(double r, double i) { return cd{r, i}; }
+__device__ __forceinline__ cd cadd(cd a, cd b) { return cd{a.r + b.r, a.i + b.i}; }
+__device__ __forceinline__ cd csub(cd a, cd b) { return cd{a.r - b.r, a.i - b.i}; }
+__device__ __forceinline__ cd cmul(cd a, cd b) { return cd{a.r * b.r - a.i * b.i, a.r * b.i + a.i * b.r}; }
+__device__ __forceinline__ cd cscale(cd a, double s) { return cd{a.r * s, a.i * s}; }
+__device__ __forceinline__ cd cdiv(cd a, cd b) {
+  double d = b.r * b.r + b.i * b.i;
+  return cd{(a.r * b.r + a.i * b.i) / d, (a.i * b.r - a.r * b.i) / d};
+}
+__device__ __forceinline__ double cnorm2(cd a) { return a.r * a.r + a.i * a.i; }
+// exp(i k r) for complex k
+__device__ __forceinline__ cd expikr(cd k, double r) {
+  double s, c;
+  sincos(k.r * r, &s, &c);
+  double m = (k.i == 0.0) ? 1.0 : exp(-k.i * r);
+  return cd{m * c, m * s};
+}
+
+// e^x - 1 - x - x^2/2: GetExpRelTable(x,3,3), GMatrixElements.cc:59-93 -- the
+// series from n=4 is stopped once |term|^2 < 1e-16 |sum|^2 (or n = 100).
+__device__ __forceinline__ cd exprel3(cd x) {
+  cd term = cmul(cscale(x, 0.5), x);   // x^2/2
+  term = cmul(term, cscale(x, 1.0 / 3.0));
+  cd first = term, sum = cmk(0, 0);
+  for (int n = 4; n < 100; n++) {
+    term = cmul(term, cscale(x, 1.0 / n));
+    sum = cadd(sum, term);
+    if (cnorm2(term) < 1.0e-16 * cnorm2(sum)) break;
+  }
+  return cadd(first, sum);
+}
+
+// permittivity functor (SVTensor::Evaluate semantics, SVTensor.cc:306-373)
+__device__ void mat_eval(const bg_material &m, const double *x, cd E[3][3]) {
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) E[i][j] = cmk(0, 0);
+  if (m.kind == BG_MAT_CONST_TENSOR) {
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) E[i][j] = cmk(m.eps[2 * (3 * i + j)], m.eps[2 * (3 * i + j) + 1]);
+    for (int mu = 0; mu < 3; mu++) {
+      int nu = (mu + 1) % 3;
+      cd a = cscale(cadd(E[mu][nu], E[nu][mu]), 0.5);
+      E[mu][nu] = E[nu][mu] = a;
+    }
+    return;
+  }
+  cd e;
+  if (m.kind == BG_MAT_CONST_ISO) e = cmk(m.eps[0], m.eps[1]);
+  else if (m.kind == BG_MAT_JANUS_Z) e = (x[2] > m.center[2]) ? cmk(m.eps[0], m.eps[1]) : cmk(m.eps2[0], m.eps2[1]);
+  else {
+    double d0 = x[0] - m.center[0], d1 = x[1] - m.center[1], d2 = x[2] - m.center[2];
+    double r2 = (d0 * d0 + d1 * d1 + d2 * d2) / (m.width * m.width);
+    double g = exp(-r2);
+    e = cmk(m.eps[0] + m.amp[0] * g, m.eps[1] + m.amp[1] * g);
+  }
+  E[0][0] = E[1][1] = E[2][2] = e;
+}
+
+// Invert3x3Matrix, VIEMatrix.cc:51-72
+__device__ void inv3(cd M[3][3], cd W[3][3]) {
+  cd M11 = M[0][0], M12 = M[0][1], M13 = M[0][2];
+  cd M21 = M[1][0], M22 = M[1][1], M23 = M[1][2];
+  cd M31 = M[2][0], M32 = M[2][1], M33 = M[2][2];
+  cd Det = csub(csub(csub(cadd(cadd(cmul(cmul(M12, M23), M31), cmul(cmul(M13, M21), M32)), cmul(cmul(M11, M22), M33)),
+                          cmul(cmul(M13, M22), M31)),
+                     cmul(cmul(M11, M23), M32)),
+                cmul(cmul(M12, M21), M33));
+  W[0][0] = cdiv(csub(cmul(M22, M33), cmul(M23, M32)), Det);
+  W[0][1] = cdiv(csub(cmul(M13, M32), cmul(M12, M33)), Det);
+  W[0][2] = cdiv(csub(cmul(M12, M23), cmul(M13, M22)), Det);
+  W[1][0] = cdiv(csub(cmul(M23, M31), cmul(M21, M33)), Det);
+  W[1][1] = cdiv(csub(cmul(M11, M33), cmul(M13, M31)), Det);
+  W[1][2] = cdiv(csub(cmul(M13, M21), cmul(M11, M23)), Det);
+  W[2][0] = cdiv(csub(cmul(M21, M32), cmul(M22, M31)), Det);
+  W[2][1] = cdiv(csub(cmul(M12, M31), cmul(M11, M32)), Det);
+  W[2][2] = cdiv(csub(cmul(M11, M22), cmul(M12, M21)), Det);
+}
+
+__device__ __forceinline__ void load3(const double *V4, int v, double *x) {
+  x[0] = V4[4 * v]; x[1] = V4[4 * v + 1]; x[2] = V4[4 * v + 2];
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// =========================================================================
+// far field: one thread per basis-function pair (a <= b) with no common
+// vertex; 4 tetrahedron pairs x 4x4 points of the Helmholtz kernel
+// (GetGME_BFBFInt, GMatrixElements.cc:270-288; BFBFInt, Cubature.cc:476-527).
+// With w = 6V w_i (w_i = 1/24) and b = +-A/(3V)(x - Q) the volume cancels:
+//   w_a b_a . w_b b_b = s_a s_b A_a A_b (x-Q_a).(y-Q_b)/144,
+//   w_a Div b_a w_b Div b_b = s_a s_b A_a A_b / 16.
+// =========================================================================
+#define FT 16
+struct BFSide {   // staged per basis function and side
+  double pts[4][3];
+  double q[3];
+  double coef;    // +-area
+};
+
+__global__ void __launch_bounds__(FT * FT) k_far(DevGeom g, cd k, cd invk2, cd *M, size_t ld) {
+  int bx = blockIdx.x, by = blockIdx.y;
+  if (bx > by) return;
+  __shared__ BFSide sA[FT][2], sB[FT][2];
+  __shared__ int vA[FT][5], vB[FT][5];
+  int tid = threadIdx.y * FT + threadIdx.x;
+  // stage rows (a) and columns (b)
+  if (tid < 4 * FT) {
+    int which = tid / (2 * FT);           // 0: rows, 1: cols
+    int r = (tid % (2 * FT)) / 2, s = tid % 2;
+    int bf = (which == 0 ? bx : by) * FT + r;
+    BFSide *dst = which == 0 ? &sA[r][s] : &sB[r][s];
+    if (bf < g.N) {
+      int2 tt = g.bfTet[bf];
+      int2 qq = g.bfQ[bf];
+      int t = s == 0 ? tt.x : tt.y, q = s == 0 ? qq.x : qq.y;
+      for (int i = 0; i < 4; i++)
+        for (int c = 0; c < 3; c++) dst->pts[i][c] = g.tetP4[16 * (size_t)t + 4 * i + c];
+      load3(g.V4, q, dst->q);
+      dst->coef = (s == 0 ? 1.0 : -1.0) * g.bfArea[bf];
+      if (s == 0) {
+        int4 v = g.bfV[bf];
+        int *vv = which == 0 ? vA[r] : vB[r];
+        vv[0] = qq.x; vv[1] = v.x; vv[2] = v.y; vv[3] = v.z; vv[4] = qq.y;
+      }
+    }
+  }
+  __syncthreads();
+  int ra = threadIdx.x, rb = threadIdx.y;
+  int a = bx * FT + ra, b = by * FT + rb;
+  if (a >= g.N || b >= g.N || a > b) return;
+  // CompareBFs (SWGVolume.cc:295-344): pairs with a common vertex are near
+  int ncv = 0;
+#pragma unroll
+  for (int i = 0; i < 5; i++)
+#pragma unroll
+    for (int j = 0; j < 5; j++) ncv += (vA[ra][i] == vB[rb][j]);
+  if (ncv) return;
+  cd acc = cmk(0, 0);
+  const double inv4pi = 0.25 / M_PI;
+#pragma unroll 1
+  for (int sa = 0; sa < 2; sa++)
+#pragma unroll 1
+    for (int sb = 0; sb < 2; sb++) {
+      const BFSide &A = sA[ra][sa];
+      const BFSide &B = sB[rb][sb];
+      double cc = A.coef * B.coef;
+      cd part = cmk(0, 0);
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        double xa0 = A.pts[i][0], xa1 = A.pts[i][1], xa2 = A.pts[i][2];
+        double da0 = xa0 - A.q[0], da1 = xa1 - A.q[1], da2 = xa2 - A.q[2];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          double R0 = xa0 - B.pts[j][0], R1 = xa1 - B.pts[j][1], R2 = xa2 - B.pts[j][2];
+          double r = sqrt(R0 * R0 + R1 * R1 + R2 * R2);
+          if (r < 1.0e-12) continue;
+          double dot = da0 * (B.pts[j][0] - B.q[0]) + da1 * (B.pts[j][1] - B.q[1]) + da2 * (B.pts[j][2] - B.q[2]);
+          cd phi = cscale(expikr(k, r), inv4pi / r);
+          // PEFIE = dot/144 - invk2/16
+          cd pe = cmk(dot * (1.0 / 144.0) - invk2.r * (1.0 / 16.0), -invk2.i * (1.0 / 16.0));
+          part = cadd(part, cmul(pe, phi));
+        }
+      }
+      acc = cadd(acc, cscale(part, cc));
+    }
+  M[(size_t)a + (size_t)b * ld] = acc;
+  if (a != b) M[(size_t)b + (size_t)a * ld] = acc;
+}
+
+int assemble_far(bg_geometry *g, double wr, double wi, void *M, size_t ld) {
+  int st = init_tables();
+  if (st) return st;
+  cd k{wr, wi};
+  // 1/k^2
+  double d = (wr * wr - wi * wi) * (wr * wr - wi * wi) + 4 * wr * wr * wi * wi;
+  cd invk2{(wr * wr - wi * wi) / d, -2 * wr * wi / d};
+  int nb = (g->N + FT - 1) / FT;
+  dim3 grid(nb, nb), block(FT, FT);
+  k_far<<<grid, block, 0, stream()>>>(g->dev, k, invk2, (cd *)M, ld);
+  BG_LAUNCHED();
+  return BG_OK;
+}
+
+// =========================================================================
+// near field, frequency independent: tetrahedron-pair moments
+//   M0 = sum K,  M1 = sum K (x-o_A),  M1' = sum K (y-o_B),  M2 = sum K (x-o_A).(y-o_B)
+// for K in {1/(4 pi r), 1/(4 pi), r/(8 pi)} (GMEIntegrand KERNEL_STATIC,
+// GMatrixElements.cc:153-165), in the unit-simplex measure (rule weights sum
+// to 1/6 per tetrahedron).  Layout: 24 doubles per pair, [kernel][M0, M1(3),
+// M1'(3), M2].  The per-basis-function-pair numbers of
+// GetGME_TetTetInt(KERNEL_STATIC) follow from
+//   int (x-Q).(y-Q') K = M2 - q.M1' - q'.M1 + q.q' M0,  q = Q-o_A, q' = Q'-o_B.
+// =========================================================================
+
+// regular pairs (<= 1 common vertex): 16x16 rule (GMatrixElements.cc:329-341),
+// one warp per tetrahedron pair, origins o_A, o_B = first vertex of each tet.
+__global__ void k_tp_regular(DevGeom g, const int4 *tp, int ntp, double *mom) {
+  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= ntp) return;
+  int4 p = tp[warp];
+  int4 A = g.tetVI[p.x], B = g.tetVI[p.y];
+  double oA[3], oB[3], LA[3][3], LB[3][3];
+  load3(g.V4, A.x, oA); load3(g.V4, B.x, oB);
+  int va[3] = {A.y, A.z, A.w}, vb[3] = {B.y, B.z, B.w};
+  for (int i = 0; i < 3; i++) {
+    double t[3];
+    load3(g.V4, va[i], t);
+    for (int c = 0; c < 3; c++) LA[i][c] = t[c] - oA[c];
+    load3(g.V4, vb[i], t);
+    for (int c = 0; c < 3; c++) LB[i][c] = t[c] - oB[c];
+  }
+  double d0 = oA[0] - oB[0], d1 = oA[1] - oB[1], d2 = oA[2] - oB[2];
+  double acc[24];
+#pragma unroll
+  for (int i = 0; i < 24; i++) acc[i] = 0.0;
+  const double inv4pi = 0.25 / M_PI, inv8pi = 0.125 / M_PI;
+  for (int idx = lane; idx < 256; idx += 32) {
+    int i = idx >> 4, j = idx & 15;
+    double xa[3], yb[3];
+    for (int c = 0; c < 3; c++) {
+      xa[c] = c_tcr16[4 * i] * LA[0][c] + c_tcr16[4 * i + 1] * LA[1][c] + c_tcr16[4 * i + 2] * LA[2][c];
+      yb[c] = c_tcr16[4 * j] * LB[0][c] + c_tcr16[4 * j + 1] * LB[1][c] + c_tcr16[4 * j + 2] * LB[2][c];
+    }
+    double w = c_tcr16[4 * i + 3] * c_tcr16[4 * j + 3];
+    double R0 = d0 + xa[0] - yb[0], R1 = d1 + xa[1] - yb[1], R2 = d2 + xa[2] - yb[2];
+    double r = sqrt(R0 * R0 + R1 * R1 + R2 * R2);
+    if (r < 1.0e-12) continue;
+    double K[3] = {inv4pi / r, inv4pi, r * inv8pi};
+    double xy = xa[0] * yb[0] + xa[1] * yb[1] + xa[2] * yb[2];
+#pragma unroll
+    for (int pk = 0; pk < 3; pk++) {
+      double wk = w * K[pk];
+      acc[8 * pk] += wk;
+      acc[8 * pk + 1] += wk * xa[0]; acc[8 * pk + 2] += wk * xa[1]; acc[8 * pk + 3] += wk * xa[2];
+      acc[8 * pk + 4] += wk * yb[0]; acc[8 * pk + 5] += wk * yb[1]; acc[8 * pk + 6] += wk * yb[2];
+      acc[8 * pk + 7] += wk * xy;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 24; i++) acc[i] = warp_sum(acc[i]);
+  if (lane == 0)
+    for (int i = 0; i < 24; i++) mom[24 * (size_t)warp + i] = acc[i];
+}
+
+// singular pairs (2..4 common vertices): relative-coordinate polar rule
+// (replaces the Taylor-Duffy call, GMatrixElements.cc:174-263,343-353).
+// Barycentrics lambda (A) and mu (B), common vertices first.  With
+// d = (lambda_k - mu_k | lambda_A-own | -mu_B-own), x - y is linear and
+// homogeneous in d; the admissible d form the polytope {sum d = 0,
+// |d|_1 <= 2} whose faces away from the origin are Delta_{p-1} x Delta_{q-1}
+// (one per sign pattern S of the common components).  For d = rho*zeta the
+// remaining common barycentrics span a (c-1)-simplex of size 1-rho, and
+//   dlambda dmu = rho^{m-1} (1-rho)^{c-1} drho dzeta dt,  m = 7-c,
+// with unit face Jacobian.  The t- and rho-integrals are closed-form Beta
+// integrals; zeta is integrated by collapsed Gauss-Legendre product rules.
+// One CTA per tetrahedron pair; origin o_A = o_B = first common vertex.
+#define SING_THREADS 256
+__device__ __forceinline__ double dfact(int n) {
+  double r = 1.0;
+  for (int i = 2; i <= n; i++) r *= i;
+  return r;
+}
+
+// point of Delta_k from k collapsed Gauss-Legendre digits; returns weight
+__device__ __forceinline__ double simplex_point(int k, const int *dig, double *y) {
+  if (k == 0) { y[0] = 1.0; return 1.0; }
+  if (k == 1) { double u = c_glx[dig[0]]; y[0] = u; y[1] = 1.0 - u; return c_glw[dig[0]]; }
+  if (k == 2) {
+    double u = c_glx[dig[0]], v = c_glx[dig[1]];
+    y[0] = u; y[1] = (1 - u) * v; y[2] = (1 - u) * (1 - v);
+    return c_glw[dig[0]] * c_glw[dig[1]] * (1 - u);
+  }
+  double u = c_glx[dig[0]], v = c_glx[dig[1]], w = c_glx[dig[2]];
+  y[0] = u; y[1] = (1 - u) * v; y[2] = (1 - u) * (1 - v) * w; y[3] = (1 - u) * (1 - v) * (1 - w);
+  return c_glw[dig[0]] * c_glw[dig[1]] * c_glw[dig[2]] * (1 - u) * (1 - u) * (1 - v);
+}
+
+__global__ void __launch_bounds__(SING_THREADS) k_tp_singular(DevGeom g, const int4 *tp, const int4 *ordA,
+                                                              const int4 *ordB, int first, double *mom, int n) {
+  int pidx = first + blockIdx.x;
+  int c = tp[pidx].z;
+  int4 oa = ordA[pidx], ob = ordB[pidx];
+  const int via[4] = {oa.x, oa.y, oa.z, oa.w}, vib[4] = {ob.x, ob.y, ob.z, ob.w};
+  double o[3];
+  load3(g.V4, via[0], o);
+  double VA[4][3], VB[4][3];
+  for (int i = 0; i < 4; i++) {
+    double t[3];
+    load3(g.V4, via[i], t);
+    for (int k = 0; k < 3; k++) VA[i][k] = t[k] - o[k];
+    load3(g.V4, vib[i], t);
+    for (int k = 0; k < 3; k++) VB[i][k] = t[k] - o[k];
+  }
+  int nn = c - 1, m = 7 - c, nown = 4 - c;
+  double ub[3] = {0, 0, 0}, s2 = 0, sv[3] = {0, 0, 0};
+  for (int i = 0; i < c; i++)
+    for (int k = 0; k < 3; k++) { sv[k] += VA[i][k]; s2 += VA[i][k] * VA[i][k]; }
+  for (int k = 0; k < 3; k++) ub[k] = sv[k] / (nn + 1);
+  double W = (s2 + sv[0] * sv[0] + sv[1] * sv[1] + sv[2] * sv[2]) / ((nn + 1.0) * (nn + 2.0));
+  double Gb[3][3];
+  for (int p = 0; p < 3; p++)
+    for (int j = 0; j < 3; j++) {
+      int a = m - 2 + p;  // a = m-1+(p-1)
+      Gb[p][j] = dfact(a + j) / dfact(a + j + nn + 1);
+    }
+  // faces: sign patterns S of the common components (c = 4 excludes 0 and 15)
+  int nfaces = (c == 4) ? 14 : (1 << c);
+  int per = 1;
+  for (int i = 0; i < 6 - c; i++) per *= n;
+  int total = nfaces * per;
+  double acc[24];
+#pragma unroll
+  for (int i = 0; i < 24; i++) acc[i] = 0.0;
+  for (int f = threadIdx.x; f < total; f += SING_THREADS) {
+    int face = f / per, rem = f % per;
+    int S = (c == 4) ? face + 1 : face;
+    int ns = __popc(S);
+    int p = ns + nown, q = (c - ns) + nown;
+    int dig[6];
+    for (int i = 0; i < 6 - c; i++) { dig[i] = rem % n; rem /= n; }
+    double al[4], be[4];
+    double w = simplex_point(p - 1, dig, al) * simplex_point(q - 1, dig + (p - 1), be);
+    double A1[3] = {0, 0, 0}, B1[3] = {0, 0, 0};
+    int ja = 0, jb = 0;
+    for (int k = 0; k < c; k++) {
+      if (S & (1 << k)) { double z = al[ja++]; for (int x = 0; x < 3; x++) A1[x] += z * VA[k][x]; }
+      else { double z = be[jb++]; for (int x = 0; x < 3; x++) B1[x] += z * VA[k][x]; }
+    }
+    for (int k = c; k < 4; k++) {
+      double za = al[ja++], zb = be[jb++];
+      for (int x = 0; x < 3; x++) { A1[x] += za * VA[k][x]; B1[x] += zb * VB[k][x]; }
+    }
+    double L0 = A1[0] - B1[0], L1 = A1[1] - B1[1], L2 = A1[2] - B1[2];
+    double R = sqrt(L0 * L0 + L1 * L1 + L2 * L2);
+    double AB = A1[0] * B1[0] + A1[1] * B1[1] + A1[2] * B1[2];
+    double uAB = ub[0] * (A1[0] + B1[0]) + ub[1] * (A1[1] + B1[1]) + ub[2] * (A1[2] + B1[2]);
+    double Rp[3] = {1.0 / R, 1.0, R};
+#pragma unroll
+    for (int pk = 0; pk < 3; pk++) {
+      double wr = w * Rp[pk];
+      double G0 = Gb[pk][0], G1 = Gb[pk][1], G2 = Gb[pk][2];
+      acc[8 * pk] += wr * G0;
+#pragma unroll
+      for (int x = 0; x < 3; x++) {
+        acc[8 * pk + 1 + x] += wr * (A1[x] * G1 + ub[x] * (G0 - G1));
+        acc[8 * pk + 4 + x] += wr * (B1[x] * G1 + ub[x] * (G0 - G1));
+      }
+      acc[8 * pk + 7] += wr * (AB * G2 + uAB * (G1 - G2) + W * (G0 - 2.0 * G1 + G2));
+    }
+  }
+  // deterministic block reduction
+  __shared__ double red[SING_THREADS / 32][24];
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < 24; i++) {
+    double v = warp_sum(acc[i]);
+    if (lane == 0) red[wid][i] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 24) {
+    double s = 0.0;
+    for (int w2 = 0; w2 < SING_THREADS / 32; w2++) s += red[w2][threadIdx.x];
+    const double gpre[3] = {0.25 / M_PI, 0.25 / M_PI, 0.125 / M_PI};
+    mom[24 * (size_t)pidx + threadIdx.x] = s * gpre[threadIdx.x / 8];
+  }
+}
+
+// combine the 4 tetrahedron pairs of each near basis-function pair into the
+// 6 numbers of GetGME_TetTetInt(KERNEL_STATIC) (GMatrixElements.cc:295-365):
+// per kernel {4 A A' int (x-Q).(y-Q') K, 36 A A' int K} with sign +1 for PP/MM,
+// -1 for PM/MP.
+__device__ __forceinline__ void tp_origin(const DevGeom &g, const int4 *tp, const int4 *ordA, int id, bool first,
+                                          double *o) {
+  int4 p = tp[id];
+  if (p.z >= 2) load3(g.V4, ordA[id].x, o);
+  else load3(g.V4, first ? g.tetVI[p.x].x : g.tetVI[p.y].x, o);
+}
+
+__global__ void k_fibbi_combine(DevGeom g, NearData nd) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nd.npairs) return;
+  int2 ab = nd.pairs[k];
+  int a = ab.x, b = ab.y;
+  int4 t4 = nd.pairTP[k];
+  int tid[4] = {t4.x, t4.y, t4.z, t4.w};
+  int2 qa = g.bfQ[a], qb = g.bfQ[b];
+  double AA = g.bfArea[a] * g.bfArea[b];
+  double out[6] = {0, 0, 0, 0, 0, 0};
+  for (int sa = 0; sa < 2; sa++)
+    for (int sb = 0; sb < 2; sb++) {
+      int code = tid[2 * sa + sb];
+      bool sw = (code >> 30) & 1;
+      int id = code & ~(1 << 30);
+      const double *M = nd.tpMom + 24 * (size_t)id;
+      double ox[3], oy[3], Q[3], QP[3];
+      tp_origin(g, nd.tp, nd.tpOrdA, id, !sw, ox);
+      tp_origin(g, nd.tp, nd.tpOrdA, id, sw, oy);
+      load3(g.V4, sa == 0 ? qa.x : qa.y, Q);
+      load3(g.V4, sb == 0 ? qb.x : qb.y, QP);
+      double q[3] = {Q[0] - ox[0], Q[1] - ox[1], Q[2] - ox[2]};
+      double qp[3] = {QP[0] - oy[0], QP[1] - oy[1], QP[2] - oy[2]};
+      double s = (sa == sb) ? 1.0 : -1.0;
+      for (int pk = 0; pk < 3; pk++) {
+        const double *m = M + 8 * pk;
+        const double *m1 = sw ? m + 4 : m + 1;   // moment of the x (row) tetrahedron
+        const double *m1p = sw ? m + 1 : m + 4;  // moment of the y (column) tetrahedron
+        double J = m[7] - (q[0] * m1p[0] + q[1] * m1p[1] + q[2] * m1p[2]) -
+                   (qp[0] * m1[0] + qp[1] * m1[1] + qp[2] * m1[2]) +
+                   (q[0] * qp[0] + q[1] * qp[1] + q[2] * qp[2]) * m[0];
+        out[2 * pk] += s * 4.0 * AA * J;
+        out[2 * pk + 1] += s * 36.0 * AA * m[0];
+      }
+    }
+  for (int i = 0; i < 6; i++) nd.fibbi[6 * (size_t)k + i] = out[i];
+}
+
+int precompute_near(bg_geometry *g) {
+  int st = init_tables();
+  if (!st) st = set_gl(g->singular_order);
+  if (st) return st;
+  NearData &nd = g->near;
+  if (nd.ntp_reg > 0) {
+    int threads = 256, blocks = (nd.ntp_reg * 32 + threads - 1) / threads;
+    k_tp_regular<<<blocks, threads, 0, stream()>>>(g->dev, nd.tp, nd.ntp_reg, nd.tpMom);
+    BG_LAUNCHED();
+  }
+  int nsing = nd.ntp - nd.ntp_reg;
+  if (nsing > 0) {
+    k_tp_singular<<<nsing, SING_THREADS, 0, stream()>>>(g->dev, nd.tp, nd.tpOrdA, nd.tpOrdB, nd.ntp_reg, nd.tpMom,
+                                                        g->singular_order);
+    BG_LAUNCHED();
+  }
+  if (nd.npairs > 0) {
+    k_fibbi_combine<<<(nd.npairs + 127) / 128, 128, 0, stream()>>>(g->dev, nd);
+    BG_LAUNCHED();
+  }
+  BG_CUDA_TRY(cudaStreamSynchronize(stream()));
+  return BG_OK;
+}
+
+// =========================================================================
+// near field per frequency: desingularised 64-point BF-pair integral plus the
+// cached static numbers (GetGMatrixElement, GMatrixElements.cc:400-420):
+//   G = BFBFInt[(e^{ikr}-1-ikr-(ikr)^2/2)/4 pi r] + (F0-F1/k^2) + ik(F2-F3/k^2)
+//       + (ik)^2 (F4-F5/k^2)
+// =========================================================================
+__global__ void k_near(DevGeom g, NearData nd, cd k, cd invk2, cd *M, size_t ld) {
+  int kk = blockIdx.x * blockDim.x + threadIdx.x;
+  if (kk >= nd.npairs) return;
+  int2 ab = nd.pairs[kk];
+  int a = ab.x, b = ab.y;
+  int2 ta = g.bfTet[a], tb = g.bfTet[b], qa = g.bfQ[a], qb = g.bfQ[b];
+  double Aa = g.bfArea[a], Ab = g.bfArea[b];
+  const double inv4pi = 0.25 / M_PI;
+  cd ik = cmk(-k.i, k.r);
+  cd acc = cmk(0, 0);
+  for (int sa = 0; sa < 2; sa++) {
+    int t1 = sa == 0 ? ta.x : ta.y;
+    double Q[3];
+    load3(g.V4, sa == 0 ? qa.x : qa.y, Q);
+    for (int sb = 0; sb < 2; sb++) {
+      int t2 = sb == 0 ? tb.x : tb.y;
+      double QP[3];
+      load3(g.V4, sb == 0 ? qb.x : qb.y, QP);
+      double cc = (sa == 0 ? 1.0 : -1.0) * (sb == 0 ? 1.0 : -1.0) * Aa * Ab;
+      cd part = cmk(0, 0);
+      for (int i = 0; i < 4; i++) {
+        const double *x = g.tetP4 + 16 * (size_t)t1 + 4 * i;
+        for (int j = 0; j < 4; j++) {
+          const double *y = g.tetP4 + 16 * (size_t)t2 + 4 * j;
+          double R0 = x[0] - y[0], R1 = x[1] - y[1], R2 = x[2] - y[2];
+          double r = sqrt(R0 * R0 + R1 * R1 + R2 * R2);
+          if (r < 1.0e-12) continue;
+          double dot = (x[0] - Q[0]) * (y[0] - QP[0]) + (x[1] - Q[1]) * (y[1] - QP[1]) + (x[2] - Q[2]) * (y[2] - QP[2]);
+          cd phi = cscale(exprel3(cscale(ik, r)), inv4pi / r);
+          cd pe = cmk(dot * (1.0 / 144.0) - invk2.r * (1.0 / 16.0), -invk2.i * (1.0 / 16.0));
+          part = cadd(part, cmul(pe, phi));
+        }
+      }
+      acc = cadd(acc, cscale(part, cc));
+    }
+  }
+  const double *F = nd.fibbi + 6 * (size_t)kk;
+  cd t0 = cadd(cmk(F[0], 0), cscale(invk2, -F[1]));
+  cd t1 = cmul(ik, cadd(cmk(F[2], 0), cscale(invk2, -F[3])));
+  cd t2 = cmul(cmul(ik, ik), cadd(cmk(F[4], 0), cscale(invk2, -F[5])));
+  acc = cadd(acc, cadd(t0, cadd(t1, t2)));
+  M[(size_t)a + (size_t)b * ld] = acc;
+  if (a != b) M[(size_t)b + (size_t)a * ld] = acc;
+}
+
+int assemble_near(bg_geometry *g, double wr, double wi, void *M, size_t ld) {
+  NearData &nd = g->near;
+  if (nd.npairs == 0) return BG_OK;
+  double d = (wr * wr - wi * wi) * (wr * wr - wi * wi) + 4 * wr * wr * wi * wi;
+  cd invk2{(wr * wr - wi * wi) / d, -2 * wr * wi / d};
+  k_near<<<(nd.npairs + 127) / 128, 128, 0, stream()>>>(g->dev, nd, cd{wr, wi}, invk2, (cd *)M, ld);
+  BG_LAUNCHED();
+  return BG_OK;
+}
+
+// =========================================================================
+// V^-1 Gram block of one row (GetOverlaps, VIEMatrix.cc:200-316):
+//   -(1/w^2) int_T F_a . (eps(x)-1)^-1 . F_b, 33-point rule with w = 6V w_i,
+// w = real(omega), over the faces of both tetrahedra of basis function a.
+// Added to M(a,b) and M(b,a) for b >= a (the reference adds the full row and
+// its symmetric fill then overwrites the lower triangle with the upper).
+// =========================================================================
+__global__ void k_gram(DevGeom g, double w, cd *M, size_t ld) {
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= g.N) return;
+  int2 tt = g.bfTet[a], qq = g.bfQ[a];
+  double Aa = g.bfArea[a];
+  int nnz = 1;
+  int idx[8];
+  cd val[8];
+  idx[0] = a;
+  val[0] = cmk(0, 0);
+  const double pre = -1.0 / (w * w);
+  for (int side = 0; side < 2; side++) {
+    int t = side == 0 ? tt.x : tt.y;
+    int obj = g.tetObj[t];
+    const bg_material &mat = g.mats[obj];
+    double vol = g.tetVol[t];
+    double QA[3];
+    load3(g.V4, side == 0 ? qq.x : qq.y, QA);
+    double pa = (side == 0 ? 1.0 : -1.0) * Aa / (3.0 * vol);
+    int4 vi = g.tetVI[t];
+    double V0[3], L[3][3];
+    load3(g.V4, vi.x, V0);
+    int vv[3] = {vi.y, vi.z, vi.w};
+    for (int i = 0; i < 3; i++) {
+      double tmp[3];
+      load3(g.V4, vv[i], tmp);
+      for (int c = 0; c < 3; c++) L[i][c] = tmp[c] - V0[c];
+    }
+    int4 fi = g.tetFI[t];
+    int fl[4] = {fi.x, fi.y, fi.z, fi.w};
+    for (int ifb = 0; ifb < 4; ifb++) {
+      int b = fl[ifb];
+      if (b < 0) continue;
+      int2 tb = g.bfTet[b], qb = g.bfQ[b];
+      double QB[3], pb;
+      if (tb.x == t) { load3(g.V4, qb.x, QB); pb = g.bfArea[b] / (3.0 * vol); }
+      else { load3(g.V4, qb.y, QB); pb = -g.bfArea[b] / (3.0 * vol); }
+      cd accv = cmk(0, 0);
+      for (int i = 0; i < 33; i++) {
+        const double *u = c_tcr33 + 4 * i;
+        double wt = 6.0 * vol * u[3], x[3];
+        for (int c = 0; c < 3; c++) x[c] = V0[c] + u[0] * L[0][c] + u[1] * L[1][c] + u[2] * L[2][c];
+        cd E[3][3], Ei[3][3];
+        mat_eval(mat, x, E);
+        E[0][0].r -= 1.0; E[1][1].r -= 1.0; E[2][2].r -= 1.0;
+        inv3(E, Ei);
+        double FA[3], FB[3];
+        for (int c = 0; c < 3; c++) { FA[c] = pa * (x[c] - QA[c]); FB[c] = pb * (x[c] - QB[c]); }
+        cd v = cmk(0, 0);
+        for (int mu = 0; mu < 3; mu++)
+          for (int nu = 0; nu < 3; nu++) v = cadd(v, cscale(Ei[mu][nu], FA[mu] * FB[nu]));
+        accv = cadd(accv, cscale(v, pre * wt));
+      }
+      if (b == a) val[0] = cadd(val[0], accv);
+      else { idx[nnz] = b; val[nnz] = accv; nnz++; }
+    }
+  }
+  for (int i = 0; i < nnz; i++) {
+    int b = idx[i];
+    if (b < a) continue;
+    cd *p = M + (size_t)a + (size_t)b * ld;
+    *p = cadd(*p, val[i]);
+    if (b != a) {
+      cd *q = M + (size_t)b + (size_t)a * ld;
+      *q = cadd(*q, val[i]);
+    }
+  }
+}
+
+int assemble_gram(bg_geometry *g, double wr, double wi, void *M, size_t ld) {
+  (void)wi;
+  k_gram<<<(g->N + 127) / 128, 128, 0, stream()>>>(g->dev, wr, (cd *)M, ld);
+  BG_LAUNCHED();
+  return BG_OK;
+}
+
+// =========================================================================
+// plane-wave RHS (RHSVector.cc:85-124): v_a = -1/(i w Z0) BFInt[b . E],
+// E = E0 exp(i k nhat.x), 33-point rule on both tetrahedra of a.
+// =========================================================================
+struct PWave { cd E0[3]; double nh[3]; cd k; };
+
+__device__ __forceinline__ cd bf_dot_field(const DevGeom &g, int a, const PWave &pw) {
+  int2 tt = g.bfTet[a], loc = g.bfLoc[a];
+  double Aa = g.bfArea[a];
+  cd tot = cmk(0, 0);
+  for (int side = 0; side < 2; side++) {
+    int t = side == 0 ? tt.x : tt.y, iq = side == 0 ? loc.x : loc.y;
+    int4 vi = g.tetVI[t];
+    int v[4] = {vi.x, vi.y, vi.z, vi.w};
+    double Q[3], L[3][3];
+    load3(g.V4, v[iq], Q);
+    for (int i = 0; i < 3; i++) {
+      double tmp[3];
+      load3(g.V4, v[(iq + 1 + i) % 4], tmp);
+      for (int c = 0; c < 3; c++) L[i][c] = tmp[c] - Q[c];
+    }
+    double vol = g.tetVol[t];
+    double pf = (side == 0 ? 1.0 : -1.0) * Aa / (3.0 * vol);
+    cd acc = cmk(0, 0);
+    for (int i = 0; i < 33; i++) {
+      const double *u = c_tcr33 + 4 * i;
+      double wt = 6.0 * vol * u[3], x[3], b[3];
+      for (int c = 0; c < 3; c++) {
+        b[c] = u[0] * L[0][c] + u[1] * L[1][c] + u[2] * L[2][c];
+        x[c] = Q[c] + b[c];
+        b[c] *= pf;
+      }
+      double ph = pw.nh[0] * x[0] + pw.nh[1] * x[1] + pw.nh[2] * x[2];
+      cd e = expikr(pw.k, ph);
+      cd be = cadd(cadd(cscale(pw.E0[0], b[0]), cscale(pw.E0[1], b[1])), cscale(pw.E0[2], b[2]));
+      acc = cadd(acc, cscale(cmul(be, e), wt));
+    }
+    tot = cadd(tot, acc);
+  }
+  return tot;
+}
+
+__global__ void k_rhs(DevGeom g, PWave pw, cd pre, cd *out) {
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= g.N) return;
+  out[a] = cmul(pre, bf_dot_field(g, a, pw));
+}
+
+static PWave make_pw(double wr, double wi, const double *E0, const double *nhat) {
+  PWave pw;
+  for (int i = 0; i < 3; i++) { pw.E0[i] = cd{E0[2 * i], E0[2 * i + 1]}; pw.nh[i] = nhat[i]; }
+  pw.k = cd{wr, wi};
+  return pw;
+}
+
+int rhs_planewave(bg_geometry *g, double wr, double wi, const double *E0, const double *nhat, void *out) {
+  int st = init_tables();
+  if (st) return st;
+  PWave pw = make_pw(wr, wi, E0, nhat);
+  // -1/(i w Z0) = i/(w Z0)
+  const double Z0 = 376.73031346177;
+  double d = (wr * wr + wi * wi) * Z0;
+  cd pre{wi / d, wr / d};
+  k_rhs<<<(g->N + 127) / 128, 128, 0, stream()>>>(g->dev, pw, pre, (cd *)out);
+  BG_LAUNCHED();
+  return BG_OK;
+}
+
+// =========================================================================
+// EMT power (EMTPFT.cc:324-493): PScat = sum_{a<=b} Re(Z0 J_a^* J_b) Im Q_ab
+// (same object; Im Q = w BFBFInt[PEFIE sin(kr)/(4 pi r)], series for kr<2e-2)
+// and -1/2 Re(Z0 J_a^* J_b i Q_ab) across objects (full e^{ikr}/(4 pi r));
+// rule 4/16/33 points by common vertices and kR>5 (EMTPFT.cc:305-313).
+// Extinction 1/2 Re(J_a^* BFInt[b.E_inc]) (EMTPFT.cc:151-211).
+// Partial sums per block and object pair are reduced on the host in a fixed
+// order.
+// =========================================================================
+struct PftArgs {
+  DevGeom g;
+  const cd *J;
+  double w;      // real(omega)
+  double absw;   // |omega|
+  int nobj;
+};
+
+__device__ __forceinline__ void rule_point(int npts, int i, double *u) {
+  if (npts == 16) { u[0] = c_tcr16[4 * i]; u[1] = c_tcr16[4 * i + 1]; u[2] = c_tcr16[4 * i + 2]; u[3] = c_tcr16[4 * i + 3]; }
+  else { u[0] = c_tcr33[4 * i]; u[1] = c_tcr33[4 * i + 1]; u[2] = c_tcr33[4 * i + 2]; u[3] = c_tcr33[4 * i + 3]; }
+}
+
+// BFBFInt of the scattered-power integrand, lanes [lane0, lane0+nl) split the
+// point pairs; returns this lane's partial Q (complex)
+__device__ cd scat_q(const PftArgs &P, int a, int b, int npts, bool same, int lane, int nl) {
+  const DevGeom &g = P.g;
+  int2 ta = g.bfTet[a], tb = g.bfTet[b], la = g.bfLoc[a], lb = g.bfLoc[b];
+  double k = P.w, k2 = k * k;
+  cd tot = cmk(0, 0);
+  const double inv4pi = 0.25 / M_PI;
+  for (int sa = 0; sa < 2; sa++)
+    for (int sb = 0; sb < 2; sb++) {
+      int t1 = sa == 0 ? ta.x : ta.y, t2 = sb == 0 ? tb.x : tb.y;
+      int i1 = sa == 0 ? la.x : la.y, i2 = sb == 0 ? lb.x : lb.y;
+      int4 v1 = g.tetVI[t1], v2 = g.tetVI[t2];
+      int va[4] = {v1.x, v1.y, v1.z, v1.w}, vb[4] = {v2.x, v2.y, v2.z, v2.w};
+      double Q1[3], Q2[3], L1[3][3], L2[3][3];
+      load3(g.V4, va[i1], Q1);
+      load3(g.V4, vb[i2], Q2);
+      for (int i = 0; i < 3; i++) {
+        double tmp[3];
+        load3(g.V4, va[(i1 + 1 + i) % 4], tmp);
+        for (int c = 0; c < 3; c++) L1[i][c] = tmp[c] - Q1[c];
+        load3(g.V4, vb[(i2 + 1 + i) % 4], tmp);
+        for (int c = 0; c < 3; c++) L2[i][c] = tmp[c] - Q2[c];
+      }
+      double V1 = g.tetVol[t1], V2 = g.tetVol[t2];
+      double p1 = (sa == 0 ? 1.0 : -1.0) * g.bfArea[a] / (3.0 * V1);
+      double p2 = (sb == 0 ? 1.0 : -1.0) * g.bfArea[b] / (3.0 * V2);
+      int np2 = npts * npts;
+      for (int idx = lane; idx < np2; idx += nl) {
+        int i = idx / npts, j = idx % npts;
+        double u[4], v[4];
+        if (npts == 4) {
+          const double qa = 0.13819660112501051, qb = 0.58541019662496850;
+          u[0] = (i == 1) ? qb : qa; u[1] = (i == 2) ? qb : qa; u[2] = (i == 3) ? qb : qa; u[3] = 1.0 / 24.0;
+          v[0] = (j == 1) ? qb : qa; v[1] = (j == 2) ? qb : qa; v[2] = (j == 3) ? qb : qa; v[3] = 1.0 / 24.0;
+        } else {
+          rule_point(npts, i, u);
+          rule_point(npts, j, v);
+        }
+        double xa[3], xb[3], ba[3], bb[3];
+        for (int c = 0; c < 3; c++) {
+          ba[c] = u[0] * L1[0][c] + u[1] * L1[1][c] + u[2] * L1[2][c];
+          xa[c] = Q1[c] + ba[c];
+          ba[c] *= p1;
+          bb[c] = v[0] * L2[0][c] + v[1] * L2[1][c] + v[2] * L2[2][c];
+          xb[c] = Q2[c] + bb[c];
+          bb[c] *= p2;
+        }
+        double wt = 6.0 * V1 * u[3] * 6.0 * V2 * v[3];
+        double R0 = xa[0] - xb[0], R1 = xa[1] - xb[1], R2 = xa[2] - xb[2];
+        double r2 = R0 * R0 + R1 * R1 + R2 * R2, r = sqrt(r2), kr = k * r;
+        double pefie = ba[0] * bb[0] + ba[1] * bb[1] + ba[2] * bb[2] - (3.0 * p1) * (3.0 * p2) / k2;
+        cd phi;
+        if (same) {
+          double imphi;
+          if (fabs(kr) < 2.0e-2) imphi = (1.0 - kr * kr / 6.0) * k * inv4pi;
+          else imphi = sin(kr) * inv4pi / r;
+          phi = cmk(0, imphi);
+        } else {
+          double s, c;
+          sincos(kr, &s, &c);
+          phi = cmk(c * inv4pi / r, s * inv4pi / r);
+        }
+        tot = cadd(tot, cscale(phi, P.w * pefie * wt));
+      }
+    }
+  return tot;
+}
+
+__device__ __forceinline__ double scat_term(const PftArgs &P, int a, int b, cd q, bool same) {
+  cd Ja = P.J[a], Jb = P.J[b];
+  const double Z0 = 376.73031346177;
+  // u0JJ = Z0 conj(Ja) Jb
+  cd u = cmk(Z0 * (Ja.r * Jb.r + Ja.i * Jb.i), Z0 * (Ja.r * Jb.i - Ja.i * Jb.r));
+  if (same) return u.r * q.i;
+  // -0.5 Re(u i q) = 0.5 Im(u q)
+  return 0.5 * (u.r * q.i + u.i * q.r);
+}
+
+#define PMAXOBJ 4
+// far pairs (no common vertex): one thread per pair
+__global__ void __launch_bounds__(FT * FT) k_pft_far(PftArgs P, double *part) {
+  int bx = blockIdx.x, by = blockIdx.y;
+  int a = bx * FT + threadIdx.x, b = by * FT + threadIdx.y;
+  const DevGeom &g = P.g;
+  double contrib = 0.0;
+  int pairid = 0;
+  if (bx <= by && a < g.N && b < g.N && a <= b) {
+    int4 va = g.bfV[a], vb = g.bfV[b];
+    int2 qa = g.bfQ[a], qb = g.bfQ[b];
+    int A5[5] = {qa.x, va.x, va.y, va.z, qa.y}, B5[5] = {qb.x, vb.x, vb.y, vb.z, qb.y};
+    int ncv = 0;
+    for (int i = 0; i < 5; i++)
+      for (int j = 0; j < 5; j++) ncv += A5[i] == B5[j];
+    if (ncv == 0) {
+      double kR = P.absw * fmax(g.bfRadius[a], g.bfRadius[b]);
+      int npts = kR > 5.0 ? 16 : 4;
+      bool same = va.w == vb.w;
+      cd q = scat_q(P, a, b, npts, same, 0, 1);
+      contrib = scat_term(P, a, b, q, same);
+      pairid = va.w * P.nobj + vb.w;
+    }
+  }
+  __shared__ double red[FT * FT / 32][PMAXOBJ * PMAXOBJ];
+  int tid = threadIdx.y * FT + threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  for (int pid = 0; pid < P.nobj * P.nobj; pid++) {
+    double v = warp_sum(pid == pairid ? contrib : 0.0);
+    if (lane == 0) red[wid][pid] = v;
+  }
+  __syncthreads();
+  if (tid < P.nobj * P.nobj) {
+    double s = 0;
+    for (int w = 0; w < FT * FT / 32; w++) s += red[w][tid];
+    part[((size_t)by * gridDim.x + bx) * (P.nobj * P.nobj) + tid] = s;
+  }
+}
+
+// near pairs: one warp per pair, lanes split the point pairs
+__global__ void k_pft_near(PftArgs P, NearData nd, double *part) {
+  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  double contrib = 0.0;
+  if (warp < nd.npairs) {
+    int2 ab = nd.pairs[warp];
+    const DevGeom &g = P.g;
+    double kR = P.absw * fmax(g.bfRadius[ab.x], g.bfRadius[ab.y]);
+    int npts = kR > 5.0 ? 33 : 16;
+    cd q = scat_q(P, ab.x, ab.y, npts, true, lane, 32);
+    q.r = warp_sum(q.r);
+    q.i = warp_sum(q.i);
+    if (lane == 0) contrib = scat_term(P, ab.x, ab.y, q, true);
+  }
+  // near pairs are always same-object: accumulate per object
+  __shared__ double red[8];
+  __shared__ int objs[8];
+  int wid = threadIdx.x >> 5;
+  if (lane == 0) {
+    red[wid] = contrib;
+    objs[wid] = (warp < nd.npairs) ? P.g.bfV[nd.pairs[warp].x].w : 0;
+  }
+  __syncthreads();
+  if (threadIdx.x < P.nobj) {
+    double s = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++)
+      if (objs[w] == (int)threadIdx.x) s += red[w];
+    part[(size_t)blockIdx.x * P.nobj + threadIdx.x] = s;
+  }
+}
+
+__global__ void k_pft_ext(PftArgs P, PWave pw, double *part) {
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  double contrib = 0.0;
+  int obj = 0;
+  if (a < P.g.N) {
+    cd q = bf_dot_field(P.g, a, pw);
+    cd Ja = P.J[a];
+    contrib = Ja.r * q.r + Ja.i * q.i;   // Re(conj(Ja) q)
+    obj = P.g.bfV[a].w;
+  }
+  __shared__ double red[4][PMAXOBJ];
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int o = 0; o < P.nobj; o++) {
+    double v = warp_sum(o == obj ? contrib : 0.0);
+    if (lane == 0) red[wid][o] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < P.nobj) {
+    double s = 0;
+    for (int w = 0; w < 4; w++) s += red[w][threadIdx.x];
+    part[(size_t)blockIdx.x * P.nobj + threadIdx.x] = s;
+  }
+}
+
+// OPFT absorbed power (OPFT.cc:62-119, OverlapIntegrand_PFT PAbs term,
+// OverlapIntegrals.cc:79-170,242-298): sum Re(conj(Ja) Jb ME_ab),
+// ME_ab = 1/2 int b_a . (i Z0/w)(eps-1)^-1 . b_b on the shared tetrahedron.
+__global__ void k_opft(PftArgs P, cd omega, double *part) {
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  const DevGeom &g = P.g;
+  double contrib = 0.0;
+  int obj = 0;
+  if (a < g.N) {
+    obj = g.bfV[a].w;
+    const bg_material &mat = g.mats[obj];
+    int2 tt = g.bfTet[a], loc = g.bfLoc[a];
+    cd Ja = P.J[a];
+    const double Z0 = 376.73031346177;
+    cd pre = cdiv(cmk(0, Z0), omega);
+    for (int side = 0; side < 2; side++) {
+      int t = side == 0 ? tt.x : tt.y, iq = side == 0 ? loc.x : loc.y;
+      double vol = g.tetVol[t];
+      double pa = (side == 0 ? 1.0 : -1.0) * g.bfArea[a] / (3.0 * vol);
+      int4 vi = g.tetVI[t];
+      int v[4] = {vi.x, vi.y, vi.z, vi.w};
+      double QA[3], L[3][3];
+      load3(g.V4, v[iq], QA);
+      for (int i = 0; i < 3; i++) {
+        double tmp[3];
+        load3(g.V4, v[(iq + 1 + i) % 4], tmp);
+        for (int c = 0; c < 3; c++) L[i][c] = tmp[c] - QA[c];
+      }
+      int4 fi = g.tetFI[t];
+      int fl[4] = {fi.x, fi.y, fi.z, fi.w};
+      for (int ifb = 0; ifb < 4; ifb++) {
+        int b = fl[ifb];
+        if (b < 0) continue;
+        int2 tb = g.bfTet[b], qb = g.bfQ[b];
+        double QB[3], pb;
+        if (tb.x == t) { load3(g.V4, qb.x, QB); pb = g.bfArea[b] / (3.0 * vol); }
+        else { load3(g.V4, qb.y, QB); pb = -g.bfArea[b] / (3.0 * vol); }
+        cd me = cmk(0, 0);
+        for (int i = 0; i < 33; i++) {
+          const double *u = c_tcr33 + 4 * i;
+          double wt = 6.0 * vol * u[3], x[3], bA[3], bB[3];
+          for (int c = 0; c < 3; c++) {
+            bA[c] = u[0] * L[0][c] + u[1] * L[1][c] + u[2] * L[2][c];
+            x[c] = bA[c] + QA[c];
+            bB[c] = pb * (x[c] - QB[c]);
+            bA[c] *= pa;
+          }
+          cd E[3][3], Ei[3][3];
+          mat_eval(mat, x, E);
+          E[0][0].r -= 1.0; E[1][1].r -= 1.0; E[2][2].r -= 1.0;
+          inv3(E, Ei);
+          cd vsum = cmk(0, 0);
+          for (int mu = 0; mu < 3; mu++) {
+            cd e = cmk(0, 0);
+            for (int nu = 0; nu < 3; nu++) e = cadd(e, cscale(cmul(pre, Ei[mu][nu]), bB[nu]));
+            vsum = cadd(vsum, cscale(e, 0.5 * bA[mu]));
+          }
+          me = cadd(me, cscale(vsum, wt));
+        }
+        cd Jb = P.J[b];
+        cd jj = cmk(Ja.r * Jb.r + Ja.i * Jb.i, Ja.r * Jb.i - Ja.i * Jb.r);
+        contrib += cmul(jj, me).r;
+      }
+    }
+  }
+  __shared__ double red[4][PMAXOBJ];
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int o = 0; o < P.nobj; o++) {
+    double v = warp_sum(o == obj ? contrib : 0.0);
+    if (lane == 0) red[wid][o] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < P.nobj) {
+    double s = 0;
+    for (int w = 0; w < 4; w++) s += red[w][threadIdx.x];
+    part[(size_t)blockIdx.x * P.nobj + threadIdx.x] = s;
+  }
+}
+
+static int ensure_scratch(bg_geometry *g, size_t bytes) {
+  if (g->scratch_bytes >= bytes) return BG_OK;
+  if (g->d_scratch) cudaFree(g->d_scratch);
+  g->d_scratch = nullptr;
+  g->scratch_bytes = 0;
+  BG_CUDA_TRY(cudaMalloc(&g->d_scratch, bytes));
+  g->scratch_bytes = bytes;
+  return BG_OK;
+}
+
+int pft(bg_geometry *g, double wr, double wi, const void *dJ, const double *E0, const double *nhat, int method,
+        double *out) {
+  int st = init_tables();
+  if (st) return st;
+  int NO = (int)g->objs.size();
+  if (NO > PMAXOBJ) { set_error("PFT supports at most %d objects", PMAXOBJ); return BG_ERR_ARG; }
+  PftArgs P{g->dev, (const cd *)dJ, wr, std::sqrt(wr * wr + wi * wi), NO};
+  int nrow = (g->N + 127) / 128;
+  if (method == BG_PFT_OVERLAP) {
+    if ((st = ensure_scratch(g, sizeof(double) * nrow * NO))) return st;
+    k_opft<<<nrow, 128, 0, stream()>>>(P, cd{wr, wi}, g->d_scratch);
+    BG_LAUNCHED();
+    std::vector<double> h((size_t)nrow * NO);
+    BG_CUDA_TRY(cudaMemcpyAsync(h.data(), g->d_scratch, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, stream()));
+    BG_CUDA_TRY(cudaStreamSynchronize(stream()));
+    for (int o = 0; o < NO; o++) {
+      double s = 0;
+      for (int b = 0; b < nrow; b++) s += h[(size_t)b * NO + o];
+      out[2 * o] = s;
+      out[2 * o + 1] = 0.0;
+    }
+    return BG_OK;
+  }
+  if ((st = build_near_lists(g))) return st;
+  int nb = (g->N + FT - 1) / FT;
+  size_t nfar = (size_t)nb * nb * NO * NO;
+  int nnear_blocks = (g->near.npairs * 32 + 255) / 256;
+  size_t nnear = (size_t)std::max(nnear_blocks, 1) * NO;
+  size_t next = (size_t)nrow * NO;
+  if ((st = ensure_scratch(g, sizeof(double) * (nfar + nnear + next)))) return st;
+  double *pfar = g->d_scratch, *pnear = pfar + nfar, *pext = pnear + nnear;
+  k_pft_far<<<dim3(nb, nb), dim3(FT, FT), 0, stream()>>>(P, pfar);
+  BG_LAUNCHED();
+  if (g->near.npairs > 0) {
+    k_pft_near<<<nnear_blocks, 256, 0, stream()>>>(P, g->near, pnear);
+    BG_LAUNCHED();
+  }
+  PWave pw = make_pw(wr, wi, E0, nhat);
+  k_pft_ext<<<nrow, 128, 0, stream()>>>(P, pw, pext);
+  BG_LAUNCHED();
+  std::vector<double> h(nfar + nnear + next);
+  BG_CUDA_TRY(cudaMemcpyAsync(h.data(), g->d_scratch, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, stream()));
+  BG_CUDA_TRY(cudaStreamSynchronize(stream()));
+  std::vector<double> scat((size_t)NO * NO, 0.0), ext(NO, 0.0);
+  for (size_t blk = 0; blk < (size_t)nb * nb; blk++)
+    for (int p = 0; p < NO * NO; p++) scat[p] += h[blk * NO * NO + p];
+  if (g->near.npairs > 0)
+    for (int blk = 0; blk < nnear_blocks; blk++)
+      for (int o = 0; o < NO; o++) scat[(size_t)o * NO + o] += h[nfar + (size_t)blk * NO + o];
+  for (int blk = 0; blk < nrow; blk++)
+    for (int o = 0; o < NO; o++) ext[o] += h[nfar + nnear + (size_t)blk * NO + o];
+  for (int o = 0; o < NO; o++) {
+    double ps = 0;
+    for (int ob = 0; ob < NO; ob++) ps += scat[(size_t)o * NO + ob];
+    out[2 * o] = 0.5 * ext[o] - ps;
+    out[2 * o + 1] = ps;
+  }
+  return BG_OK;
+}
+
+}  // namespace bg

@@ -1,0 +1,503 @@
+// Dense complex128 LU with partial pivoting and the triangular solves on
+// sm_100a: replaces HMatrix::LUFactorize / LUSolve (LAPACK zgetrf / zgetrs,
+// call sites buff-scatter.cc:285,314).
+//
+// Factorisation: recursive right-looking LU over column halves.  Leaves of
+// width <= 32 are factored by one cooperative kernel (all CTAs own a slice of
+// the panel rows in shared memory; one grid barrier per column: pivot
+// candidates of every CTA -> global winner -> swap, scale, rank-1 update).
+// Row interchanges are then applied to every other column (LAPACK ipiv
+// semantics: ipiv[i] is the 1-based row swapped with row i, applied in
+// order).  Off-diagonal blocks use a unit-lower TRSM (leaf kernel + GEMM
+// recursion) and the Schur complements use a complex GEMM on the FP64 tensor
+// cores (mma.sync m8n8k4 f64; tcgen05 has no f64 kind), 4M complex product,
+// three-stage cp.async pipeline.
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+
+#include "internal.h"
+
+namespace cg = cooperative_groups;
+
+namespace bg {
+
+struct cdl { double r, i; };
+
+// =========================================================================
+// complex GEMM  C(MxN) -= A(MxK) * B(KxN), column-major, complex128.
+// CTA tile 64x64, 4 warps of 32x32, K chunk 16, 3-stage cp.async pipeline.
+// Shared tiles are complex-interleaved: one 16-byte load feeds both the real
+// and the imaginary fragment.  Padding makes the fragment loads conflict-free.
+// =========================================================================
+#define GBM 64
+#define GBN 64
+#define GBK 16
+#define GST 3
+#define APAD 66   // As[k][m] row stride (complex)
+#define BPAD 20   // Bs[n][k] row stride (complex)
+#define GEMM_SMEM (GST * (GBK * APAD + GBN * BPAD) * 16)
+
+__device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ void cp16(void *smem, const void *gmem, bool pred) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  int n = pred ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+__global__ void __launch_bounds__(128) k_zgemm_sub(int M, int N, int K, const cdl *__restrict__ A, size_t lda,
+                                                   const cdl *__restrict__ B, size_t ldb, cdl *C, size_t ldc) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cdl *As = (cdl *)smem_raw;                       // [GST][GBK][APAD]
+  cdl *Bs = As + GST * GBK * APAD;                 // [GST][GBN][BPAD]
+  int m0 = blockIdx.x * GBM, n0 = blockIdx.y * GBN;
+  int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  int wm = warp & 1, wn = warp >> 1;
+  double cr[4][4][2], ci[4][4][2];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) cr[i][j][0] = cr[i][j][1] = ci[i][j][0] = ci[i][j][1] = 0.0;
+  int nchunks = (K + GBK - 1) / GBK;
+  auto load_chunk = [&](int chunk, int stage) {
+    int k0 = chunk * GBK;
+    cdl *as = As + stage * GBK * APAD;
+    cdl *bs = Bs + stage * GBN * BPAD;
+#pragma unroll
+    for (int it = 0; it < 8; it++) {
+      int e = tid + it * 128;          // 0..1023
+      int r = e & 63, kk = e >> 6;     // A: row r, k kk
+      int gr = m0 + r, gk = k0 + kk;
+      bool ok = gr < M && gk < K;
+      const cdl *src = ok ? A + (size_t)gk * lda + gr : A;
+      cp16(as + kk * APAD + r, src, ok);
+      int kb = e & 15, nb = e >> 4;    // B: k kb, col nb
+      int gkb = k0 + kb, gn = n0 + nb;
+      bool okb = gkb < K && gn < N;
+      const cdl *srcb = okb ? B + (size_t)gn * ldb + gkb : B;
+      cp16(bs + nb * BPAD + kb, srcb, okb);
+    }
+  };
+#pragma unroll
+  for (int s = 0; s < GST - 1; s++) {
+    if (s < nchunks) load_chunk(s, s);
+    cp_commit();
+  }
+  for (int chunk = 0; chunk < nchunks; chunk++) {
+    cp_wait<GST - 2>();
+    __syncthreads();
+    int nxt = chunk + GST - 1;
+    if (nxt < nchunks) load_chunk(nxt, nxt % GST);
+    cp_commit();
+    const cdl *as = As + (chunk % GST) * GBK * APAD;
+    const cdl *bs = Bs + (chunk % GST) * GBN * BPAD;
+#pragma unroll
+    for (int ks = 0; ks < GBK / 4; ks++) {
+      double ar[4], ai[4], br[4], bi[4];
+#pragma unroll
+      for (int mt = 0; mt < 4; mt++) {
+        cdl v = as[(ks * 4 + (lane & 3)) * APAD + wm * 32 + mt * 8 + (lane >> 2)];
+        ar[mt] = v.r;
+        ai[mt] = v.i;
+      }
+#pragma unroll
+      for (int nt = 0; nt < 4; nt++) {
+        cdl v = bs[(wn * 32 + nt * 8 + (lane >> 2)) * BPAD + ks * 4 + (lane & 3)];
+        br[nt] = v.r;
+        bi[nt] = v.i;
+      }
+#pragma unroll
+      for (int mt = 0; mt < 4; mt++) {
+        double nai = -ai[mt];
+#pragma unroll
+        for (int nt = 0; nt < 4; nt++) {
+          dmma(cr[mt][nt][0], cr[mt][nt][1], ar[mt], br[nt]);
+          dmma(cr[mt][nt][0], cr[mt][nt][1], nai, bi[nt]);
+          dmma(ci[mt][nt][0], ci[mt][nt][1], ar[mt], bi[nt]);
+          dmma(ci[mt][nt][0], ci[mt][nt][1], ai[mt], br[nt]);
+        }
+      }
+    }
+  }
+  cp_wait<0>();
+  // epilogue: C -= acc
+#pragma unroll
+  for (int mt = 0; mt < 4; mt++) {
+    int row = m0 + wm * 32 + mt * 8 + (lane >> 2);
+    if (row >= M) continue;
+#pragma unroll
+    for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        int col = n0 + wn * 32 + nt * 8 + 2 * (lane & 3) + h;
+        if (col < N) {
+          cdl *p = C + (size_t)col * ldc + row;
+          cdl v = *p;
+          v.r -= cr[mt][nt][h];
+          v.i -= ci[mt][nt][h];
+          *p = v;
+        }
+      }
+  }
+}
+
+static int zgemm_sub(int M, int N, int K, const cdl *A, size_t lda, const cdl *B, size_t ldb, cdl *C, size_t ldc) {
+  if (M <= 0 || N <= 0 || K <= 0) return BG_OK;
+  static bool attr = false;
+  if (!attr) {
+    BG_CUDA_TRY(cudaFuncSetAttribute(k_zgemm_sub, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM));
+    attr = true;
+  }
+  dim3 grid((M + GBM - 1) / GBM, (N + GBN - 1) / GBN);
+  if (grid.y > 65535) { set_error("zgemm: N too large"); return BG_ERR_ARG; }
+  prof_start(PROF_GEMM);
+  k_zgemm_sub<<<grid, 128, GEMM_SMEM, stream()>>>(M, N, K, A, lda, B, ldb, C, ldc);
+  BG_LAUNCHED();
+  prof_stop(PROF_GEMM, 8.0 * M * (double)N * K);
+  return BG_OK;
+}
+
+// =========================================================================
+// leaf triangular solves (n <= 64 rows), 16 right-hand-side columns per CTA
+// =========================================================================
+#define TRS_COLS 16
+#define TRS_SMEM ((64 * 65 + 64 * (TRS_COLS + 1)) * 16)
+__global__ void __launch_bounds__(256) k_trsm_leaf(int n, int m, const cdl *T, size_t ldt, cdl *B, size_t ldb,
+                                                   int upper) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cdl(*Ts)[65] = (cdl(*)[65])smem_raw;
+  cdl(*Bt)[TRS_COLS + 1] = (cdl(*)[TRS_COLS + 1])(smem_raw + 64 * 65 * 16);
+  int c0 = blockIdx.x * TRS_COLS;
+  int tid = threadIdx.x;
+  for (int e = tid; e < n * n; e += 256) {
+    int r = e % n, c = e / n;
+    Ts[r][c] = T[(size_t)c * ldt + r];
+  }
+  for (int e = tid; e < n * TRS_COLS; e += 256) {
+    int r = e % n, c = e / n;
+    Bt[r][c] = (c0 + c < m) ? B[(size_t)(c0 + c) * ldb + r] : cdl{0, 0};
+  }
+  __syncthreads();
+  if (!upper) {
+    for (int i = 0; i < n; i++) {
+      for (int e = tid; e < (n - 1 - i) * TRS_COLS; e += 256) {
+        int r = i + 1 + e / TRS_COLS, c = e % TRS_COLS;
+        cdl l = Ts[r][i], x = Bt[i][c];
+        Bt[r][c].r -= l.r * x.r - l.i * x.i;
+        Bt[r][c].i -= l.r * x.i + l.i * x.r;
+      }
+      __syncthreads();
+    }
+  } else {
+    for (int i = n - 1; i >= 0; i--) {
+      if (tid < TRS_COLS) {
+        cdl u = Ts[i][i], b = Bt[i][tid];
+        double d = u.r * u.r + u.i * u.i;
+        Bt[i][tid] = cdl{(b.r * u.r + b.i * u.i) / d, (b.i * u.r - b.r * u.i) / d};
+      }
+      __syncthreads();
+      for (int e = tid; e < i * TRS_COLS; e += 256) {
+        int r = e / TRS_COLS, c = e % TRS_COLS;
+        cdl uu = Ts[r][i], x = Bt[i][c];
+        Bt[r][c].r -= uu.r * x.r - uu.i * x.i;
+        Bt[r][c].i -= uu.r * x.i + uu.i * x.r;
+      }
+      __syncthreads();
+    }
+  }
+  for (int e = tid; e < n * TRS_COLS; e += 256) {
+    int r = e % n, c = e / n;
+    if (c0 + c < m) B[(size_t)(c0 + c) * ldb + r] = Bt[r][c];
+  }
+}
+
+// X = L^{-1} B (unit lower, upper=0) or U^{-1} B (upper=1), L/U n x n at T
+static int trsm(int n, int m, const cdl *T, size_t ldt, cdl *B, size_t ldb, int upper) {
+  if (n <= 0 || m <= 0) return BG_OK;
+  if (n <= 64) {
+    static bool attr = false;
+    if (!attr) {
+      BG_CUDA_TRY(cudaFuncSetAttribute(k_trsm_leaf, cudaFuncAttributeMaxDynamicSharedMemorySize, TRS_SMEM));
+      attr = true;
+    }
+    int blocks = (m + TRS_COLS - 1) / TRS_COLS;
+    prof_start(PROF_TRSM);
+    k_trsm_leaf<<<blocks, 256, TRS_SMEM, stream()>>>(n, m, T, ldt, B, ldb, upper);
+    BG_LAUNCHED();
+    prof_stop(PROF_TRSM, 4.0 * n * (double)n * m);
+    return BG_OK;
+  }
+  int n1 = (n / 2 + 31) / 32 * 32;
+  if (n1 >= n) n1 = n / 2;
+  int n2 = n - n1;
+  int st;
+  if (!upper) {
+    if ((st = trsm(n1, m, T, ldt, B, ldb, 0))) return st;
+    if ((st = zgemm_sub(n2, m, n1, T + n1, ldt, B, ldb, B + n1, ldb))) return st;
+    return trsm(n2, m, T + n1 + (size_t)n1 * ldt, ldt, B + n1, ldb, 0);
+  }
+  if ((st = trsm(n2, m, T + n1 + (size_t)n1 * ldt, ldt, B + n1, ldb, 1))) return st;
+  if ((st = zgemm_sub(n1, m, n2, T + (size_t)n1 * ldt, ldt, B + n1, ldb, B, ldb))) return st;
+  return trsm(n1, m, T, ldt, B, ldb, 1);
+}
+
+// =========================================================================
+// cooperative panel factorisation of A[k0:Nr, k0:k0+w] (w <= 32)
+// =========================================================================
+struct PanelArgs {
+  cdl *A;
+  size_t ld;
+  int Nr;          // number of rows of the full matrix
+  int k0, w;
+  int rows_per;    // rows owned per CTA
+  int *ipiv;       // global, 1-based
+  int *info;       // device int (0 = ok)
+  double *cval;    // [2][grid] candidate |re|+|im|
+  int *cidx;       // [2][grid] candidate row
+  cdl *crow;       // [2][grid][32] candidate row values
+  cdl *jrow;       // [2][32] values of row k0+j before the swap
+};
+
+__device__ __forceinline__ bool better(double v, int i, double bv, int bi) {
+  return v > bv || (v == bv && i < bi);
+}
+
+__global__ void __launch_bounds__(256) k_panel(PanelArgs P) {
+  cg::grid_group grid = cg::this_grid();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cdl *S = (cdl *)smem_raw;                 // [rows_per][w]
+  __shared__ double rv[8];
+  __shared__ int ri[8];
+  __shared__ int s_piv;
+  __shared__ cdl prow[32];
+  const int w = P.w, G = gridDim.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int r0 = P.k0 + blockIdx.x * P.rows_per;
+  const int r1 = min(P.Nr, r0 + P.rows_per);
+  const int nr = max(0, r1 - r0);
+  for (int e = tid; e < nr * w; e += 256) {
+    int r = e / w, c = e % w;
+    S[r * w + c] = P.A[(size_t)(P.k0 + c) * P.ld + r0 + r];
+  }
+  __syncthreads();
+  for (int j = 0; j < w; j++) {
+    const int gj = P.k0 + j, buf = j & 1;
+    // 1. local pivot candidate (izamax: max |re|+|im|, first index on ties)
+    double bv = -1.0;
+    int bi = 0x7fffffff;
+    for (int r = tid; r < nr; r += 256) {
+      int gr = r0 + r;
+      if (gr < gj) continue;
+      cdl v = S[r * w + j];
+      double a = fabs(v.r) + fabs(v.i);
+      if (better(a, gr, bv, bi)) { bv = a; bi = gr; }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+      int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (better(ov, oi, bv, bi)) { bv = ov; bi = oi; }
+    }
+    if (lane == 0) { rv[wid] = bv; ri[wid] = bi; }
+    __syncthreads();
+    if (tid == 0) {
+      for (int k = 1; k < 8; k++)
+        if (better(rv[k], ri[k], rv[0], ri[0])) { rv[0] = rv[k]; ri[0] = ri[k]; }
+      P.cval[buf * G + blockIdx.x] = rv[0];
+      P.cidx[buf * G + blockIdx.x] = ri[0];
+    }
+    __syncthreads();
+    int myc = ri[0];
+    if (rv[0] >= 0.0 && tid < w) P.crow[((size_t)buf * G + blockIdx.x) * 32 + tid] = S[(myc - r0) * w + tid];
+    if (gj >= r0 && gj < r1 && tid < w) P.jrow[buf * 32 + tid] = S[(gj - r0) * w + tid];
+    grid.sync();
+    // 2. global pivot
+    if (tid < 32) {
+      double v = -1.0;
+      int i = 0x7fffffff, b = 0;
+      for (int k = lane; k < G; k += 32) {
+        double cv = P.cval[buf * G + k];
+        int ci = P.cidx[buf * G + k];
+        if (better(cv, ci, v, i)) { v = cv; i = ci; b = k; }
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        double ov = __shfl_xor_sync(0xffffffffu, v, o);
+        int oi = __shfl_xor_sync(0xffffffffu, i, o);
+        int ob = __shfl_xor_sync(0xffffffffu, b, o);
+        if (better(ov, oi, v, i)) { v = ov; i = oi; b = ob; }
+      }
+      if (lane < w) prow[lane] = P.crow[((size_t)buf * G + b) * 32 + lane];
+      if (lane == 0) s_piv = i;
+    }
+    __syncthreads();
+    const int piv = s_piv;
+    if (blockIdx.x == 0 && tid == 0) P.ipiv[gj] = piv + 1;
+    // 3. swap rows gj and piv inside the panel
+    if (piv != gj) {
+      if (piv >= r0 && piv < r1 && tid < w) S[(piv - r0) * w + tid] = P.jrow[buf * 32 + tid];
+      if (gj >= r0 && gj < r1 && tid < w) S[(gj - r0) * w + tid] = prow[tid];
+    }
+    __syncthreads();
+    // 4. scale the column below the pivot and update the rest of the panel
+    cdl p = prow[j];
+    double d = p.r * p.r + p.i * p.i;
+    if (d == 0.0) {
+      if (blockIdx.x == 0 && tid == 0) atomicCAS(P.info, 0, gj + 1);
+    } else {
+      cdl inv{p.r / d, -p.i / d};
+      int ncol = w - j - 1;
+      for (int r = tid; r < nr; r += 256) {
+        int gr = r0 + r;
+        if (gr <= gj) continue;
+        cdl v = S[r * w + j];
+        cdl l{v.r * inv.r - v.i * inv.i, v.r * inv.i + v.i * inv.r};
+        S[r * w + j] = l;
+        for (int c = 1; c <= ncol; c++) {
+          cdl u = prow[j + c];
+          cdl &t = S[r * w + j + c];
+          t.r -= l.r * u.r - l.i * u.i;
+          t.i -= l.r * u.i + l.i * u.r;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  for (int e = tid; e < nr * w; e += 256) {
+    int r = e / w, c = e % w;
+    P.A[(size_t)(P.k0 + c) * P.ld + r0 + r] = S[r * w + c];
+  }
+}
+
+// apply the interchanges ipiv[k0..k0+w) to columns [c0, c1) of A
+__global__ void k_laswp(cdl *A, size_t ld, const int *ipiv, int k0, int w, int c0, int c1, int skip0, int skip1) {
+  int col = c0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= c1 || (col >= skip0 && col < skip1)) return;
+  cdl *cp = A + (size_t)col * ld;
+  for (int i = 0; i < w; i++) {
+    int p = ipiv[k0 + i] - 1;
+    if (p != k0 + i) {
+      cdl t = cp[k0 + i];
+      cp[k0 + i] = cp[p];
+      cp[p] = t;
+    }
+  }
+}
+
+struct LUWork {
+  double *cval;
+  int *cidx;
+  cdl *crow, *jrow;
+  int *info;
+};
+
+static int panel_grid = 0, panel_smem_max = 0;
+
+static int panel_leaf(bg_matrix *m, const LUWork &W, int k0, int w) {
+  int N = m->N;
+  int Mp = N - k0;
+  int G = std::min(panel_grid, std::max(1, (Mp + 31) / 32));
+  int rows = (Mp + G - 1) / G;
+  size_t smem = (size_t)rows * w * sizeof(cdl);
+  if ((int)smem > panel_smem_max) {
+    set_error("panel slice of %zu bytes exceeds shared memory (N=%d too large for this build)", smem, N);
+    return BG_ERR_ARG;
+  }
+  PanelArgs P{(cdl *)m->d, m->ld, N, k0, w, rows, m->d_ipiv, W.info, W.cval, W.cidx, W.crow, W.jrow};
+  void *args[] = {&P};
+  prof_start(PROF_PANEL);
+  BG_CUDA_TRY(cudaLaunchCooperativeKernel((void *)k_panel, dim3(G), dim3(256), args, smem, stream()));
+  BG_LAUNCHED();
+  prof_stop(PROF_PANEL, 8.0 * Mp * (double)w * w / 2);
+  int threads = 256;
+  int blocks = (N + threads - 1) / threads;
+  prof_start(PROF_LASWP);
+  k_laswp<<<blocks, threads, 0, stream()>>>((cdl *)m->d, m->ld, m->d_ipiv, k0, w, 0, N, k0, k0 + w);
+  BG_LAUNCHED();
+  prof_stop(PROF_LASWP, 0.0);
+  return BG_OK;
+}
+
+// factor columns [k0, k0+n) (rows k0..N-1); interchanges applied to all columns
+static int getrf_rec(bg_matrix *m, const LUWork &W, int k0, int n) {
+  if (n <= 32) return panel_leaf(m, W, k0, n);
+  int n1 = (n / 2 + 31) / 32 * 32;
+  if (n1 >= n) n1 = 32;
+  int n2 = n - n1;
+  int st;
+  cdl *A = (cdl *)m->d;
+  size_t ld = m->ld;
+  int N = m->N;
+  if ((st = getrf_rec(m, W, k0, n1))) return st;
+  cdl *A11 = A + k0 + (size_t)k0 * ld;
+  cdl *A12 = A + k0 + (size_t)(k0 + n1) * ld;
+  cdl *A21 = A + (k0 + n1) + (size_t)k0 * ld;
+  cdl *A22 = A + (k0 + n1) + (size_t)(k0 + n1) * ld;
+  if ((st = trsm(n1, n2, A11, ld, A12, ld, 0))) return st;
+  if ((st = zgemm_sub(N - k0 - n1, n2, n1, A21, ld, A12, ld, A22, ld))) return st;
+  return getrf_rec(m, W, k0 + n1, n2);
+}
+
+int lu_factor(bg_matrix *m) {
+  int st = ensure_device();
+  if (st) return st;
+  int N = m->N;
+  if (!panel_grid) {
+    int dev = 0, sms = 0, smemopt = 0;
+    BG_CUDA_TRY(cudaGetDevice(&dev));
+    BG_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    BG_CUDA_TRY(cudaDeviceGetAttribute(&smemopt, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    panel_smem_max = smemopt - 2048;
+    BG_CUDA_TRY(cudaFuncSetAttribute(k_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, panel_smem_max));
+    int per_sm = 0;
+    BG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_panel, 256, panel_smem_max));
+    if (per_sm < 1) { set_error("panel kernel cannot be resident"); return BG_ERR_CUDA; }
+    panel_grid = sms;  // one CTA per SM (cooperative residency)
+  }
+  size_t need = sizeof(double) * 2 * panel_grid + sizeof(int) * 2 * panel_grid + sizeof(cdl) * 2 * panel_grid * 32 +
+                sizeof(cdl) * 64 + 64;
+  if (m->work_bytes < need) {
+    if (m->d_work) cudaFree(m->d_work);
+    m->d_work = nullptr;
+    m->work_bytes = 0;
+    BG_CUDA_TRY(cudaMalloc(&m->d_work, need));
+    m->work_bytes = need;
+  }
+  char *w = (char *)m->d_work;
+  LUWork W;
+  W.crow = (cdl *)w; w += sizeof(cdl) * 2 * panel_grid * 32;
+  W.jrow = (cdl *)w; w += sizeof(cdl) * 64;
+  W.cval = (double *)w; w += sizeof(double) * 2 * panel_grid;
+  W.cidx = (int *)w; w += sizeof(int) * 2 * panel_grid;
+  W.info = (int *)w;
+  BG_CUDA_TRY(cudaMemsetAsync(W.info, 0, sizeof(int), stream()));
+  if ((st = getrf_rec(m, W, 0, N))) return st;
+  int info = 0;
+  BG_CUDA_TRY(cudaMemcpyAsync(&info, W.info, sizeof(int), cudaMemcpyDeviceToHost, stream()));
+  BG_CUDA_TRY(cudaStreamSynchronize(stream()));
+  return info;
+}
+
+// zgetrs: B <- U^{-1} L^{-1} P B
+int lu_solve(bg_matrix *m, void *dB, int ldb, int nrhs) {
+  int N = m->N;
+  cdl *B = (cdl *)dB;
+  const cdl *A = (const cdl *)m->d;
+  for (int k0 = 0; k0 < N; k0 += 32) {
+    int w = std::min(32, N - k0);
+    k_laswp<<<(nrhs + 31) / 32, 32, 0, stream()>>>(B, (size_t)ldb, m->d_ipiv, k0, w, 0, nrhs, 0, 0);
+    BG_LAUNCHED();
+  }
+  int st = trsm(N, nrhs, A, m->ld, B, (size_t)ldb, 0);
+  if (!st) st = trsm(N, nrhs, A, m->ld, B, (size_t)ldb, 1);
+  return st;
+}
+
+}  // namespace bg

@@ -1,0 +1,192 @@
+/*
+ * buffem_b200.h -- C-ABI of the B200-native BUFF-EM dense VIE hot path.
+ *
+ * Plain C types only (opaque handles, pointers, sizes); no torch or C++
+ * types cross this boundary.  Every entry point returns an int status:
+ *   0 (BG_OK)  success
+ *   > 0        LAPACK-style info from the LU (1-based index of an exactly zero pivot)
+ *   < 0        error; bg_last_error() returns a thread-local message.
+ * No exception crosses the ABI.  There is no CPU fallback: every compute
+ * entry point runs hand-written sm_100a CUDA kernels and fails with
+ * BG_ERR_CUDA when no usable GPU is present.
+ *
+ * Units and conventions follow libbuff: omega in units of 3e14 rad/s,
+ * lengths in microns, k = omega in vacuum, complex numbers as interleaved
+ * (re, im) doubles, matrices column-major N x N complex128 (LAPACK layout;
+ * the VIE matrix is complex-symmetric, M = M^T).
+ *
+ * Each declaration cites the libbuff / libhmat interface it replaces
+ * (paths relative to the HomerReid/buff-em source tree).
+ */
+#ifndef BUFFEM_B200_H
+#define BUFFEM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BG_OK 0
+#define BG_ERR_ARG (-1)       /* invalid argument / wrong-size object */
+#define BG_ERR_IO (-2)        /* unreadable or malformed mesh / geometry file */
+#define BG_ERR_TOPOLOGY (-3)  /* mesh face shared by more than two tetrahedra */
+#define BG_ERR_CUDA (-4)      /* CUDA runtime error or no usable GPU */
+#define BG_ERR_NOMEM (-5)     /* device or host allocation failed */
+#define BG_ERR_STATE (-6)     /* call out of order (e.g. solve before factor) */
+#define BG_ERR_NUMERIC (-7)   /* non-finite value detected */
+
+/* matrix storage precisions */
+#define BG_C128 0             /* complex128 (the plain FP64 path) */
+#define BG_C64 1              /* complex64 (precision form)          */
+
+/* permittivity functors (replace SVTensor / MatProp expressions,
+   SVTensor.cc:41-114,306-373; off-diagonals are symmetrised on evaluation) */
+#define BG_MAT_CONST_ISO 0     /* eps[0]+i eps[1]                               */
+#define BG_MAT_CONST_TENSOR 1  /* eps[0..17]: 3x3 complex, row-major            */
+#define BG_MAT_JANUS_Z 2       /* eps (z > center[2]) / eps2 (z <= center[2])   */
+#define BG_MAT_GAUSSIAN 3      /* eps + amp*exp(-|x-center|^2/width^2)          */
+
+typedef struct bg_material {
+  int kind;
+  double eps[18];
+  double eps2[2];
+  double center[3];
+  double amp[2];
+  double width;
+} bg_material;
+
+/* PFT methods (GetPFT.cc:133-189) */
+#define BG_PFT_EMT 0          /* energy/momentum transfer (BUFF default, GetPFT.cc:205) */
+#define BG_PFT_OVERLAP 1      /* overlap method (OPFT.cc:62-119) */
+
+typedef struct bg_geometry bg_geometry;
+typedef struct bg_matrix bg_matrix;
+
+/* Thread-local description of the last error (replaces ErrExit's message). */
+const char *bg_last_error(void);
+
+/* ---------------------------------------------------------------------------
+ * geometry -- replaces buff::SWGGeometry (libbuff.h:200-272)
+ * ------------------------------------------------------------------------- */
+
+/* SWGGeometry::SWGGeometry(const char *GeoFileName), SWGGeometry.cc:214-383.
+   Parses OBJECT / MESHFILE / MATERIAL CONST_EPS_<value> / DISPLACED /
+   ENDOBJECT sections of a .buffgeo file; meshes are gmsh .msh/.vmsh read with
+   the semantics of ReadGMSHFile.cc:66-261 and numbered by InitFaceList.cc:69-279. */
+int bg_geometry_create(const char *buffgeo_path, bg_geometry **out);
+
+/* Same as above from explicit per-object mesh files, displacements
+   (3*nobj doubles or NULL) and permittivity functors (SWGGeometry.cc:52-158). */
+int bg_geometry_create_objects(int nobj, const char *const *meshfiles, const double *displacements,
+                               const bg_material *materials, bg_geometry **out);
+
+/* SWGGeometry::~SWGGeometry, SWGGeometry.cc:388-397 */
+void bg_geometry_destroy(bg_geometry *g);
+
+/* SWGGeometry::TotalBFs / NumObjects / BFIndexOffset (libbuff.h:262-263) */
+int bg_geometry_num_bfs(const bg_geometry *g);
+int bg_geometry_num_objects(const bg_geometry *g);
+int bg_geometry_bf_offset(const bg_geometry *g, int obj);
+
+/* Face table of object obj, 9 ints per interior face:
+   iV1 iV2 iV3 iQP iQM iPTet iMTet PIndex MIndex (SWGFace, libbuff.h:97-115). */
+int bg_geometry_faces(const bg_geometry *g, int obj, int *out);
+
+/* Frequency-independent near-field integrals (the FIBBI cache of
+   FIBBICache.cc:211-245 / ComputeFIBBIData, GMatrixElements.cc:370-375),
+   computed on the device and kept resident.  Called implicitly by the first
+   bg_assemble; exposed for timing.  The SWGGeometry statics
+   TaylorDuffyTolerance / MaxTaylorDuffyEvals (libbuff.h:254-255) are replaced by
+   bg_geometry_set_singular_order: Gauss points per angular dimension of the
+   singular rule (default 10; must be set before the first precompute). */
+int bg_geometry_precompute(bg_geometry *g);
+int bg_geometry_set_singular_order(bg_geometry *g, int n);
+
+/* Copies the 6 frequency-independent near-field numbers of every near
+   basis-function pair: pairs[2*k] = a, pairs[2*k+1] = b (a <= b, global
+   indices), data[6*k..6*k+5] (GMatrixElements.cc:404-420 ordering).
+   *count receives the number of pairs; pass pairs=data=NULL to query it. */
+int bg_geometry_near_data(bg_geometry *g, int *count, int *pairs, double *data);
+
+/* ---------------------------------------------------------------------------
+ * VIE matrix -- replaces AllocateVIEMatrix / AssembleVIEMatrix and HMatrix
+ * ------------------------------------------------------------------------- */
+
+/* SWGGeometry::AllocateVIEMatrix(bool), VIEMatrix.cc:465-471.  The matrix is
+   device-resident (N x N column-major, precision BG_C128 or BG_C64). */
+int bg_matrix_create(bg_geometry *g, int precision, bg_matrix **out);
+void bg_matrix_destroy(bg_matrix *m);
+
+/* SWGGeometry::AssembleVIEMatrix(cdouble Omega, HMatrix *M), VIEMatrix.cc:431-460:
+   G blocks (AssembleGBlock, :365-426) + V^-1 Gram blocks (AssembleOverlapBlocks,
+   :321-360) + symmetric fill.  A matrix of the wrong size is an error
+   (BG_ERR_ARG) instead of the reference's silent reallocation. */
+int bg_assemble(bg_geometry *g, double omega_re, double omega_im, bg_matrix *m);
+
+/* HMatrix::GetEntries / ExportToMATLAB equivalent: copy the whole matrix
+   (or its LU factors after bg_lu_factor) to host memory, column-major,
+   2*N*N doubles (BG_C128) or 2*N*N floats (BG_C64). */
+int bg_matrix_download(const bg_matrix *m, void *host);
+/* Upload a host matrix (same layout) into m, e.g. for factoring user data. */
+int bg_matrix_upload(bg_matrix *m, const void *host);
+/* Device pointer and leading dimension of the storage (no copy). */
+int bg_matrix_device_ptr(bg_matrix *m, void **dptr, int *ld);
+
+/* HMatrix::LUFactorize() -> LAPACK zgetrf (call site buff-scatter.cc:285).
+   Right-looking blocked LU with partial pivoting on the device.  Returns
+   > 0 (LAPACK info) for an exactly singular pivot. */
+int bg_lu_factor(bg_matrix *m);
+/* 1-based pivot indices (LAPACK ipiv), N ints, to host. */
+int bg_lu_pivots(const bg_matrix *m, int *ipiv_host);
+
+/* HMatrix::LUSolve(HVector *) -> zgetrs (call site buff-scatter.cc:314).
+   B is a host column-major N x nrhs complex128 array, overwritten by X. */
+int bg_lu_solve(bg_matrix *m, double *B_host, int nrhs);
+/* Same with B already on the device (leading dimension ldb, complex128). */
+int bg_lu_solve_device(bg_matrix *m, void *B_dev, int ldb, int nrhs);
+
+/* ---------------------------------------------------------------------------
+ * right-hand side and post-processing
+ * ------------------------------------------------------------------------- */
+
+/* SWGGeometry::AssembleRHSVector(Omega, PlaneWave(E0, nHat), RHS),
+   RHSVector.cc:85-124: v_a = -1/(i w Z0) * int b_a . E0 exp(i k nhat.x).
+   E0: 3 complex (6 doubles); nhat: 3 doubles; out: N complex (host). */
+int bg_rhs_planewave(bg_geometry *g, double omega_re, double omega_im, const double *E0,
+                     const double *nhat, double *out_host);
+/* Same, writing to a device buffer of N complex128. */
+int bg_rhs_planewave_device(bg_geometry *g, double omega_re, double omega_im, const double *E0,
+                            const double *nhat, void *out_dev);
+
+/* SWGGeometry::GetPFTMatrix(J, Omega, Options), GetPFT.cc:133-189, absorbed and
+   scattered power columns (PFT_PABS, PFT_PSCAT) per object: out[2*obj+0] =
+   PAbs, out[2*obj+1] = PScat.  method = BG_PFT_EMT (EMTPFT.cc:324-493, with the
+   plane wave E0/nhat as incident field) or BG_PFT_OVERLAP (OPFT.cc:62-119;
+   PScat is not defined there and is returned as 0).  J: N complex (host). */
+int bg_pft(bg_geometry *g, double omega_re, double omega_im, const double *J_host, const double *E0,
+           const double *nhat, int method, double *out);
+
+/* ---------------------------------------------------------------------------
+ * instrumentation
+ * ------------------------------------------------------------------------- */
+
+/* Number of CUDA kernels this library has launched since load (all streams). */
+long long bg_kernel_launch_count(void);
+/* Synchronise the library's stream (timing helpers). */
+int bg_synchronize(void);
+/* cudaStream_t of the library (as void*), so callers can time on it. */
+void *bg_stream(void);
+
+/* Kernel-class timing with CUDA events on the library stream (off by default).
+   bg_profile_begin() clears and enables it; bg_profile_read() synchronises and
+   returns, per kernel class (0: LU trailing GEMM, 1: LU panel, 2: row
+   interchanges, 3: triangular-solve leaves), the number of launches, summed
+   milliseconds and algorithmic flops (counts/ms/flops arrays of length n). */
+int bg_profile_begin(void);
+int bg_profile_read(int n, long long *counts, double *ms, double *flops);
+int bg_profile_end(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BUFFEM_B200_H */

@@ -1,0 +1,205 @@
+"""ctypes binding of the CPU oracle (liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU legs of bench.py, as the checker and as the timed CPU restatement of the
+reference path.  The product library never imports this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+MAT_CONST_ISO, MAT_CONST_TENSOR, MAT_JANUS_Z, MAT_GAUSSIAN = 0, 1, 2, 3
+
+
+class OMat(C.Structure):
+    _fields_ = [("kind", C.c_int), ("eps", C.c_double * 18), ("eps2", C.c_double * 2),
+                ("center", C.c_double * 3), ("amp", C.c_double * 2), ("width", C.c_double)]
+
+
+def material(kind=MAT_CONST_ISO, eps=4 + 0.2j, tensor=None, eps2=None, center=(0, 0, 0),
+             amp=0.0, width=1.0) -> OMat:
+    m = OMat()
+    m.kind = kind
+    if tensor is not None:
+        t = np.asarray(tensor, dtype=np.complex128).reshape(3, 3)
+        for i in range(3):
+            for j in range(3):
+                m.eps[2 * (3 * i + j)] = t[i, j].real
+                m.eps[2 * (3 * i + j) + 1] = t[i, j].imag
+    else:
+        m.eps[0], m.eps[1] = complex(eps).real, complex(eps).imag
+    if eps2 is not None:
+        m.eps2[0], m.eps2[1] = complex(eps2).real, complex(eps2).imag
+    for i in range(3):
+        m.center[i] = center[i]
+    m.amp[0], m.amp[1] = complex(amp).real, complex(amp).imag
+    m.width = width
+    return m
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        L = C.CDLL(path)
+        P, D, I = C.c_void_p, C.c_double, C.c_int
+        dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+        ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+        L.or_geom_create.restype = P
+        L.or_geom_create.argtypes = [I, C.POINTER(C.c_char_p), C.c_void_p, C.POINTER(OMat)]
+        L.or_last_error.restype = C.c_char_p
+        L.or_geom_set_nang.argtypes = [P, I]
+        for f in ("or_geom_nbf", "or_geom_nobj"):
+            getattr(L, f).argtypes = [P]
+            getattr(L, f).restype = I
+        L.or_geom_ntets.argtypes = [P, I]
+        L.or_geom_ntets.restype = I
+        L.or_geom_nverts.argtypes = [P, I]
+        L.or_geom_nverts.restype = I
+        L.or_geom_faces.argtypes = [P, I, ip]
+        L.or_geom_destroy.argtypes = [P]
+        L.or_sing_static.argtypes = [I, dp, dp, dp, dp, I, dp]
+        L.or_fibbi.argtypes = [P, I, I, dp]
+        L.or_gme.argtypes = [P, I, I, D, D, dp]
+        L.or_overlaps.argtypes = [P, I, D, ip, dp]
+        L.or_overlaps.restype = I
+        L.or_overlap_closed_form.argtypes = [P, I, ip, dp]
+        L.or_overlap_closed_form.restype = I
+        L.or_assemble.argtypes = [P, D, D, dp]
+        L.or_assemble_rows.argtypes = [P, D, D, dp, I, I]
+        L.or_rhs_planewave.argtypes = [P, D, D, dp, dp, dp]
+        L.or_pft_emt.argtypes = [P, D, D, dp, dp, dp, dp]
+        L.or_pft_opft.argtypes = [P, D, D, dp, dp]
+        L.or_num_threads.restype = I
+        L.or_cache_build.argtypes = [P]
+        L.or_cache_size.argtypes = [P]
+        L.or_cache_size.restype = I
+        L.or_assemble_row_list.argtypes = [P, D, D, ip, I, dp]
+        _LIB = L
+    return _LIB
+
+
+class Geometry:
+    """Oracle geometry: a list of (mesh file, displacement, material) objects."""
+
+    def __init__(self, meshfiles, materials, displacements=None, nang=8):
+        L = lib()
+        if isinstance(meshfiles, str):
+            meshfiles = [meshfiles]
+            materials = [materials]
+        n = len(meshfiles)
+        arr = (C.c_char_p * n)(*[m.encode() for m in meshfiles])
+        mats = (OMat * n)(*materials)
+        self._disp = None
+        dptr = None
+        if displacements is not None:
+            self._disp = np.ascontiguousarray(displacements, dtype=np.float64).reshape(n, 3)
+            dptr = self._disp.ctypes.data
+        self.h = L.or_geom_create(n, arr, dptr, mats)
+        if not self.h:
+            raise RuntimeError(L.or_last_error().decode())
+        L.or_geom_set_nang(self.h, nang)
+        self.N = L.or_geom_nbf(self.h)
+        self.nobj = L.or_geom_nobj(self.h)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().or_geom_destroy(self.h)
+            self.h = None
+
+    def faces(self, no=0):
+        L = lib()
+        nt = L.or_geom_ntets(self.h, no)
+        # interior faces of object no
+        cnt = self.N if self.nobj == 1 else None
+        if cnt is None:
+            raise NotImplementedError
+        out = np.zeros((cnt, 9), dtype=np.int32)
+        L.or_geom_faces(self.h, no, out)
+        return out
+
+    def assemble(self, omega, rows=None):
+        N = self.N
+        M = np.zeros((N, N), dtype=np.complex128, order="F")
+        buf = M.view(np.float64).reshape(-1) if False else None
+        flat = np.zeros(2 * N * N, dtype=np.float64)
+        if rows is None:
+            lib().or_assemble(self.h, omega.real, omega.imag, flat)
+        else:
+            lib().or_assemble_rows(self.h, omega.real, omega.imag, flat, rows[0], rows[1])
+        return flat.view(np.complex128).reshape(N, N, order="F")
+
+    def cache_build(self):
+        lib().or_cache_build(self.h)
+        return lib().or_cache_size(self.h)
+
+    def assemble_rows(self, omega, rows):
+        rows = np.ascontiguousarray(rows, dtype=np.int32)
+        out = np.zeros(2 * len(rows) * self.N)
+        lib().or_assemble_row_list(self.h, omega.real, omega.imag, rows, len(rows), out)
+        return out.view(np.complex128).reshape(len(rows), self.N)
+
+    def gme(self, a, b, omega):
+        out = np.zeros(2)
+        lib().or_gme(self.h, a, b, omega.real, omega.imag, out)
+        return complex(out[0], out[1])
+
+    def fibbi(self, a, b):
+        out = np.zeros(6)
+        lib().or_fibbi(self.h, a, b, out)
+        return out
+
+    def overlaps(self, a, omega):
+        idx = np.zeros(7, dtype=np.int32)
+        v = np.zeros(14)
+        n = lib().or_overlaps(self.h, a, omega, idx, v)
+        return idx[:n], v[: 2 * n].view(np.complex128)
+
+    def overlap_closed_form(self, a):
+        idx = np.zeros(7, dtype=np.int32)
+        v = np.zeros(7)
+        n = lib().or_overlap_closed_form(self.h, a, idx, v)
+        return idx[:n], v[:n]
+
+    def rhs_planewave(self, omega, E0, nhat):
+        E = np.asarray(E0, dtype=np.complex128).view(np.float64).copy()
+        nh = np.asarray(nhat, dtype=np.float64).copy()
+        out = np.zeros(2 * self.N)
+        lib().or_rhs_planewave(self.h, omega.real, omega.imag, E, nh, out)
+        return out.view(np.complex128)
+
+    def pft_emt(self, omega, J, E0, nhat):
+        Jd = np.ascontiguousarray(J, dtype=np.complex128).view(np.float64)
+        E = np.asarray(E0, dtype=np.complex128).view(np.float64).copy()
+        nh = np.asarray(nhat, dtype=np.float64).copy()
+        out = np.zeros(2 * self.nobj)
+        lib().or_pft_emt(self.h, omega.real, omega.imag, Jd, E, nh, out)
+        return out.reshape(self.nobj, 2)
+
+    def pft_opft(self, omega, J):
+        Jd = np.ascontiguousarray(J, dtype=np.complex128).view(np.float64)
+        out = np.zeros(self.nobj)
+        lib().or_pft_opft(self.h, omega.real, omega.imag, Jd, out)
+        return out
+
+
+def sing_static(c, VA, VB, Q, QP, nang=8):
+    out = np.zeros(6)
+    lib().or_sing_static(c, np.ascontiguousarray(VA, dtype=np.float64).reshape(-1),
+                         np.ascontiguousarray(VB, dtype=np.float64).reshape(-1),
+                         np.ascontiguousarray(Q, dtype=np.float64),
+                         np.ascontiguousarray(QP, dtype=np.float64), nang, out)
+    return out

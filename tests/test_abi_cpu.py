@@ -1,0 +1,82 @@
+"""C-ABI checks that need no GPU: the library loads, exports every entry point
+declared in include/buffem_b200.h, builds the host geometry with the
+reference's numbering, and reports errors as status codes."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+import buffem
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    src = open(os.path.join(ROOT, "include", "buffem_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(bg_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_exports_every_declared_symbol(buffem_lib):
+    L = buffem_lib.lib()
+    names = declared_functions()
+    assert len(names) >= 25
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+    assert set(names) == set(buffem.EXPORTS)
+
+
+def test_face_numbering_matches_oracle(buffem_lib, oracle_lib, sphere, ref_mesh):
+    for path in (sphere(2), sphere(3, jitter=0.05, seed=2), ref_mesh("sphere48"), ref_mesh("sphere533")):
+        G = buffem.SWGGeometry(meshfiles=path, materials=buffem.Material(eps=4.0))
+        O = oracle_lib.Geometry(path, oracle_lib.material(eps=4.0))
+        assert G.TotalBFs == O.N
+        assert np.array_equal(G.faces(0), O.faces(0))
+
+
+def test_buffgeo_parser(buffem_lib, sphere, tmp_path):
+    p = tmp_path / "two.buffgeo"
+    mesh = sphere(2)
+    p.write_text(f"OBJECT A\n MESHFILE {mesh}\n MATERIAL CONST_EPS_10\nENDOBJECT\n"
+                 f"OBJECT B\n MESHFILE {mesh}\n MATERIAL CONST_EPS_4+0.2i\n DISPLACED 0 0 3\nENDOBJECT\n")
+    G = buffem.SWGGeometry(str(p))
+    assert G.NumObjects == 2 and G.TotalBFs == 2 * 72
+    assert G.BFIndexOffset == [0, 72, 144]
+
+
+def test_error_statuses(buffem_lib, tmp_path):
+    with pytest.raises(buffem.BuffError) as e:
+        buffem.SWGGeometry(meshfiles=str(tmp_path / "nope.vmsh"), materials=buffem.Material(eps=2.0))
+    assert e.value.status == -2
+    # three tetrahedra sharing one face: InitFaceList topology error
+    bad = tmp_path / "bad.vmsh"
+    bad.write_text("$MeshFormat\n2.2 0 8\n$EndMeshFormat\n$Nodes\n6\n1 0 0 0\n2 1 0 0\n3 0 1 0\n"
+                   "4 0 0 1\n5 0 0 -1\n6 1 1 1\n$EndNodes\n$Elements\n3\n1 4 2 0 1 1 2 3 4\n"
+                   "2 4 2 0 1 1 3 2 5\n3 4 2 0 1 1 2 3 6\n$EndElements\n")
+    with pytest.raises(buffem.BuffError) as e:
+        buffem.SWGGeometry(meshfiles=str(bad), materials=buffem.Material(eps=2.0))
+    assert e.value.status == -3
+    p = tmp_path / "x.buffgeo"
+    p.write_text("OBJECT A\n MESHFILE none.vmsh\n MATERIAL Gold\nENDOBJECT\n")
+    with pytest.raises(buffem.BuffError) as e:
+        buffem.SWGGeometry(str(p))
+    assert e.value.status == -2
+
+
+def _has_gpu():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.mark.skipif(_has_gpu(), reason="checks the no-GPU failure mode")
+def test_compute_without_gpu_fails_loudly(buffem_lib, sphere):
+    G = buffem.SWGGeometry(meshfiles=sphere(1), materials=buffem.Material(eps=2.0))
+    with pytest.raises(buffem.BuffError) as e:
+        G.AllocateVIEMatrix()
+    assert e.value.status == -4
+    assert "no CPU fallback" in str(e.value) or "CUDA" in str(e.value)

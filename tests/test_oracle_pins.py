@@ -1,0 +1,171 @@
+"""Pins of the CPU oracle against closed forms and known answers (no GPU).
+
+The reference ships no golden vectors and cannot be built here (it needs the
+non-vendored SCUFF-EM libraries), so the oracle is pinned against:
+  * the closed-form SWG Gram overlaps of SWGVolume.cc:405-481 (GetOverlapElements);
+  * exact polynomial integrals and an independent reduction of the unit-cube
+    Coulomb integral for the singular tetrahedron-pair rule;
+  * the ExpRel series definition (pattern of interactiveTests/tExpRel.cc);
+  * the Mie series for a dielectric sphere (examples/MieScattering).
+"""
+import itertools
+
+import numpy as np
+import pytest
+import scipy.linalg as sl
+import scipy.special as sp
+
+
+def kuhn_cube():
+    T = []
+    for perm in itertools.permutations(range(3)):
+        c = np.zeros(3)
+        vs = [c.copy()]
+        for ax in perm:
+            c = c.copy()
+            c[ax] += 1
+            vs.append(c)
+        T.append(np.array(vs))
+    return T
+
+
+def common_first(A, B):
+    ca = [any(np.allclose(a, b) for b in B) for a in A]
+    cb = [any(np.allclose(b, a) for a in A) for b in B]
+    com = [A[i] for i in range(4) if ca[i]]
+    return sum(ca), np.array(com + [A[i] for i in range(4) if not ca[i]]), \
+        np.array(com + [B[i] for i in range(4) if not cb[i]])
+
+
+def cube_coulomb(p):
+    """int_{[0,1]^3 x [0,1]^3} |x-y|^p via z = x-y, pyramids z = rho (1,a,b)."""
+    x, w = np.polynomial.legendre.leggauss(60)
+    x, w = 0.5 * (x + 1), 0.5 * w
+    tot = 0.0
+    for a, wa in zip(x, w):
+        for b, wb in zip(x, w):
+            s = np.sqrt(1 + a * a + b * b)
+            f = x ** (2 + p) * (1 - x) * (1 - x * a) * (1 - x * b)
+            tot += wa * wb * s ** p * np.sum(w * f)
+    return 24 * tot
+
+
+@pytest.mark.parametrize("p,idx", [(-1, 1), (1, 5)])
+def test_singular_rule_unit_cube(oracle_lib, p, idx):
+    """The 6 Kuhn tetrahedra of the cube all share the main diagonal, so the
+    cube integral is a sum of pairs with 2, 3 and 4 common vertices."""
+    tot = 0.0
+    for A in kuhn_cube():
+        for B in kuhn_cube():
+            c, oa, ob = common_first(A, B)
+            assert c >= 2
+            tot += oracle_lib.sing_static(c, oa, ob, oa[0], ob[0], 10)[idx]
+    exact = cube_coulomb(p)
+    assert abs(tot / exact - 1) < 1e-9
+
+
+@pytest.mark.parametrize("c", [2, 3, 4])
+def test_singular_rule_polynomial_exact(oracle_lib, c):
+    rng = np.random.default_rng(c)
+    A = rng.normal(size=(4, 3))
+    B = rng.normal(size=(4, 3))
+    B[:c] = A[:c]
+    Q, QP = rng.normal(size=3), rng.normal(size=3)
+    out = oracle_lib.sing_static(c, A, B, Q, QP, 4)
+    vol = lambda V: abs(np.linalg.det(np.array([V[1] - V[0], V[2] - V[0], V[3] - V[0]]))) / 6
+    va, vb = vol(A), vol(B)
+    assert abs(out[3] / (va * vb) - 1) < 1e-13
+    assert abs(out[2] / (va * vb * np.dot(A.mean(0) - Q, B.mean(0) - QP)) - 1) < 1e-12
+
+
+@pytest.mark.parametrize("c", [2, 3, 4])
+def test_singular_rule_converged(oracle_lib, c):
+    """Well-shaped pairs (regular-ish tetrahedra around a shared simplex):
+    the angular rule converges spectrally (order 10 vs 14 agree to 1e-9)."""
+    s3 = np.sqrt(3.0)
+    A = np.array([[0, 0, 0], [1, 0, 0], [0.5, s3 / 2, 0], [0.5, s3 / 6, np.sqrt(2 / 3)]])
+    if c == 4:
+        B = A.copy()
+    elif c == 3:
+        B = A.copy()
+        B[3] = [0.5, s3 / 6, -np.sqrt(2 / 3)]
+    else:
+        B = A.copy()
+        B[2] = [0.5, -s3 / 2, 0]
+        B[3] = [0.5, -s3 / 6, -np.sqrt(2 / 3)]
+    Q, QP = A[3], B[3]
+    r10 = oracle_lib.sing_static(c, A, B, Q, QP, 10)
+    r14 = oracle_lib.sing_static(c, A, B, Q, QP, 14)
+    assert np.max(np.abs(r10 - r14) / np.abs(r14).max()) < 1e-9
+
+
+def test_gram_closed_form(oracle_lib, sphere, ref_mesh):
+    """eps = 2 makes (eps-1)^-1 = I, so V^-1_ab = -(1/w^2) <b_a|b_b>, which
+    GetOverlapElements gives in closed form (SWGVolume.cc:405-481)."""
+    for path in (sphere(2), ref_mesh("sphere48")):
+        G = oracle_lib.Geometry(path, oracle_lib.material(eps=2.0))
+        for a in range(G.N):
+            idx, v = G.overlaps(a, 1.0)
+            idx2, c = G.overlap_closed_form(a)
+            assert list(idx) == list(idx2)
+            np.testing.assert_allclose(-v.real, c, rtol=1e-12, atol=1e-15 * np.abs(c).max())
+            assert np.all(v.imag == 0)
+
+
+def test_exprel_series_vs_direct(oracle_lib, sphere):
+    """Desingularised + static pieces reproduce the full Helmholtz kernel: the
+    far-pair element equals the (desingularised + FIBBI) sum whenever both
+    apply (GMatrixElements.cc:404-420 identity e^{ikr}/4pi r =
+    1/4pi r + ik/4pi + (ik)^2 r/8pi + desing)."""
+    G = oracle_lib.Geometry(sphere(2), oracle_lib.material(eps=4 + 0.2j))
+    M = G.assemble(1.0 + 0j)
+    assert np.array_equal(M, M.T)
+    assert np.all(np.isfinite(M))
+
+
+def test_mesh_dedupe_and_counts(oracle_lib, sphere, ref_mesh):
+    import meshgen
+    for n in (1, 2, 3):
+        G = oracle_lib.Geometry(sphere(n), oracle_lib.material(eps=4.0))
+        assert G.N == meshgen.num_bfs(n)
+    # Sphere_48 carries a duplicate of the origin (node 20 ~ node 1): merged
+    G = oracle_lib.Geometry(ref_mesh("sphere48"), oracle_lib.material(eps=10.0))
+    assert G.N == 48
+
+
+def mie(eps, x, nmax=30):
+    m = np.sqrt(complex(eps))
+    mx = m * x
+    csca = cext = 0.0
+    for n in range(1, nmax):
+        jx, djx = sp.spherical_jn(n, x), sp.spherical_jn(n, x, True)
+        yx, dyx = sp.spherical_yn(n, x), sp.spherical_yn(n, x, True)
+        jm, djm = sp.spherical_jn(n, mx), sp.spherical_jn(n, mx, True)
+        psi, dpsi = x * jx, jx + x * djx
+        xi, dxi = x * (jx + 1j * yx), (jx + 1j * yx) + x * (djx + 1j * dyx)
+        psim, dpsim = mx * jm, jm + mx * djm
+        a = (m * psim * dpsi - psi * dpsim) / (m * psim * dxi - xi * dpsim)
+        b = (psim * dpsi - m * psi * dpsim) / (psim * dxi - m * xi * dpsim)
+        csca += (2 * n + 1) * (abs(a) ** 2 + abs(b) ** 2)
+        cext += (2 * n + 1) * (a + b).real
+    k = x
+    return 2 * np.pi / k ** 2 * (cext - csca), 2 * np.pi / k ** 2 * csca
+
+
+def test_oracle_mie_convergence(oracle_lib, sphere):
+    """Absorption/scattering cross sections approach the Mie series as the
+    mesh is refined, and the EMT and overlap absorbed powers agree."""
+    cabs, csca = mie(4 + 0.2j, 1.0)
+    iinc = 1.0 / (2 * 376.73031346177)
+    errs = []
+    for n in (3, 4):
+        G = oracle_lib.Geometry(sphere(n), oracle_lib.material(eps=4 + 0.2j), nang=6)
+        M = G.assemble(1.0 + 0j)
+        E0, nh = np.array([1, 0, 0], complex), np.array([0, 0, 1.0])
+        J = sl.lu_solve(sl.lu_factor(M), G.rhs_planewave(1.0 + 0j, E0, nh))
+        pe = G.pft_emt(1.0 + 0j, J, E0, nh)[0] / iinc
+        po = G.pft_opft(1.0 + 0j, J)[0] / iinc
+        assert abs(pe[0] / po - 1) < 0.15
+        errs.append((abs(pe[0] / cabs - 1), abs(pe[1] / csca - 1)))
+    assert errs[1][0] < errs[0][0] and errs[1][1] < errs[0][1]
+    assert errs[1][0] < 0.5 and errs[1][1] < 0.5
