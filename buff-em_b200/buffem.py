@@ -72,6 +72,7 @@ EXPORTS = [
     "bg_matrix_device_ptr", "bg_lu_factor", "bg_lu_pivots", "bg_lu_solve", "bg_lu_solve_device",
     "bg_rhs_planewave", "bg_rhs_planewave_device", "bg_pft", "bg_kernel_launch_count",
     "bg_synchronize", "bg_stream", "bg_profile_begin", "bg_profile_read", "bg_profile_end",
+    "bg_zgemm_sub_device",
 ]
 
 
@@ -111,6 +112,7 @@ def lib():
         L.bg_kernel_launch_count.restype = C.c_longlong
         L.bg_stream.restype = VP
         L.bg_profile_read.argtypes = [I, VP, VP, VP]
+        L.bg_zgemm_sub_device.argtypes = [I, I, I, VP, I, VP, I, VP, I]
         _LIB = L
     return _LIB
 
@@ -200,7 +202,9 @@ class SWGGeometry:
             _check(lib().bg_geometry_create(GeoFileName.encode(), C.byref(h)))
         else:
             if isinstance(meshfiles, str):
-                meshfiles, materials = [meshfiles], [materials]
+                meshfiles = [meshfiles]
+            if isinstance(materials, bg_material):
+                materials = [materials]
             n = len(meshfiles)
             names = (C.c_char_p * n)(*[m.encode() for m in meshfiles])
             mats = (bg_material * n)(*materials)
@@ -267,6 +271,15 @@ class SWGGeometry:
         nh = _ptr(IF.nHat) if IF is not None else None
         _check(lib().bg_pft(self.h, Omega.real, Omega.imag, _ptr(Jc), E0, nh, method, _ptr(out)))
         return out
+
+
+def zgemm_sub_device(M, N, K, A, lda, B, ldb, C, ldc):
+    """C -= A @ B on device pointers (complex128, column-major)."""
+    _check(lib().bg_zgemm_sub_device(M, N, K, C_void(A), lda, C_void(B), ldb, C_void(C), ldc))
+
+
+def C_void(p):
+    return C.c_void_p(p)
 
 
 def launch_count():

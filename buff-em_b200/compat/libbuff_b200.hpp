@@ -1,0 +1,152 @@
+// libbuff_b200.hpp -- header-only C++ layer that recreates the libbuff /
+// libhmat names used on the VIE hot path on top of the C-ABI of
+// include/buffem_b200.h, so a buff-scatter-style driver switches by changing
+// its include and namespace:
+//
+//   buff::SWGGeometry *G = new buff::SWGGeometry(GeoFile);   // SWGGeometry.cc:214
+//   HMatrix *M = G->AllocateVIEMatrix();                      // VIEMatrix.cc:465
+//   HVector *J = G->AllocateRHSVector();                      // RHSVector.cc:49
+//   G->AssembleVIEMatrix(Omega, M);                           // VIEMatrix.cc:431
+//   M->LUFactorize();                                         // buff-scatter.cc:285
+//   G->AssembleRHSVector(Omega, IF, J);                       // RHSVector.cc:85
+//   M->LUSolve(J);                                            // buff-scatter.cc:314
+//   HMatrix *PFT = G->GetPFTMatrix(J, Omega, IF);             // GetPFT.cc:133
+//
+// Differences from the reference: errors throw buff_b200::Error (carrying the
+// C-ABI status and message) instead of calling ErrExit; the matrix lives on the
+// device and GetEntry copies it to the host lazily; the incident field is a
+// plane wave (libIncField's PlaneWave, E0 exp(i k nhat.x)).
+#pragma once
+
+#include <complex>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/buffem_b200.h"
+
+namespace buff_b200 {
+
+typedef std::complex<double> cdouble;
+
+struct Error : std::runtime_error {
+  int status;
+  Error(int st, const char *msg) : std::runtime_error(std::string(msg)), status(st) {}
+};
+
+inline int check(int st) {
+  if (st < 0) throw Error(st, bg_last_error());
+  return st;
+}
+
+class HVector {
+ public:
+  int N;
+  std::vector<cdouble> v;
+  explicit HVector(int n) : N(n), v((size_t)n) {}
+  cdouble GetEntry(int i) const { return v[(size_t)i]; }
+  void SetEntry(int i, cdouble x) { v[(size_t)i] = x; }
+  double *data() { return reinterpret_cast<double *>(v.data()); }
+};
+
+class HMatrix {
+ public:
+  int NR, NC;
+  bg_matrix *m = nullptr;
+  HMatrix(bg_geometry *g, int nr, int precision = BG_C128) : NR(nr), NC(nr) {
+    check(bg_matrix_create(g, precision, &m));
+  }
+  ~HMatrix() { bg_matrix_destroy(m); }
+  HMatrix(const HMatrix &) = delete;
+  HMatrix &operator=(const HMatrix &) = delete;
+
+  // HMatrix::LUFactorize -> zgetrf semantics; returns LAPACK info
+  int LUFactorize() {
+    int info = check(bg_lu_factor(m));
+    host_.clear();
+    if (info > 0) throw Error(info, "LUFactorize: singular matrix");
+    return info;
+  }
+  // HMatrix::LUSolve(HVector*) -> zgetrs
+  HVector *LUSolve(HVector *X) {
+    check(bg_lu_solve(m, X->data(), 1));
+    return X;
+  }
+  // multi-RHS form: column-major N x nrhs
+  void LUSolve(cdouble *B, int nrhs) { check(bg_lu_solve(m, reinterpret_cast<double *>(B), nrhs)); }
+
+  cdouble GetEntry(int r, int c) {
+    if (host_.empty()) {
+      host_.resize((size_t)NR * NC);
+      check(bg_matrix_download(m, host_.data()));
+    }
+    return host_[(size_t)r + (size_t)c * NR];
+  }
+  void invalidate() { host_.clear(); }
+
+ private:
+  std::vector<cdouble> host_;
+};
+
+// SCUFF-EM PlaneWave(E0, nHat)
+struct PlaneWave {
+  cdouble E0[3];
+  double nHat[3];
+  PlaneWave(const cdouble pE0[3], const double pnHat[3]) {
+    for (int i = 0; i < 3; i++) { E0[i] = pE0[i]; nHat[i] = pnHat[i]; }
+  }
+};
+
+class SWGGeometry {
+ public:
+  int NumObjects = 0, TotalBFs = 0;
+  std::vector<int> BFIndexOffset;
+  bg_geometry *g = nullptr;
+
+  explicit SWGGeometry(const char *GeoFileName) {
+    check(bg_geometry_create(GeoFileName, &g));
+    init();
+  }
+  SWGGeometry(int nobj, const char *const *meshes, const double *disp, const bg_material *mats) {
+    check(bg_geometry_create_objects(nobj, meshes, disp, mats, &g));
+    init();
+  }
+  ~SWGGeometry() { bg_geometry_destroy(g); }
+  SWGGeometry(const SWGGeometry &) = delete;
+  SWGGeometry &operator=(const SWGGeometry &) = delete;
+
+  HMatrix *AllocateVIEMatrix(bool PureImagFreq = false) {
+    (void)PureImagFreq;
+    return new HMatrix(g, TotalBFs);
+  }
+  HMatrix *AssembleVIEMatrix(cdouble Omega, HMatrix *M) {
+    if (!M) M = AllocateVIEMatrix();
+    check(bg_assemble(g, Omega.real(), Omega.imag(), M->m));
+    M->invalidate();
+    return M;
+  }
+  HVector *AllocateRHSVector() { return new HVector(TotalBFs); }
+  HVector *AssembleRHSVector(cdouble Omega, const PlaneWave *IF, HVector *RHS) {
+    if (!RHS) RHS = AllocateRHSVector();
+    check(bg_rhs_planewave(g, Omega.real(), Omega.imag(), reinterpret_cast<const double *>(IF->E0), IF->nHat,
+                           RHS->data()));
+    return RHS;
+  }
+  // rows = objects; columns PAbs, PScat (PFT_PABS, PFT_PSCAT)
+  std::vector<double> GetPFTMatrix(HVector *J, cdouble Omega, const PlaneWave *IF, int method = BG_PFT_EMT) {
+    std::vector<double> out(2 * (size_t)NumObjects);
+    check(bg_pft(g, Omega.real(), Omega.imag(), J->data(), IF ? reinterpret_cast<const double *>(IF->E0) : nullptr,
+                 IF ? IF->nHat : nullptr, method, out.data()));
+    return out;
+  }
+
+ private:
+  void init() {
+    NumObjects = bg_geometry_num_objects(g);
+    TotalBFs = bg_geometry_num_bfs(g);
+    for (int i = 0; i <= NumObjects; i++) BFIndexOffset.push_back(bg_geometry_bf_offset(g, i));
+  }
+};
+
+}  // namespace buff_b200

@@ -362,6 +362,15 @@ int bg_pft(bg_geometry *g, double wr, double wi, const double *J, const double *
   return st;
 }
 
+int bg_zgemm_sub_device(int M, int N, int K, const void *A, int lda, const void *B, int ldb, void *C, int ldc) {
+  if (M < 0 || N < 0 || K < 0 || (M && N && K && (!A || !B || !C)) || lda < M || ldb < K || ldc < M ||
+      lda < 1 || ldb < 1 || ldc < 1) {
+    set_error("bg_zgemm_sub_device: bad arguments");
+    return BG_ERR_ARG;
+  }
+  return zgemm_sub_device(M, N, K, A, lda, B, ldb, C, ldc);
+}
+
 long long bg_kernel_launch_count(void) { return g_launches.load(); }
 
 int bg_profile_begin(void) {

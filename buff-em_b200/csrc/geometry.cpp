@@ -322,14 +322,16 @@ int build_near_lists(bg_geometry *g) {
     int idx[4];
     for (int sa = 0; sa < 2; sa++)
       for (int sb = 0; sb < 2; sb++) {
+        // ordered (row tetrahedron, column tetrahedron): the angular rule of
+        // the singular integrals follows the row tetrahedron's vertex order
+        // (CompareTets, SWGVolume.cc:357-400), so (x,y) and (y,x) are distinct
         int x = ta[sa], y = tb[sb];
-        int lo = std::min(x, y), hi = std::max(x, y);
-        uint64_t key = ((uint64_t)(uint32_t)lo << 32) | (uint32_t)hi;
+        uint64_t key = ((uint64_t)(uint32_t)x << 32) | (uint32_t)y;
         auto it = key2tp.find(key);
         int id;
-        if (it == key2tp.end()) { id = (int)tps.size(); key2tp.emplace(key, id); tps.push_back(make_int2(lo, hi)); }
+        if (it == key2tp.end()) { id = (int)tps.size(); key2tp.emplace(key, id); tps.push_back(make_int2(x, y)); }
         else id = it->second;
-        idx[2 * sa + sb] = id | ((x > y) ? (1 << 30) : 0);
+        idx[2 * sa + sb] = id;
       }
     pairTP[k] = make_int4(idx[0], idx[1], idx[2], idx[3]);
   }

@@ -143,5 +143,6 @@ int pft(bg_geometry *g, double wr, double wi, const void *dJ, const double *E0, 
         double *out);
 int lu_factor(bg_matrix *m);
 int lu_solve(bg_matrix *m, void *dB, int ldb, int nrhs);
+int zgemm_sub_device(int M, int N, int K, const void *A, int lda, const void *B, int ldb, void *C, int ldc);
 void gauss_legendre01(int n, double *x, double *w);
 }  // namespace bg

@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 
 #include "internal.h"
 
@@ -27,23 +28,25 @@ namespace bg {
 struct cdl { double r, i; };
 
 // =========================================================================
-// complex GEMM  C(MxN) -= A(MxK) * B(KxN), column-major, complex128.
-// CTA tile 64x64, 4 warps of 32x32, K chunk 16, 3-stage cp.async pipeline.
-// Shared tiles are complex-interleaved: one 16-byte load feeds both the real
-// and the imaginary fragment.  Padding makes the fragment loads conflict-free.
+// complex GEMM  C(MxN) -= A(MxK) * B(KxN), column-major, complex128, on the
+// FP64 tensor cores with mma.sync m16n8k16 f64 (the sm_90+/sm_100 DMMA shape:
+// 2048 FMAs per instruction).  Warp tile 32x32 complex (2 x m16, 4 x n8),
+// CTA tile BM x BN, K chunk BK, STAGES-deep cp.async pipeline.  Shared tiles
+// are complex-interleaved (one 16-byte load gives re and im); row strides are
+// padded so every fragment load phase hits 32 distinct banks.
+//   Cr += Ar Br + Ai (-Bi),   Ci += Ar Bi + Ai Br        (4M product)
+// Fragment layouts (m16n8k16, lane = 4*t1 + t0):
+//   A: a[v] = A[t1 + 8(v&1)][t0 + 4(v>>1)], v = 0..7
+//   B: b[v] = B[t0 + 4v][t1],               v = 0..3
+//   C: c[v] = C[t1 + 8(v>>1)][2 t0 + (v&1)]
 // =========================================================================
-#define GBM 64
-#define GBN 64
-#define GBK 16
-#define GST 3
-#define APAD 66   // As[k][m] row stride (complex)
-#define BPAD 20   // Bs[n][k] row stride (complex)
-#define GEMM_SMEM (GST * (GBK * APAD + GBN * BPAD) * 16)
-
-__device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(d0), "+d"(d1)
-               : "d"(a), "d"(b));
+__device__ __forceinline__ void dmma16(double (&d)[4], const double (&a)[8], const double (&b)[4]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+      "{%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]),
+        "d"(b[1]), "d"(b[2]), "d"(b[3]));
 }
 
 __device__ __forceinline__ void cp16(void *smem, const void *gmem, bool pred) {
@@ -55,169 +58,195 @@ __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_grou
 template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
-__global__ void __launch_bounds__(128) k_zgemm_sub(int M, int N, int K, const cdl *__restrict__ A, size_t lda,
-                                                   const cdl *__restrict__ B, size_t ldb, cdl *C, size_t ldc) {
+template <int BM, int BN, int BK, int STAGES>
+struct GemmCfg {
+  static constexpr int WM = BM / 32, WN = BN / 32, THREADS = WM * WN * 32;
+  static constexpr int AP = BM + 2;   // As[k][m] stride (complex), = 2 mod 8
+  static constexpr int BP = BK + 4;   // Bs[n][k] stride (complex), = 4 mod 8
+  static constexpr int SMEM = STAGES * (BK * AP + BN * BP) * 16;
+};
+
+template <int BM, int BN, int BK, int STAGES>
+__global__ void __launch_bounds__(GemmCfg<BM, BN, BK, STAGES>::THREADS)
+    k_zgemm_sub(int M, int N, int K, const cdl *__restrict__ A, size_t lda, const cdl *__restrict__ B, size_t ldb,
+                cdl *C, size_t ldc) {
+  using Cfg = GemmCfg<BM, BN, BK, STAGES>;
+  constexpr int T = Cfg::THREADS, AP = Cfg::AP, BP = Cfg::BP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  cdl *As = (cdl *)smem_raw;                       // [GST][GBK][APAD]
-  cdl *Bs = As + GST * GBK * APAD;                 // [GST][GBN][BPAD]
-  int m0 = blockIdx.x * GBM, n0 = blockIdx.y * GBN;
-  int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  int wm = warp & 1, wn = warp >> 1;
-  double cr[4][4][2], ci[4][4][2];
+  cdl *As = (cdl *)smem_raw;              // [STAGES][BK][AP]
+  cdl *Bs = As + STAGES * BK * AP;        // [STAGES][BN][BP]
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp % Cfg::WM, wn = warp / Cfg::WM;
+  const int t0 = lane & 3, t1 = lane >> 2;
+  double cr[2][4][4], ci[2][4][4];
 #pragma unroll
-  for (int i = 0; i < 4; i++)
+  for (int i = 0; i < 2; i++)
 #pragma unroll
-    for (int j = 0; j < 4; j++) cr[i][j][0] = cr[i][j][1] = ci[i][j][0] = ci[i][j][1] = 0.0;
-  int nchunks = (K + GBK - 1) / GBK;
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int v = 0; v < 4; v++) cr[i][j][v] = ci[i][j][v] = 0.0;
+  const int nchunks = (K + BK - 1) / BK;
   auto load_chunk = [&](int chunk, int stage) {
-    int k0 = chunk * GBK;
-    cdl *as = As + stage * GBK * APAD;
-    cdl *bs = Bs + stage * GBN * BPAD;
+    const int k0 = chunk * BK;
+    cdl *as = As + stage * BK * AP;
+    cdl *bs = Bs + stage * BN * BP;
 #pragma unroll
-    for (int it = 0; it < 8; it++) {
-      int e = tid + it * 128;          // 0..1023
-      int r = e & 63, kk = e >> 6;     // A: row r, k kk
+    for (int it = 0; it < (BM * BK) / T; it++) {
+      int e = tid + it * T;
+      int r = e % BM, kk = e / BM;
       int gr = m0 + r, gk = k0 + kk;
       bool ok = gr < M && gk < K;
-      const cdl *src = ok ? A + (size_t)gk * lda + gr : A;
-      cp16(as + kk * APAD + r, src, ok);
-      int kb = e & 15, nb = e >> 4;    // B: k kb, col nb
-      int gkb = k0 + kb, gn = n0 + nb;
-      bool okb = gkb < K && gn < N;
-      const cdl *srcb = okb ? B + (size_t)gn * ldb + gkb : B;
-      cp16(bs + nb * BPAD + kb, srcb, okb);
+      cp16(as + kk * AP + r, ok ? A + (size_t)gk * lda + gr : A, ok);
+    }
+#pragma unroll
+    for (int it = 0; it < (BK * BN) / T; it++) {
+      int e = tid + it * T;
+      int kb = e % BK, nb = e / BK;
+      int gk = k0 + kb, gn = n0 + nb;
+      bool ok = gk < K && gn < N;
+      cp16(bs + nb * BP + kb, ok ? B + (size_t)gn * ldb + gk : B, ok);
     }
   };
 #pragma unroll
-  for (int s = 0; s < GST - 1; s++) {
+  for (int s = 0; s < STAGES - 1; s++) {
     if (s < nchunks) load_chunk(s, s);
     cp_commit();
   }
   for (int chunk = 0; chunk < nchunks; chunk++) {
-    cp_wait<GST - 2>();
+    cp_wait<STAGES - 2>();
     __syncthreads();
-    int nxt = chunk + GST - 1;
-    if (nxt < nchunks) load_chunk(nxt, nxt % GST);
+    int nxt = chunk + STAGES - 1;
+    if (nxt < nchunks) load_chunk(nxt, nxt % STAGES);
     cp_commit();
-    const cdl *as = As + (chunk % GST) * GBK * APAD;
-    const cdl *bs = Bs + (chunk % GST) * GBN * BPAD;
+    const cdl *as = As + (chunk % STAGES) * BK * AP + wm * 32 + t1;
+    const cdl *bs = Bs + (chunk % STAGES) * BN * BP + (wn * 32 + t1) * BP + t0;
 #pragma unroll
-    for (int ks = 0; ks < GBK / 4; ks++) {
-      double ar[4], ai[4], br[4], bi[4];
+    for (int ks = 0; ks < BK / 16; ks++) {
+      double ar[2][8], ai[2][8];
 #pragma unroll
-      for (int mt = 0; mt < 4; mt++) {
-        cdl v = as[(ks * 4 + (lane & 3)) * APAD + wm * 32 + mt * 8 + (lane >> 2)];
-        ar[mt] = v.r;
-        ai[mt] = v.i;
-      }
+      for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+        for (int v = 0; v < 8; v++) {
+          cdl x = as[(ks * 16 + t0 + 4 * (v >> 1)) * AP + mt * 16 + 8 * (v & 1)];
+          ar[mt][v] = x.r;
+          ai[mt][v] = x.i;
+        }
 #pragma unroll
       for (int nt = 0; nt < 4; nt++) {
-        cdl v = bs[(wn * 32 + nt * 8 + (lane >> 2)) * BPAD + ks * 4 + (lane & 3)];
-        br[nt] = v.r;
-        bi[nt] = v.i;
-      }
+        double br[4], bi[4], nbi[4];
 #pragma unroll
-      for (int mt = 0; mt < 4; mt++) {
-        double nai = -ai[mt];
+        for (int v = 0; v < 4; v++) {
+          cdl x = bs[nt * 8 * BP + ks * 16 + 4 * v];
+          br[v] = x.r;
+          bi[v] = x.i;
+          nbi[v] = -x.i;
+        }
 #pragma unroll
-        for (int nt = 0; nt < 4; nt++) {
-          dmma(cr[mt][nt][0], cr[mt][nt][1], ar[mt], br[nt]);
-          dmma(cr[mt][nt][0], cr[mt][nt][1], nai, bi[nt]);
-          dmma(ci[mt][nt][0], ci[mt][nt][1], ar[mt], bi[nt]);
-          dmma(ci[mt][nt][0], ci[mt][nt][1], ai[mt], br[nt]);
+        for (int mt = 0; mt < 2; mt++) {
+          dmma16(cr[mt][nt], ar[mt], br);
+          dmma16(cr[mt][nt], ai[mt], nbi);
+          dmma16(ci[mt][nt], ar[mt], bi);
+          dmma16(ci[mt][nt], ai[mt], br);
         }
       }
     }
   }
   cp_wait<0>();
-  // epilogue: C -= acc
 #pragma unroll
-  for (int mt = 0; mt < 4; mt++) {
-    int row = m0 + wm * 32 + mt * 8 + (lane >> 2);
-    if (row >= M) continue;
+  for (int mt = 0; mt < 2; mt++)
 #pragma unroll
     for (int nt = 0; nt < 4; nt++)
 #pragma unroll
-      for (int h = 0; h < 2; h++) {
-        int col = n0 + wn * 32 + nt * 8 + 2 * (lane & 3) + h;
-        if (col < N) {
+      for (int v = 0; v < 4; v++) {
+        int row = m0 + wm * 32 + mt * 16 + t1 + 8 * (v >> 1);
+        int col = n0 + wn * 32 + nt * 8 + 2 * t0 + (v & 1);
+        if (row < M && col < N) {
           cdl *p = C + (size_t)col * ldc + row;
-          cdl v = *p;
-          v.r -= cr[mt][nt][h];
-          v.i -= ci[mt][nt][h];
-          *p = v;
+          cdl x = *p;
+          x.r -= cr[mt][nt][v];
+          x.i -= ci[mt][nt][v];
+          *p = x;
         }
       }
-  }
 }
+
+#ifndef ZG_BM
+#define ZG_BM 64
+#define ZG_BN 64
+#define ZG_BK 16
+#define ZG_ST 3
+#endif
 
 static int zgemm_sub(int M, int N, int K, const cdl *A, size_t lda, const cdl *B, size_t ldb, cdl *C, size_t ldc) {
   if (M <= 0 || N <= 0 || K <= 0) return BG_OK;
+  using Cfg = GemmCfg<ZG_BM, ZG_BN, ZG_BK, ZG_ST>;
+  auto kern = k_zgemm_sub<ZG_BM, ZG_BN, ZG_BK, ZG_ST>;
   static bool attr = false;
   if (!attr) {
-    BG_CUDA_TRY(cudaFuncSetAttribute(k_zgemm_sub, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM));
+    BG_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM));
     attr = true;
   }
-  dim3 grid((M + GBM - 1) / GBM, (N + GBN - 1) / GBN);
+  dim3 grid((M + ZG_BM - 1) / ZG_BM, (N + ZG_BN - 1) / ZG_BN);
   if (grid.y > 65535) { set_error("zgemm: N too large"); return BG_ERR_ARG; }
   prof_start(PROF_GEMM);
-  k_zgemm_sub<<<grid, 128, GEMM_SMEM, stream()>>>(M, N, K, A, lda, B, ldb, C, ldc);
+  kern<<<grid, Cfg::THREADS, Cfg::SMEM, stream()>>>(M, N, K, A, lda, B, ldb, C, ldc);
   BG_LAUNCHED();
   prof_stop(PROF_GEMM, 8.0 * M * (double)N * K);
   return BG_OK;
 }
 
 // =========================================================================
-// leaf triangular solves (n <= 64 rows), 16 right-hand-side columns per CTA
+// leaf triangular solves (n <= 64 rows).  The triangle is staged in shared
+// memory once per CTA; each warp then solves whole right-hand-side columns:
+// lane l holds rows l and l+32 of the column in registers, the solved entry
+// of step i is broadcast with a warp shuffle, and every lane updates its two
+// rows -- no block barriers inside the substitution.
 // =========================================================================
-#define TRS_COLS 16
-#define TRS_SMEM ((64 * 65 + 64 * (TRS_COLS + 1)) * 16)
-__global__ void __launch_bounds__(256) k_trsm_leaf(int n, int m, const cdl *T, size_t ldt, cdl *B, size_t ldb,
-                                                   int upper) {
+#define TRS_WARPS 8
+#define TRS_CPW 8                         // columns per warp per CTA
+#define TRS_COLS (TRS_WARPS * TRS_CPW)
+#define TRS_SMEM (64 * 65 * 16)
+__device__ __forceinline__ cdl cshfl(cdl v, int src) {
+  return cdl{__shfl_sync(0xffffffffu, v.r, src), __shfl_sync(0xffffffffu, v.i, src)};
+}
+__global__ void __launch_bounds__(TRS_WARPS * 32) k_trsm_leaf(int n, int m, const cdl *T, size_t ldt, cdl *B,
+                                                              size_t ldb, int upper) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  cdl(*Ts)[65] = (cdl(*)[65])smem_raw;
-  cdl(*Bt)[TRS_COLS + 1] = (cdl(*)[TRS_COLS + 1])(smem_raw + 64 * 65 * 16);
-  int c0 = blockIdx.x * TRS_COLS;
-  int tid = threadIdx.x;
-  for (int e = tid; e < n * n; e += 256) {
+  cdl(*Ts)[65] = (cdl(*)[65])smem_raw;   // Ts[r][c]
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int e = tid; e < n * n; e += TRS_WARPS * 32) {
     int r = e % n, c = e / n;
     Ts[r][c] = T[(size_t)c * ldt + r];
   }
-  for (int e = tid; e < n * TRS_COLS; e += 256) {
-    int r = e % n, c = e / n;
-    Bt[r][c] = (c0 + c < m) ? B[(size_t)(c0 + c) * ldb + r] : cdl{0, 0};
-  }
   __syncthreads();
-  if (!upper) {
-    for (int i = 0; i < n; i++) {
-      for (int e = tid; e < (n - 1 - i) * TRS_COLS; e += 256) {
-        int r = i + 1 + e / TRS_COLS, c = e % TRS_COLS;
-        cdl l = Ts[r][i], x = Bt[i][c];
-        Bt[r][c].r -= l.r * x.r - l.i * x.i;
-        Bt[r][c].i -= l.r * x.i + l.i * x.r;
+  const int r0 = lane, r1 = lane + 32;
+  for (int j = 0; j < TRS_CPW; j++) {
+    const int col = blockIdx.x * TRS_COLS + warp * TRS_CPW + j;
+    if (col >= m) break;
+    cdl *bc = B + (size_t)col * ldb;
+    cdl b0 = r0 < n ? bc[r0] : cdl{0, 0};
+    cdl b1 = r1 < n ? bc[r1] : cdl{0, 0};
+    if (!upper) {
+      for (int i = 0; i < n; i++) {
+        cdl x = cshfl(i < 32 ? b0 : b1, i & 31);
+        if (r0 > i && r0 < n) { cdl l = Ts[r0][i]; b0.r -= l.r * x.r - l.i * x.i; b0.i -= l.r * x.i + l.i * x.r; }
+        if (r1 > i && r1 < n) { cdl l = Ts[r1][i]; b1.r -= l.r * x.r - l.i * x.i; b1.i -= l.r * x.i + l.i * x.r; }
       }
-      __syncthreads();
-    }
-  } else {
-    for (int i = n - 1; i >= 0; i--) {
-      if (tid < TRS_COLS) {
-        cdl u = Ts[i][i], b = Bt[i][tid];
+    } else {
+      for (int i = n - 1; i >= 0; i--) {
+        cdl v = cshfl(i < 32 ? b0 : b1, i & 31);
+        cdl u = Ts[i][i];
         double d = u.r * u.r + u.i * u.i;
-        Bt[i][tid] = cdl{(b.r * u.r + b.i * u.i) / d, (b.i * u.r - b.r * u.i) / d};
+        cdl x{(v.r * u.r + v.i * u.i) / d, (v.i * u.r - v.r * u.i) / d};
+        if (r0 == i) b0 = x;
+        if (r1 == i) b1 = x;
+        if (r0 < i) { cdl t = Ts[r0][i]; b0.r -= t.r * x.r - t.i * x.i; b0.i -= t.r * x.i + t.i * x.r; }
+        if (r1 < i) { cdl t = Ts[r1][i]; b1.r -= t.r * x.r - t.i * x.i; b1.i -= t.r * x.i + t.i * x.r; }
       }
-      __syncthreads();
-      for (int e = tid; e < i * TRS_COLS; e += 256) {
-        int r = e / TRS_COLS, c = e % TRS_COLS;
-        cdl uu = Ts[r][i], x = Bt[i][c];
-        Bt[r][c].r -= uu.r * x.r - uu.i * x.i;
-        Bt[r][c].i -= uu.r * x.i + uu.i * x.r;
-      }
-      __syncthreads();
     }
-  }
-  for (int e = tid; e < n * TRS_COLS; e += 256) {
-    int r = e % n, c = e / n;
-    if (c0 + c < m) B[(size_t)(c0 + c) * ldb + r] = Bt[r][c];
+    if (r0 < n) bc[r0] = b0;
+    if (r1 < n) bc[r1] = b1;
   }
 }
 
@@ -232,7 +261,7 @@ static int trsm(int n, int m, const cdl *T, size_t ldt, cdl *B, size_t ldb, int 
     }
     int blocks = (m + TRS_COLS - 1) / TRS_COLS;
     prof_start(PROF_TRSM);
-    k_trsm_leaf<<<blocks, 256, TRS_SMEM, stream()>>>(n, m, T, ldt, B, ldb, upper);
+    k_trsm_leaf<<<blocks, TRS_WARPS * 32, TRS_SMEM, stream()>>>(n, m, T, ldt, B, ldb, upper);
     BG_LAUNCHED();
     prof_stop(PROF_TRSM, 4.0 * n * (double)n * m);
     return BG_OK;
@@ -398,12 +427,16 @@ struct LUWork {
   int *info;
 };
 
-static int panel_grid = 0, panel_smem_max = 0;
+static int panel_grid = 0, panel_smem_max = 0, panel_rows_target = 256;
 
 static int panel_leaf(bg_matrix *m, const LUWork &W, int k0, int w) {
   int N = m->N;
   int Mp = N - k0;
-  int G = std::min(panel_grid, std::max(1, (Mp + 31) / 32));
+  // fewer CTAs make the per-column grid barrier and the candidate reduction
+  // cheaper; the slice of each CTA must still fit in shared memory
+  int G = std::min(panel_grid, std::max(8, (Mp + panel_rows_target - 1) / panel_rows_target));
+  G = std::min(G, std::max(1, (Mp + 31) / 32));
+  while (G < panel_grid && (size_t)((Mp + G - 1) / G) * w * sizeof(cdl) > (size_t)panel_smem_max) G++;
   int rows = (Mp + G - 1) / G;
   size_t smem = (size_t)rows * w * sizeof(cdl);
   if ((int)smem > panel_smem_max) {
@@ -459,7 +492,8 @@ int lu_factor(bg_matrix *m) {
     int per_sm = 0;
     BG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_panel, 256, panel_smem_max));
     if (per_sm < 1) { set_error("panel kernel cannot be resident"); return BG_ERR_CUDA; }
-    panel_grid = sms;  // one CTA per SM (cooperative residency)
+    panel_grid = sms;  // at most one CTA per SM (cooperative residency)
+    if (const char *e = std::getenv("BG_PANEL_ROWS")) panel_rows_target = std::max(32, std::atoi(e));
   }
   size_t need = sizeof(double) * 2 * panel_grid + sizeof(int) * 2 * panel_grid + sizeof(cdl) * 2 * panel_grid * 32 +
                 sizeof(cdl) * 64 + 64;
@@ -483,6 +517,12 @@ int lu_factor(bg_matrix *m) {
   BG_CUDA_TRY(cudaMemcpyAsync(&info, W.info, sizeof(int), cudaMemcpyDeviceToHost, stream()));
   BG_CUDA_TRY(cudaStreamSynchronize(stream()));
   return info;
+}
+
+int zgemm_sub_device(int M, int N, int K, const void *A, int lda, const void *B, int ldb, void *C, int ldc) {
+  int st = ensure_device();
+  if (st) return st;
+  return zgemm_sub(M, N, K, (const cdl *)A, (size_t)lda, (const cdl *)B, (size_t)ldb, (cdl *)C, (size_t)ldc);
 }
 
 // zgetrs: B <- U^{-1} L^{-1} P B

@@ -144,6 +144,12 @@ int bg_lu_solve(bg_matrix *m, double *B_host, int nrhs);
 /* Same with B already on the device (leading dimension ldb, complex128). */
 int bg_lu_solve_device(bg_matrix *m, void *B_dev, int ldb, int nrhs);
 
+/* C <- C - A*B for device column-major complex128 matrices (A: M x K, B: K x N,
+   C: M x N), the FP64 tensor-core GEMM of the LU trailing update.  Also the
+   building block of buff-neq's dressed-Rytov chain (GetFlux.cc:155-272, four
+   GEMMs per source object).  Runs on the library stream. */
+int bg_zgemm_sub_device(int M, int N, int K, const void *A, int lda, const void *B, int ldb, void *C, int ldc);
+
 /* ---------------------------------------------------------------------------
  * right-hand side and post-processing
  * ------------------------------------------------------------------------- */

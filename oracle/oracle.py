@@ -99,6 +99,7 @@ class Geometry:
         L = lib()
         if isinstance(meshfiles, str):
             meshfiles = [meshfiles]
+        if isinstance(materials, OMat):
             materials = [materials]
         n = len(meshfiles)
         arr = (C.c_char_p * n)(*[m.encode() for m in meshfiles])

@@ -1,0 +1,38 @@
+// buff-scatter-style driver on the libbuff-compatible C++ layer
+// (pattern of buff-scatter.cc:236-347 and unit-test-LFField.cc:50-71).
+// usage: scatter_driver <geo.buffgeo> <omega> [geometry-only]
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+
+#include "../../buff-em_b200/compat/libbuff_b200.hpp"
+
+using namespace buff_b200;
+
+int main(int argc, char **argv) {
+  if (argc < 3) return 2;
+  try {
+    SWGGeometry G(argv[1]);
+    std::printf("objects %d bfs %d\n", G.NumObjects, G.TotalBFs);
+    if (argc > 3 && !std::strcmp(argv[3], "geometry-only")) return 0;
+    cdouble Omega(std::atof(argv[2]), 0.0);
+    HMatrix *M = G.AllocateVIEMatrix();
+    HVector *J = G.AllocateRHSVector();
+    G.AssembleVIEMatrix(Omega, M);
+    M->LUFactorize();
+    const cdouble E0[3] = {1.0, 0.0, 0.0};
+    const double nHat[3] = {0.0, 0.0, 1.0};
+    PlaneWave PW(E0, nHat);
+    G.AssembleRHSVector(Omega, &PW, J);
+    M->LUSolve(J);
+    std::vector<double> P = G.GetPFTMatrix(J, Omega, &PW);
+    std::printf("J0 %.17g %.17g\n", J->GetEntry(0).real(), J->GetEntry(0).imag());
+    std::printf("PAbs %.17g PScat %.17g\n", P[0], P[1]);
+    delete M;
+    delete J;
+  } catch (const Error &e) {
+    std::fprintf(stderr, "error %d: %s\n", e.status, e.what());
+    return 1;
+  }
+  return 0;
+}

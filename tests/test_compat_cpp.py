@@ -1,0 +1,50 @@
+"""The libbuff-compatible C++ layer (buff-em_b200/compat/libbuff_b200.hpp)
+compiles against the C-ABI and drives the path like buff-scatter does."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import buffem
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def driver(tmp_path_factory):
+    out = str(tmp_path_factory.mktemp("cpp") / "scatter_driver")
+    lib = os.path.join(ROOT, "buff-em_b200")
+    subprocess.run(["/usr/bin/g++", "-O2", "-std=c++17", os.path.join(ROOT, "tests", "cpp", "scatter_driver.cpp"),
+                    "-L", lib, "-lbuffem_b200", f"-Wl,-rpath,{lib}", "-o", out], check=True)
+    return out
+
+
+def geo(tmp_path, mesh, eps="4+0.2i"):
+    p = tmp_path / "g.buffgeo"
+    p.write_text(f"OBJECT S\n MESHFILE {mesh}\n MATERIAL CONST_EPS_{eps}\nENDOBJECT\n")
+    return str(p)
+
+
+def test_compat_geometry(driver, sphere, tmp_path):
+    r = subprocess.run([driver, geo(tmp_path, sphere(2)), "1.0", "geometry-only"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert "bfs 72" in r.stdout
+
+
+@pytest.mark.gpu
+def test_compat_drive_matches_python(driver, sphere, tmp_path):
+    g = geo(tmp_path, sphere(3))
+    r = subprocess.run([driver, g, "1.0"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    vals = dict(line.split(" ", 1) for line in r.stdout.strip().splitlines())
+    j0 = complex(*map(float, vals["J0"].split()))
+    pabs = float(vals["PAbs"].split()[0])
+    G = buffem.SWGGeometry(g)
+    M = G.AssembleVIEMatrix(1.0)
+    M.LUFactorize()
+    pw = buffem.PlaneWave([1, 0, 0], [0, 0, 1])
+    J = G.AssembleRHSVector(1.0, pw)
+    M.LUSolve(J)
+    assert abs(J[0] - j0) <= 1e-12 * abs(J[0])
+    assert abs(G.GetPFTMatrix(J, 1.0, pw)[0, 0] - pabs) <= 1e-10 * abs(pabs)
