@@ -219,7 +219,7 @@ def run_gpu(args, rank, world, local_rank):
     phases = {"assemble_s": ev[0].elapsed_time(ev[1]) / 1e3, "lu_s": ev[1].elapsed_time(ev[2]) / 1e3,
               "rhs_solve_s": ev[2].elapsed_time(ev[3]) / 1e3}
 
-    # ---------------- timed region (device)
+    # ---------------- timed region (device): plain FP64 path
     clocks = ClockSampler(local_rank)
     if world > 1:
         dist.barrier()
@@ -237,16 +237,70 @@ def run_gpu(args, rank, world, local_rank):
     torch.cuda.synchronize()
     prof = buffem.profile_read()
     buffem.profile_end()
-    launches = buffem.launch_count() - launches0
-    clk = clocks.stop()
-    elapsed = e0.elapsed_time(e1) / 1e3
-    if world > 1:
-        t = torch.tensor([elapsed], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
-        dist.barrier()
+    launches_fp64 = buffem.launch_count() - launches0
+    elapsed_fp64 = e0.elapsed_time(e1) / 1e3
+    x_fp64 = dB.clone()
 
-    # ---------------- e2e through host buffers
+    # ---------------- precision form: FP64 assembly -> complex64 copy ->
+    # tcgen05 TF32 LU -> FP64-refined solve
+    F = G.AllocateVIEMatrix(buffem.BG_C64)
+    stats = np.zeros(3)
+
+    def step_mixed():
+        buffem._check(L.bg_assemble(G.h, OMEGA, 0.0, M.h))
+        buffem._check(L.bg_matrix_convert(M.h, F.h))
+        buffem._check(L.bg_lu_factor(F.h))
+        for i in range(nrhs):
+            buffem._check(L.bg_rhs_planewave_device(G.h, OMEGA, 0.0, buffem._ptr(E0s[i]), buffem._ptr(nhs[i]),
+                                                    buffem.C.c_void_p(dB[i].data_ptr())))
+        buffem._check(L.bg_lu_solve_refined_device(M.h, F.h, buffem.C.c_void_p(dB.data_ptr()), N, nrhs,
+                                                   args.refine_tol, 60, buffem._ptr(stats)))
+
+    for _ in range(args.warmup):
+        step_mixed()
+    buffem.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+    ev[0].record(stream)
+    buffem._check(L.bg_assemble(G.h, OMEGA, 0.0, M.h))
+    ev[1].record(stream)
+    buffem._check(L.bg_matrix_convert(M.h, F.h))
+    buffem._check(L.bg_lu_factor(F.h))
+    ev[2].record(stream)
+    for i in range(nrhs):
+        buffem._check(L.bg_rhs_planewave_device(G.h, OMEGA, 0.0, buffem._ptr(E0s[i]), buffem._ptr(nhs[i]),
+                                                buffem.C.c_void_p(dB[i].data_ptr())))
+    ev[3].record(stream)
+    buffem._check(L.bg_lu_solve_refined_device(M.h, F.h, buffem.C.c_void_p(dB.data_ptr()), N, nrhs,
+                                               args.refine_tol, 60, buffem._ptr(stats)))
+    ev[4].record(stream)
+    buffem.synchronize()
+    phases_mixed = {"assemble_s": ev[0].elapsed_time(ev[1]) / 1e3, "convert_lu_s": ev[1].elapsed_time(ev[2]) / 1e3,
+                    "rhs_s": ev[2].elapsed_time(ev[3]) / 1e3, "refined_solve_s": ev[3].elapsed_time(ev[4]) / 1e3,
+                    "refine_sweeps": int(stats[0]), "final_rel_residual": float(stats[1]),
+                    "first_rel_residual": float(stats[2])}
+    launches1 = buffem.launch_count()
+    buffem.profile_begin()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(args.steps):
+        step_mixed()
+    e3.record(stream)
+    buffem.synchronize()
+    torch.cuda.synchronize()
+    prof_mixed = buffem.profile_read()
+    buffem.profile_end()
+    launches_mixed = buffem.launch_count() - launches1
+    clk = clocks.stop()
+    elapsed_mixed = e2.elapsed_time(e3) / 1e3
+    err = float(torch.linalg.norm(dB - x_fp64) / torch.linalg.norm(x_fp64))
+    if world > 1:
+        t = torch.tensor([elapsed_fp64, elapsed_mixed], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_fp64, elapsed_mixed = float(t[0].item()), float(t[1].item())
+        dist.barrier()
+    launches = launches_mixed
+
+    # ---------------- e2e through host buffers (precision form)
     hostB = np.zeros((N, nrhs), complex, order="F")
     rhs_h = np.zeros(N, complex)
     times = []
@@ -254,23 +308,25 @@ def run_gpu(args, rank, world, local_rank):
         buffem.synchronize()
         t0 = time.perf_counter()
         buffem._check(L.bg_assemble(G.h, OMEGA, 0.0, M.h))
-        buffem._check(L.bg_lu_factor(M.h))
+        buffem._check(L.bg_matrix_convert(M.h, F.h))
+        buffem._check(L.bg_lu_factor(F.h))
         for i in range(nrhs):
             buffem._check(L.bg_rhs_planewave(G.h, OMEGA, 0.0, buffem._ptr(E0s[i]), buffem._ptr(nhs[i]),
                                              buffem._ptr(rhs_h)))
             hostB[:, i] = rhs_h
-        buffem._check(L.bg_lu_solve(M.h, buffem._ptr(hostB), nrhs))
+        buffem._check(L.bg_lu_solve_refined(M.h, F.h, buffem._ptr(hostB), nrhs, args.refine_tol, 60,
+                                            buffem._ptr(stats)))
         times.append(time.perf_counter() - t0)
     e2e_s = max(times) if times else None
     if world > 1 and e2e_s is not None:
         t = torch.tensor([e2e_s], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
+    del F
+    return dict(N=N, elapsed=elapsed_mixed, elapsed_fp64=elapsed_fp64, phases=phases, phases_mixed=phases_mixed,
+                prof=prof, prof_mixed=prof_mixed, launches=launches, launches_fp64=launches_fp64, clocks=clk,
+                precompute_s=precompute_s, e2e_s=e2e_s, nrhs=nrhs, err_vs_fp64=err)
 
-    # accuracy of this frequency's solution (residual against the assembled matrix)
-    x = hostB[:, 0].copy()
-    return dict(N=N, elapsed=elapsed, phases=phases, prof=prof, launches=launches, clocks=clk,
-                precompute_s=precompute_s, e2e_s=e2e_s, nrhs=nrhs)
 
 
 # ------------------------------------------------------------------ CPU arm
@@ -323,6 +379,8 @@ def main():
     ap.add_argument("--kernel", default=None, choices=["gemm"],
                     help="time the LU trailing-update GEMM alone on an M=N=K problem")
     ap.add_argument("--size", type=int, default=8192)
+    ap.add_argument("--refine-tol", type=float, default=1e-12,
+                    help="relative residual target of the FP64 refinement (precision form)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "b200" else args.warmup
 
@@ -368,9 +426,14 @@ def main():
     res = run_gpu(args, rank, world, local_rank)
     N = res["N"]
     config["N"] = N
+    config["paths"] = "value: precision form (FP64 assembly, complex64 tcgen05/TF32 LU, FP64-refined solve); " \
+                      "fp64: plain path (FP64 assembly, DMMA LU, FP64 solve)"
     value = res["elapsed"] / args.steps / world    # whole-job seconds per frequency
+    value_fp64 = res["elapsed_fp64"] / args.steps / world
     gemm = res["prof"]["lu_gemm"]
     achieved = gemm["flops"] / (gemm["ms"] / 1e3) / 1e12 if gemm["ms"] > 0 else None
+    gm = res["prof_mixed"]["lu_gemm"]
+    achieved_tc = gm["flops"] / (gm["ms"] / 1e3) / 1e12 if gm["ms"] > 0 else None
     peak = None
     peak_src = None
     if rank == 0 and not args.lean:
@@ -379,19 +442,29 @@ def main():
             peak_src = "measured in-run: cuBLAS ZGEMM 8192^3 (torch complex128 matmul), best of 5"
         except Exception as e:  # pragma: no cover
             peak_src = f"unavailable: {e}"
-    total_lu_ms = sum(v["ms"] for v in res["prof"].values())
+    mp = measured_peaks()
+    bf16 = mp.get("bf16_tflops")
+    total_ms = sum(v["ms"] for v in res["prof"].values())
     line = {"metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": res["elapsed"] / args.steps * 1e3, "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic", "config": config,
-            "precompute_s": res["precompute_s"], "phases": res["phases"],
-            "roofline": {"bound": "tensor", "kernel": "k_zgemm_sub (LU trailing update, DMMA f64)",
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128 (complex64 TF32 tensor-core LU + FP64 refinement)",
+            "data": "synthetic", "config": config,
+            "fp64_path": {"value": value_fp64, "unit": "s", "phases": res["phases"],
+                          "speedup_of_precision_form": value_fp64 / value, "gpu_launches": res["launches_fp64"]},
+            "precision_form": {"phases": res["phases_mixed"], "err_vs_fp64_lu": res["err_vs_fp64"]},
+            "precompute_s": res["precompute_s"],
+            "roofline": {"bound": "tensor", "kernel": "k_zgemm_sub (FP64 path LU trailing update, DMMA f64)",
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": (achieved / peak) if (achieved and peak) else None, "traffic": None,
                          "peak_source": peak_src,
                          "algorithmic": "8*M*N*K flops per launch (4M complex product)",
-                         "gemm_share_of_profiled_ms": gemm["ms"] / total_lu_ms if total_lu_ms else None,
-                         "lu_flops_rate_tflops": (8 / 3 * N ** 3) / res["phases"]["lu_s"] / 1e12},
-            "kernel_classes": res["prof"],
+                         "gemm_share_of_profiled_ms": gemm["ms"] / total_ms if total_ms else None,
+                         "lu_flops_rate_tflops": (8 / 3 * N ** 3) / res["phases"]["lu_s"] / 1e12,
+                         "precision_form_gemm": {"kernel": "k_cgemm_tf32 (tcgen05 kind::tf32)",
+                                                 "achieved": achieved_tc, "unit": "TFLOP/s",
+                                                 "peak_bf16_dense_measured": bf16,
+                                                 "frac_of_bf16_peak": (achieved_tc / bf16) if (achieved_tc and bf16) else None}},
+            "kernel_classes": res["prof"], "kernel_classes_precision_form": res["prof_mixed"],
             "e2e": {"value": res["e2e_s"] / world if res["e2e_s"] else None, "unit": "s",
                     "h2d_bytes_per_step": 16 * N * res["nrhs"],
                     "d2h_bytes_per_step": 2 * 16 * N * res["nrhs"]},

@@ -72,7 +72,7 @@ EXPORTS = [
     "bg_matrix_device_ptr", "bg_lu_factor", "bg_lu_pivots", "bg_lu_solve", "bg_lu_solve_device",
     "bg_rhs_planewave", "bg_rhs_planewave_device", "bg_pft", "bg_kernel_launch_count",
     "bg_synchronize", "bg_stream", "bg_profile_begin", "bg_profile_read", "bg_profile_end",
-    "bg_zgemm_sub_device",
+    "bg_zgemm_sub_device", "bg_matrix_convert", "bg_lu_solve_refined", "bg_lu_solve_refined_device",
 ]
 
 
@@ -113,6 +113,9 @@ def lib():
         L.bg_stream.restype = VP
         L.bg_profile_read.argtypes = [I, VP, VP, VP]
         L.bg_zgemm_sub_device.argtypes = [I, I, I, VP, I, VP, I, VP, I]
+        L.bg_matrix_convert.argtypes = [P, P]
+        L.bg_lu_solve_refined.argtypes = [P, P, VP, I, D, I, VP]
+        L.bg_lu_solve_refined_device.argtypes = [P, P, VP, I, I, D, I, VP]
         _LIB = L
     return _LIB
 
@@ -184,6 +187,20 @@ class HMatrix:
         dt = np.complex128 if self.precision == BG_C128 else np.complex64
         a = np.asfortranarray(A, dtype=dt)
         _check(lib().bg_matrix_upload(self.h, _ptr(a)))
+
+    def convert_from(self, src):
+        """Fill this (complex64) matrix from a complex128 one."""
+        _check(lib().bg_matrix_convert(src.h, self.h))
+        return self
+
+    def LUSolveRefined(self, F, B, tol=1e-12, maxit=30):
+        """Solve with complex64 factors F of this complex128 matrix plus FP64
+        iterative refinement; returns (X, stats=(sweeps, final, first residual))."""
+        arr = np.asfortranarray(B, dtype=np.complex128)
+        nrhs = 1 if arr.ndim == 1 else arr.shape[1]
+        st = np.zeros(3)
+        _check(lib().bg_lu_solve_refined(self.h, F.h, _ptr(arr), nrhs, float(tol), int(maxit), _ptr(st)))
+        return arr, st
 
     def device_ptr(self):
         p = C.c_void_p()

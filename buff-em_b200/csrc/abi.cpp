@@ -214,7 +214,9 @@ int bg_matrix_create(bg_geometry *g, int precision, bg_matrix **out) {
   m->g = g;
   m->N = g->N;
   m->precision = precision;
-  m->ld = (size_t)g->N;
+  // complex64 storage feeds TMA: 16-byte aligned column starts need an even,
+  // here 32-aligned, leading dimension
+  m->ld = precision == BG_C128 ? (size_t)g->N : ((size_t)g->N + 31) / 32 * 32;
   size_t esz = precision == BG_C128 ? 16 : 8;
   cudaError_t e = cudaMalloc(&m->d, esz * m->ld * (size_t)m->N);
   if (e != cudaSuccess) {
@@ -230,7 +232,7 @@ int bg_matrix_create(bg_geometry *g, int precision, bg_matrix **out) {
 
 void bg_matrix_destroy(bg_matrix *m) {
   if (!m) return;
-  dfree(m->d); dfree(m->d_ipiv); dfree(m->d_work);
+  dfree(m->d); dfree(m->d_ipiv); dfree(m->d_work); dfree(m->d_perm);
   delete m;
 }
 
@@ -253,7 +255,7 @@ int bg_matrix_download(const bg_matrix *m, void *host) {
   if (!m || !host) { set_error("bg_matrix_download: bad arguments"); return BG_ERR_ARG; }
   size_t esz = m->precision == BG_C128 ? 16 : 8;
   BG_CUDA_TRY(cudaStreamSynchronize(stream()));
-  BG_CUDA_TRY(cudaMemcpy(host, m->d, esz * m->ld * (size_t)m->N, cudaMemcpyDeviceToHost));
+  BG_CUDA_TRY(cudaMemcpy2D(host, esz * m->N, m->d, esz * m->ld, esz * m->N, m->N, cudaMemcpyDeviceToHost));
   return BG_OK;
 }
 
@@ -261,9 +263,45 @@ int bg_matrix_upload(bg_matrix *m, const void *host) {
   if (!m || !host) { set_error("bg_matrix_upload: bad arguments"); return BG_ERR_ARG; }
   size_t esz = m->precision == BG_C128 ? 16 : 8;
   BG_CUDA_TRY(cudaStreamSynchronize(stream()));
-  BG_CUDA_TRY(cudaMemcpy(m->d, host, esz * m->ld * (size_t)m->N, cudaMemcpyHostToDevice));
+  BG_CUDA_TRY(cudaMemcpy2D(m->d, esz * m->ld, host, esz * m->N, esz * m->N, m->N, cudaMemcpyHostToDevice));
   m->factored = false;
   return BG_OK;
+}
+
+int bg_matrix_convert(const bg_matrix *src, bg_matrix *dst) {
+  if (!src || !dst) { set_error("bg_matrix_convert: null matrix"); return BG_ERR_ARG; }
+  return matrix_convert(src, dst);
+}
+
+int bg_lu_solve_refined_device(bg_matrix *A, bg_matrix *F, void *dB, int ldb, int nrhs, double tol, int maxit,
+                               double *stats) {
+  if (!A || !F || !dB || nrhs <= 0 || ldb < A->N || maxit < 1) { set_error("bg_lu_solve_refined: bad arguments"); return BG_ERR_ARG; }
+  if (A->precision != BG_C128 || F->precision != BG_C64 || A->N != F->N) {
+    set_error("bg_lu_solve_refined: needs a complex128 matrix and complex64 factors of the same size");
+    return BG_ERR_ARG;
+  }
+  if (!F->factored) { set_error("bg_lu_solve_refined: factors missing (call bg_lu_factor on the complex64 matrix)"); return BG_ERR_STATE; }
+  if (F->info > 0) { set_error("bg_lu_solve_refined: singular factors (info=%d)", F->info); return BG_ERR_NUMERIC; }
+  return solve_refined(A, F, dB, ldb, nrhs, tol, maxit, stats);
+}
+
+int bg_lu_solve_refined(bg_matrix *A, bg_matrix *F, double *B, int nrhs, double tol, int maxit, double *stats) {
+  if (!A || !B || nrhs <= 0) { set_error("bg_lu_solve_refined: bad arguments"); return BG_ERR_ARG; }
+  size_t bytes = 16 * (size_t)A->N * nrhs;
+  void *dB = nullptr;
+  BG_CUDA_TRY(cudaMallocAsync(&dB, bytes, stream()));
+  int st = BG_OK;
+  cudaError_t e = cudaMemcpyAsync(dB, B, bytes, cudaMemcpyHostToDevice, stream());
+  if (e != cudaSuccess) { set_error("H2D: %s", cudaGetErrorString(e)); st = BG_ERR_CUDA; }
+  if (!st) st = bg_lu_solve_refined_device(A, F, dB, A->N, nrhs, tol, maxit, stats);
+  if (!st) {
+    e = cudaMemcpyAsync(B, dB, bytes, cudaMemcpyDeviceToHost, stream());
+    if (e != cudaSuccess) { set_error("D2H: %s", cudaGetErrorString(e)); st = BG_ERR_CUDA; }
+  }
+  cudaFreeAsync(dB, stream());
+  cudaError_t e2 = cudaStreamSynchronize(stream());
+  if (!st && e2 != cudaSuccess) { set_error("refined solve: %s", cudaGetErrorString(e2)); st = BG_ERR_CUDA; }
+  return st;
 }
 
 int bg_matrix_device_ptr(bg_matrix *m, void **dptr, int *ld) {
@@ -275,7 +313,6 @@ int bg_matrix_device_ptr(bg_matrix *m, void **dptr, int *ld) {
 
 int bg_lu_factor(bg_matrix *m) {
   if (!m) { set_error("bg_lu_factor: null matrix"); return BG_ERR_ARG; }
-  if (m->precision != BG_C128) { set_error("bg_lu_factor: complex128 matrices only"); return BG_ERR_ARG; }
   int st = lu_factor(m);
   if (st < 0) return st;
   m->factored = true;
@@ -295,12 +332,32 @@ int bg_lu_solve_device(bg_matrix *m, void *dB, int ldb, int nrhs) {
   if (!m || !dB || nrhs <= 0 || ldb < m->N) { set_error("bg_lu_solve_device: bad arguments"); return BG_ERR_ARG; }
   if (!m->factored) { set_error("bg_lu_solve: matrix is not LU-factored"); return BG_ERR_STATE; }
   if (m->info > 0) { set_error("bg_lu_solve: factorization is singular (info=%d)", m->info); return BG_ERR_NUMERIC; }
-  return lu_solve(m, dB, ldb, nrhs);
+  int st = lu_solve(m, dB, ldb, nrhs);
+  if (!st) st = lu_solve_status(m);
+  return st;
 }
 
 int bg_lu_solve(bg_matrix *m, double *B, int nrhs) {
   if (!m || !B || nrhs <= 0) { set_error("bg_lu_solve: bad arguments"); return BG_ERR_ARG; }
   if (!m->factored) { set_error("bg_lu_solve: matrix is not LU-factored"); return BG_ERR_STATE; }
+  if (m->precision == BG_C64) {
+    std::vector<float> h(2 * (size_t)m->N * nrhs);
+    for (size_t i = 0; i < h.size(); i++) h[i] = (float)B[i];
+    void *d = nullptr;
+    BG_CUDA_TRY(cudaMalloc(&d, sizeof(float) * h.size()));
+    int st = BG_OK;
+    cudaError_t e = cudaMemcpy(d, h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) { set_error("H2D: %s", cudaGetErrorString(e)); st = BG_ERR_CUDA; }
+    if (!st) st = bg_lu_solve_device(m, d, m->N, nrhs);
+    if (!st) {
+      cudaError_t e2 = cudaStreamSynchronize(stream());
+      if (e2 == cudaSuccess) e2 = cudaMemcpy(h.data(), d, sizeof(float) * h.size(), cudaMemcpyDeviceToHost);
+      if (e2 != cudaSuccess) { set_error("solve: %s", cudaGetErrorString(e2)); st = BG_ERR_CUDA; }
+    }
+    cudaFree(d);
+    if (!st) for (size_t i = 0; i < h.size(); i++) B[i] = h[i];
+    return st;
+  }
   size_t bytes = 16 * (size_t)m->N * nrhs;
   void *dB = nullptr;
   BG_CUDA_TRY(cudaMallocAsync(&dB, bytes, stream()));

@@ -1,0 +1,286 @@
+// Complex-FP32 GEMM on the 5th-generation tensor cores (tcgen05, kind::tf32)
+// for the precision form of the LU: C <- C - A*B with A (M x K), B (K x N),
+// C (M x N) complex64, column-major, interleaved (re, im).
+//
+// Real embedding: with A~ the 2M x 2K real matrix of 2x2 blocks
+// [[ar, -ai], [ai, ar]], B~ = B's interleaved storage read as a real
+// 2K x N column-major matrix and C~ likewise for C, C~ -= A~ B~ is exactly the
+// complex update.  So B and C are used in place; only A is expanded once
+// into a K-major (row-major 2M x 2K) copy by k_expand_a.
+//
+// Kernel: one 128 x BN tile of C~ per CTA.  Warp 0 (one elected lane) issues
+// TMA loads (128B-swizzled, 32 fp32 of K per stage row) into a STAGES-deep
+// ring guarded by mbarriers; warp 1 (one lane) issues tcgen05.mma
+// (M=128, N=BN, K=8 per instruction) accumulating in TMEM and releases ring
+// slots with tcgen05.commit; after the last MMA all four warps read the
+// accumulator with tcgen05.ld (lane = row) and update C in place.
+// Every mbarrier wait is bounded; on timeout the kernel records an error
+// code, drains, frees its TMEM and returns.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+
+#include "internal.h"
+
+namespace bg {
+
+#define TC_BM 128            // rows of C~ per CTA (= 64 complex rows)
+#define TC_BN 128            // columns of C~ per CTA
+#define TC_BK 32             // fp32 of K per stage (one 128-byte swizzle row)
+#define TC_STAGES 6
+#define TC_THREADS 128
+#define TC_A_BYTES (TC_BM * TC_BK * 4)
+#define TC_B_BYTES (TC_BN * TC_BK * 4)
+#define TC_STAGE_BYTES (TC_A_BYTES + TC_B_BYTES)
+#define TC_SMEM (TC_STAGES * TC_STAGE_BYTES + 1024 + 256)
+#define TC_SPIN_LIMIT (1u << 26)
+
+struct TcArgs {
+  int M2, N, K2;         // C~ rows (2M), columns, reduction length (2K)
+  float *C;              // interleaved complex64 storage of C (column-major, ldc complex)
+  size_t ldc;            // in complex elements
+  int *err;              // device error flag
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes));
+}
+// bounded wait on phase parity; returns false on timeout
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t addr = smem_u32(bar);
+  for (uint32_t it = 0; it < TC_SPIN_LIMIT; it++) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(addr), "r"(parity));
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+      ::"r"(smem_u32(dst)), "l"((uint64_t)map), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// K-major, 128-byte swizzle shared-memory matrix descriptor (sm_100 UMMA):
+// start>>4 in [0,14), LBO (unused for swizzled K-major) = 1 in [16,30),
+// SBO = 1024 B (one 8-row swizzle atom) >> 4 in [32,46), version 1 in [46,48),
+// layout SWIZZLE_128B = 2 in [61,64).
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+// instruction descriptor, kind::tf32: D f32 (bits 4-5 = 1), A/B tf32 (2 at
+// bits 7-9 and 10-12), both K-major, N>>3 at 17-22, M>>4 at 24-28
+__host__ __device__ constexpr uint32_t tf32_idesc(int M, int N) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    k_cgemm_tf32(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, TcArgs P) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  // 1024-byte aligned ring (the 128B swizzle pattern repeats every 1024 bytes)
+  unsigned char *ring = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t *full = (uint64_t *)(ring + TC_STAGES * TC_STAGE_BYTES);
+  uint64_t *empty = full + TC_STAGES;
+  uint64_t *done = empty + TC_STAGES;
+  uint32_t *tmem_slot = (uint32_t *)(done + 1);
+  __shared__ int s_fail, s_issued, s_consumed;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.x * TC_BM, n0 = blockIdx.y * TC_BN;
+  const int nk = (P.K2 + TC_BK - 1) / TC_BK;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < TC_STAGES; s++) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+    mbar_init(done, 1);
+    s_fail = 0;
+    s_issued = 0;
+    s_consumed = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(TC_BN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // producer: TMA into the ring
+    for (int kb = 0; kb < nk; kb++) {
+      int s = kb % TC_STAGES;
+      if (kb >= TC_STAGES) {
+        if (!mbar_wait(&empty[s], ((kb / TC_STAGES) - 1) & 1)) { s_fail = 1; break; }
+      }
+      unsigned char *sa = ring + s * TC_STAGE_BYTES;
+      unsigned char *sb = sa + TC_A_BYTES;
+      mbar_expect_tx(&full[s], TC_STAGE_BYTES);
+      tma_load_2d(sa, &mapA, kb * TC_BK, m0, &full[s]);
+      tma_load_2d(sb, &mapB, kb * TC_BK, n0, &full[s]);
+      s_issued = kb + 1;
+    }
+  } else if (warp == 1 && lane == 0) {
+    // MMA issuer
+    const uint32_t idesc = tf32_idesc(TC_BM, TC_BN);
+    bool ok = true;
+    for (int kb = 0; kb < nk && ok; kb++) {
+      int s = kb % TC_STAGES;
+      if (!mbar_wait(&full[s], (kb / TC_STAGES) & 1)) { s_fail = 2; ok = false; break; }
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      uint32_t sa = smem_u32(ring + s * TC_STAGE_BYTES);
+      uint32_t sb = sa + TC_A_BYTES;
+#pragma unroll
+      for (int k = 0; k < TC_BK / 8; k++) {
+        uint64_t da = sw128_desc(sa + k * 32), db = sw128_desc(sb + k * 32);
+        uint32_t acc = (kb > 0 || k > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}"
+            ::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc));
+      }
+      // release the slot when these MMAs have read it
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+          smem_u32(&empty[s])));
+      s_consumed = kb + 1;
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(done)));
+  }
+  __syncwarp();
+  // epilogue: all warps wait for the accumulator
+  bool ok = mbar_wait(done, 0);
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  if (!ok) s_fail = 3;
+  __syncthreads();
+  if (!s_fail) {
+    const int row = m0 + warp * 32 + lane;   // row of C~ (2*complex row + component)
+    const size_t ldr = 2 * P.ldc;           // real leading dimension
+#pragma unroll 1
+    for (int c0 = 0; c0 < TC_BN; c0 += 32) {
+      uint32_t r[32];
+      uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+          "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+            "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+            "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+            "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;");
+      if (row < P.M2) {
+#pragma unroll
+        for (int j = 0; j < 32; j++) {
+          int col = n0 + c0 + j;
+          if (col < P.N) {
+            float *p = P.C + (size_t)col * ldr + row;
+            *p -= __uint_as_float(r[j]);
+          }
+        }
+      }
+    }
+  } else if (threadIdx.x == 0) {
+    atomicExch(P.err, s_fail);
+    // drain: wait (bounded) for TMA copies issued but never consumed
+    for (int c = s_consumed; c < s_issued; c++) mbar_wait(&full[c % TC_STAGES], (c / TC_STAGES) & 1);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_BN));
+}
+
+// A~ (row-major 2M x 2K, leading dimension lda2 floats) from complex A (M x K
+// column-major, lda complex): rows 2m, 2m+1 and columns 2k, 2k+1 hold
+// [[ar, -ai], [ai, ar]]
+__global__ void k_expand_a(int M, int K, const float2 *A, size_t lda, float *At, size_t lda2) {
+  int m = blockIdx.x * blockDim.x + threadIdx.x;
+  int k = blockIdx.y;
+  if (m >= M || k >= K) return;
+  float2 a = A[(size_t)k * lda + m];
+  float *r0 = At + (size_t)(2 * m) * lda2 + 2 * k;
+  float *r1 = r0 + lda2;
+  *(float2 *)r0 = make_float2(a.x, -a.y);
+  *(float2 *)r1 = make_float2(a.y, a.x);
+}
+
+// ------------------------------------------------------------------ host side
+typedef CUresult (*PFN_encodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                    const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                    CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static PFN_encodeTiled get_encode() {
+  static PFN_encodeTiled fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_encodeTiled)p;
+  }
+  return fn;
+}
+
+// 2D fp32 tensor map over a row-major (rows x cols) array with leading
+// dimension ld floats; box = 32 floats (128 B, swizzled) x box_rows
+static int make_map(CUtensorMap *map, const float *base, uint64_t cols, uint64_t rows, uint64_t ld, uint32_t box_rows) {
+  PFN_encodeTiled enc = get_encode();
+  if (!enc) { set_error("cuTensorMapEncodeTiled unavailable"); return BG_ERR_CUDA; }
+  if (((uintptr_t)base & 15) || ((ld * 4) & 15)) { set_error("TMA base/stride not 16-byte aligned"); return BG_ERR_ARG; }
+  cuuint64_t dims[2] = {cols, rows};
+  cuuint64_t strides[1] = {ld * 4};
+  cuuint32_t box[2] = {TC_BK, box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void *)base, dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) { set_error("cuTensorMapEncodeTiled failed (%d)", (int)r); return BG_ERR_CUDA; }
+  return BG_OK;
+}
+
+// C -= A*B, complex64 column-major interleaved; At is a device scratch of at
+// least 2M x round_up(2K, 32) floats; err a device int (0 on entry).
+int cgemm_sub_tf32(int M, int N, int K, const void *A, size_t lda, const void *B, size_t ldb, void *C, size_t ldc,
+                   float *At, int *err) {
+  if (M <= 0 || N <= 0 || K <= 0) return BG_OK;
+  static bool attr = false;
+  if (!attr) {
+    BG_CUDA_TRY(cudaFuncSetAttribute(k_cgemm_tf32, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
+    attr = true;
+  }
+  size_t lda2 = ((size_t)2 * K + 31) / 32 * 32;
+  dim3 eg((M + 127) / 128, K);
+  k_expand_a<<<eg, 128, 0, stream()>>>(M, K, (const float2 *)A, lda, At, lda2);
+  BG_LAUNCHED();
+  CUtensorMap mA, mB;
+  int st = make_map(&mA, At, (uint64_t)2 * K, (uint64_t)2 * M, lda2, TC_BM);
+  if (!st) st = make_map(&mB, (const float *)B, (uint64_t)2 * K, (uint64_t)N, 2 * ldb, TC_BN);
+  if (st) return st;
+  TcArgs P{2 * M, N, 2 * K, (float *)C, ldc, err};
+  dim3 grid((2 * M + TC_BM - 1) / TC_BM, (N + TC_BN - 1) / TC_BN);
+  prof_start(PROF_GEMM);
+  k_cgemm_tf32<<<grid, TC_THREADS, TC_SMEM, stream()>>>(mA, mB, P);
+  BG_LAUNCHED();
+  prof_stop(PROF_GEMM, 8.0 * M * (double)N * K);
+  return BG_OK;
+}
+
+}  // namespace bg

@@ -128,6 +128,8 @@ struct bg_matrix {
   int info = 0;
   void *d_work = nullptr;      // LU workspace
   size_t work_bytes = 0;
+  int *d_perm = nullptr;       // row permutation of the factors + solve flags/tickets
+  int solve_epoch = 0;
 };
 
 namespace bg {
@@ -143,6 +145,9 @@ int pft(bg_geometry *g, double wr, double wi, const void *dJ, const double *E0, 
         double *out);
 int lu_factor(bg_matrix *m);
 int lu_solve(bg_matrix *m, void *dB, int ldb, int nrhs);
+int lu_solve_status(bg_matrix *m);
 int zgemm_sub_device(int M, int N, int K, const void *A, int lda, const void *B, int ldb, void *C, int ldc);
+int matrix_convert(const bg_matrix *src, bg_matrix *dst);
+int solve_refined(bg_matrix *A, bg_matrix *F, void *dB, int ldb, int nrhs, double tol, int maxit, double *stats);
 void gauss_legendre01(int n, double *x, double *w);
 }  // namespace bg

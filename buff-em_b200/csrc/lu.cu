@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
+#include <vector>
 
 #include "internal.h"
 
@@ -26,6 +27,14 @@ namespace cg = cooperative_groups;
 namespace bg {
 
 struct cdl { double r, i; };
+struct cfl { float r, i; };
+template <class C> struct CxT;
+template <> struct CxT<cdl> { typedef double R; };
+template <> struct CxT<cfl> { typedef float R; };
+
+// tensor-core complex-FP32 GEMM (gemm_tc.cu)
+int cgemm_sub_tf32(int M, int N, int K, const void *A, size_t lda, const void *B, size_t ldb, void *C, size_t ldc,
+                   float *At, int *err);
 
 // =========================================================================
 // complex GEMM  C(MxN) -= A(MxK) * B(KxN), column-major, complex128, on the
@@ -206,14 +215,16 @@ static int zgemm_sub(int M, int N, int K, const cdl *A, size_t lda, const cdl *B
 #define TRS_WARPS 8
 #define TRS_CPW 8                         // columns per warp per CTA
 #define TRS_COLS (TRS_WARPS * TRS_CPW)
-#define TRS_SMEM (64 * 65 * 16)
-__device__ __forceinline__ cdl cshfl(cdl v, int src) {
-  return cdl{__shfl_sync(0xffffffffu, v.r, src), __shfl_sync(0xffffffffu, v.i, src)};
+template <class C>
+__device__ __forceinline__ C cshfl(C v, int src) {
+  return C{__shfl_sync(0xffffffffu, v.r, src), __shfl_sync(0xffffffffu, v.i, src)};
 }
-__global__ void __launch_bounds__(TRS_WARPS * 32) k_trsm_leaf(int n, int m, const cdl *T, size_t ldt, cdl *B,
+template <class C>
+__global__ void __launch_bounds__(TRS_WARPS * 32) k_trsm_leaf(int n, int m, const C *T, size_t ldt, C *B,
                                                               size_t ldb, int upper) {
+  typedef typename CxT<C>::R R;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  cdl(*Ts)[65] = (cdl(*)[65])smem_raw;   // Ts[r][c]
+  C(*Ts)[65] = (C(*)[65])smem_raw;   // Ts[r][c]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int e = tid; e < n * n; e += TRS_WARPS * 32) {
     int r = e % n, c = e / n;
@@ -224,25 +235,25 @@ __global__ void __launch_bounds__(TRS_WARPS * 32) k_trsm_leaf(int n, int m, cons
   for (int j = 0; j < TRS_CPW; j++) {
     const int col = blockIdx.x * TRS_COLS + warp * TRS_CPW + j;
     if (col >= m) break;
-    cdl *bc = B + (size_t)col * ldb;
-    cdl b0 = r0 < n ? bc[r0] : cdl{0, 0};
-    cdl b1 = r1 < n ? bc[r1] : cdl{0, 0};
+    C *bc = B + (size_t)col * ldb;
+    C b0 = r0 < n ? bc[r0] : C{0, 0};
+    C b1 = r1 < n ? bc[r1] : C{0, 0};
     if (!upper) {
       for (int i = 0; i < n; i++) {
-        cdl x = cshfl(i < 32 ? b0 : b1, i & 31);
-        if (r0 > i && r0 < n) { cdl l = Ts[r0][i]; b0.r -= l.r * x.r - l.i * x.i; b0.i -= l.r * x.i + l.i * x.r; }
-        if (r1 > i && r1 < n) { cdl l = Ts[r1][i]; b1.r -= l.r * x.r - l.i * x.i; b1.i -= l.r * x.i + l.i * x.r; }
+        C x = cshfl(i < 32 ? b0 : b1, i & 31);
+        if (r0 > i && r0 < n) { C l = Ts[r0][i]; b0.r -= l.r * x.r - l.i * x.i; b0.i -= l.r * x.i + l.i * x.r; }
+        if (r1 > i && r1 < n) { C l = Ts[r1][i]; b1.r -= l.r * x.r - l.i * x.i; b1.i -= l.r * x.i + l.i * x.r; }
       }
     } else {
       for (int i = n - 1; i >= 0; i--) {
-        cdl v = cshfl(i < 32 ? b0 : b1, i & 31);
-        cdl u = Ts[i][i];
-        double d = u.r * u.r + u.i * u.i;
-        cdl x{(v.r * u.r + v.i * u.i) / d, (v.i * u.r - v.r * u.i) / d};
+        C v = cshfl(i < 32 ? b0 : b1, i & 31);
+        C u = Ts[i][i];
+        R d = u.r * u.r + u.i * u.i;
+        C x{(v.r * u.r + v.i * u.i) / d, (v.i * u.r - v.r * u.i) / d};
         if (r0 == i) b0 = x;
         if (r1 == i) b1 = x;
-        if (r0 < i) { cdl t = Ts[r0][i]; b0.r -= t.r * x.r - t.i * x.i; b0.i -= t.r * x.i + t.i * x.r; }
-        if (r1 < i) { cdl t = Ts[r1][i]; b1.r -= t.r * x.r - t.i * x.i; b1.i -= t.r * x.i + t.i * x.r; }
+        if (r0 < i) { C t = Ts[r0][i]; b0.r -= t.r * x.r - t.i * x.i; b0.i -= t.r * x.i + t.i * x.r; }
+        if (r1 < i) { C t = Ts[r1][i]; b1.r -= t.r * x.r - t.i * x.i; b1.i -= t.r * x.i + t.i * x.r; }
       }
     }
     if (r0 < n) bc[r0] = b0;
@@ -250,18 +261,77 @@ __global__ void __launch_bounds__(TRS_WARPS * 32) k_trsm_leaf(int n, int m, cons
   }
 }
 
+// small-N complex64 GEMM (C -= A B, N <= 16): one thread per row, used where
+// a tensor-core tile would be mostly padding (few right-hand sides)
+__global__ void k_cgemm_small(int M, int N, int K, const cfl *A, size_t lda, const cfl *B, size_t ldb, cfl *Cm,
+                              size_t ldc) {
+  int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= M) return;
+  float ar[16], ai[16];
+  for (int n = 0; n < N; n++) ar[n] = ai[n] = 0.f;
+  for (int k = 0; k < K; k++) {
+    cfl a = A[(size_t)k * lda + m];
+#pragma unroll 4
+    for (int n = 0; n < N; n++) {
+      cfl b = B[(size_t)n * ldb + k];
+      ar[n] += a.r * b.r - a.i * b.i;
+      ai[n] += a.r * b.i + a.i * b.r;
+    }
+  }
+  for (int n = 0; n < N; n++) {
+    cfl *p = Cm + (size_t)n * ldc + m;
+    p->r -= ar[n];
+    p->i -= ai[n];
+  }
+}
+
+// per-matrix scratch for the tensor-core path
+struct TcScratch {
+  float *At = nullptr;
+  size_t at_floats = 0;
+  int *err = nullptr;
+};
+static thread_local TcScratch *t_tc = nullptr;
+#define TC_MCHUNK 8192
+
+static int gemm_sub(int M, int N, int K, const cdl *A, size_t lda, const cdl *B, size_t ldb, cdl *C, size_t ldc) {
+  return zgemm_sub(M, N, K, A, lda, B, ldb, C, ldc);
+}
+static int gemm_sub(int M, int N, int K, const cfl *A, size_t lda, const cfl *B, size_t ldb, cfl *C, size_t ldc) {
+  if (M <= 0 || N <= 0 || K <= 0) return BG_OK;
+  if (N <= 16 || !t_tc) {
+    if (N > 16) { set_error("complex64 GEMM needs the tensor-core scratch"); return BG_ERR_STATE; }
+    k_cgemm_small<<<(M + 127) / 128, 128, 0, stream()>>>(M, N, K, A, lda, B, ldb, C, ldc);
+    BG_LAUNCHED();
+    return BG_OK;
+  }
+  size_t lda2 = ((size_t)2 * K + 31) / 32 * 32;
+  size_t cap = std::min<size_t>(t_tc->at_floats / (2 * lda2), TC_MCHUNK);
+  int mch = (int)std::min<size_t>((size_t)M, cap);
+  if (mch < M) mch = mch / 64 * 64;   // chunked: whole 64-row tiles per chunk
+  if (mch <= 0) { set_error("tensor-core scratch too small"); return BG_ERR_STATE; }
+  for (int m0 = 0; m0 < M; m0 += mch) {
+    int mm = std::min(mch, M - m0);
+    int st = cgemm_sub_tf32(mm, N, K, A + m0, lda, B, ldb, C + m0, ldc, t_tc->At, t_tc->err);
+    if (st) return st;
+  }
+  return BG_OK;
+}
+
 // X = L^{-1} B (unit lower, upper=0) or U^{-1} B (upper=1), L/U n x n at T
-static int trsm(int n, int m, const cdl *T, size_t ldt, cdl *B, size_t ldb, int upper) {
+template <class C>
+static int trsm(int n, int m, const C *T, size_t ldt, C *B, size_t ldb, int upper) {
   if (n <= 0 || m <= 0) return BG_OK;
   if (n <= 64) {
+    const int smem = 64 * 65 * (int)sizeof(C);
     static bool attr = false;
     if (!attr) {
-      BG_CUDA_TRY(cudaFuncSetAttribute(k_trsm_leaf, cudaFuncAttributeMaxDynamicSharedMemorySize, TRS_SMEM));
+      BG_CUDA_TRY(cudaFuncSetAttribute(k_trsm_leaf<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
       attr = true;
     }
     int blocks = (m + TRS_COLS - 1) / TRS_COLS;
     prof_start(PROF_TRSM);
-    k_trsm_leaf<<<blocks, TRS_WARPS * 32, TRS_SMEM, stream()>>>(n, m, T, ldt, B, ldb, upper);
+    k_trsm_leaf<C><<<blocks, TRS_WARPS * 32, smem, stream()>>>(n, m, T, ldt, B, ldb, upper);
     BG_LAUNCHED();
     prof_stop(PROF_TRSM, 4.0 * n * (double)n * m);
     return BG_OK;
@@ -272,19 +342,20 @@ static int trsm(int n, int m, const cdl *T, size_t ldt, cdl *B, size_t ldb, int 
   int st;
   if (!upper) {
     if ((st = trsm(n1, m, T, ldt, B, ldb, 0))) return st;
-    if ((st = zgemm_sub(n2, m, n1, T + n1, ldt, B, ldb, B + n1, ldb))) return st;
+    if ((st = gemm_sub(n2, m, n1, T + n1, ldt, B, ldb, B + n1, ldb))) return st;
     return trsm(n2, m, T + n1 + (size_t)n1 * ldt, ldt, B + n1, ldb, 0);
   }
   if ((st = trsm(n2, m, T + n1 + (size_t)n1 * ldt, ldt, B + n1, ldb, 1))) return st;
-  if ((st = zgemm_sub(n1, m, n2, T + (size_t)n1 * ldt, ldt, B + n1, ldb, B, ldb))) return st;
+  if ((st = gemm_sub(n1, m, n2, T + (size_t)n1 * ldt, ldt, B + n1, ldb, B, ldb))) return st;
   return trsm(n1, m, T, ldt, B, ldb, 1);
 }
 
 // =========================================================================
 // cooperative panel factorisation of A[k0:Nr, k0:k0+w] (w <= 32)
 // =========================================================================
+template <class C>
 struct PanelArgs {
-  cdl *A;
+  C *A;
   size_t ld;
   int Nr;          // number of rows of the full matrix
   int k0, w;
@@ -293,22 +364,24 @@ struct PanelArgs {
   int *info;       // device int (0 = ok)
   double *cval;    // [2][grid] candidate |re|+|im|
   int *cidx;       // [2][grid] candidate row
-  cdl *crow;       // [2][grid][32] candidate row values
-  cdl *jrow;       // [2][32] values of row k0+j before the swap
+  C *crow;         // [2][grid][32] candidate row values
+  C *jrow;         // [2][32] values of row k0+j before the swap
 };
 
 __device__ __forceinline__ bool better(double v, int i, double bv, int bi) {
   return v > bv || (v == bv && i < bi);
 }
 
-__global__ void __launch_bounds__(256) k_panel(PanelArgs P) {
+template <class C>
+__global__ void __launch_bounds__(256) k_panel(PanelArgs<C> P) {
+  typedef typename CxT<C>::R R;
   cg::grid_group grid = cg::this_grid();
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  cdl *S = (cdl *)smem_raw;                 // [rows_per][w]
+  C *S = (C *)smem_raw;                     // [rows_per][w]
   __shared__ double rv[8];
   __shared__ int ri[8];
   __shared__ int s_piv;
-  __shared__ cdl prow[32];
+  __shared__ C prow[32];
   const int w = P.w, G = gridDim.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int r0 = P.k0 + blockIdx.x * P.rows_per;
   const int r1 = min(P.Nr, r0 + P.rows_per);
@@ -320,14 +393,14 @@ __global__ void __launch_bounds__(256) k_panel(PanelArgs P) {
   __syncthreads();
   for (int j = 0; j < w; j++) {
     const int gj = P.k0 + j, buf = j & 1;
-    // 1. local pivot candidate (izamax: max |re|+|im|, first index on ties)
+    // 1. local pivot candidate (i[cz]amax: max |re|+|im|, first index on ties)
     double bv = -1.0;
     int bi = 0x7fffffff;
     for (int r = tid; r < nr; r += 256) {
       int gr = r0 + r;
       if (gr < gj) continue;
-      cdl v = S[r * w + j];
-      double a = fabs(v.r) + fabs(v.i);
+      C v = S[r * w + j];
+      double a = (double)(fabs(v.r) + fabs(v.i));
       if (better(a, gr, bv, bi)) { bv = a; bi = gr; }
     }
     for (int o = 16; o > 0; o >>= 1) {
@@ -376,22 +449,22 @@ __global__ void __launch_bounds__(256) k_panel(PanelArgs P) {
     }
     __syncthreads();
     // 4. scale the column below the pivot and update the rest of the panel
-    cdl p = prow[j];
-    double d = p.r * p.r + p.i * p.i;
-    if (d == 0.0) {
+    C p = prow[j];
+    R d = p.r * p.r + p.i * p.i;
+    if (d == (R)0) {
       if (blockIdx.x == 0 && tid == 0) atomicCAS(P.info, 0, gj + 1);
     } else {
-      cdl inv{p.r / d, -p.i / d};
+      C inv{p.r / d, -p.i / d};
       int ncol = w - j - 1;
       for (int r = tid; r < nr; r += 256) {
         int gr = r0 + r;
         if (gr <= gj) continue;
-        cdl v = S[r * w + j];
-        cdl l{v.r * inv.r - v.i * inv.i, v.r * inv.i + v.i * inv.r};
+        C v = S[r * w + j];
+        C l{v.r * inv.r - v.i * inv.i, v.r * inv.i + v.i * inv.r};
         S[r * w + j] = l;
         for (int c = 1; c <= ncol; c++) {
-          cdl u = prow[j + c];
-          cdl &t = S[r * w + j + c];
+          C u = prow[j + c];
+          C &t = S[r * w + j + c];
           t.r -= l.r * u.r - l.i * u.i;
           t.i -= l.r * u.i + l.i * u.r;
         }
@@ -406,14 +479,15 @@ __global__ void __launch_bounds__(256) k_panel(PanelArgs P) {
 }
 
 // apply the interchanges ipiv[k0..k0+w) to columns [c0, c1) of A
-__global__ void k_laswp(cdl *A, size_t ld, const int *ipiv, int k0, int w, int c0, int c1, int skip0, int skip1) {
+template <class C>
+__global__ void k_laswp(C *A, size_t ld, const int *ipiv, int k0, int w, int c0, int c1, int skip0, int skip1) {
   int col = c0 + blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= c1 || (col >= skip0 && col < skip1)) return;
-  cdl *cp = A + (size_t)col * ld;
+  C *cp = A + (size_t)col * ld;
   for (int i = 0; i < w; i++) {
     int p = ipiv[k0 + i] - 1;
     if (p != k0 + i) {
-      cdl t = cp[k0 + i];
+      C t = cp[k0 + i];
       cp[k0 + i] = cp[p];
       cp[p] = t;
     }
@@ -423,80 +497,91 @@ __global__ void k_laswp(cdl *A, size_t ld, const int *ipiv, int k0, int w, int c
 struct LUWork {
   double *cval;
   int *cidx;
-  cdl *crow, *jrow;
+  void *crow, *jrow;
   int *info;
 };
 
-static int panel_grid = 0, panel_smem_max = 0, panel_rows_target = 256;
+static int panel_grid = 0, panel_smem_max = 0, panel_rows_target = 32;
 
+template <class C>
 static int panel_leaf(bg_matrix *m, const LUWork &W, int k0, int w) {
   int N = m->N;
   int Mp = N - k0;
-  // fewer CTAs make the per-column grid barrier and the candidate reduction
-  // cheaper; the slice of each CTA must still fit in shared memory
-  int G = std::min(panel_grid, std::max(8, (Mp + panel_rows_target - 1) / panel_rows_target));
-  G = std::min(G, std::max(1, (Mp + 31) / 32));
-  while (G < panel_grid && (size_t)((Mp + G - 1) / G) * w * sizeof(cdl) > (size_t)panel_smem_max) G++;
+  int G = std::min(panel_grid, std::max(1, (Mp + panel_rows_target - 1) / panel_rows_target));
+  while (G < panel_grid && (size_t)((Mp + G - 1) / G) * w * sizeof(C) > (size_t)panel_smem_max) G++;
   int rows = (Mp + G - 1) / G;
-  size_t smem = (size_t)rows * w * sizeof(cdl);
+  size_t smem = (size_t)rows * w * sizeof(C);
   if ((int)smem > panel_smem_max) {
     set_error("panel slice of %zu bytes exceeds shared memory (N=%d too large for this build)", smem, N);
     return BG_ERR_ARG;
   }
-  PanelArgs P{(cdl *)m->d, m->ld, N, k0, w, rows, m->d_ipiv, W.info, W.cval, W.cidx, W.crow, W.jrow};
+  static bool attr = false;
+  if (!attr) {
+    BG_CUDA_TRY(cudaFuncSetAttribute(k_panel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, panel_smem_max));
+    attr = true;
+  }
+  PanelArgs<C> P{(C *)m->d, m->ld, N, k0, w, rows, m->d_ipiv, W.info, W.cval, W.cidx, (C *)W.crow, (C *)W.jrow};
   void *args[] = {&P};
   prof_start(PROF_PANEL);
-  BG_CUDA_TRY(cudaLaunchCooperativeKernel((void *)k_panel, dim3(G), dim3(256), args, smem, stream()));
+  BG_CUDA_TRY(cudaLaunchCooperativeKernel((void *)k_panel<C>, dim3(G), dim3(256), args, smem, stream()));
   BG_LAUNCHED();
   prof_stop(PROF_PANEL, 8.0 * Mp * (double)w * w / 2);
   int threads = 256;
   int blocks = (N + threads - 1) / threads;
   prof_start(PROF_LASWP);
-  k_laswp<<<blocks, threads, 0, stream()>>>((cdl *)m->d, m->ld, m->d_ipiv, k0, w, 0, N, k0, k0 + w);
+  k_laswp<C><<<blocks, threads, 0, stream()>>>((C *)m->d, m->ld, m->d_ipiv, k0, w, 0, N, k0, k0 + w);
   BG_LAUNCHED();
   prof_stop(PROF_LASWP, 0.0);
   return BG_OK;
 }
 
 // factor columns [k0, k0+n) (rows k0..N-1); interchanges applied to all columns
+template <class C>
 static int getrf_rec(bg_matrix *m, const LUWork &W, int k0, int n) {
-  if (n <= 32) return panel_leaf(m, W, k0, n);
+  if (n <= 32) return panel_leaf<C>(m, W, k0, n);
   int n1 = (n / 2 + 31) / 32 * 32;
   if (n1 >= n) n1 = 32;
   int n2 = n - n1;
   int st;
-  cdl *A = (cdl *)m->d;
+  C *A = (C *)m->d;
   size_t ld = m->ld;
   int N = m->N;
-  if ((st = getrf_rec(m, W, k0, n1))) return st;
-  cdl *A11 = A + k0 + (size_t)k0 * ld;
-  cdl *A12 = A + k0 + (size_t)(k0 + n1) * ld;
-  cdl *A21 = A + (k0 + n1) + (size_t)k0 * ld;
-  cdl *A22 = A + (k0 + n1) + (size_t)(k0 + n1) * ld;
-  if ((st = trsm(n1, n2, A11, ld, A12, ld, 0))) return st;
-  if ((st = zgemm_sub(N - k0 - n1, n2, n1, A21, ld, A12, ld, A22, ld))) return st;
-  return getrf_rec(m, W, k0 + n1, n2);
+  if ((st = getrf_rec<C>(m, W, k0, n1))) return st;
+  C *A11 = A + k0 + (size_t)k0 * ld;
+  C *A12 = A + k0 + (size_t)(k0 + n1) * ld;
+  C *A21 = A + (k0 + n1) + (size_t)k0 * ld;
+  C *A22 = A + (k0 + n1) + (size_t)(k0 + n1) * ld;
+  if ((st = trsm<C>(n1, n2, A11, ld, A12, ld, 0))) return st;
+  if ((st = gemm_sub(N - k0 - n1, n2, n1, A21, ld, A12, ld, A22, ld))) return st;
+  return getrf_rec<C>(m, W, k0 + n1, n2);
+}
+
+static int build_perm(bg_matrix *m);
+
+static int panel_init() {
+  if (panel_grid) return BG_OK;
+  int dev = 0, sms = 0, smemopt = 0;
+  BG_CUDA_TRY(cudaGetDevice(&dev));
+  BG_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  BG_CUDA_TRY(cudaDeviceGetAttribute(&smemopt, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  panel_smem_max = smemopt - 2048;
+  panel_grid = sms;  // at most one CTA per SM (cooperative residency)
+  if (const char *e = std::getenv("BG_PANEL_ROWS")) panel_rows_target = std::max(8, std::atoi(e));
+  return BG_OK;
 }
 
 int lu_factor(bg_matrix *m) {
   int st = ensure_device();
+  if (!st) st = panel_init();
   if (st) return st;
   int N = m->N;
-  if (!panel_grid) {
-    int dev = 0, sms = 0, smemopt = 0;
-    BG_CUDA_TRY(cudaGetDevice(&dev));
-    BG_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    BG_CUDA_TRY(cudaDeviceGetAttribute(&smemopt, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    panel_smem_max = smemopt - 2048;
-    BG_CUDA_TRY(cudaFuncSetAttribute(k_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, panel_smem_max));
-    int per_sm = 0;
-    BG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_panel, 256, panel_smem_max));
-    if (per_sm < 1) { set_error("panel kernel cannot be resident"); return BG_ERR_CUDA; }
-    panel_grid = sms;  // at most one CTA per SM (cooperative residency)
-    if (const char *e = std::getenv("BG_PANEL_ROWS")) panel_rows_target = std::max(32, std::atoi(e));
-  }
-  size_t need = sizeof(double) * 2 * panel_grid + sizeof(int) * 2 * panel_grid + sizeof(cdl) * 2 * panel_grid * 32 +
-                sizeof(cdl) * 64 + 64;
+  const size_t csz = m->precision == BG_C128 ? sizeof(cdl) : sizeof(cfl);
+  // workspace: candidate rows, j-rows, candidate values/indices, info, error
+  // flag, and (complex64) the expanded-A scratch of the tensor-core GEMM
+  size_t at_floats = 0;
+  if (m->precision == BG_C64) at_floats = (size_t)2 * TC_MCHUNK * (((size_t)2 * N + 31) / 32 * 32);
+  size_t need = csz * 2 * panel_grid * 32 + csz * 64 + sizeof(double) * 2 * panel_grid + sizeof(int) * 2 * panel_grid +
+                256 + sizeof(float) * at_floats;
   if (m->work_bytes < need) {
     if (m->d_work) cudaFree(m->d_work);
     m->d_work = nullptr;
@@ -506,17 +591,35 @@ int lu_factor(bg_matrix *m) {
   }
   char *w = (char *)m->d_work;
   LUWork W;
-  W.crow = (cdl *)w; w += sizeof(cdl) * 2 * panel_grid * 32;
-  W.jrow = (cdl *)w; w += sizeof(cdl) * 64;
+  W.crow = (void *)w; w += csz * 2 * panel_grid * 32;
+  W.jrow = (void *)w; w += csz * 64;
   W.cval = (double *)w; w += sizeof(double) * 2 * panel_grid;
   W.cidx = (int *)w; w += sizeof(int) * 2 * panel_grid;
   W.info = (int *)w;
-  BG_CUDA_TRY(cudaMemsetAsync(W.info, 0, sizeof(int), stream()));
-  if ((st = getrf_rec(m, W, 0, N))) return st;
-  int info = 0;
-  BG_CUDA_TRY(cudaMemcpyAsync(&info, W.info, sizeof(int), cudaMemcpyDeviceToHost, stream()));
+  int *tcerr = W.info + 1;
+  w += 256;
+  BG_CUDA_TRY(cudaMemsetAsync(W.info, 0, 2 * sizeof(int), stream()));
+  if (m->precision == BG_C128) {
+    if ((st = getrf_rec<cdl>(m, W, 0, N))) return st;
+  } else {
+    TcScratch sc;
+    sc.At = (float *)w;
+    sc.at_floats = at_floats;
+    sc.err = tcerr;
+    t_tc = &sc;
+    st = getrf_rec<cfl>(m, W, 0, N);
+    t_tc = nullptr;
+    if (st) return st;
+  }
+  int info[2] = {0, 0};
+  BG_CUDA_TRY(cudaMemcpyAsync(info, W.info, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream()));
   BG_CUDA_TRY(cudaStreamSynchronize(stream()));
-  return info;
+  if (info[1]) {
+    set_error("tensor-core GEMM reported a pipeline timeout (code %d)", info[1]);
+    return BG_ERR_CUDA;
+  }
+  if ((st = build_perm(m))) return st;
+  return info[0];
 }
 
 int zgemm_sub_device(int M, int N, int K, const void *A, int lda, const void *B, int ldb, void *C, int ldc) {
@@ -525,19 +628,199 @@ int zgemm_sub_device(int M, int N, int K, const void *A, int lda, const void *B,
   return zgemm_sub(M, N, K, (const cdl *)A, (size_t)lda, (const cdl *)B, (size_t)ldb, (cdl *)C, (size_t)ldc);
 }
 
-// zgetrs: B <- U^{-1} L^{-1} P B
-int lu_solve(bg_matrix *m, void *dB, int ldb, int nrhs) {
-  int N = m->N;
-  cdl *B = (cdl *)dB;
-  const cdl *A = (const cdl *)m->d;
-  for (int k0 = 0; k0 < N; k0 += 32) {
-    int w = std::min(32, N - k0);
-    k_laswp<<<(nrhs + 31) / 32, 32, 0, stream()>>>(B, (size_t)ldb, m->d_ipiv, k0, w, 0, nrhs, 0, 0);
-    BG_LAUNCHED();
+// =========================================================================
+// few-right-hand-side solves: B <- U^{-1} L^{-1} P B in one gather and two
+// single-pass triangular sweeps.  In a sweep each CTA takes the next 64-row
+// block in dependency order from a ticket counter, accumulates the products
+// with already-solved blocks as their ready flags appear (flag == epoch),
+// solves its diagonal block with warp shuffles (one warp per right-hand
+// side), publishes the block and raises its flag.  A CTA only ever waits on
+// blocks with smaller tickets, which are already running, so the sweep
+// always makes progress; every wait is bounded and a timeout is recorded in
+// the error word, which also makes the other CTAs give up early.
+// =========================================================================
+#define TV_B 64
+#define TV_MAXRHS 4
+#define TV_SPIN (1 << 22)
+
+template <class C>
+__global__ void k_gather_rows(int N, int nrhs, const int *perm, const C *src, size_t lds, C *dst, size_t ldd) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y;
+  if (i < N && j < nrhs) dst[(size_t)j * ldd + i] = src[(size_t)j * lds + perm[i]];
+}
+
+template <class C>
+__device__ __forceinline__ C ldcg_c(const C *p);
+template <>
+__device__ __forceinline__ cdl ldcg_c<cdl>(const cdl *p) {
+  double2 v = __ldcg((const double2 *)p);
+  return cdl{v.x, v.y};
+}
+template <>
+__device__ __forceinline__ cfl ldcg_c<cfl>(const cfl *p) {
+  float2 v = __ldcg((const float2 *)p);
+  return cfl{v.x, v.y};
+}
+
+template <class C, bool UPPER>
+__global__ void __launch_bounds__(128) k_trsv(int N, const C *A, size_t ld, C *X, size_t ldx, int nrhs, int *flags,
+                                              int epoch, int *ticket, int *err) {
+  typedef typename CxT<C>::R R;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C(*D)[TV_B + 1] = (C(*)[TV_B + 1])smem_raw;                    // diagonal block
+  C(*part)[TV_MAXRHS] = (C(*)[TV_MAXRHS])(smem_raw + TV_B * (TV_B + 1) * sizeof(C));   // part[row][rhs]
+  __shared__ int s_blk, s_abort;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nb = (N + TV_B - 1) / TV_B;
+  if (tid == 0) { s_blk = atomicAdd(ticket, 1); s_abort = 0; }
+  __syncthreads();
+  const int lb = s_blk;
+  const int bi = UPPER ? nb - 1 - lb : lb;
+  const int r0 = bi * TV_B, rows = min(TV_B, N - r0);
+  // stage the diagonal block
+  for (int e = tid; e < rows * rows; e += 128) {
+    int r = e % rows, c = e / rows;
+    D[r][c] = A[(size_t)(r0 + c) * ld + r0 + r];
   }
-  int st = trsm(N, nrhs, A, m->ld, B, (size_t)ldb, 0);
-  if (!st) st = trsm(N, nrhs, A, m->ld, B, (size_t)ldb, 1);
-  return st;
+  const int row = tid & (TV_B - 1), half = tid >> 6;
+  C acc[TV_MAXRHS];
+#pragma unroll
+  for (int j = 0; j < TV_MAXRHS; j++) acc[j] = C{0, 0};
+  for (int q = 0; q < lb; q++) {
+    const int bj = UPPER ? nb - 1 - q : q;
+    if (tid == 0) {
+      volatile int *f = flags + bj;
+      int it = 0;
+      while (*f != epoch) {
+        if (*(volatile int *)err || ++it > TV_SPIN) {
+          if (it > TV_SPIN) atomicCAS(err, 0, 100 + (UPPER ? 1 : 0));
+          s_abort = 1;
+          break;
+        }
+        __nanosleep(64);
+      }
+      __threadfence();
+    }
+    __syncthreads();
+    if (s_abort) return;
+    const int c0 = bj * TV_B, cols = min(TV_B, N - c0);
+    if (row < rows) {
+      const C *ap = A + (size_t)c0 * ld + r0 + row;
+      for (int c = half * 32; c < min(cols, half * 32 + 32); c++) {
+        C a = ap[(size_t)c * ld];
+        for (int j = 0; j < nrhs; j++) {
+          C x = ldcg_c(X + (size_t)j * ldx + c0 + c);
+          acc[j].r += a.r * x.r - a.i * x.i;
+          acc[j].i += a.r * x.i + a.i * x.r;
+        }
+      }
+    }
+  }
+  if (half == 1 && row < rows)
+    for (int j = 0; j < nrhs; j++) part[row][j] = acc[j];
+  __syncthreads();
+  if (half == 0 && row < rows)
+    for (int j = 0; j < nrhs; j++) {
+      C b = X[(size_t)j * ldx + r0 + row];
+      C p = part[row][j];
+      part[row][j] = C{b.r - acc[j].r - p.r, b.i - acc[j].i - p.i};
+    }
+  __syncthreads();
+  // diagonal solve: warp j handles right-hand side j, lanes hold rows l, l+32
+  if (warp < nrhs) {
+    const int j = warp, q0 = lane, q1 = lane + 32;
+    C b0 = q0 < rows ? part[q0][j] : C{0, 0};
+    C b1 = q1 < rows ? part[q1][j] : C{0, 0};
+    if (!UPPER) {
+      for (int i = 0; i < rows; i++) {
+        C x = cshfl(i < 32 ? b0 : b1, i & 31);
+        if (q0 > i && q0 < rows) { C l = D[q0][i]; b0.r -= l.r * x.r - l.i * x.i; b0.i -= l.r * x.i + l.i * x.r; }
+        if (q1 > i && q1 < rows) { C l = D[q1][i]; b1.r -= l.r * x.r - l.i * x.i; b1.i -= l.r * x.i + l.i * x.r; }
+      }
+    } else {
+      for (int i = rows - 1; i >= 0; i--) {
+        C v = cshfl(i < 32 ? b0 : b1, i & 31);
+        C u = D[i][i];
+        R d = u.r * u.r + u.i * u.i;
+        C x{(v.r * u.r + v.i * u.i) / d, (v.i * u.r - v.r * u.i) / d};
+        if (q0 == i) b0 = x;
+        if (q1 == i) b1 = x;
+        if (q0 < i) { C t = D[q0][i]; b0.r -= t.r * x.r - t.i * x.i; b0.i -= t.r * x.i + t.i * x.r; }
+        if (q1 < i) { C t = D[q1][i]; b1.r -= t.r * x.r - t.i * x.i; b1.i -= t.r * x.i + t.i * x.r; }
+      }
+    }
+    if (q0 < rows) X[(size_t)j * ldx + r0 + q0] = b0;
+    if (q1 < rows) X[(size_t)j * ldx + r0 + q1] = b1;
+  }
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) atomicExch(flags + bi, epoch);
+}
+
+// host: permutation from LAPACK interchanges, kept beside the factors
+static int build_perm(bg_matrix *m) {
+  int N = m->N;
+  std::vector<int> ipiv(N), perm(N);
+  BG_CUDA_TRY(cudaMemcpyAsync(ipiv.data(), m->d_ipiv, sizeof(int) * N, cudaMemcpyDeviceToHost, stream()));
+  BG_CUDA_TRY(cudaStreamSynchronize(stream()));
+  for (int i = 0; i < N; i++) perm[i] = i;
+  for (int i = 0; i < N; i++) std::swap(perm[i], perm[ipiv[i] - 1]);
+  if (!m->d_perm) BG_CUDA_TRY(cudaMalloc(&m->d_perm, sizeof(int) * (N + 2 * ((N + TV_B - 1) / TV_B) + 8)));
+  BG_CUDA_TRY(cudaMemcpyAsync(m->d_perm, perm.data(), sizeof(int) * N, cudaMemcpyHostToDevice, stream()));
+  // ready flags of both sweeps + tickets + error word, zeroed once
+  BG_CUDA_TRY(cudaMemsetAsync(m->d_perm + N, 0, sizeof(int) * (2 * ((N + TV_B - 1) / TV_B) + 8), stream()));
+  BG_CUDA_TRY(cudaStreamSynchronize(stream()));
+  return BG_OK;
+}
+
+template <class C>
+static int getrs(bg_matrix *m, C *B, size_t ldb, int nrhs) {
+  int N = m->N;
+  const C *A = (const C *)m->d;
+  const int nb = (N + TV_B - 1) / TV_B;
+  int *flagsL = m->d_perm + N, *flagsU = flagsL + nb, *tick = flagsU + nb, *err = tick + 2;
+  const int smem = TV_B * (TV_B + 1) * (int)sizeof(C) + TV_B * TV_MAXRHS * (int)sizeof(C);
+  static bool attr = false;
+  if (!attr) {
+    BG_CUDA_TRY(cudaFuncSetAttribute(k_trsv<C, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    BG_CUDA_TRY(cudaFuncSetAttribute(k_trsv<C, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    attr = true;
+  }
+  for (int r0 = 0; r0 < nrhs; r0 += TV_MAXRHS) {
+    int nr = std::min(TV_MAXRHS, nrhs - r0);
+    C *Bp = B + (size_t)r0 * ldb;
+    C *T = nullptr;
+    BG_CUDA_TRY(cudaMallocAsync((void **)&T, sizeof(C) * (size_t)N * nr, stream()));
+    k_gather_rows<C><<<dim3((N + 255) / 256, nr), 256, 0, stream()>>>(N, nr, m->d_perm, Bp, ldb, T, N);
+    BG_LAUNCHED();
+    int epoch = ++m->solve_epoch;
+    BG_CUDA_TRY(cudaMemsetAsync(tick, 0, 2 * sizeof(int), stream()));
+    k_trsv<C, false><<<nb, 128, smem, stream()>>>(N, A, m->ld, T, N, nr, flagsL, epoch, tick, err);
+    BG_LAUNCHED();
+    k_trsv<C, true><<<nb, 128, smem, stream()>>>(N, A, m->ld, T, N, nr, flagsU, epoch, tick + 1, err);
+    BG_LAUNCHED();
+    BG_CUDA_TRY(cudaMemcpy2DAsync(Bp, sizeof(C) * ldb, T, sizeof(C) * N, sizeof(C) * N, nr, cudaMemcpyDeviceToDevice,
+                                  stream()));
+    BG_CUDA_TRY(cudaFreeAsync(T, stream()));
+  }
+  return BG_OK;
+}
+
+int lu_solve(bg_matrix *m, void *dB, int ldb, int nrhs) {
+  if (!m->d_perm) { set_error("solve: factorization state missing"); return BG_ERR_STATE; }
+  if (m->precision == BG_C128) return getrs<cdl>(m, (cdl *)dB, (size_t)ldb, nrhs);
+  return getrs<cfl>(m, (cfl *)dB, (size_t)ldb, nrhs);
+}
+
+// error word of the triangular sweeps (0 = ok)
+int lu_solve_status(bg_matrix *m) {
+  if (!m->d_perm) return BG_OK;
+  int N = m->N, nb = (N + TV_B - 1) / TV_B, e = 0;
+  BG_CUDA_TRY(cudaMemcpyAsync(&e, m->d_perm + N + 2 * nb + 2, sizeof(int), cudaMemcpyDeviceToHost, stream()));
+  BG_CUDA_TRY(cudaStreamSynchronize(stream()));
+  if (e) { set_error("triangular solve timed out waiting for a block (code %d)", e); return BG_ERR_CUDA; }
+  return BG_OK;
 }
 
 }  // namespace bg

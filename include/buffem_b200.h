@@ -139,7 +139,8 @@ int bg_lu_factor(bg_matrix *m);
 int bg_lu_pivots(const bg_matrix *m, int *ipiv_host);
 
 /* HMatrix::LUSolve(HVector *) -> zgetrs (call site buff-scatter.cc:314).
-   B is a host column-major N x nrhs complex128 array, overwritten by X. */
+   B is a host column-major N x nrhs complex128 array, overwritten by X (for a
+   BG_C64 matrix the solve runs in complex64 and B is rounded on the way). */
 int bg_lu_solve(bg_matrix *m, double *B_host, int nrhs);
 /* Same with B already on the device (leading dimension ldb, complex128). */
 int bg_lu_solve_device(bg_matrix *m, void *B_dev, int ldb, int nrhs);
@@ -149,6 +150,25 @@ int bg_lu_solve_device(bg_matrix *m, void *B_dev, int ldb, int nrhs);
    building block of buff-neq's dressed-Rytov chain (GetFlux.cc:155-272, four
    GEMMs per source object).  Runs on the library stream. */
 int bg_zgemm_sub_device(int M, int N, int K, const void *A, int lda, const void *B, int ldb, void *C, int ldc);
+
+/* ---------------------------------------------------------------------------
+ * precision form: complex64 tensor-core LU + FP64 iterative refinement
+ * (no reference counterpart; the reference factors in complex128 only)
+ * ------------------------------------------------------------------------- */
+
+/* Copy a complex128 matrix into a complex64 one of the same size (device). */
+int bg_matrix_convert(const bg_matrix *src, bg_matrix *dst);
+
+/* Solve A X = B with the complex64 LU factors F of A (bg_lu_factor on a
+   BG_C64 matrix runs the trailing updates on the tcgen05 tensor cores in
+   TF32) and FP64 iterative refinement against the complex128 matrix A:
+   x += F^{-1} (b - A x) until max_j |b_j - A x_j| / |b_j| <= tol or maxit
+   sweeps.  B: host N x nrhs complex128 (nrhs <= 4), overwritten by X.
+   stats (3 doubles, may be NULL): sweeps, final and first relative residual.
+   Returns BG_ERR_NUMERIC if the residual becomes non-finite. */
+int bg_lu_solve_refined(bg_matrix *A, bg_matrix *F, double *B_host, int nrhs, double tol, int maxit, double *stats);
+int bg_lu_solve_refined_device(bg_matrix *A, bg_matrix *F, void *B_dev, int ldb, int nrhs, double tol, int maxit,
+                               double *stats);
 
 /* ---------------------------------------------------------------------------
  * right-hand side and post-processing
