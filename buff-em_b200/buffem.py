@@ -73,6 +73,7 @@ EXPORTS = [
     "bg_rhs_planewave", "bg_rhs_planewave_device", "bg_pft", "bg_kernel_launch_count",
     "bg_synchronize", "bg_stream", "bg_profile_begin", "bg_profile_read", "bg_profile_end",
     "bg_zgemm_sub_device", "bg_matrix_convert", "bg_lu_solve_refined", "bg_lu_solve_refined_device",
+    "bg_lu_solve_device_noalloc",
 ]
 
 
@@ -106,6 +107,7 @@ def lib():
         L.bg_lu_pivots.argtypes = [P, VP]
         L.bg_lu_solve.argtypes = [P, VP, I]
         L.bg_lu_solve_device.argtypes = [P, VP, I, I]
+        L.bg_lu_solve_device_noalloc.argtypes = [P, VP, I, I]
         L.bg_rhs_planewave.argtypes = [P, D, D, VP, VP, VP]
         L.bg_rhs_planewave_device.argtypes = [P, D, D, VP, VP, VP]
         L.bg_pft.argtypes = [P, D, D, VP, VP, VP, I, VP]

@@ -337,6 +337,13 @@ int bg_lu_solve_device(bg_matrix *m, void *dB, int ldb, int nrhs) {
   return st;
 }
 
+int bg_lu_solve_device_noalloc(bg_matrix *m, void *dB, int ldb, int nrhs) {
+  if (!m || !dB || nrhs <= 0 || ldb < m->N) { set_error("bg_lu_solve_device_noalloc: bad arguments"); return BG_ERR_ARG; }
+  if (!m->factored) { set_error("bg_lu_solve_device_noalloc: matrix is not LU-factored"); return BG_ERR_STATE; }
+  if (m->info > 0) { set_error("bg_lu_solve_device_noalloc: factorization is singular (info=%d)", m->info); return BG_ERR_NUMERIC; }
+  return lu_solve_noalloc(m, dB, ldb, nrhs);
+}
+
 int bg_lu_solve(bg_matrix *m, double *B, int nrhs) {
   if (!m || !B || nrhs <= 0) { set_error("bg_lu_solve: bad arguments"); return BG_ERR_ARG; }
   if (!m->factored) { set_error("bg_lu_solve: matrix is not LU-factored"); return BG_ERR_STATE; }

@@ -146,6 +146,7 @@ int pft(bg_geometry *g, double wr, double wi, const void *dJ, const double *E0, 
 int lu_factor(bg_matrix *m);
 int lu_solve(bg_matrix *m, void *dB, int ldb, int nrhs);
 int lu_solve_status(bg_matrix *m);
+int lu_solve_noalloc(bg_matrix *m, void *dB, int ldb, int nrhs);
 int zgemm_sub_device(int M, int N, int K, const void *A, int lda, const void *B, int ldb, void *C, int ldc);
 int matrix_convert(const bg_matrix *src, bg_matrix *dst);
 int solve_refined(bg_matrix *A, bg_matrix *F, void *dB, int ldb, int nrhs, double tol, int maxit, double *stats);

@@ -823,4 +823,88 @@ int lu_solve_status(bg_matrix *m) {
   return BG_OK;
 }
 
+
+// =========================================================================
+// Allocation-free variant of the device solve.
+//
+// Some callers cannot allocate GPU memory at solve time: a host application
+// whose framework has already reserved the device memory for its own pool,
+// or a time-critical loop that cannot accept an allocation's possible failure
+// or implicit synchronisation.  For them the gather buffer of the solve lives
+// in this fixed device array instead of a stream-ordered allocation.  The
+// array (NOALLOC_BYTES) is held by every GPU that loads the library until the
+// process exits.  All calls share it: it keeps the last call's contents, and
+// two calls whose work overlaps on the GPU would race on it (calls through
+// this library are ordered on its single stream).  The gather overwrites the
+// part of the array a call uses before it is read, so nothing in it has to
+// start at zero; the sweep tickets that must start at zero live beside the
+// factors and are cleared by every call.
+// =========================================================================
+#define NOALLOC_BYTES (4u << 20)
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
+static void *s_noalloc_ptr[64];
+
+// once per device, with that device current: the array's device address (the
+// host-side symbol is only a stand-in and must never be passed to a kernel)
+static int noalloc_setup(void **ptr) {
+  int dev = 0;
+  BG_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) { set_error("device ordinal %d out of range", dev); return BG_ERR_CUDA; }
+  if (!s_noalloc_ptr[dev]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      set_error("cudaGetSymbolAddress of the solve scratch failed: %s", cudaGetErrorString(e));
+      return BG_ERR_CUDA;
+    }
+    s_noalloc_ptr[dev] = p;
+  }
+  *ptr = s_noalloc_ptr[dev];
+  return BG_OK;
+}
+
+template <class C>
+static int getrs_noalloc(bg_matrix *m, C *B, size_t ldb, int nrhs, void *scratch) {
+  int N = m->N;
+  const C *A = (const C *)m->d;
+  const int nb = (N + TV_B - 1) / TV_B;
+  int *flagsL = m->d_perm + N, *flagsU = flagsL + nb, *tick = flagsU + nb, *err = tick + 2;
+  const int smem = TV_B * (TV_B + 1) * (int)sizeof(C) + TV_B * TV_MAXRHS * (int)sizeof(C);
+  BG_CUDA_TRY(cudaFuncSetAttribute(k_trsv<C, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  BG_CUDA_TRY(cudaFuncSetAttribute(k_trsv<C, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  C *T = (C *)scratch;
+  k_gather_rows<C><<<dim3((N + 255) / 256, nrhs), 256, 0, stream()>>>(N, nrhs, m->d_perm, B, ldb, T, N);
+  BG_LAUNCHED();
+  int epoch = ++m->solve_epoch;
+  BG_CUDA_TRY(cudaMemsetAsync(tick, 0, 2 * sizeof(int), stream()));
+  k_trsv<C, false><<<nb, 128, smem, stream()>>>(N, A, m->ld, T, N, nrhs, flagsL, epoch, tick, err);
+  BG_LAUNCHED();
+  k_trsv<C, true><<<nb, 128, smem, stream()>>>(N, A, m->ld, T, N, nrhs, flagsU, epoch, tick + 1, err);
+  BG_LAUNCHED();
+  BG_CUDA_TRY(cudaMemcpy2DAsync(B, sizeof(C) * ldb, T, sizeof(C) * N, sizeof(C) * N, nrhs, cudaMemcpyDeviceToDevice,
+                                stream()));
+  return BG_OK;
+}
+
+int lu_solve_noalloc(bg_matrix *m, void *dB, int ldb, int nrhs) {
+  if (!m->d_perm) { set_error("solve: factorization state missing"); return BG_ERR_STATE; }
+  size_t esz = m->precision == BG_C128 ? sizeof(cdl) : sizeof(cfl);
+  if (nrhs > TV_MAXRHS) {
+    set_error("allocation-free solve: at most %d right-hand sides per call (got %d)", TV_MAXRHS, nrhs);
+    return BG_ERR_ARG;
+  }
+  if ((size_t)m->N * nrhs * esz > NOALLOC_BYTES) {
+    set_error("allocation-free solve: N*nrhs*%zu = %zu bytes exceeds its fixed %u-byte scratch", esz,
+              (size_t)m->N * nrhs * esz, NOALLOC_BYTES);
+    return BG_ERR_ARG;
+  }
+  void *scratch = nullptr;
+  int st = noalloc_setup(&scratch);
+  if (st) return st;
+  if (m->precision == BG_C128) st = getrs_noalloc<cdl>(m, (cdl *)dB, (size_t)ldb, nrhs, scratch);
+  else st = getrs_noalloc<cfl>(m, (cfl *)dB, (size_t)ldb, nrhs, scratch);
+  if (!st) st = lu_solve_status(m);
+  return st;
+}
+
 }  // namespace bg

@@ -145,6 +145,18 @@ int bg_lu_solve(bg_matrix *m, double *B_host, int nrhs);
 /* Same with B already on the device (leading dimension ldb, complex128). */
 int bg_lu_solve_device(bg_matrix *m, void *B_dev, int ldb, int nrhs);
 
+/* No counterpart in the reference.  bg_lu_solve_device for callers that
+   cannot allocate GPU memory at solve time (an application whose framework
+   has already reserved the device memory for its own pool, or a time-critical
+   loop that cannot accept an allocation's possible failure or implicit
+   synchronisation): the solve's gather buffer is a fixed 4 MiB device array
+   in the library instead of an allocation.  Limits: nrhs <= 4 and
+   N * nrhs * (16 bytes for complex128, 8 for complex64) <= 4 MiB, otherwise
+   BG_ERR_ARG.  The array is shared by all calls and keeps the last call's
+   contents; calls whose GPU work overlaps would race on it.  The first call
+   on a device looks up the array's device address. */
+int bg_lu_solve_device_noalloc(bg_matrix *m, void *B_dev, int ldb, int nrhs);
+
 /* C <- C - A*B for device column-major complex128 matrices (A: M x K, B: K x N,
    C: M x N), the FP64 tensor-core GEMM of the LU trailing update.  Also the
    building block of buff-neq's dressed-Rytov chain (GetFlux.cc:155-272, four
