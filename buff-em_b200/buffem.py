@@ -29,6 +29,7 @@ _LIB = None
 BG_C128, BG_C64 = 0, 1
 BG_MAT_CONST_ISO, BG_MAT_CONST_TENSOR, BG_MAT_JANUS_Z, BG_MAT_GAUSSIAN = 0, 1, 2, 3
 BG_PFT_EMT, BG_PFT_OVERLAP = 0, 1
+BG_OK, BG_ERR_ARG, BG_ERR_IO, BG_ERR_TOPOLOGY, BG_ERR_CUDA, BG_ERR_NOMEM, BG_ERR_STATE, BG_ERR_NUMERIC = 0, -1, -2, -3, -4, -5, -6, -7
 PFT_PABS, PFT_PSCAT = 0, 1
 
 
@@ -73,7 +74,10 @@ EXPORTS = [
     "bg_rhs_planewave", "bg_rhs_planewave_device", "bg_pft", "bg_kernel_launch_count",
     "bg_synchronize", "bg_stream", "bg_profile_begin", "bg_profile_read", "bg_profile_end",
     "bg_zgemm_sub_device", "bg_matrix_convert", "bg_lu_solve_refined", "bg_lu_solve_refined_device",
-    "bg_lu_solve_device_noalloc",
+    "bg_lu_solve_device_noalloc", "bg_precond_create_jacobi", "bg_precond_destroy", "bg_precond_nnz",
+    "bg_gmres_solve", "bg_gmres_solve_device", "bg_gnn_create", "bg_gnn_destroy", "bg_gnn_num_params",
+    "bg_gnn_get_params", "bg_gnn_set_params", "bg_gnn_get_grads", "bg_gnn_train_step",
+    "bg_precond_create_learned", "bg_precond_download", "bg_gmres_solve_mixed", "bg_gmres_solve_mixed_device",
 ]
 
 
@@ -108,6 +112,23 @@ def lib():
         L.bg_lu_solve.argtypes = [P, VP, I]
         L.bg_lu_solve_device.argtypes = [P, VP, I, I]
         L.bg_lu_solve_device_noalloc.argtypes = [P, VP, I, I]
+        L.bg_precond_create_jacobi.argtypes = [P, C.POINTER(P)]
+        L.bg_precond_destroy.argtypes = [P]
+        L.bg_precond_destroy.restype = None
+        L.bg_precond_nnz.argtypes = [P]
+        L.bg_gmres_solve.argtypes = [P, P, VP, I, D, I, I, VP]
+        L.bg_gmres_solve_device.argtypes = [P, P, VP, I, I, D, I, I, VP]
+        L.bg_gmres_solve_mixed.argtypes = [P, P, P, VP, I, D, I, I, D, VP]
+        L.bg_gmres_solve_mixed_device.argtypes = [P, P, P, VP, I, I, D, I, I, D, VP]
+        L.bg_gnn_create.argtypes = [C.c_ulonglong, C.POINTER(P)]
+        L.bg_gnn_destroy.argtypes = [P]
+        L.bg_gnn_destroy.restype = None
+        L.bg_gnn_get_params.argtypes = [P, VP]
+        L.bg_gnn_set_params.argtypes = [P, VP]
+        L.bg_gnn_get_grads.argtypes = [P, VP]
+        L.bg_gnn_train_step.argtypes = [P, P, P, D, VP, I, I, VP, VP, D, D, VP]
+        L.bg_precond_create_learned.argtypes = [P, P, D, P, C.POINTER(P)]
+        L.bg_precond_download.argtypes = [P, VP, VP, VP]
         L.bg_rhs_planewave.argtypes = [P, D, D, VP, VP, VP]
         L.bg_rhs_planewave_device.argtypes = [P, D, D, VP, VP, VP]
         L.bg_pft.argtypes = [P, D, D, VP, VP, VP, I, VP]
@@ -299,6 +320,124 @@ def zgemm_sub_device(M, N, K, A, lda, B, ldb, C, ldc):
 
 def C_void(p):
     return C.c_void_p(p)
+
+
+class Preconditioner:
+    """Sparse right preconditioner for GMRES (device CSR, complex128)."""
+
+    def __init__(self, handle):
+        self.h = handle
+
+    @classmethod
+    def jacobi(cls, M):
+        h = C.c_void_p()
+        _check(lib().bg_precond_create_jacobi(M.h, C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def learned(cls, geo, M, omega, net):
+        """Sparse approximate inverse predicted by the graph network `net`."""
+        h = C.c_void_p()
+        _check(lib().bg_precond_create_learned(geo.h, M.h, float(omega), net.h, C.byref(h)))
+        return cls(h)
+
+    def nnz(self):
+        return lib().bg_precond_nnz(self.h)
+
+    def csr(self, N):
+        """(rowptr, col, val) copied to the host."""
+        nnz = self.nnz()
+        rowptr = np.zeros(N + 1, np.int32)
+        col = np.zeros(nnz, np.int32)
+        val = np.zeros(nnz, np.complex128)
+        _check(lib().bg_precond_download(self.h, _ptr(rowptr), _ptr(col), _ptr(val)))
+        return rowptr, col, val
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().bg_precond_destroy(self.h)
+            self.h = None
+
+
+DEFAULT_GNN_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights", "gnn_near_spai.f32")
+
+
+class GNN:
+    """Graph network predicting near-field sparse approximate inverses."""
+
+    def __init__(self, seed=0):
+        h = C.c_void_p()
+        _check(lib().bg_gnn_create(int(seed), C.byref(h)))
+        self.h = h
+
+    @classmethod
+    def load(cls, path=None):
+        """Network with trained weights (raw little-endian float32 file)."""
+        path = path or DEFAULT_GNN_WEIGHTS
+        w = np.fromfile(path, dtype="<f4")
+        if w.size != cls.num_params():
+            raise BuffError(-1, f"{path}: {w.size} weights, the network has {cls.num_params()}")
+        net = cls(0)
+        net.set_params(w)
+        return net
+
+    @staticmethod
+    def num_params():
+        return lib().bg_gnn_num_params()
+
+    def params(self):
+        out = np.zeros(self.num_params(), np.float32)
+        _check(lib().bg_gnn_get_params(self.h, _ptr(out)))
+        return out
+
+    def set_params(self, p):
+        arr = np.ascontiguousarray(p, dtype=np.float32)
+        assert arr.size == self.num_params()
+        _check(lib().bg_gnn_set_params(self.h, _ptr(arr)))
+
+    def grads(self):
+        out = np.zeros(self.num_params(), np.float32)
+        _check(lib().bg_gnn_get_grads(self.h, _ptr(out)))
+        return out
+
+    def train_step(self, geo, M, omega, Z, b=None, x=None, lam=0.0, lr=1e-3, probe_power=0):
+        """One Adam step (lr=0: gradients only); returns the objective before the update.
+        probe_power > 0 first maps the probes that many times through z <- z - M D^-1 z."""
+        Zf = np.asfortranarray(Z, dtype=np.complex128)
+        p = 1 if Zf.ndim == 1 else Zf.shape[1]
+        bb = None if b is None else np.ascontiguousarray(b, dtype=np.complex128)
+        xx = None if x is None else np.ascontiguousarray(x, dtype=np.complex128)
+        loss = np.zeros(1)
+        _check(lib().bg_gnn_train_step(self.h, geo.h, M.h, float(omega), _ptr(Zf), p, int(probe_power),
+                                       _ptr(bb) if bb is not None else None,
+                                       _ptr(xx) if xx is not None else None, float(lam), float(lr), _ptr(loss)))
+        return float(loss[0])
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().bg_gnn_destroy(self.h)
+            self.h = None
+
+
+def GMRESSolve(M, B, P=None, tol=1e-10, restart=50, maxit=2000):
+    """Solve M X = B (M assembled, not factored) with restarted GMRES; returns (X, stats)."""
+    arr = np.asfortranarray(B, dtype=np.complex128).copy(order="F")
+    nrhs = 1 if arr.ndim == 1 else arr.shape[1]
+    st = np.zeros(3)
+    _check(lib().bg_gmres_solve(M.h, P.h if P is not None else None, _ptr(arr), nrhs, float(tol), int(restart),
+                                int(maxit), _ptr(st)))
+    return arr, st
+
+
+def GMRESSolveMixed(M, F, B, P=None, tol=1e-10, restart=50, maxit=2000, inner_tol=1e-5):
+    """Solve M X = B with GMRES on the complex64 copy F of M plus FP64
+    iterative refinement against M; returns (X, stats)."""
+    arr = np.asfortranarray(B, dtype=np.complex128).copy(order="F")
+    nrhs = 1 if arr.ndim == 1 else arr.shape[1]
+    st = np.zeros(3)
+    _check(lib().bg_gmres_solve_mixed(M.h, F.h, P.h if P is not None else None, _ptr(arr), nrhs, float(tol),
+                                      int(restart), int(maxit), float(inner_tol), _ptr(st)))
+    return arr, st
 
 
 def launch_count():

@@ -154,6 +154,7 @@ void bg_geometry_destroy(bg_geometry *g) {
   dfree(d.bfQ); dfree(d.bfLoc); dfree(d.tetFI); dfree(d.bfV); dfree(d.bfArea); dfree(d.bfRadius); dfree(d.mats); dfree(d.objOrigin);
   NearData &n = g->near;
   dfree(n.pairs); dfree(n.pairTP); dfree(n.fibbi); dfree(n.tp); dfree(n.tpOrdA); dfree(n.tpOrdB); dfree(n.tpMom);
+  dfree(g->graph.rowptr); dfree(g->graph.col); dfree(g->graph.etr);
   dfree(g->d_scratch);
   delete g;
 }
@@ -342,6 +343,91 @@ int bg_lu_solve_device_noalloc(bg_matrix *m, void *dB, int ldb, int nrhs) {
   if (!m->factored) { set_error("bg_lu_solve_device_noalloc: matrix is not LU-factored"); return BG_ERR_STATE; }
   if (m->info > 0) { set_error("bg_lu_solve_device_noalloc: factorization is singular (info=%d)", m->info); return BG_ERR_NUMERIC; }
   return lu_solve_noalloc(m, dB, ldb, nrhs);
+}
+
+int bg_precond_create_jacobi(bg_matrix *A, bg_precond **out) {
+  if (!A || !out || A->precision != BG_C128) { set_error("bg_precond_create_jacobi: complex128 matrix required"); return BG_ERR_ARG; }
+  *out = nullptr;
+  return precond_jacobi(A, out);
+}
+
+void bg_precond_destroy(bg_precond *P) {
+  if (!P) return;
+  dfree(P->rowptr); dfree(P->col); dfree(P->val);
+  delete P;
+}
+
+int bg_precond_nnz(const bg_precond *P) { return P ? P->nnz : BG_ERR_ARG; }
+
+int bg_gmres_solve_device(bg_matrix *A, const bg_precond *P, void *dB, int ldb, int nrhs, double tol, int restart,
+                          int maxit, double *stats) {
+  if (!A || !dB || nrhs <= 0 || ldb < A->N || restart < 2 || maxit < 1 || !(tol > 0)) {
+    set_error("bg_gmres_solve: bad arguments");
+    return BG_ERR_ARG;
+  }
+  if (A->precision != BG_C128) { set_error("bg_gmres_solve: complex128 matrix required"); return BG_ERR_ARG; }
+  if (A->factored) { set_error("bg_gmres_solve: the matrix holds LU factors, not the operator"); return BG_ERR_STATE; }
+  if (P && P->N != A->N) { set_error("bg_gmres_solve: preconditioner size mismatch"); return BG_ERR_ARG; }
+  return gmres_solve(A, P, dB, ldb, nrhs, tol, restart, maxit, stats);
+}
+
+int bg_gmres_solve(bg_matrix *A, const bg_precond *P, double *B, int nrhs, double tol, int restart, int maxit,
+                   double *stats) {
+  if (!A || !B || nrhs <= 0) { set_error("bg_gmres_solve: bad arguments"); return BG_ERR_ARG; }
+  size_t bytes = 16 * (size_t)A->N * nrhs;
+  void *dB = nullptr;
+  BG_CUDA_TRY(cudaMallocAsync(&dB, bytes, stream()));
+  int st = BG_OK;
+  cudaError_t e = cudaMemcpyAsync(dB, B, bytes, cudaMemcpyHostToDevice, stream());
+  if (e != cudaSuccess) { set_error("H2D: %s", cudaGetErrorString(e)); st = BG_ERR_CUDA; }
+  if (!st) st = bg_gmres_solve_device(A, P, dB, A->N, nrhs, tol, restart, maxit, stats);
+  if (!st) {
+    e = cudaMemcpyAsync(B, dB, bytes, cudaMemcpyDeviceToHost, stream());
+    if (e != cudaSuccess) { set_error("D2H: %s", cudaGetErrorString(e)); st = BG_ERR_CUDA; }
+  }
+  cudaFreeAsync(dB, stream());
+  cudaError_t e2 = cudaStreamSynchronize(stream());
+  if (!st && e2 != cudaSuccess) { set_error("gmres: %s", cudaGetErrorString(e2)); st = BG_ERR_CUDA; }
+  return st;
+}
+
+int bg_gmres_solve_mixed_device(bg_matrix *A, bg_matrix *F, const bg_precond *P, void *dB, int ldb, int nrhs,
+                                double tol, int restart, int maxit, double inner_tol, double *stats) {
+  if (!A || !F || !dB || nrhs <= 0 || ldb < A->N || restart < 2 || maxit < 1 || !(tol > 0) || !(inner_tol > 0) ||
+      !(inner_tol < 1)) {
+    set_error("bg_gmres_solve_mixed: bad arguments");
+    return BG_ERR_ARG;
+  }
+  if (A->precision != BG_C128 || F->precision != BG_C64 || F->N != A->N) {
+    set_error("bg_gmres_solve_mixed: complex128 A and complex64 F of equal size required");
+    return BG_ERR_ARG;
+  }
+  if (A->factored || F->factored) {
+    set_error("bg_gmres_solve_mixed: the matrices hold LU factors, not the operator");
+    return BG_ERR_STATE;
+  }
+  if (P && P->N != A->N) { set_error("bg_gmres_solve_mixed: preconditioner size mismatch"); return BG_ERR_ARG; }
+  return gmres_solve_mixed(A, F, P, dB, ldb, nrhs, tol, restart, maxit, inner_tol, stats);
+}
+
+int bg_gmres_solve_mixed(bg_matrix *A, bg_matrix *F, const bg_precond *P, double *B, int nrhs, double tol,
+                         int restart, int maxit, double inner_tol, double *stats) {
+  if (!A || !B || nrhs <= 0) { set_error("bg_gmres_solve_mixed: bad arguments"); return BG_ERR_ARG; }
+  size_t bytes = 16 * (size_t)A->N * nrhs;
+  void *dB = nullptr;
+  BG_CUDA_TRY(cudaMallocAsync(&dB, bytes, stream()));
+  int st = BG_OK;
+  cudaError_t e = cudaMemcpyAsync(dB, B, bytes, cudaMemcpyHostToDevice, stream());
+  if (e != cudaSuccess) { set_error("H2D: %s", cudaGetErrorString(e)); st = BG_ERR_CUDA; }
+  if (!st) st = bg_gmres_solve_mixed_device(A, F, P, dB, A->N, nrhs, tol, restart, maxit, inner_tol, stats);
+  if (!st) {
+    e = cudaMemcpyAsync(B, dB, bytes, cudaMemcpyDeviceToHost, stream());
+    if (e != cudaSuccess) { set_error("D2H: %s", cudaGetErrorString(e)); st = BG_ERR_CUDA; }
+  }
+  cudaFreeAsync(dB, stream());
+  cudaError_t e2 = cudaStreamSynchronize(stream());
+  if (!st && e2 != cudaSuccess) { set_error("gmres: %s", cudaGetErrorString(e2)); st = BG_ERR_CUDA; }
+  return st;
 }
 
 int bg_lu_solve(bg_matrix *m, double *B, int nrhs) {

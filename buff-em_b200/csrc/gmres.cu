@@ -1,0 +1,523 @@
+// Learned form, solver side: restarted GMRES(m) in FP64 on the device with a
+// sparse right preconditioner on the near-field pattern (diagonal Jacobi or
+// the near-field sparse approximate inverse predicted by the graph network of
+// gnn.cu).  Up to four right-hand sides run in lockstep so that every Arnoldi
+// step costs one pass over the dense complex128 matrix (HBM-bound, 16 N^2
+// bytes); classical Gram-Schmidt with one re-orthogonalisation; Givens
+// rotations on the host from the per-step coefficients.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <vector>
+
+#include "internal.h"
+
+namespace bg {
+
+struct z2 { double r, i; };
+typedef std::complex<double> zc;
+
+#define GM_MAXRHS 4
+#define GV_ROWS 128
+#define GV_COLS 256
+
+// Y[:, j] = A X[:, j] for the dense complex128 matrix: partial sums per
+// 256-column chunk (summed in a fixed order by k_gm_matvec_sum); columns are
+// read four at a time so each thread keeps four 16-byte loads in flight.
+__global__ void __launch_bounds__(GV_ROWS) k_gm_matvec_part(int N, const z2 *A, size_t lda, const z2 *X, size_t ldx,
+                                                            int nrhs, z2 *partial) {
+  __shared__ z2 xs[GV_COLS][GM_MAXRHS];
+  int row = blockIdx.x * GV_ROWS + threadIdx.x;
+  int c0 = blockIdx.y * GV_COLS;
+  int nc = min(GV_COLS, N - c0);
+  for (int e = threadIdx.x; e < nc * nrhs; e += GV_ROWS) {
+    int c = e / nrhs, j = e % nrhs;
+    xs[c][j] = X[(size_t)j * ldx + c0 + c];
+  }
+  __syncthreads();
+  if (row >= N) return;
+  double ar[GM_MAXRHS] = {0, 0, 0, 0}, ai[GM_MAXRHS] = {0, 0, 0, 0};
+  const z2 *ap = A + (size_t)c0 * lda + row;
+  int c = 0;
+  for (; c + 4 <= nc; c += 4) {
+    z2 a[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      double2 t = __ldcs(reinterpret_cast<const double2 *>(ap + (size_t)(c + u) * lda));
+      a[u] = z2{t.x, t.y};
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+#pragma unroll
+      for (int j = 0; j < GM_MAXRHS; j++)
+        if (j < nrhs) {
+          z2 x = xs[c + u][j];
+          ar[j] += a[u].r * x.r - a[u].i * x.i;
+          ai[j] += a[u].r * x.i + a[u].i * x.r;
+        }
+  }
+  for (; c < nc; c++) {
+    z2 a = ap[(size_t)c * lda];
+#pragma unroll
+    for (int j = 0; j < GM_MAXRHS; j++)
+      if (j < nrhs) {
+        z2 x = xs[c][j];
+        ar[j] += a.r * x.r - a.i * x.i;
+        ai[j] += a.r * x.i + a.i * x.r;
+      }
+  }
+  for (int j = 0; j < nrhs; j++) partial[((size_t)blockIdx.y * nrhs + j) * N + row] = z2{ar[j], ai[j]};
+}
+
+// Same for the complex64 copy of the matrix: each thread takes two adjacent
+// rows (one 16-byte load per column), FP32 accumulation within a chunk, FP64
+// partial sums across chunks.  Reads row N when N is odd: complex64 matrices
+// are stored with a leading dimension padded to a multiple of 32 (> N then).
+__global__ void __launch_bounds__(GV_ROWS) k_gm_matvec_part_c64(int N, const float4 *A, size_t lda2, const z2 *X,
+                                                                size_t ldx, int nrhs, z2 *partial) {
+  __shared__ float2 xs[GV_COLS][GM_MAXRHS];
+  int row = 2 * (blockIdx.x * GV_ROWS + threadIdx.x);
+  int c0 = blockIdx.y * GV_COLS;
+  int nc = min(GV_COLS, N - c0);
+  for (int e = threadIdx.x; e < nc * nrhs; e += GV_ROWS) {
+    int c = e / nrhs, j = e % nrhs;
+    z2 x = X[(size_t)j * ldx + c0 + c];
+    xs[c][j] = make_float2((float)x.r, (float)x.i);
+  }
+  __syncthreads();
+  if (row >= N) return;
+  float ar0[GM_MAXRHS] = {0, 0, 0, 0}, ai0[GM_MAXRHS] = {0, 0, 0, 0};
+  float ar1[GM_MAXRHS] = {0, 0, 0, 0}, ai1[GM_MAXRHS] = {0, 0, 0, 0};
+  const float4 *ap = A + (size_t)c0 * lda2 + (row >> 1);
+  int c = 0;
+  for (; c + 4 <= nc; c += 4) {
+    float4 a[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) a[u] = __ldcs(ap + (size_t)(c + u) * lda2);
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+#pragma unroll
+      for (int j = 0; j < GM_MAXRHS; j++)
+        if (j < nrhs) {
+          float2 x = xs[c + u][j];
+          ar0[j] += a[u].x * x.x - a[u].y * x.y;
+          ai0[j] += a[u].x * x.y + a[u].y * x.x;
+          ar1[j] += a[u].z * x.x - a[u].w * x.y;
+          ai1[j] += a[u].z * x.y + a[u].w * x.x;
+        }
+  }
+  for (; c < nc; c++) {
+    float4 a = ap[(size_t)c * lda2];
+#pragma unroll
+    for (int j = 0; j < GM_MAXRHS; j++)
+      if (j < nrhs) {
+        float2 x = xs[c][j];
+        ar0[j] += a.x * x.x - a.y * x.y;
+        ai0[j] += a.x * x.y + a.y * x.x;
+        ar1[j] += a.z * x.x - a.w * x.y;
+        ai1[j] += a.z * x.y + a.w * x.x;
+      }
+  }
+  for (int j = 0; j < nrhs; j++) {
+    partial[((size_t)blockIdx.y * nrhs + j) * N + row] = z2{ar0[j], ai0[j]};
+    if (row + 1 < N) partial[((size_t)blockIdx.y * nrhs + j) * N + row + 1] = z2{ar1[j], ai1[j]};
+  }
+}
+
+__global__ void k_gm_matvec_sum(int N, int nchunk, int nrhs, const z2 *partial, z2 *Y, size_t ldy) {
+  int row = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y;
+  if (row >= N || j >= nrhs) return;
+  double sr = 0, si = 0;
+  for (int k = 0; k < nchunk; k++) {
+    z2 p = partial[((size_t)k * nrhs + j) * N + row];
+    sr += p.r;
+    si += p.i;
+  }
+  Y[(size_t)j * ldy + row] = z2{sr, si};
+}
+
+// Y[:, j] = M X[:, j], M in CSR (row i: sum over its near columns)
+__global__ void k_gm_spmv(int N, const int *rowptr, const int *col, const z2 *val, const z2 *X, size_t ldx, int nrhs,
+                          z2 *Y, size_t ldy) {
+  int row = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y;
+  if (row >= N || j >= nrhs) return;
+  double sr = 0, si = 0;
+  for (int p = rowptr[row]; p < rowptr[row + 1]; p++) {
+    z2 m = val[p], x = X[(size_t)j * ldx + col[p]];
+    sr += m.r * x.r - m.i * x.i;
+    si += m.r * x.i + m.i * x.r;
+  }
+  Y[(size_t)j * ldy + row] = z2{sr, si};
+}
+
+// dots[j*(k) + c] = <V_j[:,c], w_j>  (c < k), block reduction per (c, j)
+__global__ void k_gm_dots(int N, int k, const z2 *V, size_t ldv, size_t vstride, const z2 *W, size_t ldw, z2 *dots) {
+  int c = blockIdx.x, j = blockIdx.y;
+  const z2 *v = V + j * vstride + (size_t)c * ldv;
+  const z2 *w = W + (size_t)j * ldw;
+  double sr = 0, si = 0;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    z2 a = v[i], b = w[i];
+    sr += a.r * b.r + a.i * b.i;   // conj(a) b
+    si += a.r * b.i - a.i * b.r;
+  }
+  __shared__ double rs[32], is[32];
+  for (int o = 16; o > 0; o >>= 1) {
+    sr += __shfl_xor_sync(0xffffffffu, sr, o);
+    si += __shfl_xor_sync(0xffffffffu, si, o);
+  }
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) { rs[wid] = sr; is[wid] = si; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0, b = 0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); q++) { a += rs[q]; b += is[q]; }
+    dots[(size_t)j * gridDim.x + c] = z2{a, b};
+  }
+}
+
+// w_j -= V_j[:, 0:k] h_j
+__global__ void k_gm_subtract(int N, int k, const z2 *V, size_t ldv, size_t vstride, const z2 *h, size_t ldh, z2 *W,
+                              size_t ldw) {
+  int row = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y;
+  if (row >= N) return;
+  const z2 *v = V + j * vstride + row;
+  const z2 *hj = h + (size_t)j * ldh;
+  double sr = 0, si = 0;
+  for (int c = 0; c < k; c++) {
+    z2 a = v[(size_t)c * ldv], b = hj[c];
+    sr += a.r * b.r - a.i * b.i;
+    si += a.r * b.i + a.i * b.r;
+  }
+  z2 *w = W + (size_t)j * ldw + row;
+  w->r -= sr;
+  w->i -= si;
+}
+
+// V_j[:, c] = s_j * W_j ; X_j += sum_c V_j[:, c] y_j[c] ; etc.
+__global__ void k_gm_scale_copy(int N, const z2 *W, size_t ldw, const double *s, z2 *V, size_t ldv_col_stride,
+                                size_t vstride) {
+  int row = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y;
+  if (row >= N) return;
+  z2 w = W[(size_t)j * ldw + row];
+  double f = s[j];
+  V[j * vstride + ldv_col_stride + row] = z2{w.r * f, w.i * f};
+}
+
+__global__ void k_gm_combine(int N, int k, const z2 *V, size_t ldv, size_t vstride, const z2 *y, size_t ldy, z2 *Z,
+                             size_t ldz) {
+  int row = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y;
+  if (row >= N) return;
+  const z2 *v = V + j * vstride + row;
+  double sr = 0, si = 0;
+  for (int c = 0; c < k; c++) {
+    z2 a = v[(size_t)c * ldv], b = y[(size_t)j * ldy + c];
+    sr += a.r * b.r - a.i * b.i;
+    si += a.r * b.i + a.i * b.r;
+  }
+  Z[(size_t)j * ldz + row] = z2{sr, si};
+}
+
+__global__ void k_gm_axpy(int N, const z2 *D, size_t ldd, z2 *X, size_t ldx, int sign) {
+  int row = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y;
+  if (row >= N) return;
+  z2 d = D[(size_t)j * ldd + row];
+  z2 *x = X + (size_t)j * ldx + row;
+  x->r += sign * d.r;
+  x->i += sign * d.i;
+}
+
+struct GmState {
+  int N, nrhs, m;
+  z2 *V, *W, *Z, *R, *part, *dots, *h;
+  double *sc;
+  int nchunk;
+};
+
+static int dense_matvec(bg_matrix *A, const z2 *X, z2 *Y, GmState &S) {
+  int N = S.N;
+  if (A->precision == BG_C64) {
+    dim3 g1((N + 2 * GV_ROWS - 1) / (2 * GV_ROWS), S.nchunk);
+    k_gm_matvec_part_c64<<<g1, GV_ROWS, 0, stream()>>>(N, (const float4 *)A->d, A->ld / 2, X, N, S.nrhs, S.part);
+  } else {
+    dim3 g1((N + GV_ROWS - 1) / GV_ROWS, S.nchunk);
+    k_gm_matvec_part<<<g1, GV_ROWS, 0, stream()>>>(N, (const z2 *)A->d, A->ld, X, N, S.nrhs, S.part);
+  }
+  BG_LAUNCHED();
+  k_gm_matvec_sum<<<dim3((N + 255) / 256, S.nrhs), 256, 0, stream()>>>(N, S.nchunk, S.nrhs, S.part, Y, N);
+  BG_LAUNCHED();
+  return BG_OK;
+}
+
+static int precond(const bg_precond *P, const z2 *X, z2 *Y, GmState &S) {
+  int N = S.N;
+  if (!P) {
+    BG_CUDA_TRY(cudaMemcpyAsync(Y, X, sizeof(z2) * (size_t)N * S.nrhs, cudaMemcpyDeviceToDevice, stream()));
+    return BG_OK;
+  }
+  k_gm_spmv<<<dim3((N + 127) / 128, S.nrhs), 128, 0, stream()>>>(N, P->rowptr, P->col, (const z2 *)P->val, X, N,
+                                                                 S.nrhs, Y, N);
+  BG_LAUNCHED();
+  return BG_OK;
+}
+
+static int colnorms(const z2 *X, GmState &S, std::vector<double> &out) {
+  // reuse k_gm_dots with V = W = X (k = 1 column)
+  k_gm_dots<<<dim3(1, S.nrhs), 256, 0, stream()>>>(S.N, 1, X, S.N, (size_t)S.N, X, S.N, S.dots);
+  BG_LAUNCHED();
+  std::vector<z2> h(S.nrhs);
+  BG_CUDA_TRY(cudaMemcpyAsync(h.data(), S.dots, sizeof(z2) * S.nrhs, cudaMemcpyDeviceToHost, stream()));
+  BG_CUDA_TRY(cudaStreamSynchronize(stream()));
+  out.resize(S.nrhs);
+  for (int j = 0; j < S.nrhs; j++) out[j] = std::sqrt(std::max(h[j].r, 0.0));
+  return BG_OK;
+}
+
+// solve A X = B (device, N x nrhs complex128, in place), right preconditioner P
+int gmres_solve(bg_matrix *A, const bg_precond *P, void *dB, int ldb, int nrhs, double tol, int restart, int maxit,
+                double *stats) {
+  int N = A->N, m = std::max(2, std::min(restart, 200));
+  if (nrhs > GM_MAXRHS) { set_error("gmres: at most %d right-hand sides per call", GM_MAXRHS); return BG_ERR_ARG; }
+  GmState S{N, nrhs, m};
+  S.nchunk = (N + GV_COLS - 1) / GV_COLS;
+  size_t nv = (size_t)N * (m + 1) * nrhs;
+  size_t bytes = sizeof(z2) * (nv + 4 * (size_t)N * nrhs + (size_t)S.nchunk * nrhs * N + 2 * (size_t)(m + 2) * nrhs) +
+                 sizeof(double) * 8;
+  char *w = nullptr;
+  BG_CUDA_TRY(cudaMallocAsync((void **)&w, bytes, stream()));
+  S.V = (z2 *)w;
+  S.W = S.V + nv;
+  S.Z = S.W + (size_t)N * nrhs;
+  S.R = S.Z + (size_t)N * nrhs;
+  z2 *X = S.R + (size_t)N * nrhs;
+  S.part = X + (size_t)N * nrhs;
+  S.dots = S.part + (size_t)S.nchunk * nrhs * N;
+  S.h = S.dots + (size_t)(m + 2) * nrhs;
+  S.sc = (double *)(S.h + (size_t)(m + 2) * nrhs);
+  const size_t vstride = (size_t)N * (m + 1);
+  int st = BG_OK;
+  const z2 *B = (const z2 *)dB;
+  // X = 0
+  BG_CUDA_TRY(cudaMemsetAsync(X, 0, sizeof(z2) * (size_t)N * nrhs, stream()));
+  // B contiguous copy in W for norms
+  BG_CUDA_TRY(cudaMemcpy2DAsync(S.W, sizeof(z2) * N, dB, sizeof(z2) * ldb, sizeof(z2) * N, nrhs,
+                                cudaMemcpyDeviceToDevice, stream()));
+  std::vector<double> bn, rn;
+  if ((st = colnorms(S.W, S, bn))) { cudaFreeAsync(w, stream()); return st; }
+  for (auto &v : bn) v = std::max(v, 1e-300);
+  int total = 0;
+  double relres = 1.0, first = -1;
+  std::vector<int> done(nrhs, 0);
+  dim3 gr((N + 255) / 256, nrhs);
+  while (!st && total < maxit) {
+    // R = B - A X
+    if ((st = dense_matvec(A, X, S.R, S))) break;
+    BG_CUDA_TRY(cudaMemcpy2DAsync(S.Z, sizeof(z2) * N, dB, sizeof(z2) * ldb, sizeof(z2) * N, nrhs,
+                                  cudaMemcpyDeviceToDevice, stream()));
+    k_gm_axpy<<<gr, 256, 0, stream()>>>(N, S.R, N, S.Z, N, -1);   // Z = B - AX
+    g_launches++;
+    if ((st = colnorms(S.Z, S, rn))) break;
+    relres = 0;
+    for (int j = 0; j < nrhs; j++) relres = std::max(relres, rn[j] / bn[j]);
+    if (first < 0) first = relres;
+    if (relres <= tol) break;
+    // V[:,0] = Z / beta
+    std::vector<double> inv(nrhs);
+    for (int j = 0; j < nrhs; j++) inv[j] = rn[j] > 0 ? 1.0 / rn[j] : 0.0;
+    BG_CUDA_TRY(cudaMemcpyAsync(S.sc, inv.data(), sizeof(double) * nrhs, cudaMemcpyHostToDevice, stream()));
+    k_gm_scale_copy<<<gr, 256, 0, stream()>>>(N, S.Z, N, S.sc, S.V, 0, vstride);
+    g_launches++;
+    // Hessenberg and Givens state per rhs
+    std::vector<std::vector<zc>> H(nrhs, std::vector<zc>((size_t)(m + 1) * m, 0.0));
+    std::vector<std::vector<zc>> g(nrhs, std::vector<zc>(m + 1, 0.0)), cs(nrhs, std::vector<zc>(m)),
+        sn(nrhs, std::vector<zc>(m));
+    for (int j = 0; j < nrhs; j++) g[j][0] = rn[j];
+    int k = 0;
+    bool conv = false;
+    for (; k < m && total < maxit; k++, total++) {
+      // W = A M V[:,k]
+      z2 *vk = S.V + (size_t)k * N;   // rhs j at vk + j*vstride: gather into Z contiguous
+      for (int j = 0; j < nrhs; j++)
+        BG_CUDA_TRY(cudaMemcpyAsync(S.R + (size_t)j * N, vk + j * vstride, sizeof(z2) * N, cudaMemcpyDeviceToDevice,
+                                    stream()));
+      if ((st = precond(P, S.R, S.Z, S))) break;
+      if ((st = dense_matvec(A, S.Z, S.W, S))) break;
+      // CGS2
+      std::vector<zc> hcol((size_t)nrhs * (k + 2), 0.0);
+      for (int pass = 0; pass < 2; pass++) {
+        k_gm_dots<<<dim3(k + 1, nrhs), 256, 0, stream()>>>(N, k + 1, S.V, N, vstride, S.W, N, S.dots);
+        g_launches++;
+        k_gm_subtract<<<gr, 256, 0, stream()>>>(N, k + 1, S.V, N, vstride, S.dots, (size_t)(k + 1), S.W, N);
+        g_launches++;
+        std::vector<z2> hd((size_t)nrhs * (k + 1));
+        BG_CUDA_TRY(cudaMemcpyAsync(hd.data(), S.dots, sizeof(z2) * hd.size(), cudaMemcpyDeviceToHost, stream()));
+        BG_CUDA_TRY(cudaStreamSynchronize(stream()));
+        for (int j = 0; j < nrhs; j++)
+          for (int c = 0; c <= k; c++) hcol[(size_t)j * (k + 2) + c] += zc(hd[(size_t)j * (k + 1) + c].r, hd[(size_t)j * (k + 1) + c].i);
+      }
+      std::vector<double> wn;
+      if ((st = colnorms(S.W, S, wn))) break;
+      for (int j = 0; j < nrhs; j++) {
+        hcol[(size_t)j * (k + 2) + k + 1] = wn[j];
+        inv[j] = wn[j] > 0 ? 1.0 / wn[j] : 0.0;
+      }
+      BG_CUDA_TRY(cudaMemcpyAsync(S.sc, inv.data(), sizeof(double) * nrhs, cudaMemcpyHostToDevice, stream()));
+      if (k + 1 <= m) {
+        k_gm_scale_copy<<<gr, 256, 0, stream()>>>(N, S.W, N, S.sc, S.V, (size_t)(k + 1) * N, vstride);
+        g_launches++;
+      }
+      // Givens
+      relres = 0;
+      for (int j = 0; j < nrhs; j++) {
+        std::vector<zc> hc(hcol.begin() + (size_t)j * (k + 2), hcol.begin() + (size_t)(j + 1) * (k + 2));
+        for (int i = 0; i < k; i++) {
+          zc t = cs[j][i] * hc[i] + sn[j][i] * hc[i + 1];
+          hc[i + 1] = -std::conj(sn[j][i]) * hc[i] + std::conj(cs[j][i]) * hc[i + 1];
+          hc[i] = t;
+        }
+        double a = std::abs(hc[k]), b = std::abs(hc[k + 1]);
+        double r = std::sqrt(a * a + b * b);
+        // unitary [c s; -conj(s) conj(c)] with c = conj(a)/r, s = conj(b)/r maps (a, b) to (r, 0)
+        cs[j][k] = r > 0 ? std::conj(hc[k]) / r : zc(1.0);
+        sn[j][k] = r > 0 ? std::conj(hc[k + 1]) / r : zc(0.0);
+        hc[k] = r;
+        hc[k + 1] = 0.0;
+        zc gk = g[j][k];
+        g[j][k] = cs[j][k] * gk;
+        g[j][k + 1] = -std::conj(sn[j][k]) * gk;
+        for (int i = 0; i <= k; i++) H[j][(size_t)i + (size_t)k * (m + 1)] = hc[i];
+        relres = std::max(relres, std::abs(g[j][k + 1]) / bn[j]);
+      }
+      if (relres <= tol) { k++; total++; conv = true; break; }
+    }
+    if (st) break;
+    // back substitution y = H^-1 g, X += M V y
+    std::vector<z2> yh((size_t)nrhs * k);
+    for (int j = 0; j < nrhs; j++) {
+      std::vector<zc> y(k);
+      for (int i = k - 1; i >= 0; i--) {
+        zc s = g[j][i];
+        for (int c = i + 1; c < k; c++) s -= H[j][(size_t)i + (size_t)c * (m + 1)] * y[c];
+        y[i] = s / H[j][(size_t)i + (size_t)i * (m + 1)];
+      }
+      for (int i = 0; i < k; i++) yh[(size_t)j * k + i] = z2{y[i].real(), y[i].imag()};
+    }
+    BG_CUDA_TRY(cudaMemcpyAsync(S.h, yh.data(), sizeof(z2) * yh.size(), cudaMemcpyHostToDevice, stream()));
+    k_gm_combine<<<gr, 256, 0, stream()>>>(N, k, S.V, N, vstride, S.h, (size_t)k, S.R, N);
+    g_launches++;
+    if ((st = precond(P, S.R, S.Z, S))) break;
+    k_gm_axpy<<<gr, 256, 0, stream()>>>(N, S.Z, N, X, N, 1);
+    g_launches++;
+    if (conv) {
+      // confirm with the true residual
+      if ((st = dense_matvec(A, X, S.R, S))) break;
+      BG_CUDA_TRY(cudaMemcpy2DAsync(S.Z, sizeof(z2) * N, dB, sizeof(z2) * ldb, sizeof(z2) * N, nrhs,
+                                    cudaMemcpyDeviceToDevice, stream()));
+      k_gm_axpy<<<gr, 256, 0, stream()>>>(N, S.R, N, S.Z, N, -1);
+      g_launches++;
+      if ((st = colnorms(S.Z, S, rn))) break;
+      relres = 0;
+      for (int j = 0; j < nrhs; j++) relres = std::max(relres, rn[j] / bn[j]);
+      if (relres <= tol * 10) break;
+    }
+  }
+  if (!st) {
+    cudaError_t e = cudaMemcpy2DAsync(dB, sizeof(z2) * ldb, X, sizeof(z2) * N, sizeof(z2) * N, nrhs,
+                                      cudaMemcpyDeviceToDevice, stream());
+    if (e != cudaSuccess) { set_error("gmres: %s", cudaGetErrorString(e)); st = BG_ERR_CUDA; }
+  }
+  cudaFreeAsync(w, stream());
+  if (stats) { stats[0] = total; stats[1] = relres; stats[2] = first; }
+  return st;
+}
+
+// GMRES with FP64 iterative refinement: each Krylov solve runs against the
+// complex64 copy F of A (8 N^2 bytes per step instead of 16), corrections
+// accumulate in FP64 and the residual b - A x is recomputed with the
+// complex128 matrix A between solves, until max_j |b_j - A x_j| / |b_j| <= tol.
+int gmres_solve_mixed(bg_matrix *A, bg_matrix *F, const bg_precond *P, void *dB, int ldb, int nrhs, double tol,
+                      int restart, int maxit, double inner_tol, double *stats) {
+  int N = A->N;
+  if (nrhs > GM_MAXRHS) { set_error("gmres: at most %d right-hand sides per call", GM_MAXRHS); return BG_ERR_ARG; }
+  GmState S{N, nrhs, 0};
+  S.nchunk = (N + GV_COLS - 1) / GV_COLS;
+  size_t nn = (size_t)N * nrhs;
+  char *w = nullptr;
+  BG_CUDA_TRY(cudaMallocAsync((void **)&w, sizeof(z2) * (4 * nn + (size_t)S.nchunk * nn + 4 * nrhs), stream()));
+  z2 *B0 = (z2 *)w, *X = B0 + nn, *R = X + nn, *T = R + nn;
+  S.part = T + nn;
+  S.dots = S.part + (size_t)S.nchunk * nn;
+  int st = BG_OK;
+  dim3 gr((N + 255) / 256, nrhs);
+  std::vector<double> bn, rn;
+  BG_CUDA_TRY(cudaMemcpy2DAsync(B0, sizeof(z2) * N, dB, sizeof(z2) * ldb, sizeof(z2) * N, nrhs,
+                                cudaMemcpyDeviceToDevice, stream()));
+  BG_CUDA_TRY(cudaMemsetAsync(X, 0, sizeof(z2) * nn, stream()));
+  BG_CUDA_TRY(cudaMemcpyAsync(R, B0, sizeof(z2) * nn, cudaMemcpyDeviceToDevice, stream()));
+  if ((st = colnorms(B0, S, bn))) { cudaFreeAsync(w, stream()); return st; }
+  for (auto &v : bn) v = std::max(v, 1e-300);
+  int total = 0, sweeps = 0;
+  double relres = 1.0;
+  while (!st && relres > tol && total < maxit && sweeps < 40) {
+    double ist[3] = {0, 0, 0};
+    // R <- approximately F^{-1} R (in place)
+    if ((st = gmres_solve(F, P, R, N, nrhs, inner_tol, restart, maxit - total, ist))) break;
+    total += (int)ist[0];
+    sweeps++;
+    k_gm_axpy<<<gr, 256, 0, stream()>>>(N, R, N, X, N, 1);
+    g_launches++;
+    if ((st = dense_matvec(A, X, T, S))) break;
+    BG_CUDA_TRY(cudaMemcpyAsync(R, B0, sizeof(z2) * nn, cudaMemcpyDeviceToDevice, stream()));
+    k_gm_axpy<<<gr, 256, 0, stream()>>>(N, T, N, R, N, -1);
+    g_launches++;
+    if ((st = colnorms(R, S, rn))) break;
+    relres = 0;
+    for (int j = 0; j < nrhs; j++) relres = std::max(relres, rn[j] / bn[j]);
+    if (!std::isfinite(relres)) { set_error("gmres: non-finite residual"); st = BG_ERR_NUMERIC; }
+  }
+  if (!st) {
+    cudaError_t e = cudaMemcpy2DAsync(dB, sizeof(z2) * ldb, X, sizeof(z2) * N, sizeof(z2) * N, nrhs,
+                                      cudaMemcpyDeviceToDevice, stream());
+    if (e != cudaSuccess) { set_error("gmres: %s", cudaGetErrorString(e)); st = BG_ERR_CUDA; }
+  }
+  cudaFreeAsync(w, stream());
+  if (stats) { stats[0] = total; stats[1] = relres; stats[2] = sweeps; }
+  return st;
+}
+
+// diagonal (Jacobi) preconditioner from the assembled matrix
+__global__ void k_gm_diag_inv(int N, const z2 *A, size_t lda, int *rowptr, int *col, z2 *val) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > N) return;
+  rowptr[i] = i;
+  if (i == N) return;
+  z2 a = A[(size_t)i * lda + i];
+  double d = a.r * a.r + a.i * a.i;
+  col[i] = i;
+  val[i] = z2{a.r / d, -a.i / d};
+}
+
+int precond_jacobi(bg_matrix *A, bg_precond **out) {
+  bg_precond *P = new bg_precond();
+  P->N = A->N;
+  P->nnz = A->N;
+  BG_CUDA_TRY(cudaMalloc(&P->rowptr, sizeof(int) * (A->N + 1)));
+  BG_CUDA_TRY(cudaMalloc(&P->col, sizeof(int) * A->N));
+  BG_CUDA_TRY(cudaMalloc(&P->val, sizeof(z2) * A->N));
+  k_gm_diag_inv<<<(A->N + 256) / 256, 256, 0, stream()>>>(A->N, (const z2 *)A->d, A->ld, P->rowptr, P->col,
+                                                          (z2 *)P->val);
+  BG_LAUNCHED();
+  *out = P;
+  return BG_OK;
+}
+
+}  // namespace bg

@@ -104,6 +104,15 @@ struct NearData {
   double *tpMom = nullptr;     // 24 moments per tet pair
 };
 
+// near-field graph of the basis functions for the learned preconditioner:
+// CSR of pairs with a common vertex (both directions, self pairs included,
+// columns sorted), reverse-edge map, mean face radius; built once per geometry
+struct NearGraph {
+  int E = 0;
+  int *rowptr = nullptr, *col = nullptr, *etr = nullptr;
+  double h = 0;
+};
+
 }  // namespace bg
 
 struct bg_geometry {
@@ -114,8 +123,15 @@ struct bg_geometry {
   bg::NearData near;
   int singular_order = 10;
   bool uploaded = false, precomputed = false;
+  bg::NearGraph graph;
   double *d_scratch = nullptr;  // general scratch (PFT partial sums etc.)
   size_t scratch_bytes = 0;
+};
+
+struct bg_precond {
+  int N = 0, nnz = 0;
+  int *rowptr = nullptr, *col = nullptr;   // CSR on the device
+  void *val = nullptr;                     // complex128 values
 };
 
 struct bg_matrix {
@@ -147,6 +163,11 @@ int lu_factor(bg_matrix *m);
 int lu_solve(bg_matrix *m, void *dB, int ldb, int nrhs);
 int lu_solve_status(bg_matrix *m);
 int lu_solve_noalloc(bg_matrix *m, void *dB, int ldb, int nrhs);
+int gmres_solve(bg_matrix *A, const bg_precond *P, void *dB, int ldb, int nrhs, double tol, int restart, int maxit,
+                double *stats);
+int gmres_solve_mixed(bg_matrix *A, bg_matrix *F, const bg_precond *P, void *dB, int ldb, int nrhs, double tol,
+                      int restart, int maxit, double inner_tol, double *stats);
+int precond_jacobi(bg_matrix *A, bg_precond **out);
 int zgemm_sub_device(int M, int N, int K, const void *A, int lda, const void *B, int ldb, void *C, int ldc);
 int matrix_convert(const bg_matrix *src, bg_matrix *dst);
 int solve_refined(bg_matrix *A, bg_matrix *F, void *dB, int ldb, int nrhs, double tol, int maxit, double *stats);

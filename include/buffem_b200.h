@@ -60,6 +60,7 @@ typedef struct bg_material {
 
 typedef struct bg_geometry bg_geometry;
 typedef struct bg_matrix bg_matrix;
+typedef struct bg_precond bg_precond;
 
 /* Thread-local description of the last error (replaces ErrExit's message). */
 const char *bg_last_error(void);
@@ -181,6 +182,66 @@ int bg_matrix_convert(const bg_matrix *src, bg_matrix *dst);
 int bg_lu_solve_refined(bg_matrix *A, bg_matrix *F, double *B_host, int nrhs, double tol, int maxit, double *stats);
 int bg_lu_solve_refined_device(bg_matrix *A, bg_matrix *F, void *B_dev, int ldb, int nrhs, double tol, int maxit,
                                double *stats);
+
+/* ---------------------------------------------------------------------------
+ * learned form: GMRES with a sparse near-field preconditioner
+ * (no reference counterpart; the reference solves by LU only)
+ * ------------------------------------------------------------------------- */
+
+/* Diagonal (Jacobi) preconditioner of an assembled complex128 matrix. */
+int bg_precond_create_jacobi(bg_matrix *A, bg_precond **out);
+void bg_precond_destroy(bg_precond *P);
+/* Number of stored entries (complex128) of a preconditioner. */
+int bg_precond_nnz(const bg_precond *P);
+
+/* Restarted GMRES(restart) in FP64 on the device with right preconditioner P
+   (NULL: none) for A X = B; up to 4 right-hand sides advance in lockstep so
+   each step reads A once.  Stops when max_j |b_j - A x_j| / |b_j| <= tol or
+   after maxit matrix-vector steps.  stats (3 doubles, may be NULL): steps,
+   final and initial relative residual.  B: host N x nrhs complex128. */
+int bg_gmres_solve(bg_matrix *A, const bg_precond *P, double *B_host, int nrhs, double tol, int restart, int maxit,
+                   double *stats);
+int bg_gmres_solve_device(bg_matrix *A, const bg_precond *P, void *B_dev, int ldb, int nrhs, double tol, int restart,
+                          int maxit, double *stats);
+
+/* Mixed-precision GMRES: Krylov solves against the complex64 copy F of A
+   (bg_matrix_convert; 8 N^2 bytes per step) to relative residual inner_tol,
+   FP64 iterative refinement with the complex128 A between them, until
+   max_j |b_j - A x_j| / |b_j| <= tol or maxit Krylov steps in total.
+   stats (3 doubles, may be NULL): Krylov steps, final relative residual,
+   refinement sweeps.  P as for bg_gmres_solve (built from A). */
+int bg_gmres_solve_mixed(bg_matrix *A, bg_matrix *F, const bg_precond *P, double *B_host, int nrhs, double tol,
+                         int restart, int maxit, double inner_tol, double *stats);
+int bg_gmres_solve_mixed_device(bg_matrix *A, bg_matrix *F, const bg_precond *P, void *B_dev, int ldb, int nrhs,
+                                double tol, int restart, int maxit, double inner_tol, double *stats);
+
+/* Graph network (3 message-passing layers of width 64 over the near-field
+   pattern of the basis functions) that predicts the entries of a sparse
+   approximate inverse on that pattern.  Parameters live on the device; the
+   untrained network (seeded Glorot weights, zero readout) reproduces Jacobi. */
+typedef struct bg_gnn bg_gnn;
+int bg_gnn_create(unsigned long long seed, bg_gnn **out);
+void bg_gnn_destroy(bg_gnn *net);
+int bg_gnn_num_params(void);
+int bg_gnn_get_params(const bg_gnn *net, float *host);
+int bg_gnn_set_params(bg_gnn *net, const float *host);
+int bg_gnn_get_grads(const bg_gnn *net, float *host);
+/* One Adam step (lr > 0; lr == 0 computes loss and gradients only) on
+   log L, L = |A M Z - Z|_F^2 / (N p) + lambda |M b - x|^2 / |x|^2, for the
+   assembled complex128 matrix A of geometry g at frequency omega.  Z: host
+   N x p complex128 probes (p <= 16), first mapped probe_power times
+   (0..64) through z <- z - A D^{-1} z (D = diag A) and rescaled to
+   |z|^2 = 2N; b, x: host right-hand side and its solution, or NULL.
+   loss: L before the update; the stored gradients (bg_gnn_get_grads) are
+   those of log L. */
+int bg_gnn_train_step(bg_gnn *net, bg_geometry *g, bg_matrix *A, double omega, const double *Z_host, int p,
+                      int probe_power, const double *b_host, const double *x_host, double lambda, double lr,
+                      double *loss);
+/* Preconditioner predicted by the network for the assembled matrix A. */
+int bg_precond_create_learned(bg_geometry *g, bg_matrix *A, double omega, const bg_gnn *net, bg_precond **out);
+/* Copies a preconditioner's CSR (rowptr N+1 ints, col nnz ints, val 2*nnz
+   doubles) to the host; any pointer may be NULL. */
+int bg_precond_download(const bg_precond *P, int *rowptr, int *col, double *val);
 
 /* ---------------------------------------------------------------------------
  * right-hand side and post-processing
