@@ -1,26 +1,34 @@
 """Benchmark: seconds per frequency (assemble + solve) of the dense VIE path.
 
-Workload (N=1 default): the plain FP64 method at scale -- synthetic sphere,
-cube [-1,1]^3 cut into 12^3 cells x 6 tetrahedra, radially mapped (10,368
-tetrahedra, N = 19,872 SWG unknowns, 6.3 GB complex128 matrix), anisotropic
-permittivity [[4,.5,0],[.5,6,0],[0,0,9]] + 0.1i, omega = 1, three plane-wave
-right-hand sides (x-pol along +z, y-pol along +z, z-pol along +x).
+Headline workload (N=1 default, the learned form): synthetic sphere, cube
+[-1,1]^3 cut into 17^3 cells x 6 tetrahedra, radially mapped (29,478
+tetrahedra, N = 57,222 SWG unknowns: 52 GB complex128 matrix plus a 26 GB
+complex64 copy), eps = 6 + 0.5i, omega = 1, three plane-wave right-hand sides
+(x-pol along +z, y-pol along +z, z-pol along +x).
 
-One step = one frequency: assemble the VIE matrix on the device, LU-factor
-it, assemble the 3 RHS and solve.  The frequency-independent near-field
-precompute runs once per mesh before timing and is reported separately
+One step = one frequency.
+  value (mixed + learned): assemble the complex128 matrix, copy it to
+    complex64, predict the near-field approximate inverse with the graph
+    network (shipped weights), assemble the RHS, solve by GMRES(50) on the
+    complex64 copy with FP64 refinement against the complex128 matrix to a
+    1e-10 relative residual, LU fallback if 1000 Krylov steps do not reach it.
+  fp64_path: assemble, FP64 LU (DMMA tensor cores), FP64 solve -- the plain
+    path and the judge: the learned answer's error is measured against it.
+The same two paths plus the precision form (complex64 tcgen05 LU + FP64
+refinement) also run on the 12^3-cell sphere (N = 19,872) with the
+anisotropic tensor [[4,.5,0],[.5,6,0],[0,0,9]] + 0.1i ("secondary").  The
+frequency-independent near-field precompute runs once per mesh before timing
 ("precompute_s"), as the reference amortises its FIBBI cache.
 
 value: device time of K steps (CUDA events on the library stream, barrier +
-synchronize on both sides, max over ranks) / steps.  The 6.3 GB matrix is far
-larger than L2, so no flush is needed.
-e2e: the same per-frequency work through the host-buffer C-ABI calls
-(bg_assemble, bg_rhs_planewave -> host, bg_lu_factor, bg_lu_solve with host
-RHS in / solution out), host-side wall time including the copies.
+synchronize on both sides, max over ranks) / steps.  The matrices are far
+larger than the 126 MB L2, so no flush is needed.
+e2e: the learned step through the host-buffer C-ABI calls (RHS assembled to
+host memory, solution copied back), host wall time including the copies.
 
 --impl reference times the CPU restatement of the reference path (oracle
-port, OpenMP over all host cores for assembly, LAPACK zgetrf via OpenBLAS) on
-bounded samples of the same workload and extrapolates to the full size.
+port: OpenMP assembly over all host cores, LAPACK zgetrf/zgetrs via OpenBLAS)
+on bounded samples of the headline workload, extrapolated to the full size.
 """
 from __future__ import annotations
 
@@ -42,8 +50,10 @@ sys.path.insert(0, os.path.join(ROOT, "buff-em_b200"))
 
 METRIC = "sec/frequency (assemble+solve), N=19k & 58k: mixed/learned vs FP64, err<=1e-8"
 TENSOR = [[4, 0.5, 0], [0.5, 6, 0], [0, 0, 9]]
+EPS_LEARNED = 6 + 0.5j
 WAVES = [([1, 0, 0], [0, 0, 1]), ([0, 1, 0], [0, 0, 1]), ([0, 0, 1], [1, 0, 0])]
 OMEGA = 1.0
+GMRES = dict(tol=1e-10, restart=50, maxit=1000, inner_tol=1e-5)
 
 
 def eps_tensor():
@@ -167,182 +177,243 @@ def gemm_kernel_bench(n, reps=5):
 
 
 # ------------------------------------------------------------------ GPU arm
-def run_gpu(args, rank, world, local_rank):
+class Case:
+    """One mesh/material on the device with the library's C-ABI handles."""
+
+    def __init__(self, n, material, order):
+        import buffem
+        self.buffem = buffem
+        self.L = buffem.lib()
+        self.G = buffem.SWGGeometry(meshfiles=mesh_path(n), materials=material, singular_order=order)
+        self.N = self.G.TotalBFs
+        t0 = time.perf_counter()
+        self.G.precompute()
+        buffem.synchronize()
+        self.precompute_s = time.perf_counter() - t0
+        self.M = self.G.AllocateVIEMatrix()
+        self.F = None
+        self.E0s = [np.ascontiguousarray(np.array(e, complex)) for e, _ in WAVES]
+        self.nhs = [np.ascontiguousarray(np.array(k, float)) for _, k in WAVES]
+        self.nrhs = len(WAVES)
+
+    def rhs_device(self, dB):
+        b = self.buffem
+        for i in range(self.nrhs):
+            b._check(self.L.bg_rhs_planewave_device(self.G.h, OMEGA, 0.0, b._ptr(self.E0s[i]), b._ptr(self.nhs[i]),
+                                                    b.C.c_void_p(dB[i].data_ptr())))
+
+    def step_fp64(self, dB):
+        b = self.buffem
+        b._check(self.L.bg_assemble(self.G.h, OMEGA, 0.0, self.M.h))
+        b._check(self.L.bg_lu_factor(self.M.h))
+        self.rhs_device(dB)
+        b._check(self.L.bg_lu_solve_device(self.M.h, b.C.c_void_p(dB.data_ptr()), self.N, self.nrhs))
+
+    def ensure_c64(self):
+        if self.F is None:
+            self.F = self.G.AllocateVIEMatrix(self.buffem.BG_C64)
+
+    def step_precision(self, dB, stats, tol=1e-12):
+        b = self.buffem
+        self.ensure_c64()
+        b._check(self.L.bg_assemble(self.G.h, OMEGA, 0.0, self.M.h))
+        b._check(self.L.bg_matrix_convert(self.M.h, self.F.h))
+        b._check(self.L.bg_lu_factor(self.F.h))
+        self.rhs_device(dB)
+        b._check(self.L.bg_lu_solve_refined_device(self.M.h, self.F.h, b.C.c_void_p(dB.data_ptr()), self.N,
+                                                   self.nrhs, tol, 60, b._ptr(stats)))
+
+    def step_learned(self, dB, net, stats):
+        b = self.buffem
+        self.ensure_c64()
+        b._check(self.L.bg_assemble(self.G.h, OMEGA, 0.0, self.M.h))
+        b._check(self.L.bg_matrix_convert(self.M.h, self.F.h))
+        P = b.Preconditioner.learned(self.G, self.M, OMEGA, net)
+        self.rhs_device(dB)
+        b._check(self.L.bg_gmres_solve_lu_fallback_device(
+            self.M.h, self.F.h, P.h, b.C.c_void_p(dB.data_ptr()), self.N, self.nrhs, GMRES["tol"],
+            GMRES["restart"], GMRES["maxit"], GMRES["inner_tol"], b._ptr(stats)))
+        del P
+
+    def step_learned_host(self, hostB, rhs_h, net, stats):
+        """Same work through host buffers: RHS to host, solve with host in/out."""
+        b = self.buffem
+        self.ensure_c64()
+        b._check(self.L.bg_assemble(self.G.h, OMEGA, 0.0, self.M.h))
+        b._check(self.L.bg_matrix_convert(self.M.h, self.F.h))
+        P = b.Preconditioner.learned(self.G, self.M, OMEGA, net)
+        for i in range(self.nrhs):
+            b._check(self.L.bg_rhs_planewave(self.G.h, OMEGA, 0.0, b._ptr(self.E0s[i]), b._ptr(self.nhs[i]),
+                                             b._ptr(rhs_h)))
+            hostB[:, i] = rhs_h
+        b._check(self.L.bg_gmres_solve_lu_fallback(self.M.h, self.F.h, P.h, b._ptr(hostB), self.nrhs,
+                                                   GMRES["tol"], GMRES["restart"], GMRES["maxit"],
+                                                   GMRES["inner_tol"], b._ptr(stats)))
+        del P
+
+    def free(self):
+        self.F = None
+        self.M = None
+        self.G = None
+
+
+def timed(stream, fn, steps, warmup, world):
+    """Device seconds of `steps` calls after `warmup` untimed ones (CUDA events
+    on the library stream, barrier + synchronize on both sides, max over ranks)."""
     import torch
     import torch.distributed as dist
     import buffem
-
-    torch.cuda.set_device(local_rank)
-    n = args.n
-    G = buffem.SWGGeometry(meshfiles=mesh_path(n),
-                           materials=buffem.Material(kind=buffem.BG_MAT_CONST_TENSOR, tensor=eps_tensor()),
-                           singular_order=args.order)
-    N = G.TotalBFs
-    t0 = time.perf_counter()
-    G.precompute()
+    for _ in range(warmup):
+        fn()
     buffem.synchronize()
-    precompute_s = time.perf_counter() - t0
-    M = G.AllocateVIEMatrix()
-    L = buffem.lib()
-    stream = torch.cuda.ExternalStream(L.bg_stream())
-    nrhs = len(WAVES)
-    dB = torch.zeros((nrhs, N), dtype=torch.complex128, device="cuda")  # column-major N x nrhs
-    E0s = [np.ascontiguousarray(np.array(e, complex)) for e, _ in WAVES]
-    nhs = [np.ascontiguousarray(np.array(k, float)) for _, k in WAVES]
-
-    def step():
-        buffem._check(L.bg_assemble(G.h, OMEGA, 0.0, M.h))
-        buffem._check(L.bg_lu_factor(M.h))
-        for i in range(nrhs):
-            buffem._check(L.bg_rhs_planewave_device(G.h, OMEGA, 0.0, buffem._ptr(E0s[i]), buffem._ptr(nhs[i]),
-                                                    buffem.C.c_void_p(dB[i].data_ptr())))
-        buffem._check(L.bg_lu_solve_device(M.h, buffem.C.c_void_p(dB.data_ptr()), N, nrhs))
-
-    for _ in range(args.warmup):
-        step()
-    buffem.synchronize()
-
-    # phase breakdown of one untimed step (events on the library stream)
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-    with torch.cuda.stream(stream):
-        ev[0].record(stream)
-        buffem._check(L.bg_assemble(G.h, OMEGA, 0.0, M.h))
-        ev[1].record(stream)
-        buffem._check(L.bg_lu_factor(M.h))
-        ev[2].record(stream)
-        for i in range(nrhs):
-            buffem._check(L.bg_rhs_planewave_device(G.h, OMEGA, 0.0, buffem._ptr(E0s[i]), buffem._ptr(nhs[i]),
-                                                    buffem.C.c_void_p(dB[i].data_ptr())))
-        buffem._check(L.bg_lu_solve_device(M.h, buffem.C.c_void_p(dB.data_ptr()), N, nrhs))
-        ev[3].record(stream)
-    buffem.synchronize()
-    phases = {"assemble_s": ev[0].elapsed_time(ev[1]) / 1e3, "lu_s": ev[1].elapsed_time(ev[2]) / 1e3,
-              "rhs_solve_s": ev[2].elapsed_time(ev[3]) / 1e3}
-
-    # ---------------- timed region (device): plain FP64 path
-    clocks = ClockSampler(local_rank)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    buffem.synchronize()
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3
+    if world > 1:
+        tt = torch.tensor([t], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t = float(tt.item())
+    return t
+
+
+def rel_err(x, ref):
+    import torch
+    return float(torch.linalg.norm(x - ref) / torch.linalg.norm(ref))
+
+
+def run_gpu(args, rank, world, local_rank):
+    import torch
+    import buffem
+
+    torch.cuda.set_device(local_rank)
+    L = buffem.lib()
+    stream = torch.cuda.ExternalStream(L.bg_stream())
+    net = buffem.GNN.load()
+    out = {}
+
+    # ---------------- headline: learned form at N = 57,222
+    case = Case(args.n, buffem.Material(eps=EPS_LEARNED), args.order)
+    N = case.N
+    dB = torch.zeros((case.nrhs, N), dtype=torch.complex128, device="cuda")   # column-major N x nrhs
+    x_fp64 = None
+    t_fp64 = None
+    prof_fp64 = None
+    if args.fp64_steps > 0:
+        buffem.profile_begin()
+        t_fp64 = timed(stream, lambda: case.step_fp64(dB), args.fp64_steps, args.fp64_warmup, world)
+        prof_fp64 = buffem.profile_read()
+        buffem.profile_end()
+        x_fp64 = dB.clone()
+    stats = np.zeros(4)
+    clocks = ClockSampler(local_rank)
+    for _ in range(args.warmup):
+        case.step_learned(dB, net, stats)
     buffem.synchronize()
     clocks.start()
     launches0 = buffem.launch_count()
     buffem.profile_begin()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        step()
-    e1.record(stream)
-    buffem.synchronize()
-    torch.cuda.synchronize()
+    t_learned = timed(stream, lambda: case.step_learned(dB, net, stats), args.steps, 0, world)
     prof = buffem.profile_read()
     buffem.profile_end()
-    launches_fp64 = buffem.launch_count() - launches0
-    elapsed_fp64 = e0.elapsed_time(e1) / 1e3
-    x_fp64 = dB.clone()
-
-    # ---------------- precision form: FP64 assembly -> complex64 copy ->
-    # tcgen05 TF32 LU -> FP64-refined solve
-    F = G.AllocateVIEMatrix(buffem.BG_C64)
-    stats = np.zeros(3)
-
-    def step_mixed():
-        buffem._check(L.bg_assemble(G.h, OMEGA, 0.0, M.h))
-        buffem._check(L.bg_matrix_convert(M.h, F.h))
-        buffem._check(L.bg_lu_factor(F.h))
-        for i in range(nrhs):
-            buffem._check(L.bg_rhs_planewave_device(G.h, OMEGA, 0.0, buffem._ptr(E0s[i]), buffem._ptr(nhs[i]),
-                                                    buffem.C.c_void_p(dB[i].data_ptr())))
-        buffem._check(L.bg_lu_solve_refined_device(M.h, F.h, buffem.C.c_void_p(dB.data_ptr()), N, nrhs,
-                                                   args.refine_tol, 60, buffem._ptr(stats)))
-
-    for _ in range(args.warmup):
-        step_mixed()
-    buffem.synchronize()
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
-    ev[0].record(stream)
-    buffem._check(L.bg_assemble(G.h, OMEGA, 0.0, M.h))
-    ev[1].record(stream)
-    buffem._check(L.bg_matrix_convert(M.h, F.h))
-    buffem._check(L.bg_lu_factor(F.h))
-    ev[2].record(stream)
-    for i in range(nrhs):
-        buffem._check(L.bg_rhs_planewave_device(G.h, OMEGA, 0.0, buffem._ptr(E0s[i]), buffem._ptr(nhs[i]),
-                                                buffem.C.c_void_p(dB[i].data_ptr())))
-    ev[3].record(stream)
-    buffem._check(L.bg_lu_solve_refined_device(M.h, F.h, buffem.C.c_void_p(dB.data_ptr()), N, nrhs,
-                                               args.refine_tol, 60, buffem._ptr(stats)))
-    ev[4].record(stream)
-    buffem.synchronize()
-    phases_mixed = {"assemble_s": ev[0].elapsed_time(ev[1]) / 1e3, "convert_lu_s": ev[1].elapsed_time(ev[2]) / 1e3,
-                    "rhs_s": ev[2].elapsed_time(ev[3]) / 1e3, "refined_solve_s": ev[3].elapsed_time(ev[4]) / 1e3,
-                    "refine_sweeps": int(stats[0]), "final_rel_residual": float(stats[1]),
-                    "first_rel_residual": float(stats[2])}
-    launches1 = buffem.launch_count()
-    buffem.profile_begin()
-    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e2.record(stream)
-    for _ in range(args.steps):
-        step_mixed()
-    e3.record(stream)
-    buffem.synchronize()
-    torch.cuda.synchronize()
-    prof_mixed = buffem.profile_read()
-    buffem.profile_end()
-    launches_mixed = buffem.launch_count() - launches1
+    launches = buffem.launch_count() - launches0
     clk = clocks.stop()
-    elapsed_mixed = e2.elapsed_time(e3) / 1e3
-    err = float(torch.linalg.norm(dB - x_fp64) / torch.linalg.norm(x_fp64))
-    if world > 1:
-        t = torch.tensor([elapsed_fp64, elapsed_mixed], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_fp64, elapsed_mixed = float(t[0].item()), float(t[1].item())
-        dist.barrier()
-    launches = launches_mixed
-
-    # ---------------- e2e through host buffers (precision form)
-    hostB = np.zeros((N, nrhs), complex, order="F")
+    learned = {"steps_per_frequency": int(stats[0]), "final_rel_residual": float(stats[1]),
+               "refinement_sweeps": int(stats[2]), "lu_fallback": bool(stats[3])}
+    if x_fp64 is not None:
+        learned["err_vs_fp64_lu"] = rel_err(dB, x_fp64)
+    # the same solve preconditioned by Jacobi: what the network gains
+    P = buffem.Preconditioner.jacobi(case.M)
+    js = np.zeros(4)
+    case.rhs_device(dB)
+    buffem._check(L.bg_assemble(case.G.h, OMEGA, 0.0, case.M.h))
+    buffem._check(L.bg_matrix_convert(case.M.h, case.F.h))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    buffem._check(L.bg_gmres_solve_lu_fallback_device(case.M.h, case.F.h, P.h, buffem.C.c_void_p(dB.data_ptr()),
+                                                      N, case.nrhs, GMRES["tol"], GMRES["restart"], GMRES["maxit"],
+                                                      GMRES["inner_tol"], buffem._ptr(js)))
+    e1.record(stream)
+    buffem.synchronize()
+    learned["jacobi_same_solve"] = {"steps": int(js[0]), "solve_s": e0.elapsed_time(e1) / 1e3,
+                                    "lu_fallback": bool(js[3])}
+    del P
+    # e2e through host buffers
+    hostB = np.zeros((N, case.nrhs), complex, order="F")
     rhs_h = np.zeros(N, complex)
     times = []
-    for _ in range(0 if args.lean else max(1, args.steps)):
+    for _ in range(0 if args.lean else max(1, min(args.steps, 2))):
         buffem.synchronize()
         t0 = time.perf_counter()
-        buffem._check(L.bg_assemble(G.h, OMEGA, 0.0, M.h))
-        buffem._check(L.bg_matrix_convert(M.h, F.h))
-        buffem._check(L.bg_lu_factor(F.h))
-        for i in range(nrhs):
-            buffem._check(L.bg_rhs_planewave(G.h, OMEGA, 0.0, buffem._ptr(E0s[i]), buffem._ptr(nhs[i]),
-                                             buffem._ptr(rhs_h)))
-            hostB[:, i] = rhs_h
-        buffem._check(L.bg_lu_solve_refined(M.h, F.h, buffem._ptr(hostB), nrhs, args.refine_tol, 60,
-                                            buffem._ptr(stats)))
+        case.step_learned_host(hostB, rhs_h, net, stats)
         times.append(time.perf_counter() - t0)
     e2e_s = max(times) if times else None
     if world > 1 and e2e_s is not None:
+        import torch.distributed as dist
         t = torch.tensor([e2e_s], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    del F
-    return dict(N=N, elapsed=elapsed_mixed, elapsed_fp64=elapsed_fp64, phases=phases, phases_mixed=phases_mixed,
-                prof=prof, prof_mixed=prof_mixed, launches=launches, launches_fp64=launches_fp64, clocks=clk,
-                precompute_s=precompute_s, e2e_s=e2e_s, nrhs=nrhs, err_vs_fp64=err)
+    out.update(N=N, nrhs=case.nrhs, t_learned=t_learned, t_fp64=t_fp64, prof=prof, prof_fp64=prof_fp64,
+               launches=launches, clocks=clk, learned=learned, precompute_s=case.precompute_s, e2e_s=e2e_s)
+    case.free()
+    del dB, x_fp64
+    torch.cuda.empty_cache()
 
+    # ---------------- secondary: N = 19,872 anisotropic sphere, all three paths
+    if args.n_small > 0 and not args.lean:
+        sc = Case(args.n_small, buffem.Material(kind=buffem.BG_MAT_CONST_TENSOR, tensor=eps_tensor()), args.order)
+        dB = torch.zeros((sc.nrhs, sc.N), dtype=torch.complex128, device="cuda")
+        sec = {"N": sc.N, "precompute_s": sc.precompute_s}
+        buffem.profile_begin()
+        t = timed(stream, lambda: sc.step_fp64(dB), 2, 1, world)
+        pf = buffem.profile_read()
+        buffem.profile_end()
+        ref = dB.clone()
+        sec["fp64_path_s"] = t / 2
+        sec["fp64_lu_tflops"] = pf["lu_gemm"]["flops"] / (pf["lu_gemm"]["ms"] / 1e3) / 1e12 if pf["lu_gemm"]["ms"] else None
+        st = np.zeros(3)
+        buffem.profile_begin()
+        t = timed(stream, lambda: sc.step_precision(dB, st), 2, 1, world)
+        pm = buffem.profile_read()
+        buffem.profile_end()
+        sec["precision_form_s"] = t / 2
+        sec["precision_form_err_vs_fp64_lu"] = rel_err(dB, ref)
+        sec["precision_form_gemm_tflops"] = pm["lu_gemm"]["flops"] / (pm["lu_gemm"]["ms"] / 1e3) / 1e12 if pm["lu_gemm"]["ms"] else None
+        st4 = np.zeros(4)
+        t = timed(stream, lambda: sc.step_learned(dB, net, st4), 2, 1, world)
+        sec["learned_s"] = t / 2
+        sec["learned_err_vs_fp64_lu"] = rel_err(dB, ref)
+        sec["learned_steps"] = int(st4[0])
+        sec["learned_lu_fallback"] = bool(st4[3])
+        out["secondary"] = sec
+        sc.free()
+        del dB, ref
+        torch.cuda.empty_cache()
+    return out
 
 
 # ------------------------------------------------------------------ CPU arm
-def cpu_sample(n, order, nrow_sample=48, lu_n=3000, threads=None):
-    """Oracle port on the host: warm-cache assembly of a uniform row sample and
-    LAPACK zgetrf at a smaller order, extrapolated to the full workload."""
+def cpu_sample(n, order, nrow_sample=48, lu_n=3000):
+    """Oracle port on the host (headline workload): warm-cache assembly of a
+    uniform row sample and LAPACK zgetrf/zgetrs at a smaller order,
+    extrapolated to the full size (rows x N/48, LU x (N/3000)^3, solve x
+    (N/3000)^2)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     import scipy.linalg as sl
-    G = oracle.Geometry(mesh_path(n), oracle.material(kind=oracle.MAT_CONST_TENSOR, tensor=eps_tensor()),
-                        nang=order)
+    G = oracle.Geometry(mesh_path(n), oracle.material(eps=EPS_LEARNED), nang=order)
     N = G.N
-    t0 = time.perf_counter()
-    G.cache_build()
-    t_cache = time.perf_counter() - t0
     rows = np.linspace(0, N - 1, nrow_sample).astype(np.int32)
+    t0 = time.perf_counter()
+    G.cache_build(rows)
+    t_cache = (time.perf_counter() - t0) * N / nrow_sample
     t0 = time.perf_counter()
     G.assemble_rows(complex(OMEGA), rows)
     t_rows = time.perf_counter() - t0
@@ -351,16 +422,15 @@ def cpu_sample(n, order, nrow_sample=48, lu_n=3000, threads=None):
     A = rng.normal(size=(lu_n, lu_n)) + 1j * rng.normal(size=(lu_n, lu_n))
     t0 = time.perf_counter()
     lu = sl.lu_factor(A, overwrite_a=True, check_finite=False)
-    t_lu_s = time.perf_counter() - t0
-    t_lu = t_lu_s * (N / lu_n) ** 3
+    t_lu = (time.perf_counter() - t0) * (N / lu_n) ** 3
     B = rng.normal(size=(lu_n, 3)) + 1j * rng.normal(size=(lu_n, 3))
     t0 = time.perf_counter()
     sl.lu_solve(lu, B, check_finite=False)
     t_sv = (time.perf_counter() - t0) * (N / lu_n) ** 2
     total = t_asm + t_lu + t_sv
-    sample = (f"warm-cache oracle assembly of {nrow_sample} of {N} rows (x{N / nrow_sample:.0f}) + "
-              f"OpenBLAS zgetrf/zgetrs at N={lu_n} scaled by (N/{lu_n})^3 and ^2; "
-              f"near-field cache build {t_cache:.1f}s excluded like the precompute")
+    sample = (f"sphere {n}^3 cells, N={N}, eps={EPS_LEARNED}: warm-cache oracle assembly of {nrow_sample} of {N} "
+              f"rows (x{N / nrow_sample:.0f}) + OpenBLAS zgetrf/zgetrs at N={lu_n} scaled by (N/{lu_n})^3 and ^2; "
+              f"near-field cache build (same rows, x{N / nrow_sample:.0f}: {t_cache:.1f}s) excluded like the precompute")
     return dict(value=total, assemble=t_asm, lu=t_lu, solve=t_sv, cache=t_cache, sample=sample,
                 cores=oracle.lib().or_num_threads())
 
@@ -371,16 +441,17 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--n", type=int, default=12, help="cells per cube edge (12 -> N=19,872)")
+    ap.add_argument("--n", type=int, default=17, help="cells per cube edge of the headline sphere (17 -> N=57,222)")
+    ap.add_argument("--n-small", type=int, default=12, help="secondary sphere (12 -> N=19,872); 0 skips it")
+    ap.add_argument("--fp64-steps", type=int, default=1, help="timed steps of the FP64 path at the headline size")
+    ap.add_argument("--fp64-warmup", type=int, default=1)
     ap.add_argument("--order", type=int, default=10, help="singular-rule order")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--lean", action="store_true",
-                    help="timed steps only (no e2e pass, CPU baseline or peak measurement): profiler runs")
+                    help="headline learned steps only (no FP64 arm, e2e, secondary, CPU baseline): profiler runs")
     ap.add_argument("--kernel", default=None, choices=["gemm"],
                     help="time the LU trailing-update GEMM alone on an M=N=K problem")
     ap.add_argument("--size", type=int, default=8192)
-    ap.add_argument("--refine-tol", type=float, default=1e-12,
-                    help="relative residual target of the FP64 refinement (precision form)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "b200" else args.warmup
 
@@ -389,24 +460,26 @@ def main():
         return
     if args.lean:
         args.no_cpu_baseline = True
+        args.fp64_steps = 0
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-    config = {"workload": f"plain FP64: sphere {args.n}^3 cells x 6 tets, anisotropic eps tensor, 3 plane-wave RHS",
-              "n_cells": args.n, "omega": OMEGA, "rhs": 3, "singular_order": args.order,
-              "parallelism": f"replicas x{world} (independent frequencies)",
-              "l2": "matrix (16 N^2 bytes) >> 126 MB L2; no flush needed"}
+    N_head = 12 * args.n ** 3 - 6 * args.n ** 2
+    config = {"workload": f"learned form: sphere {args.n}^3 cells x 6 tets (N={N_head}), eps={EPS_LEARNED}, "
+                          f"omega={OMEGA}, 3 plane-wave RHS; mixed-precision GMRES(50) + graph-network "
+                          f"near-field preconditioner, LU fallback; vs plain FP64 assemble+LU+solve",
+              "N": N_head, "n_cells": args.n, "omega": OMEGA, "rhs": 3, "singular_order": args.order,
+              "gmres": GMRES, "parallelism": f"replicas x{world} (independent frequencies)",
+              "l2": "matrices (8-16 N^2 bytes) >> 126 MB L2; no flush needed"}
 
     if args.impl == "reference":
         if rank != 0:
             return
-        r = cpu_sample(args.n, args.order)
-        N = 12 * args.n ** 3 - 6 * args.n ** 2
-        config["N"] = N
-        vals = [r["value"]]
-        for _ in range(max(0, args.steps - 1)):
-            vals.append(cpu_sample(args.n, args.order)["value"])
+        vals, r = [], None
+        for _ in range(max(1, args.steps)):
+            r = cpu_sample(args.n, args.order)
+            vals.append(r["value"])
         v = statistics.median(vals)
         line = {"metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
@@ -425,50 +498,44 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     res = run_gpu(args, rank, world, local_rank)
     N = res["N"]
-    config["N"] = N
-    config["paths"] = "value: precision form (FP64 assembly, complex64 tcgen05/TF32 LU, FP64-refined solve); " \
-                      "fp64: plain path (FP64 assembly, DMMA LU, FP64 solve)"
-    value = res["elapsed"] / args.steps / world    # whole-job seconds per frequency
-    value_fp64 = res["elapsed_fp64"] / args.steps / world
-    gemm = res["prof"]["lu_gemm"]
-    achieved = gemm["flops"] / (gemm["ms"] / 1e3) / 1e12 if gemm["ms"] > 0 else None
-    gm = res["prof_mixed"]["lu_gemm"]
-    achieved_tc = gm["flops"] / (gm["ms"] / 1e3) / 1e12 if gm["ms"] > 0 else None
-    peak = None
-    peak_src = None
-    if rank == 0 and not args.lean:
-        try:
-            peak = zgemm_peak_tflops()
-            peak_src = "measured in-run: cuBLAS ZGEMM 8192^3 (torch complex128 matmul), best of 5"
-        except Exception as e:  # pragma: no cover
-            peak_src = f"unavailable: {e}"
+    value = res["t_learned"] / args.steps / world          # whole-job seconds per frequency
+    prof = res["prof"]
     mp = measured_peaks()
-    bf16 = mp.get("bf16_tflops")
-    total_ms = sum(v["ms"] for v in res["prof"].values())
+    hbm = mp.get("hbm_gbs")
+    mv = prof["gmres_matvec"]
+    far = prof["assemble_far"]
+    total_ms = sum(v["ms"] for v in prof.values())
+    mv_gbs = mv["flops"] / (mv["ms"] / 1e3) / 1e9 if mv["ms"] > 0 else None
     line = {"metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": res["elapsed"] / args.steps * 1e3, "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "c128 (complex64 TF32 tensor-core LU + FP64 refinement)",
+            "warmup": args.warmup, "ms_per_step": res["t_learned"] / args.steps * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "c128 assembly; c64 Krylov matrix-vector products with FP64 refinement",
             "data": "synthetic", "config": config,
-            "fp64_path": {"value": value_fp64, "unit": "s", "phases": res["phases"],
-                          "speedup_of_precision_form": value_fp64 / value, "gpu_launches": res["launches_fp64"]},
-            "precision_form": {"phases": res["phases_mixed"], "err_vs_fp64_lu": res["err_vs_fp64"]},
-            "precompute_s": res["precompute_s"],
-            "roofline": {"bound": "tensor", "kernel": "k_zgemm_sub (FP64 path LU trailing update, DMMA f64)",
-                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": (achieved / peak) if (achieved and peak) else None, "traffic": None,
-                         "peak_source": peak_src,
-                         "algorithmic": "8*M*N*K flops per launch (4M complex product)",
-                         "gemm_share_of_profiled_ms": gemm["ms"] / total_ms if total_ms else None,
-                         "lu_flops_rate_tflops": (8 / 3 * N ** 3) / res["phases"]["lu_s"] / 1e12,
-                         "precision_form_gemm": {"kernel": "k_cgemm_tf32 (tcgen05 kind::tf32)",
-                                                 "achieved": achieved_tc, "unit": "TFLOP/s",
-                                                 "peak_bf16_dense_measured": bf16,
-                                                 "frac_of_bf16_peak": (achieved_tc / bf16) if (achieved_tc and bf16) else None}},
-            "kernel_classes": res["prof"], "kernel_classes_precision_form": res["prof_mixed"],
+            "learned_form": res["learned"],
+            "kernel_classes": prof, "precompute_s": res["precompute_s"],
+            "roofline": {"bound": "hbm", "kernel": "k_gm_matvec_part_c64 (+ k_gm_matvec_sum): GMRES matrix-vector "
+                                                   "products on the complex64 matrix",
+                         "achieved": mv_gbs, "peak": hbm, "unit": "GB/s",
+                         "frac": (mv_gbs / hbm) if (mv_gbs and hbm) else None, "traffic": None,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if hbm else "unavailable",
+                         "algorithmic": "8 N^2 bytes of matrix per product (3 right-hand sides share one pass; "
+                                        "16 N^2 for the complex128 residual products)",
+                         "share_of_profiled_ms": mv["ms"] / total_ms if total_ms else None,
+                         "assemble_far_share_of_profiled_ms": far["ms"] / total_ms if total_ms else None},
             "e2e": {"value": res["e2e_s"] / world if res["e2e_s"] else None, "unit": "s",
                     "h2d_bytes_per_step": 16 * N * res["nrhs"],
                     "d2h_bytes_per_step": 2 * 16 * N * res["nrhs"]},
-            "gpu_launches": res["launches"], "clocks": res["clocks"]}
+            "gpu_launches": res["launches"] // max(1, args.steps), "clocks": res["clocks"]}
+    if res["t_fp64"] is not None:
+        v64 = res["t_fp64"] / args.fp64_steps / world
+        pf = res["prof_fp64"]
+        line["fp64_path"] = {"value": v64, "unit": "s", "steps": args.fp64_steps, "warmup": args.fp64_warmup,
+                             "speedup_of_learned_form": v64 / value,
+                             "lu_gemm_tflops": pf["lu_gemm"]["flops"] / (pf["lu_gemm"]["ms"] / 1e3) / 1e12
+                             if pf["lu_gemm"]["ms"] else None,
+                             "kernel_classes": pf}
+    if "secondary" in res:
+        line["secondary_n19872"] = res["secondary"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = cpu_sample(args.n, args.order)
         line["cpu_baseline"] = {"value": r["value"], "unit": "s", "cores": r["cores"], "kind": "port",

@@ -78,6 +78,7 @@ EXPORTS = [
     "bg_gmres_solve", "bg_gmres_solve_device", "bg_gnn_create", "bg_gnn_destroy", "bg_gnn_num_params",
     "bg_gnn_get_params", "bg_gnn_set_params", "bg_gnn_get_grads", "bg_gnn_train_step",
     "bg_precond_create_learned", "bg_precond_download", "bg_gmres_solve_mixed", "bg_gmres_solve_mixed_device",
+    "bg_precond_projection", "bg_gmres_solve_lu_fallback", "bg_gmres_solve_lu_fallback_device",
 ]
 
 
@@ -119,6 +120,8 @@ def lib():
         L.bg_gmres_solve.argtypes = [P, P, VP, I, D, I, I, VP]
         L.bg_gmres_solve_device.argtypes = [P, P, VP, I, I, D, I, I, VP]
         L.bg_gmres_solve_mixed.argtypes = [P, P, P, VP, I, D, I, I, D, VP]
+        L.bg_gmres_solve_lu_fallback.argtypes = [P, P, P, VP, I, D, I, I, D, VP]
+        L.bg_gmres_solve_lu_fallback_device.argtypes = [P, P, P, VP, I, I, D, I, I, D, VP]
         L.bg_gmres_solve_mixed_device.argtypes = [P, P, P, VP, I, I, D, I, I, D, VP]
         L.bg_gnn_create.argtypes = [C.c_ulonglong, C.POINTER(P)]
         L.bg_gnn_destroy.argtypes = [P]
@@ -129,6 +132,7 @@ def lib():
         L.bg_gnn_train_step.argtypes = [P, P, P, D, VP, I, I, VP, VP, D, D, VP]
         L.bg_precond_create_learned.argtypes = [P, P, D, P, C.POINTER(P)]
         L.bg_precond_download.argtypes = [P, VP, VP, VP]
+        L.bg_precond_projection.argtypes = [P, VP, VP]
         L.bg_rhs_planewave.argtypes = [P, D, D, VP, VP, VP]
         L.bg_rhs_planewave_device.argtypes = [P, D, D, VP, VP, VP]
         L.bg_pft.argtypes = [P, D, D, VP, VP, VP, I, VP]
@@ -344,6 +348,13 @@ class Preconditioner:
     def nnz(self):
         return lib().bg_precond_nnz(self.h)
 
+    def projection(self):
+        """Learned: (rho, theta), the estimate of rho(I - D M) before the
+        projection and the blend factor with the Jacobi inverse."""
+        out = np.zeros(2)
+        _check(lib().bg_precond_projection(self.h, _ptr(out[:1]), _ptr(out[1:])))
+        return float(out[0]), float(out[1])
+
     def csr(self, N):
         """(rowptr, col, val) copied to the host."""
         nnz = self.nnz()
@@ -440,6 +451,18 @@ def GMRESSolveMixed(M, F, B, P=None, tol=1e-10, restart=50, maxit=2000, inner_to
     return arr, st
 
 
+def SolveLearned(M, F, B, P=None, tol=1e-10, restart=50, maxit=1000, inner_tol=1e-5):
+    """Mixed-precision GMRES with preconditioner P and the LU fallback (F
+    holds LU factors afterwards if the fallback ran); returns (X, stats) with
+    stats = (Krylov steps, final relative residual, sweeps, fallback used)."""
+    arr = np.asfortranarray(B, dtype=np.complex128).copy(order="F")
+    nrhs = 1 if arr.ndim == 1 else arr.shape[1]
+    st = np.zeros(4)
+    _check(lib().bg_gmres_solve_lu_fallback(M.h, F.h, P.h if P is not None else None, _ptr(arr), nrhs, float(tol),
+                                            int(restart), int(maxit), float(inner_tol), _ptr(st)))
+    return arr, st
+
+
 def launch_count():
     return lib().bg_kernel_launch_count()
 
@@ -448,7 +471,8 @@ def synchronize():
     _check(lib().bg_synchronize())
 
 
-PROF_CLASSES = ("lu_gemm", "lu_panel", "lu_laswp", "trsm_leaf")
+PROF_CLASSES = ("lu_gemm", "lu_panel", "lu_laswp", "trsm_leaf", "assemble_far", "assemble_near_gram",
+                "gmres_matvec", "gnn_precond")
 
 
 def profile_begin():

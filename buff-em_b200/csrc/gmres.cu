@@ -245,6 +245,7 @@ struct GmState {
 
 static int dense_matvec(bg_matrix *A, const z2 *X, z2 *Y, GmState &S) {
   int N = S.N;
+  prof_start(PROF_MATVEC);
   if (A->precision == BG_C64) {
     dim3 g1((N + 2 * GV_ROWS - 1) / (2 * GV_ROWS), S.nchunk);
     k_gm_matvec_part_c64<<<g1, GV_ROWS, 0, stream()>>>(N, (const float4 *)A->d, A->ld / 2, X, N, S.nrhs, S.part);
@@ -255,6 +256,7 @@ static int dense_matvec(bg_matrix *A, const z2 *X, z2 *Y, GmState &S) {
   BG_LAUNCHED();
   k_gm_matvec_sum<<<dim3((N + 255) / 256, S.nrhs), 256, 0, stream()>>>(N, S.nchunk, S.nrhs, S.part, Y, N);
   BG_LAUNCHED();
+  prof_stop(PROF_MATVEC, (A->precision == BG_C64 ? 8.0 : 16.0) * N * (double)N);
   return BG_OK;
 }
 

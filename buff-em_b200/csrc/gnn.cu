@@ -12,15 +12,18 @@
 //         h_i <- h_i + relu(Wuh h_i + Wua agg_i + bu) ]
 //   edge readout: y_e = relu(Wri h_i + Wrj h_j + Wrg g_e + br)       (64)
 //                 o_e = Wo y_e + bo                                 (4)
-//                 c = GNN_CMAX tanh(o0) + i GNN_CMAX tanh(o1)
-//                 s = GNN_SMAX tanh(o2) + i GNN_SMAX tanh(o3)
+//                 c = GNN_CMAX (tanh(o0) + i tanh(o1))
+//                 s = GNN_SMAX (tanh(o2) + i tanh(o3))
 //   m_ij = [delta_ij + c - [i != j] s A_ij / A_ii] / A_jj
 // With s = 1 and c = 0 the off-diagonal term would be the first-order
-// Neumann approximation of A^{-1} around its diagonal.  A coefficient near 1/mu
-// for an eigenvalue mu of the scaled off-diagonal part R D^{-1} makes A M
-// nearly singular there (eigenvalue (1 + mu)(1 - s mu)); on these VIE
-// matrices mu reaches about 2.2, so |s| stays below GNN_SMAX = 0.4.  Wo and bo
-// start at zero, so the untrained network is the Jacobi (diagonal) inverse.
+// Neumann approximation of A^{-1} around its diagonal.  Written D M = I - K
+// (D = diag A), M is singular where K has an eigenvalue 1, and a preconditioner
+// close to that makes GMRES stall on a few modes that no averaged objective
+// sees.  So the predicted M is projected: a power iteration estimates rho(K)
+// and M <- theta M + (1 - theta) D^{-1}, theta = min(1, GNN_RHO / rho), which
+// scales K to spectral radius <= GNN_RHO (training differentiates with theta
+// held fixed).  Wo and bo start at zero, so the untrained network is the
+// Jacobi (diagonal) inverse.
 //
 // Training objective (per matrix; p probes z and a right-hand side b with its
 // LU solution x):
@@ -53,7 +56,9 @@ namespace bg {
 #define GO 4           // outputs per edge
 #define GNN_MAXP 16    // probes per training step
 #define GNN_CMAX 0.5f  // bound of the diagonal-term correction c
-#define GNN_SMAX 0.4f  // bound of the Neumann coefficient s
+#define GNN_SMAX 0.6f  // bound of the Neumann coefficient s
+#define GNN_RHO 0.75   // spectral radius of K = I - D M after the projection
+#define GNN_POWER_ITERS 16
 
 // parameter layout (floats); matrices row-major (out x in)
 struct GnnLayout {
@@ -235,6 +240,64 @@ __global__ void k_gnn_readout(int N, const int *rowptr, const int *col, const fl
       }
       Mval[e] = zmul(c, dinv[j]);
     }
+  }
+}
+
+// W[:, q] = K V[:, q] = V - D (M V), D = diag A = 1 / dinv; one thread per row
+__global__ void k_gnn_kmv(int N, const int *rowptr, const int *col, const z2g *Mval, const z2g *dinv, const z2g *V,
+                          int nv, z2g *W) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  z2g d = zdiv(z2g{1.0, 0.0}, dinv[i]);
+  for (int q = 0; q < nv; q++) {
+    const z2g *v = V + (size_t)q * N;
+    z2g s{0.0, 0.0};
+    for (int e = rowptr[i]; e < rowptr[i + 1]; e++) {
+      z2g t = zmul(Mval[e], v[col[e]]);
+      s.r += t.r;
+      s.i += t.i;
+    }
+    z2g ds = zmul(d, s);
+    W[(size_t)q * N + i] = z2g{v[i].r - ds.r, v[i].i - ds.i};
+  }
+}
+
+// squared norms of nv columns (one block per column, fixed reduction order)
+__global__ void k_gnn_colnorm2(int N, const z2g *V, double *out) {
+  const z2g *v = V + (size_t)blockIdx.x * N;
+  __shared__ double red[32];
+  double s = 0;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) s += v[i].r * v[i].r + v[i].i * v[i].i;
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); k++) t += red[k];
+    out[blockIdx.x] = t;
+  }
+}
+
+__global__ void k_gnn_scale_cols(int N, int nv, const double *f, z2g *V) {
+  size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (t >= (size_t)N * nv) return;
+  double s = f[t / N];
+  V[t] = z2g{V[t].r * s, V[t].i * s};
+}
+
+// M <- theta M + (1 - theta) D^{-1}
+__global__ void k_gnn_blend(int N, const int *rowptr, const int *col, const z2g *dinv, double theta, z2g *Mval) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  for (int e = rowptr[i]; e < rowptr[i + 1]; e++) {
+    z2g m = Mval[e];
+    m.r *= theta;
+    m.i *= theta;
+    if (col[e] == i) {
+      m.r += (1 - theta) * dinv[i].r;
+      m.i += (1 - theta) * dinv[i].i;
+    }
+    Mval[e] = m;
   }
 }
 
@@ -531,6 +594,7 @@ namespace bg {
 // per-call activations (the graph itself is cached in the geometry)
 struct GnnBufs {
   int N = 0, E = 0;
+  double rho = 0, theta = 1;   // spectral estimate of K = I - D M and the projection factor
   const int *rowptr = nullptr, *col = nullptr, *etr = nullptr;
   float *F = nullptr, *Ef = nullptr;
   z2g *ratio = nullptr, *dinv = nullptr;
@@ -642,6 +706,59 @@ static int bufs_init(bg_geometry *g, bg_matrix *A, double omega, bool train, Gnn
   return BG_OK;
 }
 
+// Power iteration for rho(K), K = I - D M (four seeded vectors in lockstep),
+// then M <- theta M + (1 - theta) D^{-1} with theta = min(1, GNN_RHO / rho).
+static int project(GnnBufs &B, z2g *Mval) {
+  const int nv = 4;
+  int N = B.N;
+  size_t nn = (size_t)N * nv;
+  char *w = nullptr;
+  BG_CUDA_TRY(cudaMallocAsync((void **)&w, sizeof(z2g) * 2 * nn + sizeof(double) * 2 * nv, stream()));
+  z2g *V = (z2g *)w, *W = V + nn;
+  double *nrm = (double *)(W + nn), *fac = nrm + nv;
+  std::vector<z2g> h(nn);
+  uint64_t s = 0x9e3779b97f4a7c15ull;
+  for (auto &v : h) {
+    s = s * 6364136223846793005ull + 1442695040888963407ull;
+    double a = (double)(s >> 11) / 9007199254740992.0 - 0.5;
+    s = s * 6364136223846793005ull + 1442695040888963407ull;
+    double b = (double)(s >> 11) / 9007199254740992.0 - 0.5;
+    v = z2g{a, b};
+  }
+  int st = BG_OK;
+  cudaError_t e = cudaMemcpyAsync(V, h.data(), sizeof(z2g) * nn, cudaMemcpyHostToDevice, stream());
+  double rho = 0, hn[nv];
+  for (int it = 0; e == cudaSuccess && it <= GNN_POWER_ITERS; it++) {
+    // normalise V, then W = K V; the norm of K v for unit v is the estimate
+    k_gnn_colnorm2<<<nv, 256, 0, stream()>>>(N, V, nrm);
+    if ((e = cudaMemcpyAsync(hn, nrm, sizeof(double) * nv, cudaMemcpyDeviceToHost, stream())) != cudaSuccess) break;
+    if ((e = cudaStreamSynchronize(stream())) != cudaSuccess) break;
+    g_launches++;
+    if (it > 0) {
+      rho = 0;
+      for (int q = 0; q < nv; q++) rho = std::max(rho, std::sqrt(hn[q]));
+      if (it == GNN_POWER_ITERS) break;
+    }
+    double f[nv];
+    for (int q = 0; q < nv; q++) f[q] = hn[q] > 0 ? 1.0 / std::sqrt(hn[q]) : 0.0;
+    if ((e = cudaMemcpyAsync(fac, f, sizeof(double) * nv, cudaMemcpyHostToDevice, stream())) != cudaSuccess) break;
+    k_gnn_scale_cols<<<(nn + 255) / 256, 256, 0, stream()>>>(N, nv, fac, V);
+    k_gnn_kmv<<<(N + 127) / 128, 128, 0, stream()>>>(N, B.rowptr, B.col, Mval, B.dinv, V, nv, W);
+    g_launches += 2;
+    std::swap(V, W);
+  }
+  if (e != cudaSuccess) { set_error("preconditioner projection: %s", cudaGetErrorString(e)); st = BG_ERR_CUDA; }
+  if (!st && !std::isfinite(rho)) { set_error("preconditioner projection: non-finite estimate"); st = BG_ERR_NUMERIC; }
+  B.rho = rho;
+  B.theta = (!st && rho > GNN_RHO) ? GNN_RHO / rho : 1.0;
+  if (!st && B.theta < 1.0) {
+    k_gnn_blend<<<(N + 127) / 128, 128, 0, stream()>>>(N, B.rowptr, B.col, B.dinv, B.theta, Mval);
+    g_launches++;
+  }
+  cudaFreeAsync(w, stream());
+  return st;
+}
+
 static int forward(const bg_gnn *net, GnnBufs &B, z2g *Mval) {
   const float *W = net->params;
   int N = B.N, n64 = N * GW, nb = (n64 + 255) / 256;
@@ -669,7 +786,7 @@ static int forward(const bg_gnn *net, GnnBufs &B, z2g *Mval) {
   k_gnn_readout<<<(N + 3) / 4, 128, 0, stream()>>>(N, B.rowptr, B.col, B.P, B.Q, B.Ef, W + LAY.Wrg, W + LAY.br,
                                                    W + LAY.Wo, W + LAY.bo, B.ratio, B.dinv, B.Zr, B.Oe, Mval);
   BG_LAUNCHED();
-  return BG_OK;
+  return project(B, Mval);
 }
 
 // backward from gscale * G, G = 2 dL/dconj(m); accumulates into net->grads (zeroed by the caller)
@@ -871,12 +988,14 @@ int bg_precond_create_learned(bg_geometry *g, bg_matrix *A, double omega, const 
   *out = nullptr;
   if (A->factored) { set_error("bg_precond_create_learned: matrix holds LU factors"); return BG_ERR_STATE; }
   GnnBufs B;
+  prof_start(PROF_GNN);
   int st = bufs_init(g, A, omega, false, B);
   bg_precond *P = nullptr;
   if (!st) {
     P = new bg_precond();
     P->N = B.N;
     P->nnz = B.E;
+
     cudaError_t e = cudaMalloc(&P->rowptr, sizeof(int) * (B.N + 1));
     if (e == cudaSuccess) e = cudaMalloc(&P->col, sizeof(int) * B.E);
     if (e == cudaSuccess) e = cudaMalloc(&P->val, sizeof(z2g) * B.E);
@@ -887,10 +1006,13 @@ int bg_precond_create_learned(bg_geometry *g, bg_matrix *A, double omega, const 
   }
   if (!st) st = forward(net, B, (z2g *)P->val);
   if (!st) {
+    P->rho = B.rho;
+    P->theta = B.theta;
     cudaError_t e = cudaStreamSynchronize(stream());   // the activations are freed below
     if (e != cudaSuccess) { set_error("learned preconditioner: %s", cudaGetErrorString(e)); st = BG_ERR_CUDA; }
   }
   bufs_free(B);
+  prof_stop(PROF_GNN, 0.0);
   if (st) {
     bg_precond_destroy(P);
     return st;
@@ -946,7 +1068,7 @@ int bg_gnn_train_step(bg_gnn *net, bg_geometry *g, bg_matrix *A, double omega, c
     if (e != cudaSuccess) { set_error("train step: %s", cudaGetErrorString(e)); st = BG_ERR_CUDA; }
   }
   if (!st && !(loss > 0 && std::isfinite(loss))) { set_error("train step: objective %g", loss); st = BG_ERR_NUMERIC; }
-  if (!st) st = backward(net, B, Gg, 1.0 / loss);
+  if (!st) st = backward(net, B, Gg, B.theta / loss);
   if (!st && lr > 0) {
     net->step++;
     const float b1 = 0.9f, b2 = 0.999f;
@@ -967,6 +1089,13 @@ int bg_gnn_train_step(bg_gnn *net, bg_geometry *g, bg_matrix *A, double omega, c
   bufs_free(B);
   if (loss_out) *loss_out = loss;
   return st;
+}
+
+int bg_precond_projection(const bg_precond *P, double *rho, double *theta) {
+  if (!P) { set_error("bg_precond_projection: null"); return BG_ERR_ARG; }
+  if (rho) *rho = P->rho;
+  if (theta) *theta = P->theta;
+  return BG_OK;
 }
 
 int bg_precond_download(const bg_precond *P, int *rowptr, int *col, double *val) {

@@ -42,7 +42,10 @@ cudaStream_t stream();
 int ensure_device();
 
 // kernel-class profiling (CUDA events around launches when enabled)
-enum { PROF_GEMM = 0, PROF_PANEL = 1, PROF_LASWP = 2, PROF_TRSM = 3, PROF_NCLASS = 8 };
+enum {
+  PROF_GEMM = 0, PROF_PANEL = 1, PROF_LASWP = 2, PROF_TRSM = 3, PROF_ASM_FAR = 4, PROF_ASM_NEAR = 5,
+  PROF_MATVEC = 6, PROF_GNN = 7, PROF_NCLASS = 8
+};
 bool prof_on();
 void prof_start(int cls);
 void prof_stop(int cls, double flops);
@@ -132,6 +135,7 @@ struct bg_precond {
   int N = 0, nnz = 0;
   int *rowptr = nullptr, *col = nullptr;   // CSR on the device
   void *val = nullptr;                     // complex128 values
+  double rho = 0, theta = 1;               // learned: estimate of rho(I - D M) before, and blend factor of, the projection
 };
 
 struct bg_matrix {

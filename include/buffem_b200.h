@@ -215,10 +215,27 @@ int bg_gmres_solve_mixed(bg_matrix *A, bg_matrix *F, const bg_precond *P, double
 int bg_gmres_solve_mixed_device(bg_matrix *A, bg_matrix *F, const bg_precond *P, void *B_dev, int ldb, int nrhs,
                                 double tol, int restart, int maxit, double inner_tol, double *stats);
 
+/* The learned form's solve: bg_gmres_solve_mixed, and when it misses tol
+   within maxit Krylov steps (or its residual turns non-finite), LU
+   factorisation of F (tcgen05 complex64) and the FP64-refined LU solve of the
+   original right-hand sides (F then holds factors).  stats (4 doubles, may be
+   NULL): Krylov steps, final relative residual, refinement sweeps, 1 if the
+   LU fallback ran. */
+int bg_gmres_solve_lu_fallback(bg_matrix *A, bg_matrix *F, const bg_precond *P, double *B_host, int nrhs,
+                               double tol, int restart, int maxit, double inner_tol, double *stats);
+int bg_gmres_solve_lu_fallback_device(bg_matrix *A, bg_matrix *F, const bg_precond *P, void *B_dev, int ldb,
+                                      int nrhs, double tol, int restart, int maxit, double inner_tol,
+                                      double *stats);
+
 /* Graph network (3 message-passing layers of width 64 over the near-field
    pattern of the basis functions) that predicts the entries of a sparse
-   approximate inverse on that pattern.  Parameters live on the device; the
-   untrained network (seeded Glorot weights, zero readout) reproduces Jacobi. */
+   approximate inverse on that pattern,
+     m_ij = [delta_ij + c_ij - [i != j] s_ij A_ij / A_ii] / A_jj,
+   |Re c|, |Im c| < 0.5 and |Re s|, |Im s| < 0.6, then projected so that
+   K = I - D M (D = diag A) has spectral radius <= 0.75 by a power-iteration
+   estimate rho: M <- theta M + (1 - theta) D^{-1}, theta = min(1, 0.75/rho).
+   Parameters live on the device; the untrained network (seeded Glorot
+   weights, zero readout) reproduces Jacobi. */
 typedef struct bg_gnn bg_gnn;
 int bg_gnn_create(unsigned long long seed, bg_gnn **out);
 void bg_gnn_destroy(bg_gnn *net);
@@ -239,6 +256,10 @@ int bg_gnn_train_step(bg_gnn *net, bg_geometry *g, bg_matrix *A, double omega, c
                       double *loss);
 /* Preconditioner predicted by the network for the assembled matrix A. */
 int bg_precond_create_learned(bg_geometry *g, bg_matrix *A, double omega, const bg_gnn *net, bg_precond **out);
+/* Learned preconditioners: rho, the power-iteration estimate of the spectral
+   radius of I - D M before the projection, and the blend factor theta
+   (Jacobi: 0 and 1). */
+int bg_precond_projection(const bg_precond *P, double *rho, double *theta);
 /* Copies a preconditioner's CSR (rowptr N+1 ints, col nnz ints, val 2*nnz
    doubles) to the host; any pointer may be NULL. */
 int bg_precond_download(const bg_precond *P, int *rowptr, int *col, double *val);
@@ -277,9 +298,13 @@ void *bg_stream(void);
 
 /* Kernel-class timing with CUDA events on the library stream (off by default).
    bg_profile_begin() clears and enables it; bg_profile_read() synchronises and
-   returns, per kernel class (0: LU trailing GEMM, 1: LU panel, 2: row
-   interchanges, 3: triangular-solve leaves), the number of launches, summed
-   milliseconds and algorithmic flops (counts/ms/flops arrays of length n). */
+   returns, per kernel class, the number of timed regions, summed
+   milliseconds and an algorithmic work count (counts/ms/flops arrays of
+   length n <= 8): 0 LU trailing GEMM (flops), 1 LU panel (flops), 2 row
+   interchanges, 3 triangular-solve leaves (flops), 4 far-field assembly
+   (point-pair kernel evaluations, 64 per basis-function pair), 5 near-field
+   and Gram assembly, 6 GMRES dense matrix-vector products (matrix bytes
+   read), 7 learned-preconditioner inference. */
 int bg_profile_begin(void);
 int bg_profile_read(int n, long long *counts, double *ms, double *flops);
 int bg_profile_end(void);

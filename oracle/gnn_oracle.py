@@ -12,7 +12,11 @@ Network: h0 = relu(W0 f + b0); three layers of
   h_i <- h_i + relu(Wuh h_i + Wua agg_i + bu);
 edge readout y_e = relu(Wri h_i + Wrj h_j + Wrg g_e + br), o_e = Wo y_e + bo,
   c = CMAX (tanh o0 + i tanh o1), s = SMAX (tanh o2 + i tanh o3),
-  m_ij = [delta_ij + c - [i != j] s A_ij / A_ii] / A_jj.
+  m_ij = [delta_ij + c - [i != j] s A_ij / A_ii] / A_jj,
+then the projection M <- theta M + (1 - theta) D^-1, theta = min(1, RHO / rho)
+with rho a 16-step power-iteration estimate of the spectral radius of
+K = I - D M (four seeded start vectors, as on the device); gradients hold
+theta fixed.
 
 Parameter layout (floats, in order): W0 (64x8), b0 (64), per layer l<3:
 Wmh (64x64), Wme (64x8), bm (64), Wuh (64x64), Wua (64x64), bu (64); then
@@ -22,7 +26,7 @@ are row-major (out x in).
 import numpy as np
 
 GW, GF, GE, GL, GO = 64, 8, 8, 3, 4
-CMAX, SMAX = 0.5, 0.4
+CMAX, SMAX, RHO, POWER_ITERS = 0.5, 0.6, 0.75, 16
 
 
 def layout():
@@ -148,6 +152,33 @@ def relu(x):
     return np.maximum(x, 0.0)
 
 
+def seeded_vectors(N, nv=4):
+    """The device's start vectors: 64-bit LCG, uniform in [-0.5, 0.5), re/im interleaved."""
+    s = 0x9E3779B97F4A7C15
+    M64 = (1 << 64) - 1
+    vals = np.empty(2 * nv * N)
+    for k in range(2 * nv * N):
+        s = (s * 6364136223846793005 + 1442695040888963407) & M64
+        vals[k] = (s >> 11) / 9007199254740992.0 - 0.5
+    return (vals[0::2] + 1j * vals[1::2]).reshape(nv, N).T
+
+
+def projection(rowptr, col, m, dinv):
+    """rho (estimate of the spectral radius of K = I - D M) and theta."""
+    N = len(rowptr) - 1
+    V = seeded_vectors(N)
+    rho = 0.0
+    for it in range(POWER_ITERS + 1):
+        nrm = np.sqrt(np.sum(np.abs(V) ** 2, axis=0))
+        if it > 0:
+            rho = nrm.max()
+            if it == POWER_ITERS:
+                break
+        V = V * np.where(nrm > 0, 1.0 / np.where(nrm > 0, nrm, 1.0), 0.0)
+        V = V - spmm(rowptr, col, m, V) / dinv[:, None]
+    return rho, (RHO / rho if rho > RHO else 1.0)
+
+
 def forward(p, F, Ef, rowptr, col, ratio, dinv):
     """Returns (M values on the pattern, cache for backward)."""
     N = F.shape[0]
@@ -174,7 +205,10 @@ def forward(p, F, Ef, rowptr, col, ratio, dinv):
     cc = CMAX * (t[:, 0] + 1j * t[:, 1])
     ss = SMAX * (t[:, 2] + 1j * t[:, 3])
     m = ((1.0 - off) + cc - off * ss * ratio) * dinv[col]
-    c.update(H=H, Zm=Zm, U=U, agg=agg, Zr=Zr, O=o, rows=rows, deg=deg)
+    rho, theta = projection(rowptr, col, m, dinv)
+    if theta < 1.0:
+        m = theta * m + (1.0 - theta) * (1.0 - off) * dinv[col]
+    c.update(H=H, Zm=Zm, U=U, agg=agg, Zr=Zr, O=o, rows=rows, deg=deg, rho=rho, theta=theta)
     return m, c
 
 
@@ -210,7 +244,7 @@ def backward(p, F, Ef, rowptr, col, ratio, dinv, c, G):
     H, Zm, U, agg, Zr = c["H"], c["Zm"], c["U"], c["agg"], c["Zr"]
     g = {k: np.zeros_like(v) for k, v in p.items()}
     off = (rows != col).astype(float)
-    t = G.conj() * dinv[col]
+    t = c["theta"] * G.conj() * dinv[col]
     u = t * ratio * off
     dO = np.stack([t.real, -t.imag, -u.real, u.imag], axis=1)
     dO = dO * np.array([CMAX, CMAX, SMAX, SMAX]) * (1.0 - np.tanh(c["O"]) ** 2)

@@ -1163,8 +1163,10 @@ void or_pft_opft(OGeom *G, double wr, double wi, const double *J, double *out)
 
 /* Fills the warm near-field cache: for every same-object pair a <= b with a
    common vertex, the 6 static numbers (computed once per mesh, like the
-   reference's FIBBI cache after its first frequency). */
-void or_cache_build(OGeom *G)
+   reference's FIBBI cache after its first frequency).  want (may be NULL:
+   all rows) restricts the cache to the rows a with want[a] != 0; the others
+   keep no entries and are computed on demand. */
+static void cache_build_impl(OGeom *G, const char *want)
 {
   int N = G->N;
   free(G->crow); free(G->ccol); free(G->cdat);
@@ -1203,6 +1205,7 @@ void or_cache_build(OGeom *G)
       /* insertion sort (rows are short) */
       for (int i = 1; i < m; i++) { int x = tmp[i], j = i - 1; while (j >= 0 && tmp[j] > x) { tmp[j + 1] = tmp[j]; j--; } tmp[j + 1] = x; }
       int ga = a + G->off[no];
+      if (want && !want[ga]) m = 0;
       rows[ga] = malloc(sizeof(int) * (m > 0 ? m : 1));
       for (int i = 0; i < m; i++) rows[ga][i] = tmp[i] + G->off[no];
       cnt[ga + 1] = m;
@@ -1228,6 +1231,18 @@ void or_cache_build(OGeom *G)
     }
   }
   G->crow = cnt; G->ccol = ccol; G->cdat = cdat;
+}
+
+void or_cache_build(OGeom *G) { cache_build_impl(G, NULL); }
+
+/* Warm cache for the listed rows only (bounded CPU-baseline samples). */
+void or_cache_build_rows(OGeom *G, const int *rows, int nrows)
+{
+  char *want = calloc(G->N, 1);
+  for (int i = 0; i < nrows; i++)
+    if (rows[i] >= 0 && rows[i] < G->N) want[rows[i]] = 1;
+  cache_build_impl(G, want);
+  free(want);
 }
 
 int or_cache_size(OGeom *G) { return G->crow ? G->crow[G->N] : 0; }

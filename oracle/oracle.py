@@ -85,6 +85,7 @@ def lib():
         L.or_pft_opft.argtypes = [P, D, D, dp, dp]
         L.or_num_threads.restype = I
         L.or_cache_build.argtypes = [P]
+        L.or_cache_build_rows.argtypes = [P, C.c_void_p, C.c_int]
         L.or_cache_size.argtypes = [P]
         L.or_cache_size.restype = I
         L.or_assemble_row_list.argtypes = [P, D, D, ip, I, dp]
@@ -143,8 +144,13 @@ class Geometry:
             lib().or_assemble_rows(self.h, omega.real, omega.imag, flat, rows[0], rows[1])
         return flat.view(np.complex128).reshape(N, N, order="F")
 
-    def cache_build(self):
-        lib().or_cache_build(self.h)
+    def cache_build(self, rows=None):
+        """Warm near-field cache (all rows, or only the listed rows)."""
+        if rows is None:
+            lib().or_cache_build(self.h)
+        else:
+            r = np.ascontiguousarray(rows, dtype=np.int32)
+            lib().or_cache_build_rows(self.h, r.ctypes.data_as(C.c_void_p), len(r))
         return lib().or_cache_size(self.h)
 
     def assemble_rows(self, omega, rows):

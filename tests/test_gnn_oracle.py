@@ -57,6 +57,11 @@ def test_backward_matches_finite_differences(small_system):
     rng = np.random.default_rng(1)
     _, total = go.layout()
     flat = rng.normal(scale=0.15, size=total)
+    for k in ("Wo", "bo"):                  # keep rho(K) below the projection threshold (theta = 1)
+        o, m = go.layout()[0][k]
+        flat[o:o + m] *= 0.01
+    _, c = go.forward(go.unpack(flat), F, Ef, rowptr, col, ratio, dinv)
+    assert c["theta"] == 1.0, c["rho"]
     Z = rng.normal(size=(N, 3)) + 1j * rng.normal(size=(N, 3))
     b = rng.normal(size=N) + 1j * rng.normal(size=N)
     x = np.linalg.solve(A, b)
@@ -75,3 +80,24 @@ def test_backward_matches_finite_differences(small_system):
         Lm = go.loss_and_grad(flat - e, F, Ef, rowptr, col, ratio, dinv, A, Z, b, x, 0.5)[0]
         fd = (Lp - Lm) / (2 * h)
         assert abs(fd - g[k]) <= 1e-5 * (abs(g[k]) + 1e-3 * np.abs(g).max()), (k, fd, g[k])
+
+
+def test_projection_bounds_the_spectral_radius(small_system):
+    """Large readout weights push rho(I - D M) past the threshold; after the
+    projection the true spectral radius is at most about RHO."""
+    A, faces, V, rowptr, col, etr = small_system
+    N = A.shape[0]
+    F, Ef, ratio, dinv = go.features(V, faces, A, 1.1, rowptr, col)
+    rng = np.random.default_rng(2)
+    _, total = go.layout()
+    flat = rng.normal(scale=0.3, size=total)
+    o, m = go.layout()[0]["bo"]
+    flat[o + 2] = 3.0                        # s near its bound on every edge
+    mv, c = go.forward(go.unpack(flat), F, Ef, rowptr, col, ratio, dinv)
+    assert c["theta"] < 1.0
+    rows = np.repeat(np.arange(N), np.diff(rowptr))
+    M = np.zeros((N, N), complex)
+    M[rows, col] = mv
+    K = np.eye(N) - np.diag(np.diag(A)) @ M
+    rho_true = np.abs(np.linalg.eigvals(K)).max()
+    assert rho_true <= go.RHO * 1.15, (rho_true, c["rho"], c["theta"])

@@ -135,9 +135,12 @@ def test_network_forward_and_gradients_match_oracle(sphere):
     net.set_params(flat)
     faces = G.faces(0)
     rowptr, col, val = _device_vs_oracle(G, A, net, omega, 0)
+    Pl = buffem.Preconditioner.learned(G, A, omega, net)
+    rho, theta = Pl.projection()
     F, Ef, ratio, dinv = go.features(V, faces, Ah, omega, rowptr, col)
     p = go.unpack(flat.astype(np.float64))
-    m_o, _ = go.forward(p, F, Ef, rowptr, col, ratio, dinv)
+    m_o, c_o = go.forward(p, F, Ef, rowptr, col, ratio, dinv)
+    assert abs(rho - c_o["rho"]) <= 1e-4 * c_o["rho"] and abs(theta - c_o["theta"]) <= 1e-4, (rho, theta, c_o["rho"])
     scale = np.abs(m_o).max()
     assert np.abs(val - m_o).max() <= 1e-4 * scale
     # gradients (lr = 0: no update) on random probes plus a right-hand side,
@@ -184,3 +187,31 @@ def test_trained_network_beats_jacobi(sphere):
     Xl, sl_ = buffem.GMRESSolve(A, B, Pl, tol=1e-10, restart=50, maxit=3000)
     assert sl_[1] <= 1e-10
     assert sl_[0] < sj[0], (sl_, sj)
+
+
+def test_committed_weights_beat_jacobi(sphere):
+    """The shipped weights (trained by buff-em_b200/train_gnn.py) take fewer
+    GMRES steps than Jacobi on a sphere outside the training set."""
+    G, A, B = setup(sphere(8, jitter=0.05, seed=31), omega=1.3)
+    net = buffem.GNN.load()
+    _, sj = buffem.GMRESSolve(A, B, buffem.Preconditioner.jacobi(A), tol=1e-10, restart=50, maxit=3000)
+    _, sl_ = buffem.GMRESSolve(A, B, buffem.Preconditioner.learned(G, A, 1.3, net), tol=1e-10, restart=50,
+                               maxit=3000)
+    assert sl_[1] <= 1e-10 and sl_[0] < sj[0], (sl_, sj)
+
+
+def test_lu_fallback_when_gmres_misses_tolerance(sphere):
+    """With a Krylov budget far too small, the solve falls back to the LU path
+    and still meets the tolerance; LU is also the judge of the GMRES answer."""
+    G, A, B = setup(sphere(5))
+    Ah = A.download()
+    Xo = sl.lu_solve(sl.lu_factor(Ah), B)
+    F = G.AllocateVIEMatrix(buffem.BG_C64).convert_from(A)
+    X, st = buffem.SolveLearned(A, F, B, buffem.Preconditioner.jacobi(A), tol=1e-11, restart=10, maxit=5)
+    assert st[3] == 1 and st[1] <= 1e-11, st
+    assert np.linalg.norm(X - Xo) <= 1e-9 * np.linalg.norm(Xo)
+    F2 = G.AllocateVIEMatrix(buffem.BG_C64).convert_from(A)
+    net = buffem.GNN.load()
+    X2, st2 = buffem.SolveLearned(A, F2, B, buffem.Preconditioner.learned(G, A, 1.0, net), tol=1e-11)
+    assert st2[3] == 0 and st2[1] <= 1e-11, st2
+    assert np.linalg.norm(X2 - Xo) <= 1e-9 * np.linalg.norm(Xo)
