@@ -327,6 +327,27 @@ def run_gpu(args, rank, world, local_rank):
     clk = clocks.stop()
     learned = {"steps_per_frequency": int(stats[0]), "final_rel_residual": float(stats[1]),
                "refinement_sweeps": int(stats[2]), "lu_fallback": bool(stats[3])}
+    # phase breakdown of one more (untimed) step, events on the library stream
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+    ev[0].record(stream)
+    buffem._check(L.bg_assemble(case.G.h, OMEGA, 0.0, case.M.h))
+    ev[1].record(stream)
+    buffem._check(L.bg_matrix_convert(case.M.h, case.F.h))
+    ev[2].record(stream)
+    P = buffem.Preconditioner.learned(case.G, case.M, OMEGA, net)
+    ev[3].record(stream)
+    case.rhs_device(dB)
+    ev[4].record(stream)
+    buffem._check(L.bg_gmres_solve_lu_fallback_device(case.M.h, case.F.h, P.h, buffem.C.c_void_p(dB.data_ptr()),
+                                                      N, case.nrhs, GMRES["tol"], GMRES["restart"], GMRES["maxit"],
+                                                      GMRES["inner_tol"], buffem._ptr(stats)))
+    ev[5].record(stream)
+    buffem.synchronize()
+    rho_smax = P.bound()
+    del P
+    learned["phases_s"] = {k: ev[i].elapsed_time(ev[i + 1]) / 1e3 for i, k in
+                           enumerate(("assemble", "convert_c64", "gnn_precond", "rhs", "gmres_solve"))}
+    learned["precond_bound"] = {"rho_K1": rho_smax[0], "smax": rho_smax[1]}
     if x_fp64 is not None:
         learned["err_vs_fp64_lu"] = rel_err(dB, x_fp64)
     # the same solve preconditioned by Jacobi: what the network gains

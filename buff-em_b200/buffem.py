@@ -78,7 +78,7 @@ EXPORTS = [
     "bg_gmres_solve", "bg_gmres_solve_device", "bg_gnn_create", "bg_gnn_destroy", "bg_gnn_num_params",
     "bg_gnn_get_params", "bg_gnn_set_params", "bg_gnn_get_grads", "bg_gnn_train_step",
     "bg_precond_create_learned", "bg_precond_download", "bg_gmres_solve_mixed", "bg_gmres_solve_mixed_device",
-    "bg_precond_projection", "bg_gmres_solve_lu_fallback", "bg_gmres_solve_lu_fallback_device",
+    "bg_precond_bound", "bg_gmres_solve_lu_fallback", "bg_gmres_solve_lu_fallback_device",
 ]
 
 
@@ -132,7 +132,7 @@ def lib():
         L.bg_gnn_train_step.argtypes = [P, P, P, D, VP, I, I, VP, VP, D, D, VP]
         L.bg_precond_create_learned.argtypes = [P, P, D, P, C.POINTER(P)]
         L.bg_precond_download.argtypes = [P, VP, VP, VP]
-        L.bg_precond_projection.argtypes = [P, VP, VP]
+        L.bg_precond_bound.argtypes = [P, VP, VP]
         L.bg_rhs_planewave.argtypes = [P, D, D, VP, VP, VP]
         L.bg_rhs_planewave_device.argtypes = [P, D, D, VP, VP, VP]
         L.bg_pft.argtypes = [P, D, D, VP, VP, VP, I, VP]
@@ -348,11 +348,11 @@ class Preconditioner:
     def nnz(self):
         return lib().bg_precond_nnz(self.h)
 
-    def projection(self):
-        """Learned: (rho, theta), the estimate of rho(I - D M) before the
-        projection and the blend factor with the Jacobi inverse."""
+    def bound(self):
+        """Learned: (rho(K1), smax), the near-field spectral estimate and the
+        Neumann-coefficient bound it set."""
         out = np.zeros(2)
-        _check(lib().bg_precond_projection(self.h, _ptr(out[:1]), _ptr(out[1:])))
+        _check(lib().bg_precond_bound(self.h, _ptr(out[:1]), _ptr(out[1:])))
         return float(out[0]), float(out[1])
 
     def csr(self, N):

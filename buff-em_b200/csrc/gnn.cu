@@ -13,17 +13,20 @@
 //   edge readout: y_e = relu(Wri h_i + Wrj h_j + Wrg g_e + br)       (64)
 //                 o_e = Wo y_e + bo                                 (4)
 //                 c = GNN_CMAX (tanh(o0) + i tanh(o1))
-//                 s = GNN_SMAX (tanh(o2) + i tanh(o3))
+//                 s = smax (tanh(o2) + i tanh(o3) / 2)
 //   m_ij = [delta_ij + c - [i != j] s A_ij / A_ii] / A_jj
 // With s = 1 and c = 0 the off-diagonal term would be the first-order
 // Neumann approximation of A^{-1} around its diagonal.  Written D M = I - K
 // (D = diag A), M is singular where K has an eigenvalue 1, and a preconditioner
 // close to that makes GMRES stall on a few modes that no averaged objective
-// sees.  So the predicted M is projected: a power iteration estimates rho(K)
-// and M <- theta M + (1 - theta) D^{-1}, theta = min(1, GNN_RHO / rho), which
-// scales K to spectral radius <= GNN_RHO (training differentiates with theta
-// held fixed).  Wo and bo start at zero, so the untrained network is the
-// Jacobi (diagonal) inverse.
+// sees.  For a constant coefficient K = s K1, K1 the scaled near-field
+// off-diagonal part (K1_ij = A_ij / A_jj on the pattern), whose dominant
+// eigenvalue is real and positive on these matrices (about 2.2 at N = 8k, 2.6
+// at N = 57k); GMRES stalled exactly when s crossed 1 / rho(K1).  So a power
+// iteration estimates rho(K1) for the matrix at hand and the coefficient is
+// bounded by smax = GNN_SREL / max(GNN_SREL, rho(K1)), with the diagonal
+// correction c kept small.  Wo and bo start at zero, so the untrained network
+// is the Jacobi (diagonal) inverse.
 //
 // Training objective (per matrix; p probes z and a right-hand side b with its
 // LU solution x):
@@ -55,9 +58,8 @@ namespace bg {
 #define GL 3           // message-passing layers
 #define GO 4           // outputs per edge
 #define GNN_MAXP 16    // probes per training step
-#define GNN_CMAX 0.5f  // bound of the diagonal-term correction c
-#define GNN_SMAX 0.6f  // bound of the Neumann coefficient s
-#define GNN_RHO 0.75   // spectral radius of K = I - D M after the projection
+#define GNN_CMAX 0.1f  // bound of the diagonal-term correction c
+#define GNN_SREL 0.7   // |Re s| < GNN_SREL / rho(K1)
 #define GNN_POWER_ITERS 16
 
 // parameter layout (floats); matrices row-major (out x in)
@@ -199,7 +201,7 @@ __global__ void k_gnn_residual(int n, const float *H, const float *U, float *Hn)
 // edge readout, one warp per row; lane owns hidden units lane and lane + 32
 __global__ void k_gnn_readout(int N, const int *rowptr, const int *col, const float *Pr, const float *Qr,
                               const float *Ef, const float *Wrg, const float *br, const float *Wo, const float *bo,
-                              const z2g *ratio, const z2g *dinv, float *Zr, float *Oe, z2g *Mval) {
+                              const z2g *ratio, const z2g *dinv, float smax, float *Zr, float *Oe, z2g *Mval) {
   int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   int lane = threadIdx.x & 31;
   if (i >= N) return;
@@ -234,7 +236,7 @@ __global__ void k_gnn_readout(int N, const int *rowptr, const int *col, const fl
         for (int k = 0; k < GO; k++) Oe[(size_t)e * GO + k] = o[k];
       z2g c{(i == j ? 1.0 : 0.0) + GNN_CMAX * tanhf(o[0]), (double)(GNN_CMAX * tanhf(o[1]))};
       if (i != j) {
-        z2g sr = zmul(z2g{(double)(GNN_SMAX * tanhf(o[2])), (double)(GNN_SMAX * tanhf(o[3]))}, ratio[e]);
+        z2g sr = zmul(z2g{(double)(smax * tanhf(o[2])), (double)(0.5f * smax * tanhf(o[3]))}, ratio[e]);
         c.r -= sr.r;
         c.i -= sr.i;
       }
@@ -243,22 +245,23 @@ __global__ void k_gnn_readout(int N, const int *rowptr, const int *col, const fl
   }
 }
 
-// W[:, q] = K V[:, q] = V - D (M V), D = diag A = 1 / dinv; one thread per row
-__global__ void k_gnn_kmv(int N, const int *rowptr, const int *col, const z2g *Mval, const z2g *dinv, const z2g *V,
-                          int nv, z2g *W) {
+// W[:, q] = K1 V[:, q], (K1)_ij = A_ij / A_jj = r_e dinv_j / dinv_i off the diagonal
+__global__ void k_gnn_k1mv(int N, const int *rowptr, const int *col, const z2g *ratio, const z2g *dinv,
+                           const z2g *V, int nv, z2g *W) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
-  z2g d = zdiv(z2g{1.0, 0.0}, dinv[i]);
+  z2g ai = zdiv(z2g{1.0, 0.0}, dinv[i]);
   for (int q = 0; q < nv; q++) {
     const z2g *v = V + (size_t)q * N;
     z2g s{0.0, 0.0};
     for (int e = rowptr[i]; e < rowptr[i + 1]; e++) {
-      z2g t = zmul(Mval[e], v[col[e]]);
+      int j = col[e];
+      if (j == i) continue;
+      z2g t = zmul(zmul(ratio[e], dinv[j]), v[j]);
       s.r += t.r;
       s.i += t.i;
     }
-    z2g ds = zmul(d, s);
-    W[(size_t)q * N + i] = z2g{v[i].r - ds.r, v[i].i - ds.i};
+    W[(size_t)q * N + i] = zmul(ai, s);
   }
 }
 
@@ -285,28 +288,12 @@ __global__ void k_gnn_scale_cols(int N, int nv, const double *f, z2g *V) {
   V[t] = z2g{V[t].r * s, V[t].i * s};
 }
 
-// M <- theta M + (1 - theta) D^{-1}
-__global__ void k_gnn_blend(int N, const int *rowptr, const int *col, const z2g *dinv, double theta, z2g *Mval) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
-  for (int e = rowptr[i]; e < rowptr[i + 1]; e++) {
-    z2g m = Mval[e];
-    m.r *= theta;
-    m.i *= theta;
-    if (col[e] == i) {
-      m.r += (1 - theta) * dinv[i].r;
-      m.i += (1 - theta) * dinv[i].i;
-    }
-    Mval[e] = m;
-  }
-}
-
 // ------------------------------------------------------------------ backward
 // output gradients per edge from G = 2 dL/dconj(m):
 // t = conj(G) d_j, u = conj(G) r_e d_j ; d(c, s) = (Re t, -Im t, -Re u, Im u)
 // (u terms off-diagonal only), then through the bounded tanh maps of o
 __global__ void k_gnn_dout(int N, const int *rowptr, const int *col, const z2g *G, double gscale, const z2g *ratio,
-                           const z2g *dinv, const float *Oe, float *dO) {
+                           const z2g *dinv, float smax, const float *Oe, float *dO) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   for (int e = rowptr[i]; e < rowptr[i + 1]; e++) {
@@ -326,7 +313,7 @@ __global__ void k_gnn_dout(int N, const int *rowptr, const int *col, const z2g *
     }
     for (int k = 0; k < GO; k++) {
       float th = tanhf(Oe[(size_t)e * GO + k]);
-      d[k] *= (k < 2 ? GNN_CMAX : GNN_SMAX) * (1.f - th * th);
+      d[k] *= (k < 2 ? GNN_CMAX : (k == 2 ? smax : 0.5f * smax)) * (1.f - th * th);
     }
   }
 }
@@ -594,7 +581,8 @@ namespace bg {
 // per-call activations (the graph itself is cached in the geometry)
 struct GnnBufs {
   int N = 0, E = 0;
-  double rho = 0, theta = 1;   // spectral estimate of K = I - D M and the projection factor
+  double rho_ref = 0;   // estimate of rho(K1)
+  float smax = 0;       // bound of the Neumann coefficient
   const int *rowptr = nullptr, *col = nullptr, *etr = nullptr;
   float *F = nullptr, *Ef = nullptr;
   z2g *ratio = nullptr, *dinv = nullptr;
@@ -673,6 +661,8 @@ static int ensure_graph(bg_geometry *g) {
   return BG_OK;
 }
 
+static int bound_coefficient(GnnBufs &B);
+
 static int bufs_init(bg_geometry *g, bg_matrix *A, double omega, bool train, GnnBufs &B) {
   int st = ensure_graph(g);
   if (st) return st;
@@ -703,12 +693,12 @@ static int bufs_init(bg_geometry *g, bg_matrix *A, double omega, bool train, Gnn
   k_gnn_features<<<(N + 127) / 128, 128, 0, stream()>>>(N, B.rowptr, B.col, (const z2g *)A->d, A->ld, g->dev, omega,
                                                         g->graph.h, B.F, B.Ef, B.ratio, B.dinv);
   BG_LAUNCHED();
-  return BG_OK;
+  return bound_coefficient(B);
 }
 
-// Power iteration for rho(K), K = I - D M (four seeded vectors in lockstep),
-// then M <- theta M + (1 - theta) D^{-1} with theta = min(1, GNN_RHO / rho).
-static int project(GnnBufs &B, z2g *Mval) {
+// Power iteration (four seeded vectors in lockstep, GNN_POWER_ITERS steps)
+// for the spectral radius of K1; sets the coefficient bound smax.
+static int bound_coefficient(GnnBufs &B) {
   const int nv = 4;
   int N = B.N;
   size_t nn = (size_t)N * nv;
@@ -743,19 +733,15 @@ static int project(GnnBufs &B, z2g *Mval) {
     for (int q = 0; q < nv; q++) f[q] = hn[q] > 0 ? 1.0 / std::sqrt(hn[q]) : 0.0;
     if ((e = cudaMemcpyAsync(fac, f, sizeof(double) * nv, cudaMemcpyHostToDevice, stream())) != cudaSuccess) break;
     k_gnn_scale_cols<<<(nn + 255) / 256, 256, 0, stream()>>>(N, nv, fac, V);
-    k_gnn_kmv<<<(N + 127) / 128, 128, 0, stream()>>>(N, B.rowptr, B.col, Mval, B.dinv, V, nv, W);
+    k_gnn_k1mv<<<(N + 127) / 128, 128, 0, stream()>>>(N, B.rowptr, B.col, B.ratio, B.dinv, V, nv, W);
     g_launches += 2;
     std::swap(V, W);
   }
-  if (e != cudaSuccess) { set_error("preconditioner projection: %s", cudaGetErrorString(e)); st = BG_ERR_CUDA; }
-  if (!st && !std::isfinite(rho)) { set_error("preconditioner projection: non-finite estimate"); st = BG_ERR_NUMERIC; }
-  B.rho = rho;
-  B.theta = (!st && rho > GNN_RHO) ? GNN_RHO / rho : 1.0;
-  if (!st && B.theta < 1.0) {
-    k_gnn_blend<<<(N + 127) / 128, 128, 0, stream()>>>(N, B.rowptr, B.col, B.dinv, B.theta, Mval);
-    g_launches++;
-  }
+  if (e != cudaSuccess) { set_error("near-field spectral estimate: %s", cudaGetErrorString(e)); st = BG_ERR_CUDA; }
+  if (!st && !std::isfinite(rho)) { set_error("near-field spectral estimate: non-finite"); st = BG_ERR_NUMERIC; }
   cudaFreeAsync(w, stream());
+  B.rho_ref = rho;
+  B.smax = (float)(GNN_SREL / std::max(rho, GNN_SREL));
   return st;
 }
 
@@ -784,9 +770,10 @@ static int forward(const bg_gnn *net, GnnBufs &B, z2g *Mval) {
   k_gnn_linear<<<N, GW, 0, stream()>>>(N, GW, GW, B.H[GL], GW, W + LAY.Wrj, nullptr, B.Q, GW, 0);
   BG_LAUNCHED();
   k_gnn_readout<<<(N + 3) / 4, 128, 0, stream()>>>(N, B.rowptr, B.col, B.P, B.Q, B.Ef, W + LAY.Wrg, W + LAY.br,
-                                                   W + LAY.Wo, W + LAY.bo, B.ratio, B.dinv, B.Zr, B.Oe, Mval);
+                                                   W + LAY.Wo, W + LAY.bo, B.ratio, B.dinv, B.smax, B.Zr, B.Oe,
+                                                   Mval);
   BG_LAUNCHED();
-  return project(B, Mval);
+  return BG_OK;
 }
 
 // backward from gscale * G, G = 2 dL/dconj(m); accumulates into net->grads (zeroed by the caller)
@@ -794,7 +781,8 @@ static int backward(bg_gnn *net, GnnBufs &B, const z2g *G, double gscale) {
   const float *W = net->params;
   float *dW = net->grads;
   int N = B.N, E = B.E, n64 = N * GW, nb = (n64 + 255) / 256;
-  k_gnn_dout<<<(N + 127) / 128, 128, 0, stream()>>>(N, B.rowptr, B.col, G, gscale, B.ratio, B.dinv, B.Oe, B.dO);
+  k_gnn_dout<<<(N + 127) / 128, 128, 0, stream()>>>(N, B.rowptr, B.col, G, gscale, B.ratio, B.dinv, B.smax, B.Oe,
+                                                    B.dO);
   BG_LAUNCHED();
   k_gnn_wo_grad<<<GW, 256, 0, stream()>>>(E, B.dO, B.Zr, dW + LAY.Wo, dW + LAY.bo);
   BG_LAUNCHED();
@@ -1006,8 +994,8 @@ int bg_precond_create_learned(bg_geometry *g, bg_matrix *A, double omega, const 
   }
   if (!st) st = forward(net, B, (z2g *)P->val);
   if (!st) {
-    P->rho = B.rho;
-    P->theta = B.theta;
+    P->rho = B.rho_ref;
+    P->theta = B.smax;
     cudaError_t e = cudaStreamSynchronize(stream());   // the activations are freed below
     if (e != cudaSuccess) { set_error("learned preconditioner: %s", cudaGetErrorString(e)); st = BG_ERR_CUDA; }
   }
@@ -1068,7 +1056,7 @@ int bg_gnn_train_step(bg_gnn *net, bg_geometry *g, bg_matrix *A, double omega, c
     if (e != cudaSuccess) { set_error("train step: %s", cudaGetErrorString(e)); st = BG_ERR_CUDA; }
   }
   if (!st && !(loss > 0 && std::isfinite(loss))) { set_error("train step: objective %g", loss); st = BG_ERR_NUMERIC; }
-  if (!st) st = backward(net, B, Gg, B.theta / loss);
+  if (!st) st = backward(net, B, Gg, 1.0 / loss);
   if (!st && lr > 0) {
     net->step++;
     const float b1 = 0.9f, b2 = 0.999f;
@@ -1091,10 +1079,10 @@ int bg_gnn_train_step(bg_gnn *net, bg_geometry *g, bg_matrix *A, double omega, c
   return st;
 }
 
-int bg_precond_projection(const bg_precond *P, double *rho, double *theta) {
-  if (!P) { set_error("bg_precond_projection: null"); return BG_ERR_ARG; }
+int bg_precond_bound(const bg_precond *P, double *rho, double *smax) {
+  if (!P) { set_error("bg_precond_bound: null"); return BG_ERR_ARG; }
   if (rho) *rho = P->rho;
-  if (theta) *theta = P->theta;
+  if (smax) *smax = P->theta;
   return BG_OK;
 }
 

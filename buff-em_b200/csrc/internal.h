@@ -135,7 +135,7 @@ struct bg_precond {
   int N = 0, nnz = 0;
   int *rowptr = nullptr, *col = nullptr;   // CSR on the device
   void *val = nullptr;                     // complex128 values
-  double rho = 0, theta = 1;               // learned: estimate of rho(I - D M) before, and blend factor of, the projection
+  double rho = 0, theta = 0;               // learned: estimate of rho(K1) and the coefficient bound smax
 };
 
 struct bg_matrix {

@@ -3,8 +3,9 @@ writes its weights next to this file (weights/gnn_near_spai.f32 plus a JSON
 record of the run).
 
 Data: seeded synthetic sphere meshes (N from 1350 to 8262 basis functions)
-with random jitter, radius, frequency and material (isotropic, anisotropic
-tensor or Gaussian-profile permittivity).  Each visit assembles the VIE
+with random jitter (up to 0.1 of the cell), radius (0.8-1.25), frequency
+(0.5-3) and material (isotropic, anisotropic tensor or Gaussian-profile
+permittivity).  Each visit assembles the VIE
 matrix, solves one plane-wave right-hand side by LU for the solution term of
 the objective, and takes a few Adam steps with fresh random probes.
 
@@ -49,7 +50,7 @@ def make_dataset(n_meshes, seed, meshdir):
     for s in range(n_meshes):
         n = int(rng.integers(5, 10))
         items.append(dict(n=n, jitter=float(rng.uniform(0, 0.1)), radius=float(rng.uniform(0.8, 1.25)),
-                          omega=float(rng.uniform(0.7, 1.5)), seed=seed * 100000 + s,
+                          omega=float(rng.uniform(0.5, 3.0)), seed=seed * 100000 + s,
                           mat_seed=int(rng.integers(1 << 31))))
     return items
 

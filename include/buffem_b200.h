@@ -231,11 +231,11 @@ int bg_gmres_solve_lu_fallback_device(bg_matrix *A, bg_matrix *F, const bg_preco
    pattern of the basis functions) that predicts the entries of a sparse
    approximate inverse on that pattern,
      m_ij = [delta_ij + c_ij - [i != j] s_ij A_ij / A_ii] / A_jj,
-   |Re c|, |Im c| < 0.5 and |Re s|, |Im s| < 0.6, then projected so that
-   K = I - D M (D = diag A) has spectral radius <= 0.75 by a power-iteration
-   estimate rho: M <- theta M + (1 - theta) D^{-1}, theta = min(1, 0.75/rho).
-   Parameters live on the device; the untrained network (seeded Glorot
-   weights, zero readout) reproduces Jacobi. */
+   |Re c|, |Im c| < 0.1, |Re s| < smax, |Im s| < smax / 2, where
+   smax = 0.7 / max(0.7, rho(K1)) and rho(K1) is a power-iteration estimate of
+   the spectral radius of the scaled near-field part K1_ij = A_ij / A_jj
+   (i != j on the pattern).  Parameters live on the device; the untrained
+   network (seeded Glorot weights, zero readout) reproduces Jacobi. */
 typedef struct bg_gnn bg_gnn;
 int bg_gnn_create(unsigned long long seed, bg_gnn **out);
 void bg_gnn_destroy(bg_gnn *net);
@@ -256,10 +256,9 @@ int bg_gnn_train_step(bg_gnn *net, bg_geometry *g, bg_matrix *A, double omega, c
                       double *loss);
 /* Preconditioner predicted by the network for the assembled matrix A. */
 int bg_precond_create_learned(bg_geometry *g, bg_matrix *A, double omega, const bg_gnn *net, bg_precond **out);
-/* Learned preconditioners: rho, the power-iteration estimate of the spectral
-   radius of I - D M before the projection, and the blend factor theta
-   (Jacobi: 0 and 1). */
-int bg_precond_projection(const bg_precond *P, double *rho, double *theta);
+/* Learned preconditioners: the estimate of rho(K1) and the coefficient bound
+   smax used (Jacobi: 0 and 0). */
+int bg_precond_bound(const bg_precond *P, double *rho, double *smax);
 /* Copies a preconditioner's CSR (rowptr N+1 ints, col nnz ints, val 2*nnz
    doubles) to the host; any pointer may be NULL. */
 int bg_precond_download(const bg_precond *P, int *rowptr, int *col, double *val);

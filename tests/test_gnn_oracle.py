@@ -57,11 +57,6 @@ def test_backward_matches_finite_differences(small_system):
     rng = np.random.default_rng(1)
     _, total = go.layout()
     flat = rng.normal(scale=0.15, size=total)
-    for k in ("Wo", "bo"):                  # keep rho(K) below the projection threshold (theta = 1)
-        o, m = go.layout()[0][k]
-        flat[o:o + m] *= 0.01
-    _, c = go.forward(go.unpack(flat), F, Ef, rowptr, col, ratio, dinv)
-    assert c["theta"] == 1.0, c["rho"]
     Z = rng.normal(size=(N, 3)) + 1j * rng.normal(size=(N, 3))
     b = rng.normal(size=N) + 1j * rng.normal(size=N)
     x = np.linalg.solve(A, b)
@@ -82,22 +77,27 @@ def test_backward_matches_finite_differences(small_system):
         assert abs(fd - g[k]) <= 1e-5 * (abs(g[k]) + 1e-3 * np.abs(g).max()), (k, fd, g[k])
 
 
-def test_projection_bounds_the_spectral_radius(small_system):
-    """Large readout weights push rho(I - D M) past the threshold; after the
-    projection the true spectral radius is at most about RHO."""
+def test_coefficient_bound_tracks_the_near_field_spectrum(small_system):
+    """The power-iteration estimate of rho(K1) matches the dense eigenvalue
+    computation, and a saturated readout gives s = smax on every edge."""
     A, faces, V, rowptr, col, etr = small_system
     N = A.shape[0]
     F, Ef, ratio, dinv = go.features(V, faces, A, 1.1, rowptr, col)
     rng = np.random.default_rng(2)
     _, total = go.layout()
     flat = rng.normal(scale=0.3, size=total)
+    o, m = go.layout()[0]["Wo"]
+    flat[o:o + m] = 0.0
     o, m = go.layout()[0]["bo"]
-    flat[o + 2] = 3.0                        # s near its bound on every edge
+    flat[o:o + m] = [0.0, 0.0, 30.0, 0.0]    # c = 0 and s = smax on every edge
     mv, c = go.forward(go.unpack(flat), F, Ef, rowptr, col, ratio, dinv)
-    assert c["theta"] < 1.0
     rows = np.repeat(np.arange(N), np.diff(rowptr))
-    M = np.zeros((N, N), complex)
-    M[rows, col] = mv
-    K = np.eye(N) - np.diag(np.diag(A)) @ M
-    rho_true = np.abs(np.linalg.eigvals(K)).max()
-    assert rho_true <= go.RHO * 1.15, (rho_true, c["rho"], c["theta"])
+    K1 = np.zeros((N, N), complex)
+    K1[rows, col] = np.where(rows != col, A[rows, col] / np.diag(A)[col], 0)
+    rho1_true = np.abs(np.linalg.eigvals(K1)).max()
+    assert abs(c["rho_ref"] - rho1_true) <= 0.1 * rho1_true, (c["rho_ref"], rho1_true)
+    assert c["smax"] == go.SREL / max(c["rho_ref"], go.SREL)
+    # m_ij = -smax r_ij / A_jj off the diagonal, 1 / A_jj on it
+    off = rows != col
+    np.testing.assert_allclose(mv[off], -c["smax"] * ratio[off] * dinv[col[off]], rtol=1e-12, atol=0)
+    np.testing.assert_allclose(mv[~off], dinv[col[~off]], rtol=1e-12, atol=0)

@@ -136,11 +136,12 @@ def test_network_forward_and_gradients_match_oracle(sphere):
     faces = G.faces(0)
     rowptr, col, val = _device_vs_oracle(G, A, net, omega, 0)
     Pl = buffem.Preconditioner.learned(G, A, omega, net)
-    rho, theta = Pl.projection()
+    rho1, smax = Pl.bound()
     F, Ef, ratio, dinv = go.features(V, faces, Ah, omega, rowptr, col)
     p = go.unpack(flat.astype(np.float64))
     m_o, c_o = go.forward(p, F, Ef, rowptr, col, ratio, dinv)
-    assert abs(rho - c_o["rho"]) <= 1e-4 * c_o["rho"] and abs(theta - c_o["theta"]) <= 1e-4, (rho, theta, c_o["rho"])
+    assert abs(rho1 - c_o["rho_ref"]) <= 1e-9 * c_o["rho_ref"], (rho1, c_o["rho_ref"])
+    assert abs(smax - c_o["smax"]) <= 1e-6 * c_o["smax"]
     scale = np.abs(m_o).max()
     assert np.abs(val - m_o).max() <= 1e-4 * scale
     # gradients (lr = 0: no update) on random probes plus a right-hand side,
@@ -179,7 +180,8 @@ def test_trained_network_beats_jacobi(sphere):
         N = G.TotalBFs
         Z = rng.normal(size=(N, 8)) + 1j * rng.normal(size=(N, 8))
         losses.append(net.train_step(G, A, 1.0, Z, b, x, lam=1.0, lr=2e-3, probe_power=4 * (it % 2)))
-    assert np.mean(losses[-8:]) < np.mean(losses[:8])
+    plain = losses[0::2]                      # steps on unmapped random probes
+    assert np.mean(plain[-4:]) < np.mean(plain[:4]), (plain[:4], plain[-4:])
     G, A, B = setup(sphere(5, jitter=0.15, seed=7), omega=1.0)
     Pj = buffem.Preconditioner.jacobi(A)
     Pl = buffem.Preconditioner.learned(G, A, 1.0, net)
