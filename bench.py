@@ -289,6 +289,74 @@ def rel_err(x, ref):
     return float(torch.linalg.norm(x - ref) / torch.linalg.norm(ref))
 
 
+def batch_geometries(seed=2026, count=8):
+    """Two-sphere geometries of the batching workload: radii U[0.5, 1.5],
+    surface gap U[0.2, 1] along z, cells per edge n1, n2 in 2..10 redrawn until
+    1k <= N1 + N2 <= 12k, eps(x) = 3 + 1.5 exp(-|x - c|^2) + 0.1i about each
+    sphere's own centre c."""
+    import buffem
+    import meshgen
+    rng = np.random.default_rng(seed)
+    d = os.path.join(tempfile.gettempdir(), "buffem_bench_meshes")
+    F = lambda n: 12 * n ** 3 - 6 * n ** 2
+    out = []
+    for _ in range(count):
+        r1, r2 = rng.uniform(0.5, 1.5, 2)
+        gap = rng.uniform(0.2, 1.0)
+        while True:
+            n1, n2 = rng.integers(2, 11, 2)
+            if 1000 <= F(n1) + F(n2) <= 12000:
+                break
+        z2 = r1 + gap + r2
+        mats = [buffem.Material(kind=buffem.BG_MAT_GAUSSIAN, eps=3 + 0.1j, amp=1.5, width=1.0, center=(0, 0, 0)),
+                buffem.Material(kind=buffem.BG_MAT_GAUSSIAN, eps=3 + 0.1j, amp=1.5, width=1.0, center=(0, 0, z2))]
+        G = buffem.SWGGeometry(meshfiles=[meshgen.cached_sphere(d, int(n1), float(r1)),
+                                          meshgen.cached_sphere(d, int(n2), float(r2))],
+                               materials=mats, displacements=[[0, 0, 0], [0, 0, z2]])
+        out.append((G, dict(r1=float(r1), r2=float(r2), gap=float(gap), n1=int(n1), n2=int(n2), N=G.TotalBFs)))
+    return out
+
+
+def run_batching(nomega=64):
+    """Batching form: 8 geometries x 64 log-spaced omega in [0.01, 10] through
+    bg_batch_sweep, and the same kind of job one at a time through the plain
+    calls (two frequencies per geometry) for comparison."""
+    import torch
+    import buffem
+    geo = batch_geometries()
+    omegas = np.logspace(-2, 1, nomega)
+    wave = buffem.PlaneWave([1, 0, 0], [0, 0, 1])
+    for G, _ in geo:
+        G.precompute()
+    buffem.synchronize()
+    pabs, st = buffem.BatchSweep([g for g, _ in geo], omegas, wave, max_streams=4)
+    seq = []
+    for G, meta in geo:
+        ts = []
+        for w in (omegas[10], omegas[40]):
+            buffem.synchronize()
+            t0 = time.perf_counter()
+            M = G.AssembleVIEMatrix(w)
+            M.LUFactorize()
+            x = G.AssembleRHSVector(w, wave)
+            M.LUSolve(x)
+            G.GetPFTMatrix(x, w, wave, method=buffem.BG_PFT_OVERLAP)
+            ts.append(time.perf_counter() - t0)
+            del M
+        seq.append(min(ts))
+    Ns = [m["N"] for _, m in geo]
+    seq_total = sum(t * nomega for t in seq)
+    tuning = [{"N": Ns[i], "panel_rows": int(st[4 + 3 * i]), "slots": int(st[5 + 3 * i])} for i in range(len(geo))]
+    torch.cuda.empty_cache()
+    return {"jobs": int(st[1]), "seconds": float(st[0]), "s_per_job": float(st[0] / st[1]),
+            "graphs": bool(st[2]), "capture_fell_back": bool(st[3]), "geometries": [m for _, m in geo],
+            "tuning": tuning, "one_by_one_estimate_s": seq_total,
+            "speedup_vs_one_by_one": seq_total / float(st[0]),
+            "one_by_one_note": "plain host-API calls per job (assemble, LU, RHS, solve, overlap PFT), best of 2 "
+                               "frequencies per geometry x 64",
+            "pabs_finite": bool(np.all(np.isfinite(pabs)))}
+
+
 def run_gpu(args, rank, world, local_rank):
     import torch
     import buffem
@@ -467,6 +535,7 @@ def main():
     ap.add_argument("--fp64-steps", type=int, default=1, help="timed steps of the FP64 path at the headline size")
     ap.add_argument("--fp64-warmup", type=int, default=1)
     ap.add_argument("--order", type=int, default=10, help="singular-rule order")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batching-form sweep (8 geometries x 64 omega)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--lean", action="store_true",
                     help="headline learned steps only (no FP64 arm, e2e, secondary, CPU baseline): profiler runs")
@@ -557,6 +626,8 @@ def main():
                              "kernel_classes": pf}
     if "secondary" in res:
         line["secondary_n19872"] = res["secondary"]
+    if not args.lean and not args.no_batch:
+        line["batching_form"] = run_batching()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = cpu_sample(args.n, args.order)
         line["cpu_baseline"] = {"value": r["value"], "unit": "s", "cores": r["cores"], "kind": "port",

@@ -27,6 +27,7 @@ LIB_PATH = os.path.join(_HERE, "libbuffem_b200.so")
 _LIB = None
 
 BG_C128, BG_C64 = 0, 1
+BG_BATCH_MAXOBJ, BG_BATCH_NO_GRAPHS = 4, 1
 BG_MAT_CONST_ISO, BG_MAT_CONST_TENSOR, BG_MAT_JANUS_Z, BG_MAT_GAUSSIAN = 0, 1, 2, 3
 BG_PFT_EMT, BG_PFT_OVERLAP = 0, 1
 BG_OK, BG_ERR_ARG, BG_ERR_IO, BG_ERR_TOPOLOGY, BG_ERR_CUDA, BG_ERR_NOMEM, BG_ERR_STATE, BG_ERR_NUMERIC = 0, -1, -2, -3, -4, -5, -6, -7
@@ -78,7 +79,7 @@ EXPORTS = [
     "bg_gmres_solve", "bg_gmres_solve_device", "bg_gnn_create", "bg_gnn_destroy", "bg_gnn_num_params",
     "bg_gnn_get_params", "bg_gnn_set_params", "bg_gnn_get_grads", "bg_gnn_train_step",
     "bg_precond_create_learned", "bg_precond_download", "bg_gmres_solve_mixed", "bg_gmres_solve_mixed_device",
-    "bg_precond_bound", "bg_gmres_solve_lu_fallback", "bg_gmres_solve_lu_fallback_device",
+    "bg_precond_bound", "bg_gmres_solve_lu_fallback", "bg_gmres_solve_lu_fallback_device", "bg_batch_sweep",
 ]
 
 
@@ -121,6 +122,7 @@ def lib():
         L.bg_gmres_solve_device.argtypes = [P, P, VP, I, I, D, I, I, VP]
         L.bg_gmres_solve_mixed.argtypes = [P, P, P, VP, I, D, I, I, D, VP]
         L.bg_gmres_solve_lu_fallback.argtypes = [P, P, P, VP, I, D, I, I, D, VP]
+        L.bg_batch_sweep.argtypes = [VP, I, VP, I, VP, VP, I, I, VP, VP]
         L.bg_gmres_solve_lu_fallback_device.argtypes = [P, P, P, VP, I, I, D, I, I, D, VP]
         L.bg_gmres_solve_mixed_device.argtypes = [P, P, P, VP, I, I, D, I, I, D, VP]
         L.bg_gnn_create.argtypes = [C.c_ulonglong, C.POINTER(P)]
@@ -461,6 +463,20 @@ def SolveLearned(M, F, B, P=None, tol=1e-10, restart=50, maxit=1000, inner_tol=1
     _check(lib().bg_gmres_solve_lu_fallback(M.h, F.h, P.h if P is not None else None, _ptr(arr), nrhs, float(tol),
                                             int(restart), int(maxit), float(inner_tol), _ptr(st)))
     return arr, st
+
+
+def BatchSweep(geoms, omegas, IF, max_streams=4, graphs=True):
+    """Batched frequency sweep: for every geometry and omega, assemble, LU,
+    solve the plane wave IF and return the absorbed power of each object
+    (overlap method).  Returns (pabs[ngeom, nomega, BG_BATCH_MAXOBJ], stats)."""
+    geoms = list(geoms)
+    w = np.ascontiguousarray(np.asarray(omegas, dtype=np.complex128))
+    hs = (C.c_void_p * len(geoms))(*[g.h for g in geoms])
+    out = np.zeros((len(geoms), len(w), BG_BATCH_MAXOBJ))
+    st = np.zeros(4 + 3 * len(geoms))
+    _check(lib().bg_batch_sweep(C.cast(hs, C.c_void_p), len(geoms), _ptr(w), len(w), _ptr(IF.E0), _ptr(IF.nHat),
+                                int(max_streams), 0 if graphs else BG_BATCH_NO_GRAPHS, _ptr(out), _ptr(st)))
+    return out, st
 
 
 def launch_count():

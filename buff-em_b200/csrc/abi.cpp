@@ -53,7 +53,12 @@ int ensure_device() {
   return BG_OK;
 }
 
-cudaStream_t stream() { return s_stream; }
+// A calling thread may direct the library's work to another stream (the
+// batched sweeps run several slots concurrently); by default everything runs
+// on the library stream.
+static thread_local cudaStream_t t_stream = nullptr;
+cudaStream_t stream() { return t_stream ? t_stream : s_stream; }
+void set_thread_stream(cudaStream_t s) { t_stream = s; }
 
 // ------------------------------------------------------------- profiling
 struct ProfRec { cudaEvent_t a, b; int cls; double flops; };

@@ -39,6 +39,7 @@ extern std::atomic<long long> g_launches;
   } while (0)
 
 cudaStream_t stream();
+void set_thread_stream(cudaStream_t s);   // nullptr: back to the library stream
 int ensure_device();
 
 // kernel-class profiling (CUDA events around launches when enabled)
@@ -157,16 +158,28 @@ namespace bg {
 int upload_geometry(bg_geometry *g);
 int build_near_lists(bg_geometry *g);
 int precompute_near(bg_geometry *g);
-int assemble_far(bg_geometry *g, double wr, double wi, void *M, size_t ld);
-int assemble_near(bg_geometry *g, double wr, double wi, void *M, size_t ld);
-int assemble_gram(bg_geometry *g, double wr, double wi, void *M, size_t ld);
-int rhs_planewave(bg_geometry *g, double wr, double wi, const double *E0, const double *nhat, void *out);
+// fq (optional, device {Re w, Im w}): omega read on the device instead of wr, wi
+int assemble_far(bg_geometry *g, double wr, double wi, void *M, size_t ld, const double *fq = nullptr);
+int assemble_near(bg_geometry *g, double wr, double wi, void *M, size_t ld, const double *fq = nullptr);
+int assemble_gram(bg_geometry *g, double wr, double wi, void *M, size_t ld, const double *fq = nullptr);
+int rhs_planewave(bg_geometry *g, double wr, double wi, const double *E0, const double *nhat, void *out,
+                  const double *fq = nullptr);
+int opft_enqueue(bg_geometry *g, double wr, double wi, const void *dJ, const double *fq, double *part,
+                 double *out_dev);
 int pft(bg_geometry *g, double wr, double wi, const void *dJ, const double *E0, const double *nhat, int method,
         double *out);
 int lu_factor(bg_matrix *m);
 int lu_solve(bg_matrix *m, void *dB, int ldb, int nrhs);
 int lu_solve_status(bg_matrix *m);
 int lu_solve_noalloc(bg_matrix *m, void *dB, int ldb, int nrhs);
+// capture-safe factor/solve (batched sweeps; complex128)
+int lu_capture_prepare(bg_matrix *m);
+int lu_factor_enqueue(bg_matrix *m);
+int *lu_capture_info_ptr(bg_matrix *m);
+int *lu_capture_solve_err_ptr(bg_matrix *m);
+int lu_solve_enqueue(bg_matrix *m, void *dB, int ldb, int nrhs, void *dT);
+void lu_set_panel_rows(int rows);
+int lu_get_panel_rows();
 int gmres_solve(bg_matrix *A, const bg_precond *P, void *dB, int ldb, int nrhs, double tol, int restart, int maxit,
                 double *stats);
 int gmres_solve_mixed(bg_matrix *A, bg_matrix *F, const bg_precond *P, void *dB, int ldb, int nrhs, double tol,

@@ -197,7 +197,19 @@ struct BFSide {   // staged per basis function and side
   double coef;    // +-area
 };
 
-__global__ void __launch_bounds__(FT * FT) k_far(DevGeom g, cd k, cd invk2, cd *M, size_t ld) {
+// Frequency-parameterised launches: when fq (device, {Re w, Im w}) is
+// given, the kernels below read omega from it instead of their by-value
+// arguments, so that one captured CUDA graph serves every frequency.
+__device__ __forceinline__ cd dev_invk2(double wr, double wi) {
+  double d = (wr * wr - wi * wi) * (wr * wr - wi * wi) + 4 * wr * wr * wi * wi;
+  return cd{(wr * wr - wi * wi) / d, -2 * wr * wi / d};
+}
+
+__global__ void __launch_bounds__(FT * FT) k_far(DevGeom g, cd k, cd invk2, cd *M, size_t ld, const double *fq) {
+  if (fq) {
+    k = cd{fq[0], fq[1]};
+    invk2 = dev_invk2(fq[0], fq[1]);
+  }
   int bx = blockIdx.x, by = blockIdx.y;
   if (bx > by) return;
   __shared__ BFSide sA[FT][2], sB[FT][2];
@@ -267,7 +279,7 @@ __global__ void __launch_bounds__(FT * FT) k_far(DevGeom g, cd k, cd invk2, cd *
   if (a != b) M[(size_t)b + (size_t)a * ld] = acc;
 }
 
-int assemble_far(bg_geometry *g, double wr, double wi, void *M, size_t ld) {
+int assemble_far(bg_geometry *g, double wr, double wi, void *M, size_t ld, const double *fq) {
   int st = init_tables();
   if (st) return st;
   cd k{wr, wi};
@@ -276,7 +288,7 @@ int assemble_far(bg_geometry *g, double wr, double wi, void *M, size_t ld) {
   cd invk2{(wr * wr - wi * wi) / d, -2 * wr * wi / d};
   int nb = (g->N + FT - 1) / FT;
   dim3 grid(nb, nb), block(FT, FT);
-  k_far<<<grid, block, 0, stream()>>>(g->dev, k, invk2, (cd *)M, ld);
+  k_far<<<grid, block, 0, stream()>>>(g->dev, k, invk2, (cd *)M, ld, fq);
   BG_LAUNCHED();
   return BG_OK;
 }
@@ -544,7 +556,11 @@ int precompute_near(bg_geometry *g) {
 //   G = BFBFInt[(e^{ikr}-1-ikr-(ikr)^2/2)/4 pi r] + (F0-F1/k^2) + ik(F2-F3/k^2)
 //       + (ik)^2 (F4-F5/k^2)
 // =========================================================================
-__global__ void k_near(DevGeom g, NearData nd, cd k, cd invk2, cd *M, size_t ld) {
+__global__ void k_near(DevGeom g, NearData nd, cd k, cd invk2, cd *M, size_t ld, const double *fq) {
+  if (fq) {
+    k = cd{fq[0], fq[1]};
+    invk2 = dev_invk2(fq[0], fq[1]);
+  }
   int kk = blockIdx.x * blockDim.x + threadIdx.x;
   if (kk >= nd.npairs) return;
   int2 ab = nd.pairs[kk];
@@ -589,12 +605,12 @@ __global__ void k_near(DevGeom g, NearData nd, cd k, cd invk2, cd *M, size_t ld)
   if (a != b) M[(size_t)b + (size_t)a * ld] = acc;
 }
 
-int assemble_near(bg_geometry *g, double wr, double wi, void *M, size_t ld) {
+int assemble_near(bg_geometry *g, double wr, double wi, void *M, size_t ld, const double *fq) {
   NearData &nd = g->near;
   if (nd.npairs == 0) return BG_OK;
   double d = (wr * wr - wi * wi) * (wr * wr - wi * wi) + 4 * wr * wr * wi * wi;
   cd invk2{(wr * wr - wi * wi) / d, -2 * wr * wi / d};
-  k_near<<<(nd.npairs + 127) / 128, 128, 0, stream()>>>(g->dev, nd, cd{wr, wi}, invk2, (cd *)M, ld);
+  k_near<<<(nd.npairs + 127) / 128, 128, 0, stream()>>>(g->dev, nd, cd{wr, wi}, invk2, (cd *)M, ld, fq);
   BG_LAUNCHED();
   return BG_OK;
 }
@@ -606,7 +622,8 @@ int assemble_near(bg_geometry *g, double wr, double wi, void *M, size_t ld) {
 // Added to M(a,b) and M(b,a) for b >= a (the reference adds the full row and
 // its symmetric fill then overwrites the lower triangle with the upper).
 // =========================================================================
-__global__ void k_gram(DevGeom g, double w, cd *M, size_t ld) {
+__global__ void k_gram(DevGeom g, double w, cd *M, size_t ld, const double *fq) {
+  if (fq) w = fq[0];
   int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= g.N) return;
   int2 tt = g.bfTet[a], qq = g.bfQ[a];
@@ -675,9 +692,9 @@ __global__ void k_gram(DevGeom g, double w, cd *M, size_t ld) {
   }
 }
 
-int assemble_gram(bg_geometry *g, double wr, double wi, void *M, size_t ld) {
+int assemble_gram(bg_geometry *g, double wr, double wi, void *M, size_t ld, const double *fq) {
   (void)wi;
-  k_gram<<<(g->N + 127) / 128, 128, 0, stream()>>>(g->dev, wr, (cd *)M, ld);
+  k_gram<<<(g->N + 127) / 128, 128, 0, stream()>>>(g->dev, wr, (cd *)M, ld, fq);
   BG_LAUNCHED();
   return BG_OK;
 }
@@ -724,7 +741,13 @@ __device__ __forceinline__ cd bf_dot_field(const DevGeom &g, int a, const PWave 
   return tot;
 }
 
-__global__ void k_rhs(DevGeom g, PWave pw, cd pre, cd *out) {
+__global__ void k_rhs(DevGeom g, PWave pw, cd pre, cd *out, const double *fq) {
+  if (fq) {
+    // -1/(i w Z0) = i/(w Z0)
+    double wr = fq[0], wi = fq[1], d = (wr * wr + wi * wi) * 376.73031346177;
+    pw.k = cd{wr, wi};
+    pre = cd{wi / d, wr / d};
+  }
   int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= g.N) return;
   out[a] = cmul(pre, bf_dot_field(g, a, pw));
@@ -737,7 +760,8 @@ static PWave make_pw(double wr, double wi, const double *E0, const double *nhat)
   return pw;
 }
 
-int rhs_planewave(bg_geometry *g, double wr, double wi, const double *E0, const double *nhat, void *out) {
+int rhs_planewave(bg_geometry *g, double wr, double wi, const double *E0, const double *nhat, void *out,
+                  const double *fq) {
   int st = init_tables();
   if (st) return st;
   PWave pw = make_pw(wr, wi, E0, nhat);
@@ -745,7 +769,7 @@ int rhs_planewave(bg_geometry *g, double wr, double wi, const double *E0, const 
   const double Z0 = 376.73031346177;
   double d = (wr * wr + wi * wi) * Z0;
   cd pre{wi / d, wr / d};
-  k_rhs<<<(g->N + 127) / 128, 128, 0, stream()>>>(g->dev, pw, pre, (cd *)out);
+  k_rhs<<<(g->N + 127) / 128, 128, 0, stream()>>>(g->dev, pw, pre, (cd *)out, fq);
   BG_LAUNCHED();
   return BG_OK;
 }
@@ -947,7 +971,12 @@ __global__ void k_pft_ext(PftArgs P, PWave pw, double *part) {
 // OPFT absorbed power (OPFT.cc:62-119, OverlapIntegrand_PFT PAbs term,
 // OverlapIntegrals.cc:79-170,242-298): sum Re(conj(Ja) Jb ME_ab),
 // ME_ab = 1/2 int b_a . (i Z0/w)(eps-1)^-1 . b_b on the shared tetrahedron.
-__global__ void k_opft(PftArgs P, cd omega, double *part) {
+__global__ void k_opft(PftArgs P, cd omega, double *part, const double *fq) {
+  if (fq) {
+    omega = cd{fq[0], fq[1]};
+    P.w = fq[0];
+    P.absw = sqrt(fq[0] * fq[0] + fq[1] * fq[1]);
+  }
   int a = blockIdx.x * blockDim.x + threadIdx.x;
   const DevGeom &g = P.g;
   double contrib = 0.0;
@@ -1043,7 +1072,7 @@ int pft(bg_geometry *g, double wr, double wi, const void *dJ, const double *E0, 
   int nrow = (g->N + 127) / 128;
   if (method == BG_PFT_OVERLAP) {
     if ((st = ensure_scratch(g, sizeof(double) * nrow * NO))) return st;
-    k_opft<<<nrow, 128, 0, stream()>>>(P, cd{wr, wi}, g->d_scratch);
+    k_opft<<<nrow, 128, 0, stream()>>>(P, cd{wr, wi}, g->d_scratch, nullptr);
     BG_LAUNCHED();
     std::vector<double> h((size_t)nrow * NO);
     BG_CUDA_TRY(cudaMemcpyAsync(h.data(), g->d_scratch, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, stream()));
@@ -1090,6 +1119,37 @@ int pft(bg_geometry *g, double wr, double wi, const void *dJ, const double *E0, 
     out[2 * o] = 0.5 * ext[o] - ps;
     out[2 * o + 1] = ps;
   }
+  return BG_OK;
+}
+
+// Absorbed power per object by the overlap method with every number kept on
+// the device (for captured graphs): partial sums into part (ceil(N/128) x NO
+// doubles), then out[o] = sum over blocks, o < NO.
+__global__ void k_opft_reduce(int nrow, int nobj, const double *part, double *out) {
+  int o = blockIdx.x;
+  double s = 0;
+  for (int b = threadIdx.x; b < nrow; b += blockDim.x) s += part[(size_t)b * nobj + o];
+  s = warp_sum(s);
+  __shared__ double red[8];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
+    out[o] = t;
+  }
+}
+
+int opft_enqueue(bg_geometry *g, double wr, double wi, const void *dJ, const double *fq, double *part,
+                 double *out_dev) {
+  int NO = (int)g->objs.size();
+  if (NO > PMAXOBJ) { set_error("PFT supports at most %d objects", PMAXOBJ); return BG_ERR_ARG; }
+  PftArgs P{g->dev, (const cd *)dJ, wr, std::sqrt(wr * wr + wi * wi), NO};
+  int nrow = (g->N + 127) / 128;
+  k_opft<<<nrow, 128, 0, stream()>>>(P, cd{wr, wi}, part, fq);
+  BG_LAUNCHED();
+  k_opft_reduce<<<NO, 256, 0, stream()>>>(nrow, NO, part, out_dev);
+  BG_LAUNCHED();
   return BG_OK;
 }
 

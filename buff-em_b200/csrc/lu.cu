@@ -907,4 +907,130 @@ int lu_solve_noalloc(bg_matrix *m, void *dB, int ldb, int nrhs) {
   return st;
 }
 
+// =========================================================================
+// Capture-safe factor and solve for the batched frequency sweeps: no host
+// synchronisation and no allocation between lu_capture_prepare() and the
+// end of the solve, so the whole sequence can be recorded into a CUDA graph
+// and replayed.  The pivot permutation is built on the device, the
+// factorisation status stays in the workspace (lu_capture_info), and the
+// solve clears its ready flags itself on every replay (epoch 1).
+// =========================================================================
+
+// perm = composition of the interchanges ipiv (1-based), one block; the
+// sequential swaps run in shared memory when 8 N bytes fit, else in global
+__global__ void k_build_perm(int N, const int *ipiv, int *perm, int use_smem) {
+  extern __shared__ int sp[];
+  int *p = use_smem ? sp : perm;
+  const int *iv = ipiv;
+  int *ivs = use_smem ? sp + N : nullptr;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    p[i] = i;
+    if (use_smem) ivs[i] = ipiv[i];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int *q = use_smem ? ivs : iv;
+    for (int i = 0; i < N; i++) {
+      int j = q[i] - 1, t = p[i];
+      p[i] = p[j];
+      p[j] = t;
+    }
+  }
+  __syncthreads();
+  if (use_smem)
+    for (int i = threadIdx.x; i < N; i += blockDim.x) perm[i] = p[i];
+}
+
+static size_t lu_work_bytes(bg_matrix *m) {
+  const size_t csz = m->precision == BG_C128 ? sizeof(cdl) : sizeof(cfl);
+  return csz * 2 * panel_grid * 32 + csz * 64 + sizeof(double) * 2 * panel_grid + sizeof(int) * 2 * panel_grid + 256;
+}
+
+// allocates everything the captured factor/solve touch (complex128 only)
+int lu_capture_prepare(bg_matrix *m) {
+  int st = ensure_device();
+  if (!st) st = panel_init();
+  if (st) return st;
+  if (m->precision != BG_C128) { set_error("batched sweeps factor complex128 matrices"); return BG_ERR_ARG; }
+  size_t need = lu_work_bytes(m);
+  if (m->work_bytes < need) {
+    if (m->d_work) cudaFree(m->d_work);
+    m->d_work = nullptr;
+    m->work_bytes = 0;
+    BG_CUDA_TRY(cudaMalloc(&m->d_work, need));
+    m->work_bytes = need;
+  }
+  int N = m->N;
+  if (!m->d_perm) BG_CUDA_TRY(cudaMalloc(&m->d_perm, sizeof(int) * (N + 2 * ((N + TV_B - 1) / TV_B) + 8)));
+  BG_CUDA_TRY(cudaMemsetAsync(m->d_perm + N, 0, sizeof(int) * (2 * ((N + TV_B - 1) / TV_B) + 8), stream()));
+  BG_CUDA_TRY(cudaStreamSynchronize(stream()));
+  static bool attr = false;
+  if (!attr) {
+    BG_CUDA_TRY(cudaFuncSetAttribute(k_build_perm, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    attr = true;
+  }
+  return BG_OK;
+}
+
+void lu_set_panel_rows(int rows) { panel_rows_target = std::max(8, rows); }
+int lu_get_panel_rows() { return panel_rows_target; }
+
+int lu_factor_enqueue(bg_matrix *m) {
+  int N = m->N;
+  char *w = (char *)m->d_work;
+  LUWork W;
+  W.crow = (void *)w; w += sizeof(cdl) * 2 * panel_grid * 32;
+  W.jrow = (void *)w; w += sizeof(cdl) * 64;
+  W.cval = (double *)w; w += sizeof(double) * 2 * panel_grid;
+  W.cidx = (int *)w; w += sizeof(int) * 2 * panel_grid;
+  W.info = (int *)w;
+  BG_CUDA_TRY(cudaMemsetAsync(W.info, 0, 2 * sizeof(int), stream()));
+  int st = getrf_rec<cdl>(m, W, 0, N);
+  if (st) return st;
+  int use_smem = (size_t)8 * N <= 200 * 1024;
+  k_build_perm<<<1, 1024, use_smem ? 8 * (size_t)N : 0, stream()>>>(N, m->d_ipiv, m->d_perm, use_smem);
+  BG_LAUNCHED();
+  m->factored = true;
+  return BG_OK;
+}
+
+// device address of the factorisation status of the last captured factor
+// (LAPACK info; 0 = ok) and of the triangular sweeps' sticky error word
+int *lu_capture_info_ptr(bg_matrix *m) {
+  char *w = (char *)m->d_work + sizeof(cdl) * 2 * panel_grid * 32 + sizeof(cdl) * 64 +
+            sizeof(double) * 2 * panel_grid + sizeof(int) * 2 * panel_grid;
+  return (int *)w;
+}
+int *lu_capture_solve_err_ptr(bg_matrix *m) {
+  int nb = (m->N + TV_B - 1) / TV_B;
+  return m->d_perm + m->N + 2 * nb + 2;
+}
+
+// B (N x nrhs, nrhs <= TV_MAXRHS) <- A^{-1} B with T an N x nrhs device scratch
+int lu_solve_enqueue(bg_matrix *m, void *dB, int ldb, int nrhs, void *dT) {
+  int N = m->N;
+  if (nrhs > TV_MAXRHS) { set_error("captured solve: at most %d right-hand sides", TV_MAXRHS); return BG_ERR_ARG; }
+  const cdl *A = (const cdl *)m->d;
+  cdl *B = (cdl *)dB, *T = (cdl *)dT;
+  const int nb = (N + TV_B - 1) / TV_B;
+  int *flagsL = m->d_perm + N, *flagsU = flagsL + nb, *tick = flagsU + nb, *err = tick + 2;
+  const int smem = TV_B * (TV_B + 1) * (int)sizeof(cdl) + TV_B * TV_MAXRHS * (int)sizeof(cdl);
+  static bool attr = false;
+  if (!attr) {
+    BG_CUDA_TRY(cudaFuncSetAttribute(k_trsv<cdl, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    BG_CUDA_TRY(cudaFuncSetAttribute(k_trsv<cdl, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    attr = true;
+  }
+  BG_CUDA_TRY(cudaMemsetAsync(flagsL, 0, sizeof(int) * (2 * nb + 2), stream()));
+  k_gather_rows<cdl><<<dim3((N + 255) / 256, nrhs), 256, 0, stream()>>>(N, nrhs, m->d_perm, B, ldb, T, N);
+  BG_LAUNCHED();
+  k_trsv<cdl, false><<<nb, 128, smem, stream()>>>(N, A, m->ld, T, N, nrhs, flagsL, 1, tick, err);
+  BG_LAUNCHED();
+  k_trsv<cdl, true><<<nb, 128, smem, stream()>>>(N, A, m->ld, T, N, nrhs, flagsU, 1, tick + 1, err);
+  BG_LAUNCHED();
+  BG_CUDA_TRY(cudaMemcpy2DAsync(B, sizeof(cdl) * ldb, T, sizeof(cdl) * N, sizeof(cdl) * N, nrhs,
+                                cudaMemcpyDeviceToDevice, stream()));
+  return BG_OK;
+}
+
 }  // namespace bg

@@ -264,6 +264,35 @@ int bg_precond_bound(const bg_precond *P, double *rho, double *smax);
 int bg_precond_download(const bg_precond *P, int *rowptr, int *col, double *val);
 
 /* ---------------------------------------------------------------------------
+ * batching form: frequency sweeps over several geometries
+ * (no reference counterpart; the reference assembles and factors one
+ * frequency at a time: SWGGeometry::AssembleVIEMatrix, VIEMatrix.cc:431-460,
+ * then HMatrix::LUFactorize / LUSolve)
+ * ------------------------------------------------------------------------- */
+
+#define BG_BATCH_MAXOBJ 4          /* objects per geometry in a sweep */
+#define BG_BATCH_NO_GRAPHS 1       /* flags: launch every job directly, no CUDA graphs */
+
+/* For every geometry geoms[i] and every omega[j] (complex, 2 doubles each):
+   assemble the complex128 VIE matrix, LU-factor it, solve the plane wave
+   (E0: 3 complex, nhat: 3 real) and write the absorbed power of each object
+   (overlap method, as bg_pft with BG_PFT_OVERLAP) to
+   pabs[(i * nomega + j) * BG_BATCH_MAXOBJ + object] (unused entries 0).
+   Each geometry's launch sequence is recorded once per concurrent slot into
+   a CUDA graph whose kernels read omega from device memory, and replayed per
+   frequency; up to max_streams slots run concurrently.  An online autotuner
+   picks, per size class (N rounded up to 1024), the LU panel slice height
+   (16/32/64 rows per CTA) and the slot count (1, 2, 4, ... <= max_streams)
+   by timing the sweep's own first jobs, and keeps the choice for later
+   geometries of that class.  stats (may be NULL; 4 + 3*ngeom doubles): wall
+   seconds, jobs, graphs requested, 1 if a capture fell back to direct
+   launches; then per geometry the chosen panel rows, slots and seconds per
+   job measured while tuning (0 if the class was already tuned).
+   Returns BG_ERR_NUMERIC if a matrix was singular. */
+int bg_batch_sweep(bg_geometry *const *geoms, int ngeom, const double *omega, int nomega, const double *E0,
+                   const double *nhat, int max_streams, int flags, double *pabs, double *stats);
+
+/* ---------------------------------------------------------------------------
  * right-hand side and post-processing
  * ------------------------------------------------------------------------- */
 

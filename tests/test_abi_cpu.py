@@ -80,3 +80,16 @@ def test_compute_without_gpu_fails_loudly(buffem_lib, sphere):
         G.AllocateVIEMatrix()
     assert e.value.status == -4
     assert "no CPU fallback" in str(e.value) or "CUDA" in str(e.value)
+
+
+def test_batch_sweep_rejects_bad_arguments(buffem_lib):
+    import ctypes as C
+    import numpy as np
+    L = buffem_lib.lib()
+    w = np.array([1.0, 0.0])
+    E0 = np.zeros(6)
+    nh = np.array([0.0, 0.0, 1.0])
+    out = np.zeros(4)
+    st = L.bg_batch_sweep(None, 1, w.ctypes.data_as(C.c_void_p), 1, E0.ctypes.data_as(C.c_void_p),
+                          nh.ctypes.data_as(C.c_void_p), 1, 0, out.ctypes.data_as(C.c_void_p), None)
+    assert st == buffem_lib.BG_ERR_ARG
