@@ -54,6 +54,9 @@ EPS_LEARNED = 6 + 0.5j
 WAVES = [([1, 0, 0], [0, 0, 1]), ([0, 1, 0], [0, 0, 1]), ([0, 0, 1], [1, 0, 0])]
 OMEGA = 1.0
 GMRES = dict(tol=1e-10, restart=50, maxit=1000, inner_tol=1e-5)
+# ncu --set full capture of k_gm_matvec_part_c64 (one launch, N = 19,872):
+# dram__bytes_read.sum + dram__bytes_write.sum
+MATVEC_NCU_N, MATVEC_NCU_BYTES = 19872, 3.160269e9 + 21.617664e6
 
 
 def eps_tensor():
@@ -606,7 +609,10 @@ def main():
             "roofline": {"bound": "hbm", "kernel": "k_gm_matvec_part_c64 (+ k_gm_matvec_sum): GMRES matrix-vector "
                                                    "products on the complex64 matrix",
                          "achieved": mv_gbs, "peak": hbm, "unit": "GB/s",
-                         "frac": (mv_gbs / hbm) if (mv_gbs and hbm) else None, "traffic": None,
+                         "frac": (mv_gbs / hbm) if (mv_gbs and hbm) else None,
+                         "traffic": MATVEC_NCU_BYTES * (N / MATVEC_NCU_N) ** 2,
+                         "traffic_source": f"ncu dram read+write of one launch at N={MATVEC_NCU_N} "
+                                           f"({MATVEC_NCU_BYTES:.4g} B), scaled by N^2",
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if hbm else "unavailable",
                          "algorithmic": "8 N^2 bytes of matrix per product (3 right-hand sides share one pass; "
                                         "16 N^2 for the complex128 residual products)",
