@@ -488,7 +488,7 @@ def synchronize():
 
 
 PROF_CLASSES = ("lu_gemm", "lu_panel", "lu_laswp", "trsm_leaf", "assemble_far", "assemble_near_gram",
-                "gmres_matvec", "gnn_precond")
+                "gmres_matvec", "gnn_precond", "gmres_orthogonalise", "gmres_precond_apply")
 
 
 def profile_begin():

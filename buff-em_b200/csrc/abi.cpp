@@ -76,12 +76,12 @@ bool prof_on() { return s_prof; }
 void prof_start(int cls) {
   if (!s_prof) return;
   s_open[cls] = take_event();
-  cudaEventRecord(s_open[cls], s_stream);
+  cudaEventRecord(s_open[cls], stream());
 }
 void prof_stop(int cls, double flops) {
   if (!s_prof) return;
   cudaEvent_t e = take_event();
-  cudaEventRecord(e, s_stream);
+  cudaEventRecord(e, stream());
   s_recs.push_back(ProfRec{s_open[cls], e, cls, flops});
 }
 
@@ -157,6 +157,7 @@ void bg_geometry_destroy(bg_geometry *g) {
   DevGeom &d = g->dev;
   dfree(d.V4); dfree(d.tetVI); dfree(d.tetVol); dfree(d.tetP4); dfree(d.tetObj); dfree(d.bfTet);
   dfree(d.bfQ); dfree(d.bfLoc); dfree(d.tetFI); dfree(d.bfV); dfree(d.bfArea); dfree(d.bfRadius); dfree(d.mats); dfree(d.objOrigin);
+  dfree(d.tileTet); dfree(d.tileNT); dfree(d.bfTileLoc);
   NearData &n = g->near;
   dfree(n.pairs); dfree(n.pairTP); dfree(n.fibbi); dfree(n.tp); dfree(n.tpOrdA); dfree(n.tpOrdB); dfree(n.tpMom);
   dfree(g->graph.rowptr); dfree(g->graph.col); dfree(g->graph.etr);

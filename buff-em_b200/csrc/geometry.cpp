@@ -248,8 +248,30 @@ int upload_geometry(bg_geometry *g) {
     mats.push_back(o.mat);
     for (int k = 0; k < 3; k++) origin.push_back(o.origin[k]);
   }
+  // far-field tiles: distinct tetrahedra of each run of BG_FAR_TILE basis functions
+  int ntile = (g->N + BG_FAR_TILE - 1) / BG_FAR_TILE;
+  std::vector<int> tileTet((size_t)ntile * BG_FAR_TILE_TETS, -1), tileNT(ntile, 0);
+  std::vector<int2> bfTileLoc(g->N);
+  for (int t = 0; t < ntile; t++) {
+    int *list = tileTet.data() + (size_t)t * BG_FAR_TILE_TETS;
+    int cnt = 0;
+    auto slot = [&](int tet) {
+      for (int i = 0; i < cnt; i++)
+        if (list[i] == tet) return i;
+      list[cnt] = tet;
+      return cnt++;
+    };
+    for (int a = t * BG_FAR_TILE; a < std::min(g->N, (t + 1) * BG_FAR_TILE); a++) {
+      int lp = slot(bfTet[a].x);
+      int lm = slot(bfTet[a].y);
+      bfTileLoc[a] = make_int2(lp, lm);
+    }
+    tileNT[t] = cnt;
+  }
   DevGeom &d = g->dev;
   d.N = g->N; d.NT = g->NT; d.NV = g->NV;
+  if ((st = dupload(&d.tileTet, tileTet)) || (st = dupload(&d.tileNT, tileNT)) || (st = dupload(&d.bfTileLoc, bfTileLoc)))
+    return st;
   if ((st = dupload(&d.V4, V4)) || (st = dupload(&d.tetVI, tetVI)) || (st = dupload(&d.tetVol, tetVol)) ||
       (st = dupload(&d.tetP4, tetP4)) || (st = dupload(&d.tetObj, tetObj)) || (st = dupload(&d.bfTet, bfTet)) ||
       (st = dupload(&d.bfQ, bfQ)) || (st = dupload(&d.bfLoc, bfLoc)) || (st = dupload(&d.tetFI, tetFI)) || (st = dupload(&d.bfV, bfV)) || (st = dupload(&d.bfArea, area)) ||

@@ -262,6 +262,7 @@ static int dense_matvec(bg_matrix *A, const z2 *X, z2 *Y, GmState &S) {
 
 static int precond(const bg_precond *P, const z2 *X, z2 *Y, GmState &S) {
   int N = S.N;
+  if (P) prof_start(PROF_PRECOND);
   if (!P) {
     BG_CUDA_TRY(cudaMemcpyAsync(Y, X, sizeof(z2) * (size_t)N * S.nrhs, cudaMemcpyDeviceToDevice, stream()));
     return BG_OK;
@@ -269,6 +270,7 @@ static int precond(const bg_precond *P, const z2 *X, z2 *Y, GmState &S) {
   k_gm_spmv<<<dim3((N + 127) / 128, S.nrhs), 128, 0, stream()>>>(N, P->rowptr, P->col, (const z2 *)P->val, X, N,
                                                                  S.nrhs, Y, N);
   BG_LAUNCHED();
+  prof_stop(PROF_PRECOND, 0.0);
   return BG_OK;
 }
 
@@ -355,6 +357,7 @@ int gmres_solve(bg_matrix *A, const bg_precond *P, void *dB, int ldb, int nrhs, 
       if ((st = dense_matvec(A, S.Z, S.W, S))) break;
       // CGS2
       std::vector<zc> hcol((size_t)nrhs * (k + 2), 0.0);
+      prof_start(PROF_ORTHO);
       for (int pass = 0; pass < 2; pass++) {
         k_gm_dots<<<dim3(k + 1, nrhs), 256, 0, stream()>>>(N, k + 1, S.V, N, vstride, S.W, N, S.dots);
         g_launches++;
@@ -368,6 +371,7 @@ int gmres_solve(bg_matrix *A, const bg_precond *P, void *dB, int ldb, int nrhs, 
       }
       std::vector<double> wn;
       if ((st = colnorms(S.W, S, wn))) break;
+      prof_stop(PROF_ORTHO, 0.0);
       for (int j = 0; j < nrhs; j++) {
         hcol[(size_t)j * (k + 2) + k + 1] = wn[j];
         inv[j] = wn[j] > 0 ? 1.0 / wn[j] : 0.0;

@@ -13,6 +13,9 @@
 
 namespace bg {
 
+#define BG_FAR_TILE 32                      // basis functions per far-field tile
+#define BG_FAR_TILE_TETS (2 * BG_FAR_TILE)  // distinct tetrahedra per tile, at most
+
 // ---------------------------------------------------------------- errors
 void set_error(const char *fmt, ...);
 extern std::atomic<long long> g_launches;
@@ -45,7 +48,7 @@ int ensure_device();
 // kernel-class profiling (CUDA events around launches when enabled)
 enum {
   PROF_GEMM = 0, PROF_PANEL = 1, PROF_LASWP = 2, PROF_TRSM = 3, PROF_ASM_FAR = 4, PROF_ASM_NEAR = 5,
-  PROF_MATVEC = 6, PROF_GNN = 7, PROF_NCLASS = 8
+  PROF_MATVEC = 6, PROF_GNN = 7, PROF_ORTHO = 8, PROF_PRECOND = 9, PROF_NCLASS = 12
 };
 bool prof_on();
 void prof_start(int cls);
@@ -93,6 +96,12 @@ struct DevGeom {
   double *bfRadius = nullptr;
   bg_material *mats = nullptr;  // per object
   double *objOrigin = nullptr;  // 3 per object
+  // far-field tiles of BG_FAR_TILE consecutive basis functions: the distinct
+  // tetrahedra of each tile (<= 2 per basis function) and, per basis
+  // function, the positions of its P and M tetrahedra in its tile's list
+  int *tileTet = nullptr;       // BG_FAR_TILE_TETS per tile, -1 padded
+  int *tileNT = nullptr;        // number of distinct tetrahedra per tile
+  int2 *bfTileLoc = nullptr;
 };
 
 struct NearData {

@@ -183,18 +183,37 @@ __device__ __forceinline__ double warp_sum(double v) {
 }
 
 // =========================================================================
-// far field: one thread per basis-function pair (a <= b) with no common
-// vertex; 4 tetrahedron pairs x 4x4 points of the Helmholtz kernel
-// (GetGME_BFBFInt, GMatrixElements.cc:270-288; BFBFInt, Cubature.cc:476-527).
-// With w = 6V w_i (w_i = 1/24) and b = +-A/(3V)(x - Q) the volume cancels:
+// far field (GetGME_BFBFInt, GMatrixElements.cc:270-288; BFBFInt,
+// Cubature.cc:476-527): for a basis-function pair (a, b) with no common
+// vertex, 4 tetrahedron pairs x 4x4 points of the Helmholtz kernel.  With
+// w = 6V w_i (w_i = 1/24) and b = +-A/(3V)(x - Q) the volume cancels:
 //   w_a b_a . w_b b_b = s_a s_b A_a A_b (x-Q_a).(y-Q_b)/144,
-//   w_a Div b_a w_b Div b_b = s_a s_b A_a A_b / 16.
+//   w_a Div b_a w_b Div b_b = s_a s_b A_a A_b / 16,
+// so with x~ = x - o_A, y~ = y - o_B (o = tetrahedron centroid) and
+// q = Q - o each tetrahedron pair contributes through 8 complex moments of
+// phi = exp(ikr)/(4 pi r):
+//   M0 = sum phi, M1 = sum x~ phi, M1' = sum y~ phi, M2 = sum x~.y~ phi,
+//   entry += s s' A A' [M2/144 - M0/(16k^2) - q'.M1/144 - q.M1'/144 + q.q' M0/144].
+// The moments depend on the two tetrahedra only, and a tile of 16
+// consecutive basis functions touches about 16 distinct tetrahedra (face
+// numbering follows the mesh), so a CTA computes each distinct tetrahedron
+// pair of its 16x16 tile once (about 256 instead of 1024 pairs of 16 kernel
+// evaluations) into shared memory and every thread then combines the 4
+// moment sets of its basis-function pair.
 // =========================================================================
-#define FT 16
-struct BFSide {   // staged per basis function and side
-  double pts[4][3];
-  double q[3];
-  double coef;    // +-area
+#define FT 16        // PFT tiles (k_pft_far): 16 x 16 basis functions
+#define FTF BG_FAR_TILE
+#define FTT BG_FAR_TILE_TETS
+#define FCH 8        // column tetrahedra per moment chunk
+#define FTHR 256     // threads of the far kernel: each owns 2 x 2 basis-function pairs
+
+struct FarSmem {
+  cd mom[FTT][FCH][8];          // M0, M1 (3), M1' (3), M2
+  double pA[FTT][4][3], pB[FTT][4][3];
+  double oA[FTT][3], oB[FTT][3];
+  double uA[FTF][2][4], uB[FTF][2][4];   // s A (1, Q - o) per side
+  int lA[FTF][2], lB[FTF][2];            // tile-local tetrahedron of each side
+  int vA[FTF][5], vB[FTF][5];
 };
 
 // Frequency-parameterised launches: when fq (device, {Re w, Im w}) is
@@ -205,78 +224,161 @@ __device__ __forceinline__ cd dev_invk2(double wr, double wi) {
   return cd{(wr * wr - wi * wi) / d, -2 * wr * wi / d};
 }
 
-__global__ void __launch_bounds__(FT * FT) k_far(DevGeom g, cd k, cd invk2, cd *M, size_t ld, const double *fq) {
+__device__ void far_stage_tets(const DevGeom &g, int tile, double (*P)[4][3], int tid) {
+  int nt = g.tileNT[tile];
+  for (int e = tid; e < nt * 12; e += FTHR) {
+    int t = e / 12, r = e % 12;
+    int tet = g.tileTet[(size_t)tile * FTT + t];
+    P[t][r / 3][r % 3] = g.tetP4[16 * (size_t)tet + 4 * (r / 3) + (r % 3)];
+  }
+}
+
+__device__ void far_stage_bfs(const DevGeom &g, int tile, double (*P)[4][3], double (*u)[2][4], int (*l)[2],
+                              int (*v)[5], int tid) {
+  if (tid < 2 * FTF) {
+    int r = tid >> 1, s = tid & 1;
+    int bf = tile * FTF + r;
+    if (bf < g.N) {
+      int2 loc = g.bfTileLoc[bf];
+      int lt = s == 0 ? loc.x : loc.y;
+      int2 qq = g.bfQ[bf];
+      double Q[3];
+      load3(g.V4, s == 0 ? qq.x : qq.y, Q);
+      double coef = (s == 0 ? 1.0 : -1.0) * g.bfArea[bf];
+      u[r][s][0] = coef;
+      for (int c = 0; c < 3; c++) {
+        double o = 0.25 * (P[lt][0][c] + P[lt][1][c] + P[lt][2][c] + P[lt][3][c]);
+        u[r][s][1 + c] = coef * (Q[c] - o);
+      }
+      l[r][s] = lt;
+      if (s == 0) {
+        int4 vv = g.bfV[bf];
+        v[r][0] = qq.x; v[r][1] = vv.x; v[r][2] = vv.y; v[r][3] = vv.z; v[r][4] = qq.y;
+      }
+    }
+  }
+}
+
+// one CTA per 32 x 32 tile of basis-function pairs (upper triangle of tiles)
+__global__ void __launch_bounds__(FTHR, 2) k_far(DevGeom g, cd k, cd invk2, cd *M, size_t ld, const double *fq) {
   if (fq) {
     k = cd{fq[0], fq[1]};
     invk2 = dev_invk2(fq[0], fq[1]);
   }
   int bx = blockIdx.x, by = blockIdx.y;
   if (bx > by) return;
-  __shared__ BFSide sA[FT][2], sB[FT][2];
-  __shared__ int vA[FT][5], vB[FT][5];
-  int tid = threadIdx.y * FT + threadIdx.x;
-  // stage rows (a) and columns (b)
-  if (tid < 4 * FT) {
-    int which = tid / (2 * FT);           // 0: rows, 1: cols
-    int r = (tid % (2 * FT)) / 2, s = tid % 2;
-    int bf = (which == 0 ? bx : by) * FT + r;
-    BFSide *dst = which == 0 ? &sA[r][s] : &sB[r][s];
-    if (bf < g.N) {
-      int2 tt = g.bfTet[bf];
-      int2 qq = g.bfQ[bf];
-      int t = s == 0 ? tt.x : tt.y, q = s == 0 ? qq.x : qq.y;
-      for (int i = 0; i < 4; i++)
-        for (int c = 0; c < 3; c++) dst->pts[i][c] = g.tetP4[16 * (size_t)t + 4 * i + c];
-      load3(g.V4, q, dst->q);
-      dst->coef = (s == 0 ? 1.0 : -1.0) * g.bfArea[bf];
-      if (s == 0) {
-        int4 v = g.bfV[bf];
-        int *vv = which == 0 ? vA[r] : vB[r];
-        vv[0] = qq.x; vv[1] = v.x; vv[2] = v.y; vv[3] = v.z; vv[4] = qq.y;
-      }
+  extern __shared__ __align__(16) unsigned char far_smem_raw[];
+  FarSmem &S = *reinterpret_cast<FarSmem *>(far_smem_raw);
+  const int tid = threadIdx.x;
+  const int nA = g.tileNT[bx], nB = g.tileNT[by];
+  far_stage_tets(g, bx, S.pA, tid);
+  far_stage_tets(g, by, S.pB, tid);
+  __syncthreads();
+  if (tid < FTT) {
+    for (int c = 0; c < 3; c++) {
+      S.oA[tid][c] = 0.25 * (S.pA[tid][0][c] + S.pA[tid][1][c] + S.pA[tid][2][c] + S.pA[tid][3][c]);
+      S.oB[tid][c] = 0.25 * (S.pB[tid][0][c] + S.pB[tid][1][c] + S.pB[tid][2][c] + S.pB[tid][3][c]);
     }
   }
+  far_stage_bfs(g, bx, S.pA, S.uA, S.lA, S.vA, tid);
+  far_stage_bfs(g, by, S.pB, S.uB, S.lB, S.vB, tid);
   __syncthreads();
-  int ra = threadIdx.x, rb = threadIdx.y;
-  int a = bx * FT + ra, b = by * FT + rb;
-  if (a >= g.N || b >= g.N || a > b) return;
-  // CompareBFs (SWGVolume.cc:295-344): pairs with a common vertex are near
-  int ncv = 0;
+  // this thread's 2 x 2 basis-function pairs: rows tx, tx + 16; columns ty, ty + 16
+  const int tx = tid & 15, ty = tid >> 4;
+  unsigned mine = 0;   // bit 2i+j: pair (tx + 16 i, ty + 16 j) is a far pair this tile writes
+  cd acc[2][2];
 #pragma unroll
-  for (int i = 0; i < 5; i++)
+  for (int i = 0; i < 2; i++)
 #pragma unroll
-    for (int j = 0; j < 5; j++) ncv += (vA[ra][i] == vB[rb][j]);
-  if (ncv) return;
-  cd acc = cmk(0, 0);
+    for (int j = 0; j < 2; j++) {
+      int ra = tx + 16 * i, rb = ty + 16 * j;
+      int a = bx * FTF + ra, b = by * FTF + rb;
+      bool ok = a < g.N && b < g.N && a <= b;
+      if (ok) {
+        // CompareBFs (SWGVolume.cc:295-344): pairs with a common vertex are near
+        int ncv = 0;
+        for (int p = 0; p < 5; p++)
+          for (int q = 0; q < 5; q++) ncv += (S.vA[ra][p] == S.vB[rb][q]);
+        ok = ncv == 0;
+      }
+      if (ok) mine |= 1u << (2 * i + j);
+      acc[i][j] = cmk(0, 0);
+    }
   const double inv4pi = 0.25 / M_PI;
-#pragma unroll 1
-  for (int sa = 0; sa < 2; sa++)
-#pragma unroll 1
-    for (int sb = 0; sb < 2; sb++) {
-      const BFSide &A = sA[ra][sa];
-      const BFSide &B = sB[rb][sb];
-      double cc = A.coef * B.coef;
-      cd part = cmk(0, 0);
+  for (int c0 = 0; c0 < nB; c0 += FCH) {
+    int cw = min(FCH, nB - c0);
+    // moments of the distinct tetrahedron pairs (iA, c0 + jB)
+    for (int p = tid; p < nA * cw; p += FTHR) {
+      int iA = p / cw, jB = p % cw, tB = c0 + jB;
+      cd m[8];
+#pragma unroll
+      for (int q = 0; q < 8; q++) m[q] = cmk(0, 0);
 #pragma unroll
       for (int i = 0; i < 4; i++) {
-        double xa0 = A.pts[i][0], xa1 = A.pts[i][1], xa2 = A.pts[i][2];
-        double da0 = xa0 - A.q[0], da1 = xa1 - A.q[1], da2 = xa2 - A.q[2];
+        double x0 = S.pA[iA][i][0], x1 = S.pA[iA][i][1], x2 = S.pA[iA][i][2];
+        double xt0 = x0 - S.oA[iA][0], xt1 = x1 - S.oA[iA][1], xt2 = x2 - S.oA[iA][2];
+        cd phiI = cmk(0, 0);
 #pragma unroll
         for (int j = 0; j < 4; j++) {
-          double R0 = xa0 - B.pts[j][0], R1 = xa1 - B.pts[j][1], R2 = xa2 - B.pts[j][2];
+          double y0 = S.pB[tB][j][0], y1 = S.pB[tB][j][1], y2 = S.pB[tB][j][2];
+          double R0 = x0 - y0, R1 = x1 - y1, R2 = x2 - y2;
           double r = sqrt(R0 * R0 + R1 * R1 + R2 * R2);
           if (r < 1.0e-12) continue;
-          double dot = da0 * (B.pts[j][0] - B.q[0]) + da1 * (B.pts[j][1] - B.q[1]) + da2 * (B.pts[j][2] - B.q[2]);
           cd phi = cscale(expikr(k, r), inv4pi / r);
-          // PEFIE = dot/144 - invk2/16
-          cd pe = cmk(dot * (1.0 / 144.0) - invk2.r * (1.0 / 16.0), -invk2.i * (1.0 / 16.0));
-          part = cadd(part, cmul(pe, phi));
+          double yt0 = y0 - S.oB[tB][0], yt1 = y1 - S.oB[tB][1], yt2 = y2 - S.oB[tB][2];
+          phiI = cadd(phiI, phi);
+          m[4] = cadd(m[4], cscale(phi, yt0));
+          m[5] = cadd(m[5], cscale(phi, yt1));
+          m[6] = cadd(m[6], cscale(phi, yt2));
+          m[7] = cadd(m[7], cscale(phi, xt0 * yt0 + xt1 * yt1 + xt2 * yt2));
         }
+        m[0] = cadd(m[0], phiI);
+        m[1] = cadd(m[1], cscale(phiI, xt0));
+        m[2] = cadd(m[2], cscale(phiI, xt1));
+        m[3] = cadd(m[3], cscale(phiI, xt2));
       }
-      acc = cadd(acc, cscale(part, cc));
+#pragma unroll
+      for (int q = 0; q < 8; q++) S.mom[iA][jB][q] = m[q];
     }
-  M[(size_t)a + (size_t)b * ld] = acc;
-  if (a != b) M[(size_t)b + (size_t)a * ld] = acc;
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+      for (int j = 0; j < 2; j++) {
+        if (!(mine & (1u << (2 * i + j)))) continue;
+        int ra = tx + 16 * i, rb = ty + 16 * j;
+        cd accv = acc[i][j];
+#pragma unroll
+        for (int sa = 0; sa < 2; sa++)
+#pragma unroll
+          for (int sb = 0; sb < 2; sb++) {
+            int jB = S.lB[rb][sb] - c0;
+            if (jB < 0 || jB >= cw) continue;
+            const cd *m = S.mom[S.lA[ra][sa]][jB];
+            const double *u = S.uA[ra][sa], *v = S.uB[rb][sb];
+            // u0 v0 (M2/144 - M0/(16 k^2)) - u0 (v.M1)/144 - v0 (u.M1')/144 + (u.v) M0/144
+            double uv = u[1] * v[1] + u[2] * v[2] + u[3] * v[3];
+            cd t = cscale(m[7], u[0] * v[0]);
+            t = csub(t, cscale(cadd(cadd(cscale(m[1], v[1]), cscale(m[2], v[2])), cscale(m[3], v[3])), u[0]));
+            t = csub(t, cscale(cadd(cadd(cscale(m[4], u[1]), cscale(m[5], u[2])), cscale(m[6], u[3])), v[0]));
+            t = cadd(t, cscale(m[0], uv));
+            accv = cadd(accv, cscale(t, 1.0 / 144.0));
+            accv = csub(accv, cscale(cmul(invk2, m[0]), u[0] * v[0] / 16.0));
+          }
+        acc[i][j] = accv;
+      }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+      if (!(mine & (1u << (2 * i + j)))) continue;
+      int a = bx * FTF + tx + 16 * i, b = by * FTF + ty + 16 * j;
+      cd v = acc[i][j];
+      M[(size_t)a + (size_t)b * ld] = v;
+      if (a != b) M[(size_t)b + (size_t)a * ld] = v;
+    }
 }
 
 int assemble_far(bg_geometry *g, double wr, double wi, void *M, size_t ld, const double *fq) {
@@ -286,9 +388,14 @@ int assemble_far(bg_geometry *g, double wr, double wi, void *M, size_t ld, const
   // 1/k^2
   double d = (wr * wr - wi * wi) * (wr * wr - wi * wi) + 4 * wr * wr * wi * wi;
   cd invk2{(wr * wr - wi * wi) / d, -2 * wr * wi / d};
-  int nb = (g->N + FT - 1) / FT;
-  dim3 grid(nb, nb), block(FT, FT);
-  k_far<<<grid, block, 0, stream()>>>(g->dev, k, invk2, (cd *)M, ld, fq);
+  int nb = (g->N + FTF - 1) / FTF;
+  dim3 grid(nb, nb);
+  static bool attr = false;
+  if (!attr) {
+    BG_CUDA_TRY(cudaFuncSetAttribute(k_far, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(FarSmem)));
+    attr = true;
+  }
+  k_far<<<grid, FTHR, sizeof(FarSmem), stream()>>>(g->dev, k, invk2, (cd *)M, ld, fq);
   BG_LAUNCHED();
   return BG_OK;
 }

@@ -328,11 +328,12 @@ void *bg_stream(void);
    bg_profile_begin() clears and enables it; bg_profile_read() synchronises and
    returns, per kernel class, the number of timed regions, summed
    milliseconds and an algorithmic work count (counts/ms/flops arrays of
-   length n <= 8): 0 LU trailing GEMM (flops), 1 LU panel (flops), 2 row
+   length n <= 12): 0 LU trailing GEMM (flops), 1 LU panel (flops), 2 row
    interchanges, 3 triangular-solve leaves (flops), 4 far-field assembly
    (point-pair kernel evaluations, 64 per basis-function pair), 5 near-field
    and Gram assembly, 6 GMRES dense matrix-vector products (matrix bytes
-   read), 7 learned-preconditioner inference. */
+   read), 7 learned-preconditioner inference, 8 GMRES Gram-Schmidt steps
+   (including their host reads), 9 preconditioner applications. */
 int bg_profile_begin(void);
 int bg_profile_read(int n, long long *counts, double *ms, double *flops);
 int bg_profile_end(void);
