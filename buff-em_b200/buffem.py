@@ -80,6 +80,7 @@ EXPORTS = [
     "bg_gnn_get_params", "bg_gnn_set_params", "bg_gnn_get_grads", "bg_gnn_train_step",
     "bg_precond_create_learned", "bg_precond_download", "bg_gmres_solve_mixed", "bg_gmres_solve_mixed_device",
     "bg_precond_bound", "bg_gmres_solve_lu_fallback", "bg_gmres_solve_lu_fallback_device", "bg_batch_sweep",
+    "bg_pft_full",
 ]
 
 
@@ -138,6 +139,7 @@ def lib():
         L.bg_rhs_planewave.argtypes = [P, D, D, VP, VP, VP]
         L.bg_rhs_planewave_device.argtypes = [P, D, D, VP, VP, VP]
         L.bg_pft.argtypes = [P, D, D, VP, VP, VP, I, VP]
+        L.bg_pft_full.argtypes = [P, D, D, VP, VP, VP, VP]
         L.bg_kernel_launch_count.restype = C.c_longlong
         L.bg_stream.restype = VP
         L.bg_profile_read.argtypes = [I, VP, VP, VP]
@@ -308,8 +310,16 @@ class SWGGeometry:
         _check(lib().bg_rhs_planewave(self.h, Omega.real, Omega.imag, _ptr(IF.E0), _ptr(IF.nHat), _ptr(out)))
         return out
 
-    def GetPFTMatrix(self, J, Omega, IF=None, method=BG_PFT_EMT):
-        """Rows = objects, columns = (PAbs, PScat)."""
+    def GetPFTMatrix(self, J, Omega, IF=None, method=BG_PFT_EMT, full=False):
+        """Rows = objects, columns = (PAbs, PScat); with full=True (EMT only)
+        all eight columns PAbs, PScat, Fx, Fy, Fz, Tx, Ty, Tz."""
+        if full:
+            Omega = complex(Omega)
+            Jc = np.ascontiguousarray(J, dtype=np.complex128)
+            out = np.zeros((self.NumObjects, 8))
+            _check(lib().bg_pft_full(self.h, Omega.real, Omega.imag, _ptr(Jc), _ptr(IF.E0), _ptr(IF.nHat),
+                                     _ptr(out)))
+            return out
         Omega = complex(Omega)
         Jc = np.ascontiguousarray(J, dtype=np.complex128)
         out = np.zeros((self.NumObjects, 2))

@@ -576,6 +576,24 @@ int bg_pft(bg_geometry *g, double wr, double wi, const double *J, const double *
   return st;
 }
 
+int bg_pft_full(bg_geometry *g, double wr, double wi, const double *J, const double *E0, const double *nhat,
+                double *out) {
+  if (!g || !J || !out || !E0 || !nhat) { set_error("bg_pft_full: bad arguments"); return BG_ERR_ARG; }
+  if (wr == 0.0) { set_error("bg_pft_full: the force and torque columns need real(omega) != 0"); return BG_ERR_ARG; }
+  int st = upload_geometry(g);
+  if (st) return st;
+  size_t bytes = 16 * (size_t)g->N;
+  void *d = nullptr;
+  BG_CUDA_TRY(cudaMallocAsync(&d, bytes, stream()));
+  cudaError_t e = cudaMemcpyAsync(d, J, bytes, cudaMemcpyHostToDevice, stream());
+  if (e != cudaSuccess) { set_error("H2D: %s", cudaGetErrorString(e)); st = BG_ERR_CUDA; }
+  if (!st) st = pft_emt_full(g, wr, wi, d, E0, nhat, out);
+  cudaFreeAsync(d, stream());
+  cudaError_t e2 = cudaStreamSynchronize(stream());
+  if (!st && e2 != cudaSuccess) { set_error("pft: %s", cudaGetErrorString(e2)); st = BG_ERR_CUDA; }
+  return st;
+}
+
 int bg_zgemm_sub_device(int M, int N, int K, const void *A, int lda, const void *B, int ldb, void *C, int ldc) {
   if (M < 0 || N < 0 || K < 0 || (M && N && K && (!A || !B || !C)) || lda < M || ldb < K || ldc < M ||
       lda < 1 || ldb < 1 || ldc < 1) {

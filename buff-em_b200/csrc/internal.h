@@ -177,6 +177,8 @@ int opft_enqueue(bg_geometry *g, double wr, double wi, const void *dJ, const dou
                  double *out_dev);
 int pft(bg_geometry *g, double wr, double wi, const void *dJ, const double *E0, const double *nhat, int method,
         double *out);
+int pft_emt_full(bg_geometry *g, double wr, double wi, const void *dJ, const double *E0, const double *nhat,
+                 double *out);
 int lu_factor(bg_matrix *m);
 int lu_solve(bg_matrix *m, void *dB, int ldb, int nrhs);
 int lu_solve_status(bg_matrix *m);

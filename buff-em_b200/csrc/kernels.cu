@@ -903,14 +903,22 @@ __device__ __forceinline__ void rule_point(int npts, int i, double *u) {
   else { u[0] = c_tcr33[4 * i]; u[1] = c_tcr33[4 * i + 1]; u[2] = c_tcr33[4 * i + 2]; u[3] = c_tcr33[4 * i + 3]; }
 }
 
-// BFBFInt of the scattered-power integrand, lanes [lane0, lane0+nl) split the
-// point pairs; returns this lane's partial Q (complex)
-__device__ cd scat_q(const PftArgs &P, int a, int b, int npts, bool same, int lane, int nl) {
+// Full EMT PFT (EMTPFT.cc:85-127 extinction, 216-291 scattered, 396-491 sum).
+// Ten quantities per pair, NPQ order: PScat, force (3), torque from b_A x b_B
+// (3), torque from (x_A - c_A) x R (3); c_A = torque centre (object origin).
+#define NPQ 10
+#define TEN_THIRDS (10.0 / 3.0)
+
+// BFBFInt of the scattered integrand (EMTPFT.cc:216-291); lanes [lane, nl)
+// split the point pairs; q: this lane's partial integrals
+__device__ void scat_q(const PftArgs &P, int a, int b, int npts, bool same, int lane, int nl, cd q[NPQ]) {
   const DevGeom &g = P.g;
   int2 ta = g.bfTet[a], tb = g.bfTet[b], la = g.bfLoc[a], lb = g.bfLoc[b];
   double k = P.w, k2 = k * k;
-  cd tot = cmk(0, 0);
+  for (int n = 0; n < NPQ; n++) q[n] = cmk(0, 0);
   const double inv4pi = 0.25 / M_PI;
+  int oa = g.bfV[a].w;
+  const double *tc = g.objOrigin + 3 * oa;
   for (int sa = 0; sa < 2; sa++)
     for (int sb = 0; sb < 2; sb++) {
       int t1 = sa == 0 ? ta.x : ta.y, t2 = sb == 0 ? tb.x : tb.y;
@@ -952,43 +960,68 @@ __device__ cd scat_q(const PftArgs &P, int a, int b, int npts, bool same, int la
           bb[c] *= p2;
         }
         double wt = 6.0 * V1 * u[3] * 6.0 * V2 * v[3];
-        double R0 = xa[0] - xb[0], R1 = xa[1] - xb[1], R2 = xa[2] - xb[2];
-        double r2 = R0 * R0 + R1 * R1 + R2 * R2, r = sqrt(r2), kr = k * r;
+        double R[3] = {xa[0] - xb[0], xa[1] - xb[1], xa[2] - xb[2]};
+        double r2 = R[0] * R[0] + R[1] * R[1] + R[2] * R[2], r = sqrt(r2), kr = k * r;
         double pefie = ba[0] * bb[0] + ba[1] * bb[1] + ba[2] * bb[2] - (3.0 * p1) * (3.0 * p2) / k2;
-        cd phi;
+        cd phi, psi;
         if (same) {
-          double imphi;
-          if (fabs(kr) < 2.0e-2) imphi = (1.0 - kr * kr / 6.0) * k * inv4pi;
-          else imphi = sin(kr) * inv4pi / r;
+          double imphi, impsi;
+          if (fabs(kr) < 2.0e-2) {
+            imphi = (1.0 - kr * kr / 6.0) * k * inv4pi;
+            impsi = -(1.0 - kr * kr / 10.0) * k2 * k / (12.0 * M_PI);
+          } else {
+            double s, c;
+            sincos(kr, &s, &c);
+            imphi = s * inv4pi / r;
+            impsi = (kr * c - s) * inv4pi / (r * r2);
+          }
           phi = cmk(0, imphi);
+          psi = cmk(0, impsi);
         } else {
           double s, c;
           sincos(kr, &s, &c);
           phi = cmk(c * inv4pi / r, s * inv4pi / r);
+          psi = cscale(cmul(phi, cmk(-1.0, kr)), 1.0 / r2);     // phi (ikr - 1) / r^2
         }
-        tot = cadd(tot, cscale(phi, P.w * pefie * wt));
+        double XT[3] = {xa[0] - tc[0], xa[1] - tc[1], xa[2] - tc[2]};
+        q[0] = cadd(q[0], cscale(phi, P.w * pefie * wt));
+        cd pp = cscale(psi, TEN_THIRDS * pefie * wt), pf = cscale(phi, TEN_THIRDS * wt);
+        for (int m = 0; m < 3; m++) {
+          int m1 = (m + 1) % 3, m2 = (m + 2) % 3;
+          q[1 + m] = cadd(q[1 + m], cscale(pp, R[m]));
+          q[4 + m] = cadd(q[4 + m], cscale(pf, ba[m1] * bb[m2] - ba[m2] * bb[m1]));
+          q[7 + m] = cadd(q[7 + m], cscale(pp, XT[m1] * R[m2] - XT[m2] * R[m1]));
+        }
       }
     }
-  return tot;
 }
 
-__device__ __forceinline__ double scat_term(const PftArgs &P, int a, int b, cd q, bool same) {
+// contributions of pair (a, b) to the per-object-pair sums (EMTPFT.cc:416-436)
+__device__ __forceinline__ void scat_terms(const PftArgs &P, int a, int b, const cd q[NPQ], bool same, double d[NPQ]) {
   cd Ja = P.J[a], Jb = P.J[b];
   const double Z0 = 376.73031346177;
   // u0JJ = Z0 conj(Ja) Jb
   cd u = cmk(Z0 * (Ja.r * Jb.r + Ja.i * Jb.i), Z0 * (Ja.r * Jb.i - Ja.i * Jb.r));
-  if (same) return u.r * q.i;
-  // -0.5 Re(u i q) = 0.5 Im(u q)
-  return 0.5 * (u.r * q.i + u.i * q.r);
+  if (same) {
+    d[0] = u.r * q[0].i;
+    for (int n = 1; n < NPQ; n++) d[n] = a != b ? u.i * q[n].i : 0.0;
+  } else {
+    // -0.5 Re(u i q) = 0.5 Im(u q);  -0.5 Im(u i q) = -0.5 Re(u q)
+    cd uq = cmul(u, q[0]);
+    d[0] = 0.5 * uq.i;
+    for (int n = 1; n < NPQ; n++) d[n] = -0.5 * cmul(u, q[n]).r;
+  }
 }
 
 #define PMAXOBJ 4
-// far pairs (no common vertex): one thread per pair
+// far pairs (no common vertex): one thread per pair; partial sums per block
+// and object pair: part[block][noa*NO + nob][NPQ]
 __global__ void __launch_bounds__(FT * FT) k_pft_far(PftArgs P, double *part) {
   int bx = blockIdx.x, by = blockIdx.y;
   int a = bx * FT + threadIdx.x, b = by * FT + threadIdx.y;
   const DevGeom &g = P.g;
-  double contrib = 0.0;
+  double d[NPQ];
+  for (int n = 0; n < NPQ; n++) d[n] = 0.0;
   int pairid = 0;
   if (bx <= by && a < g.N && b < g.N && a <= b) {
     int4 va = g.bfV[a], vb = g.bfV[b];
@@ -1001,77 +1034,137 @@ __global__ void __launch_bounds__(FT * FT) k_pft_far(PftArgs P, double *part) {
       double kR = P.absw * fmax(g.bfRadius[a], g.bfRadius[b]);
       int npts = kR > 5.0 ? 16 : 4;
       bool same = va.w == vb.w;
-      cd q = scat_q(P, a, b, npts, same, 0, 1);
-      contrib = scat_term(P, a, b, q, same);
+      cd q[NPQ];
+      scat_q(P, a, b, npts, same, 0, 1, q);
+      scat_terms(P, a, b, q, same, d);
       pairid = va.w * P.nobj + vb.w;
     }
   }
-  __shared__ double red[FT * FT / 32][PMAXOBJ * PMAXOBJ];
+  __shared__ double red[FT * FT / 32][PMAXOBJ * PMAXOBJ][NPQ];
   int tid = threadIdx.y * FT + threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  for (int pid = 0; pid < P.nobj * P.nobj; pid++) {
-    double v = warp_sum(pid == pairid ? contrib : 0.0);
-    if (lane == 0) red[wid][pid] = v;
-  }
+  for (int pid = 0; pid < P.nobj * P.nobj; pid++)
+    for (int n = 0; n < NPQ; n++) {
+      double v = warp_sum(pid == pairid ? d[n] : 0.0);
+      if (lane == 0) red[wid][pid][n] = v;
+    }
   __syncthreads();
-  if (tid < P.nobj * P.nobj) {
+  int nv = P.nobj * P.nobj * NPQ;
+  for (int e = tid; e < nv; e += FT * FT) {
+    int pid = e / NPQ, n = e % NPQ;
     double s = 0;
-    for (int w = 0; w < FT * FT / 32; w++) s += red[w][tid];
-    part[((size_t)by * gridDim.x + bx) * (P.nobj * P.nobj) + tid] = s;
+    for (int w = 0; w < FT * FT / 32; w++) s += red[w][pid][n];
+    part[((size_t)by * gridDim.x + bx) * nv + e] = s;
   }
 }
 
-// near pairs: one warp per pair, lanes split the point pairs
+// near pairs (same object, common vertex): one warp per pair, lanes split the
+// point pairs; partial sums per block and object: part[block][no][NPQ]
 __global__ void k_pft_near(PftArgs P, NearData nd, double *part) {
   int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  double contrib = 0.0;
+  double d[NPQ];
+  for (int n = 0; n < NPQ; n++) d[n] = 0.0;
   if (warp < nd.npairs) {
     int2 ab = nd.pairs[warp];
     const DevGeom &g = P.g;
     double kR = P.absw * fmax(g.bfRadius[ab.x], g.bfRadius[ab.y]);
     int npts = kR > 5.0 ? 33 : 16;
-    cd q = scat_q(P, ab.x, ab.y, npts, true, lane, 32);
-    q.r = warp_sum(q.r);
-    q.i = warp_sum(q.i);
-    if (lane == 0) contrib = scat_term(P, ab.x, ab.y, q, true);
+    cd q[NPQ];
+    scat_q(P, ab.x, ab.y, npts, true, lane, 32, q);
+    for (int n = 0; n < NPQ; n++) {
+      q[n].r = warp_sum(q[n].r);
+      q[n].i = warp_sum(q[n].i);
+    }
+    if (lane == 0) scat_terms(P, ab.x, ab.y, q, true, d);
   }
-  // near pairs are always same-object: accumulate per object
-  __shared__ double red[8];
+  __shared__ double red[8][NPQ];
   __shared__ int objs[8];
   int wid = threadIdx.x >> 5;
   if (lane == 0) {
-    red[wid] = contrib;
+    for (int n = 0; n < NPQ; n++) red[wid][n] = d[n];
     objs[wid] = (warp < nd.npairs) ? P.g.bfV[nd.pairs[warp].x].w : 0;
   }
   __syncthreads();
-  if (threadIdx.x < P.nobj) {
+  for (int e = threadIdx.x; e < P.nobj * NPQ; e += blockDim.x) {
+    int o = e / NPQ, n = e % NPQ;
     double s = 0;
     for (int w = 0; w < (int)(blockDim.x >> 5); w++)
-      if (objs[w] == (int)threadIdx.x) s += red[w];
-    part[(size_t)blockIdx.x * P.nobj + threadIdx.x] = s;
+      if (objs[w] == o) s += red[w][n];
+    part[(size_t)blockIdx.x * P.nobj * NPQ + e] = s;
   }
 }
 
+// extinction (EMTPFT.cc:85-127, 151-211) for a plane wave (grad E = ik nhat E):
+// per basis function q0 = int b.E, qx = int (x - c) b.E, t1 = int b x E;
+// e[0] = Re(J* q0), e[1+i] = Im(J* ik nhat_i q0), e[4+i] = Im(J* t1_i),
+// e[7+i] = Im(J* ik (qx x nhat)_i); partial sums per block and object
 __global__ void k_pft_ext(PftArgs P, PWave pw, double *part) {
   int a = blockIdx.x * blockDim.x + threadIdx.x;
-  double contrib = 0.0;
+  double e[NPQ];
+  for (int n = 0; n < NPQ; n++) e[n] = 0.0;
   int obj = 0;
   if (a < P.g.N) {
-    cd q = bf_dot_field(P.g, a, pw);
-    cd Ja = P.J[a];
-    contrib = Ja.r * q.r + Ja.i * q.i;   // Re(conj(Ja) q)
-    obj = P.g.bfV[a].w;
+    const DevGeom &g = P.g;
+    obj = g.bfV[a].w;
+    const double *tc = g.objOrigin + 3 * obj;
+    int2 tt = g.bfTet[a], loc = g.bfLoc[a];
+    double Aa = g.bfArea[a];
+    cd q0 = cmk(0, 0), qx[3] = {cmk(0, 0), cmk(0, 0), cmk(0, 0)}, t1[3] = {cmk(0, 0), cmk(0, 0), cmk(0, 0)};
+    for (int side = 0; side < 2; side++) {
+      int t = side == 0 ? tt.x : tt.y, iq = side == 0 ? loc.x : loc.y;
+      int4 vi = g.tetVI[t];
+      int v[4] = {vi.x, vi.y, vi.z, vi.w};
+      double Q[3], L[3][3];
+      load3(g.V4, v[iq], Q);
+      for (int i = 0; i < 3; i++) {
+        double tmp[3];
+        load3(g.V4, v[(iq + 1 + i) % 4], tmp);
+        for (int c = 0; c < 3; c++) L[i][c] = tmp[c] - Q[c];
+      }
+      double vol = g.tetVol[t];
+      double pf = (side == 0 ? 1.0 : -1.0) * Aa / (3.0 * vol);
+      for (int i = 0; i < 33; i++) {
+        const double *u = c_tcr33 + 4 * i;
+        double wt = 6.0 * vol * u[3], x[3], bv[3];
+        for (int c = 0; c < 3; c++) {
+          bv[c] = u[0] * L[0][c] + u[1] * L[1][c] + u[2] * L[2][c];
+          x[c] = Q[c] + bv[c];
+          bv[c] *= pf;
+        }
+        cd ph = expikr(pw.k, pw.nh[0] * x[0] + pw.nh[1] * x[1] + pw.nh[2] * x[2]);
+        cd E[3];
+        for (int c = 0; c < 3; c++) E[c] = cscale(cmul(pw.E0[c], ph), wt);
+        cd be = cadd(cadd(cscale(E[0], bv[0]), cscale(E[1], bv[1])), cscale(E[2], bv[2]));
+        q0 = cadd(q0, be);
+        for (int c = 0; c < 3; c++) qx[c] = cadd(qx[c], cscale(be, x[c] - tc[c]));
+        t1[0] = cadd(t1[0], csub(cscale(E[2], bv[1]), cscale(E[1], bv[2])));
+        t1[1] = cadd(t1[1], csub(cscale(E[0], bv[2]), cscale(E[2], bv[0])));
+        t1[2] = cadd(t1[2], csub(cscale(E[1], bv[0]), cscale(E[0], bv[1])));
+      }
+    }
+    cd Jc = cmk(P.J[a].r, -P.J[a].i);
+    cd ik = cmk(-pw.k.i, pw.k.r);
+    e[0] = cmul(Jc, q0).r;
+    for (int i = 0; i < 3; i++) {
+      int i1 = (i + 1) % 3, i2 = (i + 2) % 3;
+      e[1 + i] = cmul(Jc, cscale(cmul(ik, q0), pw.nh[i])).i;
+      e[4 + i] = cmul(Jc, t1[i]).i;
+      cd qxn = csub(cscale(qx[i1], pw.nh[i2]), cscale(qx[i2], pw.nh[i1]));
+      e[7 + i] = cmul(Jc, cmul(ik, qxn)).i;
+    }
   }
-  __shared__ double red[4][PMAXOBJ];
+  __shared__ double red[4][PMAXOBJ][NPQ];
   int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (int o = 0; o < P.nobj; o++) {
-    double v = warp_sum(o == obj ? contrib : 0.0);
-    if (lane == 0) red[wid][o] = v;
-  }
+  for (int o = 0; o < P.nobj; o++)
+    for (int n = 0; n < NPQ; n++) {
+      double v = warp_sum(o == obj ? e[n] : 0.0);
+      if (lane == 0) red[wid][o][n] = v;
+    }
   __syncthreads();
-  if (threadIdx.x < P.nobj) {
+  for (int x = threadIdx.x; x < P.nobj * NPQ; x += blockDim.x) {
+    int o = x / NPQ, n = x % NPQ;
     double s = 0;
-    for (int w = 0; w < 4; w++) s += red[w][threadIdx.x];
-    part[(size_t)blockIdx.x * P.nobj + threadIdx.x] = s;
+    for (int w = 0; w < 4; w++) s += red[w][o][n];
+    part[(size_t)blockIdx.x * P.nobj * NPQ + x] = s;
   }
 }
 
@@ -1192,12 +1285,32 @@ int pft(bg_geometry *g, double wr, double wi, const void *dJ, const double *E0, 
     }
     return BG_OK;
   }
+  double full[8 * PMAXOBJ];
+  if ((st = pft_emt_full(g, wr, wi, dJ, E0, nhat, full))) return st;
+  for (int o = 0; o < NO; o++) {
+    out[2 * o] = full[8 * o];
+    out[2 * o + 1] = full[8 * o + 1];
+  }
+  return BG_OK;
+}
+
+// GetPFTMatrix with EMT (GetPFT.cc:133-189, EMTPFT.cc:324-493): out[8*no + c],
+// c = PAbs, PScat, Fx, Fy, Fz, Tx, Ty, Tz (force and torque in the
+// reference's units, TENTHIRDS = 10/3), plane-wave incident field
+int pft_emt_full(bg_geometry *g, double wr, double wi, const void *dJ, const double *E0, const double *nhat,
+                 double *out) {
+  int st = init_tables();
+  if (st) return st;
+  int NO = (int)g->objs.size();
+  if (NO > PMAXOBJ) { set_error("PFT supports at most %d objects", PMAXOBJ); return BG_ERR_ARG; }
+  PftArgs P{g->dev, (const cd *)dJ, wr, std::sqrt(wr * wr + wi * wi), NO};
+  int nrow = (g->N + 127) / 128;
   if ((st = build_near_lists(g))) return st;
   int nb = (g->N + FT - 1) / FT;
-  size_t nfar = (size_t)nb * nb * NO * NO;
+  size_t nfar = (size_t)nb * nb * NO * NO * NPQ;
   int nnear_blocks = (g->near.npairs * 32 + 255) / 256;
-  size_t nnear = (size_t)std::max(nnear_blocks, 1) * NO;
-  size_t next = (size_t)nrow * NO;
+  size_t nnear = (size_t)std::max(nnear_blocks, 1) * NO * NPQ;
+  size_t next = (size_t)nrow * NO * NPQ;
   if ((st = ensure_scratch(g, sizeof(double) * (nfar + nnear + next)))) return st;
   double *pfar = g->d_scratch, *pnear = pfar + nfar, *pext = pnear + nnear;
   k_pft_far<<<dim3(nb, nb), dim3(FT, FT), 0, stream()>>>(P, pfar);
@@ -1212,19 +1325,29 @@ int pft(bg_geometry *g, double wr, double wi, const void *dJ, const double *E0, 
   std::vector<double> h(nfar + nnear + next);
   BG_CUDA_TRY(cudaMemcpyAsync(h.data(), g->d_scratch, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, stream()));
   BG_CUDA_TRY(cudaStreamSynchronize(stream()));
-  std::vector<double> scat((size_t)NO * NO, 0.0), ext(NO, 0.0);
+  // scat[noa][nob][n]: pair sums; ext[no][n]
+  std::vector<double> scat((size_t)NO * NO * NPQ, 0.0), ext((size_t)NO * NPQ, 0.0);
   for (size_t blk = 0; blk < (size_t)nb * nb; blk++)
-    for (int p = 0; p < NO * NO; p++) scat[p] += h[blk * NO * NO + p];
+    for (size_t e = 0; e < (size_t)NO * NO * NPQ; e++) scat[e] += h[blk * NO * NO * NPQ + e];
   if (g->near.npairs > 0)
     for (int blk = 0; blk < nnear_blocks; blk++)
-      for (int o = 0; o < NO; o++) scat[(size_t)o * NO + o] += h[nfar + (size_t)blk * NO + o];
+      for (int o = 0; o < NO; o++)
+        for (int n = 0; n < NPQ; n++) scat[((size_t)o * NO + o) * NPQ + n] += h[nfar + ((size_t)blk * NO + o) * NPQ + n];
   for (int blk = 0; blk < nrow; blk++)
-    for (int o = 0; o < NO; o++) ext[o] += h[nfar + nnear + (size_t)blk * NO + o];
+    for (size_t e = 0; e < (size_t)NO * NPQ; e++) ext[e] += h[nfar + nnear + (size_t)blk * NO * NPQ + e];
+  double ftf = 0.5 * TEN_THIRDS / wr;
   for (int o = 0; o < NO; o++) {
-    double ps = 0;
-    for (int ob = 0; ob < NO; ob++) ps += scat[(size_t)o * NO + ob];
-    out[2 * o] = 0.5 * ext[o] - ps;
-    out[2 * o + 1] = ps;
+    double s[NPQ] = {0};
+    for (int ob = 0; ob < NO; ob++)
+      for (int n = 0; n < NPQ; n++) s[n] += scat[((size_t)o * NO + ob) * NPQ + n];
+    const double *e = ext.data() + (size_t)o * NPQ;
+    double *r = out + 8 * o;
+    r[0] = 0.5 * e[0] - s[0];
+    r[1] = s[0];
+    for (int i = 0; i < 3; i++) {
+      r[2 + i] = ftf * e[1 + i] - s[1 + i];
+      r[5 + i] = ftf * (e[4 + i] + e[7 + i]) - s[4 + i] - s[7 + i];
+    }
   }
   return BG_OK;
 }

@@ -313,6 +313,15 @@ int bg_rhs_planewave_device(bg_geometry *g, double omega_re, double omega_im, co
 int bg_pft(bg_geometry *g, double omega_re, double omega_im, const double *J_host, const double *E0,
            const double *nhat, int method, double *out);
 
+/* SWGGeometry::GetPFTMatrix(J, Omega, Options) with the EMT method, all
+   columns (GetPFT.cc:133-189, EMTPFT.cc:85-127,216-291,324-493): out[8*obj +
+   c], c = PAbs, PScat, Fx, Fy, Fz, Tx, Ty, Tz, for the plane wave E0/nhat as
+   incident field.  Forces and torques use the reference's units (its 10/3
+   factor); torques are about each object's displacement (its origin).
+   J: N complex (host). */
+int bg_pft_full(bg_geometry *g, double omega_re, double omega_im, const double *J_host, const double *E0,
+                const double *nhat, double *out);
+
 /* ---------------------------------------------------------------------------
  * instrumentation
  * ------------------------------------------------------------------------- */

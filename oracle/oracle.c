@@ -1098,6 +1098,176 @@ void or_pft_emt(OGeom *G, double wr, double wi, const double *J, const double *E
   free(scat); free(ext);
 }
 
+/* ------------------------------------------------------------------------- */
+/* Full EMT PFT (EMTPFT.cc:85-127 extinction integrand, 216-291 scattered      */
+/* integrand, 396-491 accumulation): columns PAbs, PScat, Fx, Fy, Fz, Tx, Ty,  */
+/* Tz per object, for a plane-wave incident field (its gradient is ik nhat E). */
+/* The torque centre of an object is its displacement (SWGVolume Origin).      */
+/* ------------------------------------------------------------------------- */
+#define TEN_THIRDS (10.0 / 3.0)
+typedef struct { double omega; int same; const double *tcA; } SC10Data;
+
+/* 10 complex outputs: PScat, F (3), T1 = b_A x b_B term (3), T2 = (x_A - c_A) x R term (3) */
+static void scat10_integrand(const double *xA, const double *bA, double dA,
+                             const double *xB, const double *bB, double dB, void *ud, double *I_)
+{
+  SC10Data *D = ud;
+  double k = D->omega, w = D->omega;
+  double R[3] = {xA[0] - xB[0], xA[1] - xB[1], xA[2] - xB[2]};
+  double r2 = R[0] * R[0] + R[1] * R[1] + R[2] * R[2], r = sqrt(r2), kr = k * r, kr2 = kr * kr, k2 = k * k;
+  double pefie = bA[0] * bB[0] + bA[1] * bB[1] + bA[2] * bB[2] - dA * dB / k2;
+  double XT[3] = {xA[0] - D->tcA[0], xA[1] - D->tcA[1], xA[2] - D->tcA[2]};
+  double bxb[3], xtr[3];
+  for (int m = 0; m < 3; m++) {
+    int m1 = (m + 1) % 3, m2 = (m + 2) % 3;
+    bxb[m] = bA[m1] * bB[m2] - bA[m2] * bB[m1];
+    xtr[m] = XT[m1] * R[m2] - XT[m2] * R[m1];
+  }
+  cplx phi, psi;
+  if (D->same) {
+    double imphi, impsi;
+    if (fabs(kr) < 2.0e-2) {
+      imphi = (1.0 - kr2 / 6.0) * k / (4.0 * M_PI);
+      impsi = -(1.0 - kr2 / 10.0) * k2 * k / (12.0 * M_PI);
+    } else {
+      imphi = sin(kr) / (4.0 * M_PI * r);
+      impsi = (kr * cos(kr) - sin(kr)) / (4.0 * M_PI * r * r2);
+    }
+    phi = I * imphi;
+    psi = I * impsi;
+  } else {
+    phi = cexp(I * kr) / (4.0 * M_PI * r);
+    psi = phi * (I * kr - 1.0) / r2;
+  }
+  cplx q[10];
+  q[0] = w * pefie * phi;
+  for (int m = 0; m < 3; m++) {
+    q[1 + m] = TEN_THIRDS * pefie * R[m] * psi;
+    q[4 + m] = TEN_THIRDS * bxb[m] * phi;
+    q[7 + m] = TEN_THIRDS * pefie * xtr[m] * psi;
+  }
+  for (int i = 0; i < 10; i++) { I_[2 * i] = creal(q[i]); I_[2 * i + 1] = cimag(q[i]); }
+}
+
+/* extinction integrals of basis function a (33-point rule): q0 = int b.E,
+   qx[j] = int (x_j - c_j) b.E, t1 = int b x E */
+static void bf_ext_integrals(OObj *O, int a, const PW *pw, cplx *q0, cplx qx[3], cplx t1[3])
+{
+  OFace *F = O->F[a];
+  const double *cr = tet_rule(33);
+  *q0 = 0;
+  for (int j = 0; j < 3; j++) qx[j] = t1[j] = 0;
+  for (int side = 0; side < 2; side++) {
+    int nt = side == 0 ? F->iPTet : F->iMTet, iq = side == 0 ? F->PIndex : F->MIndex;
+    OTet *T = O->T + nt;
+    double sign = side == 0 ? 1.0 : -1.0;
+    const double *Q = O->V + 3 * T->VI[iq];
+    double L1[3], L2[3], L3[3];
+    for (int k = 0; k < 3; k++) {
+      L1[k] = O->V[3 * T->VI[(iq + 1) % 4] + k] - Q[k];
+      L2[k] = O->V[3 * T->VI[(iq + 2) % 4] + k] - Q[k];
+      L3[k] = O->V[3 * T->VI[(iq + 3) % 4] + k] - Q[k];
+    }
+    double pf = sign * O->F[T->FI[iq]]->area / (3.0 * T->vol);
+    for (int i = 0; i < 33; i++) {
+      double w = 6.0 * T->vol * cr[4 * i + 3], x[3], b[3];
+      for (int k = 0; k < 3; k++) {
+        b[k] = cr[4 * i] * L1[k] + cr[4 * i + 1] * L2[k] + cr[4 * i + 2] * L3[k];
+        x[k] = Q[k] + b[k];
+        b[k] *= pf;
+      }
+      cplx E[3];
+      pw_field(pw, x, E);
+      cplx be = b[0] * E[0] + b[1] * E[1] + b[2] * E[2];
+      *q0 += w * be;
+      for (int j = 0; j < 3; j++) qx[j] += w * (x[j] - O->origin[j]) * be;
+      t1[0] += w * (b[1] * E[2] - b[2] * E[1]);
+      t1[1] += w * (b[2] * E[0] - b[0] * E[2]);
+      t1[2] += w * (b[0] * E[1] - b[1] * E[0]);
+    }
+  }
+}
+
+/* out[8*no + c], c = PAbs, PScat, Fx, Fy, Fz, Tx, Ty, Tz */
+void or_pft_emt8(OGeom *G, double wr, double wi, const double *J, const double *E0, const double *nhat,
+                 double *out)
+{
+  int N = G->N, NO = G->no;
+  cplx omega = wr + I * wi;
+  double *scat = calloc((size_t)NO * NO * 10, sizeof(double));
+  double *ext = calloc((size_t)NO * 10, sizeof(double));
+  PW pw;
+  for (int i = 0; i < 3; i++) { pw.E0[i] = E0[2 * i] + I * E0[2 * i + 1]; pw.nhat[i] = nhat[i]; }
+  pw.k = omega;
+#pragma omp parallel
+  {
+    double *ls = calloc((size_t)NO * NO * 10, sizeof(double));
+    double *le = calloc((size_t)NO * 10, sizeof(double));
+#pragma omp for schedule(dynamic, 1)
+    for (int a = 0; a < N; a++) {
+      int noa, nfa;
+      OObj *OA = resolve(G, a, &noa, &nfa);
+      cplx Ja = J[2 * a] + I * J[2 * a + 1];
+      for (int b = a; b < N; b++) {
+        int nob, nfb;
+        OObj *OB = resolve(G, b, &nob, &nfb);
+        int ncv = compare_bfs(OA, nfa, OB, nfb);
+        double kR = cabs(omega) * fmax(OA->F[nfa]->radius, OB->F[nfb]->radius);
+        int hf = kR > 5.0;
+        int npts = hf ? (ncv > 0 ? 33 : 16) : (ncv > 0 ? 16 : 4);
+        SC10Data D = {creal(omega), OA == OB, OA->origin};
+        double q[20];
+        bf_bf_int(OA, nfa, OB, nfb, scat10_integrand, &D, 20, q, npts);
+        cplx Jb = J[2 * b] + I * J[2 * b + 1];
+        cplx u0jj = ZVAC * conj(Ja) * Jb;
+        double *d = ls + ((size_t)noa * NO + nob) * 10;
+        if (noa == nob) {
+          d[0] += creal(u0jj) * q[1];
+          if (a != b)
+            for (int n = 1; n < 10; n++) d[n] += cimag(u0jj) * q[2 * n + 1];
+        } else {
+          for (int n = 0; n < 10; n++) {
+            cplx z = u0jj * I * (q[2 * n] + I * q[2 * n + 1]);
+            d[n] += n == 0 ? -0.5 * creal(z) : -0.5 * cimag(z);
+          }
+        }
+      }
+      cplx q0, qx[3], t1[3];
+      bf_ext_integrals(OA, nfa, &pw, &q0, qx, t1);
+      cplx ik = I * omega;
+      double *e = le + (size_t)noa * 10;
+      e[0] += creal(conj(Ja) * q0);
+      for (int i = 0; i < 3; i++) {
+        int i1 = (i + 1) % 3, i2 = (i + 2) % 3;
+        e[1 + i] += cimag(conj(Ja) * ik * nhat[i] * q0);                          /* b . d_i E */
+        e[4 + i] += cimag(conj(Ja) * t1[i]);                                      /* (b x E)_i */
+        e[7 + i] += cimag(conj(Ja) * ik * (qx[i1] * nhat[i2] - qx[i2] * nhat[i1])); /* b . (XT x grad)_i E */
+      }
+    }
+#pragma omp critical
+    {
+      for (int i = 0; i < NO * NO * 10; i++) scat[i] += ls[i];
+      for (int i = 0; i < NO * 10; i++) ext[i] += le[i];
+    }
+    free(ls); free(le);
+  }
+  double ftf = 0.5 * TEN_THIRDS / wr;
+  for (int no = 0; no < NO; no++) {
+    double s[10] = {0};
+    for (int nob = 0; nob < NO; nob++)
+      for (int n = 0; n < 10; n++) s[n] += scat[((size_t)no * NO + nob) * 10 + n];
+    const double *e = ext + (size_t)no * 10;
+    double *o = out + 8 * no;
+    o[0] = 0.5 * e[0] - s[0];
+    o[1] = s[0];
+    for (int i = 0; i < 3; i++) {
+      o[2 + i] = ftf * e[1 + i] - s[1 + i];
+      o[5 + i] = ftf * (e[4 + i] + e[7 + i]) - s[4 + i] - s[7 + i];
+    }
+  }
+  free(scat); free(ext);
+}
+
 /* OPFT absorbed power (OPFT.cc:62-119 with OverlapIntegrand_PFT's PAbs term,
    OverlapIntegrals.cc:51-170,242-298): PAbs = sum Re(conj(Ja) Jb ME_ab),
    ME_ab = 1/2 int bA . (i Z0/w) (eps-1)^-1 . bB over the shared tets. */

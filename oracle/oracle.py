@@ -82,6 +82,7 @@ def lib():
         L.or_assemble_rows.argtypes = [P, D, D, dp, I, I]
         L.or_rhs_planewave.argtypes = [P, D, D, dp, dp, dp]
         L.or_pft_emt.argtypes = [P, D, D, dp, dp, dp, dp]
+        L.or_pft_emt8.argtypes = [P, D, D, dp, dp, dp, dp]
         L.or_pft_opft.argtypes = [P, D, D, dp, dp]
         L.or_num_threads.restype = I
         L.or_cache_build.argtypes = [P]
@@ -195,6 +196,15 @@ class Geometry:
         out = np.zeros(2 * self.nobj)
         lib().or_pft_emt(self.h, omega.real, omega.imag, Jd, E, nh, out)
         return out.reshape(self.nobj, 2)
+
+    def pft_emt8(self, omega, J, E0, nhat):
+        """Full EMT PFT: rows = objects, columns PAbs, PScat, Fx, Fy, Fz, Tx, Ty, Tz."""
+        Jd = np.ascontiguousarray(J, dtype=np.complex128).view(np.float64)
+        E = np.asarray(E0, dtype=np.complex128).view(np.float64).copy()
+        nh = np.asarray(nhat, dtype=np.float64).copy()
+        out = np.zeros(8 * self.nobj)
+        lib().or_pft_emt8(self.h, omega.real, omega.imag, Jd, E, nh, out)
+        return out.reshape(self.nobj, 8)
 
     def pft_opft(self, omega, J):
         Jd = np.ascontiguousarray(J, dtype=np.complex128).view(np.float64)

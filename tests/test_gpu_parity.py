@@ -255,3 +255,31 @@ def test_zgemm_device(M, N, K):
     out = dC.cpu().numpy().T
     ref = Cm - A @ B
     assert np.max(np.abs(out - ref)) <= 1e-13 * max(1.0, np.abs(A).max() * np.abs(B).max() * K)
+
+
+@pytest.mark.parametrize("case", ["tensor_sphere", "two_spheres"])
+def test_full_pft_parity(sphere, oracle_lib, case):
+    """GetPFTMatrix, EMT, all 8 columns (PAbs, PScat, force, torque) -- GPU vs
+    oracle, for one anisotropic sphere and for two displaced spheres (the
+    different-object formulas and two torque centres).  Tolerance 1e-9 of
+    the largest entry of each column kind."""
+    w = 1.3
+    if case == "tensor_sphere":
+        t = np.array([[4, 0.5, 0], [0.5, 6, 0], [0, 0, 9]], complex) + 0.1j * np.eye(3)
+        Gb, Go = pair(sphere(3), buffem.Material(kind=buffem.BG_MAT_CONST_TENSOR, tensor=t),
+                      oracle_lib.material(kind=oracle_lib.MAT_CONST_TENSOR, tensor=t), oracle_lib=oracle_lib)
+    else:
+        disp = [[0, 0, 0], [0.3, 0, 2.4]]
+        meshes = [sphere(2, radius=0.8), sphere(3, radius=1.0)]
+        Gb, Go = pair(meshes, [buffem.Material(eps=4 + 0.2j), buffem.Material(eps=9 + 1j)],
+                      [oracle_lib.material(eps=4 + 0.2j), oracle_lib.material(eps=9 + 1j)], disp=disp,
+                      oracle_lib=oracle_lib)
+    M = Go.assemble(complex(w))
+    E0, nh = np.array([1, 0.3j, 0], complex), np.array([0.6, 0, 0.8])
+    J = sl.lu_solve(sl.lu_factor(M), Go.rhs_planewave(complex(w), E0, nh))
+    pb = Gb.GetPFTMatrix(J, w, buffem.PlaneWave(E0, nh), full=True)
+    po = Go.pft_emt8(complex(w), J, E0, nh)
+    for cols in (slice(0, 2), slice(2, 5), slice(5, 8)):
+        scale = np.abs(po[:, cols]).max()
+        np.testing.assert_allclose(pb[:, cols], po[:, cols], rtol=0, atol=1e-9 * scale)
+    np.testing.assert_allclose(pb[:, :2], Gb.GetPFTMatrix(J, w, buffem.PlaneWave(E0, nh)), rtol=1e-13)

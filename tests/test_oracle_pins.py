@@ -169,3 +169,53 @@ def test_oracle_mie_convergence(oracle_lib, sphere):
         errs.append((abs(pe[0] / cabs - 1), abs(pe[1] / csca - 1)))
     assert errs[1][0] < errs[0][0] and errs[1][1] < errs[0][1]
     assert errs[1][0] < 0.5 and errs[1][1] < 0.5
+
+
+def mie_pressure(eps, x, nmax=30):
+    """Radiation-pressure cross section C_ext - g C_sca of a sphere (Bohren
+    & Huffman, Absorption and Scattering of Light by Small Particles, 4.62)."""
+    m = np.sqrt(complex(eps))
+    mx = m * x
+    A, B = [], []
+    for n in range(1, nmax + 2):
+        jx, djx = sp.spherical_jn(n, x), sp.spherical_jn(n, x, True)
+        yx, dyx = sp.spherical_yn(n, x), sp.spherical_yn(n, x, True)
+        jm, djm = sp.spherical_jn(n, mx), sp.spherical_jn(n, mx, True)
+        psi, dpsi = x * jx, jx + x * djx
+        xi, dxi = x * (jx + 1j * yx), (jx + 1j * yx) + x * (djx + 1j * dyx)
+        psim, dpsim = mx * jm, jm + mx * djm
+        A.append((m * psim * dpsi - psi * dpsim) / (m * psim * dxi - xi * dpsim))
+        B.append((psim * dpsi - m * psi * dpsim) / (psim * dxi - m * xi * dpsim))
+    cext = sum((2 * n + 1) * (A[n - 1] + B[n - 1]).real for n in range(1, nmax))
+    gsca = sum(n * (n + 2) / (n + 1) * (A[n - 1] * np.conj(A[n]) + B[n - 1] * np.conj(B[n])).real
+               + (2 * n + 1) / (n * (n + 1)) * (A[n - 1] * np.conj(B[n - 1])).real for n in range(1, nmax))
+    k = x
+    return 2 * np.pi / k ** 2 * cext - 4 * np.pi / k ** 2 * gsca
+
+
+def test_oracle_emt_force_and_torque(oracle_lib, sphere):
+    """Full EMT PFT (EMTPFT.cc:85-127, 216-291, 396-491) on an isotropic
+    sphere: the power columns equal the two-column EMT result; the z force
+    balances momentum, F_z = (10/3) (PAbs + PScat (1 - g)) with the Mie
+    asymmetry parameter g, and approaches the Mie radiation pressure
+    (10/3) I C_pr as the mesh is refined; the transverse force and the torque,
+    zero by symmetry, shrink."""
+    cabs, csca = mie(4 + 0.2j, 1.0)
+    cpr = mie_pressure(4 + 0.2j, 1.0)
+    g = (cabs + csca - cpr) / csca
+    iinc = 1.0 / (2 * 376.73031346177)
+    E0, nh = np.array([1, 0, 0], complex), np.array([0, 0, 1.0])
+    errs, sym = [], []
+    for n in (3, 4, 5):
+        G = oracle_lib.Geometry(sphere(n), oracle_lib.material(eps=4 + 0.2j), nang=6)
+        M = G.assemble(1.0 + 0j)
+        J = sl.lu_solve(sl.lu_factor(M), G.rhs_planewave(1.0 + 0j, E0, nh))
+        p8 = G.pft_emt8(1.0 + 0j, J, E0, nh)[0]
+        p2 = G.pft_emt(1.0 + 0j, J, E0, nh)[0]
+        np.testing.assert_allclose(p8[:2], p2, rtol=1e-13)
+        balance = 10.0 / 3.0 * (p8[0] + p8[1] * (1 - g))
+        assert abs(p8[4] / balance - 1) < 0.03, (n, p8[4], balance)
+        errs.append(abs(p8[4] / (10.0 / 3.0 * iinc * cpr) - 1))
+        sym.append(max(np.abs(p8[2:4]).max(), np.abs(p8[5:]).max()) / p8[4])
+    assert errs[2] < errs[1] < errs[0], errs
+    assert sym[2] < sym[1] < sym[0] and sym[2] < 0.05, sym
