@@ -80,7 +80,7 @@ EXPORTS = [
     "bg_gnn_get_params", "bg_gnn_set_params", "bg_gnn_get_grads", "bg_gnn_train_step",
     "bg_precond_create_learned", "bg_precond_download", "bg_gmres_solve_mixed", "bg_gmres_solve_mixed_device",
     "bg_precond_bound", "bg_gmres_solve_lu_fallback", "bg_gmres_solve_lu_fallback_device", "bg_batch_sweep",
-    "bg_pft_full",
+    "bg_pft_full", "bg_fibbi_store", "bg_fibbi_load",
 ]
 
 
@@ -140,6 +140,8 @@ def lib():
         L.bg_rhs_planewave_device.argtypes = [P, D, D, VP, VP, VP]
         L.bg_pft.argtypes = [P, D, D, VP, VP, VP, I, VP]
         L.bg_pft_full.argtypes = [P, D, D, VP, VP, VP, VP]
+        L.bg_fibbi_store.argtypes = [P, I, C.c_char_p, C.POINTER(I)]
+        L.bg_fibbi_load.argtypes = [P, I, C.c_char_p, C.POINTER(I)]
         L.bg_kernel_launch_count.restype = C.c_longlong
         L.bg_stream.restype = VP
         L.bg_profile_read.argtypes = [I, VP, VP, VP]
@@ -290,6 +292,18 @@ class SWGGeometry:
         data = np.zeros((cnt.value, 6), dtype=np.float64)
         _check(lib().bg_geometry_near_data(self.h, C.byref(cnt), _ptr(pairs), _ptr(data)))
         return pairs, data
+
+    def StoreFIBBICache(self, path, obj=0):
+        """Write object obj's near-field table as a reference FIBBI cache file; returns the record count."""
+        n = C.c_int()
+        _check(lib().bg_fibbi_store(self.h, int(obj), os.fsencode(path), C.byref(n)))
+        return n.value
+
+    def PreloadFIBBICache(self, path, obj=0):
+        """Take the near-field integrals of object obj from a reference FIBBI cache file; returns matches."""
+        n = C.c_int()
+        _check(lib().bg_fibbi_load(self.h, int(obj), os.fsencode(path), C.byref(n)))
+        return n.value
 
     def AllocateVIEMatrix(self, precision=BG_C128):
         return HMatrix(self, precision)

@@ -322,6 +322,19 @@ int bg_pft(bg_geometry *g, double omega_re, double omega_im, const double *J_hos
 int bg_pft_full(bg_geometry *g, double omega_re, double omega_im, const double *J_host, const double *E0,
                 const double *nhat, double *out);
 
+/* The reference's FIBBI cache file (FIBBICache::Store / PreLoad,
+   FIBBICache.cc:272-463): "FIBBI_GCACHE\0", then records of 27 float keys
+   (GetFIBBICacheKey, FIBBICache.cc:133-160) and the 6 static near-field
+   integrals of a basis-function pair of one object.  Store writes the near
+   table of object obj (computing it first if needed); load replaces the
+   entries of obj's near table whose keys appear in the file (for instance a
+   cache written by the reference's own tools) and reports how many did.
+   Keys are compared bit for bit, as the reference's map does, so a displaced
+   copy of an object matches only the records whose float key differences
+   the displacement leaves unchanged. */
+int bg_fibbi_store(bg_geometry *g, int obj, const char *path, int *written);
+int bg_fibbi_load(bg_geometry *g, int obj, const char *path, int *matched);
+
 /* ---------------------------------------------------------------------------
  * instrumentation
  * ------------------------------------------------------------------------- */

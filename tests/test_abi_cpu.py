@@ -93,3 +93,19 @@ def test_batch_sweep_rejects_bad_arguments(buffem_lib):
     st = L.bg_batch_sweep(None, 1, w.ctypes.data_as(C.c_void_p), 1, E0.ctypes.data_as(C.c_void_p),
                           nh.ctypes.data_as(C.c_void_p), 1, 0, out.ctypes.data_as(C.c_void_p), None)
     assert st == buffem_lib.BG_ERR_ARG
+
+
+def test_fibbi_load_rejects_foreign_files(buffem_lib, tmp_path, ref_mesh):
+    """A file without the reference's FIBBI signature, or with a partial
+    record, is refused before any device work."""
+    G = buffem_lib.SWGGeometry(meshfiles=ref_mesh("sphere48"), materials=buffem_lib.Material(eps=10.0))
+    bad = tmp_path / "bad.cache"
+    bad.write_bytes(b"NOT_A_CACHE\0\0" + bytes(156))
+    with pytest.raises(buffem_lib.BuffError) as e:
+        G.PreloadFIBBICache(str(bad))
+    assert e.value.status == buffem_lib.BG_ERR_IO
+    short = tmp_path / "short.cache"
+    short.write_bytes(b"FIBBI_GCACHE\0" + bytes(155))
+    with pytest.raises(buffem_lib.BuffError) as e:
+        G.PreloadFIBBICache(str(short))
+    assert e.value.status == buffem_lib.BG_ERR_IO
