@@ -80,7 +80,7 @@ EXPORTS = [
     "bg_gnn_get_params", "bg_gnn_set_params", "bg_gnn_get_grads", "bg_gnn_train_step",
     "bg_precond_create_learned", "bg_precond_download", "bg_gmres_solve_mixed", "bg_gmres_solve_mixed_device",
     "bg_precond_bound", "bg_gmres_solve_lu_fallback", "bg_gmres_solve_lu_fallback_device", "bg_batch_sweep",
-    "bg_pft_full", "bg_fibbi_store", "bg_fibbi_load",
+    "bg_pft_full", "bg_fibbi_store", "bg_fibbi_load", "bg_get_fields", "bg_get_fields_device",
 ]
 
 
@@ -140,6 +140,8 @@ def lib():
         L.bg_rhs_planewave_device.argtypes = [P, D, D, VP, VP, VP]
         L.bg_pft.argtypes = [P, D, D, VP, VP, VP, I, VP]
         L.bg_pft_full.argtypes = [P, D, D, VP, VP, VP, VP]
+        L.bg_get_fields.argtypes = [P, D, D, VP, VP, VP, C.c_int, VP, VP]
+        L.bg_get_fields_device.argtypes = [P, D, D, VP, VP, VP, C.c_int, VP, VP]
         L.bg_fibbi_store.argtypes = [P, I, C.c_char_p, C.POINTER(I)]
         L.bg_fibbi_load.argtypes = [P, I, C.c_char_p, C.POINTER(I)]
         L.bg_kernel_launch_count.restype = C.c_longlong
@@ -183,7 +185,7 @@ class HMatrix:
         self.precision = precision
 
     def __del__(self):
-        if getattr(self, "h", None):
+        if getattr(self, "h", None) and lib is not None:   # lib is None at interpreter exit
             lib().bg_matrix_destroy(self.h)
             self.h = None
 
@@ -272,7 +274,7 @@ class SWGGeometry:
             _check(lib().bg_geometry_set_singular_order(h, int(singular_order)))
 
     def __del__(self):
-        if getattr(self, "h", None):
+        if getattr(self, "h", None) and lib is not None:   # lib is None at interpreter exit
             lib().bg_geometry_destroy(self.h)
             self.h = None
 
@@ -322,6 +324,22 @@ class SWGGeometry:
         Omega = complex(Omega)
         out = self.AllocateRHSVector() if RHS is None else RHS
         _check(lib().bg_rhs_planewave(self.h, Omega.real, Omega.imag, _ptr(IF.E0), _ptr(IF.nHat), _ptr(out)))
+        return out
+
+    def GetFields(self, IF, J, Omega, X):
+        """SWGGeometry::GetFields (GetFields.cc:287-382): (P, 6) complex array of
+        Ex, Ey, Ez, Hx, Hy, Hz at the points X (P x 3); IF (a PlaneWave) and J
+        may each be None, as the reference's IF = 0 and J = 0."""
+        Omega = complex(Omega)
+        X = np.ascontiguousarray(X, dtype=np.float64).reshape(-1, 3)
+        out = np.zeros((len(X), 6), complex)
+        Jc = None if J is None else np.ascontiguousarray(J, dtype=np.complex128)
+        if Jc is not None and Jc.shape != (self.TotalBFs,):
+            raise ValueError("J must have TotalBFs entries")
+        E0 = _ptr(IF.E0) if IF is not None else None
+        nh = _ptr(IF.nHat) if IF is not None else None
+        _check(lib().bg_get_fields(self.h, Omega.real, Omega.imag, None if Jc is None else _ptr(Jc), E0, nh,
+                                   len(X), _ptr(X), _ptr(out)))
         return out
 
     def GetPFTMatrix(self, J, Omega, IF=None, method=BG_PFT_EMT, full=False):
@@ -391,7 +409,7 @@ class Preconditioner:
         return rowptr, col, val
 
     def __del__(self):
-        if getattr(self, "h", None):
+        if getattr(self, "h", None) and lib is not None:   # lib is None at interpreter exit
             lib().bg_precond_destroy(self.h)
             self.h = None
 
@@ -451,7 +469,7 @@ class GNN:
         return float(loss[0])
 
     def __del__(self):
-        if getattr(self, "h", None):
+        if getattr(self, "h", None) and lib is not None:   # lib is None at interpreter exit
             lib().bg_gnn_destroy(self.h)
             self.h = None
 

@@ -49,6 +49,14 @@ int ensure_device() {
     return BG_ERR_CUDA;
   }
   BG_CUDA_TRY(cudaStreamCreateWithFlags(&s_stream, cudaStreamNonBlocking));
+  // keep up to 1 GiB of freed stream-ordered allocations in this process's
+  // default pool across synchronizations, so per-call scratch buffers do not
+  // go back to the driver every call (larger transients are still returned)
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t keep = 1ull << 30;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
   s_dev_ok = 1;
   return BG_OK;
 }
@@ -162,6 +170,7 @@ void bg_geometry_destroy(bg_geometry *g) {
   dfree(n.pairs); dfree(n.pairTP); dfree(n.fibbi); dfree(n.tp); dfree(n.tpOrdA); dfree(n.tpOrdB); dfree(n.tpMom);
   dfree(g->graph.rowptr); dfree(g->graph.col); dfree(g->graph.etr);
   dfree(g->d_scratch);
+  dfree(g->d_fieldTet); dfree(g->d_fieldFace);
   delete g;
 }
 
@@ -591,6 +600,49 @@ int bg_pft_full(bg_geometry *g, double wr, double wi, const double *J, const dou
   cudaFreeAsync(d, stream());
   cudaError_t e2 = cudaStreamSynchronize(stream());
   if (!st && e2 != cudaSuccess) { set_error("pft: %s", cudaGetErrorString(e2)); st = BG_ERR_CUDA; }
+  return st;
+}
+
+static int fields_args(const char *fn, bg_geometry *g, const double *E0, const double *nhat, int npts,
+                       const void *X, const void *out) {
+  if (!g || npts < 0 || (npts > 0 && (!X || !out))) { set_error("%s: bad arguments", fn); return BG_ERR_ARG; }
+  if (E0 && !nhat) { set_error("%s: the plane wave needs nhat", fn); return BG_ERR_ARG; }
+  return BG_OK;
+}
+
+int bg_get_fields(bg_geometry *g, double wr, double wi, const double *J, const double *E0, const double *nhat,
+                  int npts, const double *X, double *out) {
+  int st = fields_args("bg_get_fields", g, E0, nhat, npts, X, out);
+  if (st || npts == 0) return st;
+  if ((st = upload_geometry(g))) return st;
+  size_t jb = J ? 16 * (size_t)g->N : 0, xb = 24 * (size_t)npts, ob = 96 * (size_t)npts;
+  char *d = nullptr;
+  BG_CUDA_TRY(cudaMallocAsync((void **)&d, jb + xb + ob, stream()));
+  void *dJ = J ? d : nullptr;
+  double *dX = (double *)(d + jb);
+  void *dO = d + jb + xb;
+  cudaError_t e = cudaSuccess;
+  if (J) e = cudaMemcpyAsync(dJ, J, jb, cudaMemcpyHostToDevice, stream());
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dX, X, xb, cudaMemcpyHostToDevice, stream());
+  if (e != cudaSuccess) { set_error("H2D: %s", cudaGetErrorString(e)); st = BG_ERR_CUDA; }
+  if (!st) st = get_fields(g, wr, wi, dJ, E0, E0 ? nhat : nullptr, npts, dX, dO);
+  if (!st) {
+    e = cudaMemcpyAsync(out, dO, ob, cudaMemcpyDeviceToHost, stream());
+    if (e != cudaSuccess) { set_error("D2H: %s", cudaGetErrorString(e)); st = BG_ERR_CUDA; }
+  }
+  cudaFreeAsync(d, stream());
+  cudaError_t e2 = cudaStreamSynchronize(stream());
+  if (!st && e2 != cudaSuccess) { set_error("get_fields: %s", cudaGetErrorString(e2)); st = BG_ERR_CUDA; }
+  return st;
+}
+
+int bg_get_fields_device(bg_geometry *g, double wr, double wi, const void *J_dev, const double *E0,
+                         const double *nhat, int npts, const double *X_dev, void *out_dev) {
+  int st = fields_args("bg_get_fields_device", g, E0, nhat, npts, X_dev, out_dev);
+  if (st || npts == 0) return st;
+  st = get_fields(g, wr, wi, J_dev, E0, E0 ? nhat : nullptr, npts, X_dev, out_dev);
+  cudaError_t e2 = cudaStreamSynchronize(stream());
+  if (!st && e2 != cudaSuccess) { set_error("get_fields: %s", cudaGetErrorString(e2)); st = BG_ERR_CUDA; }
   return st;
 }
 

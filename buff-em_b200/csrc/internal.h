@@ -138,6 +138,7 @@ struct bg_geometry {
   bool uploaded = false, precomputed = false;
   bg::NearGraph graph;
   double *d_scratch = nullptr;  // general scratch (PFT partial sums etc.)
+  double *d_fieldTet = nullptr, *d_fieldFace = nullptr;  // GetFields tables, 16 doubles per tet each
   size_t scratch_bytes = 0;
 };
 
@@ -177,6 +178,10 @@ int opft_enqueue(bg_geometry *g, double wr, double wi, const void *dJ, const dou
                  double *out_dev);
 int pft(bg_geometry *g, double wr, double wi, const void *dJ, const double *E0, const double *nhat, int method,
         double *out);
+// fields at npts points (device X: 3 per point; out: 6 complex per point);
+// dJ may be null (incident field only), E0/nhat null (no incident field)
+int get_fields(bg_geometry *g, double wr, double wi, const void *dJ, const double *E0, const double *nhat,
+               int npts, const double *dX, void *dOut);
 int pft_emt_full(bg_geometry *g, double wr, double wi, const void *dJ, const double *E0, const double *nhat,
                  double *out);
 int lu_factor(bg_matrix *m);

@@ -322,6 +322,21 @@ int bg_pft(bg_geometry *g, double omega_re, double omega_im, const double *J_hos
 int bg_pft_full(bg_geometry *g, double omega_re, double omega_im, const double *J_host, const double *E0,
                 const double *nhat, double *out);
 
+/* SWGGeometry::GetFields(IF, J, Omega, XMatrix, FMatrix), GetFields.cc:287-382:
+   total fields at npts points X (host, 3 doubles per point): the plane wave
+   E0/nhat (pass E0 = NULL for none; IF = 0 in the reference) plus the fields
+   of the currents J (N complex on the host, or NULL for none; J = 0 in the
+   reference), each basis function integrated with the 4-point rule when
+   |X - centroid| / radius > 10 and the 16-point rule otherwise
+   (Get1BFFields, GetFields.cc:265-281).  out: npts x 6 complex, point-major
+   (Ex, Ey, Ez, Hx, Hy, Hz per point), the rows of the reference's FMatrix.
+   A point closer than 1e-12 to a quadrature point skips that point. */
+int bg_get_fields(bg_geometry *g, double omega_re, double omega_im, const double *J_host, const double *E0,
+                  const double *nhat, int npts, const double *X_host, double *out_host);
+/* Same on device buffers (J_dev may be NULL); synchronizes the library stream. */
+int bg_get_fields_device(bg_geometry *g, double omega_re, double omega_im, const void *J_dev, const double *E0,
+                         const double *nhat, int npts, const double *X_dev, void *out_dev);
+
 /* The reference's FIBBI cache file (FIBBICache::Store / PreLoad,
    FIBBICache.cc:272-463): "FIBBI_GCACHE\0", then records of 27 float keys
    (GetFIBBICacheKey, FIBBICache.cc:133-160) and the 6 static near-field

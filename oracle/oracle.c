@@ -1268,6 +1268,92 @@ void or_pft_emt8(OGeom *G, double wr, double wi, const double *J, const double *
   free(scat); free(ext);
 }
 
+/* ------------------------------------------------------------------------- */
+/* Fields at points (SWGGeometry::GetFields, GetFields.cc:176-382): incident   */
+/* plane wave (H = nhat x E / Z0) plus sum_a J_a of the fields of basis        */
+/* function a, BFInt with the 4-point rule when |X - centroid| > 10 radius,    */
+/* else the 16-point rule.  The dyadic kernels restate the vacuum fields of a  */
+/* volume current (e^{-i w t}, g = e^{ikr}/(4 pi r), R = X - y):                */
+/*   E = i w Z0 g [(1 + i/kr - 1/kr^2) J + (-1 - 3i/kr + 3/kr^2) (Rh.J) Rh]     */
+/*   H = g (ik - 1/r) Rh x J                                                     */
+/* ------------------------------------------------------------------------- */
+static void bf_fields(OObj *O, int a, cplx w, const double *X, cplx EH[6])
+{
+  OFace *F = O->F[a];
+  double rrel = dist3(X, F->cen) / F->radius;
+  int npts = rrel > 10.0 ? 4 : 16;
+  const double *cr = tet_rule(npts);
+  cplx k = w;
+  for (int i = 0; i < 6; i++) EH[i] = 0;
+  for (int side = 0; side < 2; side++) {
+    int nt = side == 0 ? F->iPTet : F->iMTet, iq = side == 0 ? F->PIndex : F->MIndex;
+    OTet *T = O->T + nt;
+    double sign = side == 0 ? 1.0 : -1.0;
+    const double *Q = O->V + 3 * T->VI[iq];
+    double L1[3], L2[3], L3[3];
+    for (int c = 0; c < 3; c++) {
+      L1[c] = O->V[3 * T->VI[(iq + 1) % 4] + c] - Q[c];
+      L2[c] = O->V[3 * T->VI[(iq + 2) % 4] + c] - Q[c];
+      L3[c] = O->V[3 * T->VI[(iq + 3) % 4] + c] - Q[c];
+    }
+    double pf = sign * O->F[T->FI[iq]]->area / (3.0 * T->vol);
+    for (int i = 0; i < npts; i++) {
+      double wt = 6.0 * T->vol * cr[4 * i + 3], y[3], b[3];
+      for (int c = 0; c < 3; c++) {
+        b[c] = cr[4 * i] * L1[c] + cr[4 * i + 1] * L2[c] + cr[4 * i + 2] * L3[c];
+        y[c] = Q[c] + b[c];
+        b[c] *= pf;
+      }
+      double R[3] = {X[0] - y[0], X[1] - y[1], X[2] - y[2]};
+      double r = sqrt(R[0] * R[0] + R[1] * R[1] + R[2] * R[2]);
+      if (r < 1.0e-12) continue;
+      double Rh[3] = {R[0] / r, R[1] / r, R[2] / r};
+      cplx ikr = I * k * r;
+      cplx g = cexp(ikr) / (4.0 * M_PI * r);
+      cplx t1 = 1.0 - 1.0 / ikr + 1.0 / (ikr * ikr);          /* 1 + i/kr - 1/kr^2 */
+      cplx t2 = -1.0 + 3.0 / ikr - 3.0 / (ikr * ikr);         /* -1 - 3i/kr + 3/kr^2 */
+      double rb = Rh[0] * b[0] + Rh[1] * b[1] + Rh[2] * b[2];
+      cplx ep = I * w * ZVAC * g * wt, hp = g * (I * k - 1.0 / r) * wt;
+      for (int c = 0; c < 3; c++) EH[c] += ep * (t1 * b[c] + t2 * rb * Rh[c]);
+      EH[3] += hp * (Rh[1] * b[2] - Rh[2] * b[1]);
+      EH[4] += hp * (Rh[2] * b[0] - Rh[0] * b[2]);
+      EH[5] += hp * (Rh[0] * b[1] - Rh[1] * b[0]);
+    }
+  }
+}
+
+/* X: npts x 3; J: N complex (may be NULL: incident only); E0/nhat may be NULL
+   (no incident field); out: npts x 6 complex (Ex, Ey, Ez, Hx, Hy, Hz) */
+void or_get_fields(OGeom *G, double wr, double wi, const double *J, const double *E0, const double *nhat, int npts,
+                   const double *X, double *out)
+{
+  cplx w = wr + I * wi;
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int p = 0; p < npts; p++) {
+    const double *x = X + 3 * p;
+    cplx F[6] = {0, 0, 0, 0, 0, 0};
+    if (E0 && nhat) {
+      cplx ph = cexp(I * w * (nhat[0] * x[0] + nhat[1] * x[1] + nhat[2] * x[2]));
+      cplx E[3];
+      for (int c = 0; c < 3; c++) E[c] = (E0[2 * c] + I * E0[2 * c + 1]) * ph;
+      for (int c = 0; c < 3; c++) F[c] = E[c];
+      F[3] = (nhat[1] * E[2] - nhat[2] * E[1]) / ZVAC;
+      F[4] = (nhat[2] * E[0] - nhat[0] * E[2]) / ZVAC;
+      F[5] = (nhat[0] * E[1] - nhat[1] * E[0]) / ZVAC;
+    }
+    if (J)
+      for (int a = 0; a < G->N; a++) {
+        int no, nf;
+        OObj *O = resolve(G, a, &no, &nf);
+        cplx EH[6];
+        bf_fields(O, nf, w, x, EH);
+        cplx Ja = J[2 * a] + I * J[2 * a + 1];
+        for (int c = 0; c < 6; c++) F[c] += Ja * EH[c];
+      }
+    for (int c = 0; c < 6; c++) { out[12 * p + 2 * c] = creal(F[c]); out[12 * p + 2 * c + 1] = cimag(F[c]); }
+  }
+}
+
 /* OPFT absorbed power (OPFT.cc:62-119 with OverlapIntegrand_PFT's PAbs term,
    OverlapIntegrals.cc:51-170,242-298): PAbs = sum Re(conj(Ja) Jb ME_ab),
    ME_ab = 1/2 int bA . (i Z0/w) (eps-1)^-1 . bB over the shared tets. */

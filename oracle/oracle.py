@@ -83,6 +83,7 @@ def lib():
         L.or_rhs_planewave.argtypes = [P, D, D, dp, dp, dp]
         L.or_pft_emt.argtypes = [P, D, D, dp, dp, dp, dp]
         L.or_pft_emt8.argtypes = [P, D, D, dp, dp, dp, dp]
+        L.or_get_fields.argtypes = [P, D, D, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, dp, dp]
         L.or_pft_opft.argtypes = [P, D, D, dp, dp]
         L.or_num_threads.restype = I
         L.or_cache_build.argtypes = [P]
@@ -205,6 +206,17 @@ class Geometry:
         out = np.zeros(8 * self.nobj)
         lib().or_pft_emt8(self.h, omega.real, omega.imag, Jd, E, nh, out)
         return out.reshape(self.nobj, 8)
+
+    def get_fields(self, omega, J, X, E0=None, nhat=None):
+        """(P, 6) complex: E and H at the points X (P x 3); J and/or the plane wave may be None."""
+        X = np.ascontiguousarray(X, dtype=np.float64).reshape(-1, 3)
+        out = np.zeros(12 * len(X))
+        Jd = None if J is None else np.ascontiguousarray(J, dtype=np.complex128).view(np.float64)
+        E = None if E0 is None else np.asarray(E0, dtype=np.complex128).view(np.float64).copy()
+        nh = None if nhat is None else np.asarray(nhat, dtype=np.float64).copy()
+        ptr = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)
+        lib().or_get_fields(self.h, omega.real, omega.imag, ptr(Jd), ptr(E), ptr(nh), len(X), X, out)
+        return out.view(np.complex128).reshape(len(X), 6)
 
     def pft_opft(self, omega, J):
         Jd = np.ascontiguousarray(J, dtype=np.complex128).view(np.float64)

@@ -109,3 +109,25 @@ def test_fibbi_load_rejects_foreign_files(buffem_lib, tmp_path, ref_mesh):
     with pytest.raises(buffem_lib.BuffError) as e:
         G.PreloadFIBBICache(str(short))
     assert e.value.status == buffem_lib.BG_ERR_IO
+
+
+def test_get_fields_rejects_bad_arguments(buffem_lib, ref_mesh):
+    """GetFields checks its arguments before any device work: a negative
+    point count, missing points or output, a plane wave without nhat; zero
+    points is a no-op."""
+    import ctypes as C
+    import numpy as np
+    L = buffem_lib.lib()
+    G = buffem_lib.SWGGeometry(meshfiles=ref_mesh("sphere48"), materials=buffem_lib.Material(eps=10.0))
+    X = np.zeros((2, 3))
+    out = np.zeros(24)
+    E0 = np.zeros(6)
+    p = lambda a: a.ctypes.data_as(C.c_void_p)
+    assert L.bg_get_fields(G.h, 1.0, 0.0, None, None, None, -1, p(X), p(out)) == buffem_lib.BG_ERR_ARG
+    assert L.bg_get_fields(G.h, 1.0, 0.0, None, None, None, 2, None, p(out)) == buffem_lib.BG_ERR_ARG
+    assert L.bg_get_fields(G.h, 1.0, 0.0, None, None, None, 2, p(X), None) == buffem_lib.BG_ERR_ARG
+    assert L.bg_get_fields(G.h, 1.0, 0.0, None, p(E0), None, 2, p(X), p(out)) == buffem_lib.BG_ERR_ARG
+    assert L.bg_get_fields(None, 1.0, 0.0, None, None, None, 2, p(X), p(out)) == buffem_lib.BG_ERR_ARG
+    assert L.bg_get_fields(G.h, 1.0, 0.0, None, None, None, 0, None, None) == 0
+    with pytest.raises(ValueError):
+        G.GetFields(None, np.zeros(G.TotalBFs + 1, complex), 1.0, X)

@@ -219,3 +219,70 @@ def test_oracle_emt_force_and_torque(oracle_lib, sphere):
         sym.append(max(np.abs(p8[2:4]).max(), np.abs(p8[5:]).max()) / p8[4])
     assert errs[2] < errs[1] < errs[0], errs
     assert sym[2] < sym[1] < sym[0] and sym[2] < 0.05, sym
+
+
+def _fd_curls(G, w, J, x, E0=None, nh=None, h=1e-4):
+    pts = [x]
+    for c in range(3):
+        for s in (1, -1):
+            y = x.copy()
+            y[c] += s * h
+            pts.append(y)
+    F = G.get_fields(w, J, np.array(pts), E0, nh)
+    d = np.array([(F[1 + 2 * c] - F[2 + 2 * c]) / (2 * h) for c in range(3)])
+
+    def curl(o):
+        return np.array([d[1, o + 2] - d[2, o + 1], d[2, o] - d[0, o + 2], d[0, o + 1] - d[1, o]])
+    return F[0], curl(0), curl(3)
+
+
+def test_oracle_fields_satisfy_maxwell(oracle_lib, sphere):
+    """GetFields (GetFields.cc:176-382) outside a sphere: the fields of the
+    solved currents, with and without the incident plane wave, satisfy the
+    source-free curl equations curl E = i w Z0 H and curl H = -i w E / Z0
+    (finite differences, h = 1e-4), at a real and a complex frequency."""
+    Z0 = 376.73031346177
+    rng = np.random.default_rng(0)
+    E0, nh = np.array([1, 0.4j, -0.3j], complex), np.array([0, 0.6, 0.8])   # transverse wave
+    G = oracle_lib.Geometry(sphere(3), oracle_lib.material(eps=4 + 0.2j), nang=6)
+    for w in (1.0 + 0j, 0.8 + 0.05j):
+        J = sl.lu_solve(sl.lu_factor(G.assemble(w)), G.rhs_planewave(w, E0, nh))
+        for x in rng.normal(size=(3, 3)):
+            x *= rng.uniform(1.5, 4.0) / np.linalg.norm(x)
+            for inc in (False, True):
+                F, cE, cH = _fd_curls(G, w, J, x, E0 if inc else None, nh if inc else None)
+                assert np.abs(cE - 1j * w * Z0 * F[3:]).max() <= 1e-6 * np.abs(cE).max()
+                assert np.abs(cH + 1j * w / Z0 * F[:3]).max() <= 1e-6 * np.abs(cH).max()
+
+
+def _sphere_flux(G, w, J, R, E0=None, nh=None, nt=24, nph=48):
+    x, wq = np.polynomial.legendre.leggauss(nt)
+    ph = np.linspace(0, 2 * np.pi, nph, endpoint=False)
+    st = np.sqrt(1 - x * x)
+    pts = R * np.stack([np.outer(st, np.cos(ph)), np.outer(st, np.sin(ph)), np.outer(x, np.ones(nph))], -1)
+    pts = pts.reshape(-1, 3)
+    ws = np.repeat(wq, nph) * (2 * np.pi / nph) * R * R
+    F = G.get_fields(w, J, pts, E0, nh)
+    S = 0.5 * np.real(np.cross(F[:, :3], np.conj(F[:, 3:])))
+    return float(np.sum(ws * np.sum(S * pts / R, axis=1)))
+
+
+def test_oracle_scattered_flux_matches_emt(oracle_lib, sphere):
+    """The Poynting flux of the scattered fields through a sphere around the
+    body is the same at every radius (energy conservation of the GetFields
+    kernels) and converges to the EMT scattered power of the same currents
+    as the mesh is refined; the flux of the total fields is minus the
+    absorbed power, which it matches to the overlap-method PAbs (OPFT.cc)."""
+    w = 1.0 + 0j
+    E0, nh = np.array([1, 0, 0], complex), np.array([0, 0, 1.0])
+    rel = []
+    for n in (3, 4):
+        G = oracle_lib.Geometry(sphere(n), oracle_lib.material(eps=4 + 0.2j), nang=6)
+        J = sl.lu_solve(sl.lu_factor(G.assemble(w)), G.rhs_planewave(w, E0, nh))
+        emt = G.pft_emt(w, J, E0, nh)[0]
+        f1, f2 = _sphere_flux(G, w, J, 1.5), _sphere_flux(G, w, J, 3.0)
+        assert abs(f1 / f2 - 1) < 1e-6, (f1, f2)
+        rel.append(abs(f2 / emt[1] - 1))
+        ftot = _sphere_flux(G, w, J, 3.0, E0, nh)
+        assert abs(-ftot / G.pft_opft(w, J)[0] - 1) < 2e-3
+    assert rel[1] < 0.6 * rel[0] and rel[1] < 0.02, rel
