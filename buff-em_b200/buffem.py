@@ -81,6 +81,7 @@ EXPORTS = [
     "bg_precond_create_learned", "bg_precond_download", "bg_gmres_solve_mixed", "bg_gmres_solve_mixed_device",
     "bg_precond_bound", "bg_gmres_solve_lu_fallback", "bg_gmres_solve_lu_fallback_device", "bg_batch_sweep",
     "bg_pft_full", "bg_fibbi_store", "bg_fibbi_load", "bg_get_fields", "bg_get_fields_device",
+    "bg_neq_create", "bg_neq_destroy", "bg_neq_flux", "bg_neq_dressed_rytov", "bg_pft_dr_device",
 ]
 
 
@@ -141,6 +142,12 @@ def lib():
         L.bg_pft.argtypes = [P, D, D, VP, VP, VP, I, VP]
         L.bg_pft_full.argtypes = [P, D, D, VP, VP, VP, VP]
         L.bg_get_fields.argtypes = [P, D, D, VP, VP, VP, C.c_int, VP, VP]
+        L.bg_neq_create.argtypes = [P, C.POINTER(P)]
+        L.bg_neq_destroy.argtypes = [P]
+        L.bg_neq_destroy.restype = None
+        L.bg_neq_flux.argtypes = [P, D, D, VP]
+        L.bg_neq_dressed_rytov.argtypes = [P, D, D, I, VP]
+        L.bg_pft_dr_device.argtypes = [P, D, D, VP, I, VP]
         L.bg_get_fields_device.argtypes = [P, D, D, VP, VP, VP, C.c_int, VP, VP]
         L.bg_fibbi_store.argtypes = [P, I, C.c_char_p, C.POINTER(I)]
         L.bg_fibbi_load.argtypes = [P, I, C.c_char_p, C.POINTER(I)]
@@ -358,6 +365,40 @@ class SWGGeometry:
         E0 = _ptr(IF.E0) if IF is not None else None
         nh = _ptr(IF.nHat) if IF is not None else None
         _check(lib().bg_pft(self.h, Omega.real, Omega.imag, _ptr(Jc), E0, nh, method, _ptr(out)))
+        return out
+
+
+class NEQ:
+    """buff-neq's flux chain for one geometry (GetFlux, GetFlux.cc:291-436)
+    at a uniform temperature per object; the geometry as it stands is the
+    single transform.  Holds S^-1 and three N x N work matrices on the device."""
+
+    def __init__(self, G):
+        h = C.c_void_p()
+        _check(lib().bg_neq_create(G.h, C.byref(h)))
+        self.h, self.G = h, G
+
+    def __del__(self):
+        if getattr(self, "h", None) and lib is not None:   # lib is None at interpreter exit
+            lib().bg_neq_destroy(self.h)
+            self.h = None
+
+    def GetFlux(self, Omega):
+        """flux[s, d, q]: source s, destination d, q = PAbs, PRad, Fx, Fy, Fz,
+        Tx, Ty, Tz (EMT, the buff-neq default); multiply by Delta Theta to get
+        the spectral density of power or force."""
+        Omega = complex(Omega)
+        NO = self.G.NumObjects
+        out = np.zeros((NO, NO, 8))
+        _check(lib().bg_neq_flux(self.h, Omega.real, Omega.imag, _ptr(out)))
+        return out
+
+    def DressedRytov(self, Omega, src):
+        """DR_src = W S^-1 R_src S^-1 W^H (ComputeDressedRytovMatrix), N x N."""
+        Omega = complex(Omega)
+        N = self.G.TotalBFs
+        out = np.zeros((N, N), complex, order="F")
+        _check(lib().bg_neq_dressed_rytov(self.h, Omega.real, Omega.imag, src, _ptr(out)))
         return out
 
 

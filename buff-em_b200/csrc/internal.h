@@ -182,6 +182,12 @@ int pft(bg_geometry *g, double wr, double wi, const void *dJ, const double *E0, 
 // dJ may be null (incident field only), E0/nhat null (no incident field)
 int get_fields(bg_geometry *g, double wr, double wi, const void *dJ, const double *E0, const double *nhat,
                int npts, const double *dX, void *dOut);
+// EMT PFT with a dressed Rytov matrix (device, column-major ldr) and no incident field
+int pft_emt_dr(bg_geometry *g, double wr, double wi, const void *dDR, size_t ldr, double *out);
+// buff-neq overlap rows: 8 slots per basis function (idx -1 past cnt[a])
+int neq_overlaps(bg_geometry *g, double w, int *idx, double *S, void *V, double *R, int *cnt);
+// B <- A^{-1} B for many right-hand sides (GEMM-based triangular solves; complex128)
+int lu_solve_many(bg_matrix *m, void *dB, size_t ldb, int nrhs);
 int pft_emt_full(bg_geometry *g, double wr, double wi, const void *dJ, const double *E0, const double *nhat,
                  double *out);
 int lu_factor(bg_matrix *m);

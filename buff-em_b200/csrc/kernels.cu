@@ -896,6 +896,8 @@ struct PftArgs {
   double w;      // real(omega)
   double absw;   // |omega|
   int nobj;
+  const cd *DR = nullptr;   // dressed Rytov matrix (column-major, ldr) in place of J
+  size_t ldr = 0;
 };
 
 __device__ __forceinline__ void rule_point(int npts, int i, double *u) {
@@ -998,10 +1000,17 @@ __device__ void scat_q(const PftArgs &P, int a, int b, int npts, bool same, int 
 
 // contributions of pair (a, b) to the per-object-pair sums (EMTPFT.cc:416-436)
 __device__ __forceinline__ void scat_terms(const PftArgs &P, int a, int b, const cd q[NPQ], bool same, double d[NPQ]) {
-  cd Ja = P.J[a], Jb = P.J[b];
   const double Z0 = 376.73031346177;
-  // u0JJ = Z0 conj(Ja) Jb
-  cd u = cmk(Z0 * (Ja.r * Jb.r + Ja.i * Jb.i), Z0 * (Ja.r * Jb.i - Ja.i * Jb.r));
+  // u0JJ = Z0 GetJJ(a, b) (GetPFT.cc:108-115): Z0 DR(b, a) for a dressed
+  // Rytov matrix, else Z0 conj(Ja) Jb
+  cd u;
+  if (P.DR) {
+    cd v = P.DR[(size_t)b + (size_t)a * P.ldr];
+    u = cmk(Z0 * v.r, Z0 * v.i);
+  } else {
+    cd Ja = P.J[a], Jb = P.J[b];
+    u = cmk(Z0 * (Ja.r * Jb.r + Ja.i * Jb.i), Z0 * (Ja.r * Jb.i - Ja.i * Jb.r));
+  }
   if (same) {
     d[0] = u.r * q[0].i;
     for (int n = 1; n < NPQ; n++) d[n] = a != b ? u.i * q[n].i : 0.0;
@@ -1297,13 +1306,13 @@ int pft(bg_geometry *g, double wr, double wi, const void *dJ, const double *E0, 
 // GetPFTMatrix with EMT (GetPFT.cc:133-189, EMTPFT.cc:324-493): out[8*no + c],
 // c = PAbs, PScat, Fx, Fy, Fz, Tx, Ty, Tz (force and torque in the
 // reference's units, TENTHIRDS = 10/3), plane-wave incident field
-int pft_emt_full(bg_geometry *g, double wr, double wi, const void *dJ, const double *E0, const double *nhat,
-                 double *out) {
+static int pft_emt_impl(bg_geometry *g, double wr, double wi, const void *dJ, const void *dDR, size_t ldr,
+                        const double *E0, const double *nhat, double *out) {
   int st = init_tables();
   if (st) return st;
   int NO = (int)g->objs.size();
   if (NO > PMAXOBJ) { set_error("PFT supports at most %d objects", PMAXOBJ); return BG_ERR_ARG; }
-  PftArgs P{g->dev, (const cd *)dJ, wr, std::sqrt(wr * wr + wi * wi), NO};
+  PftArgs P{g->dev, (const cd *)dJ, wr, std::sqrt(wr * wr + wi * wi), NO, (const cd *)dDR, ldr};
   int nrow = (g->N + 127) / 128;
   if ((st = build_near_lists(g))) return st;
   int nb = (g->N + FT - 1) / FT;
@@ -1319,9 +1328,13 @@ int pft_emt_full(bg_geometry *g, double wr, double wi, const void *dJ, const dou
     k_pft_near<<<nnear_blocks, 256, 0, stream()>>>(P, g->near, pnear);
     BG_LAUNCHED();
   }
-  PWave pw = make_pw(wr, wi, E0, nhat);
-  k_pft_ext<<<nrow, 128, 0, stream()>>>(P, pw, pext);
-  BG_LAUNCHED();
+  if (E0) {
+    PWave pw = make_pw(wr, wi, E0, nhat);
+    k_pft_ext<<<nrow, 128, 0, stream()>>>(P, pw, pext);
+    BG_LAUNCHED();
+  } else {
+    BG_CUDA_TRY(cudaMemsetAsync(pext, 0, sizeof(double) * next, stream()));
+  }
   std::vector<double> h(nfar + nnear + next);
   BG_CUDA_TRY(cudaMemcpyAsync(h.data(), g->d_scratch, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, stream()));
   BG_CUDA_TRY(cudaStreamSynchronize(stream()));
@@ -1349,6 +1362,130 @@ int pft_emt_full(bg_geometry *g, double wr, double wi, const void *dJ, const dou
       r[5 + i] = ftf * (e[4 + i] + e[7 + i]) - s[4 + i] - s[7 + i];
     }
   }
+  return BG_OK;
+}
+
+int pft_emt_full(bg_geometry *g, double wr, double wi, const void *dJ, const double *E0, const double *nhat,
+                 double *out) {
+  return pft_emt_impl(g, wr, wi, dJ, nullptr, 0, E0, nhat, out);
+}
+
+// GetPFTMatrix(0, Omega, {EMT, DRMatrix}) as buff-neq calls it (GetFlux.cc:391-399):
+// the pair sums with JJ = DR(b, a) and no incident field
+int pft_emt_dr(bg_geometry *g, double wr, double wi, const void *dDR, size_t ldr, double *out) {
+  return pft_emt_impl(g, wr, wi, nullptr, dDR, ldr, nullptr, nullptr, out);
+}
+
+// =========================================================================
+// Overlap blocks for buff-neq (GetOverlaps, VIEMatrix.cc:122-316, and
+// GetOverlapElements, SWGVolume.cc:405-481), row a: up to 7 columns b with
+//   S_ab  = int b_a . b_b (closed form),
+//   V_ab  = -w^2 int b_a . (eps - 1) b_b,
+//   R_ab  = 4 w / (pi Z0) int b_a . Im(eps - 1) b_b   (uniform temperature),
+// w = real(omega), the V and R integrals by the 33-point rule on each
+// tetrahedron of a.  Slot 0 is the diagonal; cnt[a] is the number of slots.
+// =========================================================================
+__global__ void k_neq_overlaps(DevGeom g, double w, int *idx, double *S, cd *V, double *R, int *cnt) {
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= g.N) return;
+  int2 tt = g.bfTet[a], qq = g.bfQ[a];
+  int4 fv = g.bfV[a];
+  double Aa = g.bfArea[a];
+  double cen[3], P1[3], P2[3], P3[3];
+  load3(g.V4, fv.x, P1); load3(g.V4, fv.y, P2); load3(g.V4, fv.z, P3);
+  for (int c = 0; c < 3; c++) cen[c] = (P1[c] + P2[c] + P3[c]) / 3.0;
+  int nnz = 1;
+  int ix[8];
+  double sv[8], rv[8];
+  cd vv[8];
+  ix[0] = a; sv[0] = 0.0; rv[0] = 0.0; vv[0] = cmk(0, 0);
+  const double rpre = 4.0 * w / (M_PI * 376.73031346177), vpre = -w * w;
+  for (int side = 0; side < 2; side++) {
+    int t = side == 0 ? tt.x : tt.y;
+    double sa = side == 0 ? 1.0 : -1.0;
+    const bg_material &mat = g.mats[g.tetObj[t]];
+    double vol = g.tetVol[t];
+    double QA[3];
+    load3(g.V4, side == 0 ? qq.x : qq.y, QA);
+    // closed-form Gram terms of this tetrahedron
+    double L2s = 0.0, XmQ[3], XmQ2 = 0.0;
+    for (int c = 0; c < 3; c++) {
+      double d1 = P1[c] - QA[c], d2 = P2[c] - QA[c], d3 = P3[c] - QA[c];
+      L2s += d1 * d1 + d2 * d2 + d3 * d3;
+      XmQ[c] = cen[c] - QA[c];
+      XmQ2 += XmQ[c] * XmQ[c];
+    }
+    sv[0] += Aa * Aa * (XmQ2 / 20.0 + L2s / 180.0) / vol;
+    double pa = sa * Aa / (3.0 * vol);
+    int4 vi = g.tetVI[t];
+    double V0[3], L[3][3];
+    load3(g.V4, vi.x, V0);
+    int vq[3] = {vi.y, vi.z, vi.w};
+    for (int i = 0; i < 3; i++) {
+      double tmp[3];
+      load3(g.V4, vq[i], tmp);
+      for (int c = 0; c < 3; c++) L[i][c] = tmp[c] - V0[c];
+    }
+    int4 fi = g.tetFI[t];
+    int fl[4] = {fi.x, fi.y, fi.z, fi.w};
+    for (int ifb = 0; ifb < 4; ifb++) {
+      int b = fl[ifb];
+      if (b < 0) continue;
+      int2 tb = g.bfTet[b], qb = g.bfQ[b];
+      double QB[3], pb, sb;
+      if (tb.x == t) { load3(g.V4, qb.x, QB); sb = 1.0; }
+      else { load3(g.V4, qb.y, QB); sb = -1.0; }
+      pb = sb * g.bfArea[b] / (3.0 * vol);
+      cd accv = cmk(0, 0);
+      double accr = 0.0;
+      for (int i = 0; i < 33; i++) {
+        const double *u = c_tcr33 + 4 * i;
+        double wt = 6.0 * vol * u[3], x[3];
+        for (int c = 0; c < 3; c++) x[c] = V0[c] + u[0] * L[0][c] + u[1] * L[1][c] + u[2] * L[2][c];
+        cd E[3][3];
+        mat_eval(mat, x, E);
+        E[0][0].r -= 1.0; E[1][1].r -= 1.0; E[2][2].r -= 1.0;
+        double FA[3], FB[3];
+        for (int c = 0; c < 3; c++) { FA[c] = pa * (x[c] - QA[c]); FB[c] = pb * (x[c] - QB[c]); }
+        cd v = cmk(0, 0);
+        double r = 0.0;
+        for (int mu = 0; mu < 3; mu++)
+          for (int nu = 0; nu < 3; nu++) {
+            v = cadd(v, cscale(E[mu][nu], FA[mu] * FB[nu]));
+            r += FA[mu] * E[mu][nu].i * FB[nu];
+          }
+        accv = cadd(accv, cscale(v, vpre * wt));
+        accr += rpre * r * wt;
+      }
+      if (b == a) {
+        vv[0] = cadd(vv[0], accv);
+        rv[0] += accr;
+      } else {
+        double pf = 2.0 * sa * sb * Aa * g.bfArea[b] / (3.0 * vol);
+        double xd = XmQ[0] * (QA[0] - QB[0]) + XmQ[1] * (QA[1] - QB[1]) + XmQ[2] * (QA[2] - QB[2]);
+        ix[nnz] = b;
+        sv[nnz] = pf * (3.0 * XmQ2 / 40.0 + L2s / 120.0 + xd / 8.0);
+        vv[nnz] = accv;
+        rv[nnz] = accr;
+        nnz++;
+      }
+    }
+  }
+  for (int i = 0; i < 8; i++) {
+    size_t o = 8 * (size_t)a + i;
+    idx[o] = i < nnz ? ix[i] : -1;
+    S[o] = i < nnz ? sv[i] : 0.0;
+    V[o] = i < nnz ? vv[i] : cmk(0, 0);
+    R[o] = i < nnz ? rv[i] : 0.0;
+  }
+  cnt[a] = nnz;
+}
+
+int neq_overlaps(bg_geometry *g, double w, int *idx, double *S, void *V, double *R, int *cnt) {
+  int st = init_tables();
+  if (st) return st;
+  k_neq_overlaps<<<(g->N + 127) / 128, 128, 0, stream()>>>(g->dev, w, idx, S, (cd *)V, R, cnt);
+  BG_LAUNCHED();
   return BG_OK;
 }
 

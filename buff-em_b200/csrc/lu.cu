@@ -807,6 +807,37 @@ static int getrs(bg_matrix *m, C *B, size_t ldb, int nrhs) {
   return BG_OK;
 }
 
+// Many right-hand sides (N-column blocks of the buff-neq chain): one row
+// gather by the factor permutation, then the recursive GEMM-based triangular
+// solves used inside the factorisation (unit L, then U), in column chunks so
+// the scratch stays bounded.
+int lu_solve_many(bg_matrix *m, void *dB, size_t ldb, int nrhs) {
+  if (!m->d_perm) { set_error("solve: factorization state missing"); return BG_ERR_STATE; }
+  if (m->precision != BG_C128) { set_error("lu_solve_many: complex128 only"); return BG_ERR_ARG; }
+  int N = m->N;
+  const cdl *A = (const cdl *)m->d;
+  cdl *B = (cdl *)dB;
+  const int chunk = 4096;
+  cdl *T = nullptr;
+  int w = std::min(chunk, nrhs);
+  if (w <= 0) return BG_OK;
+  BG_CUDA_TRY(cudaMallocAsync((void **)&T, sizeof(cdl) * (size_t)N * w, stream()));
+  int st = BG_OK;
+  for (int r0 = 0; r0 < nrhs && !st; r0 += chunk) {
+    int nr = std::min(chunk, nrhs - r0);
+    cdl *Bp = B + (size_t)r0 * ldb;
+    k_gather_rows<cdl><<<dim3((N + 255) / 256, nr), 256, 0, stream()>>>(N, nr, m->d_perm, Bp, ldb, T, N);
+    BG_LAUNCHED();
+    if ((st = trsm<cdl>(N, nr, A, m->ld, T, N, 0))) break;
+    if ((st = trsm<cdl>(N, nr, A, m->ld, T, N, 1))) break;
+    cudaError_t e = cudaMemcpy2DAsync(Bp, sizeof(cdl) * ldb, T, sizeof(cdl) * N, sizeof(cdl) * N, nr,
+                                      cudaMemcpyDeviceToDevice, stream());
+    if (e != cudaSuccess) { set_error("lu_solve_many: %s", cudaGetErrorString(e)); st = BG_ERR_CUDA; }
+  }
+  cudaFreeAsync(T, stream());
+  return st;
+}
+
 int lu_solve(bg_matrix *m, void *dB, int ldb, int nrhs) {
   if (!m->d_perm) { set_error("solve: factorization state missing"); return BG_ERR_STATE; }
   if (m->precision == BG_C128) return getrs<cdl>(m, (cdl *)dB, (size_t)ldb, nrhs);

@@ -337,6 +337,30 @@ int bg_get_fields(bg_geometry *g, double omega_re, double omega_im, const double
 int bg_get_fields_device(bg_geometry *g, double omega_re, double omega_im, const void *J_dev, const double *E0,
                          const double *nhat, int npts, const double *X_dev, void *out_dev);
 
+/* ---------------------------------------------------------------------------
+ * buff-neq flux chain (GetFlux, GetFlux.cc:291-436; ComputeDressedRytovMatrix,
+ * GetFlux.cc:155-272) for one geometry as it stands (one transform) and a
+ * uniform temperature per object.  A handle keeps the frequency-independent
+ * inverse Gram matrix S^-1 (CreateBNEQData.cc:122-141) and three N x N
+ * complex128 work matrices on the device (4 N^2 x 16 bytes in total).
+ * ------------------------------------------------------------------------- */
+typedef struct bg_neq bg_neq;
+int bg_neq_create(bg_geometry *g, bg_neq **out);
+void bg_neq_destroy(bg_neq *h);
+/* Flux spectral densities at omega (real part nonzero): flux[(s*NO + d)*8 + q],
+   s = source object, d = destination object, q = PAbs, PRad (PScat), Fx, Fy,
+   Fz, Tx, Ty, Tz -- GetPFTMatrix(0, Omega, {EMT, DR_s}) per source object, the
+   numbers buff-neq writes to .SIFlux.EMTPFT.  W = (1 + S^-1 V S^-1 G)^-1 is
+   factored once per frequency and shared by the source objects. */
+int bg_neq_flux(bg_neq *h, double omega_re, double omega_im, double *flux);
+/* The dressed Rytov matrix DR_s = W S^-1 R_s S^-1 W^H of source object src,
+   N x N complex column-major, copied to the host. */
+int bg_neq_dressed_rytov(bg_neq *h, double omega_re, double omega_im, int src, void *out_host);
+/* GetPFTMatrix(0, Omega, {EMT, DRMatrix}) (EMTPFT.cc:324-493 with GetJJ =
+   DR(b, a), GetPFT.cc:108-115) for a device matrix DR (column-major, ld >= N):
+   out[8*obj + q] as bg_pft_full without the incident-field terms. */
+int bg_pft_dr_device(bg_geometry *g, double omega_re, double omega_im, const void *DR_dev, int ld, double *out);
+
 /* The reference's FIBBI cache file (FIBBICache::Store / PreLoad,
    FIBBICache.cc:272-463): "FIBBI_GCACHE\0", then records of 27 float keys
    (GetFIBBICacheKey, FIBBICache.cc:133-160) and the 6 static near-field

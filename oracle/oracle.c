@@ -395,6 +395,7 @@ OGeom *or_geom_create(int nobj, const char **meshfiles, const double *disp, cons
 void or_geom_set_nang(OGeom *G, int n) { G->nang = n; }
 int or_geom_nbf(OGeom *G) { return G->N; }
 int or_geom_nobj(OGeom *G) { return G->no; }
+int or_geom_bf_offset(OGeom *G, int no) { return no >= G->no ? G->N : G->off[no]; }
 int or_geom_ntets(OGeom *G, int no) { return G->O[no].nt; }
 int or_geom_nverts(OGeom *G, int no) { return G->O[no].nv; }
 
@@ -919,7 +920,7 @@ int or_overlap_closed_form(OGeom *G, int nbf, int *idx, double *vals)
 /* rows [r0,r1) only when r1 > r0 (used for bounded CPU timing samples);      */
 /* the symmetric fill is done only for a full assembly.                       */
 /* ------------------------------------------------------------------------- */
-void or_assemble_rows(OGeom *G, double wr, double wi, double *M, int r0, int r1)
+static void assemble_impl(OGeom *G, double wr, double wi, double *M, int r0, int r1, int gram)
 {
   int N = G->N;
   cplx omega = wr + I * wi;
@@ -937,6 +938,7 @@ void or_assemble_rows(OGeom *G, double wr, double wi, double *M, int r0, int r1)
       if (b > a && full) { size_t ba = 2 * ((size_t)b + (size_t)a * N); M[ba] = creal(v); M[ba + 1] = cimag(v); }
     }
     /* V^-1 block of the row (TInv->AddEntry, VIEMatrix.cc:321-360) */
+    if (!gram) continue;
     int idx[MAXOVERLAP];
     cplx vi[MAXOVERLAP];
     int nnz = overlaps(OA, nfa, creal(omega), idx, vi);
@@ -950,7 +952,77 @@ void or_assemble_rows(OGeom *G, double wr, double wi, double *M, int r0, int r1)
   }
 }
 
+void or_assemble_rows(OGeom *G, double wr, double wi, double *M, int r0, int r1)
+{
+  assemble_impl(G, wr, wi, M, r0, r1, 1);
+}
+
 void or_assemble(OGeom *G, double wr, double wi, double *M) { or_assemble_rows(G, wr, wi, M, 0, G->N); }
+
+/* the G block alone (AssembleGBlock, VIEMatrix.cc:365-426): no V^-1 Gram part */
+void or_assemble_g(OGeom *G, double wr, double wi, double *M) { assemble_impl(G, wr, wi, M, 0, G->N, 0); }
+
+/* V and Rytov entries of one row (GetOverlaps / GetOverlapIntegrand,
+   VIEMatrix.cc:122-316) for a uniform temperature (RelDeltaTheta = 1):
+   V_ab = -w^2 int b_a . (eps - 1) b_b, Rytov_ab = 4 w / (pi Z0) int b_a . Im(eps - 1) b_b,
+   w = real(omega), 33-point rule on each tetrahedron of a. */
+int or_neq_overlaps(OGeom *G, int nbf, double omega, int *idx, double *V, double *R)
+{
+  int no, a;
+  OObj *O = resolve(G, nbf, &no, &a);
+  OFace *FA = O->F[a];
+  cplx v[MAXOVERLAP];
+  double r[MAXOVERLAP];
+  idx[0] = a; v[0] = 0.0; r[0] = 0.0;
+  int nnz = 1;
+  const double *cr = tet_rule(33);
+  for (int side = 0; side < 2; side++) {
+    int nt = side == 0 ? FA->iPTet : FA->iMTet;
+    OTet *T = O->T + nt;
+    const double *QA = O->V + 3 * (side == 0 ? FA->iQP : FA->iQM);
+    double pa = (side == 0 ? 1.0 : -1.0) * FA->area / (3.0 * T->vol);
+    const double *V0 = O->V + 3 * T->VI[0];
+    double L1[3], L2[3], L3[3];
+    for (int k = 0; k < 3; k++) {
+      L1[k] = O->V[3 * T->VI[1] + k] - V0[k];
+      L2[k] = O->V[3 * T->VI[2] + k] - V0[k];
+      L3[k] = O->V[3 * T->VI[3] + k] - V0[k];
+    }
+    for (int ifb = 0; ifb < 4; ifb++) {
+      int b = T->FI[ifb];
+      if (b >= O->nif) continue;
+      OFace *FB = O->F[b];
+      const double *QB; double pb;
+      if (FB->iPTet == nt) { QB = O->V + 3 * FB->iQP; pb = FB->area / (3.0 * T->vol); }
+      else { QB = O->V + 3 * FB->iQM; pb = -FB->area / (3.0 * T->vol); }
+      cplx accv = 0.0;
+      double accr = 0.0;
+      for (int i = 0; i < 33; i++) {
+        double w = 6.0 * T->vol * cr[4 * i + 3], x[3];
+        for (int k = 0; k < 3; k++) x[k] = V0[k] + cr[4 * i] * L1[k] + cr[4 * i + 1] * L2[k] + cr[4 * i + 2] * L3[k];
+        cplx E[3][3];
+        mat_eval(&O->mat, x, E);
+        E[0][0] -= 1.0; E[1][1] -= 1.0; E[2][2] -= 1.0;
+        double FAv[3], FBv[3];
+        for (int k = 0; k < 3; k++) { FAv[k] = pa * (x[k] - QA[k]); FBv[k] = pb * (x[k] - QB[k]); }
+        cplx vv = 0.0;
+        double rr = 0.0;
+        for (int mu = 0; mu < 3; mu++)
+          for (int nu = 0; nu < 3; nu++) { vv += FAv[mu] * E[mu][nu] * FBv[nu]; rr += FAv[mu] * cimag(E[mu][nu]) * FBv[nu]; }
+        accv += w * (-omega * omega * vv);
+        accr += w * (4.0 * omega * rr / (M_PI * ZVAC));
+      }
+      if (b == a) { v[0] += accv; r[0] += accr; }
+      else { idx[nnz] = b; v[nnz] = accv; r[nnz] = accr; nnz++; }
+    }
+  }
+  for (int i = 0; i < nnz; i++) {
+    idx[i] += G->off[no];
+    V[2 * i] = creal(v[i]); V[2 * i + 1] = cimag(v[i]);
+    R[i] = r[i];
+  }
+  return nnz;
+}
 
 /* ------------------------------------------------------------------------- */
 /* plane wave (SCUFF-EM PlaneWave semantics: E = E0 exp(i k nhat.x), k = w in */
@@ -1189,15 +1261,16 @@ static void bf_ext_integrals(OObj *O, int a, const PW *pw, cplx *q0, cplx qx[3],
 }
 
 /* out[8*no + c], c = PAbs, PScat, Fx, Fy, Fz, Tx, Ty, Tz */
-void or_pft_emt8(OGeom *G, double wr, double wi, const double *J, const double *E0, const double *nhat,
-                 double *out)
+static void pft_emt8_impl(OGeom *G, double wr, double wi, const double *J, const double *DR, const double *E0,
+                          const double *nhat, double *out)
 {
   int N = G->N, NO = G->no;
   cplx omega = wr + I * wi;
   double *scat = calloc((size_t)NO * NO * 10, sizeof(double));
   double *ext = calloc((size_t)NO * 10, sizeof(double));
   PW pw;
-  for (int i = 0; i < 3; i++) { pw.E0[i] = E0[2 * i] + I * E0[2 * i + 1]; pw.nhat[i] = nhat[i]; }
+  if (E0)
+    for (int i = 0; i < 3; i++) { pw.E0[i] = E0[2 * i] + I * E0[2 * i + 1]; pw.nhat[i] = nhat[i]; }
   pw.k = omega;
 #pragma omp parallel
   {
@@ -1207,7 +1280,7 @@ void or_pft_emt8(OGeom *G, double wr, double wi, const double *J, const double *
     for (int a = 0; a < N; a++) {
       int noa, nfa;
       OObj *OA = resolve(G, a, &noa, &nfa);
-      cplx Ja = J[2 * a] + I * J[2 * a + 1];
+      cplx Ja = J ? J[2 * a] + I * J[2 * a + 1] : 0.0;
       for (int b = a; b < N; b++) {
         int nob, nfb;
         OObj *OB = resolve(G, b, &nob, &nfb);
@@ -1218,8 +1291,14 @@ void or_pft_emt8(OGeom *G, double wr, double wi, const double *J, const double *
         SC10Data D = {creal(omega), OA == OB, OA->origin};
         double q[20];
         bf_bf_int(OA, nfa, OB, nfb, scat10_integrand, &D, 20, q, npts);
-        cplx Jb = J[2 * b] + I * J[2 * b + 1];
-        cplx u0jj = ZVAC * conj(Ja) * Jb;
+        /* GetJJ (GetPFT.cc:108-115): DR(b, a) for a dressed Rytov matrix, else conj(J_a) J_b */
+        cplx u0jj;
+        if (DR) {
+          size_t ba = 2 * ((size_t)b + (size_t)a * N);
+          u0jj = ZVAC * (DR[ba] + I * DR[ba + 1]);
+        } else {
+          u0jj = ZVAC * conj(Ja) * (J[2 * b] + I * J[2 * b + 1]);
+        }
         double *d = ls + ((size_t)noa * NO + nob) * 10;
         if (noa == nob) {
           d[0] += creal(u0jj) * q[1];
@@ -1232,6 +1311,7 @@ void or_pft_emt8(OGeom *G, double wr, double wi, const double *J, const double *
           }
         }
       }
+      if (!E0) continue;
       cplx q0, qx[3], t1[3];
       bf_ext_integrals(OA, nfa, &pw, &q0, qx, t1);
       cplx ik = I * omega;
@@ -1266,6 +1346,19 @@ void or_pft_emt8(OGeom *G, double wr, double wi, const double *J, const double *
     }
   }
   free(scat); free(ext);
+}
+
+void or_pft_emt8(OGeom *G, double wr, double wi, const double *J, const double *E0, const double *nhat,
+                 double *out)
+{
+  pft_emt8_impl(G, wr, wi, J, NULL, E0, nhat, out);
+}
+
+/* GetEMTPFT with the dressed Rytov matrix of buff-neq (GetFlux.cc:391-399):
+   DR column-major N x N complex, no incident field */
+void or_pft_emt8_dr(OGeom *G, double wr, double wi, const double *DR, double *out)
+{
+  pft_emt8_impl(G, wr, wi, NULL, DR, NULL, NULL, out);
 }
 
 /* ------------------------------------------------------------------------- */

@@ -83,6 +83,12 @@ def lib():
         L.or_rhs_planewave.argtypes = [P, D, D, dp, dp, dp]
         L.or_pft_emt.argtypes = [P, D, D, dp, dp, dp, dp]
         L.or_pft_emt8.argtypes = [P, D, D, dp, dp, dp, dp]
+        L.or_assemble_g.argtypes = [P, D, D, dp]
+        L.or_geom_bf_offset.argtypes = [P, I]
+        L.or_geom_bf_offset.restype = I
+        L.or_neq_overlaps.argtypes = [P, C.c_int, D, C.c_void_p, dp, dp]
+        L.or_neq_overlaps.restype = C.c_int
+        L.or_pft_emt8_dr.argtypes = [P, D, D, dp, dp]
         L.or_get_fields.argtypes = [P, D, D, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, dp, dp]
         L.or_pft_opft.argtypes = [P, D, D, dp, dp]
         L.or_num_threads.restype = I
@@ -118,6 +124,7 @@ class Geometry:
         L.or_geom_set_nang(self.h, nang)
         self.N = L.or_geom_nbf(self.h)
         self.nobj = L.or_geom_nobj(self.h)
+        self.off = [L.or_geom_bf_offset(self.h, i) for i in range(self.nobj + 1)]
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -206,6 +213,66 @@ class Geometry:
         out = np.zeros(8 * self.nobj)
         lib().or_pft_emt8(self.h, omega.real, omega.imag, Jd, E, nh, out)
         return out.reshape(self.nobj, 8)
+
+    def assemble_g(self, omega):
+        """G block of the whole geometry (AssembleGBlock for every object pair)."""
+        flat = np.zeros(2 * self.N * self.N)
+        lib().or_assemble_g(self.h, omega.real, omega.imag, flat)
+        return flat.view(np.complex128).reshape(self.N, self.N, order="F")
+
+    def neq_overlaps(self, a, omega):
+        idx = np.zeros(7, dtype=np.int32)
+        V, R = np.zeros(14), np.zeros(7)
+        n = lib().or_neq_overlaps(self.h, a, float(np.real(omega)), idx.ctypes.data_as(C.c_void_p), V, R)
+        return idx[:n], V[: 2 * n].view(np.complex128), R[:n]
+
+    def neq_blocks(self, omega):
+        """Dense S (Gram, GetOverlapElements), V (all objects) and the Rytov
+        block of each object (AssembleOverlapBlocks with SetEntry per row)."""
+        N = self.N
+        S = np.zeros((N, N))
+        V = np.zeros((N, N), complex)
+        R = [np.zeros((N, N)) for _ in range(self.nobj)]
+        for no in range(self.nobj):
+            for a in range(self.off[no], self.off[no + 1]):
+                idx, vals = self.overlap_closed_form(a)
+                S[a, idx] = vals
+                idx, v, r = self.neq_overlaps(a, omega)
+                V[a, idx] = v
+                R[no][a, idx] = r
+        return S, V, R
+
+    def dressed_rytov(self, omega, src, blocks=None, Gm=None):
+        """ComputeDressedRytovMatrix (GetFlux.cc:155-272), its steps in order:
+        W = (1 + S^-1 V S^-1 G)^-1 by LU, then W \\ (W \\ S^-1 R_src S^-1)^H."""
+        import scipy.linalg as sl
+        S, V, R = blocks if blocks is not None else self.neq_blocks(omega)
+        Gm = self.assemble_g(omega) if Gm is None else Gm
+        Sinv = np.linalg.inv(S)                     # SInverse->LUFactorize(); LUInvert()
+        M2 = Sinv @ Gm                              # (b)
+        M1 = V @ M2                                 # (d)
+        M3 = Sinv @ M1                              # (e)
+        M3 += np.eye(self.N)                        # (f)
+        lu = sl.lu_factor(M3)                       # (g)
+        M1 = np.asarray(R[src], complex)            # (h)
+        M2 = Sinv @ M1                              # (i)
+        M1 = M2 @ Sinv                              # (j)
+        M2 = sl.lu_solve(lu, M1)                    # (k)
+        M1 = M2.conj().T                            # (l)
+        return sl.lu_solve(lu, M1)                  # (m)
+
+    def pft_emt8_dr(self, omega, DR):
+        D = np.asfortranarray(DR, dtype=np.complex128)
+        out = np.zeros(8 * self.nobj)
+        lib().or_pft_emt8_dr(self.h, omega.real, omega.imag, D.reshape(-1, order="F").view(np.float64), out)
+        return out.reshape(self.nobj, 8)
+
+    def neq_flux(self, omega):
+        """GetFlux (GetFlux.cc:291-436) for one geometry and no transforms:
+        flux[src, dst, q], q = PAbs, PScat, Fx, Fy, Fz, Tx, Ty, Tz (EMT)."""
+        blocks, Gm = self.neq_blocks(omega), self.assemble_g(omega)
+        return np.stack([self.pft_emt8_dr(omega, self.dressed_rytov(omega, s, blocks, Gm))
+                         for s in range(self.nobj)])
 
     def get_fields(self, omega, J, X, E0=None, nhat=None):
         """(P, 6) complex: E and H at the points X (P x 3); J and/or the plane wave may be None."""

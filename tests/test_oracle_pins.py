@@ -286,3 +286,73 @@ def test_oracle_scattered_flux_matches_emt(oracle_lib, sphere):
         ftot = _sphere_flux(G, w, J, 3.0, E0, nh)
         assert abs(-ftot / G.pft_opft(w, J)[0] - 1) < 2e-3
     assert rel[1] < 0.6 * rel[0] and rel[1] < 0.02, rel
+
+
+def test_oracle_emt_pscat_is_flux_plus_half_self_terms(oracle_lib, sphere):
+    """The EMT scattered power (EMTPFT.cc:396-436) sums the pairs a <= b
+    once each, so it counts every self pair (a, a) with weight 1 where the
+    radiated power -- the Poynting flux of the GetFields fields -- needs 1/2.
+    PScat_EMT - (self-pair terms)/2 equals the flux to the quadrature error,
+    for solved currents and for random ones; this ties the two restatements
+    (fields and EMT) together term by term."""
+    w = 1.0 + 0j
+    E0, nh = np.array([1, 0, 0], complex), np.array([0, 0, 1.0])
+    G = oracle_lib.Geometry(sphere(3), oracle_lib.material(eps=4 + 0.2j), nang=6)
+    J = sl.lu_solve(sl.lu_factor(G.assemble(w)), G.rhs_planewave(w, E0, nh))
+    rng = np.random.default_rng(1)
+    for c in (J, rng.normal(size=G.N) + 1j * rng.normal(size=G.N)):
+        full = G.pft_emt8_dr(w, np.outer(c, c.conj()))[0, 1]
+        selfp = G.pft_emt8_dr(w, np.diag(np.abs(c) ** 2).astype(complex))[0, 1]
+        flux = _sphere_flux(G, w, c, 3.0)
+        assert abs((full - selfp / 2) / flux - 1) < 3e-4, (full, selfp, flux)
+
+
+def _krueger_prad(eps, u, R=1.0):
+    """Radiated-power flux of a small sphere from its dipole T-matrix
+    elements (Krueger, Bimonte, Emig, Kardar, Phys. Rev. B 86, 115423 (2012),
+    eq. 131 with the small-kR expansion of the l = 1 elements)."""
+    kR = u * R
+
+    def tl(e, m):
+        f1 = 2 * (e - 1) / (3 * (e + 2))
+        f2 = (2 - 3 * e + e * e * (1 + m)) / (5 * (2 + e) ** 2)
+        f3 = -4 * (e - 1) ** 2 / (9 * (2 + e) ** 2)
+        return 1j * f1 * kR ** 3 + 2j * f2 * kR ** 5 + f3 * kR ** 6
+    t = [tl(1.0, eps), tl(eps, 1.0)]
+    return -6.0 * sum(x.real + abs(x) ** 2 for x in t) / np.pi
+
+
+def test_oracle_neq_chain(oracle_lib, sphere):
+    """buff-neq's dressed Rytov chain (GetFlux.cc:155-272) restated step by
+    step: DR is Hermitian; for a homogeneous body it equals the closed form
+    4 Im(eps) / (pi Z0 w^3 |eps - 1|^2) M^-1 S M^-H through the VIE matrix M
+    (pinned against Mie); EMT with DR = J J^H is the scattering part of EMT
+    with J; the flux has PAbs = -PRad for one body; and the radiated power
+    with the self pairs weighted 1/2 approaches Krueger's dipole formula for
+    small spheres as the mesh is refined, at two materials and frequencies."""
+    Z0 = 376.73031346177
+    eps, w = 4 + 0.2j, 0.6 + 0j
+    G = oracle_lib.Geometry(sphere(3), oracle_lib.material(eps=eps), nang=6)
+    S, V, R = G.neq_blocks(w)
+    DR = G.dressed_rytov(w, 0, (S, V, R))
+    assert np.abs(DR - DR.conj().T).max() <= 1e-12 * np.abs(DR).max()
+    M = G.assemble(w)
+    Mi = np.linalg.inv(M)
+    ref = 4 * eps.imag / (np.pi * Z0 * w.real ** 3 * abs(eps - 1) ** 2) * (Mi @ S @ Mi.conj().T)
+    assert np.abs(DR - ref).max() <= 1e-10 * np.abs(ref).max()
+    E0, nh = np.array([1, 0, 0], complex), np.array([0, 0, 1.0])
+    J = sl.lu_solve(sl.lu_factor(M), G.rhs_planewave(w, E0, nh))
+    pj = G.pft_emt8(w, J, np.zeros(3, complex), nh)[0]
+    pd = G.pft_emt8_dr(w, np.outer(J, J.conj()))[0]
+    np.testing.assert_allclose(pd, pj, rtol=1e-12, atol=1e-15 * np.abs(pj).max())
+    F = G.neq_flux(w)
+    assert F.shape == (1, 1, 8) and abs(F[0, 0, 0] + F[0, 0, 1]) <= 1e-14 * abs(F[0, 0, 1])
+    for eps, u in ((4 + 0.2j, 0.3), (9 + 3j, 0.2)):
+        r = []
+        for n in (3, 4):
+            G = oracle_lib.Geometry(sphere(n), oracle_lib.material(eps=eps), nang=6)
+            DR = G.dressed_rytov(u + 0j, 0)
+            full = G.pft_emt8_dr(u + 0j, DR)[0, 1]
+            selfp = G.pft_emt8_dr(u + 0j, np.diag(np.diag(DR)))[0, 1]
+            r.append((full - selfp / 2) / _krueger_prad(eps, u))
+        assert 0.6 < r[0] < r[1] < 1.05, (eps, u, r)
