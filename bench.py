@@ -20,11 +20,17 @@ anisotropic tensor [[4,.5,0],[.5,6,0],[0,0,9]] + 0.1i ("secondary").  The
 frequency-independent near-field precompute runs once per mesh before timing
 ("precompute_s"), as the reference amortises its FIBBI cache.
 
+Beside the headline (--no-extras skips them): "get_fields" times
+GetFields for 4096 far and 4096 near points on the N = 57,222 sphere, and
+"neq_flux" the buff-neq flux chain (dressed Rytov matrix, EMT flux columns)
+per frequency for the N = 19,872 sphere.
+
 value: device time of K steps (CUDA events on the library stream, barrier +
 synchronize on both sides, max over ranks) / steps.  The matrices are far
 larger than the 126 MB L2, so no flush is needed.
 e2e: the learned step through the host-buffer C-ABI calls (RHS assembled to
-host memory, solution copied back), host wall time including the copies.
+host memory, solution copied back), host wall time including the copies,
+mean over K steps (max over ranks).
 
 --impl reference times the CPU restatement of the reference path (oracle
 port: OpenMP assembly over all host cores, LAPACK zgetrf/zgetrs via OpenBLAS)
@@ -360,6 +366,100 @@ def run_batching(nomega=64):
             "pabs_finite": bool(np.all(np.isfinite(pabs)))}
 
 
+FIELD_FLOPS_PER_POINT = 156   # FP64 adds/multiplies of one quadrature point (FMA = 2), no sincos/rsqrt
+
+
+def run_fields(stream, n=17, npts=4096, steps=3):
+    """GetFields on the headline sphere (N = 57,222): npts far points (4-point
+    rule for every basis function) and npts near points (both rules), for
+    seeded random currents already on the device."""
+    import ctypes as C
+    import torch
+    import buffem
+    G = buffem.SWGGeometry(meshfiles=mesh_path(n), materials=buffem.Material(eps=EPS_LEARNED))
+    N, NT = G.TotalBFs, 6 * n ** 3
+    rng = np.random.default_rng(11)
+    J = torch.tensor(rng.normal(size=N) + 1j * rng.normal(size=N), dtype=torch.complex128, device="cuda")
+    L = buffem.lib()
+    out = {"N": N, "tets": NT, "points": npts}
+    for label, rmin, rmax in (("far", 5.0, 50.0), ("near", 1.02, 2.0)):
+        d = rng.normal(size=(npts, 3))
+        d /= np.linalg.norm(d, axis=1)[:, None]
+        X = torch.tensor(d * rng.uniform(rmin, rmax, size=(npts, 1)), dtype=torch.float64, device="cuda")
+        F = torch.zeros((npts, 6), dtype=torch.complex128, device="cuda")
+        fn = lambda: buffem._check(L.bg_get_fields_device(G.h, OMEGA, 0.0, C.c_void_p(J.data_ptr()), None, None,
+                                                          npts, C.c_void_p(X.data_ptr()), C.c_void_p(F.data_ptr())))
+        t = timed(stream, fn, steps, 2, 1) / steps
+        out[label] = {"ms": t * 1e3, "radius": [rmin, rmax], "tet_point_pairs_per_s": npts * NT / t}
+        if label == "far":
+            evals = 4.0 * npts * NT
+            out[label]["quadrature_points_per_s"] = evals / t
+            out[label]["fp64_tflops"] = evals * FIELD_FLOPS_PER_POINT / t / 1e12
+    del G
+    return out
+
+
+def small_case(kind, n):
+    """Profiler-sized runs of the GetFields and buff-neq kernels (wall time)."""
+    import ctypes as C
+    import torch
+    import buffem
+    G = buffem.SWGGeometry(meshfiles=mesh_path(n), materials=buffem.Material(eps=EPS_LEARNED))
+    N = G.TotalBFs
+    t0 = time.perf_counter()
+    if kind == "fields":
+        rng = np.random.default_rng(1)
+        J = torch.tensor(rng.normal(size=N) + 1j * rng.normal(size=N), dtype=torch.complex128, device="cuda")
+        P = 2048
+        d = rng.normal(size=(P, 3))
+        d /= np.linalg.norm(d, axis=1)[:, None]
+        X = torch.tensor(d * rng.uniform(5, 50, size=(P, 1)), dtype=torch.float64, device="cuda")
+        F = torch.zeros((P, 6), dtype=torch.complex128, device="cuda")
+        for _ in range(2):
+            buffem._check(buffem.lib().bg_get_fields_device(G.h, OMEGA, 0.0, C.c_void_p(J.data_ptr()), None, None,
+                                                            P, C.c_void_p(X.data_ptr()), C.c_void_p(F.data_ptr())))
+        res = {"points": P, "checksum": float(F.abs().sum())}
+    else:
+        G.precompute()
+        neq = buffem.NEQ(G)
+        neq.GetFlux(0.3)
+        F = neq.GetFlux(0.31)
+        res = {"prad": float(F[0, 0, 1])}
+    res.update({"kind": kind, "N": N, "wall_s": time.perf_counter() - t0})
+    return res
+
+
+def neq_flops(N):
+    """FP64 flops of one frequency of the flux chain for one object: S^-1 G,
+    S^-1 (V S^-1 G), LU of W, S^-1 R S^-1 (dense block), two N-column solves."""
+    return (8 + 8 + 8.0 / 3 + 8 + 8 + 8) * float(N) ** 3
+
+
+def run_neq(stream, n=12, steps=2):
+    """buff-neq flux chain for one sphere (N = 19,872 at n = 12): set-up (S^-1)
+    once, then GetFlux at distinct frequencies (each refactors W)."""
+    import buffem
+    G = buffem.SWGGeometry(meshfiles=mesh_path(n), materials=buffem.Material(eps=EPS_LEARNED))
+    N = G.TotalBFs
+    G.precompute()
+    buffem.synchronize()
+    t0 = time.perf_counter()
+    neq = buffem.NEQ(G)
+    t_setup = time.perf_counter() - t0
+    k = [0]
+
+    def fn():
+        k[0] += 1
+        neq.GetFlux(0.3 + 0.01 * k[0])
+    t = timed(stream, fn, steps, 1, 1) / steps
+    F = neq.GetFlux(0.3)
+    del neq
+    return {"N": N, "setup_s": t_setup, "s_per_frequency": t, "flops_per_frequency": neq_flops(N),
+            "fp64_tflops": neq_flops(N) / t / 1e12, "prad_at_0.3": float(F[0, 0, 1]),
+            "pabs_plus_prad": float(F[0, 0, 0] + F[0, 0, 1]),
+            "note": "one object, EMT flux columns; W factored once per frequency"}
+
+
 def run_gpu(args, rank, world, local_rank):
     import torch
     import buffem
@@ -441,12 +541,12 @@ def run_gpu(args, rank, world, local_rank):
     hostB = np.zeros((N, case.nrhs), complex, order="F")
     rhs_h = np.zeros(N, complex)
     times = []
-    for _ in range(0 if args.lean else max(1, min(args.steps, 2))):
+    for _ in range(0 if args.lean else max(1, args.steps)):
         buffem.synchronize()
         t0 = time.perf_counter()
         case.step_learned_host(hostB, rhs_h, net, stats)
         times.append(time.perf_counter() - t0)
-    e2e_s = max(times) if times else None
+    e2e_s = sum(times) / len(times) if times else None     # mean over the K steps, as value
     if world > 1 and e2e_s is not None:
         import torch.distributed as dist
         t = torch.tensor([e2e_s], device="cuda")
@@ -540,16 +640,22 @@ def main():
     ap.add_argument("--order", type=int, default=10, help="singular-rule order")
     ap.add_argument("--no-batch", action="store_true", help="skip the batching-form sweep (8 geometries x 64 omega)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the GetFields and buff-neq flux measurements")
     ap.add_argument("--lean", action="store_true",
                     help="headline learned steps only (no FP64 arm, e2e, secondary, CPU baseline): profiler runs")
-    ap.add_argument("--kernel", default=None, choices=["gemm"],
-                    help="time the LU trailing-update GEMM alone on an M=N=K problem")
+    ap.add_argument("--kernel", default=None, choices=["gemm", "fields", "neq"],
+                    help="one small case for profilers: gemm = the LU trailing-update GEMM on an M=N=K=--size "
+                         "problem; fields = two GetFields calls, 2048 far points on the --size-cell sphere; "
+                         "neq = two buff-neq flux frequencies on the --size-cell sphere")
     ap.add_argument("--size", type=int, default=8192)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "b200" else args.warmup
 
     if args.kernel == "gemm":
         print(json.dumps(gemm_kernel_bench(args.size)), flush=True)
+        return
+    if args.kernel in ("fields", "neq"):
+        print(json.dumps(small_case(args.kernel, args.size)), flush=True)
         return
     if args.lean:
         args.no_cpu_baseline = True
@@ -634,6 +740,23 @@ def main():
         line["secondary_n19872"] = res["secondary"]
     if not args.lean and not args.no_batch:
         line["batching_form"] = run_batching()
+    if not args.lean and not args.no_extras and world == 1:
+        import torch
+        import buffem
+        stream = torch.cuda.ExternalStream(buffem.lib().bg_stream())
+        zpk = zgemm_peak_tflops()
+        gf = run_fields(stream)
+        gf["roofline"] = {"bound": "fp64", "kernel": "k_fields", "achieved": gf["far"]["fp64_tflops"], "peak": zpk,
+                          "unit": "TFLOP/s", "frac": gf["far"]["fp64_tflops"] / zpk,
+                          "peak_source": "cuBLAS ZGEMM 8192^3 measured here (FP64 tensor rate; the FP64 "
+                                         "CUDA-core peak is the same nominal 40 TFLOP/s on B200)",
+                          "algorithmic": f"{FIELD_FLOPS_PER_POINT} flops per quadrature point, 4 points per "
+                                         "(point, tetrahedron) pair in the far case; sincos and rsqrt not counted"}
+        line["get_fields"] = gf
+        nq = run_neq(stream)
+        nq["roofline"] = {"bound": "tensor", "achieved": nq["fp64_tflops"], "peak": zpk, "unit": "TFLOP/s",
+                          "frac": nq["fp64_tflops"] / zpk, "peak_source": "cuBLAS ZGEMM 8192^3 measured here"}
+        line["neq_flux"] = nq
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = cpu_sample(args.n, args.order)
         line["cpu_baseline"] = {"value": r["value"], "unit": "s", "cores": r["cores"], "kind": "port",

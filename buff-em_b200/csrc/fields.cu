@@ -31,7 +31,9 @@
 //   fieldFace 16 doubles: per local face k, (centroid, radius), radius 0 if the
 //             face carries no basis function
 //   coef       8 doubles per call: g_k (4 complex) from J
-// Work split: a block owns 128 x tpt tetrahedra and a chunk of points; each
+// Work split: a block owns 128 x tpt tetrahedra (tpt = 1 with the
+// tetrahedron's data held in registers across the points while the partials
+// stay small; else tpt grows to ~8 blocks per SM) and 32 points; each
 // warp reduces its lanes per point into shared memory and the block writes one
 // partial per (tetrahedron block, point), summed in a fixed order by the
 // finishing kernel (deterministic).
@@ -171,7 +173,88 @@ __global__ void k_fields_coef(DevGeom g, const z *J, z *coef) {
   }
 }
 
+// one tetrahedron's data for the field sums: vertices, the all-faces-far
+// sphere, and the linear current alpha y - beta of all its basis functions
+struct TetData {
+  double V[4][3], ctr[3], Rall;
+  z al, be[3];
+};
+
+__device__ __forceinline__ void load_tet(const double *__restrict__ tetT, const z *__restrict__ coef, int t,
+                                         TetData &T) {
+  const double2 *T2 = reinterpret_cast<const double2 *>(tetT + 16 * (size_t)t);
+  double2 a0 = T2[0], a1 = T2[1], a2 = T2[2], a3 = T2[3], a4 = T2[4], a5 = T2[5], a6 = T2[6], a7 = T2[7];
+  T.V[0][0] = a0.x; T.V[0][1] = a0.y; T.V[0][2] = a1.x; T.V[1][0] = a1.y; T.V[1][1] = a2.x; T.V[1][2] = a2.y;
+  T.V[2][0] = a3.x; T.V[2][1] = a3.y; T.V[2][2] = a4.x; T.V[3][0] = a4.y; T.V[3][1] = a5.x; T.V[3][2] = a5.y;
+  T.ctr[0] = a6.x; T.ctr[1] = a6.y; T.ctr[2] = a7.x; T.Rall = a7.y;
+  T.al = z{0.0, 0.0};
+#pragma unroll
+  for (int c = 0; c < 3; c++) T.be[c] = z{0.0, 0.0};
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    z gk = coef[4 * (size_t)t + k];
+    T.al.r += gk.r; T.al.i += gk.i;
+#pragma unroll
+    for (int c = 0; c < 3; c++) { T.be[c].r += gk.r * T.V[k][c]; T.be[c].i += gk.i * T.V[k][c]; }
+  }
+}
+
+// fields at x of tetrahedron t (data T): the 4-point rule for all of it when
+// every face is far, else split by face with the reference's rule choice
 template <bool REALK>
+__device__ __forceinline__ void tet_point(const FieldK &K, const double *x, const TetData &T,
+                                          const double *__restrict__ tetF, const z *__restrict__ coef, int t,
+                                          double *acc) {
+  double d2 = (x[0] - T.ctr[0]) * (x[0] - T.ctr[0]) + (x[1] - T.ctr[1]) * (x[1] - T.ctr[1]) +
+              (x[2] - T.ctr[2]) * (x[2] - T.ctr[2]);
+  if (d2 > T.Rall * T.Rall) {
+    rule4<REALK>(K, x, T.V, T.al, T.be, acc);
+    return;
+  }
+  // per face: the reference's rule choice |X - centroid| / radius > 10
+  z a4{0.0, 0.0}, b4[3] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+  z a16{0.0, 0.0}, b16[3] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+  bool any4 = false, any16 = false;
+  const double4 *F4 = reinterpret_cast<const double4 *>(tetF + 16 * (size_t)t);
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    double4 f = F4[k];
+    z gk = coef[4 * (size_t)t + k];
+    double dx = x[0] - f.x, dy = x[1] - f.y, dz = x[2] - f.z;
+    bool live = f.w != 0.0;
+    bool far = live && sqrt(dx * dx + dy * dy + dz * dz) / f.w > 10.0;
+    bool near = live && !far;
+    double m4 = far ? 1.0 : 0.0, m16 = near ? 1.0 : 0.0;
+    a4.r += m4 * gk.r; a4.i += m4 * gk.i;
+    a16.r += m16 * gk.r; a16.i += m16 * gk.i;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      b4[c].r += m4 * gk.r * T.V[k][c]; b4[c].i += m4 * gk.i * T.V[k][c];
+      b16[c].r += m16 * gk.r * T.V[k][c]; b16[c].i += m16 * gk.i * T.V[k][c];
+    }
+    any4 |= far;
+    any16 |= near;
+  }
+  if (any4) rule4<REALK>(K, x, T.V, a4, b4, acc);
+  if (any16) rule16<REALK>(K, x, T.V, a16, b16, acc);
+}
+
+// warp sum of the 12 accumulators of point p into the warp's shared slot
+__device__ __forceinline__ void warp_flush(double *acc, double (*slot)[12], int p, int lane) {
+#pragma unroll
+  for (int q = 0; q < 12; q++) {
+    double v = acc[q];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    acc[q] = v;
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int q = 0; q < 12; q++) slot[p][q] = acc[q];
+  }
+}
+
+template <bool REALK, bool ONE>
 __global__ void __launch_bounds__(FTHREADS, 3)
 k_fields(const double *__restrict__ tetT, const double *__restrict__ tetF, const z *__restrict__ coef, int NT,
          int tpt, const double *__restrict__ X, int P, FieldK K, double *__restrict__ part) {
@@ -182,74 +265,33 @@ k_fields(const double *__restrict__ tetT, const double *__restrict__ tetF, const
   __syncthreads();
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int tbase = blockIdx.y * FTHREADS * tpt + threadIdx.x;
-  for (int p = 0; p < np; p++) {
-    double x[3] = {sx[p][0], sx[p][1], sx[p][2]};
-    double acc[12];
+  if (ONE) {
+    // one tetrahedron per thread: its data stays in registers for all points
+    bool live = tbase < NT;
+    TetData T;
+    if (live) load_tet(tetT, coef, tbase, T);
+    for (int p = 0; p < np; p++) {
+      double x[3] = {sx[p][0], sx[p][1], sx[p][2]};
+      double acc[12];
 #pragma unroll
-    for (int q = 0; q < 12; q++) acc[q] = 0.0;
-    for (int j = 0; j < tpt; j++) {
-      int t = tbase + j * FTHREADS;
-      if (t >= NT) break;
-      const double2 *T2 = reinterpret_cast<const double2 *>(tetT + 16 * (size_t)t);
-      double V[4][3], ctr[3], Rall;
-      {
-        double2 a0 = T2[0], a1 = T2[1], a2 = T2[2], a3 = T2[3], a4 = T2[4], a5 = T2[5], a6 = T2[6], a7 = T2[7];
-        V[0][0] = a0.x; V[0][1] = a0.y; V[0][2] = a1.x; V[1][0] = a1.y; V[1][1] = a2.x; V[1][2] = a2.y;
-        V[2][0] = a3.x; V[2][1] = a3.y; V[2][2] = a4.x; V[3][0] = a4.y; V[3][1] = a5.x; V[3][2] = a5.y;
-        ctr[0] = a6.x; ctr[1] = a6.y; ctr[2] = a7.x; Rall = a7.y;
-      }
-      z gk[4];
-#pragma unroll
-      for (int k = 0; k < 4; k++) gk[k] = coef[4 * (size_t)t + k];
-      double d2 = (x[0] - ctr[0]) * (x[0] - ctr[0]) + (x[1] - ctr[1]) * (x[1] - ctr[1]) +
-                  (x[2] - ctr[2]) * (x[2] - ctr[2]);
-      if (d2 > Rall * Rall) {
-        z al{0.0, 0.0}, be[3] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-          al.r += gk[k].r; al.i += gk[k].i;
-#pragma unroll
-          for (int c = 0; c < 3; c++) { be[c].r += gk[k].r * V[k][c]; be[c].i += gk[k].i * V[k][c]; }
-        }
-        rule4<REALK>(K, x, V, al, be, acc);
-      } else {
-        // per face: the reference's rule choice |X - centroid| / radius > 10
-        z a4{0.0, 0.0}, b4[3] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
-        z a16{0.0, 0.0}, b16[3] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
-        bool any4 = false, any16 = false;
-        const double4 *F4 = reinterpret_cast<const double4 *>(tetF + 16 * (size_t)t);
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-          double4 f = F4[k];
-          double dx = x[0] - f.x, dy = x[1] - f.y, dz = x[2] - f.z;
-          bool live = f.w != 0.0;
-          bool far = live && sqrt(dx * dx + dy * dy + dz * dz) / f.w > 10.0;
-          bool near = live && !far;
-          double m4 = far ? 1.0 : 0.0, m16 = near ? 1.0 : 0.0;
-          a4.r += m4 * gk[k].r; a4.i += m4 * gk[k].i;
-          a16.r += m16 * gk[k].r; a16.i += m16 * gk[k].i;
-#pragma unroll
-          for (int c = 0; c < 3; c++) {
-            b4[c].r += m4 * gk[k].r * V[k][c]; b4[c].i += m4 * gk[k].i * V[k][c];
-            b16[c].r += m16 * gk[k].r * V[k][c]; b16[c].i += m16 * gk[k].i * V[k][c];
-          }
-          any4 |= far;
-          any16 |= near;
-        }
-        if (any4) rule4<REALK>(K, x, V, a4, b4, acc);
-        if (any16) rule16<REALK>(K, x, V, a16, b16, acc);
-      }
+      for (int q = 0; q < 12; q++) acc[q] = 0.0;
+      if (live) tet_point<REALK>(K, x, T, tetF, coef, tbase, acc);
+      warp_flush(acc, sacc[warp], p, lane);
     }
+  } else {
+    for (int p = 0; p < np; p++) {
+      double x[3] = {sx[p][0], sx[p][1], sx[p][2]};
+      double acc[12];
 #pragma unroll
-    for (int q = 0; q < 12; q++) {
-      double v = acc[q];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-      acc[q] = v;
-    }
-    if (lane == 0) {
-#pragma unroll
-      for (int q = 0; q < 12; q++) sacc[warp][p][q] = acc[q];
+      for (int q = 0; q < 12; q++) acc[q] = 0.0;
+      for (int j = 0; j < tpt; j++) {
+        int t = tbase + j * FTHREADS;
+        if (t >= NT) break;
+        TetData T;
+        load_tet(tetT, coef, t, T);
+        tet_point<REALK>(K, x, T, tetF, coef, t, acc);
+      }
+      warp_flush(acc, sacc[warp], p, lane);
     }
   }
   __syncthreads();
@@ -360,8 +402,12 @@ int get_fields(bg_geometry *g, double wr, double wi, const void *dJ, const doubl
   int NT = g->NT;
   int ny = (npts + FPCH - 1) / FPCH, tpt = 1;
   int nbx = dJ ? (NT + FTHREADS - 1) / FTHREADS : 0;
-  // fewer, longer tetrahedron blocks once the point chunks fill the GPU
-  while (nbx > 65535 || (nbx > 1 && (long)nbx * ny > 8L * 148)) {
+  // one tetrahedron per thread (data in registers) while the partial sums
+  // (96 bytes per tetrahedron block and point) stay under 256 MiB; beyond
+  // that, longer tetrahedron blocks until the grid is about 8 blocks per SM,
+  // which amortises the per-point warp reductions over many tetrahedra
+  bool one = 96.0 * nbx * npts <= 268435456.0 && nbx <= 65535;
+  while (!one && (nbx > 65535 || (nbx > 1 && (long)nbx * ny > 8L * 148))) {
     tpt *= 2;
     nbx = (NT + FTHREADS * tpt - 1) / (FTHREADS * tpt);
   }
@@ -373,10 +419,9 @@ int get_fields(bg_geometry *g, double wr, double wi, const void *dJ, const doubl
     k_fields_coef<<<(NT + 255) / 256, 256, 0, stream()>>>(g->dev, (const z *)dJ, coef);
     BG_LAUNCHED();
     dim3 grid(ny, nbx);
-    if (wi == 0.0)
-      k_fields<true><<<grid, FTHREADS, 0, stream()>>>(g->d_fieldTet, g->d_fieldFace, coef, NT, tpt, dX, npts, K, part);
-    else
-      k_fields<false><<<grid, FTHREADS, 0, stream()>>>(g->d_fieldTet, g->d_fieldFace, coef, NT, tpt, dX, npts, K, part);
+    auto kern = wi == 0.0 ? (one ? k_fields<true, true> : k_fields<true, false>)
+                          : (one ? k_fields<false, true> : k_fields<false, false>);
+    kern<<<grid, FTHREADS, 0, stream()>>>(g->d_fieldTet, g->d_fieldFace, coef, NT, tpt, dX, npts, K, part);
     BG_LAUNCHED();
   }
   k_fields_finish<<<(npts + 127) / 128, 128, 0, stream()>>>(part, nbx, npts, dX, K, epre, inc, (z *)dOut);
