@@ -60,9 +60,9 @@ EPS_LEARNED = 6 + 0.5j
 WAVES = [([1, 0, 0], [0, 0, 1]), ([0, 1, 0], [0, 0, 1]), ([0, 0, 1], [1, 0, 0])]
 OMEGA = 1.0
 GMRES = dict(tol=1e-10, restart=50, maxit=1000, inner_tol=1e-5)
-# ncu --set full capture of k_gm_matvec_part_c64 (one launch, N = 19,872):
+# ncu --set full capture of k_gm_matvec_sym_c64 (one launch, N = 19,872):
 # dram__bytes_read.sum + dram__bytes_write.sum
-MATVEC_NCU_N, MATVEC_NCU_BYTES = 19872, 3.160269e9 + 21.617664e6
+MATVEC_NCU_N, MATVEC_NCU_BYTES = 19872, 1.600864e9 + 20.701184e6
 
 
 def eps_tensor():
@@ -712,7 +712,7 @@ def main():
             "data": "synthetic", "config": config,
             "learned_form": res["learned"],
             "kernel_classes": prof, "precompute_s": res["precompute_s"],
-            "roofline": {"bound": "hbm", "kernel": "k_gm_matvec_part_c64 (+ k_gm_matvec_sum): GMRES matrix-vector "
+            "roofline": {"bound": "hbm", "kernel": "k_gm_matvec_sym_c64 (+ k_gm_matvec_sum): GMRES matrix-vector "
                                                    "products on the complex64 matrix",
                          "achieved": mv_gbs, "peak": hbm, "unit": "GB/s",
                          "frac": (mv_gbs / hbm) if (mv_gbs and hbm) else None,
@@ -720,7 +720,8 @@ def main():
                          "traffic_source": f"ncu dram read+write of one launch at N={MATVEC_NCU_N} "
                                            f"({MATVEC_NCU_BYTES:.4g} B), scaled by N^2",
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if hbm else "unavailable",
-                         "algorithmic": "8 N^2 bytes of matrix per product (3 right-hand sides share one pass; "
+                         "algorithmic": "4 N^2 + 1024 N bytes per product: the upper-triangle 256x256 tiles of the "
+                                        "symmetric complex64 matrix, read once for all 3 right-hand sides ("
                                         "16 N^2 for the complex128 residual products)",
                          "share_of_profiled_ms": mv["ms"] / total_ms if total_ms else None,
                          "assemble_far_share_of_profiled_ms": far["ms"] / total_ms if total_ms else None},

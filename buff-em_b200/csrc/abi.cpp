@@ -268,6 +268,7 @@ int bg_assemble(bg_geometry *g, double wr, double wi, bg_matrix *m) {
   if (!st) st = assemble_near(g, wr, wi, m->d, m->ld);
   if (!st) st = assemble_gram(g, wr, wi, m->d, m->ld);
   prof_stop(PROF_ASM_NEAR, 0.0);
+  m->symmetric = !st;   // far, near and Gram entries are written symmetrically
   return st;
 }
 
@@ -285,6 +286,7 @@ int bg_matrix_upload(bg_matrix *m, const void *host) {
   BG_CUDA_TRY(cudaStreamSynchronize(stream()));
   BG_CUDA_TRY(cudaMemcpy2D(m->d, esz * m->ld, host, esz * m->N, esz * m->N, m->N, cudaMemcpyHostToDevice));
   m->factored = false;
+  m->symmetric = false;
   return BG_OK;
 }
 
@@ -328,11 +330,13 @@ int bg_matrix_device_ptr(bg_matrix *m, void **dptr, int *ld) {
   if (!m || !dptr || !ld) { set_error("bg_matrix_device_ptr: bad arguments"); return BG_ERR_ARG; }
   *dptr = m->d;
   *ld = (int)m->ld;
+  m->symmetric = false;   // the caller may write through the pointer
   return BG_OK;
 }
 
 int bg_lu_factor(bg_matrix *m) {
   if (!m) { set_error("bg_lu_factor: null matrix"); return BG_ERR_ARG; }
+  m->symmetric = false;
   int st = lu_factor(m);
   if (st < 0) return st;
   m->factored = true;

@@ -127,6 +127,138 @@ __global__ void __launch_bounds__(GV_ROWS) k_gm_matvec_part_c64(int N, const flo
   }
 }
 
+// Same product for a complex64 matrix known to be symmetric (M = M^T, as
+// every assembled VIE matrix is): only the 256 x 256 tiles (I, J) with I <= J
+// are read, half the bytes of the full product.  Tile (I, J) gives the
+// chunk-J partial of rows I (A_IJ x_J) and, for I < J, the chunk-I partial of
+// rows J (A_IJ^T x_I, which is A_JI x_I by symmetry), so every partial slot
+// of k_gm_matvec_sum is still written exactly once.  A warp owns 64 columns
+// of the tile and all 256 rows (8 per lane, two 8-byte complex entries per
+// 16-byte load, four columns per step); the transposed products of four
+// columns are reduce-scattered across the warp's lanes, the direct ones are
+// summed over the four warps through shared memory.  FP32
+// accumulation within a tile, FP64 partials, as in k_gm_matvec_part_c64.
+// Entries of rows >= N (the padding of the leading dimension) are zeroed on
+// load, never multiplied.
+template <int NR>
+__global__ void __launch_bounds__(128, 3) k_gm_matvec_sym_c64(int N, const float4 *A, size_t lda2, const z2 *X,
+                                                              size_t ldx, z2 *partial) {
+  const int I = blockIdx.x, J = blockIdx.y;
+  if (I > J) return;
+  const int r0 = I * 256, c0 = J * 256;
+  const int nr = min(256, N - r0), nc = min(256, N - c0);
+  __shared__ float2 xr[256][NR], xc[256][NR];
+  __shared__ float2 dacc[4][256][NR];
+  for (int e = threadIdx.x; e < 256 * NR; e += 128) {
+    int i = e / NR, j = e % NR;
+    z2 a = i < nr ? X[(size_t)j * ldx + r0 + i] : z2{0.0, 0.0};
+    z2 b = i < nc ? X[(size_t)j * ldx + c0 + i] : z2{0.0, 0.0};
+    xr[i][j] = make_float2((float)a.r, (float)a.i);
+    xc[i][j] = make_float2((float)b.r, (float)b.i);
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const bool trans = I < J;
+  float dr[8][NR], di[8][NR];
+#pragma unroll
+  for (int q = 0; q < 8; q++)
+#pragma unroll
+    for (int j = 0; j < NR; j++) dr[q][j] = di[q][j] = 0.f;
+  // this lane's rows: 64 k + 2 lane (+1), k = 0..3
+  bool ok0[4], ok1[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    int p = 64 * k + 2 * lane;
+    ok0[k] = p < nr;
+    ok1[k] = p + 1 < nr;
+  }
+  const float4 *base = A + (size_t)c0 * lda2 + (r0 >> 1) + lane;
+  const int cend = min(nc, 64 * w + 64);
+  // the lane that ends up holding a column's transposed sum: column 2 hi + b3
+  const int hi = (lane >> 4) & 1, b3 = (lane >> 3) & 1;
+  for (int c = 64 * w; c < cend; c += 4) {
+    // four columns at a time: 16 independent 16-byte loads per lane
+    float4 a[4][4];
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        bool ok = ok0[k] && c + u < cend;
+        a[u][k] = ok ? __ldcs(base + (size_t)(c + u) * lda2 + 32 * k) : make_float4(0.f, 0.f, 0.f, 0.f);
+        if (!ok1[k]) { a[u][k].z = 0.f; a[u][k].w = 0.f; }
+      }
+    float t[4][2 * NR];
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+#pragma unroll
+      for (int j = 0; j < NR; j++) {
+        float2 x = xc[c + u][j];          // zero past nc
+        float sr = 0.f, si = 0.f;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          float4 v = a[u][k];
+          dr[2 * k][j] += v.x * x.x - v.y * x.y;
+          di[2 * k][j] += v.x * x.y + v.y * x.x;
+          dr[2 * k + 1][j] += v.z * x.x - v.w * x.y;
+          di[2 * k + 1][j] += v.z * x.y + v.w * x.x;
+          float2 y0 = xr[64 * k + 2 * lane][j], y1 = xr[64 * k + 2 * lane + 1][j];
+          sr += v.x * y0.x - v.y * y0.y + v.z * y1.x - v.w * y1.y;
+          si += v.x * y0.y + v.y * y0.x + v.z * y1.y + v.w * y1.x;
+        }
+        t[u][2 * j] = sr;
+        t[u][2 * j + 1] = si;
+      }
+    if (trans) {
+      // reduce-scatter of the four columns over the warp: halves exchanged
+      // across lane bit 4, then bit 3, then full sums over bits 0-2
+      float k2[2][2 * NR];
+#pragma unroll
+      for (int m = 0; m < 2; m++)
+#pragma unroll
+        for (int e = 0; e < 2 * NR; e++) {
+          float keep = hi ? t[2 + m][e] : t[m][e];
+          float send = hi ? t[m][e] : t[2 + m][e];
+          k2[m][e] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+        }
+      float f[2 * NR];
+#pragma unroll
+      for (int e = 0; e < 2 * NR; e++) {
+        float keep = b3 ? k2[1][e] : k2[0][e];
+        float send = b3 ? k2[0][e] : k2[1][e];
+        f[e] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+      }
+#pragma unroll
+      for (int o = 4; o > 0; o >>= 1)
+#pragma unroll
+        for (int e = 0; e < 2 * NR; e++) f[e] += __shfl_xor_sync(0xffffffffu, f[e], o);
+      int cc = c + 2 * hi + b3;
+      if ((lane & 7) == 0 && cc < cend) {
+#pragma unroll
+        for (int j = 0; j < NR; j++) partial[((size_t)I * NR + j) * N + c0 + cc] = z2{f[2 * j], f[2 * j + 1]};
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 4; k++)
+#pragma unroll
+    for (int j = 0; j < NR; j++) {
+      dacc[w][64 * k + 2 * lane][j] = make_float2(dr[2 * k][j], di[2 * k][j]);
+      dacc[w][64 * k + 2 * lane + 1][j] = make_float2(dr[2 * k + 1][j], di[2 * k + 1][j]);
+    }
+  __syncthreads();
+  for (int e = threadIdx.x; e < nr * NR; e += 128) {
+    int i = e / NR, j = e % NR;
+    double sr = 0.0, si = 0.0;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      float2 v = dacc[q][i][j];
+      sr += v.x;
+      si += v.y;
+    }
+    partial[((size_t)J * NR + j) * N + r0 + i] = z2{sr, si};
+  }
+}
+
 __global__ void k_gm_matvec_sum(int N, int nchunk, int nrhs, const z2 *partial, z2 *Y, size_t ldy) {
   int row = blockIdx.x * blockDim.x + threadIdx.x;
   int j = blockIdx.y;
@@ -246,7 +378,17 @@ struct GmState {
 static int dense_matvec(bg_matrix *A, const z2 *X, z2 *Y, GmState &S) {
   int N = S.N;
   prof_start(PROF_MATVEC);
-  if (A->precision == BG_C64) {
+  if (A->precision == BG_C64 && A->symmetric) {
+    dim3 g1(S.nchunk, S.nchunk);
+    const float4 *a4 = (const float4 *)A->d;
+    size_t l2 = A->ld / 2;
+    switch (S.nrhs) {
+      case 1: k_gm_matvec_sym_c64<1><<<g1, 128, 0, stream()>>>(N, a4, l2, X, N, S.part); break;
+      case 2: k_gm_matvec_sym_c64<2><<<g1, 128, 0, stream()>>>(N, a4, l2, X, N, S.part); break;
+      case 3: k_gm_matvec_sym_c64<3><<<g1, 128, 0, stream()>>>(N, a4, l2, X, N, S.part); break;
+      default: k_gm_matvec_sym_c64<4><<<g1, 128, 0, stream()>>>(N, a4, l2, X, N, S.part); break;
+    }
+  } else if (A->precision == BG_C64) {
     dim3 g1((N + 2 * GV_ROWS - 1) / (2 * GV_ROWS), S.nchunk);
     k_gm_matvec_part_c64<<<g1, GV_ROWS, 0, stream()>>>(N, (const float4 *)A->d, A->ld / 2, X, N, S.nrhs, S.part);
   } else {
@@ -256,7 +398,11 @@ static int dense_matvec(bg_matrix *A, const z2 *X, z2 *Y, GmState &S) {
   BG_LAUNCHED();
   k_gm_matvec_sum<<<dim3((N + 255) / 256, S.nrhs), 256, 0, stream()>>>(N, S.nchunk, S.nrhs, S.part, Y, N);
   BG_LAUNCHED();
-  prof_stop(PROF_MATVEC, (A->precision == BG_C64 ? 8.0 : 16.0) * N * (double)N);
+  // algorithmic bytes of matrix read: the upper-triangle tiles for a
+  // symmetric complex64 matrix, the whole matrix otherwise
+  double nn = (double)N * N;
+  double bytes = A->precision == BG_C64 ? (A->symmetric ? 4.0 * nn + 4.0 * 256.0 * N : 8.0 * nn) : 16.0 * nn;
+  prof_stop(PROF_MATVEC, bytes);
   return BG_OK;
 }
 

@@ -161,6 +161,7 @@ struct bg_matrix {
   size_t work_bytes = 0;
   int *d_perm = nullptr;       // row permutation of the factors + solve flags/tickets
   int solve_epoch = 0;
+  bool symmetric = false;      // contents known to satisfy M = M^T (assembled, or converted from such)
 };
 
 namespace bg {

@@ -138,6 +138,7 @@ int matrix_convert(const bg_matrix *src, bg_matrix *dst) {
   k_c128_to_c64<<<grid, 256, 0, stream()>>>(src->N, (const c2 *)src->d, src->ld, (c1 *)dst->d, dst->ld);
   BG_LAUNCHED();
   dst->factored = false;
+  dst->symmetric = src->symmetric && !src->factored;
   return BG_OK;
 }
 
