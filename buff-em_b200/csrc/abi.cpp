@@ -54,7 +54,7 @@ int ensure_device() {
   // go back to the driver every call (larger transients are still returned)
   cudaMemPool_t pool;
   if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-    uint64_t keep = 1ull << 30;
+    uint64_t keep = 8ull << 30;
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
   }
   s_dev_ok = 1;
@@ -171,6 +171,7 @@ void bg_geometry_destroy(bg_geometry *g) {
   dfree(g->graph.rowptr); dfree(g->graph.col); dfree(g->graph.etr);
   dfree(g->d_scratch);
   dfree(g->d_fieldTet); dfree(g->d_fieldFace);
+  gnn_cache_free(g);
   delete g;
 }
 
@@ -376,7 +377,13 @@ int bg_precond_create_jacobi(bg_matrix *A, bg_precond **out) {
 
 void bg_precond_destroy(bg_precond *P) {
   if (!P) return;
-  dfree(P->rowptr); dfree(P->col); dfree(P->val);
+  // the arrays are stream-ordered allocations: freed after the work queued on
+  // the library stream, without a device-wide synchronisation
+  if (ensure_device() == BG_OK) {
+    if (P->rowptr) cudaFreeAsync(P->rowptr, stream());
+    if (P->col) cudaFreeAsync(P->col, stream());
+    if (P->val) cudaFreeAsync(P->val, stream());
+  }
   delete P;
 }
 

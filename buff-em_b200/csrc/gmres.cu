@@ -134,21 +134,44 @@ __global__ void __launch_bounds__(GV_ROWS) k_gm_matvec_part_c64(int N, const flo
 // rows J (A_IJ^T x_I, which is A_JI x_I by symmetry), so every partial slot
 // of k_gm_matvec_sum is still written exactly once.  A warp owns 64 columns
 // of the tile and all 256 rows (8 per lane, two 8-byte complex entries per
-// 16-byte load, four columns per step); the transposed products of four
-// columns are reduce-scattered across the warp's lanes, the direct ones are
-// summed over the four warps through shared memory.  FP32
+// 16-byte copy, four columns per step) and streams them through a 3-stage
+// cp.async pipeline in shared memory, so the copies of later steps are in
+// flight while a step is computed; the transposed products of four columns
+// are reduce-scattered across the warp's lanes, the direct ones summed over
+// the four warps through shared memory.  FP32
 // accumulation within a tile, FP64 partials, as in k_gm_matvec_part_c64.
-// Entries of rows >= N (the padding of the leading dimension) are zeroed on
-// load, never multiplied.
+// Entries of rows >= N (the padding of the leading dimension) are never read:
+// their copies are zero-filled.
+// 16-byte asynchronous global-to-shared copy; src_bytes < 16 zero-fills the rest
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int K>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(K) : "memory"); }
+
+#define SY_STAGES 3
+// shared memory: per warp SY_STAGES stages of 4 columns x 256 rows (as 4 x 128
+// float4), then x of the tile's rows and columns; the direct sums of the four
+// warps reuse the stage buffers after the loop
 template <int NR>
-__global__ void __launch_bounds__(128, 3) k_gm_matvec_sym_c64(int N, const float4 *A, size_t lda2, const z2 *X,
-                                                              size_t ldx, z2 *partial) {
+constexpr size_t sym_smem_bytes() {
+  return sizeof(float4) * 4 * SY_STAGES * 4 * 128 + sizeof(float2) * 2 * 256 * NR;
+}
+
+template <int NR>
+__global__ void __launch_bounds__(128) k_gm_matvec_sym_c64(int N, const float4 *A, size_t lda2, const z2 *X,
+                                                           size_t ldx, z2 *partial) {
   const int I = blockIdx.x, J = blockIdx.y;
   if (I > J) return;
   const int r0 = I * 256, c0 = J * 256;
   const int nr = min(256, N - r0), nc = min(256, N - c0);
-  __shared__ float2 xr[256][NR], xc[256][NR];
-  __shared__ float2 dacc[4][256][NR];
+  extern __shared__ __align__(16) unsigned char sym_smem[];
+  float4 *stage = reinterpret_cast<float4 *>(sym_smem);                        // [4 warps][STAGES][4][128]
+  float2 (*xr)[NR] = reinterpret_cast<float2 (*)[NR]>(stage + 4 * SY_STAGES * 4 * 128);
+  float2 (*xc)[NR] = xr + 256;
+  float2 (*dacc)[256][NR] = reinterpret_cast<float2 (*)[256][NR]>(sym_smem);  // [4][256][NR], after the loop
   for (int e = threadIdx.x; e < 256 * NR; e += 128) {
     int i = e / NR, j = e % NR;
     z2 a = i < nr ? X[(size_t)j * ldx + r0 + i] : z2{0.0, 0.0};
@@ -164,39 +187,57 @@ __global__ void __launch_bounds__(128, 3) k_gm_matvec_sym_c64(int N, const float
   for (int q = 0; q < 8; q++)
 #pragma unroll
     for (int j = 0; j < NR; j++) dr[q][j] = di[q][j] = 0.f;
-  // this lane's rows: 64 k + 2 lane (+1), k = 0..3
-  bool ok0[4], ok1[4];
+  // this lane's rows 64 k + 2 lane (+1): bytes of the pair that exist
+  int nb[4];
 #pragma unroll
   for (int k = 0; k < 4; k++) {
     int p = 64 * k + 2 * lane;
-    ok0[k] = p < nr;
-    ok1[k] = p + 1 < nr;
+    nb[k] = p + 1 < nr ? 16 : (p < nr ? 8 : 0);
   }
   const float4 *base = A + (size_t)c0 * lda2 + (r0 >> 1) + lane;
-  const int cend = min(nc, 64 * w + 64);
-  // the lane that ends up holding a column's transposed sum: column 2 hi + b3
-  const int hi = (lane >> 4) & 1, b3 = (lane >> 3) & 1;
-  for (int c = 64 * w; c < cend; c += 4) {
-    // four columns at a time: 16 independent 16-byte loads per lane
-    float4 a[4][4];
+  const int cbeg = 64 * w, cend = min(nc, 64 * w + 64);
+  const int nsteps = cend > cbeg ? (cend - cbeg + 3) / 4 : 0;
+  float4 *my = stage + (size_t)w * SY_STAGES * 4 * 128;
+  // each lane copies, and later reads, only its own rows: no warp barrier needed
+  auto issue = [&](int g) {
+    if (g < nsteps) {
+      float4 *buf = my + (g % SY_STAGES) * 4 * 128;
 #pragma unroll
-    for (int u = 0; u < 4; u++)
+      for (int u = 0; u < 4; u++) {
+        int c = cbeg + 4 * g + u;
+        bool okc = c < cend;
 #pragma unroll
-      for (int k = 0; k < 4; k++) {
-        bool ok = ok0[k] && c + u < cend;
-        a[u][k] = ok ? __ldcs(base + (size_t)(c + u) * lda2 + 32 * k) : make_float4(0.f, 0.f, 0.f, 0.f);
-        if (!ok1[k]) { a[u][k].z = 0.f; a[u][k].w = 0.f; }
+        for (int k = 0; k < 4; k++) {
+          int bytes = okc ? nb[k] : 0;
+          // nothing is read for bytes = 0; the address is then the matrix start
+          const float4 *src = bytes ? base + (size_t)c * lda2 + 32 * k : A;
+          cp_async16(buf + u * 128 + lane + 32 * k, src, bytes);
+        }
       }
+    }
+    cp_async_commit();
+  };
+  const int hi = (lane >> 4) & 1, b3 = (lane >> 3) & 1;
+#pragma unroll
+  for (int g = 0; g < SY_STAGES - 1; g++) issue(g);
+  for (int g = 0; g < nsteps; g++) {
+    issue(g + SY_STAGES - 1);
+    cp_async_wait<SY_STAGES - 1>();
+    const float4 *buf = my + (g % SY_STAGES) * 4 * 128;
+    const int c = cbeg + 4 * g;
     float t[4][2 * NR];
 #pragma unroll
-    for (int u = 0; u < 4; u++)
+    for (int u = 0; u < 4; u++) {
+      float4 a[4];
+#pragma unroll
+      for (int k = 0; k < 4; k++) a[k] = buf[u * 128 + lane + 32 * k];
 #pragma unroll
       for (int j = 0; j < NR; j++) {
         float2 x = xc[c + u][j];          // zero past nc
         float sr = 0.f, si = 0.f;
 #pragma unroll
         for (int k = 0; k < 4; k++) {
-          float4 v = a[u][k];
+          float4 v = a[k];
           dr[2 * k][j] += v.x * x.x - v.y * x.y;
           di[2 * k][j] += v.x * x.y + v.y * x.x;
           dr[2 * k + 1][j] += v.z * x.x - v.w * x.y;
@@ -208,6 +249,7 @@ __global__ void __launch_bounds__(128, 3) k_gm_matvec_sym_c64(int N, const float
         t[u][2 * j] = sr;
         t[u][2 * j + 1] = si;
       }
+    }
     if (trans) {
       // reduce-scatter of the four columns over the warp: halves exchanged
       // across lane bit 4, then bit 3, then full sums over bits 0-2
@@ -238,6 +280,8 @@ __global__ void __launch_bounds__(128, 3) k_gm_matvec_sym_c64(int N, const float
       }
     }
   }
+  cp_async_wait<0>();
+  __syncthreads();          // every warp is done with its stage buffers
 #pragma unroll
   for (int k = 0; k < 4; k++)
 #pragma unroll
@@ -368,6 +412,58 @@ __global__ void k_gm_axpy(int N, const z2 *D, size_t ldd, z2 *X, size_t ldx, int
   x->i += sign * d.i;
 }
 
+// Device-side Arnoldi bookkeeping, so that a restart cycle needs no host
+// round trip per step.  H (per right-hand side, (m+1) x m column-major), the
+// rotated residual vector g and the rotations (cs, sn) live on the device.
+// k_gm_hacc adds one Gram-Schmidt pass's coefficients into column k;
+// k_gm_givens finishes column k: subdiagonal = |w|, 1/|w| for the next basis
+// vector, the previous rotations applied, a new rotation that zeroes the
+// subdiagonal, g updated, |g[k+1]| recorded as the residual estimate.
+__global__ void k_gm_hacc(int k, int m, const z2 *dots, z2 *H, int add) {
+  int j = blockIdx.x, c = threadIdx.x;
+  if (c > k) return;
+  z2 d = dots[(size_t)j * (k + 1) + c];
+  z2 *h = H + (size_t)j * (m + 1) * m + (size_t)k * (m + 1) + c;
+  if (add) { h->r += d.r; h->i += d.i; }
+  else *h = d;
+}
+
+__device__ __forceinline__ z2 zmul2(z2 a, z2 b) { return z2{a.r * b.r - a.i * b.i, a.r * b.i + a.i * b.r}; }
+__device__ __forceinline__ z2 zconj2(z2 a) { return z2{a.r, -a.i}; }
+
+__global__ void k_gm_givens(int k, int m, int nrhs, const z2 *nrm2, z2 *H, z2 *g, z2 *cs, z2 *sn, double *sc,
+                            double *res) {
+  int j = threadIdx.x;
+  if (j >= nrhs) return;
+  double wn = sqrt(fmax(nrm2[j].r, 0.0));
+  sc[j] = wn > 0 ? 1.0 / wn : 0.0;
+  z2 *hc = H + (size_t)j * (m + 1) * m + (size_t)k * (m + 1);
+  z2 *csj = cs + (size_t)j * m, *snj = sn + (size_t)j * m, *gj = g + (size_t)j * (m + 1);
+  hc[k + 1] = z2{wn, 0.0};
+  for (int i = 0; i < k; i++) {
+    z2 a = zmul2(csj[i], hc[i]), b = zmul2(snj[i], hc[i + 1]);
+    z2 t{a.r + b.r, a.i + b.i};
+    z2 c = zmul2(z2{-snj[i].r, snj[i].i}, hc[i]), d = zmul2(zconj2(csj[i]), hc[i + 1]);
+    hc[i + 1] = z2{c.r + d.r, c.i + d.i};
+    hc[i] = t;
+  }
+  double a = hypot(hc[k].r, hc[k].i), b = hypot(hc[k + 1].r, hc[k + 1].i);
+  double r = sqrt(a * a + b * b);
+  // unitary [c s; -conj(s) conj(c)] with c = conj(hk)/r, s = conj(hk1)/r maps (hk, hk1) to (r, 0)
+  csj[k] = r > 0 ? z2{hc[k].r / r, -hc[k].i / r} : z2{1.0, 0.0};
+  snj[k] = r > 0 ? z2{hc[k + 1].r / r, -hc[k + 1].i / r} : z2{0.0, 0.0};
+  hc[k] = z2{r, 0.0};
+  hc[k + 1] = z2{0.0, 0.0};
+  z2 gk = gj[k];
+  gj[k] = zmul2(csj[k], gk);
+  gj[k + 1] = zmul2(z2{-snj[k].r, snj[k].i}, gk);
+  res[(size_t)j * m + k] = hypot(gj[k + 1].r, gj[k + 1].i);
+}
+
+// residual estimates are read back every GM_CHECK steps (and at the end of a
+// cycle): the steps in between run without host synchronisation
+#define GM_CHECK 8
+
 struct GmState {
   int N, nrhs, m;
   z2 *V, *W, *Z, *R, *part, *dots, *h;
@@ -382,11 +478,19 @@ static int dense_matvec(bg_matrix *A, const z2 *X, z2 *Y, GmState &S) {
     dim3 g1(S.nchunk, S.nchunk);
     const float4 *a4 = (const float4 *)A->d;
     size_t l2 = A->ld / 2;
+    static bool attr = false;
+    if (!attr) {
+      BG_CUDA_TRY(cudaFuncSetAttribute(k_gm_matvec_sym_c64<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sym_smem_bytes<1>()));
+      BG_CUDA_TRY(cudaFuncSetAttribute(k_gm_matvec_sym_c64<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sym_smem_bytes<2>()));
+      BG_CUDA_TRY(cudaFuncSetAttribute(k_gm_matvec_sym_c64<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sym_smem_bytes<3>()));
+      BG_CUDA_TRY(cudaFuncSetAttribute(k_gm_matvec_sym_c64<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sym_smem_bytes<4>()));
+      attr = true;
+    }
     switch (S.nrhs) {
-      case 1: k_gm_matvec_sym_c64<1><<<g1, 128, 0, stream()>>>(N, a4, l2, X, N, S.part); break;
-      case 2: k_gm_matvec_sym_c64<2><<<g1, 128, 0, stream()>>>(N, a4, l2, X, N, S.part); break;
-      case 3: k_gm_matvec_sym_c64<3><<<g1, 128, 0, stream()>>>(N, a4, l2, X, N, S.part); break;
-      default: k_gm_matvec_sym_c64<4><<<g1, 128, 0, stream()>>>(N, a4, l2, X, N, S.part); break;
+      case 1: k_gm_matvec_sym_c64<1><<<g1, 128, sym_smem_bytes<1>(), stream()>>>(N, a4, l2, X, N, S.part); break;
+      case 2: k_gm_matvec_sym_c64<2><<<g1, 128, sym_smem_bytes<2>(), stream()>>>(N, a4, l2, X, N, S.part); break;
+      case 3: k_gm_matvec_sym_c64<3><<<g1, 128, sym_smem_bytes<3>(), stream()>>>(N, a4, l2, X, N, S.part); break;
+      default: k_gm_matvec_sym_c64<4><<<g1, 128, sym_smem_bytes<4>(), stream()>>>(N, a4, l2, X, N, S.part); break;
     }
   } else if (A->precision == BG_C64) {
     dim3 g1((N + 2 * GV_ROWS - 1) / (2 * GV_ROWS), S.nchunk);
@@ -440,8 +544,10 @@ int gmres_solve(bg_matrix *A, const bg_precond *P, void *dB, int ldb, int nrhs, 
   GmState S{N, nrhs, m};
   S.nchunk = (N + GV_COLS - 1) / GV_COLS;
   size_t nv = (size_t)N * (m + 1) * nrhs;
-  size_t bytes = sizeof(z2) * (nv + 4 * (size_t)N * nrhs + (size_t)S.nchunk * nrhs * N + 2 * (size_t)(m + 2) * nrhs) +
-                 sizeof(double) * 8;
+  size_t nH = (size_t)nrhs * (m + 1) * m, ng = (size_t)nrhs * (m + 1), ncs = (size_t)nrhs * m;
+  size_t bytes = sizeof(z2) * (nv + 4 * (size_t)N * nrhs + (size_t)S.nchunk * nrhs * N + 2 * (size_t)(m + 2) * nrhs +
+                               nH + ng + 2 * ncs) +
+                 sizeof(double) * (8 + ncs);
   char *w = nullptr;
   BG_CUDA_TRY(cudaMallocAsync((void **)&w, bytes, stream()));
   S.V = (z2 *)w;
@@ -452,8 +558,19 @@ int gmres_solve(bg_matrix *A, const bg_precond *P, void *dB, int ldb, int nrhs, 
   S.part = X + (size_t)N * nrhs;
   S.dots = S.part + (size_t)S.nchunk * nrhs * N;
   S.h = S.dots + (size_t)(m + 2) * nrhs;
-  S.sc = (double *)(S.h + (size_t)(m + 2) * nrhs);
+  z2 *Hd = S.h + (size_t)(m + 2) * nrhs, *gd = Hd + nH, *csd = gd + ng, *snd = csd + ncs;
+  S.sc = (double *)(snd + ncs);
+  double *resd = S.sc + 8;
   const size_t vstride = (size_t)N * (m + 1);
+  // residual estimates read back to pinned host memory (one buffer per library instance)
+  static double *res_host = nullptr;
+  static size_t res_cap = 0;
+  if (res_cap < ncs) {
+    if (res_host) cudaFreeHost(res_host);
+    res_host = nullptr;
+    BG_CUDA_TRY(cudaMallocHost((void **)&res_host, sizeof(double) * ncs));
+    res_cap = ncs;
+  }
   int st = BG_OK;
   const z2 *B = (const z2 *)dB;
   // X = 0
@@ -486,80 +603,88 @@ int gmres_solve(bg_matrix *A, const bg_precond *P, void *dB, int ldb, int nrhs, 
     BG_CUDA_TRY(cudaMemcpyAsync(S.sc, inv.data(), sizeof(double) * nrhs, cudaMemcpyHostToDevice, stream()));
     k_gm_scale_copy<<<gr, 256, 0, stream()>>>(N, S.Z, N, S.sc, S.V, 0, vstride);
     g_launches++;
-    // Hessenberg and Givens state per rhs
-    std::vector<std::vector<zc>> H(nrhs, std::vector<zc>((size_t)(m + 1) * m, 0.0));
-    std::vector<std::vector<zc>> g(nrhs, std::vector<zc>(m + 1, 0.0)), cs(nrhs, std::vector<zc>(m)),
-        sn(nrhs, std::vector<zc>(m));
-    for (int j = 0; j < nrhs; j++) g[j][0] = rn[j];
-    int k = 0;
-    bool conv = false;
+    // Hessenberg, rotations and rotated residual on the device
+    {
+      std::vector<z2> g0(ng, z2{0.0, 0.0});
+      for (int j = 0; j < nrhs; j++) g0[(size_t)j * (m + 1)] = z2{rn[j], 0.0};
+      BG_CUDA_TRY(cudaMemcpyAsync(gd, g0.data(), sizeof(z2) * ng, cudaMemcpyHostToDevice, stream()));
+    }
+    const int total0 = total;
+    int k = 0, kconv = -1, checked = 0;
     for (; k < m && total < maxit; k++, total++) {
       // W = A M V[:,k]
-      z2 *vk = S.V + (size_t)k * N;   // rhs j at vk + j*vstride: gather into Z contiguous
+      z2 *vk = S.V + (size_t)k * N;   // rhs j at vk + j*vstride: gather into R contiguous
       for (int j = 0; j < nrhs; j++)
         BG_CUDA_TRY(cudaMemcpyAsync(S.R + (size_t)j * N, vk + j * vstride, sizeof(z2) * N, cudaMemcpyDeviceToDevice,
                                     stream()));
       if ((st = precond(P, S.R, S.Z, S))) break;
       if ((st = dense_matvec(A, S.Z, S.W, S))) break;
-      // CGS2
-      std::vector<zc> hcol((size_t)nrhs * (k + 2), 0.0);
+      // CGS2: two passes, coefficients summed into column k of H on the device
       prof_start(PROF_ORTHO);
       for (int pass = 0; pass < 2; pass++) {
         k_gm_dots<<<dim3(k + 1, nrhs), 256, 0, stream()>>>(N, k + 1, S.V, N, vstride, S.W, N, S.dots);
         g_launches++;
         k_gm_subtract<<<gr, 256, 0, stream()>>>(N, k + 1, S.V, N, vstride, S.dots, (size_t)(k + 1), S.W, N);
         g_launches++;
-        std::vector<z2> hd((size_t)nrhs * (k + 1));
-        BG_CUDA_TRY(cudaMemcpyAsync(hd.data(), S.dots, sizeof(z2) * hd.size(), cudaMemcpyDeviceToHost, stream()));
-        BG_CUDA_TRY(cudaStreamSynchronize(stream()));
-        for (int j = 0; j < nrhs; j++)
-          for (int c = 0; c <= k; c++) hcol[(size_t)j * (k + 2) + c] += zc(hd[(size_t)j * (k + 1) + c].r, hd[(size_t)j * (k + 1) + c].i);
+        k_gm_hacc<<<nrhs, 256, 0, stream()>>>(k, m, S.dots, Hd, pass);
+        g_launches++;
       }
-      std::vector<double> wn;
-      if ((st = colnorms(S.W, S, wn))) break;
+      k_gm_dots<<<dim3(1, nrhs), 256, 0, stream()>>>(N, 1, S.W, N, (size_t)N, S.W, N, S.dots);
+      g_launches++;
+      k_gm_givens<<<1, 32, 0, stream()>>>(k, m, nrhs, S.dots, Hd, gd, csd, snd, S.sc, resd);
+      g_launches++;
       prof_stop(PROF_ORTHO, 0.0);
-      for (int j = 0; j < nrhs; j++) {
-        hcol[(size_t)j * (k + 2) + k + 1] = wn[j];
-        inv[j] = wn[j] > 0 ? 1.0 / wn[j] : 0.0;
-      }
-      BG_CUDA_TRY(cudaMemcpyAsync(S.sc, inv.data(), sizeof(double) * nrhs, cudaMemcpyHostToDevice, stream()));
       if (k + 1 <= m) {
         k_gm_scale_copy<<<gr, 256, 0, stream()>>>(N, S.W, N, S.sc, S.V, (size_t)(k + 1) * N, vstride);
         g_launches++;
       }
-      // Givens
-      relres = 0;
-      for (int j = 0; j < nrhs; j++) {
-        std::vector<zc> hc(hcol.begin() + (size_t)j * (k + 2), hcol.begin() + (size_t)(j + 1) * (k + 2));
-        for (int i = 0; i < k; i++) {
-          zc t = cs[j][i] * hc[i] + sn[j][i] * hc[i + 1];
-          hc[i + 1] = -std::conj(sn[j][i]) * hc[i] + std::conj(cs[j][i]) * hc[i + 1];
-          hc[i] = t;
+      if ((k + 1) % GM_CHECK == 0 || k + 1 == m || total + 1 == maxit) {
+        // one round trip for the residual estimates of the last few steps
+        BG_CUDA_TRY(cudaMemcpy2DAsync(res_host, sizeof(double) * m, resd, sizeof(double) * m,
+                                      sizeof(double) * (k + 1), nrhs, cudaMemcpyDeviceToHost, stream()));
+        BG_CUDA_TRY(cudaStreamSynchronize(stream()));
+        for (int kk = checked; kk <= k && kconv < 0; kk++) {
+          double rr = 0;
+          for (int j = 0; j < nrhs; j++) rr = std::max(rr, res_host[(size_t)j * m + kk] / bn[j]);
+          relres = rr;
+          if (rr <= tol) kconv = kk;
         }
-        double a = std::abs(hc[k]), b = std::abs(hc[k + 1]);
-        double r = std::sqrt(a * a + b * b);
-        // unitary [c s; -conj(s) conj(c)] with c = conj(a)/r, s = conj(b)/r maps (a, b) to (r, 0)
-        cs[j][k] = r > 0 ? std::conj(hc[k]) / r : zc(1.0);
-        sn[j][k] = r > 0 ? std::conj(hc[k + 1]) / r : zc(0.0);
-        hc[k] = r;
-        hc[k + 1] = 0.0;
-        zc gk = g[j][k];
-        g[j][k] = cs[j][k] * gk;
-        g[j][k + 1] = -std::conj(sn[j][k]) * gk;
-        for (int i = 0; i <= k; i++) H[j][(size_t)i + (size_t)k * (m + 1)] = hc[i];
-        relres = std::max(relres, std::abs(g[j][k + 1]) / bn[j]);
+        checked = k + 1;
+        if (kconv >= 0) { k++; total++; break; }
       }
-      if (relres <= tol) { k++; total++; conv = true; break; }
     }
     if (st) break;
+    bool conv = kconv >= 0;
+    if (!conv && checked < k) {
+      // steps after the last check (the cycle ended on maxit)
+      BG_CUDA_TRY(cudaMemcpy2DAsync(res_host, sizeof(double) * m, resd, sizeof(double) * m, sizeof(double) * k, nrhs,
+                                    cudaMemcpyDeviceToHost, stream()));
+      BG_CUDA_TRY(cudaStreamSynchronize(stream()));
+      for (int kk = checked; kk < k && kconv < 0; kk++) {
+        double rr = 0;
+        for (int j = 0; j < nrhs; j++) rr = std::max(rr, res_host[(size_t)j * m + kk] / bn[j]);
+        relres = rr;
+        if (rr <= tol) kconv = kk;
+      }
+      conv = kconv >= 0;
+    }
+    // the least-squares problem over the first kconv + 1 columns (columns and
+    // g entries before a step are final once that step is done)
+    if (conv) k = kconv + 1;
+    total = total0 + k;
+    std::vector<z2> Hh(nH), gh(ng);
+    BG_CUDA_TRY(cudaMemcpyAsync(Hh.data(), Hd, sizeof(z2) * nH, cudaMemcpyDeviceToHost, stream()));
+    BG_CUDA_TRY(cudaMemcpyAsync(gh.data(), gd, sizeof(z2) * ng, cudaMemcpyDeviceToHost, stream()));
+    BG_CUDA_TRY(cudaStreamSynchronize(stream()));
     // back substitution y = H^-1 g, X += M V y
     std::vector<z2> yh((size_t)nrhs * k);
     for (int j = 0; j < nrhs; j++) {
+      auto Hj = [&](int r, int c) { z2 v = Hh[(size_t)j * (m + 1) * m + (size_t)c * (m + 1) + r]; return zc(v.r, v.i); };
       std::vector<zc> y(k);
       for (int i = k - 1; i >= 0; i--) {
-        zc s = g[j][i];
-        for (int c = i + 1; c < k; c++) s -= H[j][(size_t)i + (size_t)c * (m + 1)] * y[c];
-        y[i] = s / H[j][(size_t)i + (size_t)i * (m + 1)];
+        zc sum(gh[(size_t)j * (m + 1) + i].r, gh[(size_t)j * (m + 1) + i].i);
+        for (int c = i + 1; c < k; c++) sum -= Hj(i, c) * y[c];
+        y[i] = sum / Hj(i, i);
       }
       for (int i = 0; i < k; i++) yh[(size_t)j * k + i] = z2{y[i].real(), y[i].imag()};
     }
@@ -666,9 +791,9 @@ int precond_jacobi(bg_matrix *A, bg_precond **out) {
   bg_precond *P = new bg_precond();
   P->N = A->N;
   P->nnz = A->N;
-  BG_CUDA_TRY(cudaMalloc(&P->rowptr, sizeof(int) * (A->N + 1)));
-  BG_CUDA_TRY(cudaMalloc(&P->col, sizeof(int) * A->N));
-  BG_CUDA_TRY(cudaMalloc(&P->val, sizeof(z2) * A->N));
+  BG_CUDA_TRY(cudaMallocAsync((void **)&P->rowptr, sizeof(int) * (A->N + 1), stream()));
+  BG_CUDA_TRY(cudaMallocAsync((void **)&P->col, sizeof(int) * A->N, stream()));
+  BG_CUDA_TRY(cudaMallocAsync((void **)&P->val, sizeof(z2) * A->N, stream()));
   k_gm_diag_inv<<<(A->N + 256) / 256, 256, 0, stream()>>>(A->N, (const z2 *)A->d, A->ld, P->rowptr, P->col,
                                                           (z2 *)P->val);
   BG_LAUNCHED();

@@ -663,7 +663,7 @@ static int ensure_graph(bg_geometry *g) {
 
 static int bound_coefficient(GnnBufs &B);
 
-static int bufs_init(bg_geometry *g, bg_matrix *A, double omega, bool train, GnnBufs &B) {
+static int bufs_alloc(bg_geometry *g, bool train, GnnBufs &B) {
   int st = ensure_graph(g);
   if (st) return st;
   int N = g->N, E = g->graph.E;
@@ -690,10 +690,58 @@ static int bufs_init(bg_geometry *g, bg_matrix *A, double omega, bool train, Gnn
         (st = balloc(B, &B.dP, n64)) || (st = balloc(B, &B.dQ, n64)))
       return st;
   }
+  return BG_OK;
+}
+
+static int bound_coefficient(GnnBufs &B);
+
+// per-call part: features of (A, omega) and the coefficient bound
+static int bufs_compute(bg_geometry *g, bg_matrix *A, double omega, GnnBufs &B) {
+  int N = B.N;
   k_gnn_features<<<(N + 127) / 128, 128, 0, stream()>>>(N, B.rowptr, B.col, (const z2g *)A->d, A->ld, g->dev, omega,
                                                         g->graph.h, B.F, B.Ef, B.ratio, B.dinv);
   BG_LAUNCHED();
   return bound_coefficient(B);
+}
+
+static int bufs_init(bg_geometry *g, bg_matrix *A, double omega, bool train, GnnBufs &B) {
+  int st = bufs_alloc(g, train, B);
+  return st ? st : bufs_compute(g, A, omega, B);
+}
+
+// The inference buffers (about 15 node-sized and 2 edge-sized arrays) are kept
+// with the geometry and reused by every learned preconditioner built for it,
+// so a frequency step allocates no graph-network memory.
+static int inference_bufs(bg_geometry *g, GnnBufs *&B) {
+  int st = ensure_graph(g);
+  if (st) return st;
+  GnnBufs *c = static_cast<GnnBufs *>(g->gnn_cache);
+  if (c && (c->N != g->N || c->E != g->graph.E)) {
+    bufs_free(*c);
+    delete c;
+    c = nullptr;
+    g->gnn_cache = nullptr;
+  }
+  if (!c) {
+    c = new GnnBufs();
+    if ((st = bufs_alloc(g, false, *c))) {
+      bufs_free(*c);
+      delete c;
+      return st;
+    }
+    g->gnn_cache = c;
+  }
+  B = c;
+  return BG_OK;
+}
+
+void gnn_cache_free(bg_geometry *g) {
+  GnnBufs *c = static_cast<GnnBufs *>(g->gnn_cache);
+  if (c) {
+    bufs_free(*c);
+    delete c;
+  }
+  g->gnn_cache = nullptr;
 }
 
 // Power iteration (four seeded vectors in lockstep, GNN_POWER_ITERS steps)
@@ -975,18 +1023,24 @@ int bg_precond_create_learned(bg_geometry *g, bg_matrix *A, double omega, const 
   }
   *out = nullptr;
   if (A->factored) { set_error("bg_precond_create_learned: matrix holds LU factors"); return BG_ERR_STATE; }
-  GnnBufs B;
+  GnnBufs *Bp = nullptr;
   prof_start(PROF_GNN);
-  int st = bufs_init(g, A, omega, false, B);
+  int st = inference_bufs(g, Bp);
+  if (st) {
+    prof_stop(PROF_GNN, 0.0);
+    return st;
+  }
+  GnnBufs &B = *Bp;
+  st = bufs_compute(g, A, omega, B);
   bg_precond *P = nullptr;
   if (!st) {
     P = new bg_precond();
     P->N = B.N;
     P->nnz = B.E;
 
-    cudaError_t e = cudaMalloc(&P->rowptr, sizeof(int) * (B.N + 1));
-    if (e == cudaSuccess) e = cudaMalloc(&P->col, sizeof(int) * B.E);
-    if (e == cudaSuccess) e = cudaMalloc(&P->val, sizeof(z2g) * B.E);
+    cudaError_t e = cudaMallocAsync((void **)&P->rowptr, sizeof(int) * (B.N + 1), stream());
+    if (e == cudaSuccess) e = cudaMallocAsync((void **)&P->col, sizeof(int) * B.E, stream());
+    if (e == cudaSuccess) e = cudaMallocAsync((void **)&P->val, sizeof(z2g) * B.E, stream());
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(P->rowptr, B.rowptr, sizeof(int) * (B.N + 1), cudaMemcpyDeviceToDevice, stream());
     if (e == cudaSuccess) e = cudaMemcpyAsync(P->col, B.col, sizeof(int) * B.E, cudaMemcpyDeviceToDevice, stream());
@@ -996,10 +1050,7 @@ int bg_precond_create_learned(bg_geometry *g, bg_matrix *A, double omega, const 
   if (!st) {
     P->rho = B.rho_ref;
     P->theta = B.smax;
-    cudaError_t e = cudaStreamSynchronize(stream());   // the activations are freed below
-    if (e != cudaSuccess) { set_error("learned preconditioner: %s", cudaGetErrorString(e)); st = BG_ERR_CUDA; }
   }
-  bufs_free(B);
   prof_stop(PROF_GNN, 0.0);
   if (st) {
     bg_precond_destroy(P);

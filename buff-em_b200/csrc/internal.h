@@ -139,6 +139,7 @@ struct bg_geometry {
   bg::NearGraph graph;
   double *d_scratch = nullptr;  // general scratch (PFT partial sums etc.)
   double *d_fieldTet = nullptr, *d_fieldFace = nullptr;  // GetFields tables, 16 doubles per tet each
+  void *gnn_cache = nullptr;    // graph-network inference buffers, reused across learned preconditioners
   size_t scratch_bytes = 0;
 };
 
@@ -183,6 +184,8 @@ int pft(bg_geometry *g, double wr, double wi, const void *dJ, const double *E0, 
 // dJ may be null (incident field only), E0/nhat null (no incident field)
 int get_fields(bg_geometry *g, double wr, double wi, const void *dJ, const double *E0, const double *nhat,
                int npts, const double *dX, void *dOut);
+// frees the graph-network inference buffers kept with a geometry
+void gnn_cache_free(bg_geometry *g);
 // EMT PFT with a dressed Rytov matrix (device, column-major ldr) and no incident field
 int pft_emt_dr(bg_geometry *g, double wr, double wi, const void *dDR, size_t ldr, double *out);
 // buff-neq overlap rows: 8 slots per basis function (idx -1 past cnt[a])
