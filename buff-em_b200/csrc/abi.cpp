@@ -49,7 +49,7 @@ int ensure_device() {
     return BG_ERR_CUDA;
   }
   BG_CUDA_TRY(cudaStreamCreateWithFlags(&s_stream, cudaStreamNonBlocking));
-  // keep up to 1 GiB of freed stream-ordered allocations in this process's
+  // keep up to 8 GiB of freed stream-ordered allocations in this process's
   // default pool across synchronizations, so per-call scratch buffers do not
   // go back to the driver every call (larger transients are still returned)
   cudaMemPool_t pool;

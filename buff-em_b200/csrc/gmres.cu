@@ -73,11 +73,11 @@ __global__ void __launch_bounds__(GV_ROWS) k_gm_matvec_part(int N, const z2 *A, 
 }
 
 // Same for the complex64 copy of the matrix: each thread takes two adjacent
-// rows (one 16-byte load per column), FP32 accumulation within a chunk, FP64
-// partial sums across chunks.  Reads row N when N is odd: complex64 matrices
+// rows (one 16-byte load per column), FP32 accumulation within a chunk,
+// complex64 partials summed in FP64 across chunks.  Reads row N when N is odd: complex64 matrices
 // are stored with a leading dimension padded to a multiple of 32 (> N then).
 __global__ void __launch_bounds__(GV_ROWS) k_gm_matvec_part_c64(int N, const float4 *A, size_t lda2, const z2 *X,
-                                                                size_t ldx, int nrhs, z2 *partial) {
+                                                                size_t ldx, int nrhs, float2 *partial) {
   __shared__ float2 xs[GV_COLS][GM_MAXRHS];
   int row = 2 * (blockIdx.x * GV_ROWS + threadIdx.x);
   int c0 = blockIdx.y * GV_COLS;
@@ -122,8 +122,8 @@ __global__ void __launch_bounds__(GV_ROWS) k_gm_matvec_part_c64(int N, const flo
       }
   }
   for (int j = 0; j < nrhs; j++) {
-    partial[((size_t)blockIdx.y * nrhs + j) * N + row] = z2{ar0[j], ai0[j]};
-    if (row + 1 < N) partial[((size_t)blockIdx.y * nrhs + j) * N + row + 1] = z2{ar1[j], ai1[j]};
+    partial[((size_t)blockIdx.y * nrhs + j) * N + row] = make_float2(ar0[j], ai0[j]);
+    if (row + 1 < N) partial[((size_t)blockIdx.y * nrhs + j) * N + row + 1] = make_float2(ar1[j], ai1[j]);
   }
 }
 
@@ -139,7 +139,8 @@ __global__ void __launch_bounds__(GV_ROWS) k_gm_matvec_part_c64(int N, const flo
 // flight while a step is computed; the transposed products of four columns
 // are reduce-scattered across the warp's lanes, the direct ones summed over
 // the four warps through shared memory.  FP32
-// accumulation within a tile, FP64 partials, as in k_gm_matvec_part_c64.
+// accumulation within a tile, complex64 partials summed in FP64, as in
+// k_gm_matvec_part_c64.
 // Entries of rows >= N (the padding of the leading dimension) are never read:
 // their copies are zero-filled.
 // 16-byte asynchronous global-to-shared copy; src_bytes < 16 zero-fills the rest
@@ -162,7 +163,7 @@ constexpr size_t sym_smem_bytes() {
 
 template <int NR>
 __global__ void __launch_bounds__(128) k_gm_matvec_sym_c64(int N, const float4 *A, size_t lda2, const z2 *X,
-                                                           size_t ldx, z2 *partial) {
+                                                           size_t ldx, float2 *partial) {
   const int I = blockIdx.x, J = blockIdx.y;
   if (I > J) return;
   const int r0 = I * 256, c0 = J * 256;
@@ -276,7 +277,7 @@ __global__ void __launch_bounds__(128) k_gm_matvec_sym_c64(int N, const float4 *
       int cc = c + 2 * hi + b3;
       if ((lane & 7) == 0 && cc < cend) {
 #pragma unroll
-        for (int j = 0; j < NR; j++) partial[((size_t)I * NR + j) * N + c0 + cc] = z2{f[2 * j], f[2 * j + 1]};
+        for (int j = 0; j < NR; j++) partial[((size_t)I * NR + j) * N + c0 + cc] = make_float2(f[2 * j], f[2 * j + 1]);
       }
     }
   }
@@ -292,15 +293,30 @@ __global__ void __launch_bounds__(128) k_gm_matvec_sym_c64(int N, const float4 *
   __syncthreads();
   for (int e = threadIdx.x; e < nr * NR; e += 128) {
     int i = e / NR, j = e % NR;
-    double sr = 0.0, si = 0.0;
+    float sr = 0.f, si = 0.f;
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       float2 v = dacc[q][i][j];
       sr += v.x;
       si += v.y;
     }
-    partial[((size_t)J * NR + j) * N + r0 + i] = z2{sr, si};
+    partial[((size_t)J * NR + j) * N + r0 + i] = make_float2(sr, si);
   }
+}
+
+// the complex64 kernels' partials are FP32 sums already: stored as complex64
+// (half the bytes of the partial buffer) and added up in FP64 here
+__global__ void k_gm_matvec_sum_f(int N, int nchunk, int nrhs, const float2 *partial, z2 *Y, size_t ldy) {
+  int row = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y;
+  if (row >= N || j >= nrhs) return;
+  double sr = 0, si = 0;
+  for (int k = 0; k < nchunk; k++) {
+    float2 p = partial[((size_t)k * nrhs + j) * N + row];
+    sr += p.x;
+    si += p.y;
+  }
+  Y[(size_t)j * ldy + row] = z2{sr, si};
 }
 
 __global__ void k_gm_matvec_sum(int N, int nchunk, int nrhs, const z2 *partial, z2 *Y, size_t ldy) {
@@ -474,6 +490,7 @@ struct GmState {
 static int dense_matvec(bg_matrix *A, const z2 *X, z2 *Y, GmState &S) {
   int N = S.N;
   prof_start(PROF_MATVEC);
+  float2 *pf = reinterpret_cast<float2 *>(S.part);
   if (A->precision == BG_C64 && A->symmetric) {
     dim3 g1(S.nchunk, S.nchunk);
     const float4 *a4 = (const float4 *)A->d;
@@ -487,20 +504,23 @@ static int dense_matvec(bg_matrix *A, const z2 *X, z2 *Y, GmState &S) {
       attr = true;
     }
     switch (S.nrhs) {
-      case 1: k_gm_matvec_sym_c64<1><<<g1, 128, sym_smem_bytes<1>(), stream()>>>(N, a4, l2, X, N, S.part); break;
-      case 2: k_gm_matvec_sym_c64<2><<<g1, 128, sym_smem_bytes<2>(), stream()>>>(N, a4, l2, X, N, S.part); break;
-      case 3: k_gm_matvec_sym_c64<3><<<g1, 128, sym_smem_bytes<3>(), stream()>>>(N, a4, l2, X, N, S.part); break;
-      default: k_gm_matvec_sym_c64<4><<<g1, 128, sym_smem_bytes<4>(), stream()>>>(N, a4, l2, X, N, S.part); break;
+      case 1: k_gm_matvec_sym_c64<1><<<g1, 128, sym_smem_bytes<1>(), stream()>>>(N, a4, l2, X, N, pf); break;
+      case 2: k_gm_matvec_sym_c64<2><<<g1, 128, sym_smem_bytes<2>(), stream()>>>(N, a4, l2, X, N, pf); break;
+      case 3: k_gm_matvec_sym_c64<3><<<g1, 128, sym_smem_bytes<3>(), stream()>>>(N, a4, l2, X, N, pf); break;
+      default: k_gm_matvec_sym_c64<4><<<g1, 128, sym_smem_bytes<4>(), stream()>>>(N, a4, l2, X, N, pf); break;
     }
   } else if (A->precision == BG_C64) {
     dim3 g1((N + 2 * GV_ROWS - 1) / (2 * GV_ROWS), S.nchunk);
-    k_gm_matvec_part_c64<<<g1, GV_ROWS, 0, stream()>>>(N, (const float4 *)A->d, A->ld / 2, X, N, S.nrhs, S.part);
+    k_gm_matvec_part_c64<<<g1, GV_ROWS, 0, stream()>>>(N, (const float4 *)A->d, A->ld / 2, X, N, S.nrhs, pf);
   } else {
     dim3 g1((N + GV_ROWS - 1) / GV_ROWS, S.nchunk);
     k_gm_matvec_part<<<g1, GV_ROWS, 0, stream()>>>(N, (const z2 *)A->d, A->ld, X, N, S.nrhs, S.part);
   }
   BG_LAUNCHED();
-  k_gm_matvec_sum<<<dim3((N + 255) / 256, S.nrhs), 256, 0, stream()>>>(N, S.nchunk, S.nrhs, S.part, Y, N);
+  if (A->precision == BG_C64)
+    k_gm_matvec_sum_f<<<dim3((N + 255) / 256, S.nrhs), 256, 0, stream()>>>(N, S.nchunk, S.nrhs, pf, Y, N);
+  else
+    k_gm_matvec_sum<<<dim3((N + 255) / 256, S.nrhs), 256, 0, stream()>>>(N, S.nchunk, S.nrhs, S.part, Y, N);
   BG_LAUNCHED();
   // algorithmic bytes of matrix read: the upper-triangle tiles for a
   // symmetric complex64 matrix, the whole matrix otherwise

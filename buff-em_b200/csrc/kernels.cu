@@ -322,9 +322,10 @@ __global__ void __launch_bounds__(FTHR, 2) k_far(DevGeom g, cd k, cd invk2, cd *
         for (int j = 0; j < 4; j++) {
           double y0 = S.pB[tB][j][0], y1 = S.pB[tB][j][1], y2 = S.pB[tB][j][2];
           double R0 = x0 - y0, R1 = x1 - y1, R2 = x2 - y2;
-          double r = sqrt(R0 * R0 + R1 * R1 + R2 * R2);
-          if (r < 1.0e-12) continue;
-          cd phi = cscale(expikr(k, r), inv4pi / r);
+          double r2 = R0 * R0 + R1 * R1 + R2 * R2;
+          if (r2 < 1.0e-24) continue;           // r < 1e-12
+          double ir = rsqrt(r2), r = r2 * ir;   // one reciprocal square root instead of sqrt and a division
+          cd phi = cscale(expikr(k, r), inv4pi * ir);
           double yt0 = y0 - S.oB[tB][0], yt1 = y1 - S.oB[tB][1], yt2 = y2 - S.oB[tB][2];
           phiI = cadd(phiI, phi);
           m[4] = cadd(m[4], cscale(phi, yt0));
