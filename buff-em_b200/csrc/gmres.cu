@@ -183,11 +183,20 @@ __global__ void __launch_bounds__(128) k_gm_matvec_sym_c64(int N, const float4 *
   __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const bool trans = I < J;
-  float dr[8][NR], di[8][NR];
+  // packed FP32 pairs: D = (re, im) accumulators of this lane's 8 rows; the
+  // transposed products use this lane's x_I values as broadcast pairs
+  // (xr, xr) and (xi, xi), so a complex multiply-accumulate is two __ffma2_rn:
+  //   (re, im) += (ar, ai) * (yr, yr) + (-ai, ar) * (yi, yi)
+  float2 D[8][NR], Yr[8][NR], Yi[8][NR];
 #pragma unroll
   for (int q = 0; q < 8; q++)
 #pragma unroll
-    for (int j = 0; j < NR; j++) dr[q][j] = di[q][j] = 0.f;
+    for (int j = 0; j < NR; j++) {
+      D[q][j] = make_float2(0.f, 0.f);
+      float2 y = xr[64 * (q >> 1) + 2 * lane + (q & 1)][j];
+      Yr[q][j] = make_float2(y.x, y.x);
+      Yi[q][j] = make_float2(y.y, y.y);
+    }
   // this lane's rows 64 k + 2 lane (+1): bytes of the pair that exist
   int nb[4];
 #pragma unroll
@@ -229,26 +238,32 @@ __global__ void __launch_bounds__(128) k_gm_matvec_sym_c64(int N, const float4 *
     float t[4][2 * NR];
 #pragma unroll
     for (int u = 0; u < 4; u++) {
-      float4 a[4];
+      float2 T[NR];
 #pragma unroll
-      for (int k = 0; k < 4; k++) a[k] = buf[u * 128 + lane + 32 * k];
+      for (int jj = 0; jj < NR; jj++) T[jj] = make_float2(0.f, 0.f);
 #pragma unroll
-      for (int j = 0; j < NR; j++) {
-        float2 x = xc[c + u][j];          // zero past nc
-        float sr = 0.f, si = 0.f;
+      for (int k = 0; k < 4; k++) {
+        float4 v = buf[u * 128 + lane + 32 * k];
+        float2 e0 = make_float2(v.x, v.y), e1 = make_float2(v.z, v.w);
+        float2 s0 = make_float2(-v.y, v.x), s1 = make_float2(-v.w, v.z);
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
-          float4 v = a[k];
-          dr[2 * k][j] += v.x * x.x - v.y * x.y;
-          di[2 * k][j] += v.x * x.y + v.y * x.x;
-          dr[2 * k + 1][j] += v.z * x.x - v.w * x.y;
-          di[2 * k + 1][j] += v.z * x.y + v.w * x.x;
-          float2 y0 = xr[64 * k + 2 * lane][j], y1 = xr[64 * k + 2 * lane + 1][j];
-          sr += v.x * y0.x - v.y * y0.y + v.z * y1.x - v.w * y1.y;
-          si += v.x * y0.y + v.y * y0.x + v.z * y1.y + v.w * y1.x;
+        for (int jj = 0; jj < NR; jj++) {
+          float2 x = xc[c + u][jj];          // zero past nc
+          float2 xrr = make_float2(x.x, x.x), xii = make_float2(x.y, x.y);
+          D[2 * k][jj] = __ffma2_rn(e0, xrr, D[2 * k][jj]);
+          D[2 * k][jj] = __ffma2_rn(s0, xii, D[2 * k][jj]);
+          D[2 * k + 1][jj] = __ffma2_rn(e1, xrr, D[2 * k + 1][jj]);
+          D[2 * k + 1][jj] = __ffma2_rn(s1, xii, D[2 * k + 1][jj]);
+          T[jj] = __ffma2_rn(e0, Yr[2 * k][jj], T[jj]);
+          T[jj] = __ffma2_rn(s0, Yi[2 * k][jj], T[jj]);
+          T[jj] = __ffma2_rn(e1, Yr[2 * k + 1][jj], T[jj]);
+          T[jj] = __ffma2_rn(s1, Yi[2 * k + 1][jj], T[jj]);
         }
-        t[u][2 * j] = sr;
-        t[u][2 * j + 1] = si;
+      }
+#pragma unroll
+      for (int jj = 0; jj < NR; jj++) {
+        t[u][2 * jj] = T[jj].x;
+        t[u][2 * jj + 1] = T[jj].y;
       }
     }
     if (trans) {
@@ -287,8 +302,8 @@ __global__ void __launch_bounds__(128) k_gm_matvec_sym_c64(int N, const float4 *
   for (int k = 0; k < 4; k++)
 #pragma unroll
     for (int j = 0; j < NR; j++) {
-      dacc[w][64 * k + 2 * lane][j] = make_float2(dr[2 * k][j], di[2 * k][j]);
-      dacc[w][64 * k + 2 * lane + 1][j] = make_float2(dr[2 * k + 1][j], di[2 * k + 1][j]);
+      dacc[w][64 * k + 2 * lane][j] = D[2 * k][j];
+      dacc[w][64 * k + 2 * lane + 1][j] = D[2 * k + 1][j];
     }
   __syncthreads();
   for (int e = threadIdx.x; e < nr * NR; e += 128) {
