@@ -347,19 +347,37 @@ __global__ void k_gm_matvec_sum(int N, int nchunk, int nrhs, const z2 *partial, 
   Y[(size_t)j * ldy + row] = z2{sr, si};
 }
 
-// Y[:, j] = M X[:, j], M in CSR (row i: sum over its near columns)
-__global__ void k_gm_spmv(int N, const int *rowptr, const int *col, const z2 *val, const z2 *X, size_t ldx, int nrhs,
-                          z2 *Y, size_t ldy) {
-  int row = blockIdx.x * blockDim.x + threadIdx.x;
-  int j = blockIdx.y;
-  if (row >= N || j >= nrhs) return;
-  double sr = 0, si = 0;
-  for (int p = rowptr[row]; p < rowptr[row + 1]; p++) {
-    z2 m = val[p], x = X[(size_t)j * ldx + col[p]];
-    sr += m.r * x.r - m.i * x.i;
-    si += m.r * x.i + m.i * x.r;
+// Y = M X for the sparse preconditioner, eight lanes per row (the row's
+// entries are contiguous, so a warp's loads cover four rows' lists in
+// order) and every right-hand side per read of the matrix; the lanes'
+// partial sums are combined by a fixed butterfly (deterministic)
+__global__ void k_gm_spmv8(int N, const int *rowptr, const int *col, const z2 *val, const z2 *X, size_t ldx, int nrhs,
+                           z2 *Y, size_t ldy) {
+  int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 3, sub = threadIdx.x & 7;
+  double sr[GM_MAXRHS] = {0, 0, 0, 0}, si[GM_MAXRHS] = {0, 0, 0, 0};
+  if (row < N) {
+    int p1 = rowptr[row + 1];
+    for (int p = rowptr[row] + sub; p < p1; p += 8) {
+      z2 m = val[p];
+      int c = col[p];
+#pragma unroll
+      for (int j = 0; j < GM_MAXRHS; j++)
+        if (j < nrhs) {
+          z2 x = X[(size_t)j * ldx + c];
+          sr[j] += m.r * x.r - m.i * x.i;
+          si[j] += m.r * x.i + m.i * x.r;
+        }
+    }
   }
-  Y[(size_t)j * ldy + row] = z2{sr, si};
+#pragma unroll
+  for (int o = 4; o > 0; o >>= 1)
+#pragma unroll
+    for (int j = 0; j < GM_MAXRHS; j++) {
+      sr[j] += __shfl_xor_sync(0xffffffffu, sr[j], o);
+      si[j] += __shfl_xor_sync(0xffffffffu, si[j], o);
+    }
+  if (row < N && sub == 0)
+    for (int j = 0; j < nrhs; j++) Y[(size_t)j * ldy + row] = z2{sr[j], si[j]};
 }
 
 // dots[j*(k) + c] = <V_j[:,c], w_j>  (c < k), block reduction per (c, j)
@@ -443,6 +461,38 @@ __global__ void k_gm_axpy(int N, const z2 *D, size_t ldd, z2 *X, size_t ldx, int
   x->i += sign * d.i;
 }
 
+// Gram-Schmidt dot products split over GM_DSPLIT row slices, so that even the
+// first steps (one or two basis vectors) keep the GPU busy; slice s of
+// <V_j[:,c], w_j> goes to part[(j k + c) GM_DSPLIT + s] and the slices are
+// added in a fixed order by the consumer (k_gm_hacc, k_gm_givens)
+#define GM_DSPLIT 16
+__global__ void k_gm_dots_part(int N, int k, const z2 *V, size_t ldv, size_t vstride, const z2 *W, size_t ldw,
+                               z2 *part) {
+  int c = blockIdx.x, j = blockIdx.y, sl = blockIdx.z;
+  int len = (N + GM_DSPLIT - 1) / GM_DSPLIT, i0 = sl * len, i1 = min(N, i0 + len);
+  const z2 *v = V + j * vstride + (size_t)c * ldv;
+  const z2 *w = W + (size_t)j * ldw;
+  double sr = 0, si = 0;
+  for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+    z2 a = v[i], b = w[i];
+    sr += a.r * b.r + a.i * b.i;   // conj(a) b
+    si += a.r * b.i - a.i * b.r;
+  }
+  __shared__ double rs[32], is[32];
+  for (int o = 16; o > 0; o >>= 1) {
+    sr += __shfl_xor_sync(0xffffffffu, sr, o);
+    si += __shfl_xor_sync(0xffffffffu, si, o);
+  }
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) { rs[wid] = sr; is[wid] = si; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0, b = 0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); q++) { a += rs[q]; b += is[q]; }
+    part[((size_t)j * k + c) * GM_DSPLIT + sl] = z2{a, b};
+  }
+}
+
 // Device-side Arnoldi bookkeeping, so that a restart cycle needs no host
 // round trip per step.  H (per right-hand side, (m+1) x m column-major), the
 // rotated residual vector g and the rotations (cs, sn) live on the device.
@@ -450,10 +500,13 @@ __global__ void k_gm_axpy(int N, const z2 *D, size_t ldd, z2 *X, size_t ldx, int
 // k_gm_givens finishes column k: subdiagonal = |w|, 1/|w| for the next basis
 // vector, the previous rotations applied, a new rotation that zeroes the
 // subdiagonal, g updated, |g[k+1]| recorded as the residual estimate.
-__global__ void k_gm_hacc(int k, int m, const z2 *dots, z2 *H, int add) {
+__global__ void k_gm_hacc(int k, int m, const z2 *part, z2 *dots, z2 *H, int add) {
   int j = blockIdx.x, c = threadIdx.x;
   if (c > k) return;
-  z2 d = dots[(size_t)j * (k + 1) + c];
+  const z2 *p = part + ((size_t)j * (k + 1) + c) * GM_DSPLIT;
+  z2 d{0.0, 0.0};
+  for (int sl = 0; sl < GM_DSPLIT; sl++) { d.r += p[sl].r; d.i += p[sl].i; }
+  dots[(size_t)j * (k + 1) + c] = d;   // this pass's coefficients, for k_gm_subtract
   z2 *h = H + (size_t)j * (m + 1) * m + (size_t)k * (m + 1) + c;
   if (add) { h->r += d.r; h->i += d.i; }
   else *h = d;
@@ -462,11 +515,13 @@ __global__ void k_gm_hacc(int k, int m, const z2 *dots, z2 *H, int add) {
 __device__ __forceinline__ z2 zmul2(z2 a, z2 b) { return z2{a.r * b.r - a.i * b.i, a.r * b.i + a.i * b.r}; }
 __device__ __forceinline__ z2 zconj2(z2 a) { return z2{a.r, -a.i}; }
 
-__global__ void k_gm_givens(int k, int m, int nrhs, const z2 *nrm2, z2 *H, z2 *g, z2 *cs, z2 *sn, double *sc,
+__global__ void k_gm_givens(int k, int m, int nrhs, const z2 *npart, z2 *H, z2 *g, z2 *cs, z2 *sn, double *sc,
                             double *res) {
   int j = threadIdx.x;
   if (j >= nrhs) return;
-  double wn = sqrt(fmax(nrm2[j].r, 0.0));
+  double n2 = 0.0;
+  for (int sl = 0; sl < GM_DSPLIT; sl++) n2 += npart[(size_t)j * GM_DSPLIT + sl].r;
+  double wn = sqrt(fmax(n2, 0.0));
   sc[j] = wn > 0 ? 1.0 / wn : 0.0;
   z2 *hc = H + (size_t)j * (m + 1) * m + (size_t)k * (m + 1);
   z2 *csj = cs + (size_t)j * m, *snj = sn + (size_t)j * m, *gj = g + (size_t)j * (m + 1);
@@ -552,8 +607,8 @@ static int precond(const bg_precond *P, const z2 *X, z2 *Y, GmState &S) {
     BG_CUDA_TRY(cudaMemcpyAsync(Y, X, sizeof(z2) * (size_t)N * S.nrhs, cudaMemcpyDeviceToDevice, stream()));
     return BG_OK;
   }
-  k_gm_spmv<<<dim3((N + 127) / 128, S.nrhs), 128, 0, stream()>>>(N, P->rowptr, P->col, (const z2 *)P->val, X, N,
-                                                                 S.nrhs, Y, N);
+  k_gm_spmv8<<<(unsigned)(((size_t)N * 8 + 255) / 256), 256, 0, stream()>>>(N, P->rowptr, P->col, (const z2 *)P->val,
+                                                                             X, N, S.nrhs, Y, N);
   BG_LAUNCHED();
   prof_stop(PROF_PRECOND, 0.0);
   return BG_OK;
@@ -580,8 +635,9 @@ int gmres_solve(bg_matrix *A, const bg_precond *P, void *dB, int ldb, int nrhs, 
   S.nchunk = (N + GV_COLS - 1) / GV_COLS;
   size_t nv = (size_t)N * (m + 1) * nrhs;
   size_t nH = (size_t)nrhs * (m + 1) * m, ng = (size_t)nrhs * (m + 1), ncs = (size_t)nrhs * m;
+  size_t ndp = (size_t)nrhs * (m + 1) * GM_DSPLIT;
   size_t bytes = sizeof(z2) * (nv + 4 * (size_t)N * nrhs + (size_t)S.nchunk * nrhs * N + 2 * (size_t)(m + 2) * nrhs +
-                               nH + ng + 2 * ncs) +
+                               nH + ng + 2 * ncs + ndp) +
                  sizeof(double) * (8 + ncs);
   char *w = nullptr;
   BG_CUDA_TRY(cudaMallocAsync((void **)&w, bytes, stream()));
@@ -593,8 +649,8 @@ int gmres_solve(bg_matrix *A, const bg_precond *P, void *dB, int ldb, int nrhs, 
   S.part = X + (size_t)N * nrhs;
   S.dots = S.part + (size_t)S.nchunk * nrhs * N;
   S.h = S.dots + (size_t)(m + 2) * nrhs;
-  z2 *Hd = S.h + (size_t)(m + 2) * nrhs, *gd = Hd + nH, *csd = gd + ng, *snd = csd + ncs;
-  S.sc = (double *)(snd + ncs);
+  z2 *Hd = S.h + (size_t)(m + 2) * nrhs, *gd = Hd + nH, *csd = gd + ng, *snd = csd + ncs, *dpart = snd + ncs;
+  S.sc = (double *)(dpart + ndp);
   double *resd = S.sc + 8;
   const size_t vstride = (size_t)N * (m + 1);
   // residual estimates read back to pinned host memory (one buffer per library instance)
@@ -657,16 +713,16 @@ int gmres_solve(bg_matrix *A, const bg_precond *P, void *dB, int ldb, int nrhs, 
       // CGS2: two passes, coefficients summed into column k of H on the device
       prof_start(PROF_ORTHO);
       for (int pass = 0; pass < 2; pass++) {
-        k_gm_dots<<<dim3(k + 1, nrhs), 256, 0, stream()>>>(N, k + 1, S.V, N, vstride, S.W, N, S.dots);
+        k_gm_dots_part<<<dim3(k + 1, nrhs, GM_DSPLIT), 256, 0, stream()>>>(N, k + 1, S.V, N, vstride, S.W, N, dpart);
+        g_launches++;
+        k_gm_hacc<<<nrhs, 256, 0, stream()>>>(k, m, dpart, S.dots, Hd, pass);
         g_launches++;
         k_gm_subtract<<<gr, 256, 0, stream()>>>(N, k + 1, S.V, N, vstride, S.dots, (size_t)(k + 1), S.W, N);
         g_launches++;
-        k_gm_hacc<<<nrhs, 256, 0, stream()>>>(k, m, S.dots, Hd, pass);
-        g_launches++;
       }
-      k_gm_dots<<<dim3(1, nrhs), 256, 0, stream()>>>(N, 1, S.W, N, (size_t)N, S.W, N, S.dots);
+      k_gm_dots_part<<<dim3(1, nrhs, GM_DSPLIT), 256, 0, stream()>>>(N, 1, S.W, N, (size_t)N, S.W, N, dpart);
       g_launches++;
-      k_gm_givens<<<1, 32, 0, stream()>>>(k, m, nrhs, S.dots, Hd, gd, csd, snd, S.sc, resd);
+      k_gm_givens<<<1, 32, 0, stream()>>>(k, m, nrhs, dpart, Hd, gd, csd, snd, S.sc, resd);
       g_launches++;
       prof_stop(PROF_ORTHO, 0.0);
       if (k + 1 <= m) {
