@@ -62,7 +62,7 @@ OMEGA = 1.0
 GMRES = dict(tol=1e-10, restart=50, maxit=1000, inner_tol=1e-5)
 # ncu --set full capture of k_gm_matvec_sym_c64 (one launch, N = 19,872):
 # dram__bytes_read.sum + dram__bytes_write.sum
-MATVEC_NCU_N, MATVEC_NCU_BYTES = 19872, 1.600864e9 + 20.701184e6
+MATVEC_NCU_N, MATVEC_NCU_BYTES = 19872, 1.604407e9 + 38.544896e6
 
 
 def eps_tensor():
