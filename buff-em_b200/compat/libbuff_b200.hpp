@@ -11,6 +11,8 @@
 //   G->AssembleRHSVector(Omega, IF, J);                       // RHSVector.cc:85
 //   M->LUSolve(J);                                            // buff-scatter.cc:314
 //   HMatrix *PFT = G->GetPFTMatrix(J, Omega, IF);             // GetPFT.cc:133
+//   G->GetFields(IF, J, Omega, X, EH);                        // GetFields.cc:387
+//   BNEQ(G).GetFlux(Omega)                                    // buff-neq GetFlux.cc:291
 //
 // Differences from the reference: errors throw buff_b200::Error (carrying the
 // C-ABI status and message) instead of calling ErrExit; the matrix lives on the
@@ -140,6 +142,41 @@ class SWGGeometry {
                  IF ? IF->nHat : nullptr, method, out.data()));
     return out;
   }
+  // all eight EMT columns per object: PAbs, PScat, Fx, Fy, Fz, Tx, Ty, Tz (GetPFT.cc:133-189)
+  std::vector<double> GetPFTMatrixFull(HVector *J, cdouble Omega, const PlaneWave *IF) {
+    std::vector<double> out(8 * (size_t)NumObjects);
+    check(bg_pft_full(g, Omega.real(), Omega.imag(), J->data(), reinterpret_cast<const double *>(IF->E0), IF->nHat,
+                      out.data()));
+    return out;
+  }
+  // SWGGeometry::GetFields(IF, J, Omega, XMatrix, FMatrix) (GetFields.cc:287-382):
+  // X holds npts x 3 coordinates row by row; the result holds npts x 6 values
+  // (Ex, Ey, Ez, Hx, Hy, Hz) row by row.  IF and J may be null, as in the reference.
+  std::vector<cdouble> GetFields(const PlaneWave *IF, HVector *J, cdouble Omega, const std::vector<double> &X) {
+    int npts = (int)(X.size() / 3);
+    std::vector<cdouble> F(6 * (size_t)npts);
+    check(bg_get_fields(g, Omega.real(), Omega.imag(), J ? J->data() : nullptr,
+                        IF ? reinterpret_cast<const double *>(IF->E0) : nullptr, IF ? IF->nHat : nullptr, npts,
+                        X.data(), reinterpret_cast<double *>(F.data())));
+    return F;
+  }
+  // the one-point form (GetFields.cc:387-395)
+  void GetFields(const PlaneWave *IF, HVector *J, cdouble Omega, const double X[3], cdouble EH[6]) {
+    std::vector<cdouble> F = GetFields(IF, J, Omega, std::vector<double>(X, X + 3));
+    for (int i = 0; i < 6; i++) EH[i] = F[i];
+  }
+  // FIBBICache::Store / PreLoad (FIBBICache.cc:272-463) for one object; return
+  // the number of records written / matched
+  int StoreFIBBICache(int obj, const char *path) {
+    int n = 0;
+    check(bg_fibbi_store(g, obj, path, &n));
+    return n;
+  }
+  int PreloadFIBBICache(int obj, const char *path) {
+    int n = 0;
+    check(bg_fibbi_load(g, obj, path, &n));
+    return n;
+  }
 
  private:
   void init() {
@@ -147,6 +184,26 @@ class SWGGeometry {
     TotalBFs = bg_geometry_num_bfs(g);
     for (int i = 0; i <= NumObjects; i++) BFIndexOffset.push_back(bg_geometry_bf_offset(g, i));
   }
+};
+
+// buff-neq's flux chain for one geometry (GetFlux, GetFlux.cc:291-436):
+// GetFlux(Omega)[(s * NO + d) * 8 + q], source s, destination d,
+// q = PAbs, PRad, Fx, Fy, Fz, Tx, Ty, Tz (EMT, uniform temperature per object)
+class BNEQ {
+ public:
+  explicit BNEQ(SWGGeometry &G) : NO(G.NumObjects) { check(bg_neq_create(G.g, &h)); }
+  ~BNEQ() { bg_neq_destroy(h); }
+  BNEQ(const BNEQ &) = delete;
+  BNEQ &operator=(const BNEQ &) = delete;
+  std::vector<double> GetFlux(cdouble Omega) {
+    std::vector<double> out((size_t)NO * NO * 8);
+    check(bg_neq_flux(h, Omega.real(), Omega.imag(), out.data()));
+    return out;
+  }
+
+ private:
+  int NO;
+  bg_neq *h = nullptr;
 };
 
 }  // namespace buff_b200

@@ -1,6 +1,8 @@
 // buff-scatter-style driver on the libbuff-compatible C++ layer
 // (pattern of buff-scatter.cc:236-347 and unit-test-LFField.cc:50-71).
-// usage: scatter_driver <geo.buffgeo> <omega> [geometry-only]
+// usage: scatter_driver <geo.buffgeo> <omega> [geometry-only | extras]
+//   extras: also the full PFT columns, the fields at one point and the
+//   buff-neq flux of the geometry
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -28,6 +30,18 @@ int main(int argc, char **argv) {
     std::vector<double> P = G.GetPFTMatrix(J, Omega, &PW);
     std::printf("J0 %.17g %.17g\n", J->GetEntry(0).real(), J->GetEntry(0).imag());
     std::printf("PAbs %.17g PScat %.17g\n", P[0], P[1]);
+    if (argc > 3 && !std::strcmp(argv[3], "extras")) {
+      std::vector<double> P8 = G.GetPFTMatrixFull(J, Omega, &PW);
+      std::printf("Fz %.17g\n", P8[4]);
+      const double X[3] = {0.3, -0.2, 2.5};
+      cdouble EH[6];
+      G.GetFields(&PW, J, Omega, X, EH);
+      std::printf("Ex %.17g %.17g\n", EH[0].real(), EH[0].imag());
+      std::printf("Hy %.17g %.17g\n", EH[4].real(), EH[4].imag());
+      BNEQ NEQ(G);
+      std::vector<double> F = NEQ.GetFlux(Omega);
+      std::printf("PRad %.17g\n", F[1]);
+    }
     delete M;
     delete J;
   } catch (const Error &e) {

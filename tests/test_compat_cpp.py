@@ -48,3 +48,26 @@ def test_compat_drive_matches_python(driver, sphere, tmp_path):
     M.LUSolve(J)
     assert abs(J[0] - j0) <= 1e-12 * abs(J[0])
     assert abs(G.GetPFTMatrix(J, 1.0, pw)[0, 0] - pabs) <= 1e-10 * abs(pabs)
+
+
+@pytest.mark.gpu
+def test_compat_extras_match_python(driver, sphere, tmp_path):
+    """The C++ layer's full PFT, GetFields and buff-neq flux give the Python
+    binding's numbers (both sit on the same C-ABI)."""
+    g = geo(tmp_path, sphere(3))
+    r = subprocess.run([driver, g, "0.8", "extras"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    vals = dict(line.split(" ", 1) for line in r.stdout.strip().splitlines())
+    G = buffem.SWGGeometry(g)
+    M = G.AssembleVIEMatrix(0.8)
+    M.LUFactorize()
+    pw = buffem.PlaneWave([1, 0, 0], [0, 0, 1])
+    J = G.AssembleRHSVector(0.8, pw)
+    M.LUSolve(J)
+    assert abs(G.GetPFTMatrix(J, 0.8, pw, full=True)[0, 4] - float(vals["Fz"])) <= 1e-10 * abs(float(vals["Fz"]))
+    F = G.GetFields(pw, J, 0.8, np.array([[0.3, -0.2, 2.5]]))[0]
+    ex = complex(*map(float, vals["Ex"].split()))
+    hy = complex(*map(float, vals["Hy"].split()))
+    assert abs(F[0] - ex) <= 1e-10 * abs(ex) and abs(F[4] - hy) <= 1e-10 * abs(hy)
+    prad = buffem.NEQ(G).GetFlux(0.8)[0, 0, 1]
+    assert abs(prad - float(vals["PRad"])) <= 1e-9 * abs(prad)
