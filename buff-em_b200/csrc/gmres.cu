@@ -663,7 +663,6 @@ int gmres_solve(bg_matrix *A, const bg_precond *P, void *dB, int ldb, int nrhs, 
     res_cap = ncs;
   }
   int st = BG_OK;
-  const z2 *B = (const z2 *)dB;
   // X = 0
   BG_CUDA_TRY(cudaMemsetAsync(X, 0, sizeof(z2) * (size_t)N * nrhs, stream()));
   // B contiguous copy in W for norms
@@ -674,7 +673,6 @@ int gmres_solve(bg_matrix *A, const bg_precond *P, void *dB, int ldb, int nrhs, 
   for (auto &v : bn) v = std::max(v, 1e-300);
   int total = 0;
   double relres = 1.0, first = -1;
-  std::vector<int> done(nrhs, 0);
   dim3 gr((N + 255) / 256, nrhs);
   while (!st && total < maxit) {
     // R = B - A X
