@@ -13,7 +13,7 @@ One step = one frequency.
     complex64 copy with FP64 refinement against the complex128 matrix to a
     1e-10 relative residual, LU fallback if 1000 Krylov steps do not reach it.
   fp64_path: assemble, FP64 LU (DMMA tensor cores), FP64 solve -- the plain
-    path and the judge: the learned answer's error is measured against it.
+    path and the reference answer: the learned answer's error is measured against it.
 The same two paths plus the precision form (complex64 tcgen05 LU + FP64
 refinement) also run on the 12^3-cell sphere (N = 19,872) with the
 anisotropic tensor [[4,.5,0],[.5,6,0],[0,0,9]] + 0.1i ("secondary").  The

@@ -204,7 +204,7 @@ def test_committed_weights_beat_jacobi(sphere):
 
 def test_lu_fallback_when_gmres_misses_tolerance(sphere):
     """With a Krylov budget far too small, the solve falls back to the LU path
-    and still meets the tolerance; LU is also the judge of the GMRES answer."""
+    and still meets the tolerance; LU also checks the GMRES answer."""
     G, A, B = setup(sphere(5))
     Ah = A.download()
     Xo = sl.lu_solve(sl.lu_factor(Ah), B)
