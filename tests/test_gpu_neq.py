@@ -90,3 +90,19 @@ def test_neq_full_size_properties(sphere):
     buffem._check(buffem.lib().bg_pft_dr_device(G.h, w, 0.0, C.c_void_p(d.data_ptr()), N, buffem._ptr(out)))
     r = (F[0, 0, 1] - out[1] / 2) / _krueger_prad(eps, w)
     assert 0.75 < r < 1.05, r
+
+
+@pytest.mark.parametrize("kind", ["tensor", "gauss"])
+def test_neq_anisotropic_and_varying_materials(sphere, oracle_lib, kind):
+    """The overlap rows V and Rytov evaluate eps(x) at every quadrature point:
+    an anisotropic constant tensor and a Gaussian bump eps(x) against the
+    oracle (dressed Rytov matrix and flux columns)."""
+    from test_gpu_parity import mats
+    val = [[4, .5, 0], [.5, 6, 0], [0, 0, 9]] if kind == "tensor" else None
+    mb, mo = mats(kind, val, oracle_lib)
+    Gb, Go = pair(sphere(3, jitter=0.05, seed=5), mb, mo, oracle_lib=oracle_lib)
+    w = 0.7
+    neq = buffem.NEQ(Gb)
+    DRg, DRo = neq.DressedRytov(w, 0), Go.dressed_rytov(complex(w), 0)
+    assert np.abs(DRg - DRo).max() <= 1e-9 * np.abs(DRo).max()
+    flux_close(neq.GetFlux(w), Go.neq_flux(complex(w)))
