@@ -325,11 +325,23 @@ __global__ void k_gm_matvec_sum_f(int N, int nchunk, int nrhs, const float2 *par
   int row = blockIdx.x * blockDim.x + threadIdx.x;
   int j = blockIdx.y;
   if (row >= N || j >= nrhs) return;
+  // four chunks per round keep four loads in flight; the sum order is fixed
   double sr = 0, si = 0;
-  for (int k = 0; k < nchunk; k++) {
-    float2 p = partial[((size_t)k * nrhs + j) * N + row];
-    sr += p.x;
-    si += p.y;
+  const size_t stride = (size_t)nrhs * N;
+  const float2 *p = partial + (size_t)j * N + row;
+  int k = 0;
+  for (; k + 4 <= nchunk; k += 4) {
+    float2 a = p[(size_t)k * stride], b = p[(size_t)(k + 1) * stride], c = p[(size_t)(k + 2) * stride],
+           d = p[(size_t)(k + 3) * stride];
+    sr += a.x; si += a.y;
+    sr += b.x; si += b.y;
+    sr += c.x; si += c.y;
+    sr += d.x; si += d.y;
+  }
+  for (; k < nchunk; k++) {
+    float2 a = p[(size_t)k * stride];
+    sr += a.x;
+    si += a.y;
   }
   Y[(size_t)j * ldy + row] = z2{sr, si};
 }

@@ -248,20 +248,35 @@ __global__ void k_gnn_readout(int N, const int *rowptr, const int *col, const fl
 // W[:, q] = K1 V[:, q], (K1)_ij = A_ij / A_jj = r_e dinv_j / dinv_i off the diagonal
 __global__ void k_gnn_k1mv(int N, const int *rowptr, const int *col, const z2g *ratio, const z2g *dinv,
                            const z2g *V, int nv, z2g *W) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
-  z2g ai = zdiv(z2g{1.0, 0.0}, dinv[i]);
-  for (int q = 0; q < nv; q++) {
-    const z2g *v = V + (size_t)q * N;
-    z2g s{0.0, 0.0};
-    for (int e = rowptr[i]; e < rowptr[i + 1]; e++) {
+  // eight lanes per row (its entries are contiguous), all nv <= 4 vectors per
+  // read of the row; lane partial sums combined by a fixed butterfly
+  int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 3, sub = threadIdx.x & 7;
+  z2g s[4] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+  if (i < N) {
+    int e1 = rowptr[i + 1];
+    for (int e = rowptr[i] + sub; e < e1; e += 8) {
       int j = col[e];
       if (j == i) continue;
-      z2g t = zmul(zmul(ratio[e], dinv[j]), v[j]);
-      s.r += t.r;
-      s.i += t.i;
+      z2g rj = zmul(ratio[e], dinv[j]);
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        if (q < nv) {
+          z2g t = zmul(rj, V[(size_t)q * N + j]);
+          s[q].r += t.r;
+          s[q].i += t.i;
+        }
     }
-    W[(size_t)q * N + i] = zmul(ai, s);
+  }
+#pragma unroll
+  for (int o = 4; o > 0; o >>= 1)
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      s[q].r += __shfl_xor_sync(0xffffffffu, s[q].r, o);
+      s[q].i += __shfl_xor_sync(0xffffffffu, s[q].i, o);
+    }
+  if (i < N && sub == 0) {
+    z2g ai = zdiv(z2g{1.0, 0.0}, dinv[i]);
+    for (int q = 0; q < nv; q++) W[(size_t)q * N + i] = zmul(ai, s[q]);
   }
 }
 
@@ -781,7 +796,8 @@ static int bound_coefficient(GnnBufs &B) {
     for (int q = 0; q < nv; q++) f[q] = hn[q] > 0 ? 1.0 / std::sqrt(hn[q]) : 0.0;
     if ((e = cudaMemcpyAsync(fac, f, sizeof(double) * nv, cudaMemcpyHostToDevice, stream())) != cudaSuccess) break;
     k_gnn_scale_cols<<<(nn + 255) / 256, 256, 0, stream()>>>(N, nv, fac, V);
-    k_gnn_k1mv<<<(N + 127) / 128, 128, 0, stream()>>>(N, B.rowptr, B.col, B.ratio, B.dinv, V, nv, W);
+    k_gnn_k1mv<<<(unsigned)(((size_t)N * 8 + 255) / 256), 256, 0, stream()>>>(N, B.rowptr, B.col, B.ratio, B.dinv, V,
+                                                                                nv, W);
     g_launches += 2;
     std::swap(V, W);
   }
