@@ -266,6 +266,25 @@ class Case:
         self.G = None
 
 
+def max_over_ranks(t, world, device="cuda"):
+    """The largest of the ranks' values (all_reduce MAX over the process
+    group; every rank gets it); with one rank, t itself."""
+    if world <= 1:
+        return t
+    import torch
+    import torch.distributed as dist
+    tt = torch.tensor([float(t)], dtype=torch.float64, device=device)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
+def whole_job_seconds_per_frequency(t_max, steps, world):
+    """Replicas: each of the world ranks runs `steps` independent frequencies
+    in t_max seconds (the slowest rank), so the whole job processes
+    steps * world frequencies in that time."""
+    return t_max / (steps * world)
+
+
 def timed(stream, fn, steps, warmup, world):
     """Device seconds of `steps` calls after `warmup` untimed ones (CUDA events
     on the library stream, barrier + synchronize on both sides, max over ranks)."""
@@ -285,12 +304,7 @@ def timed(stream, fn, steps, warmup, world):
     e1.record(stream)
     buffem.synchronize()
     torch.cuda.synchronize()
-    t = e0.elapsed_time(e1) / 1e3
-    if world > 1:
-        tt = torch.tensor([t], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t = float(tt.item())
-    return t
+    return max_over_ranks(e0.elapsed_time(e1) / 1e3, world)
 
 
 def rel_err(x, ref):
@@ -547,11 +561,8 @@ def run_gpu(args, rank, world, local_rank):
         case.step_learned_host(hostB, rhs_h, net, stats)
         times.append(time.perf_counter() - t0)
     e2e_s = sum(times) / len(times) if times else None     # mean over the K steps, as value
-    if world > 1 and e2e_s is not None:
-        import torch.distributed as dist
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    if e2e_s is not None:
+        e2e_s = max_over_ranks(e2e_s, world)
     out.update(N=N, nrhs=case.nrhs, t_learned=t_learned, t_fp64=t_fp64, prof=prof, prof_fp64=prof_fp64,
                launches=launches, clocks=clk, learned=learned, precompute_s=case.precompute_s, e2e_s=e2e_s)
     case.free()
@@ -697,7 +708,7 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     res = run_gpu(args, rank, world, local_rank)
     N = res["N"]
-    value = res["t_learned"] / args.steps / world          # whole-job seconds per frequency
+    value = whole_job_seconds_per_frequency(res["t_learned"], args.steps, world)
     prof = res["prof"]
     mp = measured_peaks()
     hbm = mp.get("hbm_gbs")
@@ -725,12 +736,13 @@ def main():
                                         "16 N^2 for the complex128 residual products)",
                          "share_of_profiled_ms": mv["ms"] / total_ms if total_ms else None,
                          "assemble_far_share_of_profiled_ms": far["ms"] / total_ms if total_ms else None},
-            "e2e": {"value": res["e2e_s"] / world if res["e2e_s"] else None, "unit": "s",
+            "e2e": {"value": whole_job_seconds_per_frequency(res["e2e_s"], 1, world) if res["e2e_s"] else None,
+                    "unit": "s",
                     "h2d_bytes_per_step": 16 * N * res["nrhs"],
                     "d2h_bytes_per_step": 2 * 16 * N * res["nrhs"]},
             "gpu_launches": res["launches"] // max(1, args.steps), "clocks": res["clocks"]}
     if res["t_fp64"] is not None:
-        v64 = res["t_fp64"] / args.fp64_steps / world
+        v64 = whole_job_seconds_per_frequency(res["t_fp64"], args.fp64_steps, world)
         pf = res["prof_fp64"]
         line["fp64_path"] = {"value": v64, "unit": "s", "steps": args.fp64_steps, "warmup": args.fp64_warmup,
                              "speedup_of_learned_form": v64 / value,
