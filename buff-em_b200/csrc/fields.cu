@@ -343,7 +343,7 @@ __global__ void k_fields_finish(const double *__restrict__ part, int nblk, int P
 
 // per-tetrahedron field tables, built on first use
 static int field_tables(bg_geometry *g) {
-  if (g->d_fieldTet) return BG_OK;
+  if (g->d_fieldTet && g->d_fieldFace) return BG_OK;
   std::vector<double> T, F;
   T.reserve(16 * (size_t)g->NT);
   F.reserve(16 * (size_t)g->NT);
@@ -374,10 +374,20 @@ static int field_tables(bg_geometry *g) {
       T.insert(T.end(), {ctr[0], ctr[1], ctr[2], Rall});
     }
   }
-  BG_CUDA_TRY(cudaMalloc(&g->d_fieldTet, sizeof(double) * T.size()));
-  BG_CUDA_TRY(cudaMalloc(&g->d_fieldFace, sizeof(double) * F.size()));
-  BG_CUDA_TRY(cudaMemcpy(g->d_fieldTet, T.data(), sizeof(double) * T.size(), cudaMemcpyHostToDevice));
-  BG_CUDA_TRY(cudaMemcpy(g->d_fieldFace, F.data(), sizeof(double) * F.size(), cudaMemcpyHostToDevice));
+  double *dT = nullptr, *dF = nullptr;
+  cudaError_t e = cudaMalloc(&dT, sizeof(double) * T.size());
+  if (e == cudaSuccess) e = cudaMalloc(&dF, sizeof(double) * F.size());
+  if (e == cudaSuccess) e = cudaMemcpy(dT, T.data(), sizeof(double) * T.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dF, F.data(), sizeof(double) * F.size(), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    // both tables or neither: a failed build leaves the geometry as it was
+    cudaFree(dT);
+    cudaFree(dF);
+    set_error("GetFields tables: %s", cudaGetErrorString(e));
+    return BG_ERR_CUDA;
+  }
+  g->d_fieldTet = dT;
+  g->d_fieldFace = dF;
   return BG_OK;
 }
 
@@ -415,7 +425,12 @@ int get_fields(bg_geometry *g, double wr, double wi, const void *dJ, const doubl
   z *coef = nullptr;
   if (nbx) {
     BG_CUDA_TRY(cudaMallocAsync(&part, sizeof(double) * 12 * (size_t)nbx * npts, stream()));
-    BG_CUDA_TRY(cudaMallocAsync(&coef, sizeof(z) * 4 * (size_t)NT, stream()));
+    cudaError_t e = cudaMallocAsync(&coef, sizeof(z) * 4 * (size_t)NT, stream());
+    if (e != cudaSuccess) {
+      cudaFreeAsync(part, stream());
+      set_error("GetFields scratch: %s", cudaGetErrorString(e));
+      return BG_ERR_CUDA;
+    }
     k_fields_coef<<<(NT + 255) / 256, 256, 0, stream()>>>(g->dev, (const z *)dJ, coef);
     BG_LAUNCHED();
     dim3 grid(ny, nbx);
