@@ -69,6 +69,7 @@ def Material(kind=BG_MAT_CONST_ISO, eps=1.0, tensor=None, eps2=None, center=(0, 
 EXPORTS = [
     "bg_last_error", "bg_geometry_create", "bg_geometry_create_objects", "bg_geometry_destroy",
     "bg_geometry_num_bfs", "bg_geometry_num_objects", "bg_geometry_bf_offset", "bg_geometry_faces",
+    "bg_geometry_vertices",
     "bg_geometry_precompute", "bg_geometry_set_singular_order", "bg_geometry_near_data",
     "bg_matrix_create", "bg_matrix_destroy", "bg_assemble", "bg_matrix_download", "bg_matrix_upload",
     "bg_matrix_device_ptr", "bg_lu_factor", "bg_lu_pivots", "bg_lu_solve", "bg_lu_solve_device",
@@ -102,6 +103,7 @@ def lib():
             getattr(L, f).argtypes = [P]
         L.bg_geometry_bf_offset.argtypes = [P, I]
         L.bg_geometry_faces.argtypes = [P, I, VP]
+        L.bg_geometry_vertices.argtypes = [P, I, VP, VP]
         L.bg_geometry_set_singular_order.argtypes = [P, I]
         L.bg_geometry_near_data.argtypes = [P, C.POINTER(I), VP, VP]
         L.bg_matrix_create.argtypes = [P, I, C.POINTER(P)]
@@ -290,6 +292,15 @@ class SWGGeometry:
         out = np.zeros((n, 9), dtype=np.int32)
         _check(lib().bg_geometry_faces(self.h, obj, _ptr(out)))
         return out
+
+    def vertices(self, obj=0):
+        """(nv, 3) vertex coordinates of object obj after its one-time
+        transformation, and its origin (the torque centre)."""
+        nv = _check(lib().bg_geometry_vertices(self.h, obj, None, None))
+        xyz = np.zeros((nv, 3))
+        origin = np.zeros(3)
+        _check(lib().bg_geometry_vertices(self.h, obj, _ptr(xyz), _ptr(origin)))
+        return xyz, origin
 
     def precompute(self):
         _check(lib().bg_geometry_precompute(self.h))

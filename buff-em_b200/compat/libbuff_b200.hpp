@@ -22,6 +22,7 @@
 
 #include <complex>
 #include <cstring>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -100,10 +101,20 @@ struct PlaneWave {
   }
 };
 
+// The host-side fields of SWGVolume (libbuff.h:127-195) that the path's
+// callers read: vertices after the one-time DISPLACED / ROTATED
+// transformation, the origin about which torques are taken, counts, index.
+struct SWGVolume {
+  int Index = 0, NumVertices = 0, NumInteriorFaces = 0;
+  std::vector<double> Vertices;   // 3 * NumVertices
+  double Origin[3] = {0, 0, 0};
+};
+
 class SWGGeometry {
  public:
   int NumObjects = 0, TotalBFs = 0;
   std::vector<int> BFIndexOffset;
+  std::vector<std::unique_ptr<SWGVolume>> Objects;   // Objects[no]->Vertices as in libbuff
   bg_geometry *g = nullptr;
 
   explicit SWGGeometry(const char *GeoFileName) {
@@ -183,6 +194,15 @@ class SWGGeometry {
     NumObjects = bg_geometry_num_objects(g);
     TotalBFs = bg_geometry_num_bfs(g);
     for (int i = 0; i <= NumObjects; i++) BFIndexOffset.push_back(bg_geometry_bf_offset(g, i));
+    for (int i = 0; i < NumObjects; i++) {
+      std::unique_ptr<SWGVolume> O(new SWGVolume);
+      O->Index = i;
+      O->NumVertices = check(bg_geometry_vertices(g, i, nullptr, nullptr));
+      O->NumInteriorFaces = BFIndexOffset[i + 1] - BFIndexOffset[i];
+      O->Vertices.resize(3 * (size_t)O->NumVertices);
+      check(bg_geometry_vertices(g, i, O->Vertices.data(), O->Origin));
+      Objects.push_back(std::move(O));
+    }
   }
 };
 

@@ -93,9 +93,6 @@ void prof_stop(int cls, double flops) {
   s_recs.push_back(ProfRec{s_open[cls], e, cls, flops});
 }
 
-int parse_buffgeo(const char *path, std::vector<std::string> &meshes, std::vector<double> &disp,
-                  std::vector<bg_material> &mats);
-
 }  // namespace bg
 
 using namespace bg;
@@ -126,9 +123,9 @@ static int check_material(const bg_material &m) {
   return BG_OK;
 }
 
-int bg_geometry_create_objects(int nobj, const char *const *meshfiles, const double *displacements,
-                               const bg_material *materials, bg_geometry **out) {
-  if (!out || nobj <= 0 || !meshfiles || !materials) { set_error("bg_geometry_create_objects: bad arguments"); return BG_ERR_ARG; }
+// xf: 12 doubles per object (one-time transformation, M row-major then D) or null
+static int create_objects(int nobj, const char *const *meshfiles, const double *xf, const bg_material *materials,
+                          bg_geometry **out) {
   *out = nullptr;
   bg_geometry *g = new (std::nothrow) bg_geometry();
   if (!g) { set_error("out of host memory"); return BG_ERR_NOMEM; }
@@ -136,7 +133,7 @@ int bg_geometry_create_objects(int nobj, const char *const *meshfiles, const dou
   for (int i = 0; i < nobj; i++) {
     if (!meshfiles[i]) { delete g; set_error("mesh file %d is NULL", i); return BG_ERR_ARG; }
     int st = check_material(materials[i]);
-    if (!st) st = load_object(g->objs[i], meshfiles[i], displacements ? displacements + 3 * i : nullptr);
+    if (!st) st = load_object(g->objs[i], meshfiles[i], xf ? xf + 12 * i : nullptr);
     if (st) { delete g; return st; }
     g->objs[i].mat = materials[i];
   }
@@ -146,16 +143,34 @@ int bg_geometry_create_objects(int nobj, const char *const *meshfiles, const dou
   return BG_OK;
 }
 
+int bg_geometry_create_objects(int nobj, const char *const *meshfiles, const double *displacements,
+                               const bg_material *materials, bg_geometry **out) {
+  if (!out || nobj <= 0 || !meshfiles || !materials) { set_error("bg_geometry_create_objects: bad arguments"); return BG_ERR_ARG; }
+  if (!displacements) return create_objects(nobj, meshfiles, nullptr, materials, out);
+  std::vector<double> xf(12 * (size_t)nobj, 0.0);
+  for (int i = 0; i < nobj; i++) {
+    double *x = &xf[12 * (size_t)i];
+    x[0] = x[4] = x[8] = 1.0;
+    for (int k = 0; k < 3; k++) x[9 + k] = displacements[3 * i + k];
+  }
+  return create_objects(nobj, meshfiles, xf.data(), materials, out);
+}
+
 int bg_geometry_create(const char *path, bg_geometry **out) {
   if (!path || !out) { set_error("bg_geometry_create: bad arguments"); return BG_ERR_ARG; }
-  std::vector<std::string> meshes;
-  std::vector<double> disp;
-  std::vector<bg_material> mats;
-  int st = parse_buffgeo(path, meshes, disp, mats);
+  *out = nullptr;
+  std::vector<GeoObject> objs;
+  int st = parse_buffgeo(path, objs);
   if (st) return st;
   std::vector<const char *> names;
-  for (auto &s : meshes) names.push_back(s.c_str());
-  return bg_geometry_create_objects((int)meshes.size(), names.data(), disp.data(), mats.data(), out);
+  std::vector<double> xf;
+  std::vector<bg_material> mats;
+  for (auto &o : objs) {
+    names.push_back(o.mesh.c_str());
+    xf.insert(xf.end(), o.xf, o.xf + 12);
+    mats.push_back(o.mat);
+  }
+  return create_objects((int)objs.size(), names.data(), xf.data(), mats.data(), out);
 }
 
 static void dfree(void *p) { if (p) cudaFree(p); }
@@ -180,6 +195,14 @@ int bg_geometry_num_objects(const bg_geometry *g) { return g ? (int)g->objs.size
 int bg_geometry_bf_offset(const bg_geometry *g, int obj) {
   if (!g || obj < 0 || obj > (int)g->objs.size()) { set_error("bad object index"); return BG_ERR_ARG; }
   return g->bfOffset[obj];
+}
+
+int bg_geometry_vertices(const bg_geometry *g, int obj, double *xyz, double *origin) {
+  if (!g || obj < 0 || obj >= (int)g->objs.size()) { set_error("bg_geometry_vertices: bad arguments"); return BG_ERR_ARG; }
+  const Object &o = g->objs[obj];
+  if (xyz) std::memcpy(xyz, o.V.data(), sizeof(double) * o.V.size());
+  if (origin) for (int k = 0; k < 3; k++) origin[k] = o.origin[k];
+  return o.nv;
 }
 
 int bg_geometry_faces(const bg_geometry *g, int obj, int *out) {

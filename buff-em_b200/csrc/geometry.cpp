@@ -24,9 +24,8 @@ static double dist3(const double *a, const double *b) {
 // ReadGMSHFile, ReadGMSHFile.cc:66-261: $Nodes/$Elements (gmsh 2.x) or the
 // legacy $NOD/$ELM format; node ids remapped; vertices closer than 1e-6 are
 // merged onto the lower index (:130-141); only element type 4 (tetrahedron)
-// is kept; the displacement is applied before the merge, as the one-time
-// transformation is (:120-121).
-static int read_gmsh(Object &o, const char *path, const double *disp) {
+// is kept; the one-time transformation is applied before the merge (:124).
+static int read_gmsh(Object &o, const char *path, const double *xf) {
   FILE *f = std::fopen(path, "r");
   if (!f) { set_error("cannot open mesh file %s", path); return BG_ERR_IO; }
   char buf[512];
@@ -50,9 +49,12 @@ static int read_gmsh(Object &o, const char *path, const double *disp) {
     if (id < 0 || id > 2 * nv) return fail("node id out of range");
     map[id] = i;
   }
-  if (disp)
-    for (int i = 0; i < nv; i++)
-      for (int k = 0; k < 3; k++) o.V[3 * i + k] += disp[k];
+  if (xf)
+    for (int i = 0; i < nv; i++) {
+      double *x = &o.V[3 * i], y[3];
+      for (int k = 0; k < 3; k++) y[k] = xf[3 * k] * x[0] + xf[3 * k + 1] * x[1] + xf[3 * k + 2] * x[2] + xf[9 + k];
+      for (int k = 0; k < 3; k++) x[k] = y[k];
+    }
   for (int i = 0; i < nv; i++)
     for (int j = i + 1; j < nv; j++)
       if (dist3(&o.V[3 * i], &o.V[3 * j]) < 1.0e-6)
@@ -181,11 +183,13 @@ static int init_faces(Object &o) {
   return BG_OK;
 }
 
-int load_object(Object &o, const char *meshfile, const double *disp) {
+int load_object(Object &o, const char *meshfile, const double *xf) {
+  static const double eye[12] = {1, 0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0};
+  if (xf && !std::memcmp(xf, eye, sizeof eye)) xf = nullptr;   // untransformed: nodes as read
   o.meshfile = meshfile;
-  int st = read_gmsh(o, meshfile, disp);
+  int st = read_gmsh(o, meshfile, xf);
   if (st) return st;
-  if (disp) for (int k = 0; k < 3; k++) o.origin[k] = disp[k];
+  if (xf) for (int k = 0; k < 3; k++) o.origin[k] = xf[9 + k];
   return init_faces(o);
 }
 
@@ -413,85 +417,260 @@ static bool parse_complex(const char *s, double *re, double *im) {
   char *end;
   double a = std::strtod(s, &end);
   if (end == s) return false;
-  if (*end == 'i' || *end == 'j' || *end == 'I') { *re = 0; *im = a; return true; }
+  if ((*end == 'i' || *end == 'j' || *end == 'I') && end[1] == 0) { *re = 0; *im = a; return true; }
   if (*end == 0) { *re = a; *im = 0; return true; }
   const char *p = end;
   double b = std::strtod(p, &end);
-  if (end == p || (*end != 'i' && *end != 'j' && *end != 'I')) return false;
+  if (end == p || (*end != 'i' && *end != 'j' && *end != 'I') || end[1] != 0) return false;
   *re = a; *im = b;
   return true;
 }
 
-int parse_buffgeo(const char *path, std::vector<std::string> &meshes, std::vector<double> &disp,
-                  std::vector<bg_material> &mats) {
+// ------------------------------------------------ one-time transformations
+// XP = M X + D with xf = (M row-major, D): the GTransformation of SCUFF-EM's
+// libhrutil, which the reference links but does not ship.  A later
+// transformation G is composed after the running one (OTGT->Transform(G),
+// SWGGeometry.cc:111-121): M <- M_G M, D <- M_G D + D_G.
+static void xf_identity(double xf[12]) {
+  for (int k = 0; k < 12; k++) xf[k] = 0.0;
+  xf[0] = xf[4] = xf[8] = 1.0;
+}
+
+static void xf_compose(double xf[12], const double g[12]) {
+  double r[12];
+  for (int i = 0; i < 3; i++) {
+    for (int j = 0; j < 3; j++)
+      r[3 * i + j] = g[3 * i] * xf[j] + g[3 * i + 1] * xf[3 + j] + g[3 * i + 2] * xf[6 + j];
+    r[9 + i] = g[3 * i] * xf[9] + g[3 * i + 1] * xf[10] + g[3 * i + 2] * xf[11] + g[9 + i];
+  }
+  for (int k = 0; k < 12; k++) xf[k] = r[k];
+}
+
+static bool parse_real(const std::string &t, double *v) {
+  if (t.empty()) return false;
+  char *end;
+  *v = std::strtod(t.c_str(), &end);
+  return *end == 0;
+}
+
+static bool keyword_is(const std::string &t, const char *a, const char *b = nullptr) {
+  std::string U = t;
+  for (auto &c : U) c = (char)std::toupper((unsigned char)c);
+  return U == a || (b && U == b);
+}
+
+// Parses tok[0..] as a sequence of "DISPLACED dx dy dz" and
+// "ROTATED theta ABOUT ax ay az" (theta in degrees, right-handed about the
+// axis through the origin; DISP and ROT are accepted as short forms),
+// composing each onto xf in order.  The whole line must be consumed (the
+// reference's "junk at end of line", SWGGeometry.cc:122-126).
+static bool parse_transforms(const std::vector<std::string> &tok, double xf[12], std::string &err) {
+  size_t t = 0;
+  while (t < tok.size()) {
+    double g[12];
+    xf_identity(g);
+    if (keyword_is(tok[t], "DISPLACED", "DISP")) {
+      if (t + 4 > tok.size()) { err = "DISPLACED needs three numbers"; return false; }
+      for (int k = 0; k < 3; k++)
+        if (!parse_real(tok[t + 1 + k], &g[9 + k])) { err = "bad number " + tok[t + 1 + k]; return false; }
+      t += 4;
+    } else if (keyword_is(tok[t], "ROTATED", "ROT")) {
+      double th, a[3];
+      if (t + 6 > tok.size() || !keyword_is(tok[t + 2], "ABOUT")) { err = "ROTATED needs: angle ABOUT ax ay az"; return false; }
+      if (!parse_real(tok[t + 1], &th)) { err = "bad angle " + tok[t + 1]; return false; }
+      for (int k = 0; k < 3; k++)
+        if (!parse_real(tok[t + 3 + k], &a[k])) { err = "bad number " + tok[t + 3 + k]; return false; }
+      double n = std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+      if (!(n > 0)) { err = "rotation axis is zero"; return false; }
+      for (int k = 0; k < 3; k++) a[k] /= n;
+      // Rodrigues: R = cos I + sin [a]x + (1 - cos) a a^T
+      double c = std::cos(th * M_PI / 180.0), sn = std::sin(th * M_PI / 180.0);
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) g[3 * i + j] = (1.0 - c) * a[i] * a[j] + (i == j ? c : 0.0);
+      g[1] -= sn * a[2]; g[2] += sn * a[1];
+      g[3] += sn * a[2]; g[5] -= sn * a[0];
+      g[6] -= sn * a[1]; g[7] += sn * a[0];
+      t += 6;
+    } else {
+      err = t ? "junk at end of line" : "unknown transformation " + tok[t];
+      return false;
+    }
+    xf_compose(xf, g);
+  }
+  return true;
+}
+
+// ------------------------------------------------------------- .buffgeo
+static std::vector<std::string> tokenize(const char *line) {
+  std::vector<std::string> tok;
+  const char *p = line;
+  while (*p) {
+    while (*p && std::isspace((unsigned char)*p)) p++;
+    const char *q = p;
+    while (*q && !std::isspace((unsigned char)*q)) q++;
+    if (q > p) tok.emplace_back(p, q);
+    p = q;
+  }
+  return tok;
+}
+
+static bool readable(const std::string &f) {
+  FILE *t = std::fopen(f.c_str(), "r");
+  if (t) std::fclose(t);
+  return t != nullptr;
+}
+
+// Mesh files named by a relative path are looked up in the directory of the
+// .buffgeo file, then in each directory of BUFF_MESH_PATH (colon-separated,
+// the reference's search path, SWGVolume.cc:101-107), then in each MESHPATH
+// directory of the file (SWGGeometry.cc:276-292, relative ones taken from the
+// .buffgeo file's directory), then in the working directory.
+static std::string find_mesh(const std::string &fn, const std::string &dir, const std::vector<std::string> &meshpath) {
+  if (fn.empty() || fn[0] == '/') return fn;
+  std::vector<std::string> cand{dir + "/" + fn};
+  if (const char *mp = std::getenv("BUFF_MESH_PATH")) {
+    std::string s = mp;
+    size_t a = 0;
+    while (a <= s.size()) {
+      size_t b = s.find(':', a);
+      if (b == std::string::npos) b = s.size();
+      if (b > a) cand.push_back(s.substr(a, b - a) + "/" + fn);
+      a = b + 1;
+    }
+  }
+  for (auto &d : meshpath) cand.push_back(d + "/" + fn);
+  cand.push_back(fn);
+  for (auto &c : cand)
+    if (readable(c)) return c;
+  return cand[0];
+}
+
+// MATERIAL argument: CONST_EPS_<complex> or VACUUM.  Named materials, material
+// database sections and SVTENSOR files need SCUFF-EM's expression evaluator
+// and are rejected; spatially varying permittivities come through
+// bg_geometry_create_objects instead.
+static bool parse_material(const std::string &M, bg_material &m) {
+  std::string U = M;
+  for (auto &c : U) c = (char)std::toupper((unsigned char)c);
+  m = bg_material{};
+  m.kind = BG_MAT_CONST_ISO;
+  if (U.rfind("CONST_EPS_", 0) == 0) return parse_complex(M.c_str() + 10, &m.eps[0], &m.eps[1]);
+  if (U == "VACUUM") { m.eps[0] = 1.0; m.eps[1] = 0.0; return true; }
+  return false;
+}
+
+static int parse_object_lines(const std::vector<std::vector<std::string>> &lines, const std::vector<int> &lineno,
+                              int endline, const char *path, const std::string &dir,
+                              const std::vector<std::string> &meshpath, GeoObject &o) {
+  bool have_mesh = false, have_mat = false;
+  std::string err;
+  for (size_t l = 0; l < lines.size(); l++) {
+    const auto &tok = lines[l];
+    if (keyword_is(tok[0], "MESHFILE")) {
+      if (tok.size() != 2) err = "MESHFILE keyword requires one argument";
+      else { o.mesh = find_mesh(tok[1], dir, meshpath); have_mesh = true; }
+    } else if (keyword_is(tok[0], "MATERIAL", "SVTENSOR")) {
+      if (tok.size() != 2) err = tok[0] + " keyword requires one argument";
+      else if (keyword_is(tok[0], "SVTENSOR")) err = "SVTENSOR files are not supported (CONST_EPS_<value> or VACUUM only)";
+      else if (!parse_material(tok[1], o.mat)) err = "unsupported material " + tok[1] + " (CONST_EPS_<value> or VACUUM only)";
+      else have_mat = true;
+    } else if (keyword_is(tok[0], "DISPLACED") || keyword_is(tok[0], "ROTATED")) {
+      parse_transforms(tok, o.xf, err);
+    } else {
+      err = "syntax error";
+    }
+    if (!err.empty()) { set_error("%s:%d: %s", path, lineno[l], err.c_str()); return BG_ERR_IO; }
+  }
+  if (!have_mesh) { set_error("%s:%d: no MESHFILE specified for object", path, endline); return BG_ERR_IO; }
+  if (!have_mat) { set_error("%s:%d: no MATERIAL or SVTENSOR specified for object", path, endline); return BG_ERR_IO; }
+  return BG_OK;
+}
+
+// A name MESH__<mesh>[__MAT__<material>] stands for a one-object geometry
+// with MESHFILE <mesh>.vmsh (extension of <mesh> dropped) and that material
+// (SWGGeometry.cc:167-209; the reference writes it out as a .buffgeo file,
+// here it is parsed in memory).
+static bool special_name(const char *path, std::vector<std::vector<std::string>> &lines) {
+  std::string s = path;
+  if (s.size() < 7 || s.compare(0, 6, "MESH__")) return false;
+  s = s.substr(6);
+  std::string mat, svt;
+  size_t pm = s.find("__MAT__"), ps = s.find("__SVT__");
+  if (pm != std::string::npos) mat = s.substr(pm + 7, ps != std::string::npos && ps > pm ? ps - pm - 7 : std::string::npos);
+  if (ps != std::string::npos) svt = s.substr(ps + 7, pm != std::string::npos && pm > ps ? pm - ps - 7 : std::string::npos);
+  std::string mesh = s.substr(0, std::min(pm, ps));
+  size_t slash = mesh.find_last_of('/'), dot = mesh.find_last_of('.');
+  if (dot != std::string::npos && (slash == std::string::npos || dot > slash)) mesh = mesh.substr(0, dot);
+  lines.push_back({"MESHFILE", mesh + ".vmsh"});
+  if (pm != std::string::npos) lines.push_back({"MATERIAL", mat});
+  if (ps != std::string::npos) lines.push_back({"SVTENSOR", svt + ".SVTensor"});
+  return true;
+}
+
+int parse_buffgeo(const char *path, std::vector<GeoObject> &objs) {
+  std::vector<std::vector<std::string>> special;
+  if (special_name(path, special)) {
+    GeoObject o;
+    o.label = special[0][1];
+    xf_identity(o.xf);
+    std::vector<int> lineno(special.size(), 0);
+    int st = parse_object_lines(special, lineno, 0, path, ".", {}, o);
+    if (st) return st;
+    objs.push_back(o);
+    return BG_OK;
+  }
   FILE *f = std::fopen(path, "r");
-  if (!f) { set_error("cannot open geometry file %s", path); return BG_ERR_IO; }
+  if (!f) { set_error("could not open %s", path); return BG_ERR_IO; }
   std::string dir = path;
   size_t slash = dir.find_last_of('/');
   dir = (slash == std::string::npos) ? std::string(".") : dir.substr(0, slash);
-  const char *mp = std::getenv("BUFF_MESH_PATH");
-  char line[1024];
+  std::vector<std::string> meshpath;
+  char buf[1024];
+  int lineno = 0, start = 0;
   bool in = false;
-  std::string mesh;
-  double d[3] = {0, 0, 0};
-  bg_material m{};
-  int lineno = 0;
-  while (std::fgets(line, sizeof line, f)) {
+  GeoObject cur;
+  std::vector<std::vector<std::string>> body;
+  std::vector<int> bodyline;
+  auto fail = [&](int ln, const char *msg) {
+    std::fclose(f);
+    set_error("%s:%d: %s", path, ln, msg);
+    return BG_ERR_IO;
+  };
+  while (std::fgets(buf, sizeof buf, f)) {
     lineno++;
-    char *p = line;
-    while (*p && std::isspace((unsigned char)*p)) p++;
-    if (!*p || *p == '#') continue;
-    char kw[64] = {0}, arg[512] = {0};
-    int n = std::sscanf(p, "%63s %511[^\n]", kw, arg);
-    std::string K = kw;
-    for (auto &c : K) c = (char)std::toupper((unsigned char)c);
-    if (K == "OBJECT") {
-      in = true; mesh.clear(); d[0] = d[1] = d[2] = 0; m = bg_material{}; m.kind = BG_MAT_CONST_ISO;
-      m.eps[0] = 1.0;
-    } else if (K == "MESHFILE" && in && n == 2) {
-      char fn[512];
-      std::sscanf(arg, "%511s", fn);
-      std::string cand = fn;
-      if (fn[0] != '/') {
-        cand = dir + "/" + fn;
-        FILE *t = std::fopen(cand.c_str(), "r");
-        if (!t && mp) cand = std::string(mp) + "/" + fn;
-        if (t) std::fclose(t);
-      }
-      mesh = cand;
-    } else if (K == "MATERIAL" && in && n == 2) {
-      char nm[256];
-      std::sscanf(arg, "%255s", nm);
-      std::string M = nm;
-      std::string U = M;
-      for (auto &c : U) c = (char)std::toupper((unsigned char)c);
-      if (U.rfind("CONST_EPS_", 0) == 0) {
-        if (!parse_complex(M.c_str() + 10, &m.eps[0], &m.eps[1])) {
-          std::fclose(f); set_error("%s:%d: bad permittivity %s", path, lineno, nm); return BG_ERR_IO; }
-        m.kind = BG_MAT_CONST_ISO;
-      } else if (U == "VACUUM") {
-        m.kind = BG_MAT_CONST_ISO; m.eps[0] = 1.0; m.eps[1] = 0.0;
+    std::vector<std::string> tok = tokenize(buf);
+    if (tok.empty() || tok[0][0] == '#') continue;
+    if (in) {
+      if (keyword_is(tok[0], "ENDOBJECT")) {
+        int st = parse_object_lines(body, bodyline, lineno, path, dir, meshpath, cur);
+        if (st) { std::fclose(f); return st; }
+        objs.push_back(cur);
+        in = false;
       } else {
-        std::fclose(f); set_error("%s:%d: unsupported material %s (CONST_EPS_<value> only)", path, lineno, nm);
-        return BG_ERR_IO;
+        body.push_back(tok);
+        bodyline.push_back(lineno);
       }
-    } else if (K == "DISPLACED" && in) {
-      if (std::sscanf(arg, "%lf %lf %lf", d, d + 1, d + 2) != 3) {
-        std::fclose(f); set_error("%s:%d: bad DISPLACED", path, lineno); return BG_ERR_IO; }
-    } else if (K == "ENDOBJECT" && in) {
-      if (mesh.empty()) { std::fclose(f); set_error("%s:%d: object without MESHFILE", path, lineno); return BG_ERR_IO; }
-      meshes.push_back(mesh); mats.push_back(m);
-      disp.push_back(d[0]); disp.push_back(d[1]); disp.push_back(d[2]);
-      in = false;
-    } else if (K == "MATERIAL" || K == "MESHFILE") {
-      std::fclose(f); set_error("%s:%d: %s outside OBJECT", path, lineno, kw); return BG_ERR_IO;
+    } else if (keyword_is(tok[0], "OBJECT")) {
+      if (tok.size() != 2) return fail(lineno, "invalid OBJECT specification");
+      cur = GeoObject{};
+      cur.label = tok[1];
+      xf_identity(cur.xf);
+      body.clear();
+      bodyline.clear();
+      in = true;
+      start = lineno;
+    } else if (keyword_is(tok[0], "MESHPATH")) {
+      if (tok.size() != 2) return fail(lineno, "invalid MESHPATH specification");
+      meshpath.push_back(tok[1][0] == '/' ? tok[1] : dir + "/" + tok[1]);
+    } else if (keyword_is(tok[0], "MATERIAL")) {
+      return fail(lineno, "MATERIAL database sections are not supported (use MATERIAL CONST_EPS_<value> inside OBJECT)");
     } else {
-      std::fclose(f); set_error("%s:%d: unsupported keyword %s", path, lineno, kw); return BG_ERR_IO;
+      return fail(lineno, "syntax error");
     }
   }
   std::fclose(f);
-  if (in) { set_error("%s: missing ENDOBJECT", path); return BG_ERR_IO; }
-  if (meshes.empty()) { set_error("%s: no objects", path); return BG_ERR_IO; }
+  if (in) { set_error("%s:%d: OBJECT without ENDOBJECT", path, start); return BG_ERR_IO; }
+  if (objs.empty()) { set_error("%s: no objects", path); return BG_ERR_IO; }
   return BG_OK;
 }
 

@@ -72,8 +72,22 @@ struct Object {
 };
 
 // Reads a gmsh mesh (ReadGMSHFile.cc:66-261) and builds the face list
-// (InitFaceList.cc:69-279).  Returns BG_OK or an error status.
-int load_object(Object &o, const char *meshfile, const double *disp);
+// (InitFaceList.cc:69-279).  xf, when not null, is the object's one-time
+// transformation XP = M X + D as 12 doubles (M row-major, then D), applied to
+// the vertices before the merge and to the origin.  Returns BG_OK or an error
+// status.
+int load_object(Object &o, const char *meshfile, const double *xf);
+
+// One OBJECT ... ENDOBJECT section of a .buffgeo file.
+struct GeoObject {
+  std::string label, mesh;
+  bg_material mat{};
+  double xf[12];
+};
+
+// Parses a .buffgeo file (SWGGeometry.cc:52-158, 214-383) or a special
+// MESH__<mesh>__MAT__<material> name (SWGGeometry.cc:167-209).
+int parse_buffgeo(const char *path, std::vector<GeoObject> &objs);
 
 // ---------------------------------------------------------------- device SoA
 // All indices are global over the objects of a geometry (vertex and tet

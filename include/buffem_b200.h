@@ -70,9 +70,14 @@ const char *bg_last_error(void);
  * ------------------------------------------------------------------------- */
 
 /* SWGGeometry::SWGGeometry(const char *GeoFileName), SWGGeometry.cc:214-383.
-   Parses OBJECT / MESHFILE / MATERIAL CONST_EPS_<value> / DISPLACED /
-   ENDOBJECT sections of a .buffgeo file; meshes are gmsh .msh/.vmsh read with
-   the semantics of ReadGMSHFile.cc:66-261 and numbered by InitFaceList.cc:69-279. */
+   Parses MESHPATH lines and OBJECT <label> ... ENDOBJECT sections holding
+   MESHFILE, MATERIAL (CONST_EPS_<value> or VACUUM) and any number of
+   DISPLACED dx dy dz / ROTATED theta ABOUT ax ay az lines, composed in order
+   and applied to the mesh before its vertex merge (SWGGeometry.cc:52-158);
+   the special name MESH__<mesh>__MAT__<material> stands for a one-object
+   file (SWGGeometry.cc:167-209).  Meshes are gmsh .msh/.vmsh read with the
+   semantics of ReadGMSHFile.cc:66-261 and numbered by InitFaceList.cc:69-279.
+   Errors carry "<file>:<line>: <message>" as the reference's ErrExit does. */
 int bg_geometry_create(const char *buffgeo_path, bg_geometry **out);
 
 /* Same as above from explicit per-object mesh files, displacements
@@ -87,6 +92,14 @@ void bg_geometry_destroy(bg_geometry *g);
 int bg_geometry_num_bfs(const bg_geometry *g);
 int bg_geometry_num_objects(const bg_geometry *g);
 int bg_geometry_bf_offset(const bg_geometry *g, int obj);
+
+/* SWGVolume::Vertices / NumVertices / Origin (libbuff.h:73-195) of object
+   obj: 3 doubles per vertex into xyz (mesh nodes in file order after the
+   one-time transformation; merged duplicates stay in place) and the object's
+   origin, the transformed (0,0,0) about which torques are taken, into
+   origin[3].  Either pointer may be NULL.  Returns the vertex count or a
+   negative status. */
+int bg_geometry_vertices(const bg_geometry *g, int obj, double *xyz, double *origin);
 
 /* Face table of object obj, 9 ints per interior face:
    iV1 iV2 iV3 iQP iQM iPTet iMTet PIndex MIndex (SWGFace, libbuff.h:97-115). */

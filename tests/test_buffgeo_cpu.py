@@ -1,0 +1,171 @@
+""".buffgeo parsing on the host (SWGGeometry.cc:52-383): one-time DISPLACED /
+ROTATED transformations composed in order and applied before the vertex
+merge, MESHPATH and BUFF_MESH_PATH lookup, the MESH__ special names and the
+reference's error cases, checked through bg_geometry_vertices without a GPU."""
+import math
+import shutil
+
+import numpy as np
+import pytest
+
+import buffem
+
+
+def read_nodes(path):
+    lines = open(path).read().splitlines()
+    i = lines.index("$Nodes")
+    n = int(lines[i + 1])
+    return np.array([[float(v) for v in lines[i + 2 + k].split()[1:4]] for k in range(n)])
+
+
+def geo(tmp_path, body, name="g.buffgeo"):
+    p = tmp_path / name
+    p.write_text(body)
+    return str(p)
+
+
+def obj(mesh, *lines, label="A", mat="CONST_EPS_4+0.2i"):
+    inner = "".join(f" {ln}\n" for ln in lines)
+    return f"OBJECT {label}\n MESHFILE {mesh}\n MATERIAL {mat}\n{inner}ENDOBJECT\n"
+
+
+def rot(theta_deg, axis):
+    a = np.asarray(axis, float) / np.linalg.norm(axis)
+    c, s = math.cos(math.radians(theta_deg)), math.sin(math.radians(theta_deg))
+    K = np.array([[0, -a[2], a[1]], [a[2], 0, -a[0]], [-a[1], a[0], 0]])
+    return c * np.eye(3) + s * K + (1 - c) * np.outer(a, a)
+
+
+def test_untransformed_vertices_are_the_file_nodes(buffem_lib, sphere, tmp_path):
+    mesh = sphere(2)
+    G = buffem.SWGGeometry(geo(tmp_path, obj(mesh)))
+    xyz, origin = G.vertices(0)
+    assert np.array_equal(xyz, read_nodes(mesh)) and np.array_equal(origin, np.zeros(3))
+
+
+def test_displacements_compose_exactly(buffem_lib, sphere, tmp_path):
+    mesh = sphere(2)
+    G = buffem.SWGGeometry(geo(tmp_path, obj(mesh, "DISPLACED 0.5 0 1", "DISPLACED 0 -2 0.25")))
+    xyz, origin = G.vertices(0)
+    d = np.array([0.5, 0.0, 1.0]) + np.array([0.0, -2.0, 0.25])
+    assert np.array_equal(xyz, read_nodes(mesh) + d) and np.array_equal(origin, d)
+    # the displacement form of bg_geometry_create_objects gives the same vertices
+    H = buffem.SWGGeometry(meshfiles=mesh, materials=buffem.Material(eps=4 + 0.2j), displacements=[d])
+    assert np.array_equal(H.vertices(0)[0], xyz)
+
+
+def test_rotation_and_order_of_composition(buffem_lib, sphere, tmp_path):
+    mesh = sphere(2)
+    X = read_nodes(mesh)
+    R = rot(90, [0, 0, 1])
+    d = np.array([1.0, 0.0, 0.0])
+    # displaced, then rotated: XP = R (X + d); the origin goes to R d
+    G = buffem.SWGGeometry(geo(tmp_path, obj(mesh, "DISPLACED 1 0 0", "ROTATED 90 ABOUT 0 0 1")))
+    xyz, origin = G.vertices(0)
+    assert np.allclose(xyz, (X + d) @ R.T, atol=1e-14, rtol=0)
+    assert np.allclose(origin, [0, 1, 0], atol=1e-15, rtol=0)
+    # both on one line, in the same order: the same transformation
+    G1 = buffem.SWGGeometry(geo(tmp_path, obj(mesh, "DISPLACED 1 0 0 ROTATED 90 ABOUT 0 0 1"), "one.buffgeo"))
+    assert np.array_equal(G1.vertices(0)[0], xyz)
+    # rotated, then displaced: XP = R X + d
+    G2 = buffem.SWGGeometry(geo(tmp_path, obj(mesh, "ROTATED 90 ABOUT 0 0 2", "DISPLACED 1 0 0"), "two.buffgeo"))
+    xyz2, origin2 = G2.vertices(0)
+    assert np.allclose(xyz2, X @ R.T + d, atol=1e-14, rtol=0) and np.array_equal(origin2, d)
+    # a rigid motion leaves the numbering alone
+    G0 = buffem.SWGGeometry(geo(tmp_path, obj(mesh), "zero.buffgeo"))
+    assert np.array_equal(G.faces(0), G0.faces(0)) and np.array_equal(G2.faces(0), G0.faces(0))
+
+
+def test_general_rotation_is_right_handed_and_rigid(buffem_lib, sphere, tmp_path):
+    mesh = sphere(2)
+    X = read_nodes(mesh)
+    G = buffem.SWGGeometry(geo(tmp_path, obj(mesh, "ROTATED 37.5 ABOUT 1 -2 0.5", "DISPLACED 0.1 0.2 0.3")))
+    xyz, origin = G.vertices(0)
+    R = rot(37.5, [1, -2, 0.5])
+    assert np.allclose(xyz, X @ R.T + [0.1, 0.2, 0.3], atol=1e-14, rtol=0)
+    assert np.allclose(R @ R.T, np.eye(3), atol=1e-15) and np.linalg.det(R) > 0
+    # right-handed: a quarter turn about +z takes +x to +y
+    assert np.allclose(rot(90, [0, 0, 1]) @ [1, 0, 0], [0, 1, 0], atol=1e-15)
+
+
+def test_two_objects_keep_their_own_transformations(buffem_lib, sphere, tmp_path):
+    mesh = sphere(2)
+    X = read_nodes(mesh)
+    G = buffem.SWGGeometry(geo(tmp_path, obj(mesh, "ROTATED 45 ABOUT 0 1 0", label="A")
+                               + obj(mesh, "DISPLACED 0 0 3", label="B", mat="VACUUM")))
+    assert G.NumObjects == 2 and G.BFIndexOffset == [0, 72, 144]
+    assert np.allclose(G.vertices(0)[0], X @ rot(45, [0, 1, 0]).T, atol=1e-14, rtol=0)
+    assert np.array_equal(G.vertices(1)[0], X + [0, 0, 3]) and np.array_equal(G.vertices(1)[1], [0, 0, 3])
+
+
+def test_mesh_lookup(buffem_lib, sphere, tmp_path, monkeypatch):
+    mesh = sphere(2)
+    sub = tmp_path / "meshes"
+    sub.mkdir()
+    shutil.copy(mesh, sub / "ball.vmsh")
+    # MESHPATH relative to the .buffgeo file's directory
+    G = buffem.SWGGeometry(geo(tmp_path, "MESHPATH meshes\n" + obj("ball.vmsh")))
+    assert G.TotalBFs == 72
+    # BUFF_MESH_PATH, colon-separated
+    other = tmp_path / "elsewhere"
+    other.mkdir()
+    monkeypatch.setenv("BUFF_MESH_PATH", f"{tmp_path / 'none'}:{sub}")
+    G = buffem.SWGGeometry(geo(other, obj("ball.vmsh")))
+    assert G.TotalBFs == 72
+    monkeypatch.delenv("BUFF_MESH_PATH")
+    with pytest.raises(buffem.BuffError) as e:
+        buffem.SWGGeometry(geo(other, obj("ball.vmsh"), "n.buffgeo"))
+    assert e.value.status == -2 and "ball.vmsh" in str(e.value)
+
+
+def test_special_mesh_names(buffem_lib, sphere, tmp_path, monkeypatch):
+    shutil.copy(sphere(2), tmp_path / "ball.vmsh")
+    monkeypatch.chdir(tmp_path)
+    G = buffem.SWGGeometry("MESH__ball__MAT__CONST_EPS_4+0.2i")
+    assert G.NumObjects == 1 and G.TotalBFs == 72
+    assert buffem.SWGGeometry("MESH__ball.vmsh__MAT__VACUUM").TotalBFs == 72
+    with pytest.raises(buffem.BuffError) as e:
+        buffem.SWGGeometry("MESH__ball")
+    assert "no MATERIAL" in str(e.value)
+    with pytest.raises(buffem.BuffError) as e:
+        buffem.SWGGeometry("MESH__ball__SVT__eps")
+    assert "SVTENSOR" in str(e.value)
+
+
+@pytest.mark.parametrize("body,line,words", [
+    ("OBJECT A\n MESHFILE m.vmsh\n MATERIAL CONST_EPS_2\n DISPLACED 1 2 3 4\nENDOBJECT\n", 4, "junk at end of line"),
+    ("OBJECT A\n MESHFILE m.vmsh\n MATERIAL CONST_EPS_2\n ROTATED 30 0 0 1\nENDOBJECT\n", 4, "ABOUT"),
+    ("OBJECT A\n MESHFILE m.vmsh\n MATERIAL CONST_EPS_2\n ROTATED 30 ABOUT 0 0 0\nENDOBJECT\n", 4, "axis"),
+    ("OBJECT A\n MESHFILE m.vmsh\n MATERIAL CONST_EPS_2\n DISPLACED 1 x 3\nENDOBJECT\n", 4, "bad number"),
+    ("OBJECT A\n MESHFILE m.vmsh\nENDOBJECT\n", 3, "no MATERIAL"),
+    ("OBJECT A\n MATERIAL CONST_EPS_2\nENDOBJECT\n", 3, "no MESHFILE"),
+    ("OBJECT A\n MESHFILE m.vmsh\n SVTENSOR eps.SVTensor\nENDOBJECT\n", 3, "SVTENSOR"),
+    ("OBJECT A\n MESHFILE m.vmsh\n MATERIAL CONST_EPS_4+0.2ix\nENDOBJECT\n", 3, "unsupported material"),
+    ("OBJECT A\n MESHFILE m.vmsh a\n MATERIAL CONST_EPS_2\nENDOBJECT\n", 2, "one argument"),
+    ("OBJECT A\n MESHFILE m.vmsh\n MATERIAL CONST_EPS_2\n LABEL x\nENDOBJECT\n", 4, "syntax error"),
+    ("OBJECT A\n MESHFILE m.vmsh\n MATERIAL CONST_EPS_2\n ROT 9 ABOUT 0 0 1\nENDOBJECT\n", 4, "syntax error"),
+    ("# comment\n\nOBJECT\n MESHFILE m.vmsh\nENDOBJECT\n", 3, "invalid OBJECT"),
+    ("MATERIAL Gold\n Eps(w) = 1\nENDMATERIAL\n", 1, "MATERIAL database"),
+    ("MESHPATH\n", 1, "invalid MESHPATH"),
+    ("ENDOBJECT\n", 1, "syntax error"),
+    ("OBJECT A\n MESHFILE m.vmsh\n MATERIAL CONST_EPS_2\n", 1, "without ENDOBJECT"),
+])
+def test_reference_error_cases(buffem_lib, tmp_path, body, line, words):
+    path = geo(tmp_path, body)
+    with pytest.raises(buffem.BuffError) as e:
+        buffem.SWGGeometry(path)
+    assert e.value.status == -2
+    msg = str(e.value)
+    assert f"{path}:{line}:" in msg and words in msg, msg
+
+
+def test_empty_file_and_bad_vertex_queries(buffem_lib, sphere, tmp_path):
+    with pytest.raises(buffem.BuffError) as e:
+        buffem.SWGGeometry(geo(tmp_path, "# nothing\n"))
+    assert "no objects" in str(e.value)
+    G = buffem.SWGGeometry(geo(tmp_path, obj(sphere(2)), "ok.buffgeo"))
+    L = buffem.lib()
+    assert L.bg_geometry_vertices(G.h, 1, None, None) == buffem.BG_ERR_ARG
+    assert L.bg_geometry_vertices(G.h, -1, None, None) == buffem.BG_ERR_ARG
+    assert L.bg_geometry_vertices(None, 0, None, None) == buffem.BG_ERR_ARG
+    assert L.bg_geometry_vertices(G.h, 0, None, None) == len(read_nodes(sphere(2)))

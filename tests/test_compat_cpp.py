@@ -32,6 +32,24 @@ def test_compat_geometry(driver, sphere, tmp_path):
     assert "bfs 72" in r.stdout
 
 
+def test_compat_objects_carry_transformed_vertices(driver, sphere, tmp_path):
+    """Objects[no]->Vertices / Origin after ROTATED and DISPLACED lines, as the
+    Python binding reads them."""
+    mesh = sphere(2)
+    p = tmp_path / "t.buffgeo"
+    p.write_text(f"OBJECT A\n MESHFILE {mesh}\n MATERIAL VACUUM\nENDOBJECT\n"
+                 f"OBJECT B\n MESHFILE {mesh}\n MATERIAL CONST_EPS_3\n DISPLACED 0 0 3\n"
+                 f" ROTATED 30 ABOUT 1 0 0\nENDOBJECT\n")
+    r = subprocess.run([driver, str(p), "1.0", "geometry-only"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    last = [ln for ln in r.stdout.splitlines() if ln.startswith("last ")][0].split()[1:]
+    xyz, origin = buffem.SWGGeometry(str(p)).vertices(1)
+    assert int(last[0]) == len(xyz) and int(last[1]) == 72
+    assert np.array_equal(np.array(last[2:5], float), origin)
+    assert np.array_equal(np.array(last[5:8], float), xyz[0])
+    assert np.allclose(origin, [0, -3 * np.sin(np.pi / 6), 3 * np.cos(np.pi / 6)], atol=1e-15)
+
+
 @pytest.mark.gpu
 def test_compat_drive_matches_python(driver, sphere, tmp_path):
     g = geo(tmp_path, sphere(3))
