@@ -628,6 +628,85 @@ static int simplex_rule(int k, int n, const double *gx, const double *gw, double
   return np;
 }
 
+/* Per-pair data of the singular rule for the adaptive accuracy reference
+   below: vertices relative to A's first vertex, the closed-form moments of
+   the common simplex and the Beta factors (the set-up of sing_static). */
+typedef struct {
+  int c;
+  double VA[4][3], VB[4][3], Q[3], QP[3];
+  double ub[3], W, QQ, uQs, G[3][3], vol;
+} SingPair;
+
+static double tet_volume(const double V[4][3])
+{
+  double a[3], b[3], cc[3];
+  for (int k = 0; k < 3; k++) { a[k] = V[1][k] - V[0][k]; b[k] = V[2][k] - V[0][k]; cc[k] = V[3][k] - V[0][k]; }
+  return fabs(a[0] * (b[1] * cc[2] - b[2] * cc[1]) + a[1] * (b[2] * cc[0] - b[0] * cc[2]) + a[2] * (b[0] * cc[1] - b[1] * cc[0])) / 6.0;
+}
+
+static void sing_pair_init(SingPair *X, int c, const double VA_[4][3], const double VB_[4][3],
+                           const double *Q_, const double *QP_)
+{
+  const double *o = VA_[0];
+  X->c = c;
+  for (int i = 0; i < 4; i++)
+    for (int k = 0; k < 3; k++) { X->VA[i][k] = VA_[i][k] - o[k]; X->VB[i][k] = VB_[i][k] - o[k]; }
+  for (int k = 0; k < 3; k++) { X->Q[k] = Q_[k] - o[k]; X->QP[k] = QP_[k] - o[k]; }
+  int n = c - 1, m = 7 - c;
+  /* common-simplex moments */
+  double s2 = 0, sv[3] = {0, 0, 0};
+  for (int i = 0; i < c; i++)
+    for (int k = 0; k < 3; k++) { sv[k] += X->VA[i][k]; s2 += X->VA[i][k] * X->VA[i][k]; }
+  for (int k = 0; k < 3; k++) X->ub[k] = sv[k] / (n + 1);
+  X->W = (s2 + sv[0] * sv[0] + sv[1] * sv[1] + sv[2] * sv[2]) / ((n + 1.0) * (n + 2.0));
+  X->QQ = X->Q[0] * X->QP[0] + X->Q[1] * X->QP[1] + X->Q[2] * X->QP[2];
+  X->uQs = X->ub[0] * (X->Q[0] + X->QP[0]) + X->ub[1] * (X->Q[1] + X->QP[1]) + X->ub[2] * (X->Q[2] + X->QP[2]);
+  /* Beta factors G[p+1][j] = (a+j)!/(a+j+n+1)!, a = m-1+p */
+  for (int p = -1; p <= 1; p++)
+    for (int j = 0; j < 3; j++) {
+      int a = m - 1 + p;
+      X->G[p + 1][j] = fact(a + j) / fact(a + j + n + 1);
+    }
+  /* 36 |V_A| |V_B| converts the barycentric measure to volume measure */
+  X->vol = 36.0 * tet_volume(X->VA) * tet_volume(X->VB);
+}
+
+/* One angular point of face S (sign pattern of the common components):
+   barycentrics al (A side, ns + own) and be (B side), weight w; adds the six
+   radially integrated values to acc (the inner loop of sing_static, which is
+   kept as it is so that its floating-point results do not move). */
+static inline void sing_face_point(const SingPair *X, int S, const double *al, const double *be, double w,
+                                   double acc[6])
+{
+  int c = X->c;
+  double A1[3] = {0, 0, 0}, B1[3] = {0, 0, 0};
+  int ja = 0, jb = 0;
+  for (int k = 0; k < c; k++) {
+    if (S & (1 << k)) { double z = al[ja++]; for (int x = 0; x < 3; x++) A1[x] += z * X->VA[k][x]; }
+    else              { double z = be[jb++]; for (int x = 0; x < 3; x++) B1[x] += z * X->VA[k][x]; }
+  }
+  for (int k = c; k < 4; k++) {
+    double za = al[ja++], zb = be[jb++];
+    for (int x = 0; x < 3; x++) { A1[x] += za * X->VA[k][x]; B1[x] += zb * X->VB[k][x]; }
+  }
+  const double *ub = X->ub, *Q = X->Q, *QP = X->QP;
+  double L0 = A1[0] - B1[0], L1 = A1[1] - B1[1], L2 = A1[2] - B1[2];
+  double R = sqrt(L0 * L0 + L1 * L1 + L2 * L2);
+  double AB = A1[0] * B1[0] + A1[1] * B1[1] + A1[2] * B1[2];
+  double AQp = A1[0] * QP[0] + A1[1] * QP[1] + A1[2] * QP[2];
+  double BQ = B1[0] * Q[0] + B1[1] * Q[1] + B1[2] * Q[2];
+  double uAB = ub[0] * (A1[0] + B1[0]) + ub[1] * (A1[1] + B1[1]) + ub[2] * (A1[2] + B1[2]);
+  double c0 = X->QQ - X->uQs + X->W;
+  double c1 = -(AQp + BQ) + uAB + X->uQs - 2.0 * X->W;
+  double c2 = AB - uAB + X->W;
+  double Rp[3] = {1.0 / R, 1.0, R};
+  for (int pk = 0; pk < 3; pk++) {
+    double dot = c0 * X->G[pk][0] + c1 * X->G[pk][1] + c2 * X->G[pk][2];
+    acc[2 * pk] += w * Rp[pk] * dot;
+    acc[2 * pk + 1] += w * Rp[pk] * X->G[pk][0];
+  }
+}
+
 /* out[6] = { int (x-Q).(x'-Q') r^-1, int r^-1, ...r^0..., ...r^1... } over the
    true volumes of tets A (vertices VA[4][3]) and B (VB[4][3]) whose first c
    vertices coincide. */
@@ -720,6 +799,133 @@ static void sing_static(int c, const double VA_[4][3], const double VB_[4][3],
     vb = fabs(a[0] * (b[1] * cc[2] - b[2] * cc[1]) + a[1] * (b[2] * cc[0] - b[0] * cc[2]) + a[2] * (b[0] * cc[1] - b[1] * cc[0])) / 6.0;
   }
   for (int i = 0; i < 6; i++) out[i] = 36.0 * va * vb * acc[i];
+}
+
+/* ------------------------------------------------------------------------- */
+/* Accuracy reference for the singular rule (tests only; neither the fixed    */
+/* rule above nor the GPU library uses it).  Each face of the polytope is the */
+/* unit cube [0,1]^k of collapsed coordinates (k = p-1 + q-1).  A box is       */
+/* integrated with an ng^k Gauss-Legendre product rule and compared with the  */
+/* sum over its 2^k half-size children; if the two differ by more than        */
+/* tol x scale in any of the six values, each child is treated the same way  */
+/* (to depth maxdepth), otherwise the children's sum is kept.  scale is the   */
+/* magnitude of the pair's integral of each kernel (for the (x-Q).(x'-Q')     */
+/* values times the squared diameter of tet A), from a first fixed pass.      */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+  const SingPair *X;
+  int S, ka, kb, ng, maxdepth;
+  double gx[16], gw[16], tol, scale[6];
+  long evals;
+} SingAdapt;
+
+/* collapsed map of u[0..k-1] onto the k+1 barycentrics of Delta_k; returns
+   the Jacobian (1-u0)^{k-1} (1-u1)^{k-2} ... */
+static double collapse_simplex(int k, const double *u, double *b)
+{
+  double rest = 1.0, J = 1.0;
+  for (int i = 0; i < k; i++) {
+    b[i] = rest * u[i];
+    rest *= 1.0 - u[i];
+    if (i < k - 1) J *= rest;
+  }
+  b[k] = rest;
+  return J;
+}
+
+static void sing_box(SingAdapt *A, const double *lo, const double *hi, double out[6])
+{
+  int k = A->ka + A->kb, tot = 1;
+  for (int d = 0; d < k; d++) tot *= A->ng;
+  for (int i = 0; i < 6; i++) out[i] = 0.0;
+  for (int t = 0; t < tot; t++) {
+    double u[6], al[4], be[4], w = 1.0;
+    int r = t;
+    for (int d = 0; d < k; d++) {
+      int i = r % A->ng;
+      r /= A->ng;
+      u[d] = lo[d] + (hi[d] - lo[d]) * A->gx[i];
+      w *= (hi[d] - lo[d]) * A->gw[i];
+    }
+    w *= collapse_simplex(A->ka, u, al) * collapse_simplex(A->kb, u + A->ka, be);
+    sing_face_point(A->X, A->S, al, be, w, out);
+  }
+  A->evals += tot;
+}
+
+static void sing_refine(SingAdapt *A, const double *lo, const double *hi, const double parent[6], int depth,
+                        double out[6])
+{
+  int k = A->ka + A->kb, nc = 1 << k;
+  double clo[16][4], chi[16][4], ch[16][6], sum[6] = {0, 0, 0, 0, 0, 0};
+  for (int j = 0; j < nc; j++) {
+    for (int d = 0; d < k; d++) {
+      double mid = 0.5 * (lo[d] + hi[d]);
+      clo[j][d] = (j >> d & 1) ? mid : lo[d];
+      chi[j][d] = (j >> d & 1) ? hi[d] : mid;
+    }
+    sing_box(A, clo[j], chi[j], ch[j]);
+    for (int i = 0; i < 6; i++) sum[i] += ch[j][i];
+  }
+  double err = 0.0;
+  for (int i = 0; i < 6; i++) err = fmax(err, fabs(sum[i] - parent[i]) / A->scale[i]);
+  if (err <= A->tol || depth >= A->maxdepth) {
+    for (int i = 0; i < 6; i++) out[i] = sum[i];
+    return;
+  }
+  for (int i = 0; i < 6; i++) out[i] = 0.0;
+  for (int j = 0; j < nc; j++) {
+    double o[6];
+    sing_refine(A, clo[j], chi[j], ch[j], depth + 1, o);
+    for (int i = 0; i < 6; i++) out[i] += o[i];
+  }
+}
+
+/* public: the six values of sing_static to a tolerance; returns the number
+   of angular points evaluated */
+long or_sing_static_adaptive(int c, const double *VA, const double *VB, const double *Q, const double *QP,
+                             int ng, double tol, int maxdepth, double *out)
+{
+  SingPair X;
+  sing_pair_init(&X, c, (const double (*)[3])VA, (const double (*)[3])VB, Q, QP);
+  SingAdapt A;
+  A.X = &X;
+  A.ng = ng < 2 ? 2 : ng > 16 ? 16 : ng;
+  A.tol = tol;
+  A.maxdepth = maxdepth;
+  A.evals = 0;
+  gauss_legendre01(A.ng, A.gx, A.gw);
+  int nown = 4 - c;
+  double lo[4] = {0, 0, 0, 0}, hi[4] = {1, 1, 1, 1}, face[16][6], tot[6] = {0, 0, 0, 0, 0, 0};
+  for (int S = 0; S < (1 << c); S++) {
+    int ns = __builtin_popcount(S);
+    if (c == 4 && (ns == 0 || ns == 4)) continue;
+    A.S = S; A.ka = ns + nown - 1; A.kb = c - ns + nown - 1;
+    sing_box(&A, lo, hi, face[S]);
+    for (int i = 0; i < 6; i++) tot[i] += face[S][i];
+  }
+  double h2 = 0.0;
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 4; j++) {
+      double s = 0.0;
+      for (int x = 0; x < 3; x++) s += (X.VA[i][x] - X.VA[j][x]) * (X.VA[i][x] - X.VA[j][x]);
+      h2 = fmax(h2, s);
+    }
+  for (int pk = 0; pk < 3; pk++) {
+    A.scale[2 * pk] = fabs(tot[2 * pk + 1]) * h2;
+    A.scale[2 * pk + 1] = fabs(tot[2 * pk + 1]);
+  }
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (int S = 0; S < (1 << c); S++) {
+    int ns = __builtin_popcount(S);
+    if (c == 4 && (ns == 0 || ns == 4)) continue;
+    A.S = S; A.ka = ns + nown - 1; A.kb = c - ns + nown - 1;
+    double o[6];
+    sing_refine(&A, lo, hi, face[S], 0, o);
+    for (int i = 0; i < 6; i++) acc[i] += o[i];
+  }
+  for (int i = 0; i < 6; i++) out[i] = X.vol * acc[i];
+  return A.evals;
 }
 
 /* public wrapper for tests: tets given by 4 vertices each (common first) */

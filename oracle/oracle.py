@@ -72,6 +72,8 @@ def lib():
         L.or_geom_faces.argtypes = [P, I, ip]
         L.or_geom_destroy.argtypes = [P]
         L.or_sing_static.argtypes = [I, dp, dp, dp, dp, I, dp]
+        L.or_sing_static_adaptive.argtypes = [I, dp, dp, dp, dp, I, D, I, dp]
+        L.or_sing_static_adaptive.restype = C.c_long
         L.or_fibbi.argtypes = [P, I, I, dp]
         L.or_gme.argtypes = [P, I, I, D, D, dp]
         L.or_overlaps.argtypes = [P, I, D, ip, dp]
@@ -299,3 +301,15 @@ def sing_static(c, VA, VB, Q, QP, nang=8):
                          np.ascontiguousarray(Q, dtype=np.float64),
                          np.ascontiguousarray(QP, dtype=np.float64), nang, out)
     return out
+
+
+def sing_static_adaptive(c, VA, VB, Q, QP, ng=6, tol=1e-10, maxdepth=10):
+    """The six values of sing_static by adaptive bisection of the angular
+    cubes (an accuracy reference for the fixed rule); returns (values,
+    angular points evaluated)."""
+    out = np.zeros(6)
+    n = lib().or_sing_static_adaptive(c, np.ascontiguousarray(VA, dtype=np.float64).reshape(-1),
+                                      np.ascontiguousarray(VB, dtype=np.float64).reshape(-1),
+                                      np.ascontiguousarray(Q, dtype=np.float64),
+                                      np.ascontiguousarray(QP, dtype=np.float64), ng, tol, maxdepth, out)
+    return out, n

@@ -4,7 +4,8 @@ The reference ships no golden vectors and cannot be built here (it needs the
 non-vendored SCUFF-EM libraries), so the oracle is pinned against:
   * the closed-form SWG Gram overlaps of SWGVolume.cc:405-481 (GetOverlapElements);
   * exact polynomial integrals and an independent reduction of the unit-cube
-    Coulomb integral for the singular tetrahedron-pair rule;
+    Coulomb integral for the singular tetrahedron-pair rule, and an adaptive
+    accuracy reference that measures the fixed rule on the reference's mesh;
   * the ExpRel series definition (pattern of interactiveTests/tExpRel.cc);
   * the Mie series for a dielectric sphere (examples/MieScattering).
 """
@@ -97,6 +98,86 @@ def test_singular_rule_converged(oracle_lib, c):
     r10 = oracle_lib.sing_static(c, A, B, Q, QP, 10)
     r14 = oracle_lib.sing_static(c, A, B, Q, QP, 14)
     assert np.max(np.abs(r10 - r14) / np.abs(r14).max()) < 1e-9
+
+
+def test_adaptive_singular_rule_unit_cube(oracle_lib):
+    """The adaptive reference reaches the unit-cube Coulomb integral to 1e-12."""
+    tot = 0.0
+    for A in kuhn_cube():
+        for B in kuhn_cube():
+            c, oa, ob = common_first(A, B)
+            tot += oracle_lib.sing_static_adaptive(c, oa, ob, oa[0], ob[0], 6, 1e-13)[0][1]
+    assert abs(tot / cube_coulomb(-1) - 1) < 1e-12
+
+
+def singular_pairs(name):
+    """Tetrahedron pairs of one of the reference's meshes sharing 2-4 vertices,
+    vertices ordered common-first as the rule expects."""
+    import os
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_meshes.npz"))
+    ids, xyz, tets = d[name + "_ids"], d[name + "_xyz"], d[name + "_tets"]
+    row = {int(i): k for k, i in enumerate(ids)}
+    T = [[row[int(v)] for v in t] for t in tets]
+    at = {}
+    for t, vs in enumerate(T):
+        for v in vs:
+            at.setdefault(v, set()).add(t)
+    out = []
+    for t, vs in enumerate(T):
+        for u in sorted(set().union(*(at[v] for v in vs))):
+            com = [v for v in vs if v in T[u]]
+            if u >= t and len(com) >= 2:
+                VA = xyz[com + [v for v in vs if v not in com]]
+                VB = xyz[com + [v for v in T[u] if v not in com]]
+                out.append((len(com), VA, VB))
+    return out
+
+
+def rule_error(oracle_lib, c, VA, VB, ref):
+    """Error of the fixed order-10 rule relative to each kernel's magnitude
+    (the (x-Q).(x'-Q') values scaled by the squared diameter of tet A)."""
+    h2 = max(np.sum((a - b) ** 2) for a in VA for b in VA)
+    scale = np.repeat(np.abs(ref[1::2]), 2) * np.tile([h2, 1.0], 3)
+    fixed = oracle_lib.sing_static(c, VA, VB, VA[-1], VB[-1], 10)
+    return np.max(np.abs(fixed - ref) / scale)
+
+
+def test_fixed_singular_rule_accuracy_on_reference_mesh(oracle_lib):
+    """Order 10 (the GPU library's default) against the adaptive reference on
+    Sphere_533 (src/unitTests): typical pairs are accurate to ~1e-8, the
+    worst pairs (poorly shaped tetrahedra, shape ratio down to 0.036) only to
+    ~1e-3.  The bounds hold the measured figures; tightening the tail is the
+    purpose of the adaptive reference."""
+    pairs = singular_pairs("sphere533")
+    rng = np.random.default_rng(0)
+    by_c = {2: [], 3: [], 4: []}
+    c2 = [p for p in pairs if p[0] == 2]
+    sample = [c2[i] for i in rng.choice(len(c2), 40, replace=False)] + [p for p in pairs if p[0] > 2]
+    for c, VA, VB in sample:
+        ref, _ = oracle_lib.sing_static_adaptive(c, VA, VB, VA[-1], VB[-1], 5, 1e-10)
+        by_c[c].append(rule_error(oracle_lib, c, VA, VB, ref))
+    assert len(by_c[3]) > 500 and len(by_c[4]) > 300
+    for c, errs in by_c.items():
+        errs = np.array(errs)
+        assert np.median(errs) < 1e-7, (c, np.median(errs))
+        assert errs.max() < 1e-2, (c, errs.max())
+    assert np.percentile(by_c[4], 99) > 1e-5   # the documented tail is still there
+
+
+def test_adaptive_reference_is_converged_on_the_worst_pairs(oracle_lib):
+    """Tolerances 1e-10 and 1e-12 agree to 1e-10 on the self pairs of the most
+    poorly shaped tetrahedra of Sphere_533."""
+    pairs = [p for p in singular_pairs("sphere533") if p[0] == 4]
+
+    def shape(V):
+        s = np.linalg.svd(V[1:] - V[0], compute_uv=False)
+        return s[-1] / s[0]
+
+    worst = sorted(pairs, key=lambda p: shape(p[1]))[:5]
+    for c, VA, VB in worst:
+        a, _ = oracle_lib.sing_static_adaptive(c, VA, VB, VA[-1], VB[-1], 6, 1e-10)
+        b, _ = oracle_lib.sing_static_adaptive(c, VA, VB, VA[-1], VB[-1], 6, 1e-12, 14)
+        assert np.max(np.abs(a - b) / np.abs(b[1::2]).repeat(2)) < 1e-8
 
 
 def test_gram_closed_form(oracle_lib, sphere, ref_mesh):
