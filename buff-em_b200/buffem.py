@@ -69,7 +69,7 @@ def Material(kind=BG_MAT_CONST_ISO, eps=1.0, tensor=None, eps2=None, center=(0, 
 EXPORTS = [
     "bg_last_error", "bg_geometry_create", "bg_geometry_create_objects", "bg_geometry_destroy",
     "bg_geometry_num_bfs", "bg_geometry_num_objects", "bg_geometry_bf_offset", "bg_geometry_faces",
-    "bg_geometry_vertices",
+    "bg_geometry_vertices", "bg_geometry_object_index", "bg_geometry_object_label",
     "bg_geometry_precompute", "bg_geometry_set_singular_order", "bg_geometry_near_data",
     "bg_matrix_create", "bg_matrix_destroy", "bg_assemble", "bg_matrix_download", "bg_matrix_upload",
     "bg_matrix_device_ptr", "bg_lu_factor", "bg_lu_pivots", "bg_lu_solve", "bg_lu_solve_device",
@@ -104,6 +104,8 @@ def lib():
         L.bg_geometry_bf_offset.argtypes = [P, I]
         L.bg_geometry_faces.argtypes = [P, I, VP]
         L.bg_geometry_vertices.argtypes = [P, I, VP, VP]
+        L.bg_geometry_object_index.argtypes = [P, C.c_char_p]
+        L.bg_geometry_object_label.argtypes = [P, I, C.c_char_p, I]
         L.bg_geometry_set_singular_order.argtypes = [P, I]
         L.bg_geometry_near_data.argtypes = [P, C.POINTER(I), VP, VP]
         L.bg_matrix_create.argtypes = [P, I, C.POINTER(P)]
@@ -292,6 +294,18 @@ class SWGGeometry:
         out = np.zeros((n, 9), dtype=np.int32)
         _check(lib().bg_geometry_faces(self.h, obj, _ptr(out)))
         return out
+
+    def GetObjectByLabel(self, label):
+        """Index of the object labelled `label` (ignoring case), or -1
+        (SWGGeometry::GetObjectByLabel, SWGGeometry.cc:405-419)."""
+        st = lib().bg_geometry_object_index(self.h, label.encode())
+        return st if st >= 0 else -1
+
+    def label(self, obj=0):
+        n = _check(lib().bg_geometry_object_label(self.h, obj, None, 0))
+        buf = C.create_string_buffer(n + 1)
+        _check(lib().bg_geometry_object_label(self.h, obj, buf, n + 1))
+        return buf.value.decode()
 
     def vertices(self, obj=0):
         """(nv, 3) vertex coordinates of object obj after its one-time

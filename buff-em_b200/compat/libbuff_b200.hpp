@@ -105,6 +105,7 @@ struct PlaneWave {
 // callers read: vertices after the one-time DISPLACED / ROTATED
 // transformation, the origin about which torques are taken, counts, index.
 struct SWGVolume {
+  std::string Label;
   int Index = 0, NumVertices = 0, NumInteriorFaces = 0;
   std::vector<double> Vertices;   // 3 * NumVertices
   double Origin[3] = {0, 0, 0};
@@ -128,6 +129,16 @@ class SWGGeometry {
   ~SWGGeometry() { bg_geometry_destroy(g); }
   SWGGeometry(const SWGGeometry &) = delete;
   SWGGeometry &operator=(const SWGGeometry &) = delete;
+
+  // SWGGeometry::GetObjectByLabel (SWGGeometry.cc:405-419)
+  SWGVolume *GetObjectByLabel(const char *Label, int *pno = nullptr) {
+    if (pno) *pno = -1;
+    if (!Label) return nullptr;
+    int no = bg_geometry_object_index(g, Label);
+    if (no < 0) return nullptr;
+    if (pno) *pno = no;
+    return Objects[no].get();
+  }
 
   HMatrix *AllocateVIEMatrix(bool PureImagFreq = false) {
     (void)PureImagFreq;
@@ -201,6 +212,9 @@ class SWGGeometry {
       O->NumInteriorFaces = BFIndexOffset[i + 1] - BFIndexOffset[i];
       O->Vertices.resize(3 * (size_t)O->NumVertices);
       check(bg_geometry_vertices(g, i, O->Vertices.data(), O->Origin));
+      std::vector<char> label(check(bg_geometry_object_label(g, i, nullptr, 0)) + 1);
+      check(bg_geometry_object_label(g, i, label.data(), (int)label.size()));
+      O->Label = label.data();
       Objects.push_back(std::move(O));
     }
   }

@@ -2,12 +2,14 @@
 // and error reporting live here; all compute is dispatched to the CUDA
 // kernels.  No exception crosses the ABI; errors are status codes plus a
 // thread-local message.
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <new>
 #include <string>
+#include <strings.h>
 #include <vector>
 
 #include "internal.h"
@@ -123,9 +125,11 @@ static int check_material(const bg_material &m) {
   return BG_OK;
 }
 
-// xf: 12 doubles per object (one-time transformation, M row-major then D) or null
+// xf: 12 doubles per object (one-time transformation, M row-major then D) or
+// null; labels: one per object or null (the mesh file name is the label then,
+// as SWGVolume's constructor does without one)
 static int create_objects(int nobj, const char *const *meshfiles, const double *xf, const bg_material *materials,
-                          bg_geometry **out) {
+                          const std::string *labels, bg_geometry **out) {
   *out = nullptr;
   bg_geometry *g = new (std::nothrow) bg_geometry();
   if (!g) { set_error("out of host memory"); return BG_ERR_NOMEM; }
@@ -136,6 +140,7 @@ static int create_objects(int nobj, const char *const *meshfiles, const double *
     if (!st) st = load_object(g->objs[i], meshfiles[i], xf ? xf + 12 * i : nullptr);
     if (st) { delete g; return st; }
     g->objs[i].mat = materials[i];
+    g->objs[i].label = labels ? labels[i] : std::string(meshfiles[i]);
   }
   int st = finish_geometry(g);
   if (st) { delete g; return st; }
@@ -146,14 +151,14 @@ static int create_objects(int nobj, const char *const *meshfiles, const double *
 int bg_geometry_create_objects(int nobj, const char *const *meshfiles, const double *displacements,
                                const bg_material *materials, bg_geometry **out) {
   if (!out || nobj <= 0 || !meshfiles || !materials) { set_error("bg_geometry_create_objects: bad arguments"); return BG_ERR_ARG; }
-  if (!displacements) return create_objects(nobj, meshfiles, nullptr, materials, out);
+  if (!displacements) return create_objects(nobj, meshfiles, nullptr, materials, nullptr, out);
   std::vector<double> xf(12 * (size_t)nobj, 0.0);
   for (int i = 0; i < nobj; i++) {
     double *x = &xf[12 * (size_t)i];
     x[0] = x[4] = x[8] = 1.0;
     for (int k = 0; k < 3; k++) x[9 + k] = displacements[3 * i + k];
   }
-  return create_objects(nobj, meshfiles, xf.data(), materials, out);
+  return create_objects(nobj, meshfiles, xf.data(), materials, nullptr, out);
 }
 
 int bg_geometry_create(const char *path, bg_geometry **out) {
@@ -165,12 +170,14 @@ int bg_geometry_create(const char *path, bg_geometry **out) {
   std::vector<const char *> names;
   std::vector<double> xf;
   std::vector<bg_material> mats;
+  std::vector<std::string> labels;
   for (auto &o : objs) {
     names.push_back(o.mesh.c_str());
     xf.insert(xf.end(), o.xf, o.xf + 12);
     mats.push_back(o.mat);
+    labels.push_back(o.label);
   }
-  return create_objects((int)objs.size(), names.data(), xf.data(), mats.data(), out);
+  return create_objects((int)objs.size(), names.data(), xf.data(), mats.data(), labels.data(), out);
 }
 
 static void dfree(void *p) { if (p) cudaFree(p); }
@@ -195,6 +202,28 @@ int bg_geometry_num_objects(const bg_geometry *g) { return g ? (int)g->objs.size
 int bg_geometry_bf_offset(const bg_geometry *g, int obj) {
   if (!g || obj < 0 || obj > (int)g->objs.size()) { set_error("bad object index"); return BG_ERR_ARG; }
   return g->bfOffset[obj];
+}
+
+int bg_geometry_object_index(const bg_geometry *g, const char *label) {
+  if (!g || !label) { set_error("bg_geometry_object_index: bad arguments"); return BG_ERR_ARG; }
+  for (size_t i = 0; i < g->objs.size(); i++)
+    if (!strcasecmp(label, g->objs[i].label.c_str())) return (int)i;
+  set_error("no object labelled %s", label);
+  return BG_ERR_ARG;
+}
+
+int bg_geometry_object_label(const bg_geometry *g, int obj, char *buf, int cap) {
+  if (!g || obj < 0 || obj >= (int)g->objs.size() || cap < 0 || (cap > 0 && !buf)) {
+    set_error("bg_geometry_object_label: bad arguments");
+    return BG_ERR_ARG;
+  }
+  const std::string &l = g->objs[obj].label;
+  if (cap > 0) {
+    size_t n = std::min(l.size(), (size_t)cap - 1);
+    std::memcpy(buf, l.data(), n);
+    buf[n] = 0;
+  }
+  return (int)l.size();
 }
 
 int bg_geometry_vertices(const bg_geometry *g, int obj, double *xyz, double *origin) {

@@ -61,7 +61,7 @@ struct Face {
 };
 
 struct Object {
-  std::string meshfile;
+  std::string meshfile, label;
   int nv = 0, nt = 0, nif = 0, ntf = 0;
   std::vector<double> V;       // 3*nv (after displacement)
   std::vector<int> VI, FI;     // 4*nt each

@@ -93,6 +93,17 @@ int bg_geometry_num_bfs(const bg_geometry *g);
 int bg_geometry_num_objects(const bg_geometry *g);
 int bg_geometry_bf_offset(const bg_geometry *g, int obj);
 
+/* SWGGeometry::GetObjectByLabel (SWGGeometry.cc:405-419): index of the first
+   object whose label matches, ignoring case, or BG_ERR_ARG if none does.
+   Labels are the OBJECT names of a .buffgeo file, or the mesh file names
+   given to bg_geometry_create_objects. */
+int bg_geometry_object_index(const bg_geometry *g, const char *label);
+
+/* SWGVolume::Label of object obj into buf (cap bytes, NUL-terminated,
+   truncated to fit; buf may be NULL when cap is 0).  Returns the label's
+   length or a negative status. */
+int bg_geometry_object_label(const bg_geometry *g, int obj, char *buf, int cap);
+
 /* SWGVolume::Vertices / NumVertices / Origin (libbuff.h:73-195) of object
    obj: 3 doubles per vertex into xyz (mesh nodes in file order after the
    one-time transformation; merged duplicates stay in place) and the object's

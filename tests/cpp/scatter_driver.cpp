@@ -17,6 +17,8 @@ int main(int argc, char **argv) {
     SWGGeometry G(argv[1]);
     std::printf("objects %d bfs %d\n", G.NumObjects, G.TotalBFs);
     const SWGVolume *O = G.Objects[G.NumObjects - 1].get();
+    int no = -2;
+    std::printf("label %s %d\n", O->Label.c_str(), G.GetObjectByLabel(O->Label.c_str(), &no) == O ? no : -1);
     std::printf("last %d %d %.17g %.17g %.17g %.17g %.17g %.17g\n", O->NumVertices, O->NumInteriorFaces,
                 O->Origin[0], O->Origin[1], O->Origin[2], O->Vertices[0], O->Vertices[1], O->Vertices[2]);
     if (argc > 3 && !std::strcmp(argv[3], "geometry-only")) return 0;

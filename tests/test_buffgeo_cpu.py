@@ -98,6 +98,25 @@ def test_two_objects_keep_their_own_transformations(buffem_lib, sphere, tmp_path
     assert np.array_equal(G.vertices(1)[0], X + [0, 0, 3]) and np.array_equal(G.vertices(1)[1], [0, 0, 3])
 
 
+def test_object_labels(buffem_lib, sphere, tmp_path):
+    """GetObjectByLabel matches ignoring case, first match wins, -1 if none;
+    objects made from mesh files are labelled by the file name."""
+    mesh = sphere(2)
+    G = buffem.SWGGeometry(geo(tmp_path, obj(mesh, label="Sphere_A") + obj(mesh, "DISPLACED 0 0 3", label="b")
+                               + obj(mesh, "DISPLACED 0 0 6", label="SPHERE_a")))
+    assert [G.label(i) for i in range(3)] == ["Sphere_A", "b", "SPHERE_a"]
+    assert G.GetObjectByLabel("sphere_a") == 0 and G.GetObjectByLabel("B") == 1
+    assert G.GetObjectByLabel("c") == -1
+    H = buffem.SWGGeometry(meshfiles=mesh, materials=buffem.Material(eps=2.0))
+    assert H.label(0) == mesh and H.GetObjectByLabel(mesh.upper()) == 0
+    L = buffem.lib()
+    buf = buffem.C.create_string_buffer(4)
+    assert L.bg_geometry_object_label(G.h, 0, buf, 4) == 8 and buf.value == b"Sph"
+    assert L.bg_geometry_object_label(G.h, 3, None, 0) == buffem.BG_ERR_ARG
+    assert L.bg_geometry_object_label(G.h, 0, None, 4) == buffem.BG_ERR_ARG
+    assert L.bg_geometry_object_index(G.h, None) == buffem.BG_ERR_ARG
+
+
 def test_mesh_lookup(buffem_lib, sphere, tmp_path, monkeypatch):
     mesh = sphere(2)
     sub = tmp_path / "meshes"

@@ -42,6 +42,7 @@ def test_compat_objects_carry_transformed_vertices(driver, sphere, tmp_path):
                  f" ROTATED 30 ABOUT 1 0 0\nENDOBJECT\n")
     r = subprocess.run([driver, str(p), "1.0", "geometry-only"], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+    assert "label B 1" in r.stdout
     last = [ln for ln in r.stdout.splitlines() if ln.startswith("last ")][0].split()[1:]
     xyz, origin = buffem.SWGGeometry(str(p)).vertices(1)
     assert int(last[0]) == len(xyz) and int(last[1]) == 72
