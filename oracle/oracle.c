@@ -30,9 +30,13 @@
  * relative-coordinate polar rule (see `sing_static` below) that integrates the
  * radial and shared-simplex variables exactly and the remaining angular
  * variables by collapsed Gauss-Legendre product rules.  The GPU library uses
- * the same rule, so GPU-vs-oracle parity is tight; the deviation of both from
- * the original binary is bounded by the reference's own 1e-6 Taylor-Duffy
- * tolerance.
+ * the same rule, so GPU-vs-oracle parity is tight.  Its own accuracy is
+ * measured against `or_sing_static_adaptive` (an adaptive accuracy
+ * reference): on typical pairs it is far below the reference's 1e-6
+ * Taylor-Duffy tolerance, on pairs of poorly shaped tetrahedra it is not
+ * (up to ~4e-3 at order 10).  `or_sing_static_refined` is the refined rule
+ * meant to close that gap (orders n and n + 2, level-by-level refinement
+ * where they disagree).
  *
  * Parity status: the reference cannot be built here (it needs the non-vendored
  * SCUFF-EM libraries), and it ships no golden vectors, so this oracle is
@@ -924,6 +928,115 @@ long or_sing_static_adaptive(int c, const double *VA, const double *VB, const do
     sing_refine(&A, lo, hi, face[S], 0, o);
     for (int i = 0; i < 6; i++) acc[i] += o[i];
   }
+  for (int i = 0; i < 6; i++) out[i] = X.vol * acc[i];
+  return A.evals;
+}
+
+
+/* ------------------------------------------------------------------------- */
+/* Refined singular rule, shaped for one CTA per tetrahedron pair: the product*/
+/* rules of orders n and n + 2; where they agree to flag_tol x scale the      */
+/* order n + 2 value is kept.  Otherwise every face cube is refined level by  */
+/* level: each open box is halved along each of its dimensions in turn (ng^k  */
+/* points per half), the split that changes the box value most is taken, and  */
+/* the box closes when that change is within tol x scale (the two halves are  */
+/* kept) or stays open as two boxes for the next level.  At most SR_MAXBOX    */
+/* boxes are open per level and SR_MAXLEVEL levels are run; a box that cannot */
+/* be opened for lack of room, or is still open after the last level, keeps  */
+/* its halves and sets bit 0 / bit 1 of *status.                              */
+/* ------------------------------------------------------------------------- */
+#define SR_MAXBOX 2048
+#define SR_MAXLEVEL 40
+typedef struct { int S; double lo[4], hi[4], val[6]; } SingBox;
+
+long or_sing_static_refined(int c, const double *VA, const double *VB, const double *Q, const double *QP, int n,
+                            int ng, double flag_tol, double tol, double *out, int *status)
+{
+  double f0[6], f1[6];
+  *status = 0;
+  sing_static(c, (const double (*)[3])VA, (const double (*)[3])VB, Q, QP, n, f0);
+  sing_static(c, (const double (*)[3])VA, (const double (*)[3])VB, Q, QP, n + 2, f1);
+  SingPair X;
+  sing_pair_init(&X, c, (const double (*)[3])VA, (const double (*)[3])VB, Q, QP);
+  double h2 = 0.0;
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 4; j++) {
+      double s = 0.0;
+      for (int x = 0; x < 3; x++) s += (X.VA[i][x] - X.VA[j][x]) * (X.VA[i][x] - X.VA[j][x]);
+      h2 = fmax(h2, s);
+    }
+  /* scales in the barycentric measure (f / X.vol) */
+  double scale[6];
+  for (int pk = 0; pk < 3; pk++) {
+    scale[2 * pk] = fabs(f1[2 * pk + 1]) / X.vol * h2;
+    scale[2 * pk + 1] = fabs(f1[2 * pk + 1]) / X.vol;
+  }
+  double flag = 0.0;
+  for (int i = 0; i < 6; i++) flag = fmax(flag, fabs(f1[i] - f0[i]) / X.vol / scale[i]);
+  if (flag <= flag_tol) {
+    for (int i = 0; i < 6; i++) out[i] = f1[i];
+    return 0;
+  }
+  SingAdapt A;
+  A.X = &X;
+  A.ng = ng;
+  A.evals = 0;
+  gauss_legendre01(ng, A.gx, A.gw);
+  SingBox *cur = malloc(sizeof(SingBox) * SR_MAXBOX), *nxt = malloc(sizeof(SingBox) * SR_MAXBOX);
+  int ncur = 0, nown = 4 - c;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (int S = 0; S < (1 << c); S++) {
+    int ns = __builtin_popcount(S);
+    if (c == 4 && (ns == 0 || ns == 4)) continue;
+    SingBox *b = &cur[ncur++];
+    b->S = S;
+    for (int d = 0; d < 4; d++) { b->lo[d] = 0.0; b->hi[d] = 1.0; }
+    A.S = S; A.ka = ns + nown - 1; A.kb = c - ns + nown - 1;
+    sing_box(&A, b->lo, b->hi, b->val);
+  }
+  for (int level = 0; level < SR_MAXLEVEL && ncur > 0; level++) {
+    int nn = 0;
+    for (int bi = 0; bi < ncur; bi++) {
+      SingBox *b = &cur[bi];
+      int ns = __builtin_popcount(b->S);
+      A.S = b->S; A.ka = ns + nown - 1; A.kb = c - ns + nown - 1;
+      int k = A.ka + A.kb;
+      double best = -1.0, half[2][6], hl[2][4], hh[2][4];
+      for (int d = 0; d < k; d++) {
+        double l0[4], h0[4], l1[4], h1[4], v0[6], v1[6];
+        memcpy(l0, b->lo, sizeof l0); memcpy(h0, b->hi, sizeof h0);
+        memcpy(l1, b->lo, sizeof l1); memcpy(h1, b->hi, sizeof h1);
+        h0[d] = l1[d] = 0.5 * (b->lo[d] + b->hi[d]);
+        sing_box(&A, l0, h0, v0);
+        sing_box(&A, l1, h1, v1);
+        double e = 0.0;
+        for (int i = 0; i < 6; i++) e = fmax(e, fabs(v0[i] + v1[i] - b->val[i]) / scale[i]);
+        if (e > best) {
+          best = e;
+          memcpy(half[0], v0, sizeof v0); memcpy(half[1], v1, sizeof v1);
+          memcpy(hl[0], l0, sizeof l0); memcpy(hh[0], h0, sizeof h0);
+          memcpy(hl[1], l1, sizeof l1); memcpy(hh[1], h1, sizeof h1);
+        }
+      }
+      int open = best > tol;
+      if (open && nn + 2 > SR_MAXBOX) { open = 0; *status |= 1; }
+      if (open && level == SR_MAXLEVEL - 1) { open = 0; *status |= 2; }
+      if (!open) {
+        for (int i = 0; i < 6; i++) acc[i] += half[0][i] + half[1][i];
+        continue;
+      }
+      for (int h = 0; h < 2; h++) {
+        SingBox *q = &nxt[nn++];
+        q->S = b->S;
+        memcpy(q->lo, hl[h], sizeof q->lo); memcpy(q->hi, hh[h], sizeof q->hi);
+        memcpy(q->val, half[h], sizeof q->val);
+      }
+    }
+    SingBox *t = cur; cur = nxt; nxt = t;
+    ncur = nn;
+  }
+  free(cur);
+  free(nxt);
   for (int i = 0; i < 6; i++) out[i] = X.vol * acc[i];
   return A.evals;
 }

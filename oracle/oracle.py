@@ -74,6 +74,8 @@ def lib():
         L.or_sing_static.argtypes = [I, dp, dp, dp, dp, I, dp]
         L.or_sing_static_adaptive.argtypes = [I, dp, dp, dp, dp, I, D, I, dp]
         L.or_sing_static_adaptive.restype = C.c_long
+        L.or_sing_static_refined.argtypes = [I, dp, dp, dp, dp, I, I, D, D, dp, C.POINTER(I)]
+        L.or_sing_static_refined.restype = C.c_long
         L.or_fibbi.argtypes = [P, I, I, dp]
         L.or_gme.argtypes = [P, I, I, D, D, dp]
         L.or_overlaps.argtypes = [P, I, D, ip, dp]
@@ -313,3 +315,16 @@ def sing_static_adaptive(c, VA, VB, Q, QP, ng=6, tol=1e-10, maxdepth=10):
                                       np.ascontiguousarray(Q, dtype=np.float64),
                                       np.ascontiguousarray(QP, dtype=np.float64), ng, tol, maxdepth, out)
     return out, n
+
+
+def sing_static_refined(c, VA, VB, Q, QP, n=10, ng=6, flag_tol=1e-7, tol=1e-10):
+    """Orders n and n + 2, refined where they disagree (the level-by-level
+    scheme); returns (values, angular points of the refinement, status)."""
+    out = np.zeros(6)
+    st = C.c_int()
+    ne = lib().or_sing_static_refined(c, np.ascontiguousarray(VA, dtype=np.float64).reshape(-1),
+                                      np.ascontiguousarray(VB, dtype=np.float64).reshape(-1),
+                                      np.ascontiguousarray(Q, dtype=np.float64),
+                                      np.ascontiguousarray(QP, dtype=np.float64), n, ng, flag_tol, tol, out,
+                                      C.byref(st))
+    return out, ne, st.value

@@ -142,26 +142,33 @@ def rule_error(oracle_lib, c, VA, VB, ref):
     return np.max(np.abs(fixed - ref) / scale)
 
 
-def test_fixed_singular_rule_accuracy_on_reference_mesh(oracle_lib):
-    """Order 10 (the GPU library's default) against the adaptive reference on
-    Sphere_533 (src/unitTests): typical pairs are accurate to ~1e-8, the
-    worst pairs (poorly shaped tetrahedra, shape ratio down to 0.036) only to
-    ~1e-3.  The bounds hold the measured figures; tightening the tail is the
-    purpose of the adaptive reference."""
+def test_singular_rules_accuracy_on_reference_mesh(oracle_lib):
+    """Against the adaptive reference on Sphere_533 (src/unitTests): order 10
+    (the GPU library's default) is accurate to ~1e-8 on typical pairs but
+    only to ~1e-3 on the worst (poorly shaped tetrahedra, shape ratio down to
+    0.036); the refined rule (orders 10 and 12, level-by-level refinement
+    where they differ by more than 1e-7) bounds every pair by 3e-7, below the
+    reference's Taylor-Duffy tolerance of 1e-6."""
     pairs = singular_pairs("sphere533")
     rng = np.random.default_rng(0)
     by_c = {2: [], 3: [], 4: []}
+    refined = []
     c2 = [p for p in pairs if p[0] == 2]
     sample = [c2[i] for i in rng.choice(len(c2), 40, replace=False)] + [p for p in pairs if p[0] > 2]
     for c, VA, VB in sample:
         ref, _ = oracle_lib.sing_static_adaptive(c, VA, VB, VA[-1], VB[-1], 5, 1e-10)
         by_c[c].append(rule_error(oracle_lib, c, VA, VB, ref))
+        val, _, status = oracle_lib.sing_static_refined(c, VA, VB, VA[-1], VB[-1], 10, 6, 1e-7, 1e-9)
+        assert status == 0
+        h2 = max(np.sum((a - b) ** 2) for a in VA for b in VA)
+        refined.append(np.max(np.abs(val - ref) / (np.repeat(np.abs(ref[1::2]), 2) * np.tile([h2, 1.0], 3))))
     assert len(by_c[3]) > 500 and len(by_c[4]) > 300
     for c, errs in by_c.items():
         errs = np.array(errs)
         assert np.median(errs) < 1e-7, (c, np.median(errs))
         assert errs.max() < 1e-2, (c, errs.max())
-    assert np.percentile(by_c[4], 99) > 1e-5   # the documented tail is still there
+    assert np.percentile(by_c[4], 99) > 1e-5   # the tail of the fixed rule
+    assert max(refined) < 3e-7, max(refined)
 
 
 def test_adaptive_reference_is_converged_on_the_worst_pairs(oracle_lib):
