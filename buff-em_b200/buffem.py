@@ -69,7 +69,7 @@ def Material(kind=BG_MAT_CONST_ISO, eps=1.0, tensor=None, eps2=None, center=(0, 
 EXPORTS = [
     "bg_last_error", "bg_geometry_create", "bg_geometry_create_objects", "bg_geometry_destroy",
     "bg_geometry_num_bfs", "bg_geometry_num_objects", "bg_geometry_bf_offset", "bg_geometry_faces",
-    "bg_geometry_vertices", "bg_geometry_object_index", "bg_geometry_object_label",
+    "bg_geometry_vertices", "bg_geometry_object_index", "bg_geometry_object_label", "bg_geometry_material_eps",
     "bg_geometry_precompute", "bg_geometry_set_singular_order", "bg_geometry_near_data",
     "bg_matrix_create", "bg_matrix_destroy", "bg_assemble", "bg_matrix_download", "bg_matrix_upload",
     "bg_matrix_device_ptr", "bg_lu_factor", "bg_lu_pivots", "bg_lu_solve", "bg_lu_solve_device",
@@ -106,6 +106,7 @@ def lib():
         L.bg_geometry_vertices.argtypes = [P, I, VP, VP]
         L.bg_geometry_object_index.argtypes = [P, C.c_char_p]
         L.bg_geometry_object_label.argtypes = [P, I, C.c_char_p, I]
+        L.bg_geometry_material_eps.argtypes = [P, I, D, D, VP]
         L.bg_geometry_set_singular_order.argtypes = [P, I]
         L.bg_geometry_near_data.argtypes = [P, C.POINTER(I), VP, VP]
         L.bg_matrix_create.argtypes = [P, I, C.POINTER(P)]
@@ -300,6 +301,14 @@ class SWGGeometry:
         (SWGGeometry::GetObjectByLabel, SWGGeometry.cc:405-419)."""
         st = lib().bg_geometry_object_index(self.h, label.encode())
         return st if st >= 0 else -1
+
+    def material_eps(self, obj, omega):
+        """eps of object obj at Omega (units of 3e14 rad/s): a MATERIAL
+        section's Eps(w) at w = Omega x 3e14 rad/s, or the object's constant."""
+        omega = complex(omega)
+        e = np.zeros(2)
+        _check(lib().bg_geometry_material_eps(self.h, obj, omega.real, omega.imag, _ptr(e)))
+        return complex(e[0], e[1])
 
     def label(self, obj=0):
         n = _check(lib().bg_geometry_object_label(self.h, obj, None, 0))

@@ -129,7 +129,8 @@ static int check_material(const bg_material &m) {
 // null; labels: one per object or null (the mesh file name is the label then,
 // as SWGVolume's constructor does without one)
 static int create_objects(int nobj, const char *const *meshfiles, const double *xf, const bg_material *materials,
-                          const std::string *labels, bg_geometry **out) {
+                          const std::string *labels, const std::shared_ptr<const MatPropFn> *matprops,
+                          bg_geometry **out) {
   *out = nullptr;
   bg_geometry *g = new (std::nothrow) bg_geometry();
   if (!g) { set_error("out of host memory"); return BG_ERR_NOMEM; }
@@ -141,6 +142,10 @@ static int create_objects(int nobj, const char *const *meshfiles, const double *
     if (st) { delete g; return st; }
     g->objs[i].mat = materials[i];
     g->objs[i].label = labels ? labels[i] : std::string(meshfiles[i]);
+    if (matprops && matprops[i]) {
+      g->objs[i].matprop = matprops[i];
+      g->dispersive = true;
+    }
   }
   int st = finish_geometry(g);
   if (st) { delete g; return st; }
@@ -151,14 +156,14 @@ static int create_objects(int nobj, const char *const *meshfiles, const double *
 int bg_geometry_create_objects(int nobj, const char *const *meshfiles, const double *displacements,
                                const bg_material *materials, bg_geometry **out) {
   if (!out || nobj <= 0 || !meshfiles || !materials) { set_error("bg_geometry_create_objects: bad arguments"); return BG_ERR_ARG; }
-  if (!displacements) return create_objects(nobj, meshfiles, nullptr, materials, nullptr, out);
+  if (!displacements) return create_objects(nobj, meshfiles, nullptr, materials, nullptr, nullptr, out);
   std::vector<double> xf(12 * (size_t)nobj, 0.0);
   for (int i = 0; i < nobj; i++) {
     double *x = &xf[12 * (size_t)i];
     x[0] = x[4] = x[8] = 1.0;
     for (int k = 0; k < 3; k++) x[9 + k] = displacements[3 * i + k];
   }
-  return create_objects(nobj, meshfiles, xf.data(), materials, nullptr, out);
+  return create_objects(nobj, meshfiles, xf.data(), materials, nullptr, nullptr, out);
 }
 
 int bg_geometry_create(const char *path, bg_geometry **out) {
@@ -171,13 +176,15 @@ int bg_geometry_create(const char *path, bg_geometry **out) {
   std::vector<double> xf;
   std::vector<bg_material> mats;
   std::vector<std::string> labels;
+  std::vector<std::shared_ptr<const MatPropFn>> matprops;
   for (auto &o : objs) {
     names.push_back(o.mesh.c_str());
     xf.insert(xf.end(), o.xf, o.xf + 12);
     mats.push_back(o.mat);
     labels.push_back(o.label);
+    matprops.push_back(o.matprop);
   }
-  return create_objects((int)objs.size(), names.data(), xf.data(), mats.data(), labels.data(), out);
+  return create_objects((int)objs.size(), names.data(), xf.data(), mats.data(), labels.data(), matprops.data(), out);
 }
 
 static void dfree(void *p) { if (p) cudaFree(p); }
@@ -202,6 +209,18 @@ int bg_geometry_num_objects(const bg_geometry *g) { return g ? (int)g->objs.size
 int bg_geometry_bf_offset(const bg_geometry *g, int obj) {
   if (!g || obj < 0 || obj > (int)g->objs.size()) { set_error("bad object index"); return BG_ERR_ARG; }
   return g->bfOffset[obj];
+}
+
+int bg_geometry_material_eps(const bg_geometry *g, int obj, double omega_re, double omega_im, double *eps) {
+  if (!g || !eps || obj < 0 || obj >= (int)g->objs.size()) {
+    set_error("bg_geometry_material_eps: bad arguments");
+    return BG_ERR_ARG;
+  }
+  const Object &o = g->objs[obj];
+  if (o.matprop) { matprop_eps(*o.matprop, omega_re, omega_im, eps); return 1; }
+  if (o.mat.kind == BG_MAT_CONST_ISO) { eps[0] = o.mat.eps[0]; eps[1] = o.mat.eps[1]; return 0; }
+  set_error("bg_geometry_material_eps: object %d has a tensor or position-dependent permittivity", obj);
+  return BG_ERR_ARG;
 }
 
 int bg_geometry_object_index(const bg_geometry *g, const char *label) {

@@ -304,6 +304,10 @@ int bg_batch_sweep(bg_geometry *const *geoms, int ngeom, const double *omega, in
       set_error("bg_batch_sweep: at most %d objects per geometry", BATCH_MAXOBJ);
       return BG_ERR_ARG;
     }
+    if (geoms[i]->dispersive) {
+      set_error("bg_batch_sweep: geometry %d has a frequency-dependent MATERIAL; sweep it with bg_assemble", i);
+      return BG_ERR_ARG;
+    }
   }
   for (int j = 0; j < nomega; j++)
     if (omega[2 * j] == 0.0 && omega[2 * j + 1] == 0.0) { set_error("bg_batch_sweep: omega must be nonzero"); return BG_ERR_ARG; }

@@ -193,6 +193,24 @@ int load_object(Object &o, const char *meshfile, const double *xf) {
   return init_faces(o);
 }
 
+int refresh_materials(bg_geometry *g, double wr, double wi) {
+  if (!g->dispersive) return BG_OK;
+  std::vector<bg_material> mats(g->objs.size());
+  for (size_t i = 0; i < g->objs.size(); i++) {
+    Object &o = g->objs[i];
+    if (o.matprop) {
+      o.mat = bg_material{};
+      o.mat.kind = BG_MAT_CONST_ISO;
+      matprop_eps(*o.matprop, wr, wi, o.mat.eps);
+    }
+    mats[i] = o.mat;
+  }
+  if (g->dev.mats)   // pageable source: the call returns once the bytes are staged
+    BG_CUDA_TRY(cudaMemcpyAsync(g->dev.mats, mats.data(), sizeof(bg_material) * mats.size(), cudaMemcpyHostToDevice,
+                                stream()));
+  return BG_OK;
+}
+
 // ------------------------------------------------------------- device upload
 template <class T>
 static int dupload(T **dst, const std::vector<T> &src) {
@@ -453,9 +471,14 @@ static bool parse_real(const std::string &t, double *v) {
   return *end == 0;
 }
 
+static std::string upper_case(std::string s) {
+  for (auto &c : s) c = (char)std::toupper((unsigned char)c);
+  return s;
+}
+
+// t equals a (or b), ignoring the case of t; a and b are upper case
 static bool keyword_is(const std::string &t, const char *a, const char *b = nullptr) {
-  std::string U = t;
-  for (auto &c : U) c = (char)std::toupper((unsigned char)c);
+  std::string U = upper_case(t);
   return U == a || (b && U == b);
 }
 
@@ -545,10 +568,10 @@ static std::string find_mesh(const std::string &fn, const std::string &dir, cons
   return cand[0];
 }
 
-// MATERIAL argument: CONST_EPS_<complex> or VACUUM.  Named materials, material
-// database sections and SVTENSOR files need SCUFF-EM's expression evaluator
-// and are rejected; spatially varying permittivities come through
-// bg_geometry_create_objects instead.
+// MATERIAL argument: CONST_EPS_<complex> or VACUUM; other names refer to
+// MATERIAL ... ENDMATERIAL sections of the file (matprop.cpp).  SVTENSOR files
+// (eps as expressions of position) are rejected; spatially varying
+// permittivities come through bg_geometry_create_objects instead.
 static bool parse_material(const std::string &M, bg_material &m) {
   std::string U = M;
   for (auto &c : U) c = (char)std::toupper((unsigned char)c);
@@ -559,9 +582,11 @@ static bool parse_material(const std::string &M, bg_material &m) {
   return false;
 }
 
+typedef std::vector<std::pair<std::string, std::shared_ptr<const MatPropFn>>> MatDB;
+
 static int parse_object_lines(const std::vector<std::vector<std::string>> &lines, const std::vector<int> &lineno,
                               int endline, const char *path, const std::string &dir,
-                              const std::vector<std::string> &meshpath, GeoObject &o) {
+                              const std::vector<std::string> &meshpath, const MatDB &db, GeoObject &o) {
   bool have_mesh = false, have_mat = false;
   std::string err;
   for (size_t l = 0; l < lines.size(); l++) {
@@ -571,9 +596,24 @@ static int parse_object_lines(const std::vector<std::vector<std::string>> &lines
       else { o.mesh = find_mesh(tok[1], dir, meshpath); have_mesh = true; }
     } else if (keyword_is(tok[0], "MATERIAL", "SVTENSOR")) {
       if (tok.size() != 2) err = tok[0] + " keyword requires one argument";
-      else if (keyword_is(tok[0], "SVTENSOR")) err = "SVTENSOR files are not supported (CONST_EPS_<value> or VACUUM only)";
-      else if (!parse_material(tok[1], o.mat)) err = "unsupported material " + tok[1] + " (CONST_EPS_<value> or VACUUM only)";
-      else have_mat = true;
+      else if (keyword_is(tok[0], "SVTENSOR")) err = "SVTENSOR files are not supported";
+      else if (parse_material(tok[1], o.mat)) { o.matprop.reset(); have_mat = true; }
+      else if (keyword_is(tok[1].substr(0, std::min<size_t>(10, tok[1].size())), "CONST_EPS_"))
+        err = "bad permittivity " + tok[1];
+      else {
+        // the latest MATERIAL section of that name, ignoring case (as the
+        // MatProp database is searched)
+        for (size_t k = db.size(); k-- > 0 && !have_mat;)
+          if (keyword_is(tok[1], upper_case(db[k].first).c_str())) {
+            o.matprop = db[k].second;
+            o.mat = bg_material{};
+            o.mat.kind = BG_MAT_CONST_ISO;
+            matprop_eps(*o.matprop, 1.0, 0.0, o.mat.eps);   // replaced by eps(Omega) before every use
+            have_mat = true;
+          }
+        if (!have_mat)
+          err = "unknown material " + tok[1] + " (CONST_EPS_<value>, VACUUM or a MATERIAL section above)";
+      }
     } else if (keyword_is(tok[0], "DISPLACED") || keyword_is(tok[0], "ROTATED")) {
       parse_transforms(tok, o.xf, err);
     } else {
@@ -614,7 +654,7 @@ int parse_buffgeo(const char *path, std::vector<GeoObject> &objs) {
     o.label = special[0][1];
     xf_identity(o.xf);
     std::vector<int> lineno(special.size(), 0);
-    int st = parse_object_lines(special, lineno, 0, path, ".", {}, o);
+    int st = parse_object_lines(special, lineno, 0, path, ".", {}, MatDB{}, o);
     if (st) return st;
     objs.push_back(o);
     return BG_OK;
@@ -631,6 +671,11 @@ int parse_buffgeo(const char *path, std::vector<GeoObject> &objs) {
   GeoObject cur;
   std::vector<std::vector<std::string>> body;
   std::vector<int> bodyline;
+  MatDB db;
+  bool inmat = false;
+  std::string matname;
+  std::vector<std::string> matlines;
+  std::vector<int> matlineno;
   auto fail = [&](int ln, const char *msg) {
     std::fclose(f);
     set_error("%s:%d: %s", path, ln, msg);
@@ -640,9 +685,22 @@ int parse_buffgeo(const char *path, std::vector<GeoObject> &objs) {
     lineno++;
     std::vector<std::string> tok = tokenize(buf);
     if (tok.empty() || tok[0][0] == '#') continue;
+    if (inmat) {
+      if (keyword_is(tok[0], "ENDMATERIAL")) {
+        std::shared_ptr<const MatPropFn> fn;
+        int st = matprop_parse_section(matname, matlines, matlineno, path, fn);
+        if (st) { std::fclose(f); return st; }
+        db.emplace_back(matname, fn);
+        inmat = false;
+      } else {
+        matlines.push_back(buf);
+        matlineno.push_back(lineno);
+      }
+      continue;
+    }
     if (in) {
       if (keyword_is(tok[0], "ENDOBJECT")) {
-        int st = parse_object_lines(body, bodyline, lineno, path, dir, meshpath, cur);
+        int st = parse_object_lines(body, bodyline, lineno, path, dir, meshpath, db, cur);
         if (st) { std::fclose(f); return st; }
         objs.push_back(cur);
         in = false;
@@ -663,13 +721,21 @@ int parse_buffgeo(const char *path, std::vector<GeoObject> &objs) {
       if (tok.size() != 2) return fail(lineno, "invalid MESHPATH specification");
       meshpath.push_back(tok[1][0] == '/' ? tok[1] : dir + "/" + tok[1]);
     } else if (keyword_is(tok[0], "MATERIAL")) {
-      return fail(lineno, "MATERIAL database sections are not supported (use MATERIAL CONST_EPS_<value> inside OBJECT)");
+      // SWGGeometry.cc:318-330: one name, then the section up to ENDMATERIAL
+      if (tok.size() == 1) return fail(lineno, "no name given for MATERIAL");
+      if (tok.size() > 2) return fail(lineno, "syntax error");
+      inmat = true;
+      matname = tok[1];
+      matlines.clear();
+      matlineno.clear();
+      start = lineno;
     } else {
       return fail(lineno, "syntax error");
     }
   }
   std::fclose(f);
   if (in) { set_error("%s:%d: OBJECT without ENDOBJECT", path, start); return BG_ERR_IO; }
+  if (inmat) { set_error("%s:%d: MATERIAL without ENDMATERIAL", path, start); return BG_ERR_IO; }
   if (objs.empty()) { set_error("%s: no objects", path); return BG_ERR_IO; }
   return BG_OK;
 }

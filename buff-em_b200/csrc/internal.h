@@ -6,6 +6,7 @@
 
 #include <atomic>
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -60,8 +61,12 @@ struct Face {
   double cen[3], area, radius;
 };
 
+// A MATERIAL ... ENDMATERIAL section: constants and Eps(w) (matprop.cpp).
+struct MatPropFn;
+
 struct Object {
   std::string meshfile, label;
+  std::shared_ptr<const MatPropFn> matprop;   // frequency-dependent eps, or null
   int nv = 0, nt = 0, nif = 0, ntf = 0;
   std::vector<double> V;       // 3*nv (after displacement)
   std::vector<int> VI, FI;     // 4*nt each
@@ -82,8 +87,17 @@ int load_object(Object &o, const char *meshfile, const double *xf);
 struct GeoObject {
   std::string label, mesh;
   bg_material mat{};
+  std::shared_ptr<const MatPropFn> matprop;   // MATERIAL naming a MATERIAL section
   double xf[12];
 };
+
+// MATERIAL <name> ... ENDMATERIAL body lines (with their line numbers) into
+// out; errors name path:line.
+int matprop_parse_section(const std::string &name, const std::vector<std::string> &lines,
+                          const std::vector<int> &lineno, const char *path, std::shared_ptr<const MatPropFn> &out);
+// eps(Omega), Omega in units of 3e14 rad/s, into eps[2] (re, im)
+void matprop_eps(const MatPropFn &m, double omega_re, double omega_im, double eps[2]);
+const std::string &matprop_name(const MatPropFn &m);
 
 // Parses a .buffgeo file (SWGGeometry.cc:52-158, 214-383) or a special
 // MESH__<mesh>__MAT__<material> name (SWGGeometry.cc:167-209).
@@ -150,6 +164,7 @@ struct bg_geometry {
   bg::NearData near;
   int singular_order = 10;
   bool uploaded = false, precomputed = false;
+  bool dispersive = false;      // some object's eps comes from a MATERIAL section
   bg::NearGraph graph;
   double *d_scratch = nullptr;  // general scratch (PFT partial sums etc.)
   double *d_fieldTet = nullptr, *d_fieldFace = nullptr;  // GetFields tables, 16 doubles per tet each
@@ -188,6 +203,10 @@ int precompute_near(bg_geometry *g);
 int assemble_far(bg_geometry *g, double wr, double wi, void *M, size_t ld, const double *fq = nullptr);
 int assemble_near(bg_geometry *g, double wr, double wi, void *M, size_t ld, const double *fq = nullptr);
 int assemble_gram(bg_geometry *g, double wr, double wi, void *M, size_t ld, const double *fq = nullptr);
+// Frequency-dependent materials: eps(Omega) of every object with a MATERIAL
+// section into its host bg_material and, once uploaded, into the device copy
+// (a no-op for geometries without such materials).
+int refresh_materials(bg_geometry *g, double wr, double wi);
 int rhs_planewave(bg_geometry *g, double wr, double wi, const double *E0, const double *nhat, void *out,
                   const double *fq = nullptr);
 int opft_enqueue(bg_geometry *g, double wr, double wi, const void *dJ, const double *fq, double *part,

@@ -801,7 +801,9 @@ __global__ void k_gram(DevGeom g, double w, cd *M, size_t ld, const double *fq) 
 }
 
 int assemble_gram(bg_geometry *g, double wr, double wi, void *M, size_t ld, const double *fq) {
-  (void)wi;
+  if (g->dispersive && fq) { set_error("frequency-dependent materials need a host frequency"); return BG_ERR_ARG; }
+  int st = refresh_materials(g, wr, wi);
+  if (st) return st;
   k_gram<<<(g->N + 127) / 128, 128, 0, stream()>>>(g->dev, wr, (cd *)M, ld, fq);
   BG_LAUNCHED();
   return BG_OK;
@@ -1282,6 +1284,7 @@ int pft(bg_geometry *g, double wr, double wi, const void *dJ, const double *E0, 
   int nrow = (g->N + 127) / 128;
   if (method == BG_PFT_OVERLAP) {
     if ((st = ensure_scratch(g, sizeof(double) * nrow * NO))) return st;
+    if ((st = refresh_materials(g, wr, wi))) return st;
     k_opft<<<nrow, 128, 0, stream()>>>(P, cd{wr, wi}, g->d_scratch, nullptr);
     BG_LAUNCHED();
     std::vector<double> h((size_t)nrow * NO);
@@ -1485,6 +1488,7 @@ __global__ void k_neq_overlaps(DevGeom g, double w, int *idx, double *S, cd *V, 
 int neq_overlaps(bg_geometry *g, double w, int *idx, double *S, void *V, double *R, int *cnt) {
   int st = init_tables();
   if (st) return st;
+  if ((st = refresh_materials(g, w, 0.0))) return st;
   k_neq_overlaps<<<(g->N + 127) / 128, 128, 0, stream()>>>(g->dev, w, idx, S, (cd *)V, R, cnt);
   BG_LAUNCHED();
   return BG_OK;
@@ -1510,6 +1514,7 @@ __global__ void k_opft_reduce(int nrow, int nobj, const double *part, double *ou
 
 int opft_enqueue(bg_geometry *g, double wr, double wi, const void *dJ, const double *fq, double *part,
                  double *out_dev) {
+  if (g->dispersive && fq) { set_error("frequency-dependent materials need a host frequency"); return BG_ERR_ARG; }
   int NO = (int)g->objs.size();
   if (NO > PMAXOBJ) { set_error("PFT supports at most %d objects", PMAXOBJ); return BG_ERR_ARG; }
   PftArgs P{g->dev, (const cd *)dJ, wr, std::sqrt(wr * wr + wi * wi), NO};

@@ -70,8 +70,11 @@ const char *bg_last_error(void);
  * ------------------------------------------------------------------------- */
 
 /* SWGGeometry::SWGGeometry(const char *GeoFileName), SWGGeometry.cc:214-383.
-   Parses MESHPATH lines and OBJECT <label> ... ENDOBJECT sections holding
-   MESHFILE, MATERIAL (CONST_EPS_<value> or VACUUM) and any number of
+   Parses MESHPATH lines, MATERIAL <name> ... ENDMATERIAL sections (complex
+   constants and Eps(w), w in rad/s; used at every frequency the geometry is
+   assembled at, except in bg_batch_sweep) and OBJECT <label> ... ENDOBJECT
+   sections holding MESHFILE, MATERIAL (CONST_EPS_<value>, VACUUM or the name
+   of a MATERIAL section above) and any number of
    DISPLACED dx dy dz / ROTATED theta ABOUT ax ay az lines, composed in order
    and applied to the mesh before its vertex merge (SWGGeometry.cc:52-158);
    the special name MESH__<mesh>__MAT__<material> stands for a one-object
@@ -92,6 +95,14 @@ void bg_geometry_destroy(bg_geometry *g);
 int bg_geometry_num_bfs(const bg_geometry *g);
 int bg_geometry_num_objects(const bg_geometry *g);
 int bg_geometry_bf_offset(const bg_geometry *g, int obj);
+
+/* Permittivity of object obj at Omega (units of 3e14 rad/s) into eps[2]
+   (re, im): a MATERIAL ... ENDMATERIAL section's Eps(w) at w = Omega x 3e14
+   rad/s (SVTensor::Evaluate -> MatProp::GetEps, SVTensor.cc:306-316), or the
+   constant of a CONST_EPS / VACUUM / constant isotropic object.  Returns 1
+   for a frequency-dependent material, 0 for a constant one, or BG_ERR_ARG
+   (tensor and position-dependent permittivities included). */
+int bg_geometry_material_eps(const bg_geometry *g, int obj, double omega_re, double omega_im, double *eps);
 
 /* SWGGeometry::GetObjectByLabel (SWGGeometry.cc:405-419): index of the first
    object whose label matches, ignoring case, or BG_ERR_ARG if none does.

@@ -159,12 +159,12 @@ def test_special_mesh_names(buffem_lib, sphere, tmp_path, monkeypatch):
     ("OBJECT A\n MESHFILE m.vmsh\nENDOBJECT\n", 3, "no MATERIAL"),
     ("OBJECT A\n MATERIAL CONST_EPS_2\nENDOBJECT\n", 3, "no MESHFILE"),
     ("OBJECT A\n MESHFILE m.vmsh\n SVTENSOR eps.SVTensor\nENDOBJECT\n", 3, "SVTENSOR"),
-    ("OBJECT A\n MESHFILE m.vmsh\n MATERIAL CONST_EPS_4+0.2ix\nENDOBJECT\n", 3, "unsupported material"),
+    ("OBJECT A\n MESHFILE m.vmsh\n MATERIAL CONST_EPS_4+0.2ix\nENDOBJECT\n", 3, "bad permittivity"),
+    ("OBJECT A\n MESHFILE m.vmsh\n MATERIAL Gold\nENDOBJECT\n", 3, "unknown material Gold"),
     ("OBJECT A\n MESHFILE m.vmsh a\n MATERIAL CONST_EPS_2\nENDOBJECT\n", 2, "one argument"),
     ("OBJECT A\n MESHFILE m.vmsh\n MATERIAL CONST_EPS_2\n LABEL x\nENDOBJECT\n", 4, "syntax error"),
     ("OBJECT A\n MESHFILE m.vmsh\n MATERIAL CONST_EPS_2\n ROT 9 ABOUT 0 0 1\nENDOBJECT\n", 4, "syntax error"),
     ("# comment\n\nOBJECT\n MESHFILE m.vmsh\nENDOBJECT\n", 3, "invalid OBJECT"),
-    ("MATERIAL Gold\n Eps(w) = 1\nENDMATERIAL\n", 1, "MATERIAL database"),
     ("MESHPATH\n", 1, "invalid MESHPATH"),
     ("ENDOBJECT\n", 1, "syntax error"),
     ("OBJECT A\n MESHFILE m.vmsh\n MATERIAL CONST_EPS_2\n", 1, "without ENDOBJECT"),
@@ -188,3 +188,105 @@ def test_empty_file_and_bad_vertex_queries(buffem_lib, sphere, tmp_path):
     assert L.bg_geometry_vertices(G.h, -1, None, None) == buffem.BG_ERR_ARG
     assert L.bg_geometry_vertices(None, 0, None, None) == buffem.BG_ERR_ARG
     assert L.bg_geometry_vertices(G.h, 0, None, None) == len(read_nodes(sphere(2)))
+
+
+DRUDE = """MATERIAL Metal
+  # Drude model, w in rad/s
+  wp = 1.2e16;   gam = 4.0e13
+  Eps(w) = 1 - wp^2 / (w * (w + i*gam));
+ENDMATERIAL
+"""
+LORENTZ = """material Polar
+  Eps(w) = EpsInf * (w^2 + a1*i*w + a0) / (w^2 + b1*i*w + b0)
+  EpsInf = 6.5
+  a0 = -3.3e28
+  a1 = +8.9e11
+  b0 = -2.2e28; b1 = 8.9e11
+  Mu(w) = 1
+ENDMATERIAL
+"""
+
+
+def drude(w):
+    return 1 - 1.2e16 ** 2 / (w * (w + 1j * 4.0e13))
+
+
+def lorentz(w):
+    return 6.5 * (w * w + 8.9e11j * w - 3.3e28) / (w * w + 8.9e11j * w - 2.2e28)
+
+
+def test_material_sections(buffem_lib, sphere, tmp_path):
+    """MATERIAL ... ENDMATERIAL sections: Eps(w) with w = Omega x 3e14 rad/s,
+    constants in any order before use by Eps(w), semicolons, comments, names
+    matched ignoring case, Mu(w) ignored."""
+    mesh = sphere(2)
+    G = buffem.SWGGeometry(geo(tmp_path, DRUDE + LORENTZ + obj(mesh, label="A", mat="METAL")
+                               + obj(mesh, "DISPLACED 0 0 3", label="B", mat="polar")
+                               + obj(mesh, "DISPLACED 0 0 6", label="C", mat="CONST_EPS_2+0.1i")))
+    for omega in (0.1, 0.7, 1.3, 2.0 + 0.05j, 0.3j):
+        w = complex(omega) * 3e14
+        for obj_, ref in ((0, drude(w)), (1, lorentz(w))):
+            got = G.material_eps(obj_, omega)
+            assert abs(got - ref) <= 1e-13 * abs(ref), (obj_, omega, got, ref)
+        assert G.material_eps(2, omega) == 2 + 0.1j
+    L = buffem.lib()
+    e = np.zeros(2)
+    assert L.bg_geometry_material_eps(G.h, 0, 1.0, 0.0, buffem._ptr(e)) == 1
+    assert L.bg_geometry_material_eps(G.h, 2, 1.0, 0.0, buffem._ptr(e)) == 0
+    assert L.bg_geometry_material_eps(G.h, 3, 1.0, 0.0, buffem._ptr(e)) == buffem.BG_ERR_ARG
+    T = buffem.SWGGeometry(meshfiles=mesh, materials=buffem.Material(kind=buffem.BG_MAT_CONST_TENSOR,
+                                                                     tensor=np.diag([2.0, 3.0, 4.0])))
+    assert L.bg_geometry_material_eps(T.h, 0, 1.0, 0.0, buffem._ptr(e)) == buffem.BG_ERR_ARG
+
+
+@pytest.mark.parametrize("expr,value", [
+    ("-2^2", -4), ("2^3^2", 512), ("(1+2)*3-4/8", 8.5), ("2*-3", -6), ("-(1-3)", 2),
+    ("exp(i*pi)", -1), ("sqrt(-4)", 2j), ("abs(3+4*i)", 5), ("cosh(0) + sinh(0) + tanh(0)", 1),
+    ("log(e) + sin(0) + cos(0) + tan(0) + atan(0) + asin(0) + acos(1)", 2), ("1.5e3 + .5", 1500.5),
+    ("2^-1", 0.5), ("(1+i)^2", 2j), ("4^0.5", 2),
+])
+def test_material_expressions(buffem_lib, sphere, tmp_path, expr, value):
+    G = buffem.SWGGeometry(geo(tmp_path, f"MATERIAL X\n Eps(w) = {expr}\nENDMATERIAL\n" + obj(sphere(2), mat="x")))
+    assert abs(G.material_eps(0, 1.0) - value) < 1e-14 * max(1.0, abs(value))
+
+
+def test_material_constants_chain(buffem_lib, sphere, tmp_path):
+    body = "MATERIAL X\n a = 2; b = a*a + i\n c = b / a\n Eps(w) = c + w/3e14\nENDMATERIAL\n"
+    G = buffem.SWGGeometry(geo(tmp_path, body + obj(sphere(2), mat="X")))
+    assert abs(G.material_eps(0, 0.25) - ((4 + 1j) / 2 + 0.25)) < 1e-15
+
+
+@pytest.mark.parametrize("body,line,words", [
+    ("MATERIAL X\n a = 1\nENDMATERIAL\n", 2, "no Eps(w)"),
+    ("MATERIAL X\n Eps(w) = 1 + q\nENDMATERIAL\n", 2, "unknown name q"),
+    ("MATERIAL X\n a = w\n Eps(w) = a\nENDMATERIAL\n", 2, "w may only appear"),
+    ("MATERIAL X\n Eps(w) = foo(w)\nENDMATERIAL\n", 2, "unknown function foo"),
+    ("MATERIAL X\n Eps(w) = (1 + w\nENDMATERIAL\n", 2, "missing )"),
+    ("MATERIAL X\n Eps(w) = 1 w\nENDMATERIAL\n", 2, "junk after expression"),
+    ("MATERIAL X\n 2a = 1\n Eps(w) = 1\nENDMATERIAL\n", 2, "bad name"),
+    ("MATERIAL X\n Eps(w) 1\nENDMATERIAL\n", 2, "NAME = EXPRESSION"),
+    ("MATERIAL X\n Eps(w) = 1\n", 1, "without ENDMATERIAL"),
+    ("MATERIAL\n", 1, "no name given"),
+    ("MATERIAL X Y\n", 1, "syntax error"),
+    ("OBJECT A\n MESHFILE m.vmsh\n MATERIAL Later\nENDOBJECT\nMATERIAL Later\n Eps(w) = 2\nENDMATERIAL\n", 3,
+     "unknown material Later"),
+])
+def test_material_section_errors(buffem_lib, tmp_path, body, line, words):
+    path = geo(tmp_path, body)
+    with pytest.raises(buffem.BuffError) as e:
+        buffem.SWGGeometry(path)
+    assert e.value.status == -2
+    msg = str(e.value)
+    assert f"{path}:{line}:" in msg and words in msg, msg
+
+
+def test_dispersive_geometry_is_refused_by_batched_sweeps(buffem_lib, sphere, tmp_path):
+    G = buffem.SWGGeometry(geo(tmp_path, DRUDE + obj(sphere(2), mat="Metal")))
+    L = buffem.lib()
+    geoms = (buffem.C.c_void_p * 1)(G.h)
+    w = np.array([1.0, 0.0])
+    E0 = np.array([1.0, 0, 0, 0, 0, 0])
+    nh = np.array([0, 0, 1.0])
+    out = np.zeros(64)
+    st = L.bg_batch_sweep(geoms, 1, buffem._ptr(w), 1, buffem._ptr(E0), buffem._ptr(nh), 1, 0, buffem._ptr(out), None)
+    assert st == buffem.BG_ERR_ARG and "frequency-dependent" in L.bg_last_error().decode()
