@@ -130,6 +130,15 @@ class SWGGeometry {
   SWGGeometry(const SWGGeometry &) = delete;
   SWGGeometry &operator=(const SWGGeometry &) = delete;
 
+  // eps of object no at Omega (SVT->Evaluate for a homogeneous isotropic
+  // object, SVTensor.cc:306-316; MATERIAL sections are evaluated at
+  // w = Omega x 3e14 rad/s)
+  cdouble GetEps(int no, cdouble Omega) const {
+    double e[2];
+    check(bg_geometry_material_eps(g, no, Omega.real(), Omega.imag(), e));
+    return cdouble(e[0], e[1]);
+  }
+
   // SWGGeometry::GetObjectByLabel (SWGGeometry.cc:405-419)
   SWGVolume *GetObjectByLabel(const char *Label, int *pno = nullptr) {
     if (pno) *pno = -1;

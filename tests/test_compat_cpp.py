@@ -37,12 +37,16 @@ def test_compat_objects_carry_transformed_vertices(driver, sphere, tmp_path):
     Python binding reads them."""
     mesh = sphere(2)
     p = tmp_path / "t.buffgeo"
-    p.write_text(f"OBJECT A\n MESHFILE {mesh}\n MATERIAL VACUUM\nENDOBJECT\n"
-                 f"OBJECT B\n MESHFILE {mesh}\n MATERIAL CONST_EPS_3\n DISPLACED 0 0 3\n"
+    p.write_text(f"MATERIAL Drude\n wp = 3e14\n Eps(w) = 1 - wp^2/(w*(w + 1e13*i))\nENDMATERIAL\n"
+                 f"OBJECT A\n MESHFILE {mesh}\n MATERIAL VACUUM\nENDOBJECT\n"
+                 f"OBJECT B\n MESHFILE {mesh}\n MATERIAL drude\n DISPLACED 0 0 3\n"
                  f" ROTATED 30 ABOUT 1 0 0\nENDOBJECT\n")
-    r = subprocess.run([driver, str(p), "1.0", "geometry-only"], capture_output=True, text=True)
+    r = subprocess.run([driver, str(p), "0.5", "geometry-only"], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     assert "label B 1" in r.stdout
+    eps = complex(*map(float, [ln for ln in r.stdout.splitlines() if ln.startswith("eps ")][0].split()[1:]))
+    w = 0.5 * 3e14
+    assert abs(eps - (1 - 9e28 / (w * (w + 1e13j)))) <= 1e-14 * abs(eps)
     last = [ln for ln in r.stdout.splitlines() if ln.startswith("last ")][0].split()[1:]
     xyz, origin = buffem.SWGGeometry(str(p)).vertices(1)
     assert int(last[0]) == len(xyz) and int(last[1]) == 72
