@@ -1041,6 +1041,195 @@ long or_sing_static_refined(int c, const double *VA, const double *VB, const dou
   return A.evals;
 }
 
+/* ------------------------------------------------------------------------- */
+/* Moments of a singular tetrahedron pair, as the GPU's k_tp_singular keeps   */
+/* them: per kernel K in {1/4 pi r, 1/4 pi, r/8 pi} the 8 numbers             */
+/*   int K,  int K (x - o),  int K (y - o),  int K (x - o).(y - o)            */
+/* in the barycentric measure (times 36 |V_A| |V_B| for the volume measure), */
+/* o = first common vertex; (x-Q).(y-Q') follows by                           */
+/* M2 - q'.M1 - q.M1' + q.q' M0 with q = Q - o, q' = Q' - o.                  */
+/* ------------------------------------------------------------------------- */
+static inline void sing_moment_point(const SingPair *X, int S, const double *al, const double *be, double w,
+                                     double acc[24])
+{
+  int c = X->c;
+  double A1[3] = {0, 0, 0}, B1[3] = {0, 0, 0};
+  int ja = 0, jb = 0;
+  for (int k = 0; k < c; k++) {
+    if (S & (1 << k)) { double z = al[ja++]; for (int x = 0; x < 3; x++) A1[x] += z * X->VA[k][x]; }
+    else              { double z = be[jb++]; for (int x = 0; x < 3; x++) B1[x] += z * X->VA[k][x]; }
+  }
+  for (int k = c; k < 4; k++) {
+    double za = al[ja++], zb = be[jb++];
+    for (int x = 0; x < 3; x++) { A1[x] += za * X->VA[k][x]; B1[x] += zb * X->VB[k][x]; }
+  }
+  const double *ub = X->ub;
+  double L0 = A1[0] - B1[0], L1 = A1[1] - B1[1], L2 = A1[2] - B1[2];
+  double R = sqrt(L0 * L0 + L1 * L1 + L2 * L2);
+  double AB = A1[0] * B1[0] + A1[1] * B1[1] + A1[2] * B1[2];
+  double uAB = ub[0] * (A1[0] + B1[0]) + ub[1] * (A1[1] + B1[1]) + ub[2] * (A1[2] + B1[2]);
+  double Rp[3] = {1.0 / R, 1.0, R};
+  for (int pk = 0; pk < 3; pk++) {
+    double wr = w * Rp[pk], G0 = X->G[pk][0], G1 = X->G[pk][1], G2 = X->G[pk][2];
+    acc[8 * pk] += wr * G0;
+    for (int x = 0; x < 3; x++) {
+      acc[8 * pk + 1 + x] += wr * (A1[x] * G1 + ub[x] * (G0 - G1));
+      acc[8 * pk + 4 + x] += wr * (B1[x] * G1 + ub[x] * (G0 - G1));
+    }
+    acc[8 * pk + 7] += wr * (AB * G2 + uAB * (G1 - G2) + X->W * (G0 - 2.0 * G1 + G2));
+  }
+}
+
+static const double SING_GPRE[3] = {0.25 / M_PI, 0.25 / M_PI, 0.125 / M_PI};
+
+static void sing_moment_box(SingAdapt *A, const double *lo, const double *hi, double out[24])
+{
+  int k = A->ka + A->kb, tot = 1;
+  for (int d = 0; d < k; d++) tot *= A->ng;
+  for (int i = 0; i < 24; i++) out[i] = 0.0;
+  for (int t = 0; t < tot; t++) {
+    double u[6], al[4], be[4], w = 1.0;
+    int r = t;
+    for (int d = 0; d < k; d++) {
+      int i = r % A->ng;
+      r /= A->ng;
+      u[d] = lo[d] + (hi[d] - lo[d]) * A->gx[i];
+      w *= (hi[d] - lo[d]) * A->gw[i];
+    }
+    w *= collapse_simplex(A->ka, u, al) * collapse_simplex(A->kb, u + A->ka, be);
+    sing_moment_point(A->X, A->S, al, be, w, out);
+  }
+  A->evals += tot;
+}
+
+/* whole-face product rule of order n: the moments k_tp_singular computes */
+static void sing_moments_fixed(const SingPair *X, int n, double out[24])
+{
+  SingAdapt A;
+  A.X = X;
+  A.ng = n;
+  A.evals = 0;
+  gauss_legendre01(n, A.gx, A.gw);
+  double lo[4] = {0, 0, 0, 0}, hi[4] = {1, 1, 1, 1}, acc[24] = {0};
+  int c = X->c, nown = 4 - c;
+  for (int S = 0; S < (1 << c); S++) {
+    int ns = __builtin_popcount(S);
+    if (c == 4 && (ns == 0 || ns == 4)) continue;
+    A.S = S; A.ka = ns + nown - 1; A.kb = c - ns + nown - 1;
+    double f[24];
+    sing_moment_box(&A, lo, hi, f);
+    for (int i = 0; i < 24; i++) acc[i] += f[i];
+  }
+  for (int i = 0; i < 24; i++) out[i] = acc[i] * SING_GPRE[i / 8];
+}
+
+/* public: moments of order n (VA, VB common-first, 4 x 3 each) */
+void or_sing_moments(int c, const double *VA, const double *VB, int n, double *out)
+{
+  SingPair X;
+  double Q[3] = {0, 0, 0};
+  sing_pair_init(&X, c, (const double (*)[3])VA, (const double (*)[3])VB, Q, Q);
+  sing_moments_fixed(&X, n, out);
+}
+
+/* Refined moments: the scheme of or_sing_static_refined on the 24 moments,
+   each measured against its kernel's scale (|M0|, |M0| h, |M0| h^2 for the
+   zeroth, first and second moments; h = diameter of A). */
+long or_sing_moments_refined(int c, const double *VA, const double *VB, int n, int ng, double flag_tol, double tol,
+                             double *out, int *status)
+{
+  SingPair X;
+  double Q[3] = {0, 0, 0};
+  sing_pair_init(&X, c, (const double (*)[3])VA, (const double (*)[3])VB, Q, Q);
+  double f0[24], f1[24];
+  *status = 0;
+  sing_moments_fixed(&X, n, f0);
+  sing_moments_fixed(&X, n + 2, f1);
+  double h2 = 0.0;
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 4; j++) {
+      double s2 = 0.0;
+      for (int x = 0; x < 3; x++) s2 += (X.VA[i][x] - X.VA[j][x]) * (X.VA[i][x] - X.VA[j][x]);
+      h2 = fmax(h2, s2);
+    }
+  double h = sqrt(h2), scale[24];
+  for (int pk = 0; pk < 3; pk++) {
+    double m0 = fabs(f1[8 * pk]) / SING_GPRE[pk];   /* unscaled measure, as the boxes */
+    scale[8 * pk] = m0;
+    for (int x = 1; x < 7; x++) scale[8 * pk + x] = m0 * h;
+    scale[8 * pk + 7] = m0 * h2;
+  }
+  double flag = 0.0;
+  for (int i = 0; i < 24; i++) flag = fmax(flag, fabs(f1[i] - f0[i]) / SING_GPRE[i / 8] / scale[i]);
+  if (flag <= flag_tol) {
+    for (int i = 0; i < 24; i++) out[i] = f1[i];
+    return 0;
+  }
+  SingAdapt A;
+  A.X = &X;
+  A.ng = ng;
+  A.evals = 0;
+  gauss_legendre01(ng, A.gx, A.gw);
+  typedef struct { int S; double lo[4], hi[4], val[24]; } MomBox;
+  MomBox *cur = malloc(sizeof(MomBox) * SR_MAXBOX), *nxt = malloc(sizeof(MomBox) * SR_MAXBOX);
+  int ncur = 0, nown = 4 - c;
+  double acc[24] = {0};
+  for (int S = 0; S < (1 << c); S++) {
+    int ns = __builtin_popcount(S);
+    if (c == 4 && (ns == 0 || ns == 4)) continue;
+    MomBox *b = &cur[ncur++];
+    b->S = S;
+    for (int d = 0; d < 4; d++) { b->lo[d] = 0.0; b->hi[d] = 1.0; }
+    A.S = S; A.ka = ns + nown - 1; A.kb = c - ns + nown - 1;
+    sing_moment_box(&A, b->lo, b->hi, b->val);
+  }
+  for (int level = 0; level < SR_MAXLEVEL && ncur > 0; level++) {
+    int nn = 0;
+    for (int bi = 0; bi < ncur; bi++) {
+      MomBox *b = &cur[bi];
+      int ns = __builtin_popcount(b->S);
+      A.S = b->S; A.ka = ns + nown - 1; A.kb = c - ns + nown - 1;
+      int k = A.ka + A.kb;
+      double best = -1.0, half[2][24], hl[2][4], hh[2][4];
+      for (int d = 0; d < k; d++) {
+        double l0[4], h0[4], l1[4], h1[4], v0[24], v1[24];
+        memcpy(l0, b->lo, sizeof l0); memcpy(h0, b->hi, sizeof h0);
+        memcpy(l1, b->lo, sizeof l1); memcpy(h1, b->hi, sizeof h1);
+        h0[d] = l1[d] = 0.5 * (b->lo[d] + b->hi[d]);
+        sing_moment_box(&A, l0, h0, v0);
+        sing_moment_box(&A, l1, h1, v1);
+        double e = 0.0;
+        for (int i = 0; i < 24; i++) e = fmax(e, fabs(v0[i] + v1[i] - b->val[i]) / scale[i]);
+        if (e > best) {
+          best = e;
+          memcpy(half[0], v0, sizeof v0); memcpy(half[1], v1, sizeof v1);
+          memcpy(hl[0], l0, sizeof l0); memcpy(hh[0], h0, sizeof h0);
+          memcpy(hl[1], l1, sizeof l1); memcpy(hh[1], h1, sizeof h1);
+        }
+      }
+      int open = best > tol;
+      if (open && nn + 2 > SR_MAXBOX) { open = 0; *status |= 1; }
+      if (open && level == SR_MAXLEVEL - 1) { open = 0; *status |= 2; }
+      if (!open) {
+        for (int i = 0; i < 24; i++) acc[i] += half[0][i] + half[1][i];
+        continue;
+      }
+      for (int hf = 0; hf < 2; hf++) {
+        MomBox *q = &nxt[nn++];
+        q->S = b->S;
+        memcpy(q->lo, hl[hf], sizeof q->lo); memcpy(q->hi, hh[hf], sizeof q->hi);
+        memcpy(q->val, half[hf], sizeof q->val);
+      }
+    }
+    MomBox *t = cur; cur = nxt; nxt = t;
+    ncur = nn;
+  }
+  free(cur);
+  free(nxt);
+  for (int i = 0; i < 24; i++) out[i] = acc[i] * SING_GPRE[i / 8];
+  return A.evals;
+}
+
 /* public wrapper for tests: tets given by 4 vertices each (common first) */
 void or_sing_static(int c, const double *VA, const double *VB, const double *Q, const double *QP,
                     int nang, double *out)

@@ -76,6 +76,9 @@ def lib():
         L.or_sing_static_adaptive.restype = C.c_long
         L.or_sing_static_refined.argtypes = [I, dp, dp, dp, dp, I, I, D, D, dp, C.POINTER(I)]
         L.or_sing_static_refined.restype = C.c_long
+        L.or_sing_moments.argtypes = [I, dp, dp, I, dp]
+        L.or_sing_moments_refined.argtypes = [I, dp, dp, I, I, D, D, dp, C.POINTER(I)]
+        L.or_sing_moments_refined.restype = C.c_long
         L.or_fibbi.argtypes = [P, I, I, dp]
         L.or_gme.argtypes = [P, I, I, D, D, dp]
         L.or_overlaps.argtypes = [P, I, D, ip, dp]
@@ -328,3 +331,34 @@ def sing_static_refined(c, VA, VB, Q, QP, n=10, ng=6, flag_tol=1e-7, tol=1e-10):
                                       np.ascontiguousarray(QP, dtype=np.float64), n, ng, flag_tol, tol, out,
                                       C.byref(st))
     return out, ne, st.value
+
+
+def sing_moments(c, VA, VB, n=10, refined=False, ng=6, flag_tol=1e-7, tol=1e-9):
+    """The 24 moments k_tp_singular keeps for a tetrahedron pair (per kernel
+    1/4pi r, 1/4pi, r/8pi: int K, int K (x-o), int K (y-o), int K (x-o).(y-o),
+    barycentric measure, o = first common vertex), at order n or refined;
+    returns (moments, angular points of the refinement, status)."""
+    out = np.zeros(24)
+    A = np.ascontiguousarray(VA, dtype=np.float64).reshape(-1)
+    B = np.ascontiguousarray(VB, dtype=np.float64).reshape(-1)
+    if not refined:
+        lib().or_sing_moments(c, A, B, n, out)
+        return out, 0, 0
+    st = C.c_int()
+    ne = lib().or_sing_moments_refined(c, A, B, n, ng, flag_tol, tol, out, C.byref(st))
+    return out, ne, st.value
+
+
+def moments_to_values(M, VA, VB, Q, QP):
+    """The six sing_static values from the 24 moments."""
+    VA, VB = np.asarray(VA, float), np.asarray(VB, float)
+    vol = lambda V: abs(np.linalg.det(np.array([V[1] - V[0], V[2] - V[0], V[3] - V[0]]))) / 6
+    f = 36 * vol(VA) * vol(VB)
+    o = VA[0]
+    q, qp = np.asarray(Q) - o, np.asarray(QP) - o
+    out = np.zeros(6)
+    for pk, g in enumerate((0.25 / np.pi, 0.25 / np.pi, 0.125 / np.pi)):
+        m = M[8 * pk:8 * pk + 8] / g
+        out[2 * pk] = f * (m[7] - qp @ m[1:4] - q @ m[4:7] + (q @ qp) * m[0])
+        out[2 * pk + 1] = f * m[0]
+    return out

@@ -148,20 +148,26 @@ def test_singular_rules_accuracy_on_reference_mesh(oracle_lib):
     only to ~1e-3 on the worst (poorly shaped tetrahedra, shape ratio down to
     0.036); the refined rule (orders 10 and 12, level-by-level refinement
     where they differ by more than 1e-7) bounds every pair by 3e-7, below the
-    reference's Taylor-Duffy tolerance of 1e-6."""
+    reference's Taylor-Duffy tolerance of 1e-6; the same scheme on the 24
+    moments of the pair, flagged at 1e-8, bounds it by 2e-8."""
     pairs = singular_pairs("sphere533")
     rng = np.random.default_rng(0)
     by_c = {2: [], 3: [], 4: []}
     refined = []
     c2 = [p for p in pairs if p[0] == 2]
     sample = [c2[i] for i in rng.choice(len(c2), 40, replace=False)] + [p for p in pairs if p[0] > 2]
+    moments = []
     for c, VA, VB in sample:
         ref, _ = oracle_lib.sing_static_adaptive(c, VA, VB, VA[-1], VB[-1], 5, 1e-10)
         by_c[c].append(rule_error(oracle_lib, c, VA, VB, ref))
+        h2 = max(np.sum((a - b) ** 2) for a in VA for b in VA)
+        scale = np.repeat(np.abs(ref[1::2]), 2) * np.tile([h2, 1.0], 3)
         val, _, status = oracle_lib.sing_static_refined(c, VA, VB, VA[-1], VB[-1], 10, 6, 1e-7, 1e-9)
         assert status == 0
-        h2 = max(np.sum((a - b) ** 2) for a in VA for b in VA)
-        refined.append(np.max(np.abs(val - ref) / (np.repeat(np.abs(ref[1::2]), 2) * np.tile([h2, 1.0], 3))))
+        refined.append(np.max(np.abs(val - ref) / scale))
+        M, _, status = oracle_lib.sing_moments(c, VA, VB, 10, True, 6, 1e-8, 1e-9)
+        assert status == 0
+        moments.append(np.max(np.abs(oracle_lib.moments_to_values(M, VA, VB, VA[-1], VB[-1]) - ref) / scale))
     assert len(by_c[3]) > 500 and len(by_c[4]) > 300
     for c, errs in by_c.items():
         errs = np.array(errs)
@@ -169,6 +175,24 @@ def test_singular_rules_accuracy_on_reference_mesh(oracle_lib):
         assert errs.max() < 1e-2, (c, errs.max())
     assert np.percentile(by_c[4], 99) > 1e-5   # the tail of the fixed rule
     assert max(refined) < 3e-7, max(refined)
+    # the moment form (what k_tp_singular keeps), flagged at 1e-8
+    assert max(moments) < 2e-8, max(moments)
+
+
+def test_singular_moments_give_the_pair_values(oracle_lib):
+    """The 24 moments of a tetrahedron pair reproduce sing_static's six
+    values for any Q, Q' (M2 - q'.M1 - q.M1' + q.q' M0)."""
+    rng = np.random.default_rng(3)
+    for _ in range(200):
+        c = int(rng.integers(2, 5))
+        A, B = rng.normal(size=(4, 3)), rng.normal(size=(4, 3))
+        B[:c] = A[:c]
+        Q, QP = rng.normal(size=3), rng.normal(size=3)
+        n = int(rng.integers(3, 11))
+        M, _, _ = oracle_lib.sing_moments(c, A, B, n)
+        v = oracle_lib.moments_to_values(M, A, B, Q, QP)
+        ref = oracle_lib.sing_static(c, A, B, Q, QP, n)
+        assert np.max(np.abs(v - ref)) <= 1e-12 * np.abs(ref).max()
 
 
 def test_adaptive_reference_is_converged_on_the_worst_pairs(oracle_lib):
