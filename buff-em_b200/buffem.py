@@ -70,6 +70,7 @@ EXPORTS = [
     "bg_last_error", "bg_geometry_create", "bg_geometry_create_objects", "bg_geometry_destroy",
     "bg_geometry_num_bfs", "bg_geometry_num_objects", "bg_geometry_bf_offset", "bg_geometry_faces",
     "bg_geometry_vertices", "bg_geometry_object_index", "bg_geometry_object_label", "bg_geometry_material_eps",
+    "bg_trans_file_count", "bg_trans_file_tag", "bg_geometry_create_transformed",
     "bg_geometry_precompute", "bg_geometry_set_singular_order", "bg_geometry_near_data",
     "bg_matrix_create", "bg_matrix_destroy", "bg_assemble", "bg_matrix_download", "bg_matrix_upload",
     "bg_matrix_device_ptr", "bg_lu_factor", "bg_lu_pivots", "bg_lu_solve", "bg_lu_solve_device",
@@ -107,6 +108,9 @@ def lib():
         L.bg_geometry_object_index.argtypes = [P, C.c_char_p]
         L.bg_geometry_object_label.argtypes = [P, I, C.c_char_p, I]
         L.bg_geometry_material_eps.argtypes = [P, I, D, D, VP]
+        L.bg_trans_file_count.argtypes = [C.c_char_p]
+        L.bg_trans_file_tag.argtypes = [C.c_char_p, I, C.c_char_p, I]
+        L.bg_geometry_create_transformed.argtypes = [C.c_char_p, C.c_char_p, I, C.POINTER(P)]
         L.bg_geometry_set_singular_order.argtypes = [P, I]
         L.bg_geometry_near_data.argtypes = [P, C.POINTER(I), VP, VP]
         L.bg_matrix_create.argtypes = [P, I, C.POINTER(P)]
@@ -256,13 +260,29 @@ class HMatrix:
         return p.value, ld.value
 
 
+def ReadTransFile(path):
+    """Tags of the transformations of a .trans file, in order (pass the index
+    as SWGGeometry(..., TransFile=path, Transformation=k))."""
+    n = _check(lib().bg_trans_file_count(path.encode()))
+    tags = []
+    for k in range(n):
+        m = _check(lib().bg_trans_file_tag(path.encode(), k, None, 0))
+        buf = C.create_string_buffer(m + 1)
+        _check(lib().bg_trans_file_tag(path.encode(), k, buf, m + 1))
+        tags.append(buf.value.decode())
+    return tags
+
+
 class SWGGeometry:
     """Replaces buff::SWGGeometry (libbuff.h:200-272) for the VIE hot path."""
 
     def __init__(self, GeoFileName=None, meshfiles=None, materials=None, displacements=None,
-                 singular_order=None):
+                 singular_order=None, TransFile=None, Transformation=0):
         h = C.c_void_p()
-        if GeoFileName is not None:
+        if GeoFileName is not None and TransFile is not None:
+            _check(lib().bg_geometry_create_transformed(GeoFileName.encode(), TransFile.encode(), int(Transformation),
+                                                        C.byref(h)))
+        elif GeoFileName is not None:
             _check(lib().bg_geometry_create(GeoFileName.encode(), C.byref(h)))
         else:
             if isinstance(meshfiles, str):

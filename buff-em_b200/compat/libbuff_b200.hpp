@@ -122,6 +122,13 @@ class SWGGeometry {
     check(bg_geometry_create(GeoFileName, &g));
     init();
   }
+  // the geometry with transformation k of a .trans file applied
+  // (SWGGeometry::Transform, SWGGeometry.cc:426-439; one object per
+  // transformation instead of Transform / UnTransform on one)
+  SWGGeometry(const char *GeoFileName, const char *TransFile, int k) {
+    check(bg_geometry_create_transformed(GeoFileName, TransFile, k, &g));
+    init();
+  }
   SWGGeometry(int nobj, const char *const *meshes, const double *disp, const bg_material *mats) {
     check(bg_geometry_create_objects(nobj, meshes, disp, mats, &g));
     init();

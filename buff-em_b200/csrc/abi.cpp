@@ -166,12 +166,56 @@ int bg_geometry_create_objects(int nobj, const char *const *meshfiles, const dou
   return create_objects(nobj, meshfiles, xf.data(), materials, nullptr, nullptr, out);
 }
 
+static int create_from_objects(std::vector<GeoObject> &objs, bg_geometry **out);
+
 int bg_geometry_create(const char *path, bg_geometry **out) {
   if (!path || !out) { set_error("bg_geometry_create: bad arguments"); return BG_ERR_ARG; }
   *out = nullptr;
   std::vector<GeoObject> objs;
   int st = parse_buffgeo(path, objs);
   if (st) return st;
+  return create_from_objects(objs, out);
+}
+
+int bg_trans_file_count(const char *trans_path) {
+  if (!trans_path) { set_error("bg_trans_file_count: bad arguments"); return BG_ERR_ARG; }
+  std::vector<TransEntry> tr;
+  int st = parse_trans_file(trans_path, tr);
+  return st ? st : (int)tr.size();
+}
+
+int bg_trans_file_tag(const char *trans_path, int k, char *buf, int cap) {
+  if (!trans_path || k < 0 || cap < 0 || (cap > 0 && !buf)) { set_error("bg_trans_file_tag: bad arguments"); return BG_ERR_ARG; }
+  std::vector<TransEntry> tr;
+  int st = parse_trans_file(trans_path, tr);
+  if (st) return st;
+  if (k >= (int)tr.size()) { set_error("bg_trans_file_tag: %s has %d transformations", trans_path, (int)tr.size()); return BG_ERR_ARG; }
+  const std::string &t = tr[k].tag;
+  if (cap > 0) {
+    size_t n = std::min(t.size(), (size_t)cap - 1);
+    std::memcpy(buf, t.data(), n);
+    buf[n] = 0;
+  }
+  return (int)t.size();
+}
+
+int bg_geometry_create_transformed(const char *path, const char *trans_path, int k, bg_geometry **out) {
+  if (!path || !trans_path || !out || k < 0) { set_error("bg_geometry_create_transformed: bad arguments"); return BG_ERR_ARG; }
+  *out = nullptr;
+  std::vector<GeoObject> objs;
+  int st = parse_buffgeo(path, objs);
+  if (st) return st;
+  std::vector<TransEntry> tr;
+  if ((st = parse_trans_file(trans_path, tr))) return st;
+  if (k >= (int)tr.size()) {
+    set_error("bg_geometry_create_transformed: %s has %d transformations", trans_path, (int)tr.size());
+    return BG_ERR_ARG;
+  }
+  if ((st = apply_trans(tr[k], objs))) return st;
+  return create_from_objects(objs, out);
+}
+
+static int create_from_objects(std::vector<GeoObject> &objs, bg_geometry **out) {
   std::vector<const char *> names;
   std::vector<double> xf;
   std::vector<bg_material> mats;

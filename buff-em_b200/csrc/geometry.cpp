@@ -647,6 +647,93 @@ static bool special_name(const char *path, std::vector<std::vector<std::string>>
   return true;
 }
 
+// ------------------------------------------------------- .trans files
+// A list of geometrical transformations (SCUFF-EM's GTComplex list, read by
+// ReadTransFile; used by buff-neq's --TransFile, CreateBNEQData.cc:58-66):
+//   TRANS <tag> OBJECT <label> DISP dx dy dz [ROT theta ABOUT ax ay az ...]
+//               [OBJECT <label> ...]
+// on one line, or TRANS <tag> on its own line followed by OBJECT lines and
+// ENDTRANS.  Objects not named keep their position.
+static int parse_trans_tokens(const std::vector<std::string> &tok, size_t t, TransEntry &e, std::string &err) {
+  while (t < tok.size()) {
+    if (!keyword_is(tok[t], "OBJECT", "SURFACE")) { err = "expected OBJECT <label>, got " + tok[t]; return BG_ERR_IO; }
+    if (t + 1 >= tok.size()) { err = "OBJECT needs a label"; return BG_ERR_IO; }
+    std::string label = tok[t + 1];
+    size_t u = t + 2;
+    while (u < tok.size() && !keyword_is(tok[u], "OBJECT", "SURFACE")) u++;
+    std::vector<std::string> ops(tok.begin() + (long)t + 2, tok.begin() + (long)u);
+    if (ops.empty()) { err = "no transformation given for object " + label; return BG_ERR_IO; }
+    TransEntry::Op op;
+    op.label = label;
+    xf_identity(op.xf);
+    if (!parse_transforms(ops, op.xf, err)) return BG_ERR_IO;
+    e.ops.push_back(op);
+    t = u;
+  }
+  return BG_OK;
+}
+
+int parse_trans_file(const char *path, std::vector<TransEntry> &out) {
+  FILE *f = std::fopen(path, "r");
+  if (!f) { set_error("could not open %s", path); return BG_ERR_IO; }
+  char buf[4096];
+  int lineno = 0, start = 0;
+  bool open = false;
+  TransEntry cur;
+  std::string err;
+  auto fail = [&](int ln) {
+    std::fclose(f);
+    set_error("%s:%d: %s", path, ln, err.c_str());
+    return BG_ERR_IO;
+  };
+  while (std::fgets(buf, sizeof buf, f)) {
+    lineno++;
+    std::vector<std::string> tok = tokenize(buf);
+    if (tok.empty() || tok[0][0] == '#') continue;
+    if (open) {
+      if (keyword_is(tok[0], "ENDTRANS")) {
+        out.push_back(cur);
+        open = false;
+      } else if (parse_trans_tokens(tok, 0, cur, err)) {
+        return fail(lineno);
+      }
+    } else if (keyword_is(tok[0], "TRANS")) {
+      if (tok.size() < 2) { err = "TRANS needs a tag"; return fail(lineno); }
+      cur = TransEntry{};
+      cur.tag = tok[1];
+      if (tok.size() == 2) {
+        open = true;
+        start = lineno;
+      } else {
+        if (parse_trans_tokens(tok, 2, cur, err)) return fail(lineno);
+        out.push_back(cur);
+      }
+    } else {
+      err = "syntax error";
+      return fail(lineno);
+    }
+  }
+  std::fclose(f);
+  if (open) { set_error("%s:%d: TRANS without ENDTRANS", path, start); return BG_ERR_IO; }
+  if (out.empty()) { set_error("%s: no transformations", path); return BG_ERR_IO; }
+  return BG_OK;
+}
+
+// SWGGeometry::Transform (SWGGeometry.cc:426-439, SWGVolume.cc:208-236): each
+// named object's transformation is applied after its one-time one.
+int apply_trans(const TransEntry &e, std::vector<GeoObject> &objs) {
+  for (auto &op : e.ops) {
+    size_t k = 0;
+    while (k < objs.size() && upper_case(objs[k].label) != upper_case(op.label)) k++;
+    if (k == objs.size()) {
+      set_error("transformation %s: no object labelled %s", e.tag.c_str(), op.label.c_str());
+      return BG_ERR_ARG;
+    }
+    xf_compose(objs[k].xf, op.xf);
+  }
+  return BG_OK;
+}
+
 int parse_buffgeo(const char *path, std::vector<GeoObject> &objs) {
   std::vector<std::vector<std::string>> special;
   if (special_name(path, special)) {

@@ -103,6 +103,20 @@ const std::string &matprop_name(const MatPropFn &m);
 // MESH__<mesh>__MAT__<material> name (SWGGeometry.cc:167-209).
 int parse_buffgeo(const char *path, std::vector<GeoObject> &objs);
 
+// One transformation of a .trans file: a tag and, per named object, a
+// transformation (12 doubles, M row-major then D).
+struct TransEntry {
+  struct Op {
+    std::string label;
+    double xf[12];
+  };
+  std::string tag;
+  std::vector<Op> ops;
+};
+int parse_trans_file(const char *path, std::vector<TransEntry> &out);
+// composes e's transformations after the named objects' own
+int apply_trans(const TransEntry &e, std::vector<GeoObject> &objs);
+
 // ---------------------------------------------------------------- device SoA
 // All indices are global over the objects of a geometry (vertex and tet
 // indices carry per-object offsets), so basis functions of different objects

@@ -83,7 +83,24 @@ const char *bg_last_error(void);
    Errors carry "<file>:<line>: <message>" as the reference's ErrExit does. */
 int bg_geometry_create(const char *buffgeo_path, bg_geometry **out);
 
-/* Same as above from explicit per-object mesh files, displacements
+/* Transformation lists (.trans files of buff-neq's --TransFile, read by
+   ReadTransFile into GTComplex lists, CreateBNEQData.cc:58-66): lines
+   TRANS <tag> OBJECT <label> DISP dx dy dz [ROT theta ABOUT ax ay az]
+   [OBJECT ...], or TRANS <tag> followed by OBJECT lines and ENDTRANS.
+   bg_trans_file_count returns the number of transformations;
+   bg_trans_file_tag copies tag k into buf (as bg_geometry_object_label) and
+   returns its length. */
+int bg_trans_file_count(const char *trans_path);
+int bg_trans_file_tag(const char *trans_path, int k, char *buf, int cap);
+
+/* The geometry of a .buffgeo file with transformation k of a .trans file
+   applied (SWGGeometry::Transform, SWGGeometry.cc:426-439: each named
+   object's transformation follows its one-time DISPLACED / ROTATED ones).
+   One handle per transformation replaces the reference's transform /
+   untransform of a single geometry; an unknown object label is an error. */
+int bg_geometry_create_transformed(const char *buffgeo_path, const char *trans_path, int k, bg_geometry **out);
+
+/* Same as bg_geometry_create from explicit per-object mesh files, displacements
    (3*nobj doubles or NULL) and permittivity functors (SWGGeometry.cc:52-158). */
 int bg_geometry_create_objects(int nobj, const char *const *meshfiles, const double *displacements,
                                const bg_material *materials, bg_geometry **out);

@@ -290,3 +290,67 @@ def test_dispersive_geometry_is_refused_by_batched_sweeps(buffem_lib, sphere, tm
     out = np.zeros(64)
     st = L.bg_batch_sweep(geoms, 1, buffem._ptr(w), 1, buffem._ptr(E0), buffem._ptr(nh), 1, 0, buffem._ptr(out), None)
     assert st == buffem.BG_ERR_ARG and "frequency-dependent" in L.bg_last_error().decode()
+
+
+def two_spheres(tmp_path, mesh):
+    return geo(tmp_path, obj(mesh, label="Upper") + obj(mesh, "DISPLACED 0 0 -0.5", label="Lower"), "two.buffgeo")
+
+
+def test_trans_files(buffem_lib, sphere, tmp_path):
+    """TRANS lines (one-line and TRANS ... ENDTRANS forms): each
+    transformation follows the object's own DISPLACED lines; objects not
+    named stay in place."""
+    mesh = sphere(2)
+    X = read_nodes(mesh)
+    g = two_spheres(tmp_path, mesh)
+    t = tmp_path / "s.trans"
+    t.write_text("# separations\n"
+                 "TRANS 4.0 OBJECT Upper DISP 0 0 4.0\n"
+                 "TRANS  tilt\n  OBJECT lower ROT 90 ABOUT 0 0 1\n  OBJECT UPPER DISP 1 0 0 DISP 0 1 0\nENDTRANS\n"
+                 "TRANS 6 OBJECT Upper DISP 0 0 6 OBJECT Lower DISP 0 0 -1\n")
+    assert buffem.ReadTransFile(str(t)) == ["4.0", "tilt", "6"]
+    G = buffem.SWGGeometry(g, TransFile=str(t), Transformation=0)
+    assert np.array_equal(G.vertices(0)[0], X + [0, 0, 4.0]) and np.array_equal(G.vertices(0)[1], [0, 0, 4.0])
+    assert np.array_equal(G.vertices(1)[0], X + [0, 0, -0.5])
+    G = buffem.SWGGeometry(g, TransFile=str(t), Transformation=1)
+    assert np.array_equal(G.vertices(0)[0], X + [1.0, 1.0, 0])
+    R = rot(90, [0, 0, 1])
+    assert np.allclose(G.vertices(1)[0], (X + [0, 0, -0.5]) @ R.T, atol=1e-14, rtol=0)
+    G = buffem.SWGGeometry(g, TransFile=str(t), Transformation=2)
+    assert np.array_equal(G.vertices(1)[1], [0, 0, -1.5])
+    assert G.TotalBFs == 144 and G.label(0) == "Upper"
+
+
+@pytest.mark.parametrize("body,line,words", [
+    ("TRANS\n", 1, "needs a tag"),
+    ("TRANS a OBJECT\n", 1, "needs a label"),
+    ("TRANS a OBJECT Upper\n", 1, "no transformation given"),
+    ("TRANS a OBJECT Upper DISP 1 2\n", 1, "three numbers"),
+    ("TRANS a Upper DISP 1 2 3\n", 1, "expected OBJECT"),
+    ("TRANS a\n OBJECT Upper DISP 1 2 3\n", 1, "without ENDTRANS"),
+    ("SHIFT a\n", 1, "syntax error"),
+    ("TRANS a\n OBJECT Upper SPIN 3\nENDTRANS\n", 2, "unknown transformation SPIN"),
+])
+def test_trans_file_errors(buffem_lib, sphere, tmp_path, body, line, words):
+    t = tmp_path / "bad.trans"
+    t.write_text(body)
+    with pytest.raises(buffem.BuffError) as e:
+        buffem.SWGGeometry(two_spheres(tmp_path, sphere(2)), TransFile=str(t))
+    msg = str(e.value)
+    assert f"{t}:{line}:" in msg and words in msg, msg
+
+
+def test_trans_file_selection_errors(buffem_lib, sphere, tmp_path):
+    g = two_spheres(tmp_path, sphere(2))
+    t = tmp_path / "s.trans"
+    t.write_text("TRANS 1 OBJECT Middle DISP 0 0 1\n")
+    with pytest.raises(buffem.BuffError) as e:
+        buffem.SWGGeometry(g, TransFile=str(t))
+    assert "no object labelled Middle" in str(e.value)
+    with pytest.raises(buffem.BuffError) as e:
+        buffem.SWGGeometry(g, TransFile=str(t), Transformation=1)
+    assert "has 1 transformations" in str(e.value)
+    (tmp_path / "empty.trans").write_text("# nothing\n")
+    with pytest.raises(buffem.BuffError) as e:
+        buffem.ReadTransFile(str(tmp_path / "empty.trans"))
+    assert "no transformations" in str(e.value)
