@@ -97,7 +97,6 @@ int matprop_parse_section(const std::string &name, const std::vector<std::string
                           const std::vector<int> &lineno, const char *path, std::shared_ptr<const MatPropFn> &out);
 // eps(Omega), Omega in units of 3e14 rad/s, into eps[2] (re, im)
 void matprop_eps(const MatPropFn &m, double omega_re, double omega_im, double eps[2]);
-const std::string &matprop_name(const MatPropFn &m);
 
 // Parses a .buffgeo file (SWGGeometry.cc:52-158, 214-383) or a special
 // MESH__<mesh>__MAT__<material> name (SWGGeometry.cc:167-209).

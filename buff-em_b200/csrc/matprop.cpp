@@ -341,6 +341,5 @@ void matprop_eps(const MatPropFn &m, double omega_re, double omega_im, double ep
   eps[1] = v.imag();
 }
 
-const std::string &matprop_name(const MatPropFn &m) { return m.name; }
 
 }  // namespace bg
