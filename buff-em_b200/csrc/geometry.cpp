@@ -537,6 +537,17 @@ static std::vector<std::string> tokenize(const char *line) {
   return tok;
 }
 
+// one whole line of f (any length), without its newline
+static bool get_line(FILE *f, std::string &line) {
+  line.clear();
+  char buf[1024];
+  while (std::fgets(buf, sizeof buf, f)) {
+    line += buf;
+    if (!line.empty() && line.back() == '\n') { line.pop_back(); return true; }
+  }
+  return !line.empty();
+}
+
 static bool readable(const std::string &f) {
   FILE *t = std::fopen(f.c_str(), "r");
   if (t) std::fclose(t);
@@ -676,7 +687,7 @@ static int parse_trans_tokens(const std::vector<std::string> &tok, size_t t, Tra
 int parse_trans_file(const char *path, std::vector<TransEntry> &out) {
   FILE *f = std::fopen(path, "r");
   if (!f) { set_error("could not open %s", path); return BG_ERR_IO; }
-  char buf[4096];
+  std::string buf;
   int lineno = 0, start = 0;
   bool open = false;
   TransEntry cur;
@@ -686,9 +697,9 @@ int parse_trans_file(const char *path, std::vector<TransEntry> &out) {
     set_error("%s:%d: %s", path, ln, err.c_str());
     return BG_ERR_IO;
   };
-  while (std::fgets(buf, sizeof buf, f)) {
+  while (get_line(f, buf)) {
     lineno++;
-    std::vector<std::string> tok = tokenize(buf);
+    std::vector<std::string> tok = tokenize(buf.c_str());
     if (tok.empty() || tok[0][0] == '#') continue;
     if (open) {
       if (keyword_is(tok[0], "ENDTRANS")) {
@@ -752,7 +763,7 @@ int parse_buffgeo(const char *path, std::vector<GeoObject> &objs) {
   size_t slash = dir.find_last_of('/');
   dir = (slash == std::string::npos) ? std::string(".") : dir.substr(0, slash);
   std::vector<std::string> meshpath;
-  char buf[1024];
+  std::string buf;
   int lineno = 0, start = 0;
   bool in = false;
   GeoObject cur;
@@ -768,9 +779,9 @@ int parse_buffgeo(const char *path, std::vector<GeoObject> &objs) {
     set_error("%s:%d: %s", path, ln, msg);
     return BG_ERR_IO;
   };
-  while (std::fgets(buf, sizeof buf, f)) {
+  while (get_line(f, buf)) {
     lineno++;
-    std::vector<std::string> tok = tokenize(buf);
+    std::vector<std::string> tok = tokenize(buf.c_str());
     if (tok.empty() || tok[0][0] == '#') continue;
     if (inmat) {
       if (keyword_is(tok[0], "ENDMATERIAL")) {

@@ -354,3 +354,10 @@ def test_trans_file_selection_errors(buffem_lib, sphere, tmp_path):
     with pytest.raises(buffem.BuffError) as e:
         buffem.ReadTransFile(str(tmp_path / "empty.trans"))
     assert "no transformations" in str(e.value)
+
+
+def test_long_lines(buffem_lib, sphere, tmp_path):
+    """Lines of any length (a 5000-character Eps(w) expression)."""
+    terms = " + ".join(["0.001"] * 1000)
+    G = buffem.SWGGeometry(geo(tmp_path, f"MATERIAL Long\n Eps(w) = 1 + {terms}\nENDMATERIAL\n" + obj(sphere(2), mat="Long")))
+    assert abs(G.material_eps(0, 1.0) - 2.0) < 1e-12
