@@ -131,3 +131,21 @@ def test_get_fields_rejects_bad_arguments(buffem_lib, ref_mesh):
     assert L.bg_get_fields(G.h, 1.0, 0.0, None, None, None, 0, None, None) == 0
     with pytest.raises(ValueError):
         G.GetFields(None, np.zeros(G.TotalBFs + 1, complex), 1.0, X)
+
+
+def test_neq_entry_points_reject_bad_arguments(buffem_lib, ref_mesh):
+    """buff-neq's entry points check their arguments before any device work."""
+    L = buffem_lib.lib()
+    G = buffem.SWGGeometry(meshfiles=ref_mesh("sphere48"), materials=buffem.Material(eps=4.0))
+    out = C.c_void_p()
+    flux = np.zeros(8)
+    assert L.bg_neq_create(None, C.byref(out)) == buffem_lib.BG_ERR_ARG
+    assert L.bg_neq_create(G.h, None) == buffem_lib.BG_ERR_ARG
+    assert L.bg_neq_flux(None, 1.0, 0.0, flux.ctypes.data_as(C.c_void_p)) == buffem_lib.BG_ERR_ARG
+    assert L.bg_neq_dressed_rytov(None, 1.0, 0.0, 0, flux.ctypes.data_as(C.c_void_p)) == buffem_lib.BG_ERR_ARG
+    dr = np.zeros(2)
+    p = lambda a: a.ctypes.data_as(C.c_void_p)
+    assert L.bg_pft_dr_device(None, 1.0, 0.0, p(dr), 10, p(flux)) == buffem_lib.BG_ERR_ARG
+    assert L.bg_pft_dr_device(G.h, 0.0, 0.0, p(dr), G.TotalBFs, p(flux)) == buffem_lib.BG_ERR_ARG
+    assert L.bg_pft_dr_device(G.h, 1.0, 0.0, p(dr), G.TotalBFs - 1, p(flux)) == buffem_lib.BG_ERR_ARG
+    L.bg_neq_destroy(None)
