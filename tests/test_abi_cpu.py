@@ -149,3 +149,37 @@ def test_neq_entry_points_reject_bad_arguments(buffem_lib, ref_mesh):
     assert L.bg_pft_dr_device(G.h, 0.0, 0.0, p(dr), G.TotalBFs, p(flux)) == buffem_lib.BG_ERR_ARG
     assert L.bg_pft_dr_device(G.h, 1.0, 0.0, p(dr), G.TotalBFs - 1, p(flux)) == buffem_lib.BG_ERR_ARG
     L.bg_neq_destroy(None)
+
+
+NULL_PROBE = r"""
+import re, sys
+sys.path.insert(0, sys.argv[1])
+import buffem
+L = buffem.lib()
+src = open(sys.argv[2]).read().replace("\n", " ")
+for fn, args in sorted(re.findall(r"L\.(bg_[a-z0-9_]+)\.argtypes = \[([^\]]*)\]", src)):
+    parts = [a.strip() for a in re.split(r",(?![^\[]*\])", args) if a.strip()]
+    vals = [0 if a in ("I", "C.c_int", "C.c_ulonglong") else 1.0 if a == "D" else None for a in parts]
+    r = getattr(L, fn)(*vals)
+    print(fn, r, flush=True)
+"""
+
+
+def test_every_entry_point_rejects_null_arguments(buffem_lib, tmp_path):
+    """Every entry point called with null handles and pointers returns an
+    error status (void destroy functions return) instead of crashing, on a
+    machine without a GPU (where a call that gets as far as the device
+    returns the no-device status); run in a child process so a crash fails
+    the test rather than the session."""
+    import subprocess
+    import sys
+    script = tmp_path / "probe.py"
+    script.write_text(NULL_PROBE)
+    binding = os.path.join(ROOT, "buff-em_b200", "buffem.py")
+    r = subprocess.run([sys.executable, str(script), os.path.join(ROOT, "buff-em_b200"), binding],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    results = dict(line.split() for line in r.stdout.strip().splitlines())
+    assert len(results) >= 60
+    for fn, ret in results.items():
+        assert ret == "None" if fn.endswith("_destroy") else int(ret) < 0, (fn, ret)
