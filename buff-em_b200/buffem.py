@@ -70,7 +70,7 @@ EXPORTS = [
     "bg_last_error", "bg_geometry_create", "bg_geometry_create_objects", "bg_geometry_destroy",
     "bg_geometry_num_bfs", "bg_geometry_num_objects", "bg_geometry_bf_offset", "bg_geometry_faces",
     "bg_geometry_vertices", "bg_geometry_object_index", "bg_geometry_object_label", "bg_geometry_material_eps",
-    "bg_trans_file_count", "bg_trans_file_tag", "bg_geometry_create_transformed",
+    "bg_trans_file_count", "bg_trans_file_tag", "bg_geometry_create_transformed", "bg_geometry_material_tensor",
     "bg_geometry_precompute", "bg_geometry_set_singular_order", "bg_geometry_near_data",
     "bg_matrix_create", "bg_matrix_destroy", "bg_assemble", "bg_matrix_download", "bg_matrix_upload",
     "bg_matrix_device_ptr", "bg_lu_factor", "bg_lu_pivots", "bg_lu_solve", "bg_lu_solve_device",
@@ -108,6 +108,7 @@ def lib():
         L.bg_geometry_object_index.argtypes = [P, C.c_char_p]
         L.bg_geometry_object_label.argtypes = [P, I, C.c_char_p, I]
         L.bg_geometry_material_eps.argtypes = [P, I, D, D, VP]
+        L.bg_geometry_material_tensor.argtypes = [P, I, D, D, VP, VP]
         L.bg_trans_file_count.argtypes = [C.c_char_p]
         L.bg_trans_file_tag.argtypes = [C.c_char_p, I, C.c_char_p, I]
         L.bg_geometry_create_transformed.argtypes = [C.c_char_p, C.c_char_p, I, C.POINTER(P)]
@@ -329,6 +330,15 @@ class SWGGeometry:
         e = np.zeros(2)
         _check(lib().bg_geometry_material_eps(self.h, obj, omega.real, omega.imag, _ptr(e)))
         return complex(e[0], e[1])
+
+    def material_tensor(self, obj, omega, x=(0.0, 0.0, 0.0)):
+        """3x3 complex permittivity tensor of object obj at Omega and point x
+        (SVTensor::Evaluate)."""
+        omega = complex(omega)
+        X = np.ascontiguousarray(x, dtype=np.float64)
+        Q = np.zeros(18)
+        _check(lib().bg_geometry_material_tensor(self.h, obj, omega.real, omega.imag, _ptr(X), _ptr(Q)))
+        return (Q[0::2] + 1j * Q[1::2]).reshape(3, 3)
 
     def label(self, obj=0):
         n = _check(lib().bg_geometry_object_label(self.h, obj, None, 0))

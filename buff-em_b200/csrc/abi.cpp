@@ -3,6 +3,7 @@
 // kernels.  No exception crosses the ABI; errors are status codes plus a
 // thread-local message.
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -130,7 +131,7 @@ static int check_material(const bg_material &m) {
 // as SWGVolume's constructor does without one)
 static int create_objects(int nobj, const char *const *meshfiles, const double *xf, const bg_material *materials,
                           const std::string *labels, const std::shared_ptr<const MatPropFn> *matprops,
-                          bg_geometry **out) {
+                          const std::shared_ptr<const SVTensorFn> *svts, bg_geometry **out) {
   *out = nullptr;
   bg_geometry *g = new (std::nothrow) bg_geometry();
   if (!g) { set_error("out of host memory"); return BG_ERR_NOMEM; }
@@ -146,6 +147,10 @@ static int create_objects(int nobj, const char *const *meshfiles, const double *
       g->objs[i].matprop = matprops[i];
       g->dispersive = true;
     }
+    if (svts && svts[i]) {
+      g->objs[i].svt = svts[i];
+      g->dispersive = true;
+    }
   }
   int st = finish_geometry(g);
   if (st) { delete g; return st; }
@@ -156,14 +161,14 @@ static int create_objects(int nobj, const char *const *meshfiles, const double *
 int bg_geometry_create_objects(int nobj, const char *const *meshfiles, const double *displacements,
                                const bg_material *materials, bg_geometry **out) {
   if (!out || nobj <= 0 || !meshfiles || !materials) { set_error("bg_geometry_create_objects: bad arguments"); return BG_ERR_ARG; }
-  if (!displacements) return create_objects(nobj, meshfiles, nullptr, materials, nullptr, nullptr, out);
+  if (!displacements) return create_objects(nobj, meshfiles, nullptr, materials, nullptr, nullptr, nullptr, out);
   std::vector<double> xf(12 * (size_t)nobj, 0.0);
   for (int i = 0; i < nobj; i++) {
     double *x = &xf[12 * (size_t)i];
     x[0] = x[4] = x[8] = 1.0;
     for (int k = 0; k < 3; k++) x[9 + k] = displacements[3 * i + k];
   }
-  return create_objects(nobj, meshfiles, xf.data(), materials, nullptr, nullptr, out);
+  return create_objects(nobj, meshfiles, xf.data(), materials, nullptr, nullptr, nullptr, out);
 }
 
 static int create_from_objects(std::vector<GeoObject> &objs, bg_geometry **out);
@@ -221,14 +226,17 @@ static int create_from_objects(std::vector<GeoObject> &objs, bg_geometry **out) 
   std::vector<bg_material> mats;
   std::vector<std::string> labels;
   std::vector<std::shared_ptr<const MatPropFn>> matprops;
+  std::vector<std::shared_ptr<const SVTensorFn>> svts;
   for (auto &o : objs) {
     names.push_back(o.mesh.c_str());
     xf.insert(xf.end(), o.xf, o.xf + 12);
     mats.push_back(o.mat);
     labels.push_back(o.label);
     matprops.push_back(o.matprop);
+    svts.push_back(o.svt);
   }
-  return create_objects((int)objs.size(), names.data(), xf.data(), mats.data(), labels.data(), matprops.data(), out);
+  return create_objects((int)objs.size(), names.data(), xf.data(), mats.data(), labels.data(), matprops.data(),
+                        svts.data(), out);
 }
 
 static void dfree(void *p) { if (p) cudaFree(p); }
@@ -262,9 +270,54 @@ int bg_geometry_material_eps(const bg_geometry *g, int obj, double omega_re, dou
   }
   const Object &o = g->objs[obj];
   if (o.matprop) { matprop_eps(*o.matprop, omega_re, omega_im, eps); return 1; }
+  if (o.svt) {
+    set_error("bg_geometry_material_eps: object %d has a permittivity tensor (bg_geometry_material_tensor)", obj);
+    return BG_ERR_ARG;
+  }
   if (o.mat.kind == BG_MAT_CONST_ISO) { eps[0] = o.mat.eps[0]; eps[1] = o.mat.eps[1]; return 0; }
   set_error("bg_geometry_material_eps: object %d has a tensor or position-dependent permittivity", obj);
   return BG_ERR_ARG;
+}
+
+int bg_geometry_material_tensor(const bg_geometry *g, int obj, double omega_re, double omega_im, const double *x,
+                                double *Q) {
+  if (!g || !x || !Q || obj < 0 || obj >= (int)g->objs.size()) {
+    set_error("bg_geometry_material_tensor: bad arguments");
+    return BG_ERR_ARG;
+  }
+  const Object &o = g->objs[obj];
+  for (int k = 0; k < 18; k++) Q[k] = 0.0;
+  if (o.svt) { svtensor_eval(*o.svt, omega_re, omega_im, x, Q); return BG_OK; }
+  double e[2];
+  const bg_material &m = o.mat;
+  if (o.matprop) {
+    matprop_eps(*o.matprop, omega_re, omega_im, e);
+  } else if (m.kind == BG_MAT_CONST_TENSOR) {
+    // as the device evaluates it: off-diagonal pairs averaged
+    for (int k = 0; k < 18; k++) Q[k] = m.eps[k];
+    for (int a = 0; a < 3; a++) {
+      int b = (a + 1) % 3;
+      for (int c = 0; c < 2; c++) {
+        double avg = 0.5 * (Q[2 * (3 * a + b) + c] + Q[2 * (3 * b + a) + c]);
+        Q[2 * (3 * a + b) + c] = Q[2 * (3 * b + a) + c] = avg;
+      }
+    }
+    return BG_OK;
+  } else if (m.kind == BG_MAT_JANUS_Z) {
+    bool up = x[2] > m.center[2];
+    e[0] = up ? m.eps[0] : m.eps2[0];
+    e[1] = up ? m.eps[1] : m.eps2[1];
+  } else if (m.kind == BG_MAT_GAUSSIAN) {
+    double d0 = x[0] - m.center[0], d1 = x[1] - m.center[1], d2 = x[2] - m.center[2];
+    double gs = std::exp(-(d0 * d0 + d1 * d1 + d2 * d2) / (m.width * m.width));
+    e[0] = m.eps[0] + m.amp[0] * gs;
+    e[1] = m.eps[1] + m.amp[1] * gs;
+  } else {
+    e[0] = m.eps[0];
+    e[1] = m.eps[1];
+  }
+  for (int a = 0; a < 3; a++) { Q[2 * (4 * a)] = e[0]; Q[2 * (4 * a) + 1] = e[1]; }
+  return BG_OK;
 }
 
 int bg_geometry_object_index(const bg_geometry *g, const char *label) {

@@ -202,6 +202,11 @@ int refresh_materials(bg_geometry *g, double wr, double wi) {
       o.mat = bg_material{};
       o.mat.kind = BG_MAT_CONST_ISO;
       matprop_eps(*o.matprop, wr, wi, o.mat.eps);
+    } else if (o.svt) {
+      const double x0[3] = {0.0, 0.0, 0.0};   // position-independent by construction
+      o.mat = bg_material{};
+      o.mat.kind = BG_MAT_CONST_TENSOR;
+      svtensor_eval(*o.svt, wr, wi, x0, o.mat.eps);
     }
     mats[i] = o.mat;
   }
@@ -559,10 +564,11 @@ static bool readable(const std::string &f) {
 // the reference's search path, SWGVolume.cc:101-107), then in each MESHPATH
 // directory of the file (SWGGeometry.cc:276-292, relative ones taken from the
 // .buffgeo file's directory), then in the working directory.
-static std::string find_mesh(const std::string &fn, const std::string &dir, const std::vector<std::string> &meshpath) {
+static std::string find_file(const std::string &fn, const std::string &dir, const char *env,
+                             const std::vector<std::string> &meshpath) {
   if (fn.empty() || fn[0] == '/') return fn;
   std::vector<std::string> cand{dir + "/" + fn};
-  if (const char *mp = std::getenv("BUFF_MESH_PATH")) {
+  if (const char *mp = std::getenv(env)) {
     std::string s = mp;
     size_t a = 0;
     while (a <= s.size()) {
@@ -579,6 +585,10 @@ static std::string find_mesh(const std::string &fn, const std::string &dir, cons
   return cand[0];
 }
 
+static std::string find_mesh(const std::string &fn, const std::string &dir, const std::vector<std::string> &meshpath) {
+  return find_file(fn, dir, "BUFF_MESH_PATH", meshpath);
+}
+
 // MATERIAL argument: CONST_EPS_<complex> or VACUUM; other names refer to
 // MATERIAL ... ENDMATERIAL sections of the file (matprop.cpp).  SVTENSOR files
 // (eps as expressions of position) are rejected; spatially varying
@@ -593,11 +603,9 @@ static bool parse_material(const std::string &M, bg_material &m) {
   return false;
 }
 
-typedef std::vector<std::pair<std::string, std::shared_ptr<const MatPropFn>>> MatDB;
-
 static int parse_object_lines(const std::vector<std::vector<std::string>> &lines, const std::vector<int> &lineno,
                               int endline, const char *path, const std::string &dir,
-                              const std::vector<std::string> &meshpath, const MatDB &db, GeoObject &o) {
+                              const std::vector<std::string> &meshpath, MatDB &db, GeoObject &o) {
   bool have_mesh = false, have_mat = false;
   std::string err;
   for (size_t l = 0; l < lines.size(); l++) {
@@ -607,8 +615,25 @@ static int parse_object_lines(const std::vector<std::vector<std::string>> &lines
       else { o.mesh = find_mesh(tok[1], dir, meshpath); have_mesh = true; }
     } else if (keyword_is(tok[0], "MATERIAL", "SVTENSOR")) {
       if (tok.size() != 2) err = tok[0] + " keyword requires one argument";
-      else if (keyword_is(tok[0], "SVTENSOR")) err = "SVTENSOR files are not supported";
-      else if (parse_material(tok[1], o.mat)) { o.matprop.reset(); have_mat = true; }
+      else if (keyword_is(tok[0], "SVTENSOR")) {
+        // SVTensor.cc:41-84: looked up along BUFF_SVTENSOR_PATH
+        std::shared_ptr<const SVTensorFn> t;
+        std::string file = find_file(tok[1], dir, "BUFF_SVTENSOR_PATH", {});
+        if (svtensor_parse_file(file, db, t)) return BG_ERR_IO;
+        if (svtensor_position_dependent(*t)) {
+          err = "SVTENSOR " + tok[1] + ": expressions of position (x, y, z, r, Theta, Phi) are not supported "
+                "(frequency-dependent tensors are)";
+        } else {
+          o.svt = t;
+          o.matprop.reset();
+          o.mat = bg_material{};
+          o.mat.kind = BG_MAT_CONST_TENSOR;
+          const double x0[3] = {0.0, 0.0, 0.0};
+          svtensor_eval(*t, 1.0, 0.0, x0, o.mat.eps);   // replaced by the tensor at Omega before every use
+          have_mat = true;
+        }
+      }
+      else if (parse_material(tok[1], o.mat)) { o.matprop.reset(); o.svt.reset(); have_mat = true; }
       else if (keyword_is(tok[1].substr(0, std::min<size_t>(10, tok[1].size())), "CONST_EPS_"))
         err = "bad permittivity " + tok[1];
       else {
@@ -617,6 +642,7 @@ static int parse_object_lines(const std::vector<std::vector<std::string>> &lines
         for (size_t k = db.size(); k-- > 0 && !have_mat;)
           if (keyword_is(tok[1], upper_case(db[k].first).c_str())) {
             o.matprop = db[k].second;
+            o.svt.reset();
             o.mat = bg_material{};
             o.mat.kind = BG_MAT_CONST_ISO;
             matprop_eps(*o.matprop, 1.0, 0.0, o.mat.eps);   // replaced by eps(Omega) before every use
@@ -752,7 +778,8 @@ int parse_buffgeo(const char *path, std::vector<GeoObject> &objs) {
     o.label = special[0][1];
     xf_identity(o.xf);
     std::vector<int> lineno(special.size(), 0);
-    int st = parse_object_lines(special, lineno, 0, path, ".", {}, MatDB{}, o);
+    MatDB none;
+    int st = parse_object_lines(special, lineno, 0, path, ".", {}, none, o);
     if (st) return st;
     objs.push_back(o);
     return BG_OK;

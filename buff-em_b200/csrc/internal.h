@@ -64,9 +64,12 @@ struct Face {
 // A MATERIAL ... ENDMATERIAL section: constants and Eps(w) (matprop.cpp).
 struct MatPropFn;
 
+struct SVTensorFn;
+
 struct Object {
   std::string meshfile, label;
   std::shared_ptr<const MatPropFn> matprop;   // frequency-dependent eps, or null
+  std::shared_ptr<const SVTensorFn> svt;      // frequency-dependent tensor (SVTENSOR file), or null
   int nv = 0, nt = 0, nif = 0, ntf = 0;
   std::vector<double> V;       // 3*nv (after displacement)
   std::vector<int> VI, FI;     // 4*nt each
@@ -88,6 +91,7 @@ struct GeoObject {
   std::string label, mesh;
   bg_material mat{};
   std::shared_ptr<const MatPropFn> matprop;   // MATERIAL naming a MATERIAL section
+  std::shared_ptr<const SVTensorFn> svt;      // SVTENSOR file
   double xf[12];
 };
 
@@ -97,6 +101,15 @@ int matprop_parse_section(const std::string &name, const std::vector<std::string
                           const std::vector<int> &lineno, const char *path, std::shared_ptr<const MatPropFn> &out);
 // eps(Omega), Omega in units of 3e14 rad/s, into eps[2] (re, im)
 void matprop_eps(const MatPropFn &m, double omega_re, double omega_im, double eps[2]);
+
+// MATERIAL sections seen so far in a geometry's files, in order
+typedef std::vector<std::pair<std::string, std::shared_ptr<const MatPropFn>>> MatDB;
+
+// An SVTENSOR file (matprop.cpp).  Parsing adds its MATERIAL sections to db.
+int svtensor_parse_file(const std::string &path, MatDB &db, std::shared_ptr<const SVTensorFn> &out);
+bool svtensor_position_dependent(const SVTensorFn &t);
+// the tensor at Omega and point x into Q (3x3 complex, row-major re/im)
+void svtensor_eval(const SVTensorFn &t, double omega_re, double omega_im, const double *x, double Q[18]);
 
 // Parses a .buffgeo file (SWGGeometry.cc:52-158, 214-383) or a special
 // MESH__<mesh>__MAT__<material> name (SWGGeometry.cc:167-209).

@@ -13,13 +13,24 @@
 // complex expressions evaluated once, in order, each able to use the ones
 // before it; Eps(w) is an expression of the angular frequency w in rad/s,
 // i.e. Omega times 3e14 (Omega in units of c / 1 um, the solver's unit).
-// Mu(w) is accepted and ignored (the VIE path is non-magnetic).  Expressions
+// Mu(w) is accepted and ignored (the VIE path is non-magnetic).
+//
+// SVTENSOR files (SVTensor.cc:41-300) give the permittivity tensor as
+// expressions "Eps = ...", "Q = ..." (isotropic) or "Qxy = ...", "EpsXY = ...",
+// "Eps12 = ..." per component, of w (rad/s, Omega x 3e14: SVTensor.cc:332),
+// x, y, z, r, Theta, Phi and MP_<name> (the eps of a MATERIAL section or a
+// CONST_EPS_ name at that frequency), with "NAME = number" constants and
+// MATERIAL sections of their own.  Components not given keep the identity;
+// off-diagonal pairs are averaged; Qyy and Qzz default to Qxx when only Qxx
+// is given (SVTensor.cc:344-372).  Expressions
 // use + - * / ^ (right-associative), unary signs, parentheses, numbers with
 // exponents, the constants i, pi and e, and the functions exp, log, sqrt,
 // sin, cos, tan, sinh, cosh, tanh, asin, acos, atan, abs.
+#include <algorithm>
 #include <cctype>
 #include <cmath>
 #include <complex>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <string>
@@ -51,6 +62,16 @@ struct MatPropFn {
   int eps_root = -1;
 };
 
+struct SVTensorFn {
+  std::string file;
+  std::vector<std::string> const_names;
+  std::vector<cplx> const_values;
+  std::vector<ExprNode> nodes;
+  int root[3][3];
+  std::vector<std::shared_ptr<const MatPropFn>> mps;   // Eps1, Eps2, Eps3
+  bool position = false;                               // uses x, y, z, r, Theta or Phi
+};
+
 namespace {
 
 struct Parser {
@@ -59,6 +80,7 @@ struct Parser {
   std::vector<ExprNode> &nodes;
   const std::vector<std::string> &names;  // constants visible to this expression
   bool allow_w;
+  const std::vector<std::string> *extra = nullptr;  // further variables (VAR -1, -2, ...)
   std::string err;
 
   Parser(const std::string &src, std::vector<ExprNode> &n, const std::vector<std::string> &nm, bool w)
@@ -179,6 +201,13 @@ struct Parser {
           n.var = (int)k + 1;
           return add(n);
         }
+      if (extra)
+        for (size_t k = 0; k < extra->size(); k++)
+          if ((*extra)[k] == id) {
+            ExprNode n{ExprNode::VAR};
+            n.var = -(int)k - 1;
+            return add(n);
+          }
       if (id == "w") {
         if (!allow_w) return fail("w may only appear in Eps(w) or Mu(w)");
         ExprNode n{ExprNode::VAR};
@@ -208,25 +237,26 @@ cplx ipow(cplx x, long n) {
   return inv ? cplx(1.0, 0.0) / r : r;
 }
 
-cplx eval(const std::vector<ExprNode> &nodes, int id, cplx w, const std::vector<cplx> &consts) {
+cplx eval(const std::vector<ExprNode> &nodes, int id, cplx w, const std::vector<cplx> &consts,
+          const cplx *extra = nullptr) {
   const ExprNode &n = nodes[id];
   switch (n.kind) {
     case ExprNode::NUM: return n.value;
-    case ExprNode::VAR: return n.var == 0 ? w : consts[n.var - 1];
-    case ExprNode::NEG: return cplx(0.0, 0.0) - eval(nodes, n.a, w, consts);   // -(4) is (-4, +0): sqrt(-4) = 2i
-    case ExprNode::ADD: return eval(nodes, n.a, w, consts) + eval(nodes, n.b, w, consts);
-    case ExprNode::SUB: return eval(nodes, n.a, w, consts) - eval(nodes, n.b, w, consts);
-    case ExprNode::MUL: return eval(nodes, n.a, w, consts) * eval(nodes, n.b, w, consts);
-    case ExprNode::DIV: return eval(nodes, n.a, w, consts) / eval(nodes, n.b, w, consts);
+    case ExprNode::VAR: return n.var == 0 ? w : n.var > 0 ? consts[n.var - 1] : extra[-n.var - 1];
+    case ExprNode::NEG: return cplx(0.0, 0.0) - eval(nodes, n.a, w, consts, extra);   // -(4) is (-4, +0): sqrt(-4) = 2i
+    case ExprNode::ADD: return eval(nodes, n.a, w, consts, extra) + eval(nodes, n.b, w, consts, extra);
+    case ExprNode::SUB: return eval(nodes, n.a, w, consts, extra) - eval(nodes, n.b, w, consts, extra);
+    case ExprNode::MUL: return eval(nodes, n.a, w, consts, extra) * eval(nodes, n.b, w, consts, extra);
+    case ExprNode::DIV: return eval(nodes, n.a, w, consts, extra) / eval(nodes, n.b, w, consts, extra);
     case ExprNode::POW: {
-      cplx x = eval(nodes, n.a, w, consts), y = eval(nodes, n.b, w, consts);
+      cplx x = eval(nodes, n.a, w, consts, extra), y = eval(nodes, n.b, w, consts, extra);
       // integer powers by repeated multiplication (wp^2 is then exact)
       if (y.imag() == 0.0 && y.real() == std::floor(y.real()) && std::fabs(y.real()) <= 64.0)
         return ipow(x, (long)y.real());
       return std::pow(x, y);
     }
     case ExprNode::FUN: {
-      cplx x = eval(nodes, n.a, w, consts);
+      cplx x = eval(nodes, n.a, w, consts, extra);
       switch (n.fun) {
         case 0: return std::exp(x);
         case 1: return std::log(x);
@@ -341,5 +371,196 @@ void matprop_eps(const MatPropFn &m, double omega_re, double omega_im, double ep
   eps[1] = v.imag();
 }
 
+
+// ---------------------------------------------------------------- SVTENSOR
+static const std::vector<std::string> kSvtVars = {"x", "y", "z", "r", "Theta", "Phi", "Eps1", "Eps2", "Eps3"};
+
+static bool uses_position(const std::vector<ExprNode> &nodes, int id) {
+  const ExprNode &n = nodes[id];
+  if (n.kind == ExprNode::VAR) return n.var < 0 && -n.var - 1 < 6;
+  bool r = false;
+  if (n.a >= 0) r = r || uses_position(nodes, n.a);
+  if (n.b >= 0) r = r || uses_position(nodes, n.b);
+  return r;
+}
+
+// MP_<name> -> Eps<k>, resolving <name> against the MATERIAL sections seen so
+// far (latest first, ignoring case) or a CONST_EPS_ / VACUUM name
+static bool replace_mps(std::string &expr, SVTensorFn &t, const MatDB &db, std::string &err) {
+  size_t p;
+  while ((p = expr.find("MP_")) != std::string::npos) {
+    size_t q = p + 3;
+    while (q < expr.size() && (std::isalnum((unsigned char)expr[q]) || expr[q] == '_' || expr[q] == '.' ||
+                               ((expr[q] == '+' || expr[q] == '-') && upper(expr.substr(p + 3, q - p - 3)).rfind("CONST_EPS_", 0) == 0)))
+      q++;
+    std::string name = expr.substr(p + 3, q - p - 3);
+    std::shared_ptr<const MatPropFn> fn;
+    for (size_t k = db.size(); k-- > 0 && !fn;)
+      if (upper(db[k].first) == upper(name)) fn = db[k].second;
+    if (!fn) {
+      std::string U = upper(name), body;
+      if (U == "VACUUM") body = "1";
+      else if (U.rfind("CONST_EPS_", 0) == 0) {
+        // <re>, <re>+<im>i, <re>-<im>i or <im>i, as in a CONST_EPS_ MATERIAL
+        const char *c0 = name.c_str() + 10;
+        char *e1, *e2;
+        double a = std::strtod(c0, &e1), b = 0.0;
+        bool ok = e1 != c0;
+        if (ok && (*e1 == 'i' || *e1 == 'j' || *e1 == 'I') && e1[1] == 0) { b = a; a = 0.0; }
+        else if (ok && *e1 != 0) {
+          b = std::strtod(e1, &e2);
+          ok = e2 != e1 && (*e2 == 'i' || *e2 == 'j' || *e2 == 'I') && e2[1] == 0;
+        }
+        if (ok) {
+          char tmp[96];
+          std::snprintf(tmp, sizeof tmp, "(%.17g) + (%.17g)*i", a, b);
+          body = tmp;
+        }
+      }
+      if (body.empty()) { err = "unknown material MP_" + name; return false; }
+      std::shared_ptr<const MatPropFn> c;
+      std::vector<std::string> lines{"Eps(w) = " + body};
+      std::vector<int> ln{0};
+      if (matprop_parse_section(name, lines, ln, "MP_", c)) { err = "bad material MP_" + name; return false; }
+      fn = c;
+    }
+    size_t k = 0;
+    while (k < t.mps.size() && t.mps[k] != fn) k++;
+    if (k == t.mps.size()) {
+      if (t.mps.size() == 3) { err = "too many MP_ statements (at most 3 materials)"; return false; }
+      t.mps.push_back(fn);
+    }
+    expr.replace(p, q - p, "Eps" + std::to_string(k + 1));
+  }
+  return true;
+}
+
+int svtensor_parse_file(const std::string &path, MatDB &db, std::shared_ptr<const SVTensorFn> &out) {
+  FILE *f = std::fopen(path.c_str(), "r");
+  if (!f) { set_error("could not find file %s", path.c_str()); return BG_ERR_IO; }
+  auto t = std::make_shared<SVTensorFn>();
+  t->file = path;
+  for (auto &r : t->root) for (int &x : r) x = -1;
+  std::vector<std::string> all;
+  {
+    std::string line;
+    char buf[1024];
+    while (std::fgets(buf, sizeof buf, f)) {
+      line += buf;
+      if (!line.empty() && line.back() == '\n') { line.pop_back(); all.push_back(line); line.clear(); }
+    }
+    if (!line.empty()) all.push_back(line);
+  }
+  std::fclose(f);
+  auto fail = [&](size_t l, const std::string &m) {
+    set_error("%s:%d: %s", path.c_str(), (int)l + 1, m.c_str());
+    return BG_ERR_IO;
+  };
+  for (size_t l = 0; l < all.size(); l++) {
+    std::string p = trim(all[l]);
+    if (p.empty() || p[0] == '#') continue;
+    size_t semi = p.find(';');
+    if (semi != std::string::npos) p = trim(p.substr(0, semi));
+    if (p.compare(0, 8, "MATERIAL") == 0 && (p.size() == 8 || std::isspace((unsigned char)p[8]))) {
+      std::string name = trim(p.substr(8));
+      if (name.empty()) return fail(l, "no name given for MATERIAL");
+      if (name.find_first_of(" \t") != std::string::npos) return fail(l, "syntax error");
+      std::vector<std::string> body;
+      std::vector<int> ln;
+      size_t e = l + 1;
+      while (e < all.size() && upper(trim(all[e])).compare(0, 11, "ENDMATERIAL") != 0) {
+        body.push_back(all[e]);
+        ln.push_back((int)e + 1);
+        e++;
+      }
+      if (e == all.size()) return fail(l, "MATERIAL without ENDMATERIAL");
+      std::shared_ptr<const MatPropFn> fn;
+      int st = matprop_parse_section(name, body, ln, path.c_str(), fn);
+      if (st) return st;
+      db.emplace_back(name, fn);
+      l = e;
+      continue;
+    }
+    size_t eq = p.find('=');
+    if (eq == std::string::npos) return fail(l, "syntax error");
+    std::string lhs = trim(p.substr(0, eq)), rhs = p.substr(eq + 1), L = upper(lhs);
+    int M = -1, N = -1;
+    std::string comp;
+    if (L == "Q" || L == "EPS") M = N = 0;
+    else if (L.size() == 3 && L[0] == 'Q') comp = L.substr(1);
+    else if (L.size() == 5 && L.compare(0, 3, "EPS") == 0) comp = L.substr(3);
+    if (!comp.empty()) {
+      int mn[2];
+      for (int k = 0; k < 2; k++) {
+        char c = comp[k];
+        if (c >= 'X' && c <= 'Z') mn[k] = c - 'X';
+        else if (c >= '1' && c <= '3') mn[k] = c - '1';
+        else return fail(l, "invalid component " + lhs);
+      }
+      M = mn[0]; N = mn[1];
+    }
+    if (M >= 0) {
+      std::string err;
+      if (!replace_mps(rhs, *t, db, err)) return fail(l, err);
+      Parser P(rhs, t->nodes, t->const_names, true);
+      P.extra = &kSvtVars;
+      int root = P.expr();
+      P.skip();
+      if (root >= 0 && P.p != rhs.size()) P.fail("junk after expression");
+      if (!P.err.empty()) return fail(l, P.err + " in " + trim(rhs));
+      for (int k = (int)t->mps.size(); k < 3; k++)
+        if (std::string(rhs).find("Eps" + std::to_string(k + 1)) != std::string::npos) return fail(l, "Eps" + std::to_string(k + 1) + " is not defined");
+      t->root[M][N] = root;
+      t->position = t->position || uses_position(t->nodes, root);
+      continue;
+    }
+    // NAME = number (SVTensor.cc:250-270)
+    char *end;
+    std::string v = trim(rhs);
+    double cv = std::strtod(v.c_str(), &end);
+    if (v.empty() || *end != 0) return fail(l, "invalid constant value");
+    if (lhs.empty() || !(std::isalpha((unsigned char)lhs[0]) || lhs[0] == '_')) return fail(l, "syntax error");
+    t->const_names.push_back(lhs);
+    t->const_values.push_back(cplx(cv, 0.0));
+  }
+  out = t;
+  return BG_OK;
+}
+
+bool svtensor_position_dependent(const SVTensorFn &t) { return t.position; }
+
+void svtensor_eval(const SVTensorFn &t, double wr, double wi, const double *x, double Q[18]) {
+  const double kFreqUnit = 3.0e14;
+  cplx v[9];
+  v[0] = x[0]; v[1] = x[1]; v[2] = x[2];
+  v[3] = std::sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+  v[4] = std::atan2(std::sqrt(x[0] * x[0] + x[1] * x[1]), x[2]);
+  v[5] = std::atan2(x[1], x[0]);
+  for (size_t k = 0; k < 3; k++) {
+    double e[2] = {1.0, 0.0};
+    if (k < t.mps.size()) matprop_eps(*t.mps[k], wr, wi, e);
+    v[6 + k] = cplx(e[0], e[1]);
+  }
+  cplx w(wr * kFreqUnit, wi * kFreqUnit), q[3][3];
+  for (int a = 0; a < 3; a++)
+    for (int b = 0; b < 3; b++) {
+      q[a][b] = (a == b) ? cplx(1.0, 0.0) : cplx(0.0, 0.0);
+      if (t.root[a][b] >= 0) q[a][b] = eval(t.nodes, t.root[a][b], w, t.const_values, v);
+    }
+  for (int a = 0; a < 3; a++) {
+    int b = (a + 1) % 3;
+    cplx avg = 0.5 * (q[a][b] + q[b][a]);
+    q[a][b] = q[b][a] = avg;
+  }
+  if (t.root[0][0] >= 0) {
+    if (t.root[1][1] < 0) q[1][1] = q[0][0];
+    if (t.root[2][2] < 0) q[2][2] = q[0][0];
+  }
+  for (int a = 0; a < 3; a++)
+    for (int b = 0; b < 3; b++) {
+      Q[2 * (3 * a + b)] = q[a][b].real();
+      Q[2 * (3 * a + b) + 1] = q[a][b].imag();
+    }
+}
 
 }  // namespace bg

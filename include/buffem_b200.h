@@ -74,7 +74,8 @@ const char *bg_last_error(void);
    constants and Eps(w), w in rad/s; used at every frequency the geometry is
    assembled at, except in bg_batch_sweep) and OBJECT <label> ... ENDOBJECT
    sections holding MESHFILE, MATERIAL (CONST_EPS_<value>, VACUUM or the name
-   of a MATERIAL section above) and any number of
+   of a MATERIAL section above) or SVTENSOR <file> (a permittivity tensor of
+   frequency; expressions of position are refused), and any number of
    DISPLACED dx dy dz / ROTATED theta ABOUT ax ay az lines, composed in order
    and applied to the mesh before its vertex merge (SWGGeometry.cc:52-158);
    the special name MESH__<mesh>__MAT__<material> stands for a one-object
@@ -120,6 +121,14 @@ int bg_geometry_bf_offset(const bg_geometry *g, int obj);
    for a frequency-dependent material, 0 for a constant one, or BG_ERR_ARG
    (tensor and position-dependent permittivities included). */
 int bg_geometry_material_eps(const bg_geometry *g, int obj, double omega_re, double omega_im, double *eps);
+
+/* The permittivity tensor of object obj at Omega and point x[3] into
+   Q[18] (3x3 complex, row-major, re/im), as the device evaluates it
+   (SVTensor::Evaluate, SVTensor.cc:306-373): SVTENSOR files, MATERIAL
+   sections, and the bg_material functors (constant tensors with their
+   off-diagonal pairs averaged). */
+int bg_geometry_material_tensor(const bg_geometry *g, int obj, double omega_re, double omega_im, const double *x,
+                                double *Q);
 
 /* SWGGeometry::GetObjectByLabel (SWGGeometry.cc:405-419): index of the first
    object whose label matches, ignoring case, or BG_ERR_ARG if none does.

@@ -148,7 +148,7 @@ def test_special_mesh_names(buffem_lib, sphere, tmp_path, monkeypatch):
     assert "no MATERIAL" in str(e.value)
     with pytest.raises(buffem.BuffError) as e:
         buffem.SWGGeometry("MESH__ball__SVT__eps")
-    assert "SVTENSOR" in str(e.value)
+    assert "could not find file" in str(e.value) and "eps.SVTensor" in str(e.value)
 
 
 @pytest.mark.parametrize("body,line,words", [
@@ -158,7 +158,6 @@ def test_special_mesh_names(buffem_lib, sphere, tmp_path, monkeypatch):
     ("OBJECT A\n MESHFILE m.vmsh\n MATERIAL CONST_EPS_2\n DISPLACED 1 x 3\nENDOBJECT\n", 4, "bad number"),
     ("OBJECT A\n MESHFILE m.vmsh\nENDOBJECT\n", 3, "no MATERIAL"),
     ("OBJECT A\n MATERIAL CONST_EPS_2\nENDOBJECT\n", 3, "no MESHFILE"),
-    ("OBJECT A\n MESHFILE m.vmsh\n SVTENSOR eps.SVTensor\nENDOBJECT\n", 3, "SVTENSOR"),
     ("OBJECT A\n MESHFILE m.vmsh\n MATERIAL CONST_EPS_4+0.2ix\nENDOBJECT\n", 3, "bad permittivity"),
     ("OBJECT A\n MESHFILE m.vmsh\n MATERIAL Gold\nENDOBJECT\n", 3, "unknown material Gold"),
     ("OBJECT A\n MESHFILE m.vmsh a\n MATERIAL CONST_EPS_2\nENDOBJECT\n", 2, "one argument"),
@@ -361,3 +360,113 @@ def test_long_lines(buffem_lib, sphere, tmp_path):
     terms = " + ".join(["0.001"] * 1000)
     G = buffem.SWGGeometry(geo(tmp_path, f"MATERIAL Long\n Eps(w) = 1 + {terms}\nENDMATERIAL\n" + obj(sphere(2), mat="Long")))
     assert abs(G.material_eps(0, 1.0) - 2.0) < 1e-12
+
+
+SVT = """# uniaxial crystal with a Drude-like ordinary axis
+MATERIAL Ordinary
+  wp = 6e14
+  Eps(w) = 4 - wp^2/(w*(w + 1e13*i))
+ENDMATERIAL
+EpsE = 2.5;
+Qxx = MP_Ordinary
+Qyy = MP_ordinary
+Qzz = EpsE + 0.5*i
+Qxy = 0.1*MP_CONST_EPS_2+1i
+EpsYX = 0.3
+Eps13 = w/3e14
+"""
+
+
+def svt_expected(omega):
+    w = complex(omega) * 3e14
+    eo = 4 - 36e28 / (w * (w + 1e13j))
+    q = np.zeros((3, 3), complex)
+    q[0, 0] = q[1, 1] = eo
+    q[2, 2] = 2.5 + 0.5j
+    q[0, 1] = q[1, 0] = 0.5 * (0.1 * (2 + 1j) + 0.3)
+    q[0, 2] = q[2, 0] = 0.5 * (w / 3e14 + 0.0)
+    return q
+
+
+def test_svtensor_files(buffem_lib, sphere, tmp_path):
+    """SVTENSOR files: MATERIAL sections and MP_ names, numeric constants,
+    the Q/Eps component spellings, identity defaults, averaged off-diagonal
+    pairs; the tensor at each frequency is what the device receives."""
+    (tmp_path / "uni.SVTensor").write_text(SVT)
+    G = buffem.SWGGeometry(geo(tmp_path, f"OBJECT A\n MESHFILE {sphere(2)}\n SVTENSOR uni.SVTensor\nENDOBJECT\n"))
+    for omega in (0.3, 1.0, 1.7 + 0.02j):
+        got = G.material_tensor(0, omega, (0.3, -0.2, 0.1))
+        assert np.allclose(got, svt_expected(omega), rtol=1e-14, atol=0), omega
+    with pytest.raises(buffem.BuffError) as e:
+        G.material_eps(0, 1.0)
+    assert "tensor" in str(e.value)
+
+
+@pytest.mark.parametrize("body,defaults", [
+    ("Eps = 3 + w/3e14\n", "iso"),
+    ("Q = 3 + w/3e14\n", "iso"),
+    ("Qxx = 3 + w/3e14\n", "iso"),
+    ("Qyy = 5\n", "yy"),
+])
+def test_svtensor_defaults(buffem_lib, sphere, tmp_path, body, defaults):
+    (tmp_path / "t.SVTensor").write_text(body)
+    G = buffem.SWGGeometry(geo(tmp_path, f"OBJECT A\n MESHFILE {sphere(2)}\n SVTENSOR t.SVTensor\nENDOBJECT\n"))
+    q = G.material_tensor(0, 0.5)
+    if defaults == "iso":
+        assert np.allclose(q, 3.5 * np.eye(3), rtol=0, atol=1e-15)
+    else:
+        assert np.allclose(q, np.diag([1, 5, 1]), rtol=0, atol=1e-15)
+
+
+@pytest.mark.parametrize("body,words", [
+    ("Eps = 2 + x\n", "expressions of position"),
+    ("Qxy = r*Theta\n", "expressions of position"),
+    ("Qxw = 1\n", "invalid component"),
+    ("Eps = MP_Nothing\n", "unknown material MP_Nothing"),
+    ("c = two\nEps = 1\n", "invalid constant value"),
+    ("just words\n", "syntax error"),
+    ("Eps = 1 +\n", "unexpected end"),
+    ("MATERIAL M\n Eps(w) = 2\n", "without ENDMATERIAL"),
+    ("Eps = MP_CONST_EPS_1 + MP_CONST_EPS_2 + MP_CONST_EPS_3 + MP_CONST_EPS_4\n", "too many MP_"),
+])
+def test_svtensor_errors(buffem_lib, sphere, tmp_path, body, words):
+    (tmp_path / "bad.SVTensor").write_text(body)
+    with pytest.raises(buffem.BuffError) as e:
+        buffem.SWGGeometry(geo(tmp_path, f"OBJECT A\n MESHFILE {sphere(2)}\n SVTENSOR bad.SVTensor\nENDOBJECT\n"))
+    assert words in str(e.value), str(e.value)
+
+
+def test_svtensor_lookup_path_and_shared_materials(buffem_lib, sphere, tmp_path, monkeypatch):
+    """SVTENSOR files are found along BUFF_SVTENSOR_PATH and may use MATERIAL
+    sections of the .buffgeo file (one material database, as MatProp's)."""
+    sub = tmp_path / "tensors"
+    sub.mkdir()
+    (sub / "m.SVTensor").write_text("Eps = 2*MP_Host\n")
+    monkeypatch.setenv("BUFF_SVTENSOR_PATH", str(sub))
+    body = "MATERIAL Host\n Eps(w) = 1.5 + 0.25*i\nENDMATERIAL\n" + \
+        f"OBJECT A\n MESHFILE {sphere(2)}\n SVTENSOR m.SVTensor\nENDOBJECT\n"
+    G = buffem.SWGGeometry(geo(tmp_path, body))
+    assert np.allclose(G.material_tensor(0, 1.0), (3 + 0.5j) * np.eye(3), rtol=0, atol=1e-15)
+
+
+def test_material_tensor_of_functor_materials(buffem_lib, sphere):
+    """bg_geometry_material_tensor restates the device's functors on the host."""
+    mesh = sphere(2)
+    T = np.array([[2, 0.4, 0], [0.2, 3, 0.1j], [0, 0.3j, 4]], complex)
+    cases = [
+        (buffem.Material(eps=4 + 0.2j), (0, 0, 0), (4 + 0.2j) * np.eye(3)),
+        (buffem.Material(kind=buffem.BG_MAT_CONST_TENSOR, tensor=T), (0, 0, 0), None),
+        (buffem.Material(kind=buffem.BG_MAT_JANUS_Z, eps=4, eps2=12 + 1j), (0, 0, 0.2), 4 * np.eye(3)),
+        (buffem.Material(kind=buffem.BG_MAT_JANUS_Z, eps=4, eps2=12 + 1j), (0, 0, -0.2), (12 + 1j) * np.eye(3)),
+        (buffem.Material(kind=buffem.BG_MAT_GAUSSIAN, eps=3 + 0.1j, amp=1.5, width=0.7, center=(0.1, 0, 0)),
+         (0.4, 0.2, -0.1), (3 + 0.1j + 1.5 * np.exp(-(0.09 + 0.04 + 0.01) / 0.49)) * np.eye(3)),
+    ]
+    for mat, x, ref in cases:
+        G = buffem.SWGGeometry(meshfiles=mesh, materials=mat)
+        q = G.material_tensor(0, 1.0, x)
+        if ref is None:
+            ref = T.copy()
+            for a in range(3):
+                b = (a + 1) % 3
+                ref[a, b] = ref[b, a] = 0.5 * (T[a, b] + T[b, a])
+        assert np.allclose(q, ref, rtol=1e-15, atol=1e-15), (mat.kind, q, ref)

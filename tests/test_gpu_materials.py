@@ -31,3 +31,18 @@ def test_dispersive_assembly_matches_constant(sphere, tmp_path):
         pa = G.GetPFTMatrix(J, omega, pw, method=buffem.BG_PFT_OVERLAP)
         pc = H.GetPFTMatrix(J, omega, pw, method=buffem.BG_PFT_OVERLAP)
         assert np.array_equal(pa, pc), omega
+
+
+@pytest.mark.gpu
+def test_svtensor_assembly_matches_constant_tensor(sphere, tmp_path):
+    """An SVTENSOR tensor of frequency: the matrix at each frequency equals
+    that of the same mesh with the constant tensor evaluated there."""
+    mesh = sphere(3)
+    (tmp_path / "t.SVTensor").write_text(DRUDE + "Qxx = MP_Metal\nQyy = 3 + 0.1*i\nQzz = 5\nQxy = 0.2*w/3e14\n")
+    p = tmp_path / "t.buffgeo"
+    p.write_text(f"OBJECT A\n MESHFILE {mesh}\n SVTENSOR t.SVTensor\nENDOBJECT\n")
+    G = buffem.SWGGeometry(str(p))
+    for omega in (0.9, 1.4):
+        T = G.material_tensor(0, omega)
+        H = buffem.SWGGeometry(meshfiles=mesh, materials=buffem.Material(kind=buffem.BG_MAT_CONST_TENSOR, tensor=T))
+        assert np.array_equal(G.AssembleVIEMatrix(omega).download(), H.AssembleVIEMatrix(omega).download()), omega
