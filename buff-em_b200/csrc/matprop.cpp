@@ -25,7 +25,8 @@
 // is given (SVTensor.cc:344-372).  Expressions
 // use + - * / ^ (right-associative), unary signs, parentheses, numbers with
 // exponents, the constants i, pi and e, and the functions exp, log, sqrt,
-// sin, cos, tan, sinh, cosh, tanh, asin, acos, atan, abs.
+// sin, cos, tan, sinh, cosh, tanh, asin, acos, atan, abs and step (0 for a
+// negative real part, else 1).
 #include <algorithm>
 #include <cctype>
 #include <cmath>
@@ -51,7 +52,7 @@ struct ExprNode {
 };
 
 static const char *kFuncs[] = {"exp", "log", "sqrt", "sin", "cos", "tan", "sinh", "cosh", "tanh",
-                               "asin", "acos", "atan", "abs"};
+                               "asin", "acos", "atan", "abs", "step"};
 static const int kNumFuncs = (int)(sizeof kFuncs / sizeof kFuncs[0]);
 
 struct MatPropFn {
@@ -270,7 +271,8 @@ cplx eval(const std::vector<ExprNode> &nodes, int id, cplx w, const std::vector<
         case 9: return std::asin(x);
         case 10: return std::acos(x);
         case 11: return std::atan(x);
-        default: return cplx(std::abs(x), 0.0);
+        case 12: return cplx(std::abs(x), 0.0);
+        default: return cplx(x.real() < 0.0 ? 0.0 : 1.0, 0.0);   // Heaviside step of the real part
       }
     }
   }

@@ -242,7 +242,7 @@ def test_material_sections(buffem_lib, sphere, tmp_path):
     ("-2^2", -4), ("2^3^2", 512), ("(1+2)*3-4/8", 8.5), ("2*-3", -6), ("-(1-3)", 2),
     ("exp(i*pi)", -1), ("sqrt(-4)", 2j), ("abs(3+4*i)", 5), ("cosh(0) + sinh(0) + tanh(0)", 1),
     ("log(e) + sin(0) + cos(0) + tan(0) + atan(0) + asin(0) + acos(1)", 2), ("1.5e3 + .5", 1500.5),
-    ("2^-1", 0.5), ("(1+i)^2", 2j), ("4^0.5", 2),
+    ("2^-1", 0.5), ("(1+i)^2", 2j), ("4^0.5", 2), ("step(-0.5) + 2*step(0) + 4*step(3)", 6),
 ])
 def test_material_expressions(buffem_lib, sphere, tmp_path, expr, value):
     G = buffem.SWGGeometry(geo(tmp_path, f"MATERIAL X\n Eps(w) = {expr}\nENDMATERIAL\n" + obj(sphere(2), mat="x")))
@@ -421,6 +421,8 @@ def test_svtensor_defaults(buffem_lib, sphere, tmp_path, body, defaults):
 @pytest.mark.parametrize("body,words", [
     ("Eps = 2 + x\n", "expressions of position"),
     ("Qxy = r*Theta\n", "expressions of position"),
+    ("MATERIAL In\n Eps(w) = 2\nENDMATERIAL\nEps = step(1.0-r)*MP_In + step(r-1.0)*MP_VACUUM\n",
+     "expressions of position"),
     ("Qxw = 1\n", "invalid component"),
     ("Eps = MP_Nothing\n", "unknown material MP_Nothing"),
     ("c = two\nEps = 1\n", "invalid constant value"),
