@@ -146,6 +146,15 @@ class SWGGeometry {
     return cdouble(e[0], e[1]);
   }
 
+  // the permittivity tensor of object no at Omega and point X
+  // (SVTensor::Evaluate, SVTensor.cc:306-373), for every kind of material
+  void GetEpsTensor(int no, cdouble Omega, const double X[3], cdouble Q[3][3]) const {
+    double q[18];
+    check(bg_geometry_material_tensor(g, no, Omega.real(), Omega.imag(), X, q));
+    for (int a = 0; a < 3; a++)
+      for (int b = 0; b < 3; b++) Q[a][b] = cdouble(q[2 * (3 * a + b)], q[2 * (3 * a + b) + 1]);
+  }
+
   // SWGGeometry::GetObjectByLabel (SWGGeometry.cc:405-419)
   SWGVolume *GetObjectByLabel(const char *Label, int *pno = nullptr) {
     if (pno) *pno = -1;

@@ -21,6 +21,10 @@ int main(int argc, char **argv) {
     std::printf("label %s %d\n", O->Label.c_str(), G.GetObjectByLabel(O->Label.c_str(), &no) == O ? no : -1);
     cdouble eps = G.GetEps(G.NumObjects - 1, cdouble(std::atof(argv[2]), 0.0));
     std::printf("eps %.17g %.17g\n", eps.real(), eps.imag());
+    const double X0[3] = {0.1, 0.2, 0.3};
+    cdouble Q[3][3];
+    G.GetEpsTensor(G.NumObjects - 1, cdouble(std::atof(argv[2]), 0.0), X0, Q);
+    std::printf("qzz %.17g %.17g\n", Q[2][2].real(), Q[2][2].imag());
     std::printf("last %d %d %.17g %.17g %.17g %.17g %.17g %.17g\n", O->NumVertices, O->NumInteriorFaces,
                 O->Origin[0], O->Origin[1], O->Origin[2], O->Vertices[0], O->Vertices[1], O->Vertices[2]);
     if (argc > 3 && !std::strcmp(argv[3], "geometry-only")) return 0;

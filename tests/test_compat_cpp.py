@@ -47,6 +47,8 @@ def test_compat_objects_carry_transformed_vertices(driver, sphere, tmp_path):
     eps = complex(*map(float, [ln for ln in r.stdout.splitlines() if ln.startswith("eps ")][0].split()[1:]))
     w = 0.5 * 3e14
     assert abs(eps - (1 - 9e28 / (w * (w + 1e13j)))) <= 1e-14 * abs(eps)
+    qzz = complex(*map(float, [ln for ln in r.stdout.splitlines() if ln.startswith("qzz ")][0].split()[1:]))
+    assert qzz == eps
     last = [ln for ln in r.stdout.splitlines() if ln.startswith("last ")][0].split()[1:]
     xyz, origin = buffem.SWGGeometry(str(p)).vertices(1)
     assert int(last[0]) == len(xyz) and int(last[1]) == 72
