@@ -72,7 +72,9 @@ EXPORTS = [
     "bg_geometry_vertices", "bg_geometry_object_index", "bg_geometry_object_label", "bg_geometry_material_eps",
     "bg_trans_file_count", "bg_trans_file_tag", "bg_geometry_create_transformed", "bg_geometry_material_tensor",
     "bg_geometry_precompute", "bg_geometry_set_singular_order", "bg_geometry_near_data",
+    "bg_geometry_set_singular_refine", "bg_geometry_singular_stats", "bg_geometry_singular_moments",
     "bg_matrix_create", "bg_matrix_destroy", "bg_assemble", "bg_matrix_download", "bg_matrix_upload",
+    "bg_matrix_get_rows",
     "bg_matrix_device_ptr", "bg_lu_factor", "bg_lu_pivots", "bg_lu_solve", "bg_lu_solve_device",
     "bg_rhs_planewave", "bg_rhs_planewave_device", "bg_pft", "bg_kernel_launch_count",
     "bg_synchronize", "bg_stream", "bg_profile_begin", "bg_profile_read", "bg_profile_end",
@@ -113,6 +115,9 @@ def lib():
         L.bg_trans_file_tag.argtypes = [C.c_char_p, I, C.c_char_p, I]
         L.bg_geometry_create_transformed.argtypes = [C.c_char_p, C.c_char_p, I, C.POINTER(P)]
         L.bg_geometry_set_singular_order.argtypes = [P, I]
+        L.bg_geometry_set_singular_refine.argtypes = [P, I, D, D]
+        L.bg_geometry_singular_stats.argtypes = [P, VP]
+        L.bg_geometry_singular_moments.argtypes = [P, C.POINTER(I), VP, VP, VP]
         L.bg_geometry_near_data.argtypes = [P, C.POINTER(I), VP, VP]
         L.bg_matrix_create.argtypes = [P, I, C.POINTER(P)]
         L.bg_matrix_destroy.argtypes = [P]
@@ -120,6 +125,7 @@ def lib():
         L.bg_assemble.argtypes = [P, D, D, P]
         L.bg_matrix_download.argtypes = [P, VP]
         L.bg_matrix_upload.argtypes = [P, VP]
+        L.bg_matrix_get_rows.argtypes = [P, I, VP, VP]
         L.bg_matrix_device_ptr.argtypes = [P, C.POINTER(VP), C.POINTER(I)]
         L.bg_lu_factor.argtypes = [P]
         L.bg_lu_pivots.argtypes = [P, VP]
@@ -235,6 +241,14 @@ class HMatrix:
         _check(lib().bg_matrix_download(self.h, _ptr(out)))
         return out
 
+    def rows(self, rows):
+        """Rows of the matrix, (len(rows), N), without downloading the rest."""
+        dt = np.complex128 if self.precision == BG_C128 else np.complex64
+        r = np.ascontiguousarray(rows, dtype=np.int32)
+        out = np.zeros((len(r), self.NC), dtype=dt)
+        _check(lib().bg_matrix_get_rows(self.h, len(r), _ptr(r), _ptr(out)))
+        return out
+
     def upload(self, A):
         dt = np.complex128 if self.precision == BG_C128 else np.complex64
         a = np.asfortranarray(A, dtype=dt)
@@ -278,7 +292,8 @@ class SWGGeometry:
     """Replaces buff::SWGGeometry (libbuff.h:200-272) for the VIE hot path."""
 
     def __init__(self, GeoFileName=None, meshfiles=None, materials=None, displacements=None,
-                 singular_order=None, TransFile=None, Transformation=0):
+                 singular_order=None, TransFile=None, Transformation=0, singular_refine=None,
+                 singular_tol=(1e-8, 1e-9)):
         h = C.c_void_p()
         if GeoFileName is not None and TransFile is not None:
             _check(lib().bg_geometry_create_transformed(GeoFileName.encode(), TransFile.encode(), int(Transformation),
@@ -303,6 +318,11 @@ class SWGGeometry:
         self.TotalBFs = lib().bg_geometry_num_bfs(h)
         self.NumObjects = lib().bg_geometry_num_objects(h)
         self.BFIndexOffset = [lib().bg_geometry_bf_offset(h, i) for i in range(self.NumObjects + 1)]
+        # the singular rule (TaylorDuffyTolerance's role): refined by default;
+        # singular_refine=False keeps the fixed rule of singular_order alone
+        if singular_refine is not None:
+            _check(lib().bg_geometry_set_singular_refine(h, 1 if singular_refine else 0, float(singular_tol[0]),
+                                                         float(singular_tol[1])))
         if singular_order is not None:
             _check(lib().bg_geometry_set_singular_order(h, int(singular_order)))
 
@@ -310,6 +330,26 @@ class SWGGeometry:
         if getattr(self, "h", None) and lib is not None:   # lib is None at interpreter exit
             lib().bg_geometry_destroy(self.h)
             self.h = None
+
+    def singular_stats(self):
+        """dict of the singular-pair statistics (bg_geometry_singular_stats)."""
+        out = np.zeros(6, dtype=np.int64)
+        _check(lib().bg_geometry_singular_stats(self.h, _ptr(out)))
+        keys = ("pairs", "refined", "fixed_points", "refine_points", "status", "refine_on")
+        return {k: int(v) for k, v in zip(keys, out)}
+
+    def singular_moments(self):
+        """(pairs (P, 4): row tet, column tet, common vertices, flags;
+        verts (P, 8): vertex indices, common first; moments (P, 24))."""
+        n = C.c_int()
+        _check(lib().bg_geometry_singular_moments(self.h, C.byref(n), None, None, None))
+        P = n.value
+        pairs = np.zeros((P, 4), dtype=np.int32)
+        verts = np.zeros((P, 8), dtype=np.int32)
+        mom = np.zeros((P, 24))
+        if P:
+            _check(lib().bg_geometry_singular_moments(self.h, C.byref(n), _ptr(pairs), _ptr(verts), _ptr(mom)))
+        return pairs, verts, mom
 
     def faces(self, obj=0):
         n = self.BFIndexOffset[obj + 1] - self.BFIndexOffset[obj]

@@ -248,7 +248,7 @@ void bg_geometry_destroy(bg_geometry *g) {
   dfree(d.bfQ); dfree(d.bfLoc); dfree(d.tetFI); dfree(d.bfV); dfree(d.bfArea); dfree(d.bfRadius); dfree(d.mats); dfree(d.objOrigin);
   dfree(d.tileTet); dfree(d.tileNT); dfree(d.bfTileLoc);
   NearData &n = g->near;
-  dfree(n.pairs); dfree(n.pairTP); dfree(n.fibbi); dfree(n.tp); dfree(n.tpOrdA); dfree(n.tpOrdB); dfree(n.tpMom);
+  dfree(n.pairs); dfree(n.pairTP); dfree(n.fibbi); dfree(n.tp); dfree(n.tpOrdA); dfree(n.tpOrdB); dfree(n.tpMom); dfree(n.tpFlag);
   dfree(g->graph.rowptr); dfree(g->graph.col); dfree(g->graph.etr);
   dfree(g->d_scratch);
   dfree(g->d_fieldTet); dfree(g->d_fieldFace);
@@ -364,8 +364,62 @@ int bg_geometry_faces(const bg_geometry *g, int obj, int *out) {
 
 int bg_geometry_set_singular_order(bg_geometry *g, int n) {
   if (!g || n < 2 || n > 16) { set_error("singular order must be in [2,16]"); return BG_ERR_ARG; }
+  if (g->sing_refine && n > 14) { set_error("with the refined singular rule the order must be in [2,14] (orders n and n+2 are used)"); return BG_ERR_ARG; }
   if (g->precomputed && n != g->singular_order) { set_error("singular order must be set before the precompute"); return BG_ERR_STATE; }
   g->singular_order = n;
+  return BG_OK;
+}
+
+int bg_geometry_set_singular_refine(bg_geometry *g, int on, double flag_tol, double tol) {
+  if (!g || (on != 0 && on != 1)) { set_error("bg_geometry_set_singular_refine: bad arguments"); return BG_ERR_ARG; }
+  if (on && !(flag_tol > 0.0 && tol > 0.0 && flag_tol < 1.0 && tol < 1.0)) {
+    set_error("bg_geometry_set_singular_refine: tolerances must be in (0, 1)");
+    return BG_ERR_ARG;
+  }
+  if (on && g->singular_order > 14) { set_error("with the refined singular rule the order must be in [2,14] (orders n and n+2 are used)"); return BG_ERR_ARG; }
+  bool same = (bool)on == g->sing_refine && (!on || (flag_tol == g->sing_flag_tol && tol == g->sing_tol));
+  if (g->precomputed && !same) { set_error("the singular rule must be set before the precompute"); return BG_ERR_STATE; }
+  g->sing_refine = on != 0;
+  if (on) { g->sing_flag_tol = flag_tol; g->sing_tol = tol; }
+  return BG_OK;
+}
+
+int bg_geometry_singular_stats(bg_geometry *g, long long *out) {
+  if (!g || !out) { set_error("bg_geometry_singular_stats: bad arguments"); return BG_ERR_ARG; }
+  int st = bg_geometry_precompute(g);
+  if (st) return st;
+  for (int i = 0; i < 6; i++) out[i] = g->sing_stats[i];
+  return BG_OK;
+}
+
+int bg_geometry_singular_moments(bg_geometry *g, int *count, int *pairs, int *verts, double *mom) {
+  if (!g || !count) { set_error("bg_geometry_singular_moments: bad arguments"); return BG_ERR_ARG; }
+  int st = bg_geometry_precompute(g);
+  if (st) return st;
+  const NearData &nd = g->near;
+  int ns = nd.ntp - nd.ntp_reg;
+  *count = ns;
+  if (ns <= 0) return BG_OK;
+  if (pairs) {
+    std::vector<int4> tp(ns);
+    std::vector<unsigned char> fl(ns);
+    BG_CUDA_TRY(cudaMemcpy(tp.data(), nd.tp + nd.ntp_reg, sizeof(int4) * ns, cudaMemcpyDeviceToHost));
+    BG_CUDA_TRY(cudaMemcpy(fl.data(), nd.tpFlag, (size_t)ns, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < ns; i++) {
+      pairs[4 * i] = tp[i].x; pairs[4 * i + 1] = tp[i].y; pairs[4 * i + 2] = tp[i].z; pairs[4 * i + 3] = fl[i];
+    }
+  }
+  if (verts) {
+    std::vector<int4> a(ns), b(ns);
+    BG_CUDA_TRY(cudaMemcpy(a.data(), nd.tpOrdA + nd.ntp_reg, sizeof(int4) * ns, cudaMemcpyDeviceToHost));
+    BG_CUDA_TRY(cudaMemcpy(b.data(), nd.tpOrdB + nd.ntp_reg, sizeof(int4) * ns, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < ns; i++) {
+      int *q = verts + 8 * i;
+      q[0] = a[i].x; q[1] = a[i].y; q[2] = a[i].z; q[3] = a[i].w;
+      q[4] = b[i].x; q[5] = b[i].y; q[6] = b[i].z; q[7] = b[i].w;
+    }
+  }
+  if (mom) BG_CUDA_TRY(cudaMemcpy(mom, nd.tpMom + 24 * (size_t)nd.ntp_reg, sizeof(double) * 24 * ns, cudaMemcpyDeviceToHost));
   return BG_OK;
 }
 
@@ -446,6 +500,19 @@ int bg_matrix_download(const bg_matrix *m, void *host) {
   size_t esz = m->precision == BG_C128 ? 16 : 8;
   BG_CUDA_TRY(cudaStreamSynchronize(stream()));
   BG_CUDA_TRY(cudaMemcpy2D(host, esz * m->N, m->d, esz * m->ld, esz * m->N, m->N, cudaMemcpyDeviceToHost));
+  return BG_OK;
+}
+
+int bg_matrix_get_rows(const bg_matrix *m, int nrows, const int *rows, void *host) {
+  if (!m || nrows < 0 || (nrows > 0 && (!rows || !host))) { set_error("bg_matrix_get_rows: bad arguments"); return BG_ERR_ARG; }
+  for (int k = 0; k < nrows; k++)
+    if (rows[k] < 0 || rows[k] >= m->N) { set_error("bg_matrix_get_rows: row %d out of range", rows[k]); return BG_ERR_ARG; }
+  size_t esz = m->precision == BG_C128 ? 16 : 8;
+  BG_CUDA_TRY(cudaStreamSynchronize(stream()));
+  // row r of the column-major matrix: N elements esz bytes wide, ld elements apart
+  for (int k = 0; k < nrows; k++)
+    BG_CUDA_TRY(cudaMemcpy2D((char *)host + esz * (size_t)m->N * k, esz, (const char *)m->d + esz * (size_t)rows[k],
+                             esz * m->ld, esz, m->N, cudaMemcpyDeviceToHost));
   return BG_OK;
 }
 

@@ -425,6 +425,8 @@ int build_near_lists(bg_geometry *g) {
   nd.npairs = (int)pairs.size();
   nd.ntp = ntp;
   nd.ntp_reg = nreg;
+  for (int i = 0; i < ntp; i++)
+    if (common[i] >= 2) nd.nsing_c[std::min(common[i], 4) - 2]++;
   int st;
   if ((st = dupload(&nd.pairs, pairs)) || (st = dupload(&nd.pairTP, pairTP)) || (st = dupload(&nd.tp, tpl)) ||
       (st = dupload(&nd.tpOrdA, ordA)) || (st = dupload(&nd.tpOrdB, ordB)))

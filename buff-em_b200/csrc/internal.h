@@ -169,6 +169,8 @@ struct NearData {
   int4 *tp = nullptr;          // (tA, tB, c, 0); singular pairs: vertex order in tpOrd
   int4 *tpOrdA = nullptr, *tpOrdB = nullptr;  // common-first vertex orders (global vertex ids)
   double *tpMom = nullptr;     // 24 moments per tet pair
+  int nsing_c[3] = {0, 0, 0};  // singular pairs with 2, 3, 4 common vertices (in that order after ntp_reg)
+  unsigned char *tpFlag = nullptr;  // per singular pair: bit 0 refined, bits 1-2 refinement status
 };
 
 // near-field graph of the basis functions for the learned preconditioner:
@@ -189,6 +191,12 @@ struct bg_geometry {
   bg::DevGeom dev;
   bg::NearData near;
   int singular_order = 10;
+  // refined singular rule (singular.cu): on by default; flag and box tolerances
+  bool sing_refine = true;
+  double sing_flag_tol = 1e-8, sing_tol = 1e-9;
+  // singular pairs, refined pairs, fixed-rule points, refinement points,
+  // refinement status bits (1: box pool full, 2: level limit), refinement on
+  long long sing_stats[6] = {0, 0, 0, 0, 0, 0};
   bool uploaded = false, precomputed = false;
   bool dispersive = false;      // some object's eps comes from a MATERIAL section
   bg::NearGraph graph;
@@ -225,6 +233,7 @@ namespace bg {
 int upload_geometry(bg_geometry *g);
 int build_near_lists(bg_geometry *g);
 int precompute_near(bg_geometry *g);
+int singular_precompute(bg_geometry *g);
 // fq (optional, device {Re w, Im w}): omega read on the device instead of wr, wi
 int assemble_far(bg_geometry *g, double wr, double wi, void *M, size_t ld, const double *fq = nullptr);
 int assemble_near(bg_geometry *g, double wr, double wi, void *M, size_t ld, const double *fq = nullptr);

@@ -26,9 +26,8 @@ namespace bg {
 // does not depend on which vertex is taken as origin.
 __constant__ double c_tcr16[64];
 __constant__ double c_tcr33[132];
-__constant__ double c_glx[16], c_glw[16];   // Gauss-Legendre on [0,1], current singular order
 static double h_tcr16[64], h_tcr33[132];
-static int s_tables_ok = 0, s_gl_n = 0;
+static int s_tables_ok = 0;
 
 static void fill_rule(double *dst, const char *pat, const double *vals, double w, int *np) {
   for (const char *p = pat; *p;) {
@@ -81,16 +80,6 @@ void gauss_legendre01(int n, double *x, double *w) {
     x[i] = 0.5 * (1.0 - z);
     w[i] = 1.0 / ((1.0 - z * z) * pp * pp);
   }
-}
-
-static int set_gl(int n) {
-  if (s_gl_n == n) return BG_OK;
-  double x[16] = {0}, w[16] = {0};
-  gauss_legendre01(n, x, w);
-  BG_CUDA_TRY(cudaMemcpyToSymbol(c_glx, x, sizeof x));
-  BG_CUDA_TRY(cudaMemcpyToSymbol(c_glw, w, sizeof w));
-  s_gl_n = n;
-  return BG_OK;
 }
 
 // ----------------------------------------------------------------- complex
@@ -462,128 +451,7 @@ __global__ void k_tp_regular(DevGeom g, const int4 *tp, int ntp, double *mom) {
     for (int i = 0; i < 24; i++) mom[24 * (size_t)warp + i] = acc[i];
 }
 
-// singular pairs (2..4 common vertices): relative-coordinate polar rule
-// (replaces the Taylor-Duffy call, GMatrixElements.cc:174-263,343-353).
-// Barycentrics lambda (A) and mu (B), common vertices first.  With
-// d = (lambda_k - mu_k | lambda_A-own | -mu_B-own), x - y is linear and
-// homogeneous in d; the admissible d form the polytope {sum d = 0,
-// |d|_1 <= 2} whose faces away from the origin are Delta_{p-1} x Delta_{q-1}
-// (one per sign pattern S of the common components).  For d = rho*zeta the
-// remaining common barycentrics span a (c-1)-simplex of size 1-rho, and
-//   dlambda dmu = rho^{m-1} (1-rho)^{c-1} drho dzeta dt,  m = 7-c,
-// with unit face Jacobian.  The t- and rho-integrals are closed-form Beta
-// integrals; zeta is integrated by collapsed Gauss-Legendre product rules.
-// One CTA per tetrahedron pair; origin o_A = o_B = first common vertex.
-#define SING_THREADS 256
-__device__ __forceinline__ double dfact(int n) {
-  double r = 1.0;
-  for (int i = 2; i <= n; i++) r *= i;
-  return r;
-}
-
-// point of Delta_k from k collapsed Gauss-Legendre digits; returns weight
-__device__ __forceinline__ double simplex_point(int k, const int *dig, double *y) {
-  if (k == 0) { y[0] = 1.0; return 1.0; }
-  if (k == 1) { double u = c_glx[dig[0]]; y[0] = u; y[1] = 1.0 - u; return c_glw[dig[0]]; }
-  if (k == 2) {
-    double u = c_glx[dig[0]], v = c_glx[dig[1]];
-    y[0] = u; y[1] = (1 - u) * v; y[2] = (1 - u) * (1 - v);
-    return c_glw[dig[0]] * c_glw[dig[1]] * (1 - u);
-  }
-  double u = c_glx[dig[0]], v = c_glx[dig[1]], w = c_glx[dig[2]];
-  y[0] = u; y[1] = (1 - u) * v; y[2] = (1 - u) * (1 - v) * w; y[3] = (1 - u) * (1 - v) * (1 - w);
-  return c_glw[dig[0]] * c_glw[dig[1]] * c_glw[dig[2]] * (1 - u) * (1 - u) * (1 - v);
-}
-
-__global__ void __launch_bounds__(SING_THREADS) k_tp_singular(DevGeom g, const int4 *tp, const int4 *ordA,
-                                                              const int4 *ordB, int first, double *mom, int n) {
-  int pidx = first + blockIdx.x;
-  int c = tp[pidx].z;
-  int4 oa = ordA[pidx], ob = ordB[pidx];
-  const int via[4] = {oa.x, oa.y, oa.z, oa.w}, vib[4] = {ob.x, ob.y, ob.z, ob.w};
-  double o[3];
-  load3(g.V4, via[0], o);
-  double VA[4][3], VB[4][3];
-  for (int i = 0; i < 4; i++) {
-    double t[3];
-    load3(g.V4, via[i], t);
-    for (int k = 0; k < 3; k++) VA[i][k] = t[k] - o[k];
-    load3(g.V4, vib[i], t);
-    for (int k = 0; k < 3; k++) VB[i][k] = t[k] - o[k];
-  }
-  int nn = c - 1, m = 7 - c, nown = 4 - c;
-  double ub[3] = {0, 0, 0}, s2 = 0, sv[3] = {0, 0, 0};
-  for (int i = 0; i < c; i++)
-    for (int k = 0; k < 3; k++) { sv[k] += VA[i][k]; s2 += VA[i][k] * VA[i][k]; }
-  for (int k = 0; k < 3; k++) ub[k] = sv[k] / (nn + 1);
-  double W = (s2 + sv[0] * sv[0] + sv[1] * sv[1] + sv[2] * sv[2]) / ((nn + 1.0) * (nn + 2.0));
-  double Gb[3][3];
-  for (int p = 0; p < 3; p++)
-    for (int j = 0; j < 3; j++) {
-      int a = m - 2 + p;  // a = m-1+(p-1)
-      Gb[p][j] = dfact(a + j) / dfact(a + j + nn + 1);
-    }
-  // faces: sign patterns S of the common components (c = 4 excludes 0 and 15)
-  int nfaces = (c == 4) ? 14 : (1 << c);
-  int per = 1;
-  for (int i = 0; i < 6 - c; i++) per *= n;
-  int total = nfaces * per;
-  double acc[24];
-#pragma unroll
-  for (int i = 0; i < 24; i++) acc[i] = 0.0;
-  for (int f = threadIdx.x; f < total; f += SING_THREADS) {
-    int face = f / per, rem = f % per;
-    int S = (c == 4) ? face + 1 : face;
-    int ns = __popc(S);
-    int p = ns + nown, q = (c - ns) + nown;
-    int dig[6];
-    for (int i = 0; i < 6 - c; i++) { dig[i] = rem % n; rem /= n; }
-    double al[4], be[4];
-    double w = simplex_point(p - 1, dig, al) * simplex_point(q - 1, dig + (p - 1), be);
-    double A1[3] = {0, 0, 0}, B1[3] = {0, 0, 0};
-    int ja = 0, jb = 0;
-    for (int k = 0; k < c; k++) {
-      if (S & (1 << k)) { double z = al[ja++]; for (int x = 0; x < 3; x++) A1[x] += z * VA[k][x]; }
-      else { double z = be[jb++]; for (int x = 0; x < 3; x++) B1[x] += z * VA[k][x]; }
-    }
-    for (int k = c; k < 4; k++) {
-      double za = al[ja++], zb = be[jb++];
-      for (int x = 0; x < 3; x++) { A1[x] += za * VA[k][x]; B1[x] += zb * VB[k][x]; }
-    }
-    double L0 = A1[0] - B1[0], L1 = A1[1] - B1[1], L2 = A1[2] - B1[2];
-    double R = sqrt(L0 * L0 + L1 * L1 + L2 * L2);
-    double AB = A1[0] * B1[0] + A1[1] * B1[1] + A1[2] * B1[2];
-    double uAB = ub[0] * (A1[0] + B1[0]) + ub[1] * (A1[1] + B1[1]) + ub[2] * (A1[2] + B1[2]);
-    double Rp[3] = {1.0 / R, 1.0, R};
-#pragma unroll
-    for (int pk = 0; pk < 3; pk++) {
-      double wr = w * Rp[pk];
-      double G0 = Gb[pk][0], G1 = Gb[pk][1], G2 = Gb[pk][2];
-      acc[8 * pk] += wr * G0;
-#pragma unroll
-      for (int x = 0; x < 3; x++) {
-        acc[8 * pk + 1 + x] += wr * (A1[x] * G1 + ub[x] * (G0 - G1));
-        acc[8 * pk + 4 + x] += wr * (B1[x] * G1 + ub[x] * (G0 - G1));
-      }
-      acc[8 * pk + 7] += wr * (AB * G2 + uAB * (G1 - G2) + W * (G0 - 2.0 * G1 + G2));
-    }
-  }
-  // deterministic block reduction
-  __shared__ double red[SING_THREADS / 32][24];
-  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-  for (int i = 0; i < 24; i++) {
-    double v = warp_sum(acc[i]);
-    if (lane == 0) red[wid][i] = v;
-  }
-  __syncthreads();
-  if (threadIdx.x < 24) {
-    double s = 0.0;
-    for (int w2 = 0; w2 < SING_THREADS / 32; w2++) s += red[w2][threadIdx.x];
-    const double gpre[3] = {0.25 / M_PI, 0.25 / M_PI, 0.125 / M_PI};
-    mom[24 * (size_t)pidx + threadIdx.x] = s * gpre[threadIdx.x / 8];
-  }
-}
+// singular pairs (2..4 common vertices): singular.cu (singular_precompute)
 
 // combine the 4 tetrahedron pairs of each near basis-function pair into the
 // 6 numbers of GetGME_TetTetInt(KERNEL_STATIC) (GMatrixElements.cc:295-365):
@@ -636,7 +504,6 @@ __global__ void k_fibbi_combine(DevGeom g, NearData nd) {
 
 int precompute_near(bg_geometry *g) {
   int st = init_tables();
-  if (!st) st = set_gl(g->singular_order);
   if (st) return st;
   NearData &nd = g->near;
   if (nd.ntp_reg > 0) {
@@ -644,12 +511,7 @@ int precompute_near(bg_geometry *g) {
     k_tp_regular<<<blocks, threads, 0, stream()>>>(g->dev, nd.tp, nd.ntp_reg, nd.tpMom);
     BG_LAUNCHED();
   }
-  int nsing = nd.ntp - nd.ntp_reg;
-  if (nsing > 0) {
-    k_tp_singular<<<nsing, SING_THREADS, 0, stream()>>>(g->dev, nd.tp, nd.tpOrdA, nd.tpOrdB, nd.ntp_reg, nd.tpMom,
-                                                        g->singular_order);
-    BG_LAUNCHED();
-  }
+  if ((st = singular_precompute(g))) return st;
   if (nd.npairs > 0) {
     k_fibbi_combine<<<(nd.npairs + 127) / 128, 128, 0, stream()>>>(g->dev, nd);
     BG_LAUNCHED();

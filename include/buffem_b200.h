@@ -163,6 +163,39 @@ int bg_geometry_faces(const bg_geometry *g, int obj, int *out);
 int bg_geometry_precompute(bg_geometry *g);
 int bg_geometry_set_singular_order(bg_geometry *g, int n);
 
+/* Replaces the statics SWGGeometry::TaylorDuffyTolerance / MaxTaylorDuffyEvals
+   (libbuff.h:254-255, set at SWGGeometry.cc:46-47) that bound the reference's
+   adaptive Taylor-Duffy integrals (TTaylorDuffy.cc:284-343) of tetrahedron
+   pairs sharing 2-4 vertices.  on = 1 (the default, flag_tol 1e-8, tol 1e-9):
+   every such pair is integrated with the singular rule at orders n and n+2
+   (n = the singular order, at most 14 here); where any of its 24 moments
+   differ by more than flag_tol of their scale, the face cubes are refined
+   level by level (6 Gauss points per dimension per box, boxes closed when a
+   split changes them by at most tol of the scale; at most 2048 open boxes per
+   level and 40 levels per pair).  on = 0: the fixed rule of order n alone.
+   Must be set before the first precompute (BG_ERR_STATE otherwise). */
+int bg_geometry_set_singular_refine(bg_geometry *g, int on, double flag_tol, double tol);
+
+/* Statistics of the singular pairs (runs the precompute if needed), 6 values:
+   [0] tetrahedron pairs sharing 2-4 vertices, [1] pairs refined,
+   [2] angular points of the fixed rules, [3] angular points of the
+   refinement, [4] status bits OR-ed over the pairs (1: a pair's box pool was
+   full, 2: a pair still had open boxes after the last level; its halves are
+   kept either way), [5] 1 if the refined rule is on. */
+int bg_geometry_singular_stats(bg_geometry *g, long long *out);
+
+/* The frequency-independent moments of the singular tetrahedron pairs as the
+   device keeps them (the tetrahedron-pair form of ComputeFIBBIData's
+   Taylor-Duffy branch, GMatrixElements.cc:343-353): *count pairs; per pair
+   pairs[4i..] = row tetrahedron, column tetrahedron, common vertices,
+   flags (bit 0 refined, bits 1-2 status); verts[8i..] = the two
+   tetrahedra's global vertex indices, common vertices first in the row
+   tetrahedron's order (CompareTets, SWGVolume.cc:357-400); mom[24i..] = per
+   kernel 1/(4 pi r), 1/(4 pi), r/(8 pi): int K, int K (x-o) (3),
+   int K (y-o) (3), int K (x-o).(y-o), unit-simplex measure, o = the first
+   common vertex.  Any output pointer may be NULL. */
+int bg_geometry_singular_moments(bg_geometry *g, int *count, int *pairs, int *verts, double *mom);
+
 /* Copies the 6 frequency-independent near-field numbers of every near
    basis-function pair: pairs[2*k] = a, pairs[2*k+1] = b (a <= b, global
    indices), data[6*k..6*k+5] (GMatrixElements.cc:404-420 ordering).
@@ -188,6 +221,10 @@ int bg_assemble(bg_geometry *g, double omega_re, double omega_im, bg_matrix *m);
    (or its LU factors after bg_lu_factor) to host memory, column-major,
    2*N*N doubles (BG_C128) or 2*N*N floats (BG_C64). */
 int bg_matrix_download(const bg_matrix *m, void *host);
+/* HMatrix::GetEntries for whole rows: rows[k] of the matrix (or of its
+   factors) into host row-major nrows x N (complex128 or complex64 as the
+   matrix), without copying the rest of the matrix. */
+int bg_matrix_get_rows(const bg_matrix *m, int nrows, const int *rows, void *host);
 /* Upload a host matrix (same layout) into m, e.g. for factoring user data. */
 int bg_matrix_upload(bg_matrix *m, const void *host);
 /* Device pointer and leading dimension of the storage (no copy). */

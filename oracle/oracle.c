@@ -222,6 +222,17 @@ typedef struct {
   OObj *O;
   int *off;
   int nang;      /* angular points per dimension of the singular rule */
+  /* refined singular rule (or_geom_set_singular_refine): Gauss points per
+     dimension of a refinement box, flag and box tolerances, and a table of
+     the ordered tetrahedron pairs sharing >= 2 vertices (sorted keys) whose
+     24 moments are computed on first use (state 0 none, 1 being written,
+     2 ready) */
+  int refine, rng;
+  double rflag, rtol;
+  long nsp;
+  unsigned long long *skey;
+  double *smom;
+  int *sstate, sstatus;
   /* warm near-field cache (the FIBBI cache of FIBBICache.cc:211-245, kept in
      memory for all same-object pairs with a common vertex): CSR over rows */
   int *crow, *ccol;
@@ -419,6 +430,7 @@ void or_geom_destroy(OGeom *G)
 {
   if (!G) return;
   free(G->crow); free(G->ccol); free(G->cdat);
+  free(G->skey); free(G->smom); free(G->sstate);
   for (int no = 0; no < G->no; no++) {
     OObj *O = G->O + no;
     for (int i = 0; i < O->ntf; i++) free(O->F[i]);
@@ -1134,22 +1146,24 @@ void or_sing_moments(int c, const double *VA, const double *VB, int n, double *o
 
 /* Refined moments: the scheme of or_sing_static_refined on the 24 moments,
    each measured against its kernel's scale (|M0|, |M0| h, |M0| h^2 for the
-   zeroth, first and second moments; h = diameter of A). */
-long or_sing_moments_refined(int c, const double *VA, const double *VB, int n, int ng, double flag_tol, double tol,
-                             double *out, int *status)
+   zeroth, first and second moments; h = diameter of A).  *peak receives the
+   largest number of boxes open at one level and *levels the number of
+   levels run (both 0 for an unflagged pair). */
+static long sing_moments_refined(const SingPair *X, int n, int ng, double flag_tol, double tol, double *out,
+                                 int *status, int *peak, int *levels)
 {
-  SingPair X;
-  double Q[3] = {0, 0, 0};
-  sing_pair_init(&X, c, (const double (*)[3])VA, (const double (*)[3])VB, Q, Q);
+  int c = X->c;
   double f0[24], f1[24];
   *status = 0;
-  sing_moments_fixed(&X, n, f0);
-  sing_moments_fixed(&X, n + 2, f1);
+  *peak = 0;
+  *levels = 0;
+  sing_moments_fixed(X, n, f0);
+  sing_moments_fixed(X, n + 2, f1);
   double h2 = 0.0;
   for (int i = 0; i < 4; i++)
     for (int j = 0; j < 4; j++) {
       double s2 = 0.0;
-      for (int x = 0; x < 3; x++) s2 += (X.VA[i][x] - X.VA[j][x]) * (X.VA[i][x] - X.VA[j][x]);
+      for (int x = 0; x < 3; x++) s2 += (X->VA[i][x] - X->VA[j][x]) * (X->VA[i][x] - X->VA[j][x]);
       h2 = fmax(h2, s2);
     }
   double h = sqrt(h2), scale[24];
@@ -1166,7 +1180,7 @@ long or_sing_moments_refined(int c, const double *VA, const double *VB, int n, i
     return 0;
   }
   SingAdapt A;
-  A.X = &X;
+  A.X = X;
   A.ng = ng;
   A.evals = 0;
   gauss_legendre01(ng, A.gx, A.gw);
@@ -1185,6 +1199,8 @@ long or_sing_moments_refined(int c, const double *VA, const double *VB, int n, i
   }
   for (int level = 0; level < SR_MAXLEVEL && ncur > 0; level++) {
     int nn = 0;
+    if (ncur > *peak) *peak = ncur;
+    *levels = level + 1;
     for (int bi = 0; bi < ncur; bi++) {
       MomBox *b = &cur[bi];
       int ns = __builtin_popcount(b->S);
@@ -1230,12 +1246,140 @@ long or_sing_moments_refined(int c, const double *VA, const double *VB, int n, i
   return A.evals;
 }
 
+long or_sing_moments_refined(int c, const double *VA, const double *VB, int n, int ng, double flag_tol, double tol,
+                             double *out, int *status)
+{
+  SingPair X;
+  double Q[3] = {0, 0, 0};
+  int peak, levels;
+  sing_pair_init(&X, c, (const double (*)[3])VA, (const double (*)[3])VB, Q, Q);
+  return sing_moments_refined(&X, n, ng, flag_tol, tol, out, status, &peak, &levels);
+}
+
+/* Many pairs at once (OpenMP over pairs): pair p has c[p] common vertices and
+   vertices VA[12p..], VB[12p..] (common first); out[24p..] its refined
+   moments; per pair the status bits, the angular points of the refinement,
+   the largest number of boxes open at one level and the levels run. */
+void or_sing_moments_refined_batch(int np, const int *c, const double *VA, const double *VB, int n, int ng,
+                                   double flag_tol, double tol, double *out, int *status, long *evals, int *peak,
+                                   int *levels)
+{
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int p = 0; p < np; p++) {
+    SingPair X;
+    double Q[3] = {0, 0, 0};
+    sing_pair_init(&X, c[p], (const double (*)[3])(VA + 12 * (size_t)p), (const double (*)[3])(VB + 12 * (size_t)p),
+                   Q, Q);
+    evals[p] = sing_moments_refined(&X, n, ng, flag_tol, tol, out + 24 * (size_t)p, status + p, peak + p,
+                                    levels + p);
+  }
+}
+
 /* public wrapper for tests: tets given by 4 vertices each (common first) */
 void or_sing_static(int c, const double *VA, const double *VB, const double *Q, const double *QP,
                     int nang, double *out)
 {
   sing_static(c, (const double (*)[3])VA, (const double (*)[3])VB, Q, QP, nang, out);
 }
+
+/* ------------------------------------------------------------------------- */
+/* Refined singular rule for a whole geometry: the moments of every ordered   */
+/* tetrahedron pair sharing >= 2 vertices, computed once on first use (the   */
+/* per-mesh table the GPU keeps), so that FIBBI data of the basis-function     */
+/* pairs reuse them.                                                          */
+/* ------------------------------------------------------------------------- */
+static unsigned long long sing_key(int no, int ta, int tb)
+{
+  return ((unsigned long long)no << 48) | ((unsigned long long)ta << 24) | (unsigned long long)tb;
+}
+
+static void sing_pair_moments(OGeom *G, int no, int ta, int tb, int ncv, double VA[4][3], double VB[4][3],
+                              double M[24])
+{
+  unsigned long long key = sing_key(no, ta, tb);
+  long lo = 0, hi = G->nsp - 1, at = -1;
+  while (lo <= hi) {
+    long mid = (lo + hi) / 2;
+    if (G->skey[mid] == key) { at = mid; break; }
+    if (G->skey[mid] < key) lo = mid + 1; else hi = mid - 1;
+  }
+  if (at >= 0 && __atomic_load_n(&G->sstate[at], __ATOMIC_ACQUIRE) == 2) {
+    memcpy(M, G->smom + 24 * (size_t)at, sizeof(double) * 24);
+    return;
+  }
+  SingPair X;
+  double Q0[3] = {0, 0, 0};
+  int status, peak, levels;
+  sing_pair_init(&X, ncv, (const double (*)[3])VA, (const double (*)[3])VB, Q0, Q0);
+  sing_moments_refined(&X, G->nang, G->rng, G->rflag, G->rtol, M, &status, &peak, &levels);
+  if (status) __atomic_fetch_or(&G->sstatus, status, __ATOMIC_RELAXED);
+  int expect = 0;
+  if (at >= 0 && __atomic_compare_exchange_n(&G->sstate[at], &expect, 1, 0, __ATOMIC_ACQ_REL, __ATOMIC_ACQUIRE)) {
+    memcpy(G->smom + 24 * (size_t)at, M, sizeof(double) * 24);
+    __atomic_store_n(&G->sstate[at], 2, __ATOMIC_RELEASE);
+  }
+}
+
+static int cmp_u64(const void *a, const void *b)
+{
+  unsigned long long x = *(const unsigned long long *)a, y = *(const unsigned long long *)b;
+  return x < y ? -1 : x > y;
+}
+
+/* on != 0: static integrals of tetrahedra sharing >= 2 vertices by the
+   refined rule (orders nang and nang + 2, box refinement with ng points per
+   dimension where they differ by more than flag_tol, boxes closed at tol);
+   on == 0: the fixed rule of order nang.  Clears the warm cache. */
+void or_geom_set_singular_refine(OGeom *G, int on, int ng, double flag_tol, double tol)
+{
+  free(G->crow); free(G->ccol); free(G->cdat);
+  G->crow = NULL; G->ccol = NULL; G->cdat = NULL;
+  free(G->skey); free(G->smom); free(G->sstate);
+  G->skey = NULL; G->smom = NULL; G->sstate = NULL; G->nsp = 0; G->sstatus = 0;
+  G->refine = on;
+  G->rng = ng; G->rflag = flag_tol; G->rtol = tol;
+  if (!on) return;
+  long cap = 0;
+  for (int no = 0; no < G->no; no++) cap += 64L * G->O[no].nt;
+  unsigned long long *keys = malloc(sizeof(unsigned long long) * (cap > 0 ? cap : 1));
+  long nk = 0;
+  for (int no = 0; no < G->no; no++) {
+    OObj *O = G->O + no;
+    int *vc = calloc(O->nv + 1, sizeof(int));
+    for (int t = 0; t < O->nt; t++)
+      for (int k = 0; k < 4; k++) vc[O->T[t].VI[k] + 1]++;
+    for (int v = 0; v < O->nv; v++) vc[v + 1] += vc[v];
+    int *fill = malloc(sizeof(int) * (O->nv + 1)), *inc = malloc(sizeof(int) * (vc[O->nv] + 1));
+    memcpy(fill, vc, sizeof(int) * (O->nv + 1));
+    for (int t = 0; t < O->nt; t++)
+      for (int k = 0; k < 4; k++) inc[fill[O->T[t].VI[k]]++] = t;
+    for (int t = 0; t < O->nt; t++)
+      for (int k = 0; k < 4; k++) {
+        int v = O->T[t].VI[k];
+        for (int i = vc[v]; i < vc[v + 1]; i++) {
+          int u = inc[i], com = 0;
+          for (int x = 0; x < 4; x++)
+            for (int y = 0; y < 4; y++) com += O->T[t].VI[x] == O->T[u].VI[y];
+          if (com < 2) continue;
+          if (nk == cap) { cap *= 2; keys = realloc(keys, sizeof(unsigned long long) * cap); }
+          keys[nk++] = sing_key(no, t, u);
+        }
+      }
+    free(vc); free(fill); free(inc);
+  }
+  qsort(keys, nk, sizeof *keys, cmp_u64);
+  long m = 0;
+  for (long i = 0; i < nk; i++)
+    if (m == 0 || keys[i] != keys[m - 1]) keys[m++] = keys[i];
+  G->skey = keys;
+  G->nsp = m;
+  G->smom = malloc(sizeof(double) * 24 * (size_t)(m > 0 ? m : 1));
+  G->sstate = calloc(m > 0 ? m : 1, sizeof(int));
+}
+
+/* OR of the refinement status bits seen so far (1: box pool full, 2: last
+   level reached with boxes open) */
+int or_geom_singular_status(OGeom *G) { return G->sstatus; }
 
 /* ------------------------------------------------------------------------- */
 /* FIBBI data: GetGME_TetTetInt(KERNEL_STATIC), GMatrixElements.cc:295-375     */
@@ -1264,14 +1408,32 @@ static void fibbi(OGeom *G, OObj *OA, int a, OObj *OB, int b, double out[6])
         double VA[4][3], VB[4][3];
         for (int i = 0; i < 4; i++)
           for (int k = 0; k < 3; k++) { VA[i][k] = OA->V[3 * OVIA[i] + k]; VB[i][k] = OB->V[3 * OVIB[i] + k]; }
-        double J[6];
-        sing_static(ncv, (const double (*)[3])VA, (const double (*)[3])VB, OA->V + 3 * qa, OB->V + 3 * qb,
-                    G->nang, J);
-        double vv = fabs(OA->T[ta].vol * OB->T[tb].vol);
-        const double gpre[3] = {1.0 / (4.0 * M_PI), 1.0 / (4.0 * M_PI), 1.0 / (8.0 * M_PI)};
-        for (int p = 0; p < 3; p++) {
-          tti[2 * p] = area * gpre[p] * J[2 * p] / (9.0 * vv);
-          tti[2 * p + 1] = area * gpre[p] * J[2 * p + 1] / vv;
+        if (G->refine) {
+          /* moments of the ordered pair (ta, tb) about its first common
+             vertex o, combined as M2 - q.M1' - q'.M1 + q.q' M0 with
+             q = Q - o, q' = Q' - o (the pair values times 9 |V_A||V_B| / 4) */
+          double M[24];
+          sing_pair_moments(G, (int)(OA - G->O), ta, tb, ncv, VA, VB, M);
+          const double *Q = OA->V + 3 * qa, *QP = OB->V + 3 * qb;
+          double q[3], qp[3];
+          for (int k = 0; k < 3; k++) { q[k] = Q[k] - VA[0][k]; qp[k] = QP[k] - VA[0][k]; }
+          for (int p = 0; p < 3; p++) {
+            const double *m = M + 8 * p;
+            double J = m[7] - (q[0] * m[4] + q[1] * m[5] + q[2] * m[6]) - (qp[0] * m[1] + qp[1] * m[2] + qp[2] * m[3]) +
+                       (q[0] * qp[0] + q[1] * qp[1] + q[2] * qp[2]) * m[0];
+            tti[2 * p] = 4.0 * area * J;
+            tti[2 * p + 1] = 36.0 * area * m[0];
+          }
+        } else {
+          double J[6];
+          sing_static(ncv, (const double (*)[3])VA, (const double (*)[3])VB, OA->V + 3 * qa, OB->V + 3 * qb,
+                      G->nang, J);
+          double vv = fabs(OA->T[ta].vol * OB->T[tb].vol);
+          const double gpre[3] = {1.0 / (4.0 * M_PI), 1.0 / (4.0 * M_PI), 1.0 / (8.0 * M_PI)};
+          for (int p = 0; p < 3; p++) {
+            tti[2 * p] = area * gpre[p] * J[2 * p] / (9.0 * vv);
+            tti[2 * p + 1] = area * gpre[p] * J[2 * p + 1] / vv;
+          }
         }
       }
       double s = (sa == sb) ? 1.0 : -1.0;

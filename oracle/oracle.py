@@ -17,6 +17,11 @@ _LIB = None
 
 MAT_CONST_ISO, MAT_CONST_TENSOR, MAT_JANUS_Z, MAT_GAUSSIAN = 0, 1, 2, 3
 
+# refined singular rule: fixed orders n and n + 2 (n = 10), refinement boxes
+# of 6 Gauss points per dimension where the two orders differ by more than
+# 1e-8 of a moment's scale, boxes closed when a split changes them by <= 1e-9
+REFINE_ORDER, REFINE_NG, REFINE_FLAG, REFINE_TOL = 10, 6, 1e-8, 1e-9
+
 
 class OMat(C.Structure):
     _fields_ = [("kind", C.c_int), ("eps", C.c_double * 18), ("eps2", C.c_double * 2),
@@ -79,6 +84,11 @@ def lib():
         L.or_sing_moments.argtypes = [I, dp, dp, I, dp]
         L.or_sing_moments_refined.argtypes = [I, dp, dp, I, I, D, D, dp, C.POINTER(I)]
         L.or_sing_moments_refined.restype = C.c_long
+        lp = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+        L.or_sing_moments_refined_batch.argtypes = [I, ip, dp, dp, I, I, D, D, dp, ip, lp, ip, ip]
+        L.or_geom_set_singular_refine.argtypes = [P, I, I, D, D]
+        L.or_geom_singular_status.argtypes = [P]
+        L.or_geom_singular_status.restype = I
         L.or_fibbi.argtypes = [P, I, I, dp]
         L.or_gme.argtypes = [P, I, I, D, D, dp]
         L.or_overlaps.argtypes = [P, I, D, ip, dp]
@@ -111,7 +121,7 @@ def lib():
 class Geometry:
     """Oracle geometry: a list of (mesh file, displacement, material) objects."""
 
-    def __init__(self, meshfiles, materials, displacements=None, nang=8):
+    def __init__(self, meshfiles, materials, displacements=None, nang=8, refine=False):
         L = lib()
         if isinstance(meshfiles, str):
             meshfiles = [meshfiles]
@@ -129,6 +139,8 @@ class Geometry:
         if not self.h:
             raise RuntimeError(L.or_last_error().decode())
         L.or_geom_set_nang(self.h, nang)
+        if refine:
+            L.or_geom_set_singular_refine(self.h, 1, REFINE_NG, REFINE_FLAG, REFINE_TOL)
         self.N = L.or_geom_nbf(self.h)
         self.nobj = L.or_geom_nobj(self.h)
         self.off = [L.or_geom_bf_offset(self.h, i) for i in range(self.nobj + 1)]
@@ -347,6 +359,21 @@ def sing_moments(c, VA, VB, n=10, refined=False, ng=6, flag_tol=1e-7, tol=1e-9):
     st = C.c_int()
     ne = lib().or_sing_moments_refined(c, A, B, n, ng, flag_tol, tol, out, C.byref(st))
     return out, ne, st.value
+
+
+def sing_moments_refined_batch(cs, VA, VB, n=REFINE_ORDER, ng=REFINE_NG, flag_tol=REFINE_FLAG, tol=REFINE_TOL):
+    """Refined moments of many pairs (cs: common-vertex counts, VA/VB: (P, 4, 3)
+    common-first vertices), OpenMP over pairs; returns (moments (P, 24),
+    status, angular points of the refinement, peak open boxes, levels)."""
+    cs = np.ascontiguousarray(cs, dtype=np.int32)
+    P = len(cs)
+    A = np.ascontiguousarray(VA, dtype=np.float64).reshape(-1)
+    B = np.ascontiguousarray(VB, dtype=np.float64).reshape(-1)
+    out = np.zeros(24 * P)
+    st, pk, lv = (np.zeros(P, dtype=np.int32) for _ in range(3))
+    ev = np.zeros(P, dtype=np.int64)
+    lib().or_sing_moments_refined_batch(P, cs, A, B, n, ng, flag_tol, tol, out, st, ev, pk, lv)
+    return out.reshape(P, 24), st, ev, pk, lv
 
 
 def moments_to_values(M, VA, VB, Q, QP):

@@ -12,7 +12,7 @@ import buffem
 
 pytestmark = pytest.mark.gpu
 
-ORDER = 6  # singular-rule order used on both sides to keep the oracle fast
+ORDER = 6  # fixed singular-rule order used on both sides to keep the oracle fast
 
 
 def entry_close(Mg, Mo, rtol=1e-10):
@@ -22,10 +22,14 @@ def entry_close(Mg, Mo, rtol=1e-10):
     return (not bad.any()), float((err / (np.abs(Mo) + 1e-13 * scale)).max())
 
 
-def pair(path_or_paths, mats_b, mats_o, disp=None, order=ORDER, oracle_lib=None):
+def pair(path_or_paths, mats_b, mats_o, disp=None, order=ORDER, oracle_lib=None, refine=False):
+    """GPU and oracle geometries with the same singular rule: the fixed rule
+    of the given order (refine=False, fast on the CPU) or the library's
+    default refined rule (orders 10 and 12 with box refinement)."""
     paths = [path_or_paths] if isinstance(path_or_paths, str) else path_or_paths
-    Gb = buffem.SWGGeometry(meshfiles=paths, materials=mats_b, displacements=disp, singular_order=order)
-    Go = oracle_lib.Geometry(paths, mats_o, displacements=disp, nang=order)
+    Gb = buffem.SWGGeometry(meshfiles=paths, materials=mats_b, displacements=disp, singular_order=order,
+                            singular_refine=refine)
+    Go = oracle_lib.Geometry(paths, mats_o, displacements=disp, nang=order, refine=refine)
     return Gb, Go
 
 
