@@ -271,8 +271,14 @@ int bg_geometry_material_eps(const bg_geometry *g, int obj, double omega_re, dou
   const Object &o = g->objs[obj];
   if (o.matprop) { matprop_eps(*o.matprop, omega_re, omega_im, eps); return 1; }
   if (o.svt) {
-    set_error("bg_geometry_material_eps: object %d has a permittivity tensor (bg_geometry_material_tensor)", obj);
-    return BG_ERR_ARG;
+    // the scalar SVTensor::Evaluate(Omega, x) returns the xx component
+    // (SVTensor.cc:375-380); SVTENSOR objects here depend on frequency only
+    double Q[18];
+    const double x0[3] = {0.0, 0.0, 0.0};
+    svtensor_eval(*o.svt, omega_re, omega_im, x0, Q);
+    eps[0] = Q[0];
+    eps[1] = Q[1];
+    return 1;
   }
   if (o.mat.kind == BG_MAT_CONST_ISO) { eps[0] = o.mat.eps[0]; eps[1] = o.mat.eps[1]; return 0; }
   set_error("bg_geometry_material_eps: object %d has a tensor or position-dependent permittivity", obj);
@@ -599,6 +605,8 @@ int bg_lu_solve_device(bg_matrix *m, void *dB, int ldb, int nrhs) {
 
 int bg_lu_solve_device_noalloc(bg_matrix *m, void *dB, int ldb, int nrhs) {
   if (!m || !dB || nrhs <= 0 || ldb < m->N) { set_error("bg_lu_solve_device_noalloc: bad arguments"); return BG_ERR_ARG; }
+  int st = lu_noalloc_check(m, nrhs);
+  if (st) return st;
   if (!m->factored) { set_error("bg_lu_solve_device_noalloc: matrix is not LU-factored"); return BG_ERR_STATE; }
   if (m->info > 0) { set_error("bg_lu_solve_device_noalloc: factorization is singular (info=%d)", m->info); return BG_ERR_NUMERIC; }
   return lu_solve_noalloc(m, dB, ldb, nrhs);

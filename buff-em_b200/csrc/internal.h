@@ -266,6 +266,8 @@ int lu_factor(bg_matrix *m);
 int lu_solve(bg_matrix *m, void *dB, int ldb, int nrhs);
 int lu_solve_status(bg_matrix *m);
 int lu_solve_noalloc(bg_matrix *m, void *dB, int ldb, int nrhs);
+// the allocation-free solve's size limits (BG_ERR_ARG with a message beyond them)
+int lu_noalloc_check(const bg_matrix *m, int nrhs);
 // capture-safe factor/solve (batched sweeps; complex128)
 int lu_capture_prepare(bg_matrix *m);
 int lu_factor_enqueue(bg_matrix *m);

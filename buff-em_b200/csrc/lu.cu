@@ -15,6 +15,8 @@
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
@@ -874,6 +876,7 @@ int lu_solve_status(bg_matrix *m) {
 #define NOALLOC_BYTES (4u << 20)
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
 static void *s_noalloc_ptr[64];
+static std::mutex s_noalloc_mu;
 
 // once per device, with that device current: the array's device address (the
 // host-side symbol is only a stand-in and must never be passed to a kernel)
@@ -881,6 +884,7 @@ static int noalloc_setup(void **ptr) {
   int dev = 0;
   BG_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) { set_error("device ordinal %d out of range", dev); return BG_ERR_CUDA; }
+  std::lock_guard<std::mutex> lock(s_noalloc_mu);
   if (!s_noalloc_ptr[dev]) {
     void *p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
@@ -917,8 +921,7 @@ static int getrs_noalloc(bg_matrix *m, C *B, size_t ldb, int nrhs, void *scratch
   return BG_OK;
 }
 
-int lu_solve_noalloc(bg_matrix *m, void *dB, int ldb, int nrhs) {
-  if (!m->d_perm) { set_error("solve: factorization state missing"); return BG_ERR_STATE; }
+int lu_noalloc_check(const bg_matrix *m, int nrhs) {
   size_t esz = m->precision == BG_C128 ? sizeof(cdl) : sizeof(cfl);
   if (nrhs > TV_MAXRHS) {
     set_error("allocation-free solve: at most %d right-hand sides per call (got %d)", TV_MAXRHS, nrhs);
@@ -929,6 +932,13 @@ int lu_solve_noalloc(bg_matrix *m, void *dB, int ldb, int nrhs) {
               (size_t)m->N * nrhs * esz, NOALLOC_BYTES);
     return BG_ERR_ARG;
   }
+  return BG_OK;
+}
+
+int lu_solve_noalloc(bg_matrix *m, void *dB, int ldb, int nrhs) {
+  int st0 = lu_noalloc_check(m, nrhs);
+  if (st0) return st0;
+  if (!m->d_perm) { set_error("solve: factorization state missing"); return BG_ERR_STATE; }
   void *scratch = nullptr;
   int st = noalloc_setup(&scratch);
   if (st) return st;

@@ -377,6 +377,20 @@ void matprop_eps(const MatPropFn &m, double omega_re, double omega_im, double ep
 // ---------------------------------------------------------------- SVTENSOR
 static const std::vector<std::string> kSvtVars = {"x", "y", "z", "r", "Theta", "Phi", "Eps1", "Eps2", "Eps3"};
 
+// the smallest k in 1..3 such that the expression reads Eps<k> although only
+// nmat MP_ materials exist (k > nmat), or 0
+static int uses_material_beyond(const std::vector<ExprNode> &nodes, int id, int nmat) {
+  if (id < 0) return 0;
+  const ExprNode &n = nodes[id];
+  if (n.kind == ExprNode::VAR && n.var < 0) {
+    int k = -n.var - 1 - 6 + 1;   // Eps1..Eps3 are extra variables 6..8
+    return (k >= 1 && k <= 3 && k > nmat) ? k : 0;
+  }
+  int a = uses_material_beyond(nodes, n.a, nmat), b = uses_material_beyond(nodes, n.b, nmat);
+  if (a && b) return std::min(a, b);
+  return a ? a : b;
+}
+
 static bool uses_position(const std::vector<ExprNode> &nodes, int id) {
   const ExprNode &n = nodes[id];
   if (n.kind == ExprNode::VAR) return n.var < 0 && -n.var - 1 < 6;
@@ -458,6 +472,15 @@ int svtensor_parse_file(const std::string &path, MatDB &db, std::shared_ptr<cons
     set_error("%s:%d: %s", path.c_str(), (int)l + 1, m.c_str());
     return BG_ERR_IO;
   };
+  // The whole file is read before any component expression is parsed
+  // (SVTensor.cc:88-113 sets every constant on every expression after
+  // parsing), so a constant or MATERIAL section may come after its use.
+  struct Component {
+    size_t line;
+    int M, N;
+    std::string rhs;
+  };
+  std::vector<Component> comps;
   for (size_t l = 0; l < all.size(); l++) {
     std::string p = trim(all[l]);
     if (p.empty() || p[0] == '#') continue;
@@ -502,18 +525,7 @@ int svtensor_parse_file(const std::string &path, MatDB &db, std::shared_ptr<cons
       M = mn[0]; N = mn[1];
     }
     if (M >= 0) {
-      std::string err;
-      if (!replace_mps(rhs, *t, db, err)) return fail(l, err);
-      Parser P(rhs, t->nodes, t->const_names, true);
-      P.extra = &kSvtVars;
-      int root = P.expr();
-      P.skip();
-      if (root >= 0 && P.p != rhs.size()) P.fail("junk after expression");
-      if (!P.err.empty()) return fail(l, P.err + " in " + trim(rhs));
-      for (int k = (int)t->mps.size(); k < 3; k++)
-        if (std::string(rhs).find("Eps" + std::to_string(k + 1)) != std::string::npos) return fail(l, "Eps" + std::to_string(k + 1) + " is not defined");
-      t->root[M][N] = root;
-      t->position = t->position || uses_position(t->nodes, root);
+      comps.push_back({l, M, N, rhs});
       continue;
     }
     // NAME = number (SVTensor.cc:250-270)
@@ -524,6 +536,22 @@ int svtensor_parse_file(const std::string &path, MatDB &db, std::shared_ptr<cons
     if (lhs.empty() || !(std::isalpha((unsigned char)lhs[0]) || lhs[0] == '_')) return fail(l, "syntax error");
     t->const_names.push_back(lhs);
     t->const_values.push_back(cplx(cv, 0.0));
+  }
+  for (const Component &c : comps) {
+    std::string rhs = c.rhs, err;
+    if (!replace_mps(rhs, *t, db, err)) return fail(c.line, err);
+    Parser P(rhs, t->nodes, t->const_names, true);
+    P.extra = &kSvtVars;
+    int root = P.expr();
+    P.skip();
+    if (root >= 0 && P.p != rhs.size()) P.fail("junk after expression");
+    if (!P.err.empty()) return fail(c.line, P.err + " in " + trim(rhs));
+    // Eps1..Eps3 (the MP_ materials, variables 7-9 of kSvtVars) beyond the
+    // materials named so far
+    int undefined = uses_material_beyond(t->nodes, root, (int)t->mps.size());
+    if (undefined) return fail(c.line, "Eps" + std::to_string(undefined) + " is not defined");
+    t->root[c.M][c.N] = root;
+    t->position = t->position || uses_position(t->nodes, root);
   }
   out = t;
   return BG_OK;

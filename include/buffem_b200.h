@@ -116,10 +116,12 @@ int bg_geometry_bf_offset(const bg_geometry *g, int obj);
 
 /* Permittivity of object obj at Omega (units of 3e14 rad/s) into eps[2]
    (re, im): a MATERIAL ... ENDMATERIAL section's Eps(w) at w = Omega x 3e14
-   rad/s (SVTensor::Evaluate -> MatProp::GetEps, SVTensor.cc:306-316), or the
-   constant of a CONST_EPS / VACUUM / constant isotropic object.  Returns 1
-   for a frequency-dependent material, 0 for a constant one, or BG_ERR_ARG
-   (tensor and position-dependent permittivities included). */
+   rad/s (SVTensor::Evaluate -> MatProp::GetEps, SVTensor.cc:306-316), the
+   xx component of an SVTENSOR object's tensor (the scalar SVTensor::Evaluate,
+   SVTensor.cc:375-380), or the constant of a CONST_EPS / VACUUM / constant
+   isotropic object.  Returns 1 for a frequency-dependent material, 0 for a
+   constant one, or BG_ERR_ARG (constant tensors and the eps(x) functors of
+   bg_geometry_create_objects: bg_geometry_material_tensor). */
 int bg_geometry_material_eps(const bg_geometry *g, int obj, double omega_re, double omega_im, double *eps);
 
 /* The permittivity tensor of object obj at Omega and point x[3] into

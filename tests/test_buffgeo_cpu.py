@@ -397,9 +397,23 @@ def test_svtensor_files(buffem_lib, sphere, tmp_path):
     for omega in (0.3, 1.0, 1.7 + 0.02j):
         got = G.material_tensor(0, omega, (0.3, -0.2, 0.1))
         assert np.allclose(got, svt_expected(omega), rtol=1e-14, atol=0), omega
-    with pytest.raises(buffem.BuffError) as e:
-        G.material_eps(0, 1.0)
-    assert "tensor" in str(e.value)
+    # the scalar query is the xx component (SVTensor::Evaluate(Omega, x),
+    # SVTensor.cc:375-380)
+    for omega in (0.3, 1.7 + 0.02j):
+        assert G.material_eps(0, omega) == pytest.approx(svt_expected(omega)[0, 0], rel=1e-14)
+
+
+def test_svtensor_reads_the_whole_file_first(buffem_lib, sphere, tmp_path):
+    """Constants and MATERIAL sections may follow the expressions that use
+    them (the reference parses the whole file, then sets every constant on
+    every expression: SVTensor.cc:88-113); a constant whose name contains
+    'Eps2' (MyEps2) is an ordinary constant."""
+    body = ("Qzz = A + 1\nQxx = MyEps2 * MP_Late\nA = 3\nMyEps2 = 0.5\n"
+            "MATERIAL Late\n Eps(w) = 4 + 2*i\nENDMATERIAL\n")
+    (tmp_path / "late.SVTensor").write_text(body)
+    G = buffem.SWGGeometry(geo(tmp_path, f"OBJECT A\n MESHFILE {sphere(2)}\n SVTENSOR late.SVTensor\nENDOBJECT\n"))
+    q = G.material_tensor(0, 1.0)
+    assert np.allclose(q, np.diag([2 + 1j, 2 + 1j, 4]), rtol=0, atol=1e-15)
 
 
 @pytest.mark.parametrize("body,defaults", [
@@ -430,6 +444,7 @@ def test_svtensor_defaults(buffem_lib, sphere, tmp_path, body, defaults):
     ("Eps = 1 +\n", "unexpected end"),
     ("MATERIAL M\n Eps(w) = 2\n", "without ENDMATERIAL"),
     ("Eps = MP_CONST_EPS_1 + MP_CONST_EPS_2 + MP_CONST_EPS_3 + MP_CONST_EPS_4\n", "too many MP_"),
+    ("Eps = MP_CONST_EPS_2 + Eps2\n", "Eps2 is not defined"),
 ])
 def test_svtensor_errors(buffem_lib, sphere, tmp_path, body, words):
     (tmp_path / "bad.SVTensor").write_text(body)

@@ -53,3 +53,26 @@ def test_noalloc_solve_rejects_sizes_beyond_its_scratch(sphere):
     st = buffem.lib().bg_lu_solve_device_noalloc(M.h, C.c_void_p(d.data_ptr()), N, 5)
     assert st == -1
     assert "at most 4" in buffem.lib().bg_last_error().decode()
+
+
+def test_noalloc_solve_rejects_more_bytes_than_its_scratch(tmp_path):
+    """N = 65,537 with 4 complex128 right-hand sides needs 4 MiB + 64 bytes,
+    just above the fixed array: rejected before any device work (the size is
+    checked before the factorization state, so the 69 GB matrix is only
+    allocated, never assembled or factored)."""
+    import torch
+    from test_gpu_parity import _chain_mesh
+    N = 65537
+    need = 16 * N * N
+    if torch.cuda.mem_get_info()[0] < need + (4 << 30):
+        pytest.skip("not enough free device memory for the N = 65,537 matrix")
+    path = str(tmp_path / "chain.vmsh")
+    _chain_mesh(path, N)
+    G = buffem.SWGGeometry(meshfiles=path, materials=buffem.Material(eps=2.0))
+    assert G.TotalBFs == N
+    M = G.AllocateVIEMatrix()
+    d = torch.zeros((4, N), dtype=torch.complex128, device="cuda")
+    st = buffem.lib().bg_lu_solve_device_noalloc(M.h, C.c_void_p(d.data_ptr()), N, 4)
+    assert st == -1
+    assert "exceeds its fixed" in buffem.lib().bg_last_error().decode()
+    del M
