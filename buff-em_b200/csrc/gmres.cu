@@ -152,17 +152,19 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int K>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(K) : "memory"); }
 
-#define SY_STAGES 3
+#define SY_STAGES 2
 // shared memory: per warp SY_STAGES stages of 4 columns x 256 rows (as 4 x 128
-// float4), then x of the tile's rows and columns; the direct sums of the four
-// warps reuse the stage buffers after the loop
+// float4), then x of the tile's columns.  x of the tile's rows is staged in
+// the stage buffers (read into registers before the first copy is issued)
+// and the direct sums of the four warps reuse them after the loop, so a
+// block needs 72 KB for 3 right-hand sides and three blocks fit on an SM.
 template <int NR>
 constexpr size_t sym_smem_bytes() {
-  return sizeof(float4) * 4 * SY_STAGES * 4 * 128 + sizeof(float2) * 2 * 256 * NR;
+  return sizeof(float4) * 4 * SY_STAGES * 4 * 128 + sizeof(float2) * 256 * NR;
 }
 
 template <int NR>
-__global__ void __launch_bounds__(128) k_gm_matvec_sym_c64(int N, const float4 *A, size_t lda2, const z2 *X,
+__global__ void __launch_bounds__(128, 3) k_gm_matvec_sym_c64(int N, const float4 *A, size_t lda2, const z2 *X,
                                                            size_t ldx, float2 *partial) {
   const int I = blockIdx.x, J = blockIdx.y;
   if (I > J) return;
@@ -170,8 +172,8 @@ __global__ void __launch_bounds__(128) k_gm_matvec_sym_c64(int N, const float4 *
   const int nr = min(256, N - r0), nc = min(256, N - c0);
   extern __shared__ __align__(16) unsigned char sym_smem[];
   float4 *stage = reinterpret_cast<float4 *>(sym_smem);                        // [4 warps][STAGES][4][128]
-  float2 (*xr)[NR] = reinterpret_cast<float2 (*)[NR]>(stage + 4 * SY_STAGES * 4 * 128);
-  float2 (*xc)[NR] = xr + 256;
+  float2 (*xr)[NR] = reinterpret_cast<float2 (*)[NR]>(sym_smem);              // in the stage buffers, until loaded
+  float2 (*xc)[NR] = reinterpret_cast<float2 (*)[NR]>(stage + 4 * SY_STAGES * 4 * 128);
   float2 (*dacc)[256][NR] = reinterpret_cast<float2 (*)[256][NR]>(sym_smem);  // [4][256][NR], after the loop
   for (int e = threadIdx.x; e < 256 * NR; e += 128) {
     int i = e / NR, j = e % NR;
@@ -197,6 +199,7 @@ __global__ void __launch_bounds__(128) k_gm_matvec_sym_c64(int N, const float4 *
       Yr[q][j] = make_float2(y.x, y.x);
       Yi[q][j] = make_float2(y.y, y.y);
     }
+  __syncthreads();   // x of the rows is in registers: the stage buffers are free
   // this lane's rows 64 k + 2 lane (+1): bytes of the pair that exist
   int nb[4];
 #pragma unroll
@@ -238,9 +241,10 @@ __global__ void __launch_bounds__(128) k_gm_matvec_sym_c64(int N, const float4 *
     float t[4][2 * NR];
 #pragma unroll
     for (int u = 0; u < 4; u++) {
-      float2 T[NR];
+      // transposed sums in two independent chains (even and odd rows)
+      float2 T0[NR], T1[NR];
 #pragma unroll
-      for (int jj = 0; jj < NR; jj++) T[jj] = make_float2(0.f, 0.f);
+      for (int jj = 0; jj < NR; jj++) T0[jj] = T1[jj] = make_float2(0.f, 0.f);
 #pragma unroll
       for (int k = 0; k < 4; k++) {
         float4 v = buf[u * 128 + lane + 32 * k];
@@ -254,16 +258,16 @@ __global__ void __launch_bounds__(128) k_gm_matvec_sym_c64(int N, const float4 *
           D[2 * k][jj] = __ffma2_rn(s0, xii, D[2 * k][jj]);
           D[2 * k + 1][jj] = __ffma2_rn(e1, xrr, D[2 * k + 1][jj]);
           D[2 * k + 1][jj] = __ffma2_rn(s1, xii, D[2 * k + 1][jj]);
-          T[jj] = __ffma2_rn(e0, Yr[2 * k][jj], T[jj]);
-          T[jj] = __ffma2_rn(s0, Yi[2 * k][jj], T[jj]);
-          T[jj] = __ffma2_rn(e1, Yr[2 * k + 1][jj], T[jj]);
-          T[jj] = __ffma2_rn(s1, Yi[2 * k + 1][jj], T[jj]);
+          T0[jj] = __ffma2_rn(e0, Yr[2 * k][jj], T0[jj]);
+          T0[jj] = __ffma2_rn(s0, Yi[2 * k][jj], T0[jj]);
+          T1[jj] = __ffma2_rn(e1, Yr[2 * k + 1][jj], T1[jj]);
+          T1[jj] = __ffma2_rn(s1, Yi[2 * k + 1][jj], T1[jj]);
         }
       }
 #pragma unroll
       for (int jj = 0; jj < NR; jj++) {
-        t[u][2 * jj] = T[jj].x;
-        t[u][2 * jj + 1] = T[jj].y;
+        t[u][2 * jj] = T0[jj].x + T1[jj].x;
+        t[u][2 * jj + 1] = T0[jj].y + T1[jj].y;
       }
     }
     if (trans) {

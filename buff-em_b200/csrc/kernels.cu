@@ -102,6 +102,29 @@ __device__ __forceinline__ cd expikr(cd k, double r) {
   return cd{m * c, m * s};
 }
 
+// exp(i x) for |x| <= 1: Taylor series of cos and sin at y = x/2 (terms to
+// y^15; the first omitted terms, y^16/16! and y^17/17!, are below 1e-18 for
+// |y| <= 1/2), then cos x = c^2 - s^2, sin x = 2 c s
+__device__ __forceinline__ cd expi_small(double x) {
+  double y = 0.5 * x, y2 = y * y;
+  double c = 1.0 - y2 * (1.0 / 182.0);   // 1/(13 * 14)
+  c = 1.0 - y2 * (1.0 / 132.0) * c;      // 1/(11 * 12)
+  c = 1.0 - y2 * (1.0 / 90.0) * c;
+  c = 1.0 - y2 * (1.0 / 56.0) * c;
+  c = 1.0 - y2 * (1.0 / 30.0) * c;
+  c = 1.0 - y2 * (1.0 / 12.0) * c;
+  c = 1.0 - y2 * 0.5 * c;
+  double sn = 1.0 - y2 * (1.0 / 210.0);  // 1/(14 * 15)
+  sn = 1.0 - y2 * (1.0 / 156.0) * sn;     // 1/(12 * 13)
+  sn = 1.0 - y2 * (1.0 / 110.0) * sn;
+  sn = 1.0 - y2 * (1.0 / 72.0) * sn;
+  sn = 1.0 - y2 * (1.0 / 42.0) * sn;
+  sn = 1.0 - y2 * (1.0 / 20.0) * sn;
+  sn = 1.0 - y2 * (1.0 / 6.0) * sn;
+  sn *= y;
+  return cd{c * c - sn * sn, 2.0 * c * sn};
+}
+
 // e^x - 1 - x - x^2/2: GetExpRelTable(x,3,3), GMatrixElements.cc:59-93 -- the
 // series from n=4 is stopped once |term|^2 < 1e-16 |sum|^2 (or n = 100).
 __device__ __forceinline__ cd exprel3(cd x) {
@@ -183,26 +206,37 @@ __device__ __forceinline__ double warp_sum(double v) {
 // phi = exp(ikr)/(4 pi r):
 //   M0 = sum phi, M1 = sum x~ phi, M1' = sum y~ phi, M2 = sum x~.y~ phi,
 //   entry += s s' A A' [M2/144 - M0/(16k^2) - q'.M1/144 - q.M1'/144 + q.q' M0/144].
-// The moments depend on the two tetrahedra only, and a tile of 16
-// consecutive basis functions touches about 16 distinct tetrahedra (face
+// The moments depend on the two tetrahedra only, and a tile of 32
+// consecutive basis functions touches about 29 distinct tetrahedra (face
 // numbering follows the mesh), so a CTA computes each distinct tetrahedron
-// pair of its 16x16 tile once (about 256 instead of 1024 pairs of 16 kernel
-// evaluations) into shared memory and every thread then combines the 4
-// moment sets of its basis-function pair.
+// pair of its 32 x 32 tile once (about 850 instead of 4096 pairs of 16
+// kernel evaluations).  The thread that computes a pair's 8 moments forms,
+// while they are in registers, the terms of every basis-function pair of
+// the tile that uses it (side sa of row ra on tetrahedron iA, side sb of
+// column rb on tetrahedron jB: term slot (ra, rb, 2 sa + sb), written by
+// exactly one thread); after one barrier each basis-function pair adds its
+// four slots in a fixed order.
+// Phase: for real k, exp(ikr) = exp(ik rc) exp(ik (r - rc)) with rc the
+// centroid distance and |r - rc| <= rA + rB (triangle inequality, rA the
+// largest distance of a rule point from its centroid); when |k| (rA + rB)
+// <= 1 the second factor is a short Taylor series (expi_small), so one
+// sincos serves the 16 point pairs.
 // =========================================================================
 #define FT 16        // PFT tiles (k_pft_far): 16 x 16 basis functions
 #define FTF BG_FAR_TILE
 #define FTT BG_FAR_TILE_TETS
-#define FCH 8        // column tetrahedra per moment chunk
-#define FTHR 256     // threads of the far kernel: each owns 2 x 2 basis-function pairs
+#define FTHR 256     // threads of the far kernel
 
 struct FarSmem {
-  cd mom[FTT][FCH][8];          // M0, M1 (3), M1' (3), M2
+  cd slot[FTF][FTF][4];         // term (sa, sb) of the basis-function pair (row ra, column rb) of the tile
   double pA[FTT][4][3], pB[FTT][4][3];
   double oA[FTT][3], oB[FTT][3];
+  double rA[FTT], rB[FTT];      // largest distance of a rule point from its centroid
   double uA[FTF][2][4], uB[FTF][2][4];   // s A (1, Q - o) per side
-  int lA[FTF][2], lB[FTF][2];            // tile-local tetrahedron of each side
+  int lA[FTF][2], lB[FTF][2];            // tile-local tetrahedron of each side, -1 past N
   int vA[FTF][5], vB[FTF][5];
+  unsigned char sA[FTT][4], sB[FTT][4];  // sides on each tetrahedron: row << 1 | side
+  int nsA[FTT], nsB[FTT];
 };
 
 // Frequency-parameterised launches: when fq (device, {Re w, Im w}) is
@@ -227,6 +261,7 @@ __device__ void far_stage_bfs(const DevGeom &g, int tile, double (*P)[4][3], dou
   if (tid < 2 * FTF) {
     int r = tid >> 1, s = tid & 1;
     int bf = tile * FTF + r;
+    l[r][s] = -1;
     if (bf < g.N) {
       int2 loc = g.bfTileLoc[bf];
       int lt = s == 0 ? loc.x : loc.y;
@@ -248,6 +283,27 @@ __device__ void far_stage_bfs(const DevGeom &g, int tile, double (*P)[4][3], dou
   }
 }
 
+// centroid, point radius and the sides resting on tetrahedron t of a tile
+__device__ void far_stage_tet_info(int t, const double (*P)[4][3], double (*o)[3], double *rad, const int (*l)[2],
+                                   unsigned char (*sides)[4], int *ns) {
+  for (int c = 0; c < 3; c++) o[t][c] = 0.25 * (P[t][0][c] + P[t][1][c] + P[t][2][c] + P[t][3][c]);
+  double r2 = 0.0;
+  for (int i = 0; i < 4; i++) {
+    double a2 = 0.0;
+    for (int c = 0; c < 3; c++) {
+      double d = P[t][i][c] - o[t][c];
+      a2 += d * d;
+    }
+    r2 = fmax(r2, a2);
+  }
+  rad[t] = sqrt(r2);
+  int n = 0;
+  for (int r = 0; r < FTF; r++)
+    for (int s = 0; s < 2; s++)
+      if (l[r][s] == t && n < 4) sides[t][n++] = (unsigned char)(r << 1 | s);
+  ns[t] = n;
+}
+
 // one CTA per 32 x 32 tile of basis-function pairs (upper triangle of tiles)
 __global__ void __launch_bounds__(FTHR, 2) k_far(DevGeom g, cd k, cd invk2, cd *M, size_t ld, const double *fq) {
   if (fq) {
@@ -263,109 +319,90 @@ __global__ void __launch_bounds__(FTHR, 2) k_far(DevGeom g, cd k, cd invk2, cd *
   far_stage_tets(g, bx, S.pA, tid);
   far_stage_tets(g, by, S.pB, tid);
   __syncthreads();
-  if (tid < FTT) {
-    for (int c = 0; c < 3; c++) {
-      S.oA[tid][c] = 0.25 * (S.pA[tid][0][c] + S.pA[tid][1][c] + S.pA[tid][2][c] + S.pA[tid][3][c]);
-      S.oB[tid][c] = 0.25 * (S.pB[tid][0][c] + S.pB[tid][1][c] + S.pB[tid][2][c] + S.pB[tid][3][c]);
-    }
-  }
   far_stage_bfs(g, bx, S.pA, S.uA, S.lA, S.vA, tid);
   far_stage_bfs(g, by, S.pB, S.uB, S.lB, S.vB, tid);
   __syncthreads();
+  if (tid < FTT) {
+    if (tid < nA) far_stage_tet_info(tid, S.pA, S.oA, S.rA, S.lA, S.sA, S.nsA);
+  } else if (tid < 2 * FTT) {
+    if (tid - FTT < nB) far_stage_tet_info(tid - FTT, S.pB, S.oB, S.rB, S.lB, S.sB, S.nsB);
+  }
+  __syncthreads();
+  const double inv4pi = 0.25 / M_PI;
+  for (int p = tid; p < nA * nB; p += FTHR) {
+    const int iA = p / nB, tB = p - iA * nB;
+    cd m[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) m[q] = cmk(0, 0);
+    // phase about the centroid distance rc (see above)
+    const double e0 = S.oA[iA][0] - S.oB[tB][0], e1 = S.oA[iA][1] - S.oB[tB][1], e2 = S.oA[iA][2] - S.oB[tB][2];
+    const double rc = sqrt(e0 * e0 + e1 * e1 + e2 * e2);
+    const bool series = k.i == 0.0 && fabs(k.r) * (S.rA[iA] + S.rB[tB]) <= 1.0;
+    const cd ec = series ? expikr(k, rc) : cmk(1.0, 0.0);
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      double x0 = S.pA[iA][i][0], x1 = S.pA[iA][i][1], x2 = S.pA[iA][i][2];
+      double xt0 = x0 - S.oA[iA][0], xt1 = x1 - S.oA[iA][1], xt2 = x2 - S.oA[iA][2];
+      cd phiI = cmk(0, 0);
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        double y0 = S.pB[tB][j][0], y1 = S.pB[tB][j][1], y2 = S.pB[tB][j][2];
+        double R0 = x0 - y0, R1 = x1 - y1, R2 = x2 - y2;
+        double r2 = R0 * R0 + R1 * R1 + R2 * R2;
+        if (r2 < 1.0e-24) continue;           // r < 1e-12
+        double ir = rsqrt(r2), r = r2 * ir;   // one reciprocal square root instead of sqrt and a division
+        cd phi = cscale(series ? cmul(ec, expi_small(k.r * (r - rc))) : expikr(k, r), inv4pi * ir);
+        double yt0 = y0 - S.oB[tB][0], yt1 = y1 - S.oB[tB][1], yt2 = y2 - S.oB[tB][2];
+        phiI = cadd(phiI, phi);
+        m[4] = cadd(m[4], cscale(phi, yt0));
+        m[5] = cadd(m[5], cscale(phi, yt1));
+        m[6] = cadd(m[6], cscale(phi, yt2));
+        m[7] = cadd(m[7], cscale(phi, xt0 * yt0 + xt1 * yt1 + xt2 * yt2));
+      }
+      m[0] = cadd(m[0], phiI);
+      m[1] = cadd(m[1], cscale(phiI, xt0));
+      m[2] = cadd(m[2], cscale(phiI, xt1));
+      m[3] = cadd(m[3], cscale(phiI, xt2));
+    }
+    // terms of the basis-function pairs on (iA, tB):
+    //   s s' A A' [M2/144 - M0/(16 k^2) - q'.M1/144 - q.M1'/144 + q.q' M0/144]
+    const cd kM0 = cmul(invk2, m[0]);
+    const int na = S.nsA[iA], nb = S.nsB[tB];
+    for (int ia = 0; ia < na; ia++) {
+      const int ca = S.sA[iA][ia], ra = ca >> 1, sa = ca & 1;
+      const double *u = S.uA[ra][sa];
+      const double u0 = u[0], u1 = u[1], u2 = u[2], u3 = u[3];
+      // the row side's part: u0 M2 - u0 (.M1 with v) ... arranged per column below
+      for (int ib = 0; ib < nb; ib++) {
+        const int cb = S.sB[tB][ib], rb = cb >> 1, sb = cb & 1;
+        const double *v = S.uB[rb][sb];
+        double uv = u1 * v[1] + u2 * v[2] + u3 * v[3];
+        cd t = cscale(m[7], u0 * v[0]);
+        t = csub(t, cscale(cadd(cadd(cscale(m[1], v[1]), cscale(m[2], v[2])), cscale(m[3], v[3])), u0));
+        t = csub(t, cscale(cadd(cadd(cscale(m[4], u1), cscale(m[5], u2)), cscale(m[6], u3)), v[0]));
+        t = cadd(t, cscale(m[0], uv));
+        t = csub(cscale(t, 1.0 / 144.0), cscale(kM0, u0 * v[0] / 16.0));
+        S.slot[ra][rb][2 * sa + sb] = t;
+      }
+    }
+  }
+  __syncthreads();
   // this thread's 2 x 2 basis-function pairs: rows tx, tx + 16; columns ty, ty + 16
   const int tx = tid & 15, ty = tid >> 4;
-  unsigned mine = 0;   // bit 2i+j: pair (tx + 16 i, ty + 16 j) is a far pair this tile writes
-  cd acc[2][2];
 #pragma unroll
   for (int i = 0; i < 2; i++)
 #pragma unroll
     for (int j = 0; j < 2; j++) {
       int ra = tx + 16 * i, rb = ty + 16 * j;
       int a = bx * FTF + ra, b = by * FTF + rb;
-      bool ok = a < g.N && b < g.N && a <= b;
-      if (ok) {
-        // CompareBFs (SWGVolume.cc:295-344): pairs with a common vertex are near
-        int ncv = 0;
-        for (int p = 0; p < 5; p++)
-          for (int q = 0; q < 5; q++) ncv += (S.vA[ra][p] == S.vB[rb][q]);
-        ok = ncv == 0;
-      }
-      if (ok) mine |= 1u << (2 * i + j);
-      acc[i][j] = cmk(0, 0);
-    }
-  const double inv4pi = 0.25 / M_PI;
-  for (int c0 = 0; c0 < nB; c0 += FCH) {
-    int cw = min(FCH, nB - c0);
-    // moments of the distinct tetrahedron pairs (iA, c0 + jB)
-    for (int p = tid; p < nA * cw; p += FTHR) {
-      int iA = p / cw, jB = p % cw, tB = c0 + jB;
-      cd m[8];
-#pragma unroll
-      for (int q = 0; q < 8; q++) m[q] = cmk(0, 0);
-#pragma unroll
-      for (int i = 0; i < 4; i++) {
-        double x0 = S.pA[iA][i][0], x1 = S.pA[iA][i][1], x2 = S.pA[iA][i][2];
-        double xt0 = x0 - S.oA[iA][0], xt1 = x1 - S.oA[iA][1], xt2 = x2 - S.oA[iA][2];
-        cd phiI = cmk(0, 0);
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-          double y0 = S.pB[tB][j][0], y1 = S.pB[tB][j][1], y2 = S.pB[tB][j][2];
-          double R0 = x0 - y0, R1 = x1 - y1, R2 = x2 - y2;
-          double r2 = R0 * R0 + R1 * R1 + R2 * R2;
-          if (r2 < 1.0e-24) continue;           // r < 1e-12
-          double ir = rsqrt(r2), r = r2 * ir;   // one reciprocal square root instead of sqrt and a division
-          cd phi = cscale(expikr(k, r), inv4pi * ir);
-          double yt0 = y0 - S.oB[tB][0], yt1 = y1 - S.oB[tB][1], yt2 = y2 - S.oB[tB][2];
-          phiI = cadd(phiI, phi);
-          m[4] = cadd(m[4], cscale(phi, yt0));
-          m[5] = cadd(m[5], cscale(phi, yt1));
-          m[6] = cadd(m[6], cscale(phi, yt2));
-          m[7] = cadd(m[7], cscale(phi, xt0 * yt0 + xt1 * yt1 + xt2 * yt2));
-        }
-        m[0] = cadd(m[0], phiI);
-        m[1] = cadd(m[1], cscale(phiI, xt0));
-        m[2] = cadd(m[2], cscale(phiI, xt1));
-        m[3] = cadd(m[3], cscale(phiI, xt2));
-      }
-#pragma unroll
-      for (int q = 0; q < 8; q++) S.mom[iA][jB][q] = m[q];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < 2; i++)
-#pragma unroll
-      for (int j = 0; j < 2; j++) {
-        if (!(mine & (1u << (2 * i + j)))) continue;
-        int ra = tx + 16 * i, rb = ty + 16 * j;
-        cd accv = acc[i][j];
-#pragma unroll
-        for (int sa = 0; sa < 2; sa++)
-#pragma unroll
-          for (int sb = 0; sb < 2; sb++) {
-            int jB = S.lB[rb][sb] - c0;
-            if (jB < 0 || jB >= cw) continue;
-            const cd *m = S.mom[S.lA[ra][sa]][jB];
-            const double *u = S.uA[ra][sa], *v = S.uB[rb][sb];
-            // u0 v0 (M2/144 - M0/(16 k^2)) - u0 (v.M1)/144 - v0 (u.M1')/144 + (u.v) M0/144
-            double uv = u[1] * v[1] + u[2] * v[2] + u[3] * v[3];
-            cd t = cscale(m[7], u[0] * v[0]);
-            t = csub(t, cscale(cadd(cadd(cscale(m[1], v[1]), cscale(m[2], v[2])), cscale(m[3], v[3])), u[0]));
-            t = csub(t, cscale(cadd(cadd(cscale(m[4], u[1]), cscale(m[5], u[2])), cscale(m[6], u[3])), v[0]));
-            t = cadd(t, cscale(m[0], uv));
-            accv = cadd(accv, cscale(t, 1.0 / 144.0));
-            accv = csub(accv, cscale(cmul(invk2, m[0]), u[0] * v[0] / 16.0));
-          }
-        acc[i][j] = accv;
-      }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int i = 0; i < 2; i++)
-#pragma unroll
-    for (int j = 0; j < 2; j++) {
-      if (!(mine & (1u << (2 * i + j)))) continue;
-      int a = bx * FTF + tx + 16 * i, b = by * FTF + ty + 16 * j;
-      cd v = acc[i][j];
+      if (!(a < g.N && b < g.N && a <= b)) continue;
+      // CompareBFs (SWGVolume.cc:295-344): pairs with a common vertex are near
+      int ncv = 0;
+      for (int p = 0; p < 5; p++)
+        for (int q = 0; q < 5; q++) ncv += (S.vA[ra][p] == S.vB[rb][q]);
+      if (ncv) continue;
+      const cd *sl = S.slot[ra][rb];
+      cd v = cadd(cadd(cadd(sl[0], sl[1]), sl[2]), sl[3]);
       M[(size_t)a + (size_t)b * ld] = v;
       if (a != b) M[(size_t)b + (size_t)a * ld] = v;
     }

@@ -1,5 +1,7 @@
 """Regenerates tests/golden/*.npz from the reference tree (run where the
-reference is mounted; the committed .npz files are what the tests read).
+reference is mounted; the committed .npz files are what the tests read):
+
+    python tests/golden/make_fixtures.py <path of the buff-em source tree>
 
 Fixtures
   ref_meshes.npz : the reference's own test meshes, as parsed gmsh arrays
@@ -16,7 +18,6 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
 OUT = os.path.dirname(os.path.abspath(__file__))
 FILES = {
     "sphere48": "src/unitTests/Sphere_48.vmsh",
@@ -46,9 +47,12 @@ def parse(path):
 
 
 def main():
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_fixtures.py <path of the buff-em source tree>")
+    ref = sys.argv[1]
     out = {}
     for name, rel in FILES.items():
-        ids, xyz, tets = parse(os.path.join(REF, rel))
+        ids, xyz, tets = parse(os.path.join(ref, rel))
         out[name + "_ids"] = ids
         out[name + "_xyz"] = xyz
         out[name + "_tets"] = tets
