@@ -152,11 +152,8 @@ class Geometry:
 
     def faces(self, no=0):
         L = lib()
-        nt = L.or_geom_ntets(self.h, no)
         # interior faces of object no
-        cnt = self.N if self.nobj == 1 else None
-        if cnt is None:
-            raise NotImplementedError
+        cnt = self.off[no + 1] - self.off[no]
         out = np.zeros((cnt, 9), dtype=np.int32)
         L.or_geom_faces(self.h, no, out)
         return out

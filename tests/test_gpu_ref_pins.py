@@ -1,0 +1,85 @@
+"""The CUDA path against the reference's own libbuff code (needs a B200: -m gpu).
+
+The inputs are the reference-pinned golden cases (tests/golden/ref_libbuff.npz,
+made by tests/golden/make_ref_fixtures.py from the reference's libbuff
+sources compiled in place), read through the library's own .buffgeo, mesh,
+MATERIAL and SVTENSOR parsers where the library reads that form of the file
+(constant, MATERIAL CONST_EPS_ and tensor materials), else through the
+material API with the same function of position (Janus and Gaussian eps(x)).
+The library runs its default refined singular rule; the reference ran its
+own code with the oracle's refined static integrals for tetrahedron pairs
+sharing >= 2 vertices.
+
+Tolerances: face tables bit-exact; matrix entries 1e-10 per entry (relative,
+floor 1e-3 of the largest); RHS 1e-12; GPU LU solution 1e-10 in norm; EMT
+power/force/torque 1e-9 per column plus 1e-12 of the largest column; overlap
+absorbed power 1e-9; scattered fields 1e-9.
+"""
+import tempfile
+
+import numpy as np
+import pytest
+
+import buffem
+import refpin_cases as rc
+
+pytestmark = pytest.mark.gpu
+
+CASES, FIX = rc.load()
+NAMES = [c["name"] for c in CASES]
+
+
+def geometry(case, d):
+    geo, meshes, disp = rc.write_inputs(case, d)
+    if all(o["material"] in ("const", "tensor") for o in case["objects"]):
+        return buffem.SWGGeometry(GeoFileName=geo)
+    mats = []
+    for o in case["objects"]:
+        if o["material"] == "janus":
+            mats.append(buffem.Material(kind=buffem.BG_MAT_JANUS_Z, eps=4 + 0.2j, eps2=12 + 1j))
+        else:
+            mats.append(buffem.Material(kind=buffem.BG_MAT_GAUSSIAN, eps=3 + 0.1j, amp=1.5,
+                                        center=tuple(o["center"])))
+    return buffem.SWGGeometry(meshfiles=meshes, materials=mats, displacements=disp)
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_case_matches_reference(name):
+    case = CASES[NAMES.index(name)]
+    with tempfile.TemporaryDirectory() as d:
+        G = geometry(case, d)
+        N = G.TotalBFs
+        assert N == int(FIX[name + "/N"])
+        for k in range(G.NumObjects):
+            np.testing.assert_array_equal(G.faces(k), FIX["%s/faces%d" % (name, k)])
+        rows = FIX[name + "/rows"] if (name + "/rows") in FIX.files else None
+        pw = buffem.PlaneWave(*rc.WAVE)
+        for i, (wr, wi) in enumerate(case["omegas"]):
+            w = complex(wr, wi)
+            M = G.AssembleVIEMatrix(w)
+            A = M.download() if rows is None else M.rows(rows)
+            ok, worst = rc.close(A, FIX["%s/matrix%d" % (name, i)], 1e-10)
+            assert ok, (name, i, "matrix", worst)
+            if not case.get("solve", True):
+                continue
+            b = G.AssembleRHSVector(w, pw)
+            ok, worst = rc.close(b, FIX["%s/rhs%d" % (name, i)], 1e-12)
+            assert ok, (name, i, "rhs", worst)
+            M.LUFactorize()
+            J = b.copy()
+            M.LUSolve(J)
+            Jr = FIX["%s/solution%d" % (name, i)]
+            err = np.linalg.norm(J - Jr) / np.linalg.norm(Jr)
+            assert err <= 1e-10, (name, i, "solution", err)
+            P = G.GetPFTMatrix(Jr, w, pw, full=True)
+            Pr = FIX["%s/pft_emt%d" % (name, i)]
+            floor = 1e-12 * np.abs(Pr).max()
+            assert np.all(np.abs(P - Pr) <= 1e-9 * np.abs(Pr) + floor), (name, i, P, Pr)
+            Po = G.GetPFTMatrix(Jr, w, None, method=buffem.BG_PFT_OVERLAP)[:, 0]
+            Pro = FIX["%s/pft_overlap%d" % (name, i)][:, 0]
+            assert np.all(np.abs(Po - Pro) <= 1e-9 * np.abs(Pro) + floor), (name, i, Po, Pro)
+            if ("%s/fields%d" % (name, i)) in FIX.files:
+                X = FIX["%s/field_points%d" % (name, i)]
+                F = G.GetFields(None, Jr, w, X)
+                ok, worst = rc.close(F, FIX["%s/fields%d" % (name, i)], 1e-9)
+                assert ok, (name, i, "fields", worst)
