@@ -50,6 +50,8 @@ char *vstrdup(const char *format, ...);
 char *vstrappend(char *s, const char *format, ...);
 void vsnprintfEC(char *buf, size_t n, const char *format, va_list ap);
 
+void fprintVecCR(FILE *f, cdouble *v, int n);
+
 // a complex number as text, for log messages (static buffer)
 const char *z2s(cdouble z);
 

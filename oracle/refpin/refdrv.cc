@@ -8,28 +8,23 @@
 // unit-test-LFField.cc:50-71): SWGGeometry(buffgeo), AssembleVIEMatrix,
 // AssembleRHSVector(PlaneWave), GetPFTMatrix, GetFields.
 //
-// Frequency-independent near-field data (the FIBBI cache) is preloaded by the
-// reference's own FIBBICache constructor from ${BUFF_CACHE_PATH}/<mesh>.cache
-// (FIBBICache.cc:108-160).  Tetrahedron pairs sharing two or more vertices
-// whose record is missing would need the Taylor-Duffy integrator, whose
-// adaptive cubature library is not vendored; in this build they end the
-// process (TTaylorDuffy below), so a fixture never holds a stand-in value.
+// Frequency-independent near-field data (the FIBBI cache) is either
+// preloaded by the reference's own FIBBICache constructor from
+// ${BUFF_CACHE_PATH}/<mesh>.cache (FIBBICache.cc:108-160) or computed by the
+// reference itself, Taylor-Duffy included (TTaylorDuffy.cc, compiled with
+// the project's adaptive cubature and kernel functions, shim.cc), at the
+// tolerance set by rp_set_taylor_duffy.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 
 #include "libbuff.h"
-#include "TTaylorDuffy.h"
 
 using namespace buff;
 
-void InitTTDArgs(TTDArgStruct *) {}
-void TTaylorDuffy(TTDArgStruct *, void *) {
-  ErrExit("a singular tetrahedron pair is missing from the preloaded near-field cache");
-}
-
 namespace buff {
 void GetFIBBICacheKey(SWGVolume *OA, int nfA, SWGVolume *OB, int nfB, float *K);
+void ComputeFIBBIData(SWGVolume *OA, int nfA, SWGVolume *OB, int nfB, double GFI[FIBBIDATALEN]);
 
 // PFT methods of the reference that the pin does not compile (MomentPFT.cc,
 // DSIPFT.cc need more of SCUFF-EM); selecting them ends the process.
@@ -53,6 +48,23 @@ void *rp_geometry(const char *buffgeo) {
   SWGGeometry *G = new SWGGeometry(buffgeo);
   G->LogLevel = BUFF_NO_LOGGING;
   return G;
+}
+
+// SWGGeometry::TaylorDuffyTolerance and MaxTaylorDuffyEvals (defaults 1e-6
+// and 1e4, SWGGeometry.cc:46-47).
+void rp_set_taylor_duffy(double reltol, int maxevals) {
+  SWGGeometry::TaylorDuffyTolerance = reltol;
+  SWGGeometry::MaxTaylorDuffyEvals = maxevals;
+}
+
+// The near-field record of the basis-function pair (a, b) of object no,
+// computed by the reference (ComputeFIBBIData, GMatrixElements.cc:362-368):
+// the 16x16 rule for tetrahedron pairs sharing <= 1 vertex, Taylor-Duffy for
+// the others.  n pairs, 6 doubles each; OpenMP over the pairs.
+void rp_fibbi(void *g, int no, int n, const int *pairs, double *out) {
+  SWGVolume *O = ((SWGGeometry *)g)->Objects[no];
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int i = 0; i < n; i++) ComputeFIBBIData(O, pairs[2 * i], O, pairs[2 * i + 1], out + 6 * i);
 }
 
 void rp_geometry_free(void *g) { delete (SWGGeometry *)g; }

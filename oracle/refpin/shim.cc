@@ -5,10 +5,11 @@
 // vendored with the reference; every body here is the project's own, written
 // from what the reference's call sites require of it.
 //
-// Entry points that the pinned hot path must never reach (adaptive cubature,
-// the Taylor-Duffy integrator, the moment and displaced-surface PFT methods,
-// sparse matrices) end the process with a message, so that a fixture can
-// never silently contain their stand-in values.
+// Entry points that the pinned hot path must never reach (the moment and
+// displaced-surface PFT methods, sparse matrices, Helmholtz Taylor-Duffy
+// kernels) end the process with a message, so that a fixture can never
+// silently contain a stand-in's value.
+#include <algorithm>
 #include <cctype>
 #include <cmath>
 #include <complex>
@@ -686,23 +687,189 @@ void PlaneWave::GetFieldGradients(const double X[3], cdouble dEH[3][6]) {
     for (int n = 0; n < 6; n++) dEH[mu][n] = ik * nHat[mu] * EH[n];
 }
 
-/* ------------------------------------------------------------ not on the pinned path */
-int hcubature(unsigned, integrand, void *, unsigned, const double *, const double *, size_t, double, double,
-              error_norm, double *, double *) {
-  ErrExit("adaptive cubature is not part of the pinned path");
-  return 1;
+/* ------------------------------------------------------------ adaptive cubature */
+// h-adaptive cubature over a box, the published algorithm of A. C. Genz and
+// A. A. Malik, "An adaptive algorithm for numerical integration over an
+// N-dimensional rectangular region", J. Comput. Appl. Math. 6 (1980) 295-302:
+// a degree-7 fully symmetric rule with an embedded degree-5 rule; the box with
+// the largest error estimate |I7 - I5| is halved along the coordinate with the
+// largest fourth divided difference until every component's summed error is
+// within max(reqAbsError, reqRelError |I|) (ERROR_INDIVIDUAL) or maxEval
+// evaluations are spent (maxEval 0: no limit).  The cubature library the
+// reference links (SGJ's) is not vendored; this is the project's own code.
+namespace {
+struct Box {
+  std::vector<double> c, h;       // centre, half-widths
+  std::vector<double> I, E;       // integral and error per component
+  int split;                      // coordinate to halve next
+  double key;                     // largest error component
+};
+
+int gm_eval(integrand f, void *fdata, unsigned n, unsigned fdim, Box &b, size_t &evals) {
+  const double l2 = sqrt(9.0 / 70.0), l4 = sqrt(9.0 / 10.0), l5 = sqrt(9.0 / 19.0);
+  const double nn = n;
+  const double w1 = (12824.0 - 9120.0 * nn + 400.0 * nn * nn) / 19683.0, w2 = 980.0 / 6561.0,
+               w3 = (1820.0 - 400.0 * nn) / 19683.0, w4 = 200.0 / 19683.0, w5 = 6859.0 / 19683.0 / ldexp(1.0, n);
+  const double v1 = (729.0 - 950.0 * nn + 50.0 * nn * nn) / 729.0, v2 = 245.0 / 486.0,
+               v3 = (265.0 - 100.0 * nn) / 1458.0, v4 = 25.0 / 729.0;
+  std::vector<double> x(n), f0(fdim), fp(fdim), fm(fdim), s2(fdim, 0), s3(fdim, 0), s4(fdim, 0), s5(fdim, 0);
+  double vol = 1.0;
+  for (unsigned i = 0; i < n; i++) vol *= 2.0 * b.h[i];
+  auto at = [&](std::vector<double> &fv) {
+    if (f(n, x.data(), fdata, fdim, fv.data())) return 1;
+    evals++;
+    return 0;
+  };
+  x = b.c;
+  if (at(f0)) return 1;
+  double best = -1;
+  b.split = 0;
+  for (unsigned i = 0; i < n; i++) {
+    std::vector<double> a2(fdim), a3(fdim);
+    for (int sgn = 0; sgn < 2; sgn++) {
+      x = b.c;
+      x[i] += (sgn ? -1 : 1) * l2 * b.h[i];
+      if (at(sgn ? fm : fp)) return 1;
+    }
+    for (unsigned k = 0; k < fdim; k++) {
+      a2[k] = fp[k] + fm[k];
+      s2[k] += a2[k];
+    }
+    for (int sgn = 0; sgn < 2; sgn++) {
+      x = b.c;
+      x[i] += (sgn ? -1 : 1) * l4 * b.h[i];
+      if (at(sgn ? fm : fp)) return 1;
+    }
+    for (unsigned k = 0; k < fdim; k++) {
+      a3[k] = fp[k] + fm[k];
+      s3[k] += a3[k];
+    }
+    // fourth difference along i, summed over the components
+    double diff = 0;
+    for (unsigned k = 0; k < fdim; k++)
+      diff += std::fabs(a2[k] - 2 * f0[k] - (l2 * l2 / (l4 * l4)) * (a3[k] - 2 * f0[k]));
+    if (diff > best * (1 + 1e-12)) {
+      best = diff;
+      b.split = i;
+    }
+  }
+  for (unsigned i = 0; i < n; i++)
+    for (unsigned j = i + 1; j < n; j++)
+      for (int si = 0; si < 2; si++)
+        for (int sj = 0; sj < 2; sj++) {
+          x = b.c;
+          x[i] += (si ? -1 : 1) * l4 * b.h[i];
+          x[j] += (sj ? -1 : 1) * l4 * b.h[j];
+          if (at(fp)) return 1;
+          for (unsigned k = 0; k < fdim; k++) s4[k] += fp[k];
+        }
+  for (unsigned m = 0; m < (1u << n); m++) {
+    for (unsigned i = 0; i < n; i++) x[i] = b.c[i] + (((m >> i) & 1) ? -1 : 1) * l5 * b.h[i];
+    if (at(fp)) return 1;
+    for (unsigned k = 0; k < fdim; k++) s5[k] += fp[k];
+  }
+  b.I.assign(fdim, 0);
+  b.E.assign(fdim, 0);
+  b.key = 0;
+  for (unsigned k = 0; k < fdim; k++) {
+    double i7 = vol * (w1 * f0[k] + w2 * s2[k] + w3 * s3[k] + w4 * s4[k] + w5 * s5[k]);
+    double i5 = vol * (v1 * f0[k] + v2 * s2[k] + v3 * s3[k] + v4 * s4[k]);
+    b.I[k] = i7;
+    b.E[k] = std::fabs(i7 - i5);
+    if (b.E[k] > b.key) b.key = b.E[k];
+  }
+  return 0;
 }
-int CCCubature(int, unsigned, integrand, void *, unsigned, const double *, const double *, size_t, double, double,
-               error_norm, double *, double *) {
-  ErrExit("Clenshaw-Curtis cubature is not part of the pinned path");
-  return 1;
+}  // namespace
+
+int hcubature(unsigned fdim, integrand f, void *fdata, unsigned dim, const double *xmin, const double *xmax,
+              size_t maxEval, double reqAbsError, double reqRelError, error_norm, double *val, double *err) {
+  std::vector<Box> heap(1);
+  heap[0].c.resize(dim);
+  heap[0].h.resize(dim);
+  for (unsigned i = 0; i < dim; i++) {
+    heap[0].c[i] = 0.5 * (xmin[i] + xmax[i]);
+    heap[0].h[i] = 0.5 * (xmax[i] - xmin[i]);
+  }
+  size_t evals = 0;
+  if (gm_eval(f, fdata, dim, fdim, heap[0], evals)) return 1;
+  auto cmp = [](const Box &a, const Box &b) { return a.key < b.key; };
+  std::vector<double> I(heap[0].I), E(heap[0].E);
+  for (;;) {
+    bool done = true;
+    for (unsigned k = 0; k < fdim; k++)
+      if (E[k] > reqAbsError && E[k] > reqRelError * std::fabs(I[k])) done = false;
+    if (done || (maxEval && evals >= maxEval)) break;
+    std::pop_heap(heap.begin(), heap.end(), cmp);
+    Box b = heap.back();
+    heap.pop_back();
+    Box c1 = b, c2 = b;
+    int s = b.split;
+    c1.h[s] = c2.h[s] = 0.5 * b.h[s];
+    c1.c[s] = b.c[s] - c1.h[s];
+    c2.c[s] = b.c[s] + c2.h[s];
+    if (gm_eval(f, fdata, dim, fdim, c1, evals) || gm_eval(f, fdata, dim, fdim, c2, evals)) return 1;
+    for (unsigned k = 0; k < fdim; k++) {
+      I[k] += c1.I[k] + c2.I[k] - b.I[k];
+      E[k] += c1.E[k] + c2.E[k] - b.E[k];
+    }
+    heap.push_back(c1);
+    std::push_heap(heap.begin(), heap.end(), cmp);
+    heap.push_back(c2);
+    std::push_heap(heap.begin(), heap.end(), cmp);
+    // summed estimates drift by rounding over many splits: re-sum now and then
+    if (heap.size() % 256 == 0) {
+      std::fill(I.begin(), I.end(), 0.0);
+      std::fill(E.begin(), E.end(), 0.0);
+      for (auto &h : heap)
+        for (unsigned k = 0; k < fdim; k++) {
+          I[k] += h.I[k];
+          E[k] += h.E[k];
+        }
+    }
+  }
+  for (unsigned k = 0; k < fdim; k++) {
+    val[k] = 0;
+    if (err) err[k] = 0;
+  }
+  for (auto &h : heap)
+    for (unsigned k = 0; k < fdim; k++) {
+      val[k] += h.I[k];
+      if (err) err[k] += h.E[k];
+    }
+  return 0;
 }
+
+// The reference calls this for integrals of dimension <= 2 (and for fixed
+// orders); here it is the same adaptive rule.
+int CCCubature(int, unsigned fdim, integrand f, void *fdata, unsigned dim, const double *xmin, const double *xmax,
+               size_t maxEval, double reqAbsError, double reqRelError, error_norm norm, double *val, double *err) {
+  return hcubature(fdim, f, fdata, dim, xmin, xmax, maxEval, reqAbsError, reqRelError, norm, val, err);
+}
+
 double *GetTCR(int, int *NumPts) {
   if (NumPts) *NumPts = 0;
   return 0;
 }
 
+void fprintVecCR(FILE *f, cdouble *v, int n) {
+  for (int i = 0; i < n; i++) fprintf(f, "%+.8e %+.8e ", real(v[i]), imag(v[i]));
+  fprintf(f, "\n");
+}
+
 namespace scuff {
+// The kernel functions of the generalised Taylor-Duffy method (M. T. H. Reid,
+// J. K. White, S. G. Johnson, IEEE Trans. Antennas Propag. 63(1), 2015):
+// K_n(X) = int_0^1 w^n K(w X) dw for n = nMin..nMax (stored at index n).
+// For the power kernels K(r) = r^p (TTD_RP, p = real(KParam)) this is
+// X^p / (n + p + 1).  The Helmholtz kernels are not part of the pinned path
+// (the near field is assembled from static integrals).
+void GetScriptK(int WhichK, cdouble KParam, double X, int nMin, int nMax, cdouble *KVector) {
+  if (WhichK != 0) ErrExit("only the power kernels of Taylor-Duffy are part of the pinned path");
+  double p = real(KParam);
+  for (int n = nMin; n <= nMax; n++) KVector[n] = std::pow(X, p) / (n + p + 1.0);
+}
+
 // Homogeneous dyadic Green's functions of the field routine (restated from
 // their definitions, SCUFF-EM's own CalcGC is not vendored), R = R1 - R2:
 //   G_mn = [delta_mn + d_m d_n / k^2] phi,   C_mn = (1 / ik) eps_mnr d_r phi,

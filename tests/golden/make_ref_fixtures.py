@@ -21,24 +21,31 @@ integrals, the 16x16 static rule for tetrahedron pairs sharing <= 1 vertex,
 the V^-1 Gram blocks with SVTensor materials, the RHS, the EMT and overlap
 power/force/torque and the scattered fields.
 
-What does not: the static integrals of tetrahedron pairs sharing >= 2
-vertices (the reference computes them with Taylor-Duffy through an adaptive
-cubature library that is not vendored).  Their near-field cache records
-(one per basis-function pair that has such a tetrahedron pair) are written
-by the project's CPU oracle with its refined singular rule, in the
-reference's cache file format, and loaded by the reference's own
-FIBBICache::PreLoad through BUFF_CACHE_PATH.  The reference computes every
-other record itself.  Also restated rather than the reference's: the
-plane wave (E = E0 exp(i k nHat.x), H = nHat x E / Z0, k = Omega), the
-dyadic Green's functions of the field routine (CalcGC), and the complex
-expression evaluator of the material files.
+The static integrals of tetrahedron pairs sharing >= 2 vertices: the
+reference computes them with its Taylor-Duffy code (TTaylorDuffy.cc, also
+compiled in place) through an adaptive cubature library that is not
+vendored; here that cubature is the project's own (Genz-Malik, shim.cc) and
+the kernel functions K_n(X) are restated from the Taylor-Duffy paper.  Case
+s48 runs it for every record at RelTol 1e-8 (the reference's default is
+1e-6) and stores the singular records themselves ('td_pairs', 'td_records')
+beside the matrices.  For the other cases (Taylor-Duffy at that tolerance
+takes seconds per record) the records of the basis-function pairs that have
+such a tetrahedron pair are written by the project's CPU oracle with its
+refined singular rule, in the reference's cache file format, and loaded by
+the reference's own FIBBICache::PreLoad through BUFF_CACHE_PATH; the
+reference computes every other record itself.  Also restated rather than
+the reference's: the plane wave (E = E0 exp(i k nHat.x), H = nHat x E / Z0,
+k = Omega), the dyadic Green's functions of the field routine (CalcGC), and
+the complex expression evaluator of the material files.
 
 Cases (inputs are regenerated by the tests from the metadata stored beside
 the outputs; meshes come from buff-em_b200/meshgen.py or the reference's own
 test meshes in tests/golden/ref_meshes.npz; tests/refpin_cases.py writes
 them, here and in the tests):
-  s48       Sphere_48 (src/unitTests), CONST_EPS_10, omega 0.1 and 1.0:
-            full matrices, RHS, LAPACK solution, EMT and overlap PFT, fields
+  s48       Sphere_48 (src/unitTests), CONST_EPS_10, omega 0.1 and 1.0,
+            every near record by the reference (Taylor-Duffy at 1e-8):
+            full matrices, RHS, LAPACK solution, EMT and overlap PFT,
+            fields, and the 624 singular records
   s533      Sphere_533 with E10Sphere_533.buffgeo's eps = 10, omega = 0.1
             (unit-test-LFField.cc:50-71): 16 seeded rows, RHS, solution, PFT,
             fields
@@ -76,7 +83,7 @@ SIG = b"FIBBI_GCACHE\0"
 
 CASES = [
     dict(name="s48", objects=[dict(mesh="ref:sphere48", material="const", eps=[10.0, 0.0])],
-         omegas=[[0.1, 0.0], [1.0, 0.0]], rows=None, fields=True),
+         omegas=[[0.1, 0.0], [1.0, 0.0]], rows=None, fields=True, taylor_duffy=[1e-8, 200000]),
     dict(name="s533", objects=[dict(mesh="ref:sphere533", material="const", eps=[10.0, 0.0])],
          omegas=[[0.1, 0.0]], rows=16, fields=True),
     dict(name="n5", objects=[dict(mesh="sphere:5", material="const", eps=[4.0, 0.2])],
@@ -111,6 +118,8 @@ def ref_lib(ref):
     L.rp_rhs.argtypes = [P, C.c_double, C.c_double, P, P, P]
     L.rp_pft.argtypes = [P, P, C.c_double, C.c_double, P, P, C.c_int, P]
     L.rp_fields.argtypes = [P, P, C.c_double, C.c_double, C.c_int, P, P]
+    L.rp_set_taylor_duffy.argtypes = [C.c_double, C.c_int]
+    L.rp_fibbi.argtypes = [P, C.c_int, C.c_int, P, P]
     return L
 
 
@@ -141,6 +150,15 @@ def run_case(L, case, d):
         L.rp_singular_pairs(G, k, ptr(pairs), cnt)
         off = Go.off[k]
         base = os.path.splitext(os.path.basename(meshes[k]))[0]
+        if "taylor_duffy" in case:
+            # the reference computes every record itself, Taylor-Duffy included
+            tol, maxe = case["taylor_duffy"]
+            L.rp_set_taylor_duffy(tol, maxe)
+            rec = np.zeros((cnt, 6))
+            L.rp_fibbi(G, k, cnt, ptr(pairs), ptr(rec))
+            out["td_pairs%d" % k] = pairs
+            out["td_records%d" % k] = rec
+            continue
         with open(os.path.join(cachedir, base + ".cache"), "wb") as f:
             f.write(SIG)
             key = np.zeros(27, np.float32)
@@ -149,7 +167,7 @@ def run_case(L, case, d):
                 f.write(key.tobytes())
                 f.write(np.asarray(Go.fibbi(int(a + off), int(b + off)), np.float64).tobytes())
         nrec += cnt
-    out["singular_records"] = np.array(nrec)
+    out["singular_records"] = np.array(0 if "taylor_duffy" in case else nrec)
     os.environ["BUFF_CACHE_PATH"] = cachedir
     rng = np.random.default_rng(len(case["name"]) * 7919 + N)
     rows = None if case["rows"] is None else np.sort(rng.choice(N, case["rows"], replace=False))

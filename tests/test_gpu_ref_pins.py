@@ -7,13 +7,17 @@ MATERIAL and SVTENSOR parsers where the library reads that form of the file
 (constant, MATERIAL CONST_EPS_ and tensor materials), else through the
 material API with the same function of position (Janus and Gaussian eps(x)).
 The library runs its default refined singular rule; the reference ran its
-own code with the oracle's refined static integrals for tetrahedron pairs
-sharing >= 2 vertices.
+own code throughout for case s48 (Taylor-Duffy at RelTol 1e-8 included) and,
+in the other cases, with the oracle's refined static integrals for
+tetrahedron pairs sharing >= 2 vertices.
 
 Tolerances: face tables bit-exact; matrix entries 1e-10 per entry (relative,
-floor 1e-3 of the largest); RHS 1e-12; GPU LU solution 1e-10 in norm; EMT
-power/force/torque 1e-9 per column plus 1e-12 of the largest column; overlap
-absorbed power 1e-9; scattered fields 1e-9.
+floor 1e-3 of the largest; 3e-8 for s48, the Taylor-Duffy tolerance); the
+device near-field records of s48 within 2e-8 of the reference's Taylor-Duffy
+records (per kernel scale); RHS 1e-12; GPU LU solution 1e-10 in norm (2e-8
+for s48); EMT power/force/torque 1e-9 per column plus 1e-12 of the largest
+column (2e-8 for s48); overlap absorbed power likewise; scattered fields
+1e-9 (2e-8 for s48).
 """
 import tempfile
 
@@ -27,6 +31,11 @@ pytestmark = pytest.mark.gpu
 
 CASES, FIX = rc.load()
 NAMES = [c["name"] for c in CASES]
+
+
+def tolerances(name):
+    """(matrix, solution/fields/PFT) relative tolerances of a case."""
+    return (3e-8, 2e-8) if name == "s48" else (1e-10, 1e-10)
 
 
 def geometry(case, d):
@@ -54,11 +63,23 @@ def test_case_matches_reference(name):
             np.testing.assert_array_equal(G.faces(k), FIX["%s/faces%d" % (name, k)])
         rows = FIX[name + "/rows"] if (name + "/rows") in FIX.files else None
         pw = buffem.PlaneWave(*rc.WAVE)
+        tm, ts = tolerances(name)
+        if (name + "/td_pairs0") in FIX.files:
+            # the device's near-field records against the reference's Taylor-Duffy ones
+            pairs, data = G.near_data()
+            lookup = {(int(a), int(b)): k for k, (a, b) in enumerate(np.asarray(pairs)[:, :2])}
+            ref = FIX[name + "/td_records0"]
+            got = np.array([np.asarray(data)[lookup[(int(a), int(b))]] for a, b in FIX[name + "/td_pairs0"]])
+            err = np.zeros_like(ref)
+            for k in range(6):
+                sc = np.abs(ref[:, 2 * (k // 2):2 * (k // 2) + 2]).max()
+                err[:, k] = np.abs(got[:, k] - ref[:, k]) / np.maximum(np.abs(ref[:, k]), 1e-3 * sc)
+            assert err.max() < 2e-8, err.max()
         for i, (wr, wi) in enumerate(case["omegas"]):
             w = complex(wr, wi)
             M = G.AssembleVIEMatrix(w)
             A = M.download() if rows is None else M.rows(rows)
-            ok, worst = rc.close(A, FIX["%s/matrix%d" % (name, i)], 1e-10)
+            ok, worst = rc.close(A, FIX["%s/matrix%d" % (name, i)], tm)
             assert ok, (name, i, "matrix", worst)
             if not case.get("solve", True):
                 continue
@@ -70,16 +91,17 @@ def test_case_matches_reference(name):
             M.LUSolve(J)
             Jr = FIX["%s/solution%d" % (name, i)]
             err = np.linalg.norm(J - Jr) / np.linalg.norm(Jr)
-            assert err <= 1e-10, (name, i, "solution", err)
+            assert err <= ts, (name, i, "solution", err)
+            tp = max(ts, 1e-9)
             P = G.GetPFTMatrix(Jr, w, pw, full=True)
             Pr = FIX["%s/pft_emt%d" % (name, i)]
             floor = 1e-12 * np.abs(Pr).max()
-            assert np.all(np.abs(P - Pr) <= 1e-9 * np.abs(Pr) + floor), (name, i, P, Pr)
+            assert np.all(np.abs(P - Pr) <= tp * np.abs(Pr) + floor), (name, i, P, Pr)
             Po = G.GetPFTMatrix(Jr, w, None, method=buffem.BG_PFT_OVERLAP)[:, 0]
             Pro = FIX["%s/pft_overlap%d" % (name, i)][:, 0]
-            assert np.all(np.abs(Po - Pro) <= 1e-9 * np.abs(Pro) + floor), (name, i, Po, Pro)
+            assert np.all(np.abs(Po - Pro) <= tp * np.abs(Pro) + floor), (name, i, Po, Pro)
             if ("%s/fields%d" % (name, i)) in FIX.files:
                 X = FIX["%s/field_points%d" % (name, i)]
                 F = G.GetFields(None, Jr, w, X)
-                ok, worst = rc.close(F, FIX["%s/fields%d" % (name, i)], 1e-9)
+                ok, worst = rc.close(F, FIX["%s/fields%d" % (name, i)], tp)
                 assert ok, (name, i, "fields", worst)
