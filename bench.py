@@ -20,6 +20,13 @@ anisotropic tensor [[4,.5,0],[.5,6,0],[0,0,9]] + 0.1i ("secondary").  The
 frequency-independent near-field precompute runs once per mesh before timing
 ("precompute_s"), as the reference amortises its FIBBI cache.
 
+Also beside the headline: "learned_form.omega_sweep" runs the learned step
+at omega = 0.5, 2 and 3 on the same sphere (the workload's frequency range
+is [0.5, 3]) with Jacobi's step count beside it, and "jittered_n19872" the
+12^3-cell sphere with jittered vertices -- the precision-form configuration
+(+-0.05 h, Janus eps 4+0.2i / 12+1i) and the graph network's held-out check
+(+-0.1 h, eps 6+0.5i) -- through the FP64, precision and learned paths.
+
 Beside the headline (--no-extras skips them): "get_fields" times
 GetFields for 4096 far and 4096 near points on the N = 57,222 sphere, and
 "neq_flux" the buff-neq flux chain (dressed Rytov matrix, EMT flux columns)
@@ -74,10 +81,10 @@ def eps_tensor():
     return np.array(TENSOR, complex) + 0.1j * np.eye(3)
 
 
-def mesh_path(n):
+def mesh_path(n, jitter=0.0, seed=0):
     import meshgen
     d = os.path.join(tempfile.gettempdir(), "buffem_bench_meshes")
-    return meshgen.cached_sphere(d, n)
+    return meshgen.cached_sphere(d, n, 1.0, jitter, seed)
 
 
 # ------------------------------------------------------------------ clocks
@@ -197,15 +204,42 @@ def gemm_kernel_bench(n, reps=5):
             "cublas_zgemm_tflops": cub, "frac_of_cublas": ours / cub}
 
 
+def cgemm_kernel_bench(n, reps=5):
+    """Library complex64 GEMM (C -= A B on the tcgen05 TF32 tensor cores) on
+    one n^3 problem, CUDA events on the library stream, best of reps."""
+    import torch
+    import buffem
+    L = buffem.lib()
+    stream = torch.cuda.ExternalStream(L.bg_stream())
+    g = torch.Generator(device="cuda").manual_seed(0)
+    A = torch.randn(n, n, dtype=torch.complex64, device="cuda", generator=g)
+    B = torch.randn(n, n, dtype=torch.complex64, device="cuda", generator=g)
+    C = torch.zeros(n, n, dtype=torch.complex64, device="cuda")
+    best = 1e30
+    for i in range(reps + 1):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        buffem.cgemm_sub_device(n, n, n, A.data_ptr(), n, B.data_ptr(), n, C.data_ptr(), n)
+        e1.record(stream)
+        buffem.synchronize()
+        if i:
+            best = min(best, e0.elapsed_time(e1) / 1e3)
+    tf = 8.0 * n ** 3 / best / 1e12
+    mp = measured_peaks().get("bf16_tflops")
+    return {"kernel": "k_cgemm_tf32 (+ k_expand_a)", "shape": [n, n, n], "tflops": tf, "ms": best * 1e3,
+            "tf32_peak_tflops": mp / 2 if mp else None, "peak_source": "half the measured dense BF16 burst rate",
+            "frac_of_tf32_peak": tf / (mp / 2) if mp else None}
+
+
 # ------------------------------------------------------------------ GPU arm
 class Case:
     """One mesh/material on the device with the library's C-ABI handles."""
 
-    def __init__(self, n, material, order):
+    def __init__(self, n, material, order, jitter=0.0, seed=0):
         import buffem
         self.buffem = buffem
         self.L = buffem.lib()
-        self.G = buffem.SWGGeometry(meshfiles=mesh_path(n), materials=material, singular_order=order)
+        self.G = buffem.SWGGeometry(meshfiles=mesh_path(n, jitter, seed), materials=material, singular_order=order)
         self.N = self.G.TotalBFs
         t0 = time.perf_counter()
         self.G.precompute()
@@ -217,40 +251,40 @@ class Case:
         self.nhs = [np.ascontiguousarray(np.array(k, float)) for _, k in WAVES]
         self.nrhs = len(WAVES)
 
-    def rhs_device(self, dB):
+    def rhs_device(self, dB, w=OMEGA):
         b = self.buffem
         for i in range(self.nrhs):
-            b._check(self.L.bg_rhs_planewave_device(self.G.h, OMEGA, 0.0, b._ptr(self.E0s[i]), b._ptr(self.nhs[i]),
+            b._check(self.L.bg_rhs_planewave_device(self.G.h, w, 0.0, b._ptr(self.E0s[i]), b._ptr(self.nhs[i]),
                                                     b.C.c_void_p(dB[i].data_ptr())))
 
-    def step_fp64(self, dB):
+    def step_fp64(self, dB, w=OMEGA):
         b = self.buffem
-        b._check(self.L.bg_assemble(self.G.h, OMEGA, 0.0, self.M.h))
+        b._check(self.L.bg_assemble(self.G.h, w, 0.0, self.M.h))
         b._check(self.L.bg_lu_factor(self.M.h))
-        self.rhs_device(dB)
+        self.rhs_device(dB, w)
         b._check(self.L.bg_lu_solve_device(self.M.h, b.C.c_void_p(dB.data_ptr()), self.N, self.nrhs))
 
     def ensure_c64(self):
         if self.F is None:
             self.F = self.G.AllocateVIEMatrix(self.buffem.BG_C64)
 
-    def step_precision(self, dB, stats, tol=1e-12):
+    def step_precision(self, dB, stats, tol=1e-12, w=OMEGA):
         b = self.buffem
         self.ensure_c64()
-        b._check(self.L.bg_assemble(self.G.h, OMEGA, 0.0, self.M.h))
+        b._check(self.L.bg_assemble(self.G.h, w, 0.0, self.M.h))
         b._check(self.L.bg_matrix_convert(self.M.h, self.F.h))
         b._check(self.L.bg_lu_factor(self.F.h))
-        self.rhs_device(dB)
+        self.rhs_device(dB, w)
         b._check(self.L.bg_lu_solve_refined_device(self.M.h, self.F.h, b.C.c_void_p(dB.data_ptr()), self.N,
                                                    self.nrhs, tol, 60, b._ptr(stats)))
 
-    def step_learned(self, dB, net, stats):
+    def step_learned(self, dB, net, stats, w=OMEGA, jacobi=False):
         b = self.buffem
         self.ensure_c64()
-        b._check(self.L.bg_assemble(self.G.h, OMEGA, 0.0, self.M.h))
+        b._check(self.L.bg_assemble(self.G.h, w, 0.0, self.M.h))
         b._check(self.L.bg_matrix_convert(self.M.h, self.F.h))
-        P = b.Preconditioner.learned(self.G, self.M, OMEGA, net)
-        self.rhs_device(dB)
+        P = b.Preconditioner.jacobi(self.M) if jacobi else b.Preconditioner.learned(self.G, self.M, w, net)
+        self.rhs_device(dB, w)
         b._check(self.L.bg_gmres_solve_lu_fallback_device(
             self.M.h, self.F.h, P.h, b.C.c_void_p(dB.data_ptr()), self.N, self.nrhs, GMRES["tol"],
             GMRES["restart"], GMRES["maxit"], GMRES["inner_tol"], b._ptr(stats)))
@@ -533,7 +567,7 @@ def run_gpu(args, rank, world, local_rank):
     launches = buffem.launch_count() - launches0
     clk = clocks.stop()
     learned = {"steps_per_frequency": int(stats[0]), "final_rel_residual": float(stats[1]),
-               "refinement_sweeps": int(stats[2]), "lu_fallback": bool(stats[3])}
+               "refinement_sweeps": int(stats[2]), "lu_fallback": bool(stats[3]), "gmres": buffem.GMRESLastInfo()}
     # phase breakdown of one more (untimed) step, events on the library stream
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
     ev[0].record(stream)
@@ -573,6 +607,22 @@ def run_gpu(args, rank, world, local_rank):
     learned["jacobi_same_solve"] = {"steps": int(js[0]), "solve_s": e0.elapsed_time(e1) / 1e3,
                                     "lu_fallback": bool(js[3])}
     del P
+    # the learned form across the frequency range of the workload (omega in
+    # [0.5, 3]; the headline runs omega = 1): steps, fallback and device time
+    # of one whole step each, beside Jacobi's steps at the same omega
+    if not args.lean:
+        sweep = []
+        for w in (0.5, 2.0, 3.0):
+            st = np.zeros(4)
+            t = timed(stream, lambda: case.step_learned(dB, net, st, w=w), 1, 0, world)
+            info = buffem.GMRESLastInfo()
+            sj = np.zeros(4)
+            tj = timed(stream, lambda: case.step_learned(dB, net, sj, w=w, jacobi=True), 1, 0, world)
+            sweep.append({"omega": w, "step_s": t, "steps": int(st[0]), "final_rel_residual": float(st[1]),
+                          "lu_fallback": bool(st[3]), "switched_to_jacobi": info["switched_to_jacobi"],
+                          "stopped_early": info["stopped_early"], "longest_cycle": info["longest_cycle"],
+                          "jacobi_steps": int(sj[0]), "jacobi_step_s": tj, "jacobi_lu_fallback": bool(sj[3])})
+        learned["omega_sweep"] = sweep
     # e2e through host buffers
     hostB = np.zeros((N, case.nrhs), complex, order="F")
     rhs_h = np.zeros(N, complex)
@@ -611,6 +661,8 @@ def run_gpu(args, rank, world, local_rank):
         sec["precision_form_s"] = t / 2
         sec["precision_form_err_vs_fp64_lu"] = rel_err(dB, ref)
         sec["precision_form_gemm_tflops"] = pm["lu_gemm"]["flops"] / (pm["lu_gemm"]["ms"] / 1e3) / 1e12 if pm["lu_gemm"]["ms"] else None
+        sec["precision_form_kernel_ms_per_step"] = {k: v["ms"] / 2 for k, v in pm.items() if v["launches"]}
+        sec["fp64_kernel_ms_per_step"] = {k: v["ms"] / 2 for k, v in pf.items() if v["launches"]}
         st4 = np.zeros(4)
         t = timed(stream, lambda: sc.step_learned(dB, net, st4), 2, 1, world)
         sec["learned_s"] = t / 2
@@ -621,7 +673,46 @@ def run_gpu(args, rank, world, local_rank):
         sc.free()
         del dB, ref
         torch.cuda.empty_cache()
+        out["jittered_n19872"] = run_jittered(args, stream, net, world)
     return out
+
+
+def run_jittered(args, stream, net, world):
+    """The 12^3-cell sphere with jittered vertices: (a) the precision-form
+    configuration (+-0.05 h, seed 2, Janus eps = 4+0.2i for z > 0, 12+1i
+    below), precision form and learned form against the FP64 path; (b) the
+    graph network's held-out training check (+-0.1 h, seed 4254, eps 6+0.5i),
+    learned form against Jacobi.  omega = 1, three plane waves."""
+    import torch
+    import buffem
+    res = {}
+    cases = (("janus_jitter0.05", buffem.Material(kind=buffem.BG_MAT_JANUS_Z, eps=4 + 0.2j, eps2=12 + 1j), 0.05, 2),
+             ("eps6_jitter0.1", buffem.Material(eps=EPS_LEARNED), 0.1, 4242 + 12))
+    for name, mat, jit, seed in cases:
+        sc = Case(args.n_small, mat, args.order, jitter=jit, seed=seed)
+        dB = torch.zeros((sc.nrhs, sc.N), dtype=torch.complex128, device="cuda")
+        r = {"N": sc.N, "jitter": jit, "seed": seed, "precompute_s": sc.precompute_s}
+        r["fp64_path_s"] = timed(stream, lambda: sc.step_fp64(dB), 1, 1, world)
+        ref = dB.clone()
+        st = np.zeros(3)
+        r["precision_form_s"] = timed(stream, lambda: sc.step_precision(dB, st), 1, 1, world)
+        r["precision_form_err_vs_fp64_lu"] = rel_err(dB, ref)
+        r["precision_form_refinement_sweeps"] = int(st[0])
+        st4 = np.zeros(4)
+        r["learned_s"] = timed(stream, lambda: sc.step_learned(dB, net, st4), 1, 1, world)
+        r["learned_gmres"] = buffem.GMRESLastInfo()
+        r["learned_err_vs_fp64_lu"] = rel_err(dB, ref)
+        r["learned_steps"] = int(st4[0])
+        r["learned_lu_fallback"] = bool(st4[3])
+        sj = np.zeros(4)
+        r["jacobi_s"] = timed(stream, lambda: sc.step_learned(dB, net, sj, jacobi=True), 1, 0, world)
+        r["jacobi_steps"] = int(sj[0])
+        r["jacobi_lu_fallback"] = bool(sj[3])
+        res[name] = r
+        sc.free()
+        del dB, ref
+        torch.cuda.empty_cache()
+    return res
 
 
 # ------------------------------------------------------------------ CPU arm
@@ -780,8 +871,10 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the GetFields and buff-neq flux measurements")
     ap.add_argument("--lean", action="store_true",
                     help="headline learned steps only (no FP64 arm, e2e, secondary, CPU baseline): profiler runs")
-    ap.add_argument("--kernel", default=None, choices=["gemm", "fields", "neq"],
+    ap.add_argument("--kernel", default=None, choices=["gemm", "cgemm", "fields", "neq"],
                     help="one small case for profilers: gemm = the LU trailing-update GEMM on an M=N=K=--size "
+                         "problem (complex128, DMMA); cgemm = the same on the complex64 tcgen05 GEMM of the "
+                         "precision form; "
                          "problem; fields = two GetFields calls, 2048 far points on the --size-cell sphere; "
                          "neq = two buff-neq flux frequencies on the --size-cell sphere")
     ap.add_argument("--size", type=int, default=8192)
@@ -790,6 +883,9 @@ def main():
 
     if args.kernel == "gemm":
         print(json.dumps(gemm_kernel_bench(args.size)), flush=True)
+        return
+    if args.kernel == "cgemm":
+        print(json.dumps(cgemm_kernel_bench(args.size)), flush=True)
         return
     if args.kernel in ("fields", "neq"):
         print(json.dumps(small_case(args.kernel, args.size)), flush=True)
@@ -886,6 +982,8 @@ def main():
                              "kernel_classes": pf}
     if "secondary" in res:
         line["secondary_n19872"] = res["secondary"]
+    if "jittered_n19872" in res:
+        line["jittered_n19872"] = res["jittered_n19872"]
     if not args.lean and not args.no_batch:
         line["batching_form"] = run_batching()
     if not args.lean and not args.no_extras and world == 1:

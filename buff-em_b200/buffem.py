@@ -78,13 +78,13 @@ EXPORTS = [
     "bg_matrix_device_ptr", "bg_lu_factor", "bg_lu_pivots", "bg_lu_solve", "bg_lu_solve_device",
     "bg_rhs_planewave", "bg_rhs_planewave_device", "bg_pft", "bg_kernel_launch_count",
     "bg_synchronize", "bg_stream", "bg_profile_begin", "bg_profile_read", "bg_profile_end",
-    "bg_zgemm_sub_device", "bg_matrix_convert", "bg_lu_solve_refined", "bg_lu_solve_refined_device",
+    "bg_zgemm_sub_device", "bg_cgemm_sub_device", "bg_matrix_convert", "bg_lu_solve_refined", "bg_lu_solve_refined_device",
     "bg_lu_solve_device_noalloc", "bg_precond_create_jacobi", "bg_precond_destroy", "bg_precond_nnz",
     "bg_gmres_solve", "bg_gmres_solve_device", "bg_gnn_create", "bg_gnn_destroy", "bg_gnn_num_params",
     "bg_gnn_get_params", "bg_gnn_set_params", "bg_gnn_get_grads", "bg_gnn_train_step",
     "bg_precond_create_learned", "bg_precond_download", "bg_gmres_solve_mixed", "bg_gmres_solve_mixed_device",
     "bg_precond_bound", "bg_gmres_solve_lu_fallback", "bg_gmres_solve_lu_fallback_device", "bg_batch_sweep",
-    "bg_pft_full", "bg_fibbi_store", "bg_fibbi_load", "bg_get_fields", "bg_get_fields_device",
+    "bg_pft_full", "bg_gmres_last_info", "bg_fibbi_store", "bg_fibbi_load", "bg_get_fields", "bg_get_fields_device",
     "bg_neq_create", "bg_neq_destroy", "bg_neq_flux", "bg_neq_dressed_rytov", "bg_pft_dr_device",
 ]
 
@@ -157,6 +157,7 @@ def lib():
         L.bg_rhs_planewave_device.argtypes = [P, D, D, VP, VP, VP]
         L.bg_pft.argtypes = [P, D, D, VP, VP, VP, I, VP]
         L.bg_pft_full.argtypes = [P, D, D, VP, VP, VP, VP]
+        L.bg_gmres_last_info.argtypes = [VP]
         L.bg_get_fields.argtypes = [P, D, D, VP, VP, VP, C.c_int, VP, VP]
         L.bg_neq_create.argtypes = [P, C.POINTER(P)]
         L.bg_neq_destroy.argtypes = [P]
@@ -171,6 +172,7 @@ def lib():
         L.bg_stream.restype = VP
         L.bg_profile_read.argtypes = [I, VP, VP, VP]
         L.bg_zgemm_sub_device.argtypes = [I, I, I, VP, I, VP, I, VP, I]
+        L.bg_cgemm_sub_device.argtypes = [I, I, I, VP, I, VP, I, VP, I]
         L.bg_matrix_convert.argtypes = [P, P]
         L.bg_lu_solve_refined.argtypes = [P, P, VP, I, D, I, VP]
         L.bg_lu_solve_refined_device.argtypes = [P, P, VP, I, I, D, I, VP]
@@ -506,6 +508,11 @@ class NEQ:
         return out
 
 
+def cgemm_sub_device(M, N, K, A, lda, B, ldb, C, ldc):
+    """C -= A B for device complex64 column-major matrices (tcgen05 TF32 GEMM)."""
+    _check(lib().bg_cgemm_sub_device(M, N, K, C_void(A), lda, C_void(B), ldb, C_void(C), ldc))
+
+
 def zgemm_sub_device(M, N, K, A, lda, B, ldb, C, ldc):
     """C -= A @ B on device pointers (complex128, column-major)."""
     _check(lib().bg_zgemm_sub_device(M, N, K, C_void(A), lda, C_void(B), ldb, C_void(C), ldc))
@@ -638,6 +645,15 @@ def GMRESSolveMixed(M, F, B, P=None, tol=1e-10, restart=50, maxit=2000, inner_to
     _check(lib().bg_gmres_solve_mixed(M.h, F.h, P.h if P is not None else None, _ptr(arr), nrhs, float(tol),
                                       int(restart), int(maxit), float(inner_tol), _ptr(st)))
     return arr, st
+
+
+def GMRESLastInfo():
+    """The calling thread's last mixed-precision solve: dict of steps,
+    relres, sweeps, switched_to_jacobi, stopped_early, longest_cycle."""
+    out = np.zeros(6)
+    _check(lib().bg_gmres_last_info(_ptr(out)))
+    return {"steps": int(out[0]), "relres": float(out[1]), "sweeps": int(out[2]),
+            "switched_to_jacobi": bool(out[3]), "stopped_early": bool(out[4]), "longest_cycle": int(out[5])}
 
 
 def SolveLearned(M, F, B, P=None, tol=1e-10, restart=50, maxit=1000, inner_tol=1e-5):

@@ -737,6 +737,18 @@ int bg_gmres_solve_lu_fallback_device(bg_matrix *A, bg_matrix *F, const bg_preco
   return st;
 }
 
+int bg_gmres_last_info(double *out) {
+  if (!out) { set_error("bg_gmres_last_info: null output"); return BG_ERR_ARG; }
+  GmInfo g = gmres_last_info();
+  out[0] = g.steps;
+  out[1] = g.relres;
+  out[2] = g.sweeps;
+  out[3] = g.switched;
+  out[4] = g.gave_up;
+  out[5] = g.longest_cycle;
+  return BG_OK;
+}
+
 int bg_gmres_solve_lu_fallback(bg_matrix *A, bg_matrix *F, const bg_precond *P, double *B, int nrhs, double tol,
                                int restart, int maxit, double inner_tol, double *stats) {
   if (!A || !B || nrhs <= 0) { set_error("bg_gmres_solve_lu_fallback: bad arguments"); return BG_ERR_ARG; }
@@ -907,6 +919,17 @@ int bg_zgemm_sub_device(int M, int N, int K, const void *A, int lda, const void 
     return BG_ERR_ARG;
   }
   return zgemm_sub_device(M, N, K, A, lda, B, ldb, C, ldc);
+}
+
+int bg_cgemm_sub_device(int M, int N, int K, const void *A, int lda, const void *B, int ldb, void *C, int ldc) {
+  if (M < 0 || N < 0 || K < 0 || (M && N && K && (!A || !B || !C)) || lda < M || ldb < K || ldc < M ||
+      lda < 1 || ldb < 1 || ldc < 1) {
+    set_error("bg_cgemm_sub_device: bad arguments");
+    return BG_ERR_ARG;
+  }
+  int st = ensure_device();
+  if (st) return st;
+  return cgemm_sub_device(M, N, K, A, lda, B, ldb, C, ldc);
 }
 
 long long bg_kernel_launch_count(void) { return g_launches.load(); }

@@ -642,10 +642,30 @@ static int colnorms(const z2 *X, GmState &S, std::vector<double> &out) {
   return BG_OK;
 }
 
+// Restart policy.  A cycle has the requested length (restart); after a cycle
+// that fails to halve the true residual the next one is twice as long, up
+// to GM_MAXGROW times the request and at most GM_MAXM steps (restarted
+// GMRES stagnates on indefinite problems -- the VIE system at high
+// frequency -- where a longer cycle still converges; a cycle that keeps
+// halving the residual never grows).  With an alternative preconditioner
+// Palt, a first cycle of P that fails to halve the residual switches to
+// Palt for the rest of the solve (right preconditioning: every restart
+// solves for a correction, so the switch needs nothing else).  The solve
+// stops early, unconverged, once the rate of the last cycle could not reach
+// tol within the remaining steps even at twice that rate, so that a caller
+// with a direct fallback does not spend the whole budget first.
+#define GM_MAXM 200
+#define GM_MAXGROW 4
+
+static thread_local GmInfo t_gm_info;
+GmInfo gmres_last_info() { return t_gm_info; }
+
 // solve A X = B (device, N x nrhs complex128, in place), right preconditioner P
 int gmres_solve(bg_matrix *A, const bg_precond *P, void *dB, int ldb, int nrhs, double tol, int restart, int maxit,
-                double *stats) {
-  int N = A->N, m = std::max(2, std::min(restart, 200));
+                double *stats, const bg_precond *Palt) {
+  const int m0 = std::max(2, std::min(restart, GM_MAXM));
+  const int N = A->N, m = std::max(m0, std::min(GM_MAXGROW * m0, GM_MAXM));   // m: allocation and strides
+  int mc = m0;                                                                 // current cycle length
   if (nrhs > GM_MAXRHS) { set_error("gmres: at most %d right-hand sides per call", GM_MAXRHS); return BG_ERR_ARG; }
   GmState S{N, nrhs, m};
   S.nchunk = (N + GV_COLS - 1) / GV_COLS;
@@ -687,8 +707,9 @@ int gmres_solve(bg_matrix *A, const bg_precond *P, void *dB, int ldb, int nrhs, 
   std::vector<double> bn, rn;
   if ((st = colnorms(S.W, S, bn))) { cudaFreeAsync(w, stream()); return st; }
   for (auto &v : bn) v = std::max(v, 1e-300);
-  int total = 0;
-  double relres = 1.0, first = -1;
+  int total = 0, cycles = 0, switched = 0, gave_up = 0, longest = mc;
+  double relres = 1.0, first = -1, prev = -1;
+  int prev_len = 0;
   dim3 gr((N + 255) / 256, nrhs);
   while (!st && total < maxit) {
     // R = B - A X
@@ -702,6 +723,31 @@ int gmres_solve(bg_matrix *A, const bg_precond *P, void *dB, int ldb, int nrhs, 
     for (int j = 0; j < nrhs; j++) relres = std::max(relres, rn[j] / bn[j]);
     if (first < 0) first = relres;
     if (relres <= tol) break;
+    if (prev > 0 && prev_len > 0) {
+      const double red = relres / prev;   // reduction over the last cycle
+      if (red > 0.5) {
+        if (cycles == 1 && Palt && !switched) {
+          P = Palt;              // the given preconditioner stagnates: switch
+          switched = 1;
+          mc = m0;
+        } else if (mc < m) {
+          mc = std::min(2 * mc, m);
+        }
+      }
+      // early stop: at twice the last cycle's rate per step the target is
+      // still out of reach within the remaining steps
+      if (!switched || cycles > 1) {
+        double rate = std::pow(std::max(red, 1e-300), 1.0 / prev_len);
+        double need = std::log(tol / relres) / std::log(std::max(rate * rate, 1e-300));
+        if (rate >= 1.0 || (std::isfinite(need) && need > (double)(maxit - total))) {
+          gave_up = 1;
+          break;
+        }
+      }
+    }
+    prev = relres;
+    longest = std::max(longest, mc);
+    cycles++;
     // V[:,0] = Z / beta
     std::vector<double> inv(nrhs);
     for (int j = 0; j < nrhs; j++) inv[j] = rn[j] > 0 ? 1.0 / rn[j] : 0.0;
@@ -716,7 +762,7 @@ int gmres_solve(bg_matrix *A, const bg_precond *P, void *dB, int ldb, int nrhs, 
     }
     const int total0 = total;
     int k = 0, kconv = -1, checked = 0;
-    for (; k < m && total < maxit; k++, total++) {
+    for (; k < mc && total < maxit; k++, total++) {
       // W = A M V[:,k]
       z2 *vk = S.V + (size_t)k * N;   // rhs j at vk + j*vstride: gather into R contiguous
       for (int j = 0; j < nrhs; j++)
@@ -743,7 +789,7 @@ int gmres_solve(bg_matrix *A, const bg_precond *P, void *dB, int ldb, int nrhs, 
         k_gm_scale_copy<<<gr, 256, 0, stream()>>>(N, S.W, N, S.sc, S.V, (size_t)(k + 1) * N, vstride);
         g_launches++;
       }
-      if ((k + 1) % GM_CHECK == 0 || k + 1 == m || total + 1 == maxit) {
+      if ((k + 1) % GM_CHECK == 0 || k + 1 == mc || total + 1 == maxit) {
         // one round trip for the residual estimates of the last few steps
         BG_CUDA_TRY(cudaMemcpy2DAsync(res_host, sizeof(double) * m, resd, sizeof(double) * m,
                                       sizeof(double) * (k + 1), nrhs, cudaMemcpyDeviceToHost, stream()));
@@ -777,6 +823,7 @@ int gmres_solve(bg_matrix *A, const bg_precond *P, void *dB, int ldb, int nrhs, 
     // g entries before a step are final once that step is done)
     if (conv) k = kconv + 1;
     total = total0 + k;
+    prev_len = k;
     std::vector<z2> Hh(nH), gh(ng);
     BG_CUDA_TRY(cudaMemcpyAsync(Hh.data(), Hd, sizeof(z2) * nH, cudaMemcpyDeviceToHost, stream()));
     BG_CUDA_TRY(cudaMemcpyAsync(gh.data(), gd, sizeof(z2) * ng, cudaMemcpyDeviceToHost, stream()));
@@ -819,6 +866,9 @@ int gmres_solve(bg_matrix *A, const bg_precond *P, void *dB, int ldb, int nrhs, 
   }
   cudaFreeAsync(w, stream());
   if (stats) { stats[0] = total; stats[1] = relres; stats[2] = first; }
+  t_gm_info.switched |= switched;
+  t_gm_info.gave_up |= gave_up;
+  t_gm_info.longest_cycle = std::max(t_gm_info.longest_cycle, longest);
   return st;
 }
 
@@ -851,14 +901,22 @@ int gmres_solve_mixed(bg_matrix *A, bg_matrix *F, const bg_precond *P, void *dB,
   for (auto &v : bn) v = std::max(v, 1e-300);
   int total = 0, sweeps = 0;
   double relres = 1.0;
+  t_gm_info = GmInfo{};
+  // the diagonal of A: the preconditioner a stagnating P is replaced by
+  bg_precond *J = nullptr;
+  if (P && (st = precond_jacobi(A, &J))) { cudaFreeAsync(w, stream()); return st; }
+  const bg_precond *Pcur = P;
   while (!st && relres > tol && total < maxit && sweeps < 40) {
     double ist[3] = {0, 0, 0};
     // R <- approximately F^{-1} R (in place); the last sweeps only need the
     // remaining reduction (with a 0.3 margin), not a full inner_tol
     double itol = std::min(0.5, std::max(inner_tol, 0.3 * tol / relres));
-    if ((st = gmres_solve(F, P, R, N, nrhs, itol, restart, maxit - total, ist))) break;
+    const int sw0 = t_gm_info.switched;
+    if ((st = gmres_solve(F, Pcur, R, N, nrhs, itol, restart, maxit - total, ist, Pcur == P ? J : nullptr))) break;
+    if (t_gm_info.switched && !sw0) Pcur = J;   // later sweeps keep the replacement
     total += (int)ist[0];
     sweeps++;
+    if (t_gm_info.gave_up) break;
     k_gm_axpy<<<gr, 256, 0, stream()>>>(N, R, N, X, N, 1);
     g_launches++;
     if ((st = dense_matvec(A, X, T, S))) break;
@@ -875,8 +933,12 @@ int gmres_solve_mixed(bg_matrix *A, bg_matrix *F, const bg_precond *P, void *dB,
                                       cudaMemcpyDeviceToDevice, stream());
     if (e != cudaSuccess) { set_error("gmres: %s", cudaGetErrorString(e)); st = BG_ERR_CUDA; }
   }
+  if (J) bg_precond_destroy(J);
   cudaFreeAsync(w, stream());
   if (stats) { stats[0] = total; stats[1] = relres; stats[2] = sweeps; }
+  t_gm_info.steps = total;
+  t_gm_info.relres = relres;
+  t_gm_info.sweeps = sweeps;
   return st;
 }
 

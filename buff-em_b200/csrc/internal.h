@@ -277,11 +277,21 @@ int lu_solve_enqueue(bg_matrix *m, void *dB, int ldb, int nrhs, void *dT);
 void lu_set_panel_rows(int rows);
 int lu_get_panel_rows();
 int gmres_solve(bg_matrix *A, const bg_precond *P, void *dB, int ldb, int nrhs, double tol, int restart, int maxit,
-                double *stats);
+                double *stats, const bg_precond *Palt = nullptr);
+// what the last mixed-precision solve of this thread did beyond its stats
+struct GmInfo {
+  int steps = 0, sweeps = 0;
+  double relres = 0;
+  int switched = 0;        // the given preconditioner stagnated: the rest ran with Jacobi
+  int gave_up = 0;         // stopped early: the observed rate could not reach the target
+  int longest_cycle = 0;   // longest restart cycle used
+};
+GmInfo gmres_last_info();
 int gmres_solve_mixed(bg_matrix *A, bg_matrix *F, const bg_precond *P, void *dB, int ldb, int nrhs, double tol,
                       int restart, int maxit, double inner_tol, double *stats);
 int precond_jacobi(bg_matrix *A, bg_precond **out);
 int zgemm_sub_device(int M, int N, int K, const void *A, int lda, const void *B, int ldb, void *C, int ldc);
+int cgemm_sub_device(int M, int N, int K, const void *A, int lda, const void *B, int ldb, void *C, int ldc);
 int matrix_convert(const bg_matrix *src, bg_matrix *dst);
 int solve_refined(bg_matrix *A, bg_matrix *F, void *dB, int ldb, int nrhs, double tol, int maxit, double *stats);
 void gauss_legendre01(int n, double *x, double *w);

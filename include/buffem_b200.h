@@ -264,6 +264,14 @@ int bg_lu_solve_device_noalloc(bg_matrix *m, void *B_dev, int ldb, int nrhs);
    GEMMs per source object).  Runs on the library stream. */
 int bg_zgemm_sub_device(int M, int N, int K, const void *A, int lda, const void *B, int ldb, void *C, int ldc);
 
+/* C <- C - A*B for device column-major complex64 matrices: the tcgen05
+   (kind::tf32) tensor-core GEMM of the precision form's LU trailing update
+   (no reference counterpart).  TF32 products, FP32 accumulation.  B is read
+   through a tensor map: it must start on a 16-byte boundary and ldb must be
+   even (BG_ERR_ARG otherwise).  Synchronises the library stream; a pipeline
+   timeout inside the kernel is reported as BG_ERR_CUDA. */
+int bg_cgemm_sub_device(int M, int N, int K, const void *A, int lda, const void *B, int ldb, void *C, int ldc);
+
 /* ---------------------------------------------------------------------------
  * precision form: complex64 tensor-core LU + FP64 iterative refinement
  * (no reference counterpart; the reference factors in complex128 only)
@@ -297,8 +305,12 @@ int bg_precond_nnz(const bg_precond *P);
 /* Restarted GMRES(restart) in FP64 on the device with right preconditioner P
    (NULL: none) for A X = B; up to 4 right-hand sides advance in lockstep so
    each step reads A once.  Stops when max_j |b_j - A x_j| / |b_j| <= tol or
-   after maxit matrix-vector steps.  stats (3 doubles, may be NULL): steps,
-   final and initial relative residual.  B: host N x nrhs complex128. */
+   after maxit matrix-vector steps.  A cycle that fails to halve the true
+   residual doubles the next cycle's length (up to 4 x restart, at most 200;
+   a converging GMRES(restart) is unchanged), and the solve returns early,
+   unconverged, once the last cycle's rate could not reach tol within the
+   remaining steps even if it doubled.  stats (3 doubles, may be NULL):
+   steps, final and initial relative residual.  B: host N x nrhs complex128. */
 int bg_gmres_solve(bg_matrix *A, const bg_precond *P, double *B_host, int nrhs, double tol, int restart, int maxit,
                    double *stats);
 int bg_gmres_solve_device(bg_matrix *A, const bg_precond *P, void *B_dev, int ldb, int nrhs, double tol, int restart,
@@ -309,7 +321,10 @@ int bg_gmres_solve_device(bg_matrix *A, const bg_precond *P, void *B_dev, int ld
    FP64 iterative refinement with the complex128 A between them, until
    max_j |b_j - A x_j| / |b_j| <= tol or maxit Krylov steps in total.
    stats (3 doubles, may be NULL): Krylov steps, final relative residual,
-   refinement sweeps.  P as for bg_gmres_solve (built from A). */
+   refinement sweeps.  P as for bg_gmres_solve (built from A); when the first
+   cycle with a given P fails to halve the residual, the solve continues
+   with the diagonal (Jacobi) preconditioner of A (bg_gmres_last_info
+   reports it). */
 int bg_gmres_solve_mixed(bg_matrix *A, bg_matrix *F, const bg_precond *P, double *B_host, int nrhs, double tol,
                          int restart, int maxit, double inner_tol, double *stats);
 int bg_gmres_solve_mixed_device(bg_matrix *A, bg_matrix *F, const bg_precond *P, void *B_dev, int ldb, int nrhs,
@@ -323,6 +338,11 @@ int bg_gmres_solve_mixed_device(bg_matrix *A, bg_matrix *F, const bg_precond *P,
    LU fallback ran. */
 int bg_gmres_solve_lu_fallback(bg_matrix *A, bg_matrix *F, const bg_precond *P, double *B_host, int nrhs,
                                double tol, int restart, int maxit, double inner_tol, double *stats);
+/* What the calling thread's last mixed-precision solve did (6 doubles):
+   Krylov steps, final relative residual, refinement sweeps, 1 if the given
+   preconditioner was replaced by Jacobi, 1 if the Krylov solve stopped early
+   on its convergence rate, the longest restart cycle used. */
+int bg_gmres_last_info(double *out);
 int bg_gmres_solve_lu_fallback_device(bg_matrix *A, bg_matrix *F, const bg_precond *P, void *B_dev, int ldb,
                                       int nrhs, double tol, int restart, int maxit, double inner_tol,
                                       double *stats);

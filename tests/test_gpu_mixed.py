@@ -67,3 +67,30 @@ def test_mixed_singular_reports_info():
     with pytest.raises(buffem.BuffError) as e:
         F.LUFactorize()
     assert e.value.status == 8
+
+
+@pytest.mark.parametrize("M,N,K", [(1, 1, 1), (70, 33, 17), (300, 130, 64), (513, 200, 1000), (2100, 300, 40),
+                                   (8192, 600, 256)])
+def test_cgemm_tf32_device(M, N, K):
+    """C -= A B on the tcgen05 TF32 tensor cores (complex64): against the
+    complex128 product of the same complex64 inputs, entrywise within
+    2^-9 (|A| |B|)_ij plus FP32 rounding of C -- TF32 keeps 10 mantissa bits
+    of each operand and accumulates in FP32.  The shapes cover ragged tiles,
+    both tile widths (N <= 128 and N > 128) and more tiles than SMs, so the
+    persistent CTAs cycle through both TMEM accumulators."""
+    import torch
+    rng = np.random.default_rng(M + 3 * N + 7 * K)
+    A = (rng.normal(size=(M, K)) + 1j * rng.normal(size=(M, K))).astype(np.complex64)
+    B = (rng.normal(size=(K, N)) + 1j * rng.normal(size=(K, N))).astype(np.complex64)
+    Cm = (rng.normal(size=(M, N)) + 1j * rng.normal(size=(M, N))).astype(np.complex64)
+    ldb = K + (K & 1)                 # B's columns on 16-byte boundaries (tensor map)
+    Bp = np.zeros((N, ldb), np.complex64)
+    Bp[:, :K] = B.T
+    dA = torch.tensor(A.T.copy(), device="cuda")
+    dB = torch.tensor(Bp, device="cuda")
+    dC = torch.tensor(Cm.T.copy(), device="cuda")
+    buffem.cgemm_sub_device(M, N, K, dA.data_ptr(), M, dB.data_ptr(), ldb, dC.data_ptr(), M)
+    out = dC.cpu().numpy().T.astype(np.complex128)
+    ref = Cm.astype(np.complex128) - A.astype(np.complex128) @ B.astype(np.complex128)
+    bound = 2.0 ** -9 * (np.abs(A).astype(np.float64) @ np.abs(B).astype(np.float64)) + 1e-6 * np.abs(Cm)
+    assert np.all(np.abs(out - ref) <= bound), float((np.abs(out - ref) / bound).max())
