@@ -691,7 +691,8 @@ def synchronize():
 
 
 PROF_CLASSES = ("lu_gemm", "lu_panel", "lu_laswp", "trsm_leaf", "assemble_far", "assemble_near_gram",
-                "gmres_matvec", "gnn_precond", "gmres_orthogonalise", "gmres_precond_apply")
+                "gmres_matvec", "gnn_precond", "gmres_orthogonalise", "gmres_precond_apply", "lu_solve_trsv",
+                "refine_residual")
 
 
 def profile_begin():

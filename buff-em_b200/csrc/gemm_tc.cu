@@ -270,16 +270,26 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 
 // A~ (row-major 2M x 2K, leading dimension lda2 floats) from complex A (M x K
 // column-major, lda complex): rows 2m, 2m+1 and columns 2k, 2k+1 hold
-// [[ar, -ai], [ai, ar]]
-__global__ void k_expand_a(int M, int K, const float2 *A, size_t lda, float *At, size_t lda2) {
-  int m = blockIdx.x * blockDim.x + threadIdx.x;
-  int k = blockIdx.y;
-  if (m >= M || k >= K) return;
-  float2 a = A[(size_t)k * lda + m];
-  float *r0 = At + (size_t)(2 * m) * lda2 + 2 * k;
-  float *r1 = r0 + lda2;
-  *(float2 *)r0 = make_float2(a.x, -a.y);
-  *(float2 *)r1 = make_float2(a.y, a.x);
+// [[ar, -ai], [ai, ar]].  32 x 32 tiles through shared memory: reads
+// coalesced along m (A's columns), writes coalesced along k (A~'s rows).
+__global__ void __launch_bounds__(256) k_expand_a(int M, int K, const float2 *A, size_t lda, float *At, size_t lda2) {
+  __shared__ float2 tile[32][33];
+  const int m0 = blockIdx.x * 32, k0 = blockIdx.y * 32, tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int k = k0 + ty + 8 * q, m = m0 + tx;
+    if (k < K && m < M) tile[ty + 8 * q][tx] = A[(size_t)k * lda + m];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int m = m0 + ty + 8 * q, k = k0 + tx;
+    if (k < K && m < M) {
+      const float2 a = tile[tx][ty + 8 * q];
+      *(float2 *)(At + (size_t)(2 * m) * lda2 + 2 * k) = make_float2(a.x, -a.y);
+      *(float2 *)(At + (size_t)(2 * m + 1) * lda2 + 2 * k) = make_float2(a.y, a.x);
+    }
+  }
 }
 
 // ------------------------------------------------------------------ host side
@@ -340,8 +350,8 @@ int cgemm_sub_tf32(int M, int N, int K, const void *A, size_t lda, const void *B
                    float *At, int *err) {
   if (M <= 0 || N <= 0 || K <= 0) return BG_OK;
   size_t lda2 = ((size_t)2 * K + 31) / 32 * 32;
-  dim3 eg((M + 127) / 128, K);
-  k_expand_a<<<eg, 128, 0, stream()>>>(M, K, (const float2 *)A, lda, At, lda2);
+  dim3 eg((M + 31) / 32, (K + 31) / 32);
+  k_expand_a<<<eg, 256, 0, stream()>>>(M, K, (const float2 *)A, lda, At, lda2);
   BG_LAUNCHED();
   const int BN = N > 128 ? 256 : 128;
   CUtensorMap mA, mB;

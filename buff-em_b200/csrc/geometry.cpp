@@ -254,13 +254,19 @@ int upload_geometry(bg_geometry *g) {
         fi[k] = (f >= 0 && f < o.nif) ? f + g->bfOffset[no] : -1;
       }
       tetFI.push_back(make_int4(fi[0], fi[1], fi[2], fi[3]));
+      double cen[3] = {0, 0, 0};
+      for (int i = 0; i < 4; i++)
+        for (int k = 0; k < 3; k++) cen[k] += 0.25 * o.V[3 * T[i] + k];
       for (int j = 0; j < 4; j++) {
+        double d2 = 0.0;
         for (int k = 0; k < 3; k++) {
           double s = 0.0;
           for (int i = 0; i < 4; i++) s += (i == j ? qb : qa) * o.V[3 * T[i] + k];
           tetP4.push_back(s);
+          d2 += (s - cen[k]) * (s - cen[k]);
         }
         tetP4.push_back(0.0);
+        g->rule_rmax = std::max(g->rule_rmax, std::sqrt(d2));
       }
     }
     for (int a = 0; a < o.nif; a++) {

@@ -643,17 +643,18 @@ static int colnorms(const z2 *X, GmState &S, std::vector<double> &out) {
 }
 
 // Restart policy.  A cycle has the requested length (restart); after a cycle
-// that fails to halve the true residual the next one is twice as long, up
-// to GM_MAXGROW times the request and at most GM_MAXM steps (restarted
-// GMRES stagnates on indefinite problems -- the VIE system at high
-// frequency -- where a longer cycle still converges; a cycle that keeps
-// halving the residual never grows).  With an alternative preconditioner
-// Palt, a first cycle of P that fails to halve the residual switches to
-// Palt for the rest of the solve (right preconditioning: every restart
-// solves for a correction, so the switch needs nothing else).  The solve
-// stops early, unconverged, once the rate of the last cycle could not reach
-// tol within the remaining steps even at twice that rate, so that a caller
-// with a direct fallback does not spend the whole budget first.
+// that reduces the true residual by less than a factor 10 the next one is
+// twice as long, up to GM_MAXGROW times the request and at most GM_MAXM
+// steps (restarted GMRES stagnates on indefinite problems -- the VIE system
+// at high frequency -- where a longer cycle still converges; a cycle that
+// gains a digit or more never grows).  With an alternative preconditioner
+// Palt, a cycle of full length that still gains less than a digit switches
+// to Palt for the rest of the solve (right preconditioning: every restart
+// solves for a correction, so the switch needs nothing else).  Once at full
+// length with nothing left to switch to, the solve stops early,
+// unconverged, when the last cycle's rate could not reach tol within the
+// remaining steps even at twice that rate, so that a caller with a direct
+// fallback does not spend the whole budget first.
 #define GM_MAXM 200
 #define GM_MAXGROW 4
 
@@ -662,10 +663,11 @@ GmInfo gmres_last_info() { return t_gm_info; }
 
 // solve A X = B (device, N x nrhs complex128, in place), right preconditioner P
 int gmres_solve(bg_matrix *A, const bg_precond *P, void *dB, int ldb, int nrhs, double tol, int restart, int maxit,
-                double *stats, const bg_precond *Palt) {
+                double *stats, const bg_precond *Palt, int *cycle) {
   const int m0 = std::max(2, std::min(restart, GM_MAXM));
   const int N = A->N, m = std::max(m0, std::min(GM_MAXGROW * m0, GM_MAXM));   // m: allocation and strides
-  int mc = m0;                                                                 // current cycle length
+  // current cycle length (a caller's earlier solve of the same system may have grown it)
+  int mc = cycle ? std::max(m0, std::min(*cycle, m)) : m0;
   if (nrhs > GM_MAXRHS) { set_error("gmres: at most %d right-hand sides per call", GM_MAXRHS); return BG_ERR_ARG; }
   GmState S{N, nrhs, m};
   S.nchunk = (N + GV_COLS - 1) / GV_COLS;
@@ -725,18 +727,21 @@ int gmres_solve(bg_matrix *A, const bg_precond *P, void *dB, int ldb, int nrhs, 
     if (relres <= tol) break;
     if (prev > 0 && prev_len > 0) {
       const double red = relres / prev;   // reduction over the last cycle
-      if (red > 0.5) {
-        if (cycles == 1 && Palt && !switched) {
-          P = Palt;              // the given preconditioner stagnates: switch
-          switched = 1;
-          mc = m0;
-        } else if (mc < m) {
+      const bool full = prev_len >= m;    // the last cycle had the longest length
+      bool just_switched = false;
+      if (red > 0.1) {
+        if (!full) {
           mc = std::min(2 * mc, m);
+        } else if (Palt && !switched) {
+          P = Palt;              // the given preconditioner stagnates at full length: switch
+          switched = 1;
+          just_switched = true;
         }
       }
-      // early stop: at twice the last cycle's rate per step the target is
-      // still out of reach within the remaining steps
-      if (!switched || cycles > 1) {
+      // early stop, at full length with nothing left to switch to (the rate
+      // of a cycle run with the replaced preconditioner does not count): at
+      // twice the last cycle's rate per step the target is still out of reach
+      if (full && (!Palt || switched) && !just_switched) {
         double rate = std::pow(std::max(red, 1e-300), 1.0 / prev_len);
         double need = std::log(tol / relres) / std::log(std::max(rate * rate, 1e-300));
         if (rate >= 1.0 || (std::isfinite(need) && need > (double)(maxit - total))) {
@@ -866,6 +871,7 @@ int gmres_solve(bg_matrix *A, const bg_precond *P, void *dB, int ldb, int nrhs, 
   }
   cudaFreeAsync(w, stream());
   if (stats) { stats[0] = total; stats[1] = relres; stats[2] = first; }
+  if (cycle) *cycle = mc;
   t_gm_info.switched |= switched;
   t_gm_info.gave_up |= gave_up;
   t_gm_info.longest_cycle = std::max(t_gm_info.longest_cycle, longest);
@@ -904,15 +910,17 @@ int gmres_solve_mixed(bg_matrix *A, bg_matrix *F, const bg_precond *P, void *dB,
   t_gm_info = GmInfo{};
   // the diagonal of A: the preconditioner a stagnating P is replaced by
   bg_precond *J = nullptr;
-  if (P && (st = precond_jacobi(A, &J))) { cudaFreeAsync(w, stream()); return st; }
+  if (P && !P->jacobi && (st = precond_jacobi(A, &J))) { cudaFreeAsync(w, stream()); return st; }
   const bg_precond *Pcur = P;
+  int cycle = restart;   // restart cycle length, carried over the refinement sweeps
   while (!st && relres > tol && total < maxit && sweeps < 40) {
     double ist[3] = {0, 0, 0};
     // R <- approximately F^{-1} R (in place); the last sweeps only need the
     // remaining reduction (with a 0.3 margin), not a full inner_tol
     double itol = std::min(0.5, std::max(inner_tol, 0.3 * tol / relres));
     const int sw0 = t_gm_info.switched;
-    if ((st = gmres_solve(F, Pcur, R, N, nrhs, itol, restart, maxit - total, ist, Pcur == P ? J : nullptr))) break;
+    if ((st = gmres_solve(F, Pcur, R, N, nrhs, itol, restart, maxit - total, ist, Pcur == P ? J : nullptr, &cycle)))
+      break;
     if (t_gm_info.switched && !sw0) Pcur = J;   // later sweeps keep the replacement
     total += (int)ist[0];
     sweeps++;
@@ -958,6 +966,7 @@ int precond_jacobi(bg_matrix *A, bg_precond **out) {
   bg_precond *P = new bg_precond();
   P->N = A->N;
   P->nnz = A->N;
+  P->jacobi = true;
   BG_CUDA_TRY(cudaMallocAsync((void **)&P->rowptr, sizeof(int) * (A->N + 1), stream()));
   BG_CUDA_TRY(cudaMallocAsync((void **)&P->col, sizeof(int) * A->N, stream()));
   BG_CUDA_TRY(cudaMallocAsync((void **)&P->val, sizeof(z2) * A->N, stream()));

@@ -49,7 +49,8 @@ int ensure_device();
 // kernel-class profiling (CUDA events around launches when enabled)
 enum {
   PROF_GEMM = 0, PROF_PANEL = 1, PROF_LASWP = 2, PROF_TRSM = 3, PROF_ASM_FAR = 4, PROF_ASM_NEAR = 5,
-  PROF_MATVEC = 6, PROF_GNN = 7, PROF_ORTHO = 8, PROF_PRECOND = 9, PROF_NCLASS = 12
+  PROF_MATVEC = 6, PROF_GNN = 7, PROF_ORTHO = 8, PROF_PRECOND = 9, PROF_TRSV = 10, PROF_RESID = 11,
+  PROF_NCLASS = 12
 };
 bool prof_on();
 void prof_start(int cls);
@@ -199,6 +200,7 @@ struct bg_geometry {
   long long sing_stats[6] = {0, 0, 0, 0, 0, 0};
   bool uploaded = false, precomputed = false;
   bool dispersive = false;      // some object's eps comes from a MATERIAL section
+  double rule_rmax = 0.0;       // largest distance of a 4-point rule point from its tetrahedron's centroid
   bg::NearGraph graph;
   double *d_scratch = nullptr;  // general scratch (PFT partial sums etc.)
   double *d_fieldTet = nullptr, *d_fieldFace = nullptr;  // GetFields tables, 16 doubles per tet each
@@ -211,6 +213,7 @@ struct bg_precond {
   int *rowptr = nullptr, *col = nullptr;   // CSR on the device
   void *val = nullptr;                     // complex128 values
   double rho = 0, theta = 0;               // learned: estimate of rho(K1) and the coefficient bound smax
+  bool jacobi = false;                     // the diagonal preconditioner
 };
 
 struct bg_matrix {
@@ -277,7 +280,7 @@ int lu_solve_enqueue(bg_matrix *m, void *dB, int ldb, int nrhs, void *dT);
 void lu_set_panel_rows(int rows);
 int lu_get_panel_rows();
 int gmres_solve(bg_matrix *A, const bg_precond *P, void *dB, int ldb, int nrhs, double tol, int restart, int maxit,
-                double *stats, const bg_precond *Palt = nullptr);
+                double *stats, const bg_precond *Palt = nullptr, int *cycle = nullptr);
 // what the last mixed-precision solve of this thread did beyond its stats
 struct GmInfo {
   int steps = 0, sweeps = 0;

@@ -102,27 +102,49 @@ __device__ __forceinline__ cd expikr(cd k, double r) {
   return cd{m * c, m * s};
 }
 
-// exp(i x) for |x| <= 1: Taylor series of cos and sin at y = x/2 (terms to
-// y^15; the first omitted terms, y^16/16! and y^17/17!, are below 1e-18 for
-// |y| <= 1/2), then cos x = c^2 - s^2, sin x = 2 c s
+// exp(i x) for |x| <= 1: Taylor series of cos and sin at y = x/2 in Horner
+// form (one fused multiply-add per term), then cos x = c^2 - s^2,
+// sin x = 2 c s.  Terms to y^14 / y^15: the first omitted terms, y^16/16!
+// and y^17/17!, are below 1e-18 for |y| <= 1/2.  expi_small_short serves
+// |x| <= 1/4 (|y| <= 1/8) with terms to y^10 / y^11 (first omitted terms
+// below 2e-20).
+#define EXPI_C(n, f) (((n) & 1 ? -1.0 : 1.0) / (f))
+__device__ __forceinline__ cd expi_halfangle(double c, double sn) { return cd{c * c - sn * sn, 2.0 * c * sn}; }
 __device__ __forceinline__ cd expi_small(double x) {
   double y = 0.5 * x, y2 = y * y;
-  double c = 1.0 - y2 * (1.0 / 182.0);   // 1/(13 * 14)
-  c = 1.0 - y2 * (1.0 / 132.0) * c;      // 1/(11 * 12)
-  c = 1.0 - y2 * (1.0 / 90.0) * c;
-  c = 1.0 - y2 * (1.0 / 56.0) * c;
-  c = 1.0 - y2 * (1.0 / 30.0) * c;
-  c = 1.0 - y2 * (1.0 / 12.0) * c;
-  c = 1.0 - y2 * 0.5 * c;
-  double sn = 1.0 - y2 * (1.0 / 210.0);  // 1/(14 * 15)
-  sn = 1.0 - y2 * (1.0 / 156.0) * sn;     // 1/(12 * 13)
-  sn = 1.0 - y2 * (1.0 / 110.0) * sn;
-  sn = 1.0 - y2 * (1.0 / 72.0) * sn;
-  sn = 1.0 - y2 * (1.0 / 42.0) * sn;
-  sn = 1.0 - y2 * (1.0 / 20.0) * sn;
-  sn = 1.0 - y2 * (1.0 / 6.0) * sn;
-  sn *= y;
-  return cd{c * c - sn * sn, 2.0 * c * sn};
+  double c = EXPI_C(7, 87178291200.0);           // 1/14!
+  c = fma(c, y2, EXPI_C(6, 479001600.0));        // 1/12!
+  c = fma(c, y2, EXPI_C(5, 3628800.0));
+  c = fma(c, y2, EXPI_C(4, 40320.0));
+  c = fma(c, y2, EXPI_C(3, 720.0));
+  c = fma(c, y2, EXPI_C(2, 24.0));
+  c = fma(c, y2, EXPI_C(1, 2.0));
+  c = fma(c, y2, 1.0);
+  double sn = EXPI_C(7, 1307674368000.0);        // 1/15!
+  sn = fma(sn, y2, EXPI_C(6, 6227020800.0));     // 1/13!
+  sn = fma(sn, y2, EXPI_C(5, 39916800.0));
+  sn = fma(sn, y2, EXPI_C(4, 362880.0));
+  sn = fma(sn, y2, EXPI_C(3, 5040.0));
+  sn = fma(sn, y2, EXPI_C(2, 120.0));
+  sn = fma(sn, y2, EXPI_C(1, 6.0));
+  sn = fma(sn, y2, 1.0) * y;
+  return expi_halfangle(c, sn);
+}
+__device__ __forceinline__ cd expi_small_short(double x) {
+  double y = 0.5 * x, y2 = y * y;
+  double c = EXPI_C(5, 3628800.0);               // 1/10!
+  c = fma(c, y2, EXPI_C(4, 40320.0));
+  c = fma(c, y2, EXPI_C(3, 720.0));
+  c = fma(c, y2, EXPI_C(2, 24.0));
+  c = fma(c, y2, EXPI_C(1, 2.0));
+  c = fma(c, y2, 1.0);
+  double sn = EXPI_C(5, 39916800.0);             // 1/11!
+  sn = fma(sn, y2, EXPI_C(4, 362880.0));
+  sn = fma(sn, y2, EXPI_C(3, 5040.0));
+  sn = fma(sn, y2, EXPI_C(2, 120.0));
+  sn = fma(sn, y2, EXPI_C(1, 6.0));
+  sn = fma(sn, y2, 1.0) * y;
+  return expi_halfangle(c, sn);
 }
 
 // e^x - 1 - x - x^2/2: GetExpRelTable(x,3,3), GMatrixElements.cc:59-93 -- the
@@ -304,7 +326,14 @@ __device__ void far_stage_tet_info(int t, const double (*P)[4][3], double (*o)[3
   ns[t] = n;
 }
 
-// one CTA per 32 x 32 tile of basis-function pairs (upper triangle of tiles)
+// one CTA per 32 x 32 tile of basis-function pairs (upper triangle of tiles).
+// MODE, the phase of exp(ikr) per point pair, fixed per launch so that one
+// code path is compiled into each instantiation: 2 = ec * (short series)
+// (|k| (rA + rB) <= 1/4 for every pair of the mesh), 1 = ec * (series)
+// (<= 1), 0 = sincos per point pair (complex k or coarse pairs), 3 = chosen
+// per tetrahedron pair (launches that read omega from device memory, whose
+// frequency the host does not know when it launches them).
+template <int MODE>
 __global__ void __launch_bounds__(FTHR, 2) k_far(DevGeom g, cd k, cd invk2, cd *M, size_t ld, const double *fq) {
   if (fq) {
     k = cd{fq[0], fq[1]};
@@ -334,25 +363,30 @@ __global__ void __launch_bounds__(FTHR, 2) k_far(DevGeom g, cd k, cd invk2, cd *
     cd m[8];
 #pragma unroll
     for (int q = 0; q < 8; q++) m[q] = cmk(0, 0);
-    // phase about the centroid distance rc (see above)
+    // phase about the centroid distance rc (see above); mode 2: |k|(rA+rB)
+    // <= 1/4 (every pair of a fine mesh at moderate frequency), mode 1:
+    // <= 1, mode 0: a sincos per point pair.  1/(4 pi) rides on ec.
     const double e0 = S.oA[iA][0] - S.oB[tB][0], e1 = S.oA[iA][1] - S.oB[tB][1], e2 = S.oA[iA][2] - S.oB[tB][2];
     const double rc = sqrt(e0 * e0 + e1 * e1 + e2 * e2);
-    const bool series = k.i == 0.0 && fabs(k.r) * (S.rA[iA] + S.rB[tB]) <= 1.0;
-    const cd ec = series ? expikr(k, rc) : cmk(1.0, 0.0);
+    const double span = fabs(k.r) * (S.rA[iA] + S.rB[tB]);
+    const int mode = MODE != 3 ? MODE : (k.i != 0.0 ? 0 : (span <= 0.25 ? 2 : (span <= 1.0 ? 1 : 0)));
+    const cd ec = mode ? cscale(expikr(k, rc), inv4pi) : cmk(inv4pi, 0.0);
 #pragma unroll
     for (int i = 0; i < 4; i++) {
-      double x0 = S.pA[iA][i][0], x1 = S.pA[iA][i][1], x2 = S.pA[iA][i][2];
-      double xt0 = x0 - S.oA[iA][0], xt1 = x1 - S.oA[iA][1], xt2 = x2 - S.oA[iA][2];
+      const double xt0 = S.pA[iA][i][0] - S.oA[iA][0], xt1 = S.pA[iA][i][1] - S.oA[iA][1],
+                   xt2 = S.pA[iA][i][2] - S.oA[iA][2];
       cd phiI = cmk(0, 0);
 #pragma unroll
       for (int j = 0; j < 4; j++) {
-        double y0 = S.pB[tB][j][0], y1 = S.pB[tB][j][1], y2 = S.pB[tB][j][2];
-        double R0 = x0 - y0, R1 = x1 - y1, R2 = x2 - y2;
+        const double y0 = S.pB[tB][j][0], y1 = S.pB[tB][j][1], y2 = S.pB[tB][j][2];
+        double R0 = S.pA[iA][i][0] - y0, R1 = S.pA[iA][i][1] - y1, R2 = S.pA[iA][i][2] - y2;
         double r2 = R0 * R0 + R1 * R1 + R2 * R2;
         if (r2 < 1.0e-24) continue;           // r < 1e-12
         double ir = rsqrt(r2), r = r2 * ir;   // one reciprocal square root instead of sqrt and a division
-        cd phi = cscale(series ? cmul(ec, expi_small(k.r * (r - rc))) : expikr(k, r), inv4pi * ir);
-        double yt0 = y0 - S.oB[tB][0], yt1 = y1 - S.oB[tB][1], yt2 = y2 - S.oB[tB][2];
+        cd ph = mode == 2 ? cmul(ec, expi_small_short(k.r * (r - rc)))
+                          : (mode == 1 ? cmul(ec, expi_small(k.r * (r - rc))) : cscale(expikr(k, r), inv4pi));
+        cd phi = cscale(ph, ir);
+        const double yt0 = y0 - S.oB[tB][0], yt1 = y1 - S.oB[tB][1], yt2 = y2 - S.oB[tB][2];
         phiI = cadd(phiI, phi);
         m[4] = cadd(m[4], cscale(phi, yt0));
         m[5] = cadd(m[5], cscale(phi, yt1));
@@ -419,10 +453,23 @@ int assemble_far(bg_geometry *g, double wr, double wi, void *M, size_t ld, const
   dim3 grid(nb, nb);
   static bool attr = false;
   if (!attr) {
-    BG_CUDA_TRY(cudaFuncSetAttribute(k_far, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(FarSmem)));
+    const int sm = (int)sizeof(FarSmem);
+    BG_CUDA_TRY(cudaFuncSetAttribute(k_far<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    BG_CUDA_TRY(cudaFuncSetAttribute(k_far<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    BG_CUDA_TRY(cudaFuncSetAttribute(k_far<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    BG_CUDA_TRY(cudaFuncSetAttribute(k_far<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
     attr = true;
   }
-  k_far<<<grid, FTHR, sizeof(FarSmem), stream()>>>(g->dev, k, invk2, (cd *)M, ld, fq);
+  // the largest phase span |k| (rA + rB) of any tetrahedron pair of the mesh
+  const double span = std::fabs(wr) * 2.0 * g->rule_rmax;
+  const int mode = fq ? 3 : (wi != 0.0 ? 0 : (span <= 0.25 ? 2 : (span <= 1.0 ? 1 : 0)));
+  const size_t sm = sizeof(FarSmem);
+  switch (mode) {
+    case 0: k_far<0><<<grid, FTHR, sm, stream()>>>(g->dev, k, invk2, (cd *)M, ld, fq); break;
+    case 1: k_far<1><<<grid, FTHR, sm, stream()>>>(g->dev, k, invk2, (cd *)M, ld, fq); break;
+    case 2: k_far<2><<<grid, FTHR, sm, stream()>>>(g->dev, k, invk2, (cd *)M, ld, fq); break;
+    default: k_far<3><<<grid, FTHR, sm, stream()>>>(g->dev, k, invk2, (cd *)M, ld, fq); break;
+  }
   BG_LAUNCHED();
   return BG_OK;
 }

@@ -798,10 +798,13 @@ static int getrs(bg_matrix *m, C *B, size_t ldb, int nrhs) {
     BG_LAUNCHED();
     int epoch = ++m->solve_epoch;
     BG_CUDA_TRY(cudaMemsetAsync(tick, 0, 2 * sizeof(int), stream()));
+    prof_start(PROF_TRSV);
     k_trsv<C, false><<<nb, 128, smem, stream()>>>(N, A, m->ld, T, N, nr, flagsL, epoch, tick, err);
     BG_LAUNCHED();
     k_trsv<C, true><<<nb, 128, smem, stream()>>>(N, A, m->ld, T, N, nr, flagsU, epoch, tick + 1, err);
     BG_LAUNCHED();
+    // bytes of the two triangles read once
+    prof_stop(PROF_TRSV, (double)sizeof(C) * (double)N * N);
     BG_CUDA_TRY(cudaMemcpy2DAsync(Bp, sizeof(C) * ldb, T, sizeof(C) * N, sizeof(C) * N, nr, cudaMemcpyDeviceToDevice,
                                   stream()));
     BG_CUDA_TRY(cudaFreeAsync(T, stream()));

@@ -192,10 +192,12 @@ int solve_refined(bg_matrix *A, bg_matrix *F, void *dB, int ldb, int nrhs, doubl
     if ((st = lu_solve(F, R32, N, nrhs))) break;
     k_axpy_c64<<<(N * nrhs + 255) / 256, 256, 0, stream()>>>(N * nrhs, R32, X);
     g_launches++;
+    prof_start(PROF_RESID);
     k_matvec_part<<<dim3(nrb, nchunk), MV_ROWS, 0, stream()>>>(N, (const c2 *)A->d, A->ld, X, N, nrhs, part);
     g_launches++;
     k_matvec_reduce<<<nb256, 256, 0, stream()>>>(N, nchunk, nrhs, part, B0, N, R, N, sq);
     g_launches++;
+    prof_stop(PROF_RESID, 16.0 * (double)N * N);
     if ((e = cudaGetLastError()) != cudaSuccess) { st = fail(e); break; }
     if ((st = sum_blocks(sq, nb256, nrhs, rn))) break;
     last = 0;

@@ -305,10 +305,11 @@ int bg_precond_nnz(const bg_precond *P);
 /* Restarted GMRES(restart) in FP64 on the device with right preconditioner P
    (NULL: none) for A X = B; up to 4 right-hand sides advance in lockstep so
    each step reads A once.  Stops when max_j |b_j - A x_j| / |b_j| <= tol or
-   after maxit matrix-vector steps.  A cycle that fails to halve the true
-   residual doubles the next cycle's length (up to 4 x restart, at most 200;
-   a converging GMRES(restart) is unchanged), and the solve returns early,
-   unconverged, once the last cycle's rate could not reach tol within the
+   after maxit matrix-vector steps.  A cycle that reduces the true residual
+   by less than a factor 10 doubles the next cycle's length (up to
+   4 x restart, at most 200; a GMRES(restart) that gains a digit per cycle is
+   unchanged), and, once at that length, the solve returns early,
+   unconverged, when the last cycle's rate could not reach tol within the
    remaining steps even if it doubled.  stats (3 doubles, may be NULL):
    steps, final and initial relative residual.  B: host N x nrhs complex128. */
 int bg_gmres_solve(bg_matrix *A, const bg_precond *P, double *B_host, int nrhs, double tol, int restart, int maxit,
@@ -321,10 +322,10 @@ int bg_gmres_solve_device(bg_matrix *A, const bg_precond *P, void *B_dev, int ld
    FP64 iterative refinement with the complex128 A between them, until
    max_j |b_j - A x_j| / |b_j| <= tol or maxit Krylov steps in total.
    stats (3 doubles, may be NULL): Krylov steps, final relative residual,
-   refinement sweeps.  P as for bg_gmres_solve (built from A); when the first
-   cycle with a given P fails to halve the residual, the solve continues
-   with the diagonal (Jacobi) preconditioner of A (bg_gmres_last_info
-   reports it). */
+   refinement sweeps.  P as for bg_gmres_solve (built from A); when a cycle
+   of the longest length with a given P still gains less than a factor 10,
+   the solve continues with the diagonal (Jacobi) preconditioner of A
+   (bg_gmres_last_info reports it). */
 int bg_gmres_solve_mixed(bg_matrix *A, bg_matrix *F, const bg_precond *P, double *B_host, int nrhs, double tol,
                          int restart, int maxit, double inner_tol, double *stats);
 int bg_gmres_solve_mixed_device(bg_matrix *A, bg_matrix *F, const bg_precond *P, void *B_dev, int ldb, int nrhs,
@@ -514,7 +515,9 @@ void *bg_stream(void);
    (point-pair kernel evaluations, 64 per basis-function pair), 5 near-field
    and Gram assembly, 6 GMRES dense matrix-vector products (matrix bytes
    read), 7 learned-preconditioner inference, 8 GMRES Gram-Schmidt steps
-   (including their host reads), 9 preconditioner applications. */
+   (including their host reads), 9 preconditioner applications, 10 the two
+   triangular sweeps of an LU solve (factor bytes read), 11 the complex128
+   residual products of iterative refinement (matrix bytes read). */
 int bg_profile_begin(void);
 int bg_profile_read(int n, long long *counts, double *ms, double *flops);
 int bg_profile_end(void);
