@@ -72,9 +72,9 @@ EPS_LEARNED = 6 + 0.5j
 WAVES = [([1, 0, 0], [0, 0, 1]), ([0, 1, 0], [0, 0, 1]), ([0, 0, 1], [1, 0, 0])]
 OMEGA = 1.0
 GMRES = dict(tol=1e-10, restart=50, maxit=1000, inner_tol=1e-5)
-# ncu --set full capture of k_gm_matvec_sym_c64 (one launch, N = 19,872):
-# dram__bytes_read.sum + dram__bytes_write.sum
-MATVEC_NCU_N, MATVEC_NCU_BYTES = 19872, 1.604407e9 + 38.544896e6
+# ncu --set full capture of k_gm_matvec_sym_c64 (one launch, N = 5,760,
+# profiles/gmres_matvec_c64_n5760.md): dram__bytes_read.sum + dram__bytes_write.sum
+MATVEC_NCU_N, MATVEC_NCU_BYTES = 5760, 138.911232e6 + 5.009664e6
 
 
 def eps_tensor():
@@ -204,29 +204,31 @@ def gemm_kernel_bench(n, reps=5):
             "cublas_zgemm_tflops": cub, "frac_of_cublas": ours / cub}
 
 
-def cgemm_kernel_bench(n, reps=5):
+def cgemm_kernel_bench(n, reps=5, shape=None):
     """Library complex64 GEMM (C -= A B on the tcgen05 TF32 tensor cores) on
-    one n^3 problem, CUDA events on the library stream, best of reps."""
+    one n^3 (or M x N x K) problem, CUDA events on the library stream, best
+    of reps."""
     import torch
     import buffem
     L = buffem.lib()
     stream = torch.cuda.ExternalStream(L.bg_stream())
+    M, Nc, K = shape if shape else (n, n, n)
     g = torch.Generator(device="cuda").manual_seed(0)
-    A = torch.randn(n, n, dtype=torch.complex64, device="cuda", generator=g)
-    B = torch.randn(n, n, dtype=torch.complex64, device="cuda", generator=g)
-    C = torch.zeros(n, n, dtype=torch.complex64, device="cuda")
+    A = torch.randn(K, M, dtype=torch.complex64, device="cuda", generator=g)      # column-major M x K
+    B = torch.randn(Nc, K, dtype=torch.complex64, device="cuda", generator=g)     # column-major K x N
+    C = torch.zeros(Nc, M, dtype=torch.complex64, device="cuda")
     best = 1e30
     for i in range(reps + 1):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        buffem.cgemm_sub_device(n, n, n, A.data_ptr(), n, B.data_ptr(), n, C.data_ptr(), n)
+        buffem.cgemm_sub_device(M, Nc, K, A.data_ptr(), M, B.data_ptr(), K, C.data_ptr(), M)
         e1.record(stream)
         buffem.synchronize()
         if i:
             best = min(best, e0.elapsed_time(e1) / 1e3)
-    tf = 8.0 * n ** 3 / best / 1e12
+    tf = 8.0 * M * Nc * K / best / 1e12
     mp = measured_peaks().get("bf16_tflops")
-    return {"kernel": "k_cgemm_tf32 (+ k_expand_a)", "shape": [n, n, n], "tflops": tf, "ms": best * 1e3,
+    return {"kernel": "k_cgemm_tf32 (+ k_expand_a)", "shape": [M, Nc, K], "tflops": tf, "ms": best * 1e3,
             "tf32_peak_tflops": mp / 2 if mp else None, "peak_source": "half the measured dense BF16 burst rate",
             "frac_of_tf32_peak": tf / (mp / 2) if mp else None}
 
@@ -878,6 +880,7 @@ def main():
                          "problem; fields = two GetFields calls, 2048 far points on the --size-cell sphere; "
                          "neq = two buff-neq flux frequencies on the --size-cell sphere")
     ap.add_argument("--size", type=int, default=8192)
+    ap.add_argument("--shape", default=None, help="M,N,K for --kernel cgemm (default: --size cubed)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "b200" else args.warmup
 
@@ -885,7 +888,8 @@ def main():
         print(json.dumps(gemm_kernel_bench(args.size)), flush=True)
         return
     if args.kernel == "cgemm":
-        print(json.dumps(cgemm_kernel_bench(args.size)), flush=True)
+        shape = tuple(int(v) for v in args.shape.split(",")) if args.shape else None
+        print(json.dumps(cgemm_kernel_bench(args.size, shape=shape)), flush=True)
         return
     if args.kernel in ("fields", "neq"):
         print(json.dumps(small_case(args.kernel, args.size)), flush=True)

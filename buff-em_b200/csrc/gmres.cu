@@ -643,18 +643,20 @@ static int colnorms(const z2 *X, GmState &S, std::vector<double> &out) {
 }
 
 // Restart policy.  A cycle has the requested length (restart); after a cycle
-// that reduces the true residual by less than a factor 10 the next one is
-// twice as long, up to GM_MAXGROW times the request and at most GM_MAXM
-// steps (restarted GMRES stagnates on indefinite problems -- the VIE system
-// at high frequency -- where a longer cycle still converges; a cycle that
-// gains a digit or more never grows).  With an alternative preconditioner
-// Palt, a cycle of full length that still gains less than a digit switches
-// to Palt for the rest of the solve (right preconditioning: every restart
-// solves for a correction, so the switch needs nothing else).  Once at full
-// length with nothing left to switch to, the solve stops early,
+// that gains fewer than GM_SLOW digits of the true residual per step the
+// next one is twice as long, up to GM_MAXGROW times the request and at most
+// GM_MAXM steps (restarted GMRES stagnates on indefinite problems -- the VIE
+// system at high frequency -- where a longer cycle still converges; the
+// learned or Jacobi-preconditioned VIE solves at moderate frequency gain
+// 0.05-0.08 digits per step and never grow).  With an alternative
+// preconditioner Palt, a cycle of full length that gains less than one digit
+// switches to Palt for the rest of the solve (right preconditioning: every
+// restart solves for a correction, so the switch needs nothing else).  Once
+// at full length with nothing left to switch to, the solve stops early,
 // unconverged, when the last cycle's rate could not reach tol within the
 // remaining steps even at twice that rate, so that a caller with a direct
 // fallback does not spend the whole budget first.
+#define GM_SLOW 0.025
 #define GM_MAXM 200
 #define GM_MAXGROW 4
 
@@ -729,14 +731,13 @@ int gmres_solve(bg_matrix *A, const bg_precond *P, void *dB, int ldb, int nrhs, 
       const double red = relres / prev;   // reduction over the last cycle
       const bool full = prev_len >= m;    // the last cycle had the longest length
       bool just_switched = false;
-      if (red > 0.1) {
-        if (!full) {
-          mc = std::min(2 * mc, m);
-        } else if (Palt && !switched) {
-          P = Palt;              // the given preconditioner stagnates at full length: switch
-          switched = 1;
-          just_switched = true;
-        }
+      const double digits_per_step = -std::log10(std::max(red, 1e-300)) / prev_len;
+      if (!full && digits_per_step < GM_SLOW) {
+        mc = std::min(2 * mc, m);
+      } else if (full && red > 0.1 && Palt && !switched) {
+        P = Palt;              // the given preconditioner stagnates at full length: switch
+        switched = 1;
+        just_switched = true;
       }
       // early stop, at full length with nothing left to switch to (the rate
       // of a cycle run with the replaced preconditioner does not count): at

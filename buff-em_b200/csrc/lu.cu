@@ -665,6 +665,11 @@ __device__ __forceinline__ cfl ldcg_c<cfl>(const cfl *p) {
   return cfl{v.x, v.y};
 }
 
+template <class C>
+constexpr int trsv_smem() {
+  return TV_B * (TV_B + 1) * (int)sizeof(C) + 2 * TV_B * TV_MAXRHS * (int)sizeof(C);
+}
+
 template <class C, bool UPPER>
 __global__ void __launch_bounds__(128) k_trsv(int N, const C *A, size_t ld, C *X, size_t ldx, int nrhs, int *flags,
                                               int epoch, int *ticket, int *err) {
@@ -672,6 +677,7 @@ __global__ void __launch_bounds__(128) k_trsv(int N, const C *A, size_t ld, C *X
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C(*D)[TV_B + 1] = (C(*)[TV_B + 1])smem_raw;                    // diagonal block
   C(*part)[TV_MAXRHS] = (C(*)[TV_MAXRHS])(smem_raw + TV_B * (TV_B + 1) * sizeof(C));   // part[row][rhs]
+  C(*xs)[TV_MAXRHS] = part + TV_B;                                                    // solved block x[col][rhs]
   __shared__ int s_blk, s_abort;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nb = (N + TV_B - 1) / TV_B;
@@ -707,27 +713,50 @@ __global__ void __launch_bounds__(128) k_trsv(int N, const C *A, size_t ld, C *X
     __syncthreads();
     if (s_abort) return;
     const int c0 = bj * TV_B, cols = min(TV_B, N - c0);
+    // the solved block's x, once per CTA
+    for (int e = tid; e < cols * nrhs; e += 128) {
+      const int c = e % cols, j = e / cols;
+      xs[c][j] = ldcg_c(X + (size_t)j * ldx + c0 + c);
+    }
+    __syncthreads();
     if (row < rows) {
+      // this thread's row against half of the block's columns, eight
+      // independent loads of A in flight at a time
       const C *ap = A + (size_t)c0 * ld + r0 + row;
-      for (int c = half * 32; c < min(cols, half * 32 + 32); c++) {
-        C a = ap[(size_t)c * ld];
-        for (int j = 0; j < nrhs; j++) {
-          C x = ldcg_c(X + (size_t)j * ldx + c0 + c);
-          acc[j].r += a.r * x.r - a.i * x.i;
-          acc[j].i += a.r * x.i + a.i * x.r;
+      const int ce = min(cols, half * 32 + 32);
+      for (int c8 = half * 32; c8 < ce; c8 += 8) {
+        C a[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) a[u] = c8 + u < ce ? ap[(size_t)(c8 + u) * ld] : C{0, 0};
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          if (c8 + u >= ce) break;
+#pragma unroll
+          for (int j = 0; j < TV_MAXRHS; j++) {
+            if (j < nrhs) {
+              const C x = xs[c8 + u][j];
+              acc[j].r += a[u].r * x.r - a[u].i * x.i;
+              acc[j].i += a[u].r * x.i + a[u].i * x.r;
+            }
+          }
         }
       }
     }
+    __syncthreads();   // xs is rewritten for the next block
   }
   if (half == 1 && row < rows)
-    for (int j = 0; j < nrhs; j++) part[row][j] = acc[j];
+#pragma unroll
+    for (int j = 0; j < TV_MAXRHS; j++)
+      if (j < nrhs) part[row][j] = acc[j];
   __syncthreads();
   if (half == 0 && row < rows)
-    for (int j = 0; j < nrhs; j++) {
-      C b = X[(size_t)j * ldx + r0 + row];
-      C p = part[row][j];
-      part[row][j] = C{b.r - acc[j].r - p.r, b.i - acc[j].i - p.i};
-    }
+#pragma unroll
+    for (int j = 0; j < TV_MAXRHS; j++)
+      if (j < nrhs) {
+        C b = X[(size_t)j * ldx + r0 + row];
+        C p = part[row][j];
+        part[row][j] = C{b.r - acc[j].r - p.r, b.i - acc[j].i - p.i};
+      }
   __syncthreads();
   // diagonal solve: warp j handles right-hand side j, lanes hold rows l, l+32
   if (warp < nrhs) {
@@ -782,7 +811,7 @@ static int getrs(bg_matrix *m, C *B, size_t ldb, int nrhs) {
   const C *A = (const C *)m->d;
   const int nb = (N + TV_B - 1) / TV_B;
   int *flagsL = m->d_perm + N, *flagsU = flagsL + nb, *tick = flagsU + nb, *err = tick + 2;
-  const int smem = TV_B * (TV_B + 1) * (int)sizeof(C) + TV_B * TV_MAXRHS * (int)sizeof(C);
+  const int smem = trsv_smem<C>();
   static bool attr = false;
   if (!attr) {
     BG_CUDA_TRY(cudaFuncSetAttribute(k_trsv<C, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
@@ -907,7 +936,7 @@ static int getrs_noalloc(bg_matrix *m, C *B, size_t ldb, int nrhs, void *scratch
   const C *A = (const C *)m->d;
   const int nb = (N + TV_B - 1) / TV_B;
   int *flagsL = m->d_perm + N, *flagsU = flagsL + nb, *tick = flagsU + nb, *err = tick + 2;
-  const int smem = TV_B * (TV_B + 1) * (int)sizeof(C) + TV_B * TV_MAXRHS * (int)sizeof(C);
+  const int smem = trsv_smem<C>();
   BG_CUDA_TRY(cudaFuncSetAttribute(k_trsv<C, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   BG_CUDA_TRY(cudaFuncSetAttribute(k_trsv<C, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   C *T = (C *)scratch;
@@ -1058,7 +1087,7 @@ int lu_solve_enqueue(bg_matrix *m, void *dB, int ldb, int nrhs, void *dT) {
   cdl *B = (cdl *)dB, *T = (cdl *)dT;
   const int nb = (N + TV_B - 1) / TV_B;
   int *flagsL = m->d_perm + N, *flagsU = flagsL + nb, *tick = flagsU + nb, *err = tick + 2;
-  const int smem = TV_B * (TV_B + 1) * (int)sizeof(cdl) + TV_B * TV_MAXRHS * (int)sizeof(cdl);
+  const int smem = trsv_smem<cdl>();
   static bool attr = false;
   if (!attr) {
     BG_CUDA_TRY(cudaFuncSetAttribute(k_trsv<cdl, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));

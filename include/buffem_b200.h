@@ -305,10 +305,10 @@ int bg_precond_nnz(const bg_precond *P);
 /* Restarted GMRES(restart) in FP64 on the device with right preconditioner P
    (NULL: none) for A X = B; up to 4 right-hand sides advance in lockstep so
    each step reads A once.  Stops when max_j |b_j - A x_j| / |b_j| <= tol or
-   after maxit matrix-vector steps.  A cycle that reduces the true residual
-   by less than a factor 10 doubles the next cycle's length (up to
-   4 x restart, at most 200; a GMRES(restart) that gains a digit per cycle is
-   unchanged), and, once at that length, the solve returns early,
+   after maxit matrix-vector steps.  A cycle that gains fewer than 0.025
+   digits of the true residual per step doubles the next cycle's length (up
+   to 4 x restart, at most 200; a GMRES(restart) converging faster than that
+   is unchanged), and, once at that length, the solve returns early,
    unconverged, when the last cycle's rate could not reach tol within the
    remaining steps even if it doubled.  stats (3 doubles, may be NULL):
    steps, final and initial relative residual.  B: host N x nrhs complex128. */
