@@ -138,7 +138,8 @@ static int create_objects(int nobj, const char *const *meshfiles, const double *
   g->objs.resize(nobj);
   for (int i = 0; i < nobj; i++) {
     if (!meshfiles[i]) { delete g; set_error("mesh file %d is NULL", i); return BG_ERR_ARG; }
-    int st = check_material(materials[i]);
+    // BG_MAT_EXPR comes only with a position-dependent SVTENSOR file
+    int st = (svts && svts[i] && materials[i].kind == BG_MAT_EXPR) ? BG_OK : check_material(materials[i]);
     if (!st) st = load_object(g->objs[i], meshfiles[i], xf ? xf + 12 * i : nullptr);
     if (st) { delete g; return st; }
     g->objs[i].mat = materials[i];
@@ -245,7 +246,7 @@ void bg_geometry_destroy(bg_geometry *g) {
   if (!g) return;
   DevGeom &d = g->dev;
   dfree(d.V4); dfree(d.tetVI); dfree(d.tetVol); dfree(d.tetP4); dfree(d.tetObj); dfree(d.bfTet);
-  dfree(d.bfQ); dfree(d.bfLoc); dfree(d.tetFI); dfree(d.bfV); dfree(d.bfArea); dfree(d.bfRadius); dfree(d.mats); dfree(d.objOrigin);
+  dfree(d.bfQ); dfree(d.bfLoc); dfree(d.tetFI); dfree(d.bfV); dfree(d.bfArea); dfree(d.bfRadius); dfree(d.mats); dfree(d.expr); dfree(d.objOrigin);
   dfree(d.tileTet); dfree(d.tileNT); dfree(d.bfTileLoc);
   NearData &n = g->near;
   dfree(n.pairs); dfree(n.pairTP); dfree(n.fibbi); dfree(n.tp); dfree(n.tpOrdA); dfree(n.tpOrdB); dfree(n.tpMom); dfree(n.tpFlag);
@@ -272,7 +273,9 @@ int bg_geometry_material_eps(const bg_geometry *g, int obj, double omega_re, dou
   if (o.matprop) { matprop_eps(*o.matprop, omega_re, omega_im, eps); return 1; }
   if (o.svt) {
     // the scalar SVTensor::Evaluate(Omega, x) returns the xx component
-    // (SVTensor.cc:375-380); SVTENSOR objects here depend on frequency only
+    // (SVTensor.cc:375-380); this query has no point, so a position-dependent
+    // tensor is taken at the origin of coordinates (bg_geometry_material_tensor
+    // takes one)
     double Q[18];
     const double x0[3] = {0.0, 0.0, 0.0};
     svtensor_eval(*o.svt, omega_re, omega_im, x0, Q);

@@ -8,8 +8,8 @@
 // complex update.  So B and C are used in place; only A is expanded once
 // into a K-major (row-major 2M x 2K) copy by k_expand_a.
 //
-// Kernel: persistent, one CTA per SM, tiles of 128 rows x BN (128 or 256)
-// columns of C~, taken in a grouped raster (TC_GROUP row blocks at a time,
+// Kernel: persistent, one CTA per SM, tiles of 128 rows x BN (64, 128 or
+// 256: the widest that gives every SM a tile) columns of C~, taken in a grouped raster (TC_GROUP row blocks at a time,
 // all column blocks of the group, rows fastest) so that the tiles running at
 // once share their A rows and B columns in L2.  Warp roles:
 //   warp 0, one lane: TMA producer -- 128B-swizzled boxes of 32 fp32 of K
@@ -353,14 +353,24 @@ int cgemm_sub_tf32(int M, int N, int K, const void *A, size_t lda, const void *B
   dim3 eg((M + 31) / 32, (K + 31) / 32);
   k_expand_a<<<eg, 256, 0, stream()>>>(M, K, (const float2 *)A, lda, At, lda2);
   BG_LAUNCHED();
-  const int BN = N > 128 ? 256 : 128;
+  // widest tile that still gives every SM a tile (skinny updates of the
+  // triangular solves have one row block and few column blocks)
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    BG_CUDA_TRY(cudaGetDevice(&dev));
+    BG_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  }
+  const long ntm = (2L * M + TC_BM - 1) / TC_BM;
+  int BN = N > 128 ? 256 : (N > 64 ? 128 : 64);
+  while (BN > 64 && ntm * ((N + BN - 1) / BN) < sms) BN /= 2;
   CUtensorMap mA, mB;
   int st = make_map(&mA, At, (uint64_t)2 * K, (uint64_t)2 * M, lda2, TC_BM);
   if (!st) st = make_map(&mB, (const float *)B, (uint64_t)2 * K, (uint64_t)N, 2 * ldb, BN);
   if (st) return st;
   TcArgs P{2 * M, N, 2 * K, (float *)C, ldc, err, 0, 0};
   prof_start(PROF_GEMM);
-  st = BN == 256 ? launch_tf32<256>(mA, mB, P) : launch_tf32<128>(mA, mB, P);
+  st = BN == 256 ? launch_tf32<256>(mA, mB, P) : (BN == 128 ? launch_tf32<128>(mA, mB, P) : launch_tf32<64>(mA, mB, P));
   prof_stop(PROF_GEMM, 8.0 * M * (double)N * K);
   return st;
 }

@@ -202,6 +202,16 @@ int refresh_materials(bg_geometry *g, double wr, double wi) {
       o.mat = bg_material{};
       o.mat.kind = BG_MAT_CONST_ISO;
       matprop_eps(*o.matprop, wr, wi, o.mat.eps);
+    } else if (o.svt && svtensor_position_dependent(*o.svt)) {
+      // the program at this Omega: w, the constants and Eps1-3 folded in
+      o.mat = bg_material{};
+      o.mat.kind = BG_MAT_EXPR;
+      if (!g->dev.expr) { set_error("compiled SVTENSOR programs are not on the device"); return BG_ERR_STATE; }
+      DevExpr prog{};
+      int st = svtensor_compile(*o.svt, wr, wi, &prog);
+      if (st) return st;
+      // synchronous from pageable memory: prog may leave scope at once
+      BG_CUDA_TRY(cudaMemcpy(g->dev.expr + i, &prog, sizeof(DevExpr), cudaMemcpyHostToDevice));
     } else if (o.svt) {
       const double x0[3] = {0.0, 0.0, 0.0};   // position-independent by construction
       o.mat = bg_material{};
@@ -310,6 +320,12 @@ int upload_geometry(bg_geometry *g) {
       (st = dupload(&d.bfQ, bfQ)) || (st = dupload(&d.bfLoc, bfLoc)) || (st = dupload(&d.tetFI, tetFI)) || (st = dupload(&d.bfV, bfV)) || (st = dupload(&d.bfArea, area)) ||
       (st = dupload(&d.bfRadius, radius)) || (st = dupload(&d.mats, mats)) || (st = dupload(&d.objOrigin, origin)))
     return st;
+  bool any_expr = false;
+  for (const Object &o : g->objs) any_expr = any_expr || o.mat.kind == BG_MAT_EXPR;
+  if (any_expr) {
+    BG_CUDA_TRY(cudaMalloc((void **)&d.expr, sizeof(DevExpr) * g->objs.size()));
+    BG_CUDA_TRY(cudaMemset(d.expr, 0, sizeof(DevExpr) * g->objs.size()));
+  }
   g->uploaded = true;
   return BG_OK;
 }
@@ -599,8 +615,8 @@ static std::string find_mesh(const std::string &fn, const std::string &dir, cons
 
 // MATERIAL argument: CONST_EPS_<complex> or VACUUM; other names refer to
 // MATERIAL ... ENDMATERIAL sections of the file (matprop.cpp).  SVTENSOR files
-// (eps as expressions of position) are rejected; spatially varying
-// permittivities come through bg_geometry_create_objects instead.
+// may depend on frequency and on position: position-dependent ones are
+// compiled at each frequency into device programs (BG_MAT_EXPR).
 static bool parse_material(const std::string &M, bg_material &m) {
   std::string U = M;
   for (auto &c : U) c = (char)std::toupper((unsigned char)c);
@@ -628,18 +644,18 @@ static int parse_object_lines(const std::vector<std::vector<std::string>> &lines
         std::shared_ptr<const SVTensorFn> t;
         std::string file = find_file(tok[1], dir, "BUFF_SVTENSOR_PATH", {});
         if (svtensor_parse_file(file, db, t)) return BG_ERR_IO;
+        o.svt = t;
+        o.matprop.reset();
+        o.mat = bg_material{};
         if (svtensor_position_dependent(*t)) {
-          err = "SVTENSOR " + tok[1] + ": expressions of position (x, y, z, r, Theta, Phi) are not supported "
-                "(frequency-dependent tensors are)";
+          // evaluated on the device from a program compiled at each Omega
+          o.mat.kind = BG_MAT_EXPR;
         } else {
-          o.svt = t;
-          o.matprop.reset();
-          o.mat = bg_material{};
           o.mat.kind = BG_MAT_CONST_TENSOR;
           const double x0[3] = {0.0, 0.0, 0.0};
           svtensor_eval(*t, 1.0, 0.0, x0, o.mat.eps);   // replaced by the tensor at Omega before every use
-          have_mat = true;
         }
+        have_mat = true;
       }
       else if (parse_material(tok[1], o.mat)) { o.matprop.reset(); o.svt.reset(); have_mat = true; }
       else if (keyword_is(tok[1].substr(0, std::min<size_t>(10, tok[1].size())), "CONST_EPS_"))

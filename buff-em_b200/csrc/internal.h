@@ -109,6 +109,10 @@ typedef std::vector<std::pair<std::string, std::shared_ptr<const MatPropFn>>> Ma
 // An SVTENSOR file (matprop.cpp).  Parsing adds its MATERIAL sections to db.
 int svtensor_parse_file(const std::string &path, MatDB &db, std::shared_ptr<const SVTensorFn> &out);
 bool svtensor_position_dependent(const SVTensorFn &t);
+// the device program of a position-dependent tensor at Omega (w, Eps1-3 and
+// the constants folded in); BG_ERR_ARG with a message if it is too long
+struct DevExpr;
+int svtensor_compile(const SVTensorFn &t, double omega_re, double omega_im, DevExpr *out);
 // the tensor at Omega and point x into Q (3x3 complex, row-major re/im)
 void svtensor_eval(const SVTensorFn &t, double omega_re, double omega_im, const double *x, double Q[18]);
 
@@ -134,6 +138,23 @@ int apply_trans(const TransEntry &e, std::vector<GeoObject> &objs);
 // All indices are global over the objects of a geometry (vertex and tet
 // indices carry per-object offsets), so basis functions of different objects
 // never share a vertex index, matching CompareBFs' OA != OB rule.
+// An SVTENSOR permittivity that depends on position, compiled per frequency
+// into postfix programs (one per tensor component, row-major) for the device
+// (matprop.cpp: svtensor_compile; kernels.cu: mat_eval).  op = code << 16 |
+// argument: 0 push constant con[arg], 1 push position variable arg (x, y, z,
+// r, Theta, Phi), 2 negate, 3 add, 4 subtract, 5 multiply, 6 divide, 7 power,
+// 8 function arg (exp log sqrt sin cos tan sinh cosh tanh asin acos atan abs
+// step).
+#define BG_MAT_EXPR 16           // internal material kind: eps from DevGeom::expr[object]
+#define BG_EXPR_MAXOPS 512
+#define BG_EXPR_MAXCON 128
+#define BG_EXPR_STACK 24
+struct DevExpr {
+  int start[9], len[9];          // component (row-major) program; len 0: not given
+  int op[BG_EXPR_MAXOPS];
+  double con[2 * BG_EXPR_MAXCON];
+};
+
 struct DevGeom {
   int N = 0, NT = 0, NV = 0;
   double *V4 = nullptr;      // 4 doubles per vertex (x, y, z, 0)
@@ -150,6 +171,7 @@ struct DevGeom {
   double *bfArea = nullptr;
   double *bfRadius = nullptr;
   bg_material *mats = nullptr;  // per object
+  DevExpr *expr = nullptr;      // per object (allocated when some object is BG_MAT_EXPR)
   double *objOrigin = nullptr;  // 3 per object
   // far-field tiles of BG_FAR_TILE consecutive basis functions: the distinct
   // tetrahedra of each tile (<= 2 per basis function) and, per basis

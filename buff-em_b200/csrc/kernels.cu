@@ -161,10 +161,145 @@ __device__ __forceinline__ cd exprel3(cd x) {
   return cadd(first, sum);
 }
 
-// permittivity functor (SVTensor::Evaluate semantics, SVTensor.cc:306-373)
-__device__ void mat_eval(const bg_material &m, const double *x, cd E[3][3]) {
+// complex functions of the SVTENSOR programs, from their definitions in
+// terms of the real exp, log, sincos, sinh, cosh, sqrt, hypot and atan2
+__device__ cd cx_exp(cd z) {
+  double s, c, e = exp(z.r);
+  sincos(z.i, &s, &c);
+  return cd{e * c, e * s};
+}
+__device__ cd cx_log(cd z) { return cd{log(hypot(z.r, z.i)), atan2(z.i, z.r)}; }
+__device__ cd cx_sqrt(cd z) {   // principal branch
+  double r = hypot(z.r, z.i);
+  if (r == 0.0) return cd{0.0, 0.0};
+  if (z.r >= 0.0) {
+    double t = sqrt(0.5 * (r + z.r));
+    return cd{t, z.i / (2.0 * t)};
+  }
+  double t = sqrt(0.5 * (r - z.r));
+  return cd{fabs(z.i) / (2.0 * t), copysign(t, z.i)};
+}
+__device__ cd cx_sin(cd z) {
+  double s, c;
+  sincos(z.r, &s, &c);
+  return cd{s * cosh(z.i), c * sinh(z.i)};
+}
+__device__ cd cx_cos(cd z) {
+  double s, c;
+  sincos(z.r, &s, &c);
+  return cd{c * cosh(z.i), -s * sinh(z.i)};
+}
+__device__ cd cx_sinh(cd z) {
+  double s, c;
+  sincos(z.i, &s, &c);
+  return cd{sinh(z.r) * c, cosh(z.r) * s};
+}
+__device__ cd cx_cosh(cd z) {
+  double s, c;
+  sincos(z.i, &s, &c);
+  return cd{cosh(z.r) * c, sinh(z.r) * s};
+}
+// asin z = -i log(iz + sqrt(1 - z^2)), acos z = pi/2 - asin z,
+// atan z = (i/2) [log(1 - iz) - log(1 + iz)]
+__device__ cd cx_asin(cd z) {
+  cd w = cx_log(cadd(cd{-z.i, z.r}, cx_sqrt(csub(cd{1.0, 0.0}, cmul(z, z)))));
+  return cd{w.i, -w.r};
+}
+__device__ cd cx_atan(cd z) {
+  cd a = cx_log(cd{1.0 + z.i, -z.r}), b = cx_log(cd{1.0 - z.i, z.r});
+  cd d = csub(a, b);
+  return cd{-0.5 * d.i, 0.5 * d.r};
+}
+__device__ cd cx_pow(cd x, cd y) {
+  // integer powers by repeated squaring, as the host evaluator (matprop.cpp)
+  if (y.i == 0.0 && y.r == floor(y.r) && fabs(y.r) <= 64.0) {
+    long n = (long)y.r;
+    bool inv = n < 0;
+    unsigned long m = inv ? (unsigned long)(-n) : (unsigned long)n;
+    cd r{1.0, 0.0};
+    while (m) {
+      if (m & 1) r = cmul(r, x);
+      x = cmul(x, x);
+      m >>= 1;
+    }
+    return inv ? cdiv(cd{1.0, 0.0}, r) : r;
+  }
+  return cx_exp(cmul(y, cx_log(x)));
+}
+
+// one component program of a compiled SVTENSOR (DevExpr) at point x
+__device__ cd expr_eval(const DevExpr &e, int comp, const double *x) {
+  cd st[BG_EXPR_STACK];
+  int sp = 0;
+  const int b = e.start[comp], n = e.len[comp];
+  for (int k = 0; k < n; k++) {
+    const int w = e.op[b + k], code = w >> 16, arg = w & 0xffff;
+    switch (code) {
+      case 0: st[sp++] = cd{e.con[2 * arg], e.con[2 * arg + 1]}; break;
+      case 1: {
+        double v;
+        if (arg < 3) v = x[arg];
+        else if (arg == 3) v = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+        else if (arg == 4) v = atan2(sqrt(x[0] * x[0] + x[1] * x[1]), x[2]);
+        else v = atan2(x[1], x[0]);
+        st[sp++] = cd{v, 0.0};
+        break;
+      }
+      case 2: st[sp - 1] = csub(cd{0.0, 0.0}, st[sp - 1]); break;
+      case 8: {
+        cd a = st[sp - 1], r;
+        switch (arg) {
+          case 0: r = cx_exp(a); break;
+          case 1: r = cx_log(a); break;
+          case 2: r = cx_sqrt(a); break;
+          case 3: r = cx_sin(a); break;
+          case 4: r = cx_cos(a); break;
+          case 5: r = cdiv(cx_sin(a), cx_cos(a)); break;
+          case 6: r = cx_sinh(a); break;
+          case 7: r = cx_cosh(a); break;
+          case 8: r = cdiv(cx_sinh(a), cx_cosh(a)); break;
+          case 9: r = cx_asin(a); break;
+          case 10: r = csub(cd{0.5 * M_PI, 0.0}, cx_asin(a)); break;
+          case 11: r = cx_atan(a); break;
+          case 12: r = cd{hypot(a.r, a.i), 0.0}; break;
+          default: r = cd{a.r < 0.0 ? 0.0 : 1.0, 0.0}; break;
+        }
+        st[sp - 1] = r;
+        break;
+      }
+      default: {
+        cd bb = st[--sp], aa = st[sp - 1];
+        st[sp - 1] = code == 3 ? cadd(aa, bb) : code == 4 ? csub(aa, bb) : code == 5 ? cmul(aa, bb)
+                   : code == 6 ? cdiv(aa, bb) : cx_pow(aa, bb);
+        break;
+      }
+    }
+  }
+  return st[0];
+}
+
+// permittivity functor (SVTensor::Evaluate semantics, SVTensor.cc:306-373);
+// ex: the object's compiled program when m.kind == BG_MAT_EXPR
+__device__ void mat_eval(const bg_material &m, const DevExpr *ex, const double *x, cd E[3][3]) {
   for (int i = 0; i < 3; i++)
     for (int j = 0; j < 3; j++) E[i][j] = cmk(0, 0);
+  if (m.kind == BG_MAT_EXPR) {
+    // components not given keep the identity, off-diagonal pairs are
+    // averaged, yy and zz follow xx when only xx is given (SVTensor.cc:344-372)
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++)
+        E[i][j] = ex->len[3 * i + j] ? expr_eval(*ex, 3 * i + j, x) : cmk(i == j ? 1.0 : 0.0, 0.0);
+    for (int mu = 0; mu < 3; mu++) {
+      int nu = (mu + 1) % 3;
+      cd a = cscale(cadd(E[mu][nu], E[nu][mu]), 0.5);
+      E[mu][nu] = E[nu][mu] = a;
+    }
+    if (ex->len[0]) {
+      if (!ex->len[4]) E[1][1] = E[0][0];
+      if (!ex->len[8]) E[2][2] = E[0][0];
+    }
+    return;
+  }
   if (m.kind == BG_MAT_CONST_TENSOR) {
     for (int i = 0; i < 3; i++)
       for (int j = 0; j < 3; j++) E[i][j] = cmk(m.eps[2 * (3 * i + j)], m.eps[2 * (3 * i + j) + 1]);
@@ -692,6 +827,7 @@ __global__ void k_gram(DevGeom g, double w, cd *M, size_t ld, const double *fq) 
     int t = side == 0 ? tt.x : tt.y;
     int obj = g.tetObj[t];
     const bg_material &mat = g.mats[obj];
+    const DevExpr *mex = g.expr ? g.expr + obj : nullptr;
     double vol = g.tetVol[t];
     double QA[3];
     load3(g.V4, side == 0 ? qq.x : qq.y, QA);
@@ -720,7 +856,7 @@ __global__ void k_gram(DevGeom g, double w, cd *M, size_t ld, const double *fq) 
         double wt = 6.0 * vol * u[3], x[3];
         for (int c = 0; c < 3; c++) x[c] = V0[c] + u[0] * L[0][c] + u[1] * L[1][c] + u[2] * L[2][c];
         cd E[3][3], Ei[3][3];
-        mat_eval(mat, x, E);
+        mat_eval(mat, mex, x, E);
         E[0][0].r -= 1.0; E[1][1].r -= 1.0; E[2][2].r -= 1.0;
         inv3(E, Ei);
         double FA[3], FB[3];
@@ -1142,6 +1278,7 @@ __global__ void k_opft(PftArgs P, cd omega, double *part, const double *fq) {
   if (a < g.N) {
     obj = g.bfV[a].w;
     const bg_material &mat = g.mats[obj];
+    const DevExpr *mex = g.expr ? g.expr + obj : nullptr;
     int2 tt = g.bfTet[a], loc = g.bfLoc[a];
     cd Ja = P.J[a];
     const double Z0 = 376.73031346177;
@@ -1179,7 +1316,7 @@ __global__ void k_opft(PftArgs P, cd omega, double *part, const double *fq) {
             bA[c] *= pa;
           }
           cd E[3][3], Ei[3][3];
-          mat_eval(mat, x, E);
+          mat_eval(mat, mex, x, E);
           E[0][0].r -= 1.0; E[1][1].r -= 1.0; E[2][2].r -= 1.0;
           inv3(E, Ei);
           cd vsum = cmk(0, 0);
@@ -1354,6 +1491,7 @@ __global__ void k_neq_overlaps(DevGeom g, double w, int *idx, double *S, cd *V, 
     int t = side == 0 ? tt.x : tt.y;
     double sa = side == 0 ? 1.0 : -1.0;
     const bg_material &mat = g.mats[g.tetObj[t]];
+    const DevExpr *mex = g.expr ? g.expr + g.tetObj[t] : nullptr;
     double vol = g.tetVol[t];
     double QA[3];
     load3(g.V4, side == 0 ? qq.x : qq.y, QA);
@@ -1393,7 +1531,7 @@ __global__ void k_neq_overlaps(DevGeom g, double w, int *idx, double *S, cd *V, 
         double wt = 6.0 * vol * u[3], x[3];
         for (int c = 0; c < 3; c++) x[c] = V0[c] + u[0] * L[0][c] + u[1] * L[1][c] + u[2] * L[2][c];
         cd E[3][3];
-        mat_eval(mat, x, E);
+        mat_eval(mat, mex, x, E);
         E[0][0].r -= 1.0; E[1][1].r -= 1.0; E[2][2].r -= 1.0;
         double FA[3], FB[3];
         for (int c = 0; c < 3; c++) { FA[c] = pa * (x[c] - QA[c]); FB[c] = pb * (x[c] - QB[c]); }

@@ -559,6 +559,78 @@ int svtensor_parse_file(const std::string &path, MatDB &db, std::shared_ptr<cons
 
 bool svtensor_position_dependent(const SVTensorFn &t) { return t.position; }
 
+// Postfix program of the subtree at id: w, the constants and Eps1-3 become
+// constants of the program (their values at this frequency), x, y, z, r,
+// Theta and Phi stay variables.
+namespace {
+struct ExprEmitter {
+  const SVTensorFn &t;
+  cplx w, eps[3];
+  DevExpr *out;
+  int nop = 0, ncon = 0, depth = 0, maxdepth = 0;
+  std::string err;
+  void op(int code, int arg) {
+    if (nop >= BG_EXPR_MAXOPS) { err = "too long"; return; }
+    out->op[nop++] = code << 16 | arg;
+  }
+  void con(cplx v) {
+    if (ncon >= BG_EXPR_MAXCON) { err = "too many constants"; return; }
+    out->con[2 * ncon] = v.real();
+    out->con[2 * ncon + 1] = v.imag();
+    op(0, ncon++);
+  }
+  void push() { maxdepth = std::max(maxdepth, ++depth); }
+  void emit(int id) {
+    if (!err.empty()) return;
+    const ExprNode &n = t.nodes[id];
+    switch (n.kind) {
+      case ExprNode::NUM: con(n.value); push(); return;
+      case ExprNode::VAR:
+        if (n.var == 0) con(w);
+        else if (n.var > 0) con(t.const_values[n.var - 1]);
+        else if (-n.var - 1 < 6) op(1, -n.var - 1);
+        else con(eps[-n.var - 1 - 6]);
+        push();
+        return;
+      case ExprNode::NEG: emit(n.a); op(2, 0); return;
+      case ExprNode::FUN: emit(n.a); op(8, n.fun); return;
+      default: break;
+    }
+    emit(n.a);
+    emit(n.b);
+    int code = n.kind == ExprNode::ADD ? 3 : n.kind == ExprNode::SUB ? 4 : n.kind == ExprNode::MUL ? 5
+             : n.kind == ExprNode::DIV ? 6 : 7;
+    op(code, 0);
+    depth--;
+  }
+};
+}  // namespace
+
+int svtensor_compile(const SVTensorFn &t, double wr, double wi, DevExpr *out) {
+  const double kFreqUnit = 3.0e14;
+  ExprEmitter E{t, cplx(wr * kFreqUnit, wi * kFreqUnit), {cplx(1.0, 0.0), cplx(1.0, 0.0), cplx(1.0, 0.0)}, out};
+  for (size_t k = 0; k < 3 && k < t.mps.size(); k++) {
+    double e[2];
+    matprop_eps(*t.mps[k], wr, wi, e);
+    E.eps[k] = cplx(e[0], e[1]);
+  }
+  for (int a = 0; a < 3; a++)
+    for (int b = 0; b < 3; b++) {
+      const int c = 3 * a + b;
+      out->start[c] = E.nop;
+      E.depth = 0;
+      if (t.root[a][b] >= 0) E.emit(t.root[a][b]);
+      out->len[c] = E.nop - out->start[c];
+    }
+  if (E.err.empty() && E.maxdepth > BG_EXPR_STACK) E.err = "nested too deeply";
+  if (!E.err.empty()) {
+    set_error("SVTENSOR %s: expression %s for the device (at most %d operations, %d constants, depth %d)",
+              t.file.c_str(), E.err.c_str(), BG_EXPR_MAXOPS, BG_EXPR_MAXCON, BG_EXPR_STACK);
+    return BG_ERR_ARG;
+  }
+  return BG_OK;
+}
+
 void svtensor_eval(const SVTensorFn &t, double wr, double wi, const double *x, double Q[18]) {
   const double kFreqUnit = 3.0e14;
   cplx v[9];

@@ -432,11 +432,23 @@ def test_svtensor_defaults(buffem_lib, sphere, tmp_path, body, defaults):
         assert np.allclose(q, np.diag([1, 5, 1]), rtol=0, atol=1e-15)
 
 
+@pytest.mark.parametrize("body,x,want", [
+    ("Eps = 2 + x\n", (0.25, 0, 0), 2.25 * np.eye(3)),
+    # the given Qxy and the identity's Qyx = 0 are averaged (SVTensor.cc:362-367)
+    ("Qxy = r*Theta\n", (0, 0.5, 0), np.array([[1, 0.125 * np.pi, 0], [0.125 * np.pi, 1, 0], [0, 0, 1]])),
+    ("MATERIAL In\n Eps(w) = 2\nENDMATERIAL\nEps = step(1.0-r)*MP_In + step(r-1.0)*MP_VACUUM\n", (0.3, 0.2, 0.1),
+     2 * np.eye(3)),
+])
+def test_svtensor_of_position(buffem_lib, sphere, tmp_path, body, x, want):
+    """SVTENSOR expressions of position (SVTensor.cc:96-102: x, y, z, r,
+    Theta, Phi) load and evaluate at a point on the host; the assembly
+    compiles them for the device at each frequency (tests/test_gpu_ref_pins)."""
+    (tmp_path / "p.SVTensor").write_text(body)
+    G = buffem.SWGGeometry(geo(tmp_path, f"OBJECT A\n MESHFILE {sphere(2)}\n SVTENSOR p.SVTensor\nENDOBJECT\n"))
+    assert np.allclose(G.material_tensor(0, 1.0, x), want, rtol=0, atol=1e-14)
+
+
 @pytest.mark.parametrize("body,words", [
-    ("Eps = 2 + x\n", "expressions of position"),
-    ("Qxy = r*Theta\n", "expressions of position"),
-    ("MATERIAL In\n Eps(w) = 2\nENDMATERIAL\nEps = step(1.0-r)*MP_In + step(r-1.0)*MP_VACUUM\n",
-     "expressions of position"),
     ("Qxw = 1\n", "invalid component"),
     ("Eps = MP_Nothing\n", "unknown material MP_Nothing"),
     ("c = two\nEps = 1\n", "invalid constant value"),

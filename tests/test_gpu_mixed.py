@@ -70,14 +70,15 @@ def test_mixed_singular_reports_info():
 
 
 @pytest.mark.parametrize("M,N,K", [(1, 1, 1), (70, 33, 17), (300, 130, 64), (513, 200, 1000), (2100, 300, 40),
-                                   (8192, 600, 256)])
+                                   (4096, 300, 100), (8192, 600, 256)])
 def test_cgemm_tf32_device(M, N, K):
     """C -= A B on the tcgen05 TF32 tensor cores (complex64): against the
     complex128 product of the same complex64 inputs, entrywise within
     2^-9 (|A| |B|)_ij plus FP32 rounding of C -- TF32 keeps 10 mantissa bits
     of each operand and accumulates in FP32.  The shapes cover ragged tiles,
     both tile widths (N <= 128 and N > 128) and more tiles than SMs, so the
-    persistent CTAs cycle through both TMEM accumulators."""
+    persistent CTAs cycle through both TMEM accumulators; the tile width
+    (64, 128 or 256 columns) follows the shape, all three occur."""
     import torch
     rng = np.random.default_rng(M + 3 * N + 7 * K)
     A = (rng.normal(size=(M, K)) + 1j * rng.normal(size=(M, K))).astype(np.complex64)

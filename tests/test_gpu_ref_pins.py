@@ -3,9 +3,9 @@
 The inputs are the reference-pinned golden cases (tests/golden/ref_libbuff.npz,
 made by tests/golden/make_ref_fixtures.py from the reference's libbuff
 sources compiled in place), read through the library's own .buffgeo, mesh,
-MATERIAL and SVTENSOR parsers where the library reads that form of the file
-(constant, MATERIAL CONST_EPS_ and tensor materials), else through the
-material API with the same function of position (Janus and Gaussian eps(x)).
+MATERIAL and SVTENSOR parsers -- the Janus and Gaussian eps(x) as SVTENSOR
+expressions of position, compiled into device programs -- and, for those two,
+once more through the material API with the same function of position.
 The library runs its default refined singular rule; the reference ran its
 own code throughout for case s48 (Taylor-Duffy at RelTol 1e-8 included) and,
 in the other cases, with the oracle's refined static integrals for
@@ -38,9 +38,9 @@ def tolerances(name):
     return (3e-8, 2e-8) if name == "s48" else (1e-10, 1e-10)
 
 
-def geometry(case, d):
+def geometry(case, d, api=False):
     geo, meshes, disp = rc.write_inputs(case, d)
-    if all(o["material"] in ("const", "tensor") for o in case["objects"]):
+    if not api:
         return buffem.SWGGeometry(GeoFileName=geo)
     mats = []
     for o in case["objects"]:
@@ -105,3 +105,18 @@ def test_case_matches_reference(name):
                 F = G.GetFields(None, Jr, w, X)
                 ok, worst = rc.close(F, FIX["%s/fields%d" % (name, i)], tp)
                 assert ok, (name, i, "fields", worst)
+
+
+@pytest.mark.parametrize("name", ["n3janus", "gauss2"])
+def test_material_api_matches_svtensor_files(name):
+    """The same eps(x) given through bg_material (Janus, Gaussian kinds) and
+    as SVTENSOR expressions of position compiled for the device: the
+    matrices agree to 1e-12 (the two evaluate the same function by different
+    code)."""
+    case = CASES[NAMES.index(name)]
+    with tempfile.TemporaryDirectory() as d:
+        w = complex(*case["omegas"][0])
+        A1 = geometry(case, d).AssembleVIEMatrix(w).download()
+        A2 = geometry(case, d, api=True).AssembleVIEMatrix(w).download()
+        ok, worst = rc.close(A1, A2, 1e-12)
+        assert ok, worst
