@@ -422,7 +422,9 @@ def run_batching(nomega=64):
     lu_flops = sum(8.0 / 3.0 * float(n) ** 3 for n in Ns) * nomega
     zpk = zgemm_peak_tflops()
     achieved = lu_flops / float(st[0]) / 1e12
-    tuning = [{"N": Ns[i], "panel_rows": int(st[4 + 3 * i]), "slots": int(st[5 + 3 * i])} for i in range(len(geo))]
+    tiles = ("64x64", "128x64", "64x128")
+    tuning = [{"N": Ns[i], "panel_rows": int(st[4 + 4 * i]), "slots": int(st[5 + 4 * i]),
+               "gemm_tile": tiles[int(st[7 + 4 * i])]} for i in range(len(geo))]
     torch.cuda.empty_cache()
     return {"jobs": int(st[1]), "seconds": float(st[0]), "s_per_job": float(st[0] / st[1]),
             "graphs": bool(st[2]), "capture_fell_back": bool(st[3]), "geometries": [m for _, m in geo],

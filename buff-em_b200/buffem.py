@@ -676,7 +676,7 @@ def BatchSweep(geoms, omegas, IF, max_streams=4, graphs=True):
     w = np.ascontiguousarray(np.asarray(omegas, dtype=np.complex128))
     hs = (C.c_void_p * len(geoms))(*[g.h for g in geoms])
     out = np.zeros((len(geoms), len(w), BG_BATCH_MAXOBJ))
-    st = np.zeros(4 + 3 * len(geoms))
+    st = np.zeros(4 + 4 * len(geoms))
     _check(lib().bg_batch_sweep(C.cast(hs, C.c_void_p), len(geoms), _ptr(w), len(w), _ptr(IF.E0), _ptr(IF.nHat),
                                 int(max_streams), 0 if graphs else BG_BATCH_NO_GRAPHS, _ptr(out), _ptr(st)))
     return out, st

@@ -17,9 +17,10 @@
 //    matrix and buffers, so that small factorisations run concurrently;
 //  * an online autotuner picks, per size class (N rounded up to 1024), the
 //    LU panel slice height (rows per CTA of the cooperative panel kernel:
-//    16, 32 or 64) and the number of concurrent slots (1, 2 or 4) by timing
-//    the sweep's own first jobs (their results are kept), and remembers the
-//    choice for later geometries of the same class.
+//    16, 32 or 64), the CTA tile of the complex128 tensor-core GEMM (64 x 64,
+//    128 x 64 or 64 x 128) and the number of concurrent slots (1, 2 or 4) by
+//    timing the sweep's own first jobs (their results are kept), and
+//    remembers the choice for later geometries of the same class.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -157,7 +158,7 @@ static int run_job(bg_geometry *g, Slot &S, const double *w, const double *E0, c
 }
 
 // autotuner memory: size class -> (panel rows, slots)
-struct Tuned { int rows = 0, slots = 0; double s_per_job = 0; };
+struct Tuned { int rows = 0, slots = 0, tile = 0; double s_per_job = 0; };
 static std::map<int, Tuned> s_tuned;
 static std::mutex s_tune_mu;
 static int size_class(int N) { return (N + 1023) / 1024; }
@@ -216,7 +217,7 @@ static int sweep_geometry(bg_geometry *g, const double *omega, int nw, const dou
   }
   int j = 0;
   std::vector<Slot> slots;
-  const int saved_rows = lu_get_panel_rows();
+  const int saved_rows = lu_get_panel_rows(), saved_tile = lu_get_gemm_tile();
   const bool tuned_now = tn.rows == 0;
   if (tuned_now) {
     // panel slice height, one slot, one job each (the first is also the warm-up)
@@ -241,6 +242,25 @@ static int sweep_geometry(bg_geometry *g, const double *omega, int nw, const dou
     }
     if (st) { free_slots(slots); lu_set_panel_rows(saved_rows); return st; }
     lu_set_panel_rows(best_rows);
+    // GEMM tile: the 64 x 64 default was timed above; one job each for the others
+    int best_tile = saved_tile;
+    for (int tile = 1; tile <= 2 && j < nw && !st; tile++) {
+      lu_set_gemm_tile(tile);
+      slots.resize(1);
+      if ((st = slot_init(g, slots[0], E0, nhat, use_graph))) break;
+      double t = 0;
+      if ((st = run_range(g, slots, omega, j, j + 1, E0, nhat, d_out, &t))) break;
+      j++;
+      if (j < nw) {
+        if ((st = run_range(g, slots, omega, j, j + 1, E0, nhat, d_out, &t))) break;
+        j++;
+      }
+      if (t < best) { best = t; best_tile = tile; }
+      st = check_slots(slots);
+      free_slots(slots);
+    }
+    if (st) { free_slots(slots); lu_set_panel_rows(saved_rows); lu_set_gemm_tile(saved_tile); return st; }
+    lu_set_gemm_tile(best_tile);
     // concurrent slots: time two jobs per slot for each count
     double best_rate = best;
     int best_slots = 1;
@@ -264,14 +284,16 @@ static int sweep_geometry(bg_geometry *g, const double *omega, int nw, const dou
       free_slots(slots);
       if (st) break;
     }
-    if (st) { free_slots(slots); lu_set_panel_rows(saved_rows); return st; }
+    if (st) { free_slots(slots); lu_set_panel_rows(saved_rows); lu_set_gemm_tile(saved_tile); return st; }
     tn.rows = best_rows;
+    tn.tile = best_tile;
     tn.slots = best_slots;
     tn.s_per_job = best_rate;
     std::lock_guard<std::mutex> lk(s_tune_mu);
     s_tuned[cls] = tn;
   }
   lu_set_panel_rows(tn.rows);
+  lu_set_gemm_tile(tn.tile);
   double t = 0;
   if (j < nw) {
     slots.resize(std::min(tn.slots, nw - j));
@@ -282,7 +304,13 @@ static int sweep_geometry(bg_geometry *g, const double *omega, int nw, const dou
   if (!st) st = check_slots(slots);
   free_slots(slots);
   lu_set_panel_rows(saved_rows);
-  if (tuning) { tuning[0] = tn.rows; tuning[1] = tn.slots; tuning[2] = tuned_now ? tn.s_per_job : 0.0; }
+  lu_set_gemm_tile(saved_tile);
+  if (tuning) {
+    tuning[0] = tn.rows;
+    tuning[1] = tn.slots;
+    tuning[2] = tuned_now ? tn.s_per_job : 0.0;
+    tuning[3] = tn.tile;
+  }
   return st;
 }
 
@@ -321,7 +349,7 @@ int bg_batch_sweep(bg_geometry *const *geoms, int ngeom, const double *omega, in
   if (ea != cudaSuccess) { cudaFreeHost(h_w); set_error("bg_batch_sweep: %s", cudaGetErrorString(ea)); return BG_ERR_NOMEM; }
   double t0 = std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
   for (int i = 0; i < ngeom && !st; i++) {
-    double tun[3] = {0, 0, 0};
+    double tun[4] = {0, 0, 0, 0};
     cudaError_t e0 = cudaMemset(d_out, 0, sizeof(double) * BATCH_MAXOBJ * (size_t)nomega);
     if (e0 != cudaSuccess) { set_error("bg_batch_sweep: %s", cudaGetErrorString(e0)); st = BG_ERR_CUDA; break; }
     st = sweep_geometry(geoms[i], h_w, nomega, E0, nhat, max_streams, use_graph, d_out, tun);
@@ -331,9 +359,10 @@ int bg_batch_sweep(bg_geometry *const *geoms, int ngeom, const double *omega, in
       if (e != cudaSuccess) { set_error("bg_batch_sweep: %s", cudaGetErrorString(e)); st = BG_ERR_CUDA; }
     }
     if (stats) {
-      stats[4 + 3 * i] = tun[0];
-      stats[5 + 3 * i] = tun[1];
-      stats[6 + 3 * i] = tun[2];
+      stats[4 + 4 * i] = tun[0];
+      stats[5 + 4 * i] = tun[1];
+      stats[6 + 4 * i] = tun[2];
+      stats[7 + 4 * i] = tun[3];
     }
   }
   double t1 = std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();

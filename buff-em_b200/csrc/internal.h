@@ -301,6 +301,8 @@ int *lu_capture_solve_err_ptr(bg_matrix *m);
 int lu_solve_enqueue(bg_matrix *m, void *dB, int ldb, int nrhs, void *dT);
 void lu_set_panel_rows(int rows);
 int lu_get_panel_rows();
+void lu_set_gemm_tile(int tile);   // complex128 GEMM CTA tile: 0 64x64, 1 128x64, 2 64x128
+int lu_get_gemm_tile();
 int gmres_solve(bg_matrix *A, const bg_precond *P, void *dB, int ldb, int nrhs, double tol, int restart, int maxit,
                 double *stats, const bg_precond *Palt = nullptr, int *cycle = nullptr);
 // what the last mixed-precision solve of this thread did beyond its stats

@@ -182,29 +182,37 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, BK, STAGES>::THREADS)
       }
 }
 
-#ifndef ZG_BM
-#define ZG_BM 64
-#define ZG_BN 64
-#define ZG_BK 16
-#define ZG_ST 3
-#endif
+// CTA tile of the complex128 GEMM, chosen at run time (the batching form's
+// autotuner times them per size class): 0 = 64 x 64, 1 = 128 x 64,
+// 2 = 64 x 128 complex outputs; warps always own 32 x 32.
+static int zg_tile = 0;
+void lu_set_gemm_tile(int t) { zg_tile = (t >= 0 && t <= 2) ? t : 0; }
+int lu_get_gemm_tile() { return zg_tile; }
 
-static int zgemm_sub(int M, int N, int K, const cdl *A, size_t lda, const cdl *B, size_t ldb, cdl *C, size_t ldc) {
-  if (M <= 0 || N <= 0 || K <= 0) return BG_OK;
-  using Cfg = GemmCfg<ZG_BM, ZG_BN, ZG_BK, ZG_ST>;
-  auto kern = k_zgemm_sub<ZG_BM, ZG_BN, ZG_BK, ZG_ST>;
+template <int BM, int BN>
+static int zgemm_launch(int M, int N, int K, const cdl *A, size_t lda, const cdl *B, size_t ldb, cdl *C, size_t ldc) {
+  using Cfg = GemmCfg<BM, BN, 16, 3>;
+  auto kern = k_zgemm_sub<BM, BN, 16, 3>;
   static bool attr = false;
   if (!attr) {
     BG_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM));
     attr = true;
   }
-  dim3 grid((M + ZG_BM - 1) / ZG_BM, (N + ZG_BN - 1) / ZG_BN);
+  dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN);
   if (grid.y > 65535) { set_error("zgemm: N too large"); return BG_ERR_ARG; }
-  prof_start(PROF_GEMM);
   kern<<<grid, Cfg::THREADS, Cfg::SMEM, stream()>>>(M, N, K, A, lda, B, ldb, C, ldc);
   BG_LAUNCHED();
-  prof_stop(PROF_GEMM, 8.0 * M * (double)N * K);
   return BG_OK;
+}
+
+static int zgemm_sub(int M, int N, int K, const cdl *A, size_t lda, const cdl *B, size_t ldb, cdl *C, size_t ldc) {
+  if (M <= 0 || N <= 0 || K <= 0) return BG_OK;
+  prof_start(PROF_GEMM);
+  int st = zg_tile == 1 ? zgemm_launch<128, 64>(M, N, K, A, lda, B, ldb, C, ldc)
+         : zg_tile == 2 ? zgemm_launch<64, 128>(M, N, K, A, lda, B, ldb, C, ldc)
+                        : zgemm_launch<64, 64>(M, N, K, A, lda, B, ldb, C, ldc);
+  prof_stop(PROF_GEMM, 8.0 * M * (double)N * K);
+  return st;
 }
 
 // =========================================================================

@@ -403,12 +403,14 @@ int bg_precond_download(const bg_precond *P, int *rowptr, int *col, double *val)
    a CUDA graph whose kernels read omega from device memory, and replayed per
    frequency; up to max_streams slots run concurrently.  An online autotuner
    picks, per size class (N rounded up to 1024), the LU panel slice height
-   (16/32/64 rows per CTA) and the slot count (1, 2, 4, ... <= max_streams)
-   by timing the sweep's own first jobs, and keeps the choice for later
-   geometries of that class.  stats (may be NULL; 4 + 3*ngeom doubles): wall
-   seconds, jobs, graphs requested, 1 if a capture fell back to direct
-   launches; then per geometry the chosen panel rows, slots and seconds per
-   job measured while tuning (0 if the class was already tuned).
+   (16/32/64 rows per CTA), the CTA tile of the complex128 tensor-core GEMM
+   (0: 64 x 64, 1: 128 x 64, 2: 64 x 128) and the slot count (1, 2, 4, ...
+   <= max_streams) by timing the sweep's own first jobs, and keeps the
+   choice for later geometries of that class.  stats (may be NULL;
+   4 + 4*ngeom doubles): wall seconds, jobs, graphs requested, 1 if a capture
+   fell back to direct launches; then per geometry the chosen panel rows,
+   slots, seconds per job measured while tuning (0 if the class was already
+   tuned) and GEMM tile.
    Returns BG_ERR_NUMERIC if a matrix was singular. */
 int bg_batch_sweep(bg_geometry *const *geoms, int ngeom, const double *omega, int nomega, const double *E0,
                    const double *nhat, int max_streams, int flags, double *pabs, double *stats);

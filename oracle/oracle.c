@@ -1795,15 +1795,18 @@ void or_pft_emt(OGeom *G, double wr, double wi, const double *J, const double *E
   PW pw;
   for (int i = 0; i < 3; i++) { pw.E0[i] = E0[2 * i] + I * E0[2 * i + 1]; pw.nhat[i] = nhat[i]; }
   pw.k = omega;
+  /* per-row partial sums, added in row order after the parallel loop, so
+     that the result does not depend on the thread schedule */
+  double *rs = calloc((size_t)N * NO * NO, sizeof(double));
+  double *re_ = calloc((size_t)N * NO, sizeof(double));
 #pragma omp parallel
   {
-    double *ls = calloc((size_t)NO * NO, sizeof(double));
-    double *le = calloc(NO, sizeof(double));
 #pragma omp for schedule(dynamic, 1)
     for (int a = 0; a < N; a++) {
       int noa, nfa;
       OObj *OA = resolve(G, a, &noa, &nfa);
       cplx Ja = J[2 * a] + I * J[2 * a + 1];
+      double *ls = rs + (size_t)a * NO * NO, *le = re_ + (size_t)a * NO;
       for (int b = a; b < N; b++) {
         int nob, nfb;
         OObj *OB = resolve(G, b, &nob, &nfb);
@@ -1824,13 +1827,12 @@ void or_pft_emt(OGeom *G, double wr, double wi, const double *J, const double *E
       cplx qe = bf_dot_field(OA, nfa, &pw);
       le[noa] += creal(conj(Ja) * qe);
     }
-#pragma omp critical
-    {
-      for (int i = 0; i < NO * NO; i++) scat[i] += ls[i];
-      for (int i = 0; i < NO; i++) ext[i] += le[i];
-    }
-    free(ls); free(le);
   }
+  for (int a = 0; a < N; a++) {
+    for (int i = 0; i < NO * NO; i++) scat[i] += rs[(size_t)a * NO * NO + i];
+    for (int i = 0; i < NO; i++) ext[i] += re_[(size_t)a * NO + i];
+  }
+  free(rs); free(re_);
   for (int no = 0; no < NO; no++) {
     double ps = 0.0;
     for (int nob = 0; nob < NO; nob++) ps += scat[no * NO + nob];
@@ -1942,15 +1944,18 @@ static void pft_emt8_impl(OGeom *G, double wr, double wi, const double *J, const
   if (E0)
     for (int i = 0; i < 3; i++) { pw.E0[i] = E0[2 * i] + I * E0[2 * i + 1]; pw.nhat[i] = nhat[i]; }
   pw.k = omega;
+  /* per-row partial sums, added in row order after the parallel loop */
+  size_t RS = (size_t)NO * NO * 10, RE = (size_t)NO * 10;
+  double *rs = calloc((size_t)N * RS, sizeof(double));
+  double *re_ = calloc((size_t)N * RE, sizeof(double));
 #pragma omp parallel
   {
-    double *ls = calloc((size_t)NO * NO * 10, sizeof(double));
-    double *le = calloc((size_t)NO * 10, sizeof(double));
 #pragma omp for schedule(dynamic, 1)
     for (int a = 0; a < N; a++) {
       int noa, nfa;
       OObj *OA = resolve(G, a, &noa, &nfa);
       cplx Ja = J ? J[2 * a] + I * J[2 * a + 1] : 0.0;
+      double *ls = rs + (size_t)a * RS, *le = re_ + (size_t)a * RE;
       for (int b = a; b < N; b++) {
         int nob, nfb;
         OObj *OB = resolve(G, b, &nob, &nfb);
@@ -1994,13 +1999,12 @@ static void pft_emt8_impl(OGeom *G, double wr, double wi, const double *J, const
         e[7 + i] += cimag(conj(Ja) * ik * (qx[i1] * nhat[i2] - qx[i2] * nhat[i1])); /* b . (XT x grad)_i E */
       }
     }
-#pragma omp critical
-    {
-      for (int i = 0; i < NO * NO * 10; i++) scat[i] += ls[i];
-      for (int i = 0; i < NO * 10; i++) ext[i] += le[i];
-    }
-    free(ls); free(le);
   }
+  for (int a = 0; a < N; a++) {
+    for (size_t i = 0; i < RS; i++) scat[i] += rs[(size_t)a * RS + i];
+    for (size_t i = 0; i < RE; i++) ext[i] += re_[(size_t)a * RE + i];
+  }
+  free(rs); free(re_);
   double ftf = 0.5 * TEN_THIRDS / wr;
   for (int no = 0; no < NO; no++) {
     double s[10] = {0};

@@ -58,8 +58,9 @@ def test_batch_sweep_reuses_tuning_for_a_size_class(sphere):
     G2 = buffem.SWGGeometry(meshfiles=sphere(5, jitter=0.05, seed=2), materials=buffem.Material(eps=6 + 0.5j))
     omegas = np.linspace(0.5, 3.0, 12)
     pabs, st = buffem.BatchSweep([G1, G2], omegas, WAVE, max_streams=4)
-    rows1, slots1, t1 = st[4:7]
-    rows2, slots2, t2 = st[7:10]
-    assert rows1 in (16, 32, 64) and slots1 in (1, 2, 4) and t1 > 0
-    assert (rows2, slots2) == (rows1, slots1) and t2 == 0   # same size class: the first geometry's choice
+    rows1, slots1, t1, tile1 = st[4:8]
+    rows2, slots2, t2, tile2 = st[8:12]
+    assert rows1 in (16, 32, 64) and slots1 in (1, 2, 4) and t1 > 0 and tile1 in (0, 1, 2)
+    # same size class: the first geometry's choice
+    assert (rows2, slots2, tile2) == (rows1, slots1, tile1) and t2 == 0
     np.testing.assert_allclose(pabs[1], sequential(G2, omegas), rtol=1e-10)
