@@ -227,6 +227,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       const int row = tm * TC_BM + q * 32 + lane;   // row of C~ (2 x complex row + component)
 #pragma unroll 1
       for (int c0 = 0; c0 < BN; c0 += 32) {
+        // the 32 loads of C are issued together, before the TMEM read, so
+        // that their latencies overlap (a load-subtract-store per column
+        // would wait for the previous column's store: C's columns may alias
+        // as far as the compiler knows)
+        const int col0 = tn * BN + c0;
+        float *pc = P.C + (size_t)col0 * ldr + row;
+        float cv[32];
+        if (row < P.M2) {
+#pragma unroll
+          for (int j = 0; j < 32; j++) cv[j] = col0 + j < P.N ? pc[(size_t)j * ldr] : 0.f;
+        }
         uint32_t r[32];
         const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BN + c0);
         asm volatile(
@@ -240,14 +251,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             : "r"(taddr));
         asm volatile("tcgen05.wait::ld.sync.aligned;");
         if (row < P.M2) {
-          const int col0 = tn * BN + c0;
 #pragma unroll
-          for (int j = 0; j < 32; j++) {
-            if (col0 + j < P.N) {
-              float *p = P.C + (size_t)(col0 + j) * ldr + row;
-              *p -= __uint_as_float(r[j]);
-            }
-          }
+          for (int j = 0; j < 32; j++)
+            if (col0 + j < P.N) pc[(size_t)j * ldr] = cv[j] - __uint_as_float(r[j]);
         }
       }
       // this warp has read accumulator b: hand it back to the MMA issuer

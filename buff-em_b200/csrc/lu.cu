@@ -164,22 +164,34 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, BK, STAGES>::THREADS)
     }
   }
   cp_wait<0>();
+  // C -= accumulators, eight entries at a time: the loads of a group are
+  // issued together before its stores (one memory round trip per group
+  // instead of one per entry)
 #pragma unroll
-  for (int mt = 0; mt < 2; mt++)
+  for (int nt = 0; nt < 4; nt++) {
+    cdl x[2][4];
 #pragma unroll
-    for (int nt = 0; nt < 4; nt++)
+    for (int mt = 0; mt < 2; mt++)
 #pragma unroll
       for (int v = 0; v < 4; v++) {
-        int row = m0 + wm * 32 + mt * 16 + t1 + 8 * (v >> 1);
-        int col = n0 + wn * 32 + nt * 8 + 2 * t0 + (v & 1);
+        const int row = m0 + wm * 32 + mt * 16 + t1 + 8 * (v >> 1);
+        const int col = n0 + wn * 32 + nt * 8 + 2 * t0 + (v & 1);
+        x[mt][v] = (row < M && col < N) ? C[(size_t)col * ldc + row] : cdl{0.0, 0.0};
+      }
+#pragma unroll
+    for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+      for (int v = 0; v < 4; v++) {
+        const int row = m0 + wm * 32 + mt * 16 + t1 + 8 * (v >> 1);
+        const int col = n0 + wn * 32 + nt * 8 + 2 * t0 + (v & 1);
         if (row < M && col < N) {
-          cdl *p = C + (size_t)col * ldc + row;
-          cdl x = *p;
-          x.r -= cr[mt][nt][v];
-          x.i -= ci[mt][nt][v];
-          *p = x;
+          cdl y = x[mt][v];
+          y.r -= cr[mt][nt][v];
+          y.i -= ci[mt][nt][v];
+          C[(size_t)col * ldc + row] = y;
         }
       }
+  }
 }
 
 // CTA tile of the complex128 GEMM, chosen at run time (the batching form's
@@ -217,10 +229,12 @@ static int zgemm_sub(int M, int N, int K, const cdl *A, size_t lda, const cdl *B
 
 // =========================================================================
 // leaf triangular solves (n <= 64 rows).  The triangle is staged in shared
-// memory once per CTA; each warp then solves whole right-hand-side columns:
-// lane l holds rows l and l+32 of the column in registers, the solved entry
-// of step i is broadcast with a warp shuffle, and every lane updates its two
-// rows -- no block barriers inside the substitution.
+// memory once per CTA; each warp then solves TRS_CPW right-hand-side columns
+// together: lane l holds rows l and l+32 of each of its columns in registers,
+// the solved entries of step i are broadcast with warp shuffles, and every
+// lane updates its two rows of every column with the one triangle entry it
+// read -- TRS_CPW independent recurrences per step, no block barriers inside
+// the substitution.
 // =========================================================================
 #define TRS_WARPS 8
 #define TRS_CPW 8                         // columns per warp per CTA
@@ -236,38 +250,67 @@ __global__ void __launch_bounds__(TRS_WARPS * 32) k_trsm_leaf(int n, int m, cons
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C(*Ts)[65] = (C(*)[65])smem_raw;   // Ts[r][c]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int e = tid; e < n * n; e += TRS_WARPS * 32) {
-    int r = e % n, c = e / n;
-    Ts[r][c] = T[(size_t)c * ldt + r];
+  // staged eight loads per thread at a time (their latencies overlap)
+  for (int e0 = 0; e0 < n * n; e0 += 8 * TRS_WARPS * 32) {
+    C v[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int e = e0 + u * TRS_WARPS * 32 + tid;
+      v[u] = e < n * n ? T[(size_t)(e / n) * ldt + e % n] : C{0, 0};
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int e = e0 + u * TRS_WARPS * 32 + tid;
+      if (e < n * n) Ts[e % n][e / n] = v[u];
+    }
   }
   __syncthreads();
   const int r0 = lane, r1 = lane + 32;
+  const int cbase = blockIdx.x * TRS_COLS + warp * TRS_CPW;
+  if (cbase >= m) return;
+  C b0[TRS_CPW], b1[TRS_CPW];
+#pragma unroll
   for (int j = 0; j < TRS_CPW; j++) {
-    const int col = blockIdx.x * TRS_COLS + warp * TRS_CPW + j;
-    if (col >= m) break;
-    C *bc = B + (size_t)col * ldb;
-    C b0 = r0 < n ? bc[r0] : C{0, 0};
-    C b1 = r1 < n ? bc[r1] : C{0, 0};
-    if (!upper) {
-      for (int i = 0; i < n; i++) {
-        C x = cshfl(i < 32 ? b0 : b1, i & 31);
-        if (r0 > i && r0 < n) { C l = Ts[r0][i]; b0.r -= l.r * x.r - l.i * x.i; b0.i -= l.r * x.i + l.i * x.r; }
-        if (r1 > i && r1 < n) { C l = Ts[r1][i]; b1.r -= l.r * x.r - l.i * x.i; b1.i -= l.r * x.i + l.i * x.r; }
-      }
-    } else {
-      for (int i = n - 1; i >= 0; i--) {
-        C v = cshfl(i < 32 ? b0 : b1, i & 31);
-        C u = Ts[i][i];
-        R d = u.r * u.r + u.i * u.i;
-        C x{(v.r * u.r + v.i * u.i) / d, (v.i * u.r - v.r * u.i) / d};
-        if (r0 == i) b0 = x;
-        if (r1 == i) b1 = x;
-        if (r0 < i) { C t = Ts[r0][i]; b0.r -= t.r * x.r - t.i * x.i; b0.i -= t.r * x.i + t.i * x.r; }
-        if (r1 < i) { C t = Ts[r1][i]; b1.r -= t.r * x.r - t.i * x.i; b1.i -= t.r * x.i + t.i * x.r; }
+    const int col = cbase + j;
+    const C *bc = B + (size_t)col * ldb;
+    b0[j] = (col < m && r0 < n) ? bc[r0] : C{0, 0};
+    b1[j] = (col < m && r1 < n) ? bc[r1] : C{0, 0};
+  }
+  if (!upper) {
+    for (int i = 0; i < n; i++) {
+      const bool u0 = r0 > i && r0 < n, u1 = r1 > i && r1 < n;
+      const C l0 = u0 ? Ts[r0][i] : C{0, 0}, l1 = u1 ? Ts[r1][i] : C{0, 0};
+#pragma unroll
+      for (int j = 0; j < TRS_CPW; j++) {
+        const C x = cshfl(i < 32 ? b0[j] : b1[j], i & 31);
+        if (u0) { b0[j].r -= l0.r * x.r - l0.i * x.i; b0[j].i -= l0.r * x.i + l0.i * x.r; }
+        if (u1) { b1[j].r -= l1.r * x.r - l1.i * x.i; b1[j].i -= l1.r * x.i + l1.i * x.r; }
       }
     }
-    if (r0 < n) bc[r0] = b0;
-    if (r1 < n) bc[r1] = b1;
+  } else {
+    for (int i = n - 1; i >= 0; i--) {
+      const C u = Ts[i][i];
+      const R d = u.r * u.r + u.i * u.i;
+      const bool u0 = r0 < i, u1 = r1 < i;
+      const C t0 = u0 ? Ts[r0][i] : C{0, 0}, t1 = u1 ? Ts[r1][i] : C{0, 0};
+#pragma unroll
+      for (int j = 0; j < TRS_CPW; j++) {
+        const C v = cshfl(i < 32 ? b0[j] : b1[j], i & 31);
+        const C x{(v.r * u.r + v.i * u.i) / d, (v.i * u.r - v.r * u.i) / d};
+        if (r0 == i) b0[j] = x;
+        if (r1 == i) b1[j] = x;
+        if (u0) { b0[j].r -= t0.r * x.r - t0.i * x.i; b0[j].i -= t0.r * x.i + t0.i * x.r; }
+        if (u1) { b1[j].r -= t1.r * x.r - t1.i * x.i; b1[j].i -= t1.r * x.i + t1.i * x.r; }
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < TRS_CPW; j++) {
+    const int col = cbase + j;
+    if (col >= m) break;
+    C *bc = B + (size_t)col * ldb;
+    if (r0 < n) bc[r0] = b0[j];
+    if (r1 < n) bc[r1] = b1[j];
   }
 }
 
@@ -361,7 +404,11 @@ static int trsm(int n, int m, const C *T, size_t ldt, C *B, size_t ldb, int uppe
 }
 
 // =========================================================================
-// cooperative panel factorisation of A[k0:Nr, k0:k0+w] (w <= 32)
+// cooperative panel factorisation of A[k0:Nr, k0:k0+w] (w <= 32).  Each CTA
+// holds a slice of rows_per rows in shared memory, column-major (column c at
+// S + c * rows_per): the pivot scan and the rank-1 update walk a column with
+// consecutive threads on consecutive rows, free of bank conflicts.  One grid
+// barrier per column exchanges the CTAs' pivot candidates.
 // =========================================================================
 template <class C>
 struct PanelArgs {
@@ -387,7 +434,7 @@ __global__ void __launch_bounds__(256) k_panel(PanelArgs<C> P) {
   typedef typename CxT<C>::R R;
   cg::grid_group grid = cg::this_grid();
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C *S = (C *)smem_raw;                     // [rows_per][w]
+  C *S = (C *)smem_raw;                     // [w][rows_per]: column c at S + c * rows_per
   __shared__ double rv[8];
   __shared__ int ri[8];
   __shared__ int s_piv;
@@ -395,10 +442,20 @@ __global__ void __launch_bounds__(256) k_panel(PanelArgs<C> P) {
   const int w = P.w, G = gridDim.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int r0 = P.k0 + blockIdx.x * P.rows_per;
   const int r1 = min(P.Nr, r0 + P.rows_per);
-  const int nr = max(0, r1 - r0);
-  for (int e = tid; e < nr * w; e += 256) {
-    int r = e / w, c = e % w;
-    S[r * w + c] = P.A[(size_t)(P.k0 + c) * P.ld + r0 + r];
+  const int nr = max(0, r1 - r0), lds = P.rows_per;
+  // slice staged with eight loads per thread in flight
+  for (int e0 = 0; e0 < nr * w; e0 += 8 * 256) {
+    C v[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int e = e0 + u * 256 + tid;
+      v[u] = e < nr * w ? P.A[(size_t)(P.k0 + e / nr) * P.ld + r0 + e % nr] : C{0, 0};
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int e = e0 + u * 256 + tid;
+      if (e < nr * w) S[(e / nr) * lds + e % nr] = v[u];
+    }
   }
   __syncthreads();
   for (int j = 0; j < w; j++) {
@@ -409,7 +466,7 @@ __global__ void __launch_bounds__(256) k_panel(PanelArgs<C> P) {
     for (int r = tid; r < nr; r += 256) {
       int gr = r0 + r;
       if (gr < gj) continue;
-      C v = S[r * w + j];
+      C v = S[j * lds + r];
       double a = (double)(fabs(v.r) + fabs(v.i));
       if (better(a, gr, bv, bi)) { bv = a; bi = gr; }
     }
@@ -428,8 +485,8 @@ __global__ void __launch_bounds__(256) k_panel(PanelArgs<C> P) {
     }
     __syncthreads();
     int myc = ri[0];
-    if (rv[0] >= 0.0 && tid < w) P.crow[((size_t)buf * G + blockIdx.x) * 32 + tid] = S[(myc - r0) * w + tid];
-    if (gj >= r0 && gj < r1 && tid < w) P.jrow[buf * 32 + tid] = S[(gj - r0) * w + tid];
+    if (rv[0] >= 0.0 && tid < w) P.crow[((size_t)buf * G + blockIdx.x) * 32 + tid] = S[tid * lds + myc - r0];
+    if (gj >= r0 && gj < r1 && tid < w) P.jrow[buf * 32 + tid] = S[tid * lds + gj - r0];
     grid.sync();
     // 2. global pivot
     if (tid < 32) {
@@ -454,8 +511,8 @@ __global__ void __launch_bounds__(256) k_panel(PanelArgs<C> P) {
     if (blockIdx.x == 0 && tid == 0) P.ipiv[gj] = piv + 1;
     // 3. swap rows gj and piv inside the panel
     if (piv != gj) {
-      if (piv >= r0 && piv < r1 && tid < w) S[(piv - r0) * w + tid] = P.jrow[buf * 32 + tid];
-      if (gj >= r0 && gj < r1 && tid < w) S[(gj - r0) * w + tid] = prow[tid];
+      if (piv >= r0 && piv < r1 && tid < w) S[tid * lds + piv - r0] = P.jrow[buf * 32 + tid];
+      if (gj >= r0 && gj < r1 && tid < w) S[tid * lds + gj - r0] = prow[tid];
     }
     __syncthreads();
     // 4. scale the column below the pivot and update the rest of the panel
@@ -469,12 +526,12 @@ __global__ void __launch_bounds__(256) k_panel(PanelArgs<C> P) {
       for (int r = tid; r < nr; r += 256) {
         int gr = r0 + r;
         if (gr <= gj) continue;
-        C v = S[r * w + j];
+        C v = S[j * lds + r];
         C l{v.r * inv.r - v.i * inv.i, v.r * inv.i + v.i * inv.r};
-        S[r * w + j] = l;
+        S[j * lds + r] = l;
         for (int c = 1; c <= ncol; c++) {
           C u = prow[j + c];
-          C &t = S[r * w + j + c];
+          C &t = S[(j + c) * lds + r];
           t.r -= l.r * u.r - l.i * u.i;
           t.i -= l.r * u.i + l.i * u.r;
         }
@@ -483,9 +540,22 @@ __global__ void __launch_bounds__(256) k_panel(PanelArgs<C> P) {
     __syncthreads();
   }
   for (int e = tid; e < nr * w; e += 256) {
-    int r = e / w, c = e % w;
-    P.A[(size_t)(P.k0 + c) * P.ld + r0 + r] = S[r * w + c];
+    const int r = e % nr, c = e / nr;
+    P.A[(size_t)(P.k0 + c) * P.ld + r0 + r] = S[c * lds + r];
   }
+}
+
+template <class C>
+__device__ __forceinline__ C ldcg_c(const C *p);
+template <>
+__device__ __forceinline__ cdl ldcg_c<cdl>(const cdl *p) {
+  double2 v = __ldcg((const double2 *)p);
+  return cdl{v.x, v.y};
+}
+template <>
+__device__ __forceinline__ cfl ldcg_c<cfl>(const cfl *p) {
+  float2 v = __ldcg((const float2 *)p);
+  return cfl{v.x, v.y};
 }
 
 // apply the interchanges ipiv[k0..k0+w) to columns [c0, c1) of A
@@ -661,19 +731,6 @@ __global__ void k_gather_rows(int N, int nrhs, const int *perm, const C *src, si
 }
 
 template <class C>
-__device__ __forceinline__ C ldcg_c(const C *p);
-template <>
-__device__ __forceinline__ cdl ldcg_c<cdl>(const cdl *p) {
-  double2 v = __ldcg((const double2 *)p);
-  return cdl{v.x, v.y};
-}
-template <>
-__device__ __forceinline__ cfl ldcg_c<cfl>(const cfl *p) {
-  float2 v = __ldcg((const float2 *)p);
-  return cfl{v.x, v.y};
-}
-
-template <class C>
 constexpr int trsv_smem() {
   return TV_B * (TV_B + 1) * (int)sizeof(C) + 2 * TV_B * TV_MAXRHS * (int)sizeof(C);
 }
@@ -694,17 +751,42 @@ __global__ void __launch_bounds__(128) k_trsv(int N, const C *A, size_t ld, C *X
   const int lb = s_blk;
   const int bi = UPPER ? nb - 1 - lb : lb;
   const int r0 = bi * TV_B, rows = min(TV_B, N - r0);
-  // stage the diagonal block
-  for (int e = tid; e < rows * rows; e += 128) {
-    int r = e % rows, c = e / rows;
-    D[r][c] = A[(size_t)(r0 + c) * ld + r0 + r];
-  }
   const int row = tid & (TV_B - 1), half = tid >> 6;
+  // this block's right-hand-side rows (written by no other CTA), read now
+  // so that the final combine does not wait for memory
+  C bx[TV_MAXRHS];
+#pragma unroll
+  for (int j = 0; j < TV_MAXRHS; j++)
+    bx[j] = (half == 0 && row < rows && j < nrhs) ? X[(size_t)j * ldx + r0 + row] : C{0, 0};
+  // stage the diagonal block, eight loads per thread in flight
+  for (int e0 = 0; e0 < rows * rows; e0 += 8 * 128) {
+    C v[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int e = e0 + u * 128 + tid;
+      v[u] = e < rows * rows ? A[(size_t)(r0 + e / rows) * ld + r0 + e % rows] : C{0, 0};
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int e = e0 + u * 128 + tid;
+      if (e < rows * rows) D[e % rows][e / rows] = v[u];
+    }
+  }
   C acc[TV_MAXRHS];
 #pragma unroll
   for (int j = 0; j < TV_MAXRHS; j++) acc[j] = C{0, 0};
   for (int q = 0; q < lb; q++) {
     const int bj = UPPER ? nb - 1 - q : q;
+    const int c0 = bj * TV_B, cols = min(TV_B, N - c0);
+    // this thread's row of block (bi, bj) over its half of the columns:
+    // A does not depend on x, so it is read before waiting for block bj
+    C a[32];
+    {
+      const C *ap = A + (size_t)(c0 + half * 32) * ld + r0 + row;
+#pragma unroll
+      for (int u = 0; u < 32; u++)
+        a[u] = (row < rows && half * 32 + u < cols) ? ap[(size_t)u * ld] : C{0, 0};
+    }
     if (tid == 0) {
       volatile int *f = flags + bj;
       int it = 0;
@@ -720,32 +802,31 @@ __global__ void __launch_bounds__(128) k_trsv(int N, const C *A, size_t ld, C *X
     }
     __syncthreads();
     if (s_abort) return;
-    const int c0 = bj * TV_B, cols = min(TV_B, N - c0);
-    // the solved block's x, once per CTA
-    for (int e = tid; e < cols * nrhs; e += 128) {
-      const int c = e % cols, j = e / cols;
-      xs[c][j] = ldcg_c(X + (size_t)j * ldx + c0 + c);
+    // the solved block's x, once per CTA (at most 2 per thread)
+    {
+      C v[2];
+#pragma unroll
+      for (int u = 0; u < 2; u++) {
+        const int e = u * 128 + tid;
+        v[u] = e < cols * nrhs ? ldcg_c(X + (size_t)(e / cols) * ldx + c0 + e % cols) : C{0, 0};
+      }
+#pragma unroll
+      for (int u = 0; u < 2; u++) {
+        const int e = u * 128 + tid;
+        if (e < cols * nrhs) xs[e % cols][e / cols] = v[u];
+      }
     }
     __syncthreads();
     if (row < rows) {
-      // this thread's row against half of the block's columns, eight
-      // independent loads of A in flight at a time
-      const C *ap = A + (size_t)c0 * ld + r0 + row;
-      const int ce = min(cols, half * 32 + 32);
-      for (int c8 = half * 32; c8 < ce; c8 += 8) {
-        C a[8];
 #pragma unroll
-        for (int u = 0; u < 8; u++) a[u] = c8 + u < ce ? ap[(size_t)(c8 + u) * ld] : C{0, 0};
+      for (int u = 0; u < 32; u++) {
+        if (half * 32 + u >= cols) break;
 #pragma unroll
-        for (int u = 0; u < 8; u++) {
-          if (c8 + u >= ce) break;
-#pragma unroll
-          for (int j = 0; j < TV_MAXRHS; j++) {
-            if (j < nrhs) {
-              const C x = xs[c8 + u][j];
-              acc[j].r += a[u].r * x.r - a[u].i * x.i;
-              acc[j].i += a[u].r * x.i + a[u].i * x.r;
-            }
+        for (int j = 0; j < TV_MAXRHS; j++) {
+          if (j < nrhs) {
+            const C x = xs[half * 32 + u][j];
+            acc[j].r += a[u].r * x.r - a[u].i * x.i;
+            acc[j].i += a[u].r * x.i + a[u].i * x.r;
           }
         }
       }
@@ -761,7 +842,7 @@ __global__ void __launch_bounds__(128) k_trsv(int N, const C *A, size_t ld, C *X
 #pragma unroll
     for (int j = 0; j < TV_MAXRHS; j++)
       if (j < nrhs) {
-        C b = X[(size_t)j * ldx + r0 + row];
+        const C b = bx[j];
         C p = part[row][j];
         part[row][j] = C{b.r - acc[j].r - p.r, b.i - acc[j].i - p.i};
       }

@@ -57,6 +57,32 @@ def test_mixed_random_matrix_sizes():
         assert np.linalg.norm(X - xo) <= 1e-10 * np.linalg.norm(xo), (N, st)
 
 
+@pytest.mark.parametrize("N", [300, 2500])
+def test_c64_factors_partial_pivoting(N):
+    """The complex64 factorisation itself (cooperative panels over up to 79
+    CTAs, TF32 trailing updates): P A = L U to TF32
+    accuracy -- 4 sqrt(N) 2^-11 of |A| in Frobenius norm (observed 6.6e-3 at
+    N = 300, against ~8e-3 expected from K = 300 reductions at TF32's unit
+    roundoff; a wrong swap or update leaves O(1) errors) -- and partial
+    pivoting by |re|+|im| bounds every multiplier by sqrt(2) in modulus."""
+    rng = np.random.default_rng(11)
+    A = (rng.normal(size=(N, N)) + 1j * rng.normal(size=(N, N))).astype(np.complex128)
+    from test_gpu_parity import RawMatrix
+    M = RawMatrix(N)
+    M.upload(A)
+    F = M.G.AllocateVIEMatrix(buffem.BG_C64).convert_from(M.M)
+    F.LUFactorize()
+    LU = F.download().astype(np.complex128)
+    piv = F.pivots() - 1
+    L = np.tril(LU, -1) + np.eye(N)
+    U = np.triu(LU)
+    PA = A.copy()
+    for i, p in enumerate(piv):
+        PA[[i, p]] = PA[[p, i]]
+    assert np.abs(np.tril(LU, -1)).max() <= np.sqrt(2) * (1 + 1e-6)
+    assert np.linalg.norm(PA - L @ U) <= 4 * np.sqrt(N) * 2.0 ** -11 * np.linalg.norm(A)
+
+
 def test_mixed_singular_reports_info():
     from test_gpu_parity import RawMatrix
     M = RawMatrix(50)
