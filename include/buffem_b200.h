@@ -75,7 +75,7 @@ const char *bg_last_error(void);
    assembled at, except in bg_batch_sweep) and OBJECT <label> ... ENDOBJECT
    sections holding MESHFILE, MATERIAL (CONST_EPS_<value>, VACUUM or the name
    of a MATERIAL section above) or SVTENSOR <file> (a permittivity tensor of
-   frequency; expressions of position are refused), and any number of
+   frequency and position, evaluated on the device), and any number of
    DISPLACED dx dy dz / ROTATED theta ABOUT ax ay az lines, composed in order
    and applied to the mesh before its vertex merge (SWGGeometry.cc:52-158);
    the special name MESH__<mesh>__MAT__<material> stands for a one-object
