@@ -503,6 +503,31 @@ def small_case(kind, n):
     return res
 
 
+def precision_case(n, order):
+    """Profiler-sized run of the precision form: the --n-cell sphere with the
+    anisotropic tensor eps, one warm-up step, then one step inside an NVTX
+    range 'prec' (for ncu --nvtx-include "prec/"), timed with CUDA events,
+    with its kernel classes."""
+    import torch
+    import buffem
+    L = buffem.lib()
+    stream = torch.cuda.ExternalStream(L.bg_stream())
+    sc = Case(n, buffem.Material(kind=buffem.BG_MAT_CONST_TENSOR, tensor=eps_tensor()), order)
+    dB = torch.zeros((sc.nrhs, sc.N), dtype=torch.complex128, device="cuda")
+    st = np.zeros(3)
+    sc.step_precision(dB, st)
+    buffem.synchronize()
+    buffem.profile_begin()
+    torch.cuda.nvtx.range_push("prec")
+    t = timed(stream, lambda: sc.step_precision(dB, st), 1, 0, 1)
+    torch.cuda.nvtx.range_pop()
+    pm = buffem.profile_read()
+    buffem.profile_end()
+    return {"kind": "precision", "N": sc.N, "step_s": t, "refinement_sweeps": int(st[0]),
+            "kernel_ms": {k: round(v["ms"], 2) for k, v in pm.items() if v["launches"]},
+            "launches": {k: v["launches"] for k, v in pm.items() if v["launches"]}}
+
+
 def neq_flops(N):
     """FP64 flops of one frequency of the flux chain for one object: S^-1 G,
     S^-1 (V S^-1 G), LU of W, S^-1 R S^-1 (dense block), two N-column solves."""
@@ -875,12 +900,12 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the GetFields and buff-neq flux measurements")
     ap.add_argument("--lean", action="store_true",
                     help="headline learned steps only (no FP64 arm, e2e, secondary, CPU baseline): profiler runs")
-    ap.add_argument("--kernel", default=None, choices=["gemm", "cgemm", "fields", "neq"],
+    ap.add_argument("--kernel", default=None, choices=["gemm", "cgemm", "fields", "neq", "precision"],
                     help="one small case for profilers: gemm = the LU trailing-update GEMM on an M=N=K=--size "
                          "problem (complex128, DMMA); cgemm = the same on the complex64 tcgen05 GEMM of the "
-                         "precision form; "
-                         "problem; fields = two GetFields calls, 2048 far points on the --size-cell sphere; "
-                         "neq = two buff-neq flux frequencies on the --size-cell sphere")
+                         "precision form; fields = two GetFields calls, 2048 far points on the --size-cell "
+                         "sphere; neq = two buff-neq flux frequencies on the --size-cell sphere; precision = "
+                         "one precision-form step (complex64 LU + FP64 refinement) on the --n-cell sphere")
     ap.add_argument("--size", type=int, default=8192)
     ap.add_argument("--shape", default=None, help="M,N,K for --kernel cgemm (default: --size cubed)")
     args = ap.parse_args()
@@ -895,6 +920,9 @@ def main():
         return
     if args.kernel in ("fields", "neq"):
         print(json.dumps(small_case(args.kernel, args.size)), flush=True)
+        return
+    if args.kernel == "precision":
+        print(json.dumps(precision_case(args.n, args.order)), flush=True)
         return
     if args.lean:
         args.no_cpu_baseline = True
