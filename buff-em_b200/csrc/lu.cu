@@ -237,7 +237,7 @@ static int zgemm_sub(int M, int N, int K, const cdl *A, size_t lda, const cdl *B
 // the substitution.
 // =========================================================================
 #define TRS_WARPS 8
-#define TRS_CPW 8                         // columns per warp per CTA
+#define TRS_CPW 4                         // columns per warp per CTA
 #define TRS_COLS (TRS_WARPS * TRS_CPW)
 template <class C>
 __device__ __forceinline__ C cshfl(C v, int src) {
