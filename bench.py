@@ -691,6 +691,23 @@ def run_gpu(args, rank, world, local_rank):
         sec["precision_form_err_vs_fp64_lu"] = rel_err(dB, ref)
         sec["precision_form_gemm_tflops"] = pm["lu_gemm"]["flops"] / (pm["lu_gemm"]["ms"] / 1e3) / 1e12 if pm["lu_gemm"]["ms"] else None
         sec["precision_form_kernel_ms_per_step"] = {k: v["ms"] / 2 for k, v in pm.items() if v["launches"]}
+        # roofline of the precision form's LU: the TF32 trailing updates
+        # against the TF32 tensor rate (half the measured dense BF16 burst),
+        # and the factorisation's 8/3 N^3 flops over all its LU kernels
+        mp = measured_peaks().get("bf16_tflops")
+        lu_ms = sum(pm[c]["ms"] for c in ("lu_gemm", "lu_panel", "lu_laswp", "trsm_leaf")) / 2
+        lu_tf = 8.0 / 3.0 * float(sc.N) ** 3 / (lu_ms / 1e3) / 1e12 if lu_ms else None
+        gtf = sec["precision_form_gemm_tflops"]
+        sec["precision_form_roofline"] = {
+            "bound": "tensor", "kernel": "k_cgemm_tf32 (tcgen05 kind::tf32, complex64 trailing updates)",
+            "achieved": gtf, "peak": mp / 2 if mp else None, "unit": "TFLOP/s",
+            "frac": gtf / (mp / 2) if (mp and gtf) else None,
+            "algorithmic": "8 M N K real flops per complex64 GEMM call, summed over the factorisation, over the "
+                           "calls' CUDA-event time",
+            "peak_source": "half the measured dense BF16 burst of MEASURED_PEAKS.json (of measured)",
+            "lu_step": {"flops": 8.0 / 3.0 * float(sc.N) ** 3, "lu_kernels_ms": lu_ms, "achieved_tflops": lu_tf,
+                        "frac_of_tf32": lu_tf / (mp / 2) if (mp and lu_tf) else None,
+                        "note": "the panels, TRSM leaves and interchanges are latency-bound; the GEMMs are not"}}
         sec["fp64_kernel_ms_per_step"] = {k: v["ms"] / 2 for k, v in pf.items() if v["launches"]}
         st4 = np.zeros(4)
         t = timed(stream, lambda: sc.step_learned(dB, net, st4), 2, 1, world)

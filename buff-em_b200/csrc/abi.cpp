@@ -472,6 +472,13 @@ int bg_matrix_create(bg_geometry *g, int precision, bg_matrix **out) {
     set_error("cannot allocate %.2f GB matrix on the device: %s", esz * (double)g->N * g->N / 1e9, cudaGetErrorString(e));
     return BG_ERR_NOMEM;
   }
+  if (m->ld > (size_t)m->N) {
+    // the padding rows N .. ld-1 are zero for good: no kernel writes them, and
+    // the symmetric complex64 product copies one of them with an odd N
+    e = cudaMemset2DAsync((char *)m->d + esz * (size_t)m->N, esz * m->ld, 0, esz * (m->ld - (size_t)m->N), m->N,
+                          stream());
+    if (e != cudaSuccess) { cudaFree(m->d); delete m; set_error("cudaMemset2DAsync: %s", cudaGetErrorString(e)); return BG_ERR_CUDA; }
+  }
   e = cudaMalloc(&m->d_ipiv, sizeof(int) * (size_t)m->N);
   if (e != cudaSuccess) { cudaFree(m->d); delete m; set_error("cannot allocate pivots"); return BG_ERR_NOMEM; }
   *out = m;

@@ -134,15 +134,16 @@ __global__ void __launch_bounds__(GV_ROWS) k_gm_matvec_part_c64(int N, const flo
 // rows J (A_IJ^T x_I, which is A_JI x_I by symmetry), so every partial slot
 // of k_gm_matvec_sum is still written exactly once.  A warp owns 64 columns
 // of the tile and all 256 rows (8 per lane, two 8-byte complex entries per
-// 16-byte copy, four columns per step) and streams them through a 3-stage
-// cp.async pipeline in shared memory, so the copies of later steps are in
+// 16-byte read, four columns per step) and streams them into shared memory
+// with one bulk copy per column segment (2 KB, issued by one lane, counted on
+// an mbarrier per stage), two stages deep, so the next step's copies are in
 // flight while a step is computed; the transposed products of four columns
 // are reduce-scattered across the warp's lanes, the direct ones summed over
 // the four warps through shared memory.  FP32
 // accumulation within a tile, complex64 partials summed in FP64, as in
 // k_gm_matvec_part_c64.
-// Entries of rows >= N (the padding of the leading dimension) are never read:
-// their copies are zero-filled.
+// The last tile's segments are N's rows rounded up to an even count: the
+// padding rows of a complex64 matrix are zero from its allocation.
 // 16-byte asynchronous global-to-shared copy; src_bytes < 16 zero-fills the rest
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes) {
   unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -151,6 +152,41 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int K>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(K) : "memory"); }
+
+// Bulk copies of the symmetric product: one cp.async.bulk per column segment
+// (global -> this CTA's shared memory, completion counted in bytes on an
+// mbarrier), every wait bounded.  A wait that runs out sets g_mv_timeout,
+// which the solve reads back and reports.
+#define SY_SPIN (1u << 24)
+__device__ int g_mv_timeout;
+__device__ __forceinline__ unsigned sy_saddr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void sy_mbar_init(unsigned long long *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(sy_saddr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void sy_mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sy_saddr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool sy_mbar_wait(unsigned long long *bar, unsigned parity) {
+  const unsigned a = sy_saddr(bar);
+  for (unsigned it = 0; it < SY_SPIN; it++) {
+    unsigned done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+__device__ __forceinline__ void sy_bulk_g2s(void *dst, const void *src, unsigned bytes, unsigned long long *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   sy_saddr(dst)),
+               "l"(src), "r"(bytes), "r"(sy_saddr(bar))
+               : "memory");
+}
 
 #define SY_STAGES 2
 // shared memory: per warp SY_STAGES stages of 4 columns x 256 rows (as 4 x 128
@@ -171,6 +207,7 @@ __global__ void __launch_bounds__(128, 3) k_gm_matvec_sym_c64(int N, const float
   const int r0 = I * 256, c0 = J * 256;
   const int nr = min(256, N - r0), nc = min(256, N - c0);
   extern __shared__ __align__(16) unsigned char sym_smem[];
+  __shared__ __align__(8) unsigned long long sy_bar[4][SY_STAGES];            // per warp and stage
   float4 *stage = reinterpret_cast<float4 *>(sym_smem);                        // [4 warps][STAGES][4][128]
   float2 (*xr)[NR] = reinterpret_cast<float2 (*)[NR]>(sym_smem);              // in the stage buffers, until loaded
   float2 (*xc)[NR] = reinterpret_cast<float2 (*)[NR]>(stage + 4 * SY_STAGES * 4 * 128);
@@ -200,42 +237,45 @@ __global__ void __launch_bounds__(128, 3) k_gm_matvec_sym_c64(int N, const float
       Yi[q][j] = make_float2(y.y, y.y);
     }
   __syncthreads();   // x of the rows is in registers: the stage buffers are free
-  // this lane's rows 64 k + 2 lane (+1): bytes of the pair that exist
-  int nb[4];
-#pragma unroll
-  for (int k = 0; k < 4; k++) {
-    int p = 64 * k + 2 * lane;
-    nb[k] = p + 1 < nr ? 16 : (p < nr ? 8 : 0);
-  }
-  const float4 *base = A + (size_t)c0 * lda2 + (r0 >> 1) + lane;
+  // column segments of this tile: rows r0 .. r0 + nr rounded up to an even
+  // count (16-byte copies; the padding rows of a complex64 matrix are zero)
+  const float4 *colbase = A + (size_t)c0 * lda2 + (r0 >> 1);
+  const unsigned segbytes = (unsigned)((nr + 1) >> 1) * 16u;
   const int cbeg = 64 * w, cend = min(nc, 64 * w + 64);
   const int nsteps = cend > cbeg ? (cend - cbeg + 3) / 4 : 0;
   float4 *my = stage + (size_t)w * SY_STAGES * 4 * 128;
-  // each lane copies, and later reads, only its own rows: no warp barrier needed
+  unsigned long long *bar = sy_bar[w];
+  // The warp's stage buffers start at zero: rows past the copied segment and
+  // columns past the tile's last are never written, and enter the products
+  // only with zero factors (x of those rows and columns is zero).
+  for (int e = lane; e < SY_STAGES * 4 * 128; e += 32) my[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (lane == 0)
+    for (int q = 0; q < SY_STAGES; q++) sy_mbar_init(&bar[q], 1);
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // the zeros before any bulk copy
+  if (lane == 0) asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  __syncwarp();
+  // lane 0 issues step g's copies: one per column of the step
   auto issue = [&](int g) {
-    if (g < nsteps) {
+    if (g < nsteps && lane == 0) {
+      const int cb = cbeg + 4 * g, ncol = min(4, cend - cb);
       float4 *buf = my + (g % SY_STAGES) * 4 * 128;
-#pragma unroll
-      for (int u = 0; u < 4; u++) {
-        int c = cbeg + 4 * g + u;
-        bool okc = c < cend;
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-          int bytes = okc ? nb[k] : 0;
-          // nothing is read for bytes = 0; the address is then the matrix start
-          const float4 *src = bytes ? base + (size_t)c * lda2 + 32 * k : A;
-          cp_async16(buf + u * 128 + lane + 32 * k, src, bytes);
-        }
-      }
+      unsigned long long *b = &bar[g % SY_STAGES];
+      sy_mbar_expect_tx(b, (unsigned)ncol * segbytes);
+      for (int u = 0; u < ncol; u++) sy_bulk_g2s(buf + u * 128, colbase + (size_t)(cb + u) * lda2, segbytes, b);
     }
-    cp_async_commit();
   };
   const int hi = (lane >> 4) & 1, b3 = (lane >> 3) & 1;
-#pragma unroll
-  for (int g = 0; g < SY_STAGES - 1; g++) issue(g);
+  int fail = 0, waited = 0;
+  issue(0);
   for (int g = 0; g < nsteps; g++) {
-    issue(g + SY_STAGES - 1);
-    cp_async_wait<SY_STAGES - 1>();
+    __syncwarp();          // every lane has read the buffer that step g + 1 refills
+    issue(g + 1);
+    const bool ok = sy_mbar_wait(&bar[g % SY_STAGES], (unsigned)(g / SY_STAGES) & 1u);
+    waited = g + 1;
+    if (__any_sync(0xffffffffu, !ok)) {
+      fail = 1;
+      break;
+    }
     const float4 *buf = my + (g % SY_STAGES) * 4 * 128;
     const int c = cbeg + 4 * g;
     float t[4][2 * NR];
@@ -300,7 +340,13 @@ __global__ void __launch_bounds__(128, 3) k_gm_matvec_sym_c64(int N, const float
       }
     }
   }
-  cp_async_wait<0>();
+  if (fail) {
+    if (lane == 0) atomicExch(&g_mv_timeout, 1);
+    // copies still in flight land before the buffers are reused (bounded)
+    // (the step whose wait ran out and the one issued after it)
+    for (int g = waited - 1; g <= min(nsteps - 1, waited); g++)
+      sy_mbar_wait(&bar[g % SY_STAGES], (unsigned)(g / SY_STAGES) & 1u);
+  }
   __syncthreads();          // every warp is done with its stage buffers
 #pragma unroll
   for (int k = 0; k < 4; k++)
@@ -703,6 +749,8 @@ int gmres_solve(bg_matrix *A, const bg_precond *P, void *dB, int ldb, int nrhs, 
     res_cap = ncs;
   }
   int st = BG_OK;
+  static const int zero = 0;
+  BG_CUDA_TRY(cudaMemcpyToSymbolAsync(g_mv_timeout, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, stream()));
   // X = 0
   BG_CUDA_TRY(cudaMemsetAsync(X, 0, sizeof(z2) * (size_t)N * nrhs, stream()));
   // B contiguous copy in W for norms
@@ -869,6 +917,14 @@ int gmres_solve(bg_matrix *A, const bg_precond *P, void *dB, int ldb, int nrhs, 
     cudaError_t e = cudaMemcpy2DAsync(dB, sizeof(z2) * ldb, X, sizeof(z2) * N, sizeof(z2) * N, nrhs,
                                       cudaMemcpyDeviceToDevice, stream());
     if (e != cudaSuccess) { set_error("gmres: %s", cudaGetErrorString(e)); st = BG_ERR_CUDA; }
+  }
+  if (!st) {
+    // a bounded wait of the symmetric product that ran out (none expected)
+    int to = 0;
+    cudaError_t e = cudaMemcpyFromSymbolAsync(&to, g_mv_timeout, sizeof(int), 0, cudaMemcpyDeviceToHost, stream());
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream());
+    if (e != cudaSuccess) { set_error("gmres: %s", cudaGetErrorString(e)); st = BG_ERR_CUDA; }
+    else if (to) { set_error("gmres: a bulk copy of the matrix-vector product timed out"); st = BG_ERR_CUDA; }
   }
   cudaFreeAsync(w, stream());
   if (stats) { stats[0] = total; stats[1] = relres; stats[2] = first; }
