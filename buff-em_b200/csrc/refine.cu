@@ -62,7 +62,26 @@ __global__ void __launch_bounds__(MV_ROWS) k_matvec_part(int N, const c2 *A, siz
   if (row >= N) return;
   double ar[MV_MAXRHS] = {0, 0, 0, 0}, ai[MV_MAXRHS] = {0, 0, 0, 0};
   const c2 *ap = A + (size_t)c0 * lda + row;
-  for (int c = 0; c < nc; c++) {
+  int c = 0;
+  // eight columns' loads in flight per thread, then their products in order
+  for (; c + 8 <= nc; c += 8) {
+    c2 a[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      double2 t = __ldcs(reinterpret_cast<const double2 *>(ap + (size_t)(c + u) * lda));
+      a[u] = c2{t.x, t.y};
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++)
+#pragma unroll
+      for (int j = 0; j < MV_MAXRHS; j++)
+        if (j < nrhs) {
+          c2 x = xs[c + u][j];
+          ar[j] += a[u].r * x.r - a[u].i * x.i;
+          ai[j] += a[u].r * x.i + a[u].i * x.r;
+        }
+  }
+  for (; c < nc; c++) {
     c2 a = ap[(size_t)c * lda];
 #pragma unroll
     for (int j = 0; j < MV_MAXRHS; j++) {
