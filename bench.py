@@ -9,7 +9,7 @@ complex64 copy), eps = 6 + 0.5i, omega = 1, three plane-wave right-hand sides
 One step = one frequency.
   value (mixed + learned): assemble the complex128 matrix, copy it to
     complex64, predict the near-field approximate inverse with the graph
-    network (shipped weights), assemble the RHS, solve by GMRES(50) on the
+    network (shipped weights), assemble the RHS, solve by GMRES(80) on the
     complex64 copy with FP64 refinement against the complex128 matrix to a
     1e-10 relative residual, LU fallback if 1000 Krylov steps do not reach it.
   fp64_path: assemble, FP64 LU (DMMA tensor cores), FP64 solve -- the plain
@@ -71,7 +71,7 @@ TENSOR = [[4, 0.5, 0], [0.5, 6, 0], [0, 0, 9]]
 EPS_LEARNED = 6 + 0.5j
 WAVES = [([1, 0, 0], [0, 0, 1]), ([0, 1, 0], [0, 0, 1]), ([0, 0, 1], [1, 0, 0])]
 OMEGA = 1.0
-GMRES = dict(tol=1e-10, restart=50, maxit=1000, inner_tol=1e-5)
+GMRES = dict(tol=1e-10, restart=80, maxit=1000, inner_tol=1e-5)
 # ncu --set full capture of k_gm_matvec_sym_c64 (one launch, N = 5,760,
 # profiles/gmres_matvec_c64_n5760.md): dram__bytes_read.sum + dram__bytes_write.sum
 MATVEC_NCU_N, MATVEC_NCU_BYTES = 5760, 138.911232e6 + 5.009664e6
@@ -954,7 +954,7 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     N_head = 12 * args.n ** 3 - 6 * args.n ** 2
     config = {"workload": f"learned form: sphere {args.n}^3 cells x 6 tets (N={N_head}), eps={EPS_LEARNED}, "
-                          f"omega={OMEGA}, 3 plane-wave RHS; mixed-precision GMRES(50) + graph-network "
+                          f"omega={OMEGA}, 3 plane-wave RHS; mixed-precision GMRES(80) + graph-network "
                           f"near-field preconditioner, LU fallback; vs plain FP64 assemble+LU+solve",
               "N": N_head, "n_cells": args.n, "omega": OMEGA, "rhs": 3, "singular_order": args.order,
               "gmres": GMRES, "parallelism": f"replicas x{world} (independent frequencies)",

@@ -656,7 +656,7 @@ def GMRESLastInfo():
             "switched_to_jacobi": bool(out[3]), "stopped_early": bool(out[4]), "longest_cycle": int(out[5])}
 
 
-def SolveLearned(M, F, B, P=None, tol=1e-10, restart=50, maxit=1000, inner_tol=1e-5):
+def SolveLearned(M, F, B, P=None, tol=1e-10, restart=80, maxit=1000, inner_tol=1e-5):
     """Mixed-precision GMRES with preconditioner P and the LU fallback (F
     holds LU factors afterwards if the fallback ran); returns (X, stats) with
     stats = (Krylov steps, final relative residual, sweeps, fallback used)."""
