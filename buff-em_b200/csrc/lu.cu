@@ -558,6 +558,141 @@ __device__ __forceinline__ cfl ldcg_c<cfl>(const cfl *p) {
   return cfl{v.x, v.y};
 }
 
+// The same panel on one thread-block cluster (up to 16 CTAs, the slices in
+// their shared memory): when the panel fits, the per-column grid barrier
+// becomes a cluster barrier and the candidate exchange reads the other CTAs'
+// shared memory directly (distributed shared memory) instead of global
+// memory.  Pivot choice, interchanges and arithmetic are those of k_panel.
+// Candidate slots are double-buffered by column parity: a CTA writing the
+// slots of column j + 2 has passed the barrier of column j + 1, which every
+// CTA reaches only after reading column j's slots.  The last barrier keeps
+// every CTA's shared memory alive until all remote reads are done.
+#define PCL_THREADS 512     // threads per CTA of the cluster panel (about one row each)
+template <class C>
+__global__ void __launch_bounds__(PCL_THREADS) k_panel_cl(PanelArgs<C> P) {
+  typedef typename CxT<C>::R R;
+  cg::cluster_group cl = cg::this_cluster();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *S = (C *)smem_raw;                     // [w][rows_per]: column c at S + c * rows_per
+  __shared__ double rv[PCL_THREADS / 32];
+  __shared__ int ri[PCL_THREADS / 32];
+  __shared__ double cval[2];                // this CTA's candidate, per column parity
+  __shared__ int cidx[2];
+  __shared__ C crow[2][32];                 // its candidate row
+  __shared__ C jrow[2][32];                 // row k0 + j before the swap (CTA holding it)
+  __shared__ int s_piv;
+  __shared__ C prow[32], jr[32];
+  const int w = P.w, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int rank = (int)cl.block_rank(), G = (int)cl.num_blocks();
+  const int r0 = P.k0 + rank * P.rows_per;
+  const int r1 = min(P.Nr, r0 + P.rows_per);
+  const int nr = max(0, r1 - r0), lds = P.rows_per;
+  for (int e0 = 0; e0 < nr * w; e0 += 8 * PCL_THREADS) {
+    C v[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int e = e0 + u * PCL_THREADS + tid;
+      v[u] = e < nr * w ? P.A[(size_t)(P.k0 + e / nr) * P.ld + r0 + e % nr] : C{0, 0};
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int e = e0 + u * PCL_THREADS + tid;
+      if (e < nr * w) S[(e / nr) * lds + e % nr] = v[u];
+    }
+  }
+  __syncthreads();
+  for (int j = 0; j < w; j++) {
+    const int gj = P.k0 + j, buf = j & 1;
+    // 1. local pivot candidate (i[cz]amax: max |re|+|im|, first index on ties)
+    double bv = -1.0;
+    int bi = 0x7fffffff;
+    for (int r = tid; r < nr; r += PCL_THREADS) {
+      int gr = r0 + r;
+      if (gr < gj) continue;
+      C v = S[j * lds + r];
+      double a = (double)(fabs(v.r) + fabs(v.i));
+      if (better(a, gr, bv, bi)) { bv = a; bi = gr; }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+      int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (better(ov, oi, bv, bi)) { bv = ov; bi = oi; }
+    }
+    if (lane == 0) { rv[wid] = bv; ri[wid] = bi; }
+    __syncthreads();
+    if (tid == 0) {
+      for (int k = 1; k < PCL_THREADS / 32; k++)
+        if (better(rv[k], ri[k], rv[0], ri[0])) { rv[0] = rv[k]; ri[0] = ri[k]; }
+      cval[buf] = rv[0];
+      cidx[buf] = ri[0];
+    }
+    __syncthreads();
+    const int myc = ri[0];
+    if (rv[0] >= 0.0 && tid < w) crow[buf][tid] = S[tid * lds + myc - r0];
+    if (gj >= r0 && gj < r1 && tid < w) jrow[buf][tid] = S[tid * lds + gj - r0];
+    cl.sync();   // every CTA's candidate is visible in the cluster
+    // 2. global pivot: lane k reads CTA k's candidate
+    if (tid < 32) {
+      double v = -1.0;
+      int i = 0x7fffffff, b = 0;
+      if (lane < G) {
+        v = *cl.map_shared_rank(&cval[buf], lane);
+        i = *cl.map_shared_rank(&cidx[buf], lane);
+        b = lane;
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        double ov = __shfl_xor_sync(0xffffffffu, v, o);
+        int oi = __shfl_xor_sync(0xffffffffu, i, o);
+        int ob = __shfl_xor_sync(0xffffffffu, b, o);
+        if (better(ov, oi, v, i)) { v = ov; i = oi; b = ob; }
+      }
+      const int owner = (gj - P.k0) / P.rows_per;   // CTA holding row gj
+      if (lane < w) {
+        prow[lane] = *cl.map_shared_rank(&crow[buf][lane], b);
+        jr[lane] = *cl.map_shared_rank(&jrow[buf][lane], owner);
+      }
+      if (lane == 0) s_piv = i;
+    }
+    __syncthreads();
+    const int piv = s_piv;
+    if (rank == 0 && tid == 0) P.ipiv[gj] = piv + 1;
+    // 3. swap rows gj and piv inside the panel
+    if (piv != gj) {
+      if (piv >= r0 && piv < r1 && tid < w) S[tid * lds + piv - r0] = jr[tid];
+      if (gj >= r0 && gj < r1 && tid < w) S[tid * lds + gj - r0] = prow[tid];
+    }
+    __syncthreads();
+    // 4. scale the column below the pivot and update the rest of the panel
+    C p = prow[j];
+    R d = p.r * p.r + p.i * p.i;
+    if (d == (R)0) {
+      if (rank == 0 && tid == 0) atomicCAS(P.info, 0, gj + 1);
+    } else {
+      C inv{p.r / d, -p.i / d};
+      int ncol = w - j - 1;
+      for (int r = tid; r < nr; r += PCL_THREADS) {
+        int gr = r0 + r;
+        if (gr <= gj) continue;
+        C v = S[j * lds + r];
+        C l{v.r * inv.r - v.i * inv.i, v.r * inv.i + v.i * inv.r};
+        S[j * lds + r] = l;
+        for (int c = 1; c <= ncol; c++) {
+          C u = prow[j + c];
+          C &t = S[(j + c) * lds + r];
+          t.r -= l.r * u.r - l.i * u.i;
+          t.i -= l.r * u.i + l.i * u.r;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  for (int e = tid; e < nr * w; e += PCL_THREADS) {
+    const int r = e % nr, c = e / nr;
+    P.A[(size_t)(P.k0 + c) * P.ld + r0 + r] = S[c * lds + r];
+  }
+  cl.sync();   // no CTA leaves while another may still read its shared memory
+}
+
 // apply the interchanges ipiv[k0..k0+w) to columns [c0, c1) of A
 template <class C>
 __global__ void k_laswp(C *A, size_t ld, const int *ipiv, int k0, int w, int c0, int c1, int skip0, int skip1) {
@@ -583,10 +718,85 @@ struct LUWork {
 
 static int panel_grid = 0, panel_smem_max = 0, panel_rows_target = 32;
 
+// cluster size of k_panel_cl<C> on this device (0: no cluster path), found
+// once: the largest of 16 and 8 that the occupancy query allows with a full
+// slice of shared memory per CTA
+static int panel_cl_smem_max = 0;
+template <class C>
+static int panel_cluster_size() {
+  static int cs = -1;
+  if (cs >= 0) return cs;
+  cs = 0;
+  int dev = 0, smemopt = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&smemopt, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+    return cs;
+  panel_cl_smem_max = smemopt - 6 * 1024;   // room for the kernel's static shared memory
+  if (cudaFuncSetAttribute(k_panel_cl<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, panel_cl_smem_max) != cudaSuccess ||
+      cudaFuncSetAttribute(k_panel_cl<C>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+    cudaGetLastError();
+    return cs;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(16);
+  cfg.blockDim = dim3(PCL_THREADS);
+  cfg.dynamicSmemBytes = panel_cl_smem_max;
+  int best = 0;
+  if (cudaOccupancyMaxPotentialClusterSize(&best, (void *)k_panel_cl<C>, &cfg) != cudaSuccess) best = 0;
+  int want = best >= 16 ? 16 : (best >= 8 ? 8 : 0);
+  if (want) {
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = want;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(want);
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int nclusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, (void *)k_panel_cl<C>, &cfg) != cudaSuccess || nclusters < 1) want = 0;
+  }
+  cudaGetLastError();
+  cs = want;
+  return cs;
+}
+
 template <class C>
 static int panel_leaf(bg_matrix *m, const LUWork &W, int k0, int w) {
   int N = m->N;
   int Mp = N - k0;
+  // the whole panel in one cluster's shared memory: cluster barriers and
+  // distributed shared memory instead of a grid barrier per column
+  const int CS = panel_cluster_size<C>();
+  if (CS) {
+    const int G = std::min(CS, std::max(1, (Mp + panel_rows_target - 1) / panel_rows_target));
+    const int rows = (Mp + G - 1) / G;
+    const size_t smem = (size_t)rows * w * sizeof(C);
+    if (smem <= (size_t)panel_cl_smem_max) {
+      PanelArgs<C> P{(C *)m->d, m->ld, N, k0, w, rows, m->d_ipiv, W.info, W.cval, W.cidx, (C *)W.crow, (C *)W.jrow};
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(G);
+      cfg.blockDim = dim3(PCL_THREADS);
+      cfg.dynamicSmemBytes = smem;
+      cfg.stream = stream();
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = G;
+      at[0].val.clusterDim.y = 1;
+      at[0].val.clusterDim.z = 1;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      prof_start(PROF_PANEL);
+      BG_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_panel_cl<C>, P));
+      BG_LAUNCHED();
+      prof_stop(PROF_PANEL, 8.0 * Mp * (double)w * w / 2);
+      prof_start(PROF_LASWP);
+      k_laswp<C><<<(N + 255) / 256, 256, 0, stream()>>>((C *)m->d, m->ld, m->d_ipiv, k0, w, 0, N, k0, k0 + w);
+      BG_LAUNCHED();
+      prof_stop(PROF_LASWP, 0.0);
+      return BG_OK;
+    }
+  }
   int G = std::min(panel_grid, std::max(1, (Mp + panel_rows_target - 1) / panel_rows_target));
   while (G < panel_grid && (size_t)((Mp + G - 1) / G) * w * sizeof(C) > (size_t)panel_smem_max) G++;
   int rows = (Mp + G - 1) / G;
