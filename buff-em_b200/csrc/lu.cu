@@ -772,7 +772,9 @@ static int panel_leaf(bg_matrix *m, const LUWork &W, int k0, int w) {
     const int G = std::min(CS, std::max(1, (Mp + panel_rows_target - 1) / panel_rows_target));
     const int rows = (Mp + G - 1) / G;
     const size_t smem = (size_t)rows * w * sizeof(C);
-    if (smem <= (size_t)panel_cl_smem_max) {
+    // past ~512 rows per CTA the row updates of 16 CTAs cost more than the
+    // grid barrier they save (148 CTAs share them in the grid form)
+    if (rows <= 512 && smem <= (size_t)panel_cl_smem_max) {
       PanelArgs<C> P{(C *)m->d, m->ld, N, k0, w, rows, m->d_ipiv, W.info, W.cval, W.cidx, (C *)W.crow, (C *)W.jrow};
       cudaLaunchConfig_t cfg = {};
       cfg.gridDim = dim3(G);
