@@ -956,6 +956,7 @@ __global__ void __launch_bounds__(128) k_trsv(int N, const C *A, size_t ld, C *X
   C(*part)[TV_MAXRHS] = (C(*)[TV_MAXRHS])(smem_raw + TV_B * (TV_B + 1) * sizeof(C));   // part[row][rhs]
   C(*xs)[TV_MAXRHS] = part + TV_B;                                                    // solved block x[col][rhs]
   __shared__ int s_blk, s_abort;
+  __shared__ C dinv[TV_B];   // upper sweep: 1 / u_ii of the diagonal block
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nb = (N + TV_B - 1) / TV_B;
   if (tid == 0) { s_blk = atomicAdd(ticket, 1); s_abort = 0; }
@@ -982,6 +983,18 @@ __global__ void __launch_bounds__(128) k_trsv(int N, const C *A, size_t ld, C *X
     for (int u = 0; u < 8; u++) {
       const int e = e0 + u * 128 + tid;
       if (e < rows * rows) D[e % rows][e / rows] = v[u];
+    }
+  }
+  if (UPPER) {
+    // reciprocals of the diagonal, conj(u) / |u|^2, computed before this
+    // block waits for anything (the solve below multiplies instead of
+    // dividing on its sequential path); barriers of the loop or of the
+    // combine below order them before their use
+    if (tid < rows) {
+      const int e = tid * rows + tid;
+      const C u = A[(size_t)(r0 + e / rows) * ld + r0 + e % rows];
+      const R d = u.r * u.r + u.i * u.i;
+      dinv[tid] = C{u.r / d, -u.i / d};
     }
   }
   C acc[TV_MAXRHS];
@@ -1073,9 +1086,8 @@ __global__ void __launch_bounds__(128) k_trsv(int N, const C *A, size_t ld, C *X
     } else {
       for (int i = rows - 1; i >= 0; i--) {
         C v = cshfl(i < 32 ? b0 : b1, i & 31);
-        C u = D[i][i];
-        R d = u.r * u.r + u.i * u.i;
-        C x{(v.r * u.r + v.i * u.i) / d, (v.i * u.r - v.r * u.i) / d};
+        const C iu = dinv[i];
+        C x{v.r * iu.r - v.i * iu.i, v.r * iu.i + v.i * iu.r};
         if (q0 == i) b0 = x;
         if (q1 == i) b1 = x;
         if (q0 < i) { C t = D[q0][i]; b0.r -= t.r * x.r - t.i * x.i; b0.i -= t.r * x.i + t.i * x.r; }
