@@ -400,7 +400,7 @@ def run_batching(nomega=64):
     for G, _ in geo:
         G.precompute()
     buffem.synchronize()
-    pabs, st = buffem.BatchSweep([g for g, _ in geo], omegas, wave, max_streams=4)
+    pabs, st = buffem.BatchSweep([g for g, _ in geo], omegas, wave, max_streams=8)
     seq = []
     for G, meta in geo:
         ts = []

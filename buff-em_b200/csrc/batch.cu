@@ -18,7 +18,8 @@
 //  * an online autotuner picks, per size class (N rounded up to 1024), the
 //    LU panel slice height (rows per CTA of the cooperative panel kernel:
 //    16, 32 or 64), the CTA tile of the complex128 tensor-core GEMM (64 x 64,
-//    128 x 64 or 64 x 128) and the number of concurrent slots (1, 2 or 4) by
+//    128 x 64 or 64 x 128) and the number of concurrent slots (1, 2, 4, ... up
+//    to the caller's maximum) by
 //    timing the sweep's own first jobs (their results are kept), and
 //    remembers the choice for later geometries of the same class.
 #include <cuda_runtime.h>
