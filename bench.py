@@ -273,8 +273,7 @@ class Case:
     def step_precision(self, dB, stats, tol=1e-12, w=OMEGA):
         b = self.buffem
         self.ensure_c64()
-        b._check(self.L.bg_assemble(self.G.h, w, 0.0, self.M.h))
-        b._check(self.L.bg_matrix_convert(self.M.h, self.F.h))
+        b._check(self.L.bg_assemble_with_copy(self.G.h, w, 0.0, self.M.h, self.F.h))
         b._check(self.L.bg_lu_factor(self.F.h))
         self.rhs_device(dB, w)
         b._check(self.L.bg_lu_solve_refined_device(self.M.h, self.F.h, b.C.c_void_p(dB.data_ptr()), self.N,
@@ -283,8 +282,7 @@ class Case:
     def step_learned(self, dB, net, stats, w=OMEGA, jacobi=False):
         b = self.buffem
         self.ensure_c64()
-        b._check(self.L.bg_assemble(self.G.h, w, 0.0, self.M.h))
-        b._check(self.L.bg_matrix_convert(self.M.h, self.F.h))
+        b._check(self.L.bg_assemble_with_copy(self.G.h, w, 0.0, self.M.h, self.F.h))
         P = b.Preconditioner.jacobi(self.M) if jacobi else b.Preconditioner.learned(self.G, self.M, w, net)
         self.rhs_device(dB, w)
         b._check(self.L.bg_gmres_solve_lu_fallback_device(
@@ -296,8 +294,7 @@ class Case:
         """Same work through host buffers: RHS to host, solve with host in/out."""
         b = self.buffem
         self.ensure_c64()
-        b._check(self.L.bg_assemble(self.G.h, OMEGA, 0.0, self.M.h))
-        b._check(self.L.bg_matrix_convert(self.M.h, self.F.h))
+        b._check(self.L.bg_assemble_with_copy(self.G.h, OMEGA, 0.0, self.M.h, self.F.h))
         P = b.Preconditioner.learned(self.G, self.M, OMEGA, net)
         for i in range(self.nrhs):
             b._check(self.L.bg_rhs_planewave(self.G.h, OMEGA, 0.0, b._ptr(self.E0s[i]), b._ptr(self.nhs[i]),
@@ -600,25 +597,23 @@ def run_gpu(args, rank, world, local_rank):
     learned = {"steps_per_frequency": int(stats[0]), "final_rel_residual": float(stats[1]),
                "refinement_sweeps": int(stats[2]), "lu_fallback": bool(stats[3]), "gmres": buffem.GMRESLastInfo()}
     # phase breakdown of one more (untimed) step, events on the library stream
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
     ev[0].record(stream)
-    buffem._check(L.bg_assemble(case.G.h, OMEGA, 0.0, case.M.h))
+    buffem._check(L.bg_assemble_with_copy(case.G.h, OMEGA, 0.0, case.M.h, case.F.h))   # + complex64 copy
     ev[1].record(stream)
-    buffem._check(L.bg_matrix_convert(case.M.h, case.F.h))
-    ev[2].record(stream)
     P = buffem.Preconditioner.learned(case.G, case.M, OMEGA, net)
-    ev[3].record(stream)
+    ev[2].record(stream)
     case.rhs_device(dB)
-    ev[4].record(stream)
+    ev[3].record(stream)
     buffem._check(L.bg_gmres_solve_lu_fallback_device(case.M.h, case.F.h, P.h, buffem.C.c_void_p(dB.data_ptr()),
                                                       N, case.nrhs, GMRES["tol"], GMRES["restart"], GMRES["maxit"],
                                                       GMRES["inner_tol"], buffem._ptr(stats)))
-    ev[5].record(stream)
+    ev[4].record(stream)
     buffem.synchronize()
     rho_smax = P.bound()
     del P
     learned["phases_s"] = {k: ev[i].elapsed_time(ev[i + 1]) / 1e3 for i, k in
-                           enumerate(("assemble", "convert_c64", "gnn_precond", "rhs", "gmres_solve"))}
+                           enumerate(("assemble_with_c64_copy", "gnn_precond", "rhs", "gmres_solve"))}
     learned["precond_bound"] = {"rho_K1": rho_smax[0], "smax": rho_smax[1]}
     if x_fp64 is not None:
         learned["err_vs_fp64_lu"] = rel_err(dB, x_fp64)
@@ -626,8 +621,7 @@ def run_gpu(args, rank, world, local_rank):
     P = buffem.Preconditioner.jacobi(case.M)
     js = np.zeros(4)
     case.rhs_device(dB)
-    buffem._check(L.bg_assemble(case.G.h, OMEGA, 0.0, case.M.h))
-    buffem._check(L.bg_matrix_convert(case.M.h, case.F.h))
+    buffem._check(L.bg_assemble_with_copy(case.G.h, OMEGA, 0.0, case.M.h, case.F.h))
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     buffem._check(L.bg_gmres_solve_lu_fallback_device(case.M.h, case.F.h, P.h, buffem.C.c_void_p(dB.data_ptr()),

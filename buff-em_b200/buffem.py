@@ -73,7 +73,8 @@ EXPORTS = [
     "bg_trans_file_count", "bg_trans_file_tag", "bg_geometry_create_transformed", "bg_geometry_material_tensor",
     "bg_geometry_precompute", "bg_geometry_set_singular_order", "bg_geometry_near_data",
     "bg_geometry_set_singular_refine", "bg_geometry_singular_stats", "bg_geometry_singular_moments",
-    "bg_matrix_create", "bg_matrix_destroy", "bg_assemble", "bg_matrix_download", "bg_matrix_upload",
+    "bg_matrix_create", "bg_matrix_destroy", "bg_assemble", "bg_assemble_with_copy", "bg_matrix_download",
+    "bg_matrix_upload",
     "bg_matrix_get_rows",
     "bg_matrix_device_ptr", "bg_lu_factor", "bg_lu_pivots", "bg_lu_solve", "bg_lu_solve_device",
     "bg_rhs_planewave", "bg_rhs_planewave_device", "bg_pft", "bg_kernel_launch_count",
@@ -123,6 +124,7 @@ def lib():
         L.bg_matrix_destroy.argtypes = [P]
         L.bg_matrix_destroy.restype = None
         L.bg_assemble.argtypes = [P, D, D, P]
+        L.bg_assemble_with_copy.argtypes = [P, D, D, P, P]
         L.bg_matrix_download.argtypes = [P, VP]
         L.bg_matrix_upload.argtypes = [P, VP]
         L.bg_matrix_get_rows.argtypes = [P, I, VP, VP]
@@ -429,6 +431,18 @@ class SWGGeometry:
         Omega = complex(Omega)
         _check(lib().bg_assemble(self.h, Omega.real, Omega.imag, M.h))
         return M
+
+    def AssembleVIEMatrixWithCopy(self, Omega, M=None, F=None):
+        """AssembleVIEMatrix plus its complex64 copy written by the same
+        kernels (the matrix the mixed-precision solvers run on); returns
+        (M, F)."""
+        if M is None:
+            M = self.AllocateVIEMatrix()
+        if F is None:
+            F = self.AllocateVIEMatrix(BG_C64)
+        Omega = complex(Omega)
+        _check(lib().bg_assemble_with_copy(self.h, Omega.real, Omega.imag, M.h, F.h))
+        return M, F
 
     def AllocateRHSVector(self):
         return np.zeros(self.TotalBFs, dtype=np.complex128)

@@ -511,6 +511,33 @@ int bg_assemble(bg_geometry *g, double wr, double wi, bg_matrix *m) {
   return st;
 }
 
+int bg_assemble_with_copy(bg_geometry *g, double wr, double wi, bg_matrix *m, bg_matrix *f) {
+  if (!g || !m || !f) { set_error("bg_assemble_with_copy: null argument"); return BG_ERR_ARG; }
+  if (m->N != g->N || f->N != g->N) {
+    set_error("wrong-size matrix passed to bg_assemble_with_copy (%d, %d != %d)", m->N, f->N, g->N);
+    return BG_ERR_ARG;
+  }
+  if (m->precision != BG_C128 || f->precision != BG_C64) {
+    set_error("bg_assemble_with_copy: a complex128 matrix and a complex64 copy are required");
+    return BG_ERR_ARG;
+  }
+  if (wr == 0.0 && wi == 0.0) { set_error("bg_assemble_with_copy: omega must be nonzero"); return BG_ERR_ARG; }
+  int st = bg_geometry_precompute(g);
+  if (st) return st;
+  m->factored = false;
+  f->factored = false;
+  prof_start(PROF_ASM_FAR);
+  st = assemble_far(g, wr, wi, m->d, m->ld, nullptr, f->d, f->ld);
+  prof_stop(PROF_ASM_FAR, 64.0 * g->N * (double)g->N);
+  prof_start(PROF_ASM_NEAR);
+  if (!st) st = assemble_near(g, wr, wi, m->d, m->ld, nullptr, f->d, f->ld);
+  if (!st) st = assemble_gram(g, wr, wi, m->d, m->ld, nullptr, f->d, f->ld);
+  prof_stop(PROF_ASM_NEAR, 0.0);
+  m->symmetric = !st;
+  f->symmetric = !st;
+  return st;
+}
+
 int bg_matrix_download(const bg_matrix *m, void *host) {
   if (!m || !host) { set_error("bg_matrix_download: bad arguments"); return BG_ERR_ARG; }
   size_t esz = m->precision == BG_C128 ? 16 : 8;

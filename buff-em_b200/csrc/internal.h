@@ -260,9 +260,14 @@ int build_near_lists(bg_geometry *g);
 int precompute_near(bg_geometry *g);
 int singular_precompute(bg_geometry *g);
 // fq (optional, device {Re w, Im w}): omega read on the device instead of wr, wi
-int assemble_far(bg_geometry *g, double wr, double wi, void *M, size_t ld, const double *fq = nullptr);
-int assemble_near(bg_geometry *g, double wr, double wi, void *M, size_t ld, const double *fq = nullptr);
-int assemble_gram(bg_geometry *g, double wr, double wi, void *M, size_t ld, const double *fq = nullptr);
+// F (optional): a complex64 matrix (leading dimension ldf) that receives the
+// complex64 value of every entry the kernel leaves in M
+int assemble_far(bg_geometry *g, double wr, double wi, void *M, size_t ld, const double *fq = nullptr,
+                 void *F = nullptr, size_t ldf = 0);
+int assemble_near(bg_geometry *g, double wr, double wi, void *M, size_t ld, const double *fq = nullptr,
+                  void *F = nullptr, size_t ldf = 0);
+int assemble_gram(bg_geometry *g, double wr, double wi, void *M, size_t ld, const double *fq = nullptr,
+                  void *F = nullptr, size_t ldf = 0);
 // Frequency-dependent materials: eps(Omega) of every object with a MATERIAL
 // section into its host bg_material and, once uploaded, into the device copy
 // (a no-op for geometries without such materials).

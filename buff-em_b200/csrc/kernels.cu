@@ -469,7 +469,8 @@ __device__ void far_stage_tet_info(int t, const double (*P)[4][3], double (*o)[3
 // per tetrahedron pair (launches that read omega from device memory, whose
 // frequency the host does not know when it launches them).
 template <int MODE>
-__global__ void __launch_bounds__(FTHR, 2) k_far(DevGeom g, cd k, cd invk2, cd *M, size_t ld, const double *fq) {
+__global__ void __launch_bounds__(FTHR, 2) k_far(DevGeom g, cd k, cd invk2, cd *M, size_t ld, const double *fq,
+                                                  float2 *F, size_t ldf) {
   if (fq) {
     k = cd{fq[0], fq[1]};
     invk2 = dev_invk2(fq[0], fq[1]);
@@ -574,10 +575,15 @@ __global__ void __launch_bounds__(FTHR, 2) k_far(DevGeom g, cd k, cd invk2, cd *
       cd v = cadd(cadd(cadd(sl[0], sl[1]), sl[2]), sl[3]);
       M[(size_t)a + (size_t)b * ld] = v;
       if (a != b) M[(size_t)b + (size_t)a * ld] = v;
+      if (F) {   // the complex64 copy, as k_c128_to_c64 would convert it
+        const float2 f = make_float2((float)v.r, (float)v.i);
+        F[(size_t)a + (size_t)b * ldf] = f;
+        if (a != b) F[(size_t)b + (size_t)a * ldf] = f;
+      }
     }
 }
 
-int assemble_far(bg_geometry *g, double wr, double wi, void *M, size_t ld, const double *fq) {
+int assemble_far(bg_geometry *g, double wr, double wi, void *M, size_t ld, const double *fq, void *F, size_t ldf) {
   int st = init_tables();
   if (st) return st;
   cd k{wr, wi};
@@ -600,10 +606,10 @@ int assemble_far(bg_geometry *g, double wr, double wi, void *M, size_t ld, const
   const int mode = fq ? 3 : (wi != 0.0 ? 0 : (span <= 0.25 ? 2 : (span <= 1.0 ? 1 : 0)));
   const size_t sm = sizeof(FarSmem);
   switch (mode) {
-    case 0: k_far<0><<<grid, FTHR, sm, stream()>>>(g->dev, k, invk2, (cd *)M, ld, fq); break;
-    case 1: k_far<1><<<grid, FTHR, sm, stream()>>>(g->dev, k, invk2, (cd *)M, ld, fq); break;
-    case 2: k_far<2><<<grid, FTHR, sm, stream()>>>(g->dev, k, invk2, (cd *)M, ld, fq); break;
-    default: k_far<3><<<grid, FTHR, sm, stream()>>>(g->dev, k, invk2, (cd *)M, ld, fq); break;
+    case 0: k_far<0><<<grid, FTHR, sm, stream()>>>(g->dev, k, invk2, (cd *)M, ld, fq, (float2 *)F, ldf); break;
+    case 1: k_far<1><<<grid, FTHR, sm, stream()>>>(g->dev, k, invk2, (cd *)M, ld, fq, (float2 *)F, ldf); break;
+    case 2: k_far<2><<<grid, FTHR, sm, stream()>>>(g->dev, k, invk2, (cd *)M, ld, fq, (float2 *)F, ldf); break;
+    default: k_far<3><<<grid, FTHR, sm, stream()>>>(g->dev, k, invk2, (cd *)M, ld, fq, (float2 *)F, ldf); break;
   }
   BG_LAUNCHED();
   return BG_OK;
@@ -745,7 +751,8 @@ int precompute_near(bg_geometry *g) {
 //   G = BFBFInt[(e^{ikr}-1-ikr-(ikr)^2/2)/4 pi r] + (F0-F1/k^2) + ik(F2-F3/k^2)
 //       + (ik)^2 (F4-F5/k^2)
 // =========================================================================
-__global__ void k_near(DevGeom g, NearData nd, cd k, cd invk2, cd *M, size_t ld, const double *fq) {
+__global__ void k_near(DevGeom g, NearData nd, cd k, cd invk2, cd *M, size_t ld, const double *fq, float2 *Fc,
+                       size_t ldf) {
   if (fq) {
     k = cd{fq[0], fq[1]};
     invk2 = dev_invk2(fq[0], fq[1]);
@@ -792,14 +799,20 @@ __global__ void k_near(DevGeom g, NearData nd, cd k, cd invk2, cd *M, size_t ld,
   acc = cadd(acc, cadd(t0, cadd(t1, t2)));
   M[(size_t)a + (size_t)b * ld] = acc;
   if (a != b) M[(size_t)b + (size_t)a * ld] = acc;
+  if (Fc) {   // the complex64 copy
+    const float2 f = make_float2((float)acc.r, (float)acc.i);
+    Fc[(size_t)a + (size_t)b * ldf] = f;
+    if (a != b) Fc[(size_t)b + (size_t)a * ldf] = f;
+  }
 }
 
-int assemble_near(bg_geometry *g, double wr, double wi, void *M, size_t ld, const double *fq) {
+int assemble_near(bg_geometry *g, double wr, double wi, void *M, size_t ld, const double *fq, void *F, size_t ldf) {
   NearData &nd = g->near;
   if (nd.npairs == 0) return BG_OK;
   double d = (wr * wr - wi * wi) * (wr * wr - wi * wi) + 4 * wr * wr * wi * wi;
   cd invk2{(wr * wr - wi * wi) / d, -2 * wr * wi / d};
-  k_near<<<(nd.npairs + 127) / 128, 128, 0, stream()>>>(g->dev, nd, cd{wr, wi}, invk2, (cd *)M, ld, fq);
+  k_near<<<(nd.npairs + 127) / 128, 128, 0, stream()>>>(g->dev, nd, cd{wr, wi}, invk2, (cd *)M, ld, fq,
+                                                       (float2 *)F, ldf);
   BG_LAUNCHED();
   return BG_OK;
 }
@@ -811,7 +824,7 @@ int assemble_near(bg_geometry *g, double wr, double wi, void *M, size_t ld, cons
 // Added to M(a,b) and M(b,a) for b >= a (the reference adds the full row and
 // its symmetric fill then overwrites the lower triangle with the upper).
 // =========================================================================
-__global__ void k_gram(DevGeom g, double w, cd *M, size_t ld, const double *fq) {
+__global__ void k_gram(DevGeom g, double w, cd *M, size_t ld, const double *fq, float2 *F, size_t ldf) {
   if (fq) w = fq[0];
   int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= g.N) return;
@@ -874,19 +887,27 @@ __global__ void k_gram(DevGeom g, double w, cd *M, size_t ld, const double *fq) 
     int b = idx[i];
     if (b < a) continue;
     cd *p = M + (size_t)a + (size_t)b * ld;
-    *p = cadd(*p, val[i]);
+    const cd v = cadd(*p, val[i]);
+    *p = v;
     if (b != a) {
       cd *q = M + (size_t)b + (size_t)a * ld;
       *q = cadd(*q, val[i]);
     }
+    if (F) {   // the final value of these entries: the complex64 copy
+      F[(size_t)a + (size_t)b * ldf] = make_float2((float)v.r, (float)v.i);
+      if (b != a) {
+        const cd *q = M + (size_t)b + (size_t)a * ld;
+        F[(size_t)b + (size_t)a * ldf] = make_float2((float)q->r, (float)q->i);
+      }
+    }
   }
 }
 
-int assemble_gram(bg_geometry *g, double wr, double wi, void *M, size_t ld, const double *fq) {
+int assemble_gram(bg_geometry *g, double wr, double wi, void *M, size_t ld, const double *fq, void *F, size_t ldf) {
   if (g->dispersive && fq) { set_error("frequency-dependent materials need a host frequency"); return BG_ERR_ARG; }
   int st = refresh_materials(g, wr, wi);
   if (st) return st;
-  k_gram<<<(g->N + 127) / 128, 128, 0, stream()>>>(g->dev, wr, (cd *)M, ld, fq);
+  k_gram<<<(g->N + 127) / 128, 128, 0, stream()>>>(g->dev, wr, (cd *)M, ld, fq, (float2 *)F, ldf);
   BG_LAUNCHED();
   return BG_OK;
 }

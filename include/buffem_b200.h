@@ -218,6 +218,12 @@ void bg_matrix_destroy(bg_matrix *m);
    :321-360) + symmetric fill.  A matrix of the wrong size is an error
    (BG_ERR_ARG) instead of the reference's silent reallocation. */
 int bg_assemble(bg_geometry *g, double omega_re, double omega_im, bg_matrix *m);
+/* bg_assemble into m (BG_C128) that also writes f (BG_C64, same N) = m
+   converted to complex64 (as bg_matrix_convert would) in the same kernels:
+   the copy the mixed-precision solvers run on, without a separate pass over
+   the complex128 matrix.  No reference counterpart (the reference assembles
+   one precision). */
+int bg_assemble_with_copy(bg_geometry *g, double omega_re, double omega_im, bg_matrix *m, bg_matrix *f);
 
 /* HMatrix::GetEntries / ExportToMATLAB equivalent: copy the whole matrix
    (or its LU factors after bg_lu_factor) to host memory, column-major,

@@ -83,6 +83,23 @@ def test_c64_factors_partial_pivoting(N):
     assert np.linalg.norm(PA - L @ U) <= 4 * np.sqrt(N) * 2.0 ** -11 * np.linalg.norm(A)
 
 
+@pytest.mark.parametrize("which", ["sphere3", "sphere677"])
+def test_assemble_with_copy_matches_convert(sphere, ref_mesh, which):
+    """bg_assemble_with_copy writes the complex64 copy in the assembly
+    kernels themselves: the complex128 matrix is the plain assembly's and the
+    copy equals its conversion, bit for bit (far, near and Gram entries; odd
+    N with a padded complex64 leading dimension for Sphere_677)."""
+    path = sphere(3) if which == "sphere3" else ref_mesh("sphere677")
+    G = vie_pair(path, 4 + 0.2j)
+    w = 0.8 + 0.05j
+    A = G.AssembleVIEMatrix(w).download()
+    M, F = G.AssembleVIEMatrixWithCopy(w)
+    np.testing.assert_array_equal(M.download(), A)
+    C = G.AllocateVIEMatrix(buffem.BG_C64).convert_from(M)
+    np.testing.assert_array_equal(F.download(), C.download())
+    np.testing.assert_array_equal(F.download(), A.astype(np.complex64))
+
+
 def test_mixed_singular_reports_info():
     from test_gpu_parity import RawMatrix
     M = RawMatrix(50)
