@@ -133,6 +133,16 @@ def test_get_fields_rejects_bad_arguments(buffem_lib, ref_mesh):
         G.GetFields(None, np.zeros(G.TotalBFs + 1, complex), 1.0, X)
 
 
+def test_assemble_with_copy_rejects_missing_matrices(buffem_lib, ref_mesh):
+    """The assembly with a complex64 copy checks its handles before any device
+    work: a missing geometry, matrix or copy is BG_ERR_ARG with a message."""
+    L = buffem_lib.lib()
+    G = buffem_lib.SWGGeometry(meshfiles=ref_mesh("sphere48"), materials=buffem_lib.Material(eps=10.0))
+    assert L.bg_assemble_with_copy(None, 1.0, 0.0, None, None) == buffem_lib.BG_ERR_ARG
+    assert L.bg_assemble_with_copy(G.h, 1.0, 0.0, None, None) == buffem_lib.BG_ERR_ARG
+    assert b"bg_assemble_with_copy" in L.bg_last_error()
+
+
 def test_neq_entry_points_reject_bad_arguments(buffem_lib, ref_mesh):
     """buff-neq's entry points check their arguments before any device work."""
     L = buffem_lib.lib()
